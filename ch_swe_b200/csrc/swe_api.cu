@@ -1,0 +1,905 @@
+// swe_api.cu -- C ABI (include/chswe.h) of the B200 shallow-water step: context
+// and state-vector management, host-side FP64 geometry, kernel launches and
+// CUDA-graph capture of the RK4 loop.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chswe.h"
+#include "swe_common.cuh"
+#include "swe_kernels.cuh"
+
+namespace chswe {
+
+// ---------------------------------------------------------------------------
+// cube geometry (host)
+// ---------------------------------------------------------------------------
+
+// Panel frames of the reference's cube (cubed_sphere_topology_mod.f90:29-55):
+// panel corner R*N + (i-1) EX + (j-1) EY on the integer lattice [0,N]^3, inward normal NRM.
+static const int EX[NPAN][3] = {{-1, 0, 0}, {0, 0, -1}, {1, 0, 0}, {0, 0, 1}, {1, 0, 0}, {1, 0, 0}};
+static const int EY[NPAN][3] = {{0, 1, 0}, {0, 1, 0}, {0, 1, 0}, {0, 1, 0}, {0, 0, 1}, {0, 0, -1}};
+static const int NRM[NPAN][3] = {{0, 0, 1}, {-1, 0, 0}, {0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
+static const int ORG[NPAN][3] = {{1, 0, 0}, {1, 0, 1}, {0, 0, 1}, {0, 0, 0}, {0, 0, 0}, {0, 1, 1}};
+
+static void lattice_point(int p, int i, int j, int n, int out[3])
+{
+    for (int d = 0; d < 3; d++) out[d] = n * ORG[p][d] + (i - 1) * EX[p][d] + (j - 1) * EY[p][d];
+}
+
+static void side_ij(int n, int s, int a, int &i, int &j)
+{
+    switch (s) {
+    case SIDE_L: i = 1; j = a; break;
+    case SIDE_R: i = n + 1; j = a; break;
+    case SIDE_B: i = a; j = 1; break;
+    default: i = a; j = n + 1; break;
+    }
+}
+
+// Edge connectivity from the lattice: two vertices of side s of panel p are
+// located on the sides of the other panels; their order gives the direction.
+// The covariant component continuing across the edge keeps its sign when the
+// coordinate that increases outward from p increases inward on the neighbour.
+static void compute_links(Link L[NPAN][4])
+{
+    const int n = 4;
+    for (int p = 0; p < NPAN; p++)
+        for (int s = 0; s < 4; s++) {
+            int i1, j1, i2, j2, P1[3], P2[3];
+            side_ij(n, s, 2, i1, j1);
+            side_ij(n, s, 3, i2, j2);
+            lattice_point(p, i1, j1, n, P1);
+            lattice_point(p, i2, j2, n, P2);
+            L[p][s] = Link{-1, -1, 0, 0, 0};
+            for (int q = 0; q < NPAN; q++) {
+                if (q == p) continue;
+                for (int s2 = 0; s2 < 4; s2++) {
+                    int a1 = -1, a2 = -1;
+                    for (int a = 1; a <= n + 1; a++) {
+                        int ii, jj, X[3];
+                        side_ij(n, s2, a, ii, jj);
+                        lattice_point(q, ii, jj, n, X);
+                        if (X[0] == P1[0] && X[1] == P1[1] && X[2] == P1[2]) a1 = a;
+                        if (X[0] == P2[0] && X[1] == P2[1] && X[2] == P2[2]) a2 = a;
+                    }
+                    if (a1 > 0 && a2 > 0) {
+                        int rev = a2 < a1;
+                        int out_p = (s == SIDE_R || s == SIDE_T) ? 1 : -1;
+                        int in_q = (s2 == SIDE_L || s2 == SIDE_B) ? 1 : -1;
+                        L[p][s] = Link{q, s2, rev, out_p * in_q, rev ? -1 : 1};
+                    }
+                }
+            }
+        }
+}
+
+// Host FP64 metric of the equiangular panel (metric_2d_ecs_mod.f90:338-411):
+// X = tan(alpha), Y = tan(beta), sigma = sqrt(1 + X^2 + Y^2).
+struct HostMetric {
+    int nx, ny;
+    std::vector<double> J, Q1, Q2, Q3;   // [j][i], panel independent
+};
+
+static HostMetric host_metric(int N, double shift_i, double shift_j)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    HostMetric m;
+    m.nx = shift_i == 0.0 ? N + 1 : N;
+    m.ny = shift_j == 0.0 ? N + 1 : N;
+    const double a0 = -0.25 * pi, a1 = 0.25 * pi;
+    const double hx = (a1 - a0) / ((double)m.nx - 1 + 2.0 * shift_i);
+    const double hy = (a1 - a0) / ((double)m.ny - 1 + 2.0 * shift_j);
+    m.J.resize((size_t)m.nx * m.ny); m.Q1 = m.J; m.Q2 = m.J; m.Q3 = m.J;
+    for (int j = 1; j <= m.ny; j++) {
+        double tb = std::tan(a0 + (j - 1 + shift_j) * hy);
+        for (int i = 1; i <= m.nx; i++) {
+            double ta = std::tan(a0 + (i - 1 + shift_i) * hx);
+            double sg = std::sqrt(1.0 + ta * ta + tb * tb), s2 = sg * sg;
+            size_t k = (size_t)(j - 1) * m.nx + (i - 1);
+            m.Q1[k] = s2 / (1.0 + ta * ta);
+            m.Q2[k] = s2 * ta * tb / ((1 + ta * ta) * (1 + tb * tb));
+            m.Q3[k] = s2 / (1.0 + tb * tb);
+            m.J[k] = (1.0 + ta * ta) * (1.0 + tb * tb) / (sg * sg * sg);
+        }
+    }
+    return m;
+}
+
+// Unit position vector of an xy vertex on panel p (ecs_proto2realface, identity rotation).
+static void vertex_r(int N, int p, int i, int j, double r[3])
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    double ta = std::tan(-0.25 * pi + (i - 1) * hx), tb = std::tan(-0.25 * pi + (j - 1) * hx);
+    double sg = std::sqrt(1.0 + ta * ta + tb * tb);
+    double rp[3] = {ta / sg, tb / sg, 1.0 / sg};
+    for (int d = 0; d < 3; d++) r[d] = EX[p][d] * rp[0] + EY[p][d] * rp[1] - NRM[p][d] * rp[2];
+}
+
+// Proto-face tangent vectors (metric_2d_ecs_mod.f90:136-199) for the vector-sync weights.
+static void a1p(double al, double be, double a[3])
+{
+    double ta = std::tan(al), tb = std::tan(be);
+    double s = std::pow(1.0 + std::pow(ta, 2.0) + std::pow(tb, 2.0), 1.5);
+    a[0] = (1.0 + std::pow(ta, 2.0)) * (1.0 + std::pow(tb, 2.0)) / s;
+    a[1] = -ta * tb * (1.0 + std::pow(ta, 2.0)) / s;
+    a[2] = -ta * (1.0 + std::pow(ta, 2.0)) / s;
+}
+static void a2p(double al, double be, double a[3])
+{
+    double ta = std::tan(al), tb = std::tan(be);
+    double s = std::pow(1.0 + std::pow(ta, 2.0) + std::pow(tb, 2.0), 1.5);
+    a[0] = -ta * tb * (1.0 + std::pow(tb, 2.0)) / s;
+    a[1] = (1.0 + std::pow(ta, 2.0)) * (1.0 + std::pow(tb, 2.0)) / s;
+    a[2] = -tb * (1.0 + std::pow(tb, 2.0)) / s;
+}
+static void b1p(double al, double be, double b[3])
+{
+    double ta = std::tan(al), tb = std::tan(be), sg = std::sqrt(1.0 + ta * ta + tb * tb);
+    b[0] = (1.0 + tb * tb - (ta * tb) * (ta * tb) / (1.0 + ta * ta)) / sg;
+    b[1] = 0.0;
+    b[2] = -ta * (1.0 + tb * tb / (1 + ta * ta)) / sg;
+}
+static void b2p(double al, double be, double b[3])
+{
+    double ta = std::tan(al), tb = std::tan(be), sg = std::sqrt(1.0 + ta * ta + tb * tb);
+    b[0] = 0.0;
+    b[1] = ((1 + ta * ta) - (ta * tb) * (ta * tb) / (1 + tb * tb)) / sg;
+    b[2] = -tb * (ta * ta / (1 + tb * tb) + 1.0) / sg;
+}
+
+// Covariant ECS vector-sync weights (ecs_Ah_vec_sync_factory_mod.f90:97-158).
+static void sync_weights(int N, std::vector<double> &qb, std::vector<double> &qt, std::vector<double> &ql,
+                         std::vector<double> &qr)
+{
+    const double pi = 3.141592653589793238462643383279502884, q = 0.25 * pi;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    qb.resize(N + 1); qt.resize(N + 1); ql.resize(N + 1); qr.resize(N + 1);
+    for (int i = 1; i <= N + 1; i++) {
+        double al = -0.25 * pi + (i - 1) * hx, a[3], v[3];
+        a2p(al, -q, a); b1p(al, q, v);
+        qb[i - 1] = a[0] * v[0] + a[1] * (-v[2]) + a[2] * v[1];
+        a2p(al, q, a); b1p(al, -q, v);
+        qt[i - 1] = a[0] * v[0] + a[1] * v[2] + a[2] * (-v[1]);
+        double be = al;
+        a1p(-q, be, a); b2p(q, be, v);
+        ql[i - 1] = a[0] * (-v[2]) + a[1] * v[1] + a[2] * v[0];
+        a1p(q, be, a); b2p(-q, be, v);
+        qr[i - 1] = a[0] * v[2] + a[1] * v[1] + a[2] * (-v[0]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SBP 4-2 tables
+// ---------------------------------------------------------------------------
+template <class T>
+static void fill_tables(OpTab<T> op[4], T sat[8])
+{
+    auto set = [](T *w, double a, double b, double c, double d, double e) {
+        w[0] = T(a); w[1] = T(b); w[2] = T(c); w[3] = T(d); w[4] = T(e);
+    };
+    std::memset(op, 0, sizeof(OpTab<T>) * 4);
+    // difference nodes -> centres (sbp_diff_i2c_42_mod.f90:12-20)
+    {
+        const double q11 = -79.0 / 78.0, q12 = 27.0 / 26.0, q13 = -1.0 / 26.0, q14 = 1.0 / 78.0, q21 = 2.0 / 21.0,
+                     q22 = -9.0 / 7.0, q23 = 9.0 / 7.0, q24 = -2.0 / 21.0, q31 = 1.0 / 75.0, q33 = -27.0 / 25.0,
+                     q34 = 83.0 / 75.0, q35 = -1.0 / 25.0;
+        OpTab<T> &o = op[OP_DI2C];
+        o.L = 3;
+        o.lstart[0] = o.lstart[1] = o.lstart[2] = 1;
+        set(o.lw[0], q11, q12, q13, q14, 0);
+        set(o.lw[1], q21, q22, q23, q24, 0);
+        set(o.lw[2], q31, 0, q33, q34, q35);
+        o.rstart[0] = -2; set(o.rw[0], -q14, -q13, -q12, -q11, 0);
+        o.rstart[1] = -2; set(o.rw[1], -q24, -q23, -q22, -q21, 0);
+        o.rstart[2] = -3; set(o.rw[2], -q35, -q34, -q33, 0, -q31);
+        o.ioff = -1; set(o.iw, 1.0 / 24.0, -27.0 / 24.0, 27.0 / 24.0, -1.0 / 24.0, 0);
+    }
+    // difference centres -> nodes (sbp_diff_c2i_42_mod.f90:12-22)
+    {
+        const double q11 = -2.0, q12 = 3.0, q13 = -1.0, q21 = -1.0, q22 = 1.0, q31 = 1.0 / 24.0, q32 = -9.0 / 8.0,
+                     q33 = 9.0 / 8.0, q34 = -1.0 / 24.0, q41 = -1.0 / 71.0, q42 = 6.0 / 71.0, q43 = -83.0 / 71.0,
+                     q44 = 81.0 / 71.0, q45 = -3.0 / 71.0;
+        OpTab<T> &o = op[OP_DC2I];
+        o.L = 4;
+        o.lstart[0] = o.lstart[1] = o.lstart[2] = o.lstart[3] = 1;
+        set(o.lw[0], q11, q12, q13, 0, 0);
+        set(o.lw[1], q21, q22, 0, 0, 0);
+        set(o.lw[2], q31, q32, q33, q34, 0);
+        set(o.lw[3], q41, q42, q43, q44, q45);
+        o.rstart[0] = -3; set(o.rw[0], -q13, -q12, -q11, 0, 0);
+        o.rstart[1] = -2; set(o.rw[1], -q22, -q21, 0, 0, 0);
+        o.rstart[2] = -4; set(o.rw[2], -q34, -q33, -q32, -q31, 0);
+        o.rstart[3] = -5; set(o.rw[3], -q45, -q44, -q43, -q42, -q41);
+        o.ioff = -2; set(o.iw, 1.0 / 24.0, -27.0 / 24.0, 27.0 / 24.0, -1.0 / 24.0, 0);
+    }
+    const double c13 = 0.1264926207034815, c14 = -0.029892648949074313;
+    // interpolation nodes -> centres (sbp_interp_i2c_42_mod.f90:18-35)
+    {
+        const double q11 = 1.0 / 2.0 + c13 + 2.0 * c14, q12 = 1.0 / 2.0 - 2.0 * c13 - 3.0 * c14, q13 = c13, q14 = c14,
+                     q21 = -8.0 / 63.0 - 52.0 / 21.0 * c13 - 104.0 / 21.0 * c14,
+                     q22 = 29.0 / 42.0 + 104.0 / 21.0 * c13 + 52.0 / 7.0 * c14, q23 = -52.0 / 21.0 * c13 + 1.0 / 2.0,
+                     q24 = -52.0 / 21.0 * c14 - 4.0 / 63.0, q31 = 26.0 / 25.0 * c13 + 52.0 / 25.0 * c14 - 1.0 / 25.0,
+                     q32 = -1.0 / 50.0 - 52.0 / 25.0 * c13 - 78.0 / 25.0 * c14, q33 = 3.0 / 5.0 + 26.0 / 25.0 * c13,
+                     q34 = 13.0 / 25.0 + 26.0 / 25.0 * c14, q35 = -3.0 / 50.0;
+        OpTab<T> &o = op[OP_II2C];
+        o.L = 3;
+        o.lstart[0] = o.lstart[1] = o.lstart[2] = 1;
+        set(o.lw[0], q11, q12, q13, q14, 0);
+        set(o.lw[1], q21, q22, q23, q24, 0);
+        set(o.lw[2], q31, q32, q33, q34, q35);
+        o.rstart[0] = -2; set(o.rw[0], q14, q13, q12, q11, 0);
+        o.rstart[1] = -2; set(o.rw[1], q24, q23, q22, q21, 0);
+        o.rstart[2] = -3; set(o.rw[2], q35, q34, q33, q32, q31);
+        o.ioff = -1; set(o.iw, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0, 0);
+    }
+    // interpolation centres -> nodes (sbp_interp_c2i_42_mod.f90:13-27)
+    {
+        const double q11 = 39.0 / 28.0 + 39.0 / 14.0 * c13 + 39.0 / 7.0 * c14,
+                     q12 = -2.0 / 7.0 - 39.0 / 7.0 * c13 - 78.0 / 7.0 * c14,
+                     q13 = 39.0 / 14.0 * c13 + 39.0 / 7.0 * c14 - 3.0 / 28.0,
+                     q21 = 13.0 / 27.0 - 52.0 / 27.0 * c13 - 26.0 / 9.0 * c14,
+                     q22 = 29.0 / 54.0 + 104.0 / 27.0 * c13 + 52.0 / 9.0 * c14,
+                     q23 = -1.0 / 54.0 - 52.0 / 27.0 * c13 - 26.0 / 9.0 * c14, q31 = 13.0 / 12.0 * c13,
+                     q32 = -13.0 / 6.0 * c13 + 7.0 / 16.0, q33 = 5.0 / 8.0 + 13.0 / 12.0 * c13, q34 = -1.0 / 16.0,
+                     q41 = 78.0 / 71.0 * c14, q42 = -156.0 / 71.0 * c14 - 4.0 / 71.0,
+                     q43 = 39.0 / 71.0 + 78.0 / 71.0 * c14, q44 = 81.0 / 142.0, q45 = -9.0 / 142.0;
+        OpTab<T> &o = op[OP_IC2I];
+        o.L = 4;
+        o.lstart[0] = o.lstart[1] = o.lstart[2] = o.lstart[3] = 1;
+        set(o.lw[0], q11, q12, q13, 0, 0);
+        set(o.lw[1], q21, q22, q23, 0, 0);
+        set(o.lw[2], q31, q32, q33, q34, 0);
+        set(o.lw[3], q41, q42, q43, q44, q45);
+        o.rstart[0] = -3; set(o.rw[0], q13, q12, q11, 0, 0);
+        o.rstart[1] = -3; set(o.rw[1], q23, q22, q21, 0, 0);
+        o.rstart[2] = -4; set(o.rw[2], q34, q33, q32, q31, 0);
+        o.rstart[3] = -5; set(o.rw[3], q45, q44, q43, q42, q41);
+        o.ioff = -2; set(o.iw, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0, 0);
+    }
+    const double R11 = 15.0 / 8.0, R12 = -5.0 / 4.0, R13 = 3.0 / 8.0;
+    sat[0] = T(0.5 * R11 / (13.0 / 12.0));
+    sat[1] = T(0.5 * R12 / (7.0 / 8.0));
+    sat[2] = T(0.5 * R13 / (25.0 / 24.0));
+    sat[3] = T(0.5 / (7.0 / 18.0));
+    sat[4] = T(R11); sat[5] = T(R12); sat[6] = T(R13); sat[7] = T(0);
+}
+
+}  // namespace chswe
+
+using namespace chswe;
+
+// ---------------------------------------------------------------------------
+// context and state vectors
+// ---------------------------------------------------------------------------
+
+template <class T>
+struct DevMetric {
+    T *base = nullptr;   // one allocation for everything below
+    MetricView<T> v{};
+};
+
+struct swe_ctx {
+    swe_cfg cfg{};
+    Dims dims{};
+    int device = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    size_t elem = 8;                 // bytes per element
+    size_t box_elems = 0;            // elements of one state vector (all members)
+    // device metric (the context uses the one matching its precision)
+    DevMetric<double> m64;
+    DevMetric<float> m32;
+    double *Hm = nullptr;            // per-member H (device)
+    std::vector<double> Hhost;
+    // scratch (stage buffers and contravariant intermediates)
+    void *ya = nullptr, *yb = nullptr, *acc = nullptr, *w = nullptr;
+    // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x meshes, [N+1][P]
+    double *qw = nullptr;
+    double *red = nullptr;           // reduction partials
+    // captured RK4 step
+    cudaGraphExec_t graph = nullptr;
+    const void *graph_v0 = nullptr;
+    double graph_dt = 0.0;
+    int graph_kernels = 0;
+};
+
+struct swe_stvec {
+    swe_ctx *ctx = nullptr;
+    void *d = nullptr;       // state
+    float *cmp = nullptr;    // Kahan compensation of the FP32 RK4 state update
+};
+
+static int fail(swe_ctx *c, int code, const char *fmt, ...)
+{
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CU(ctx, call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail((ctx), SWE_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static bool g_tables_ready[64] = {false};
+
+static int upload_tables(swe_ctx *c)
+{
+    if (c->device >= 0 && c->device < 64 && g_tables_ready[c->device]) return SWE_OK;
+    OpTab<double> o64[4];
+    OpTab<float> o32[4];
+    double s64[8];
+    float s32[8];
+    fill_tables<double>(o64, s64);
+    fill_tables<float>(o32, s32);
+    Link L[NPAN][4];
+    compute_links(L);
+    CU(c, cudaMemcpyToSymbol(c_op64, o64, sizeof(o64)));
+    CU(c, cudaMemcpyToSymbol(c_op32, o32, sizeof(o32)));
+    CU(c, cudaMemcpyToSymbol(c_sat64, s64, sizeof(s64)));
+    CU(c, cudaMemcpyToSymbol(c_sat32, s32, sizeof(s32)));
+    CU(c, cudaMemcpyToSymbol(c_link, L, sizeof(L)));
+    if (c->device >= 0 && c->device < 64) g_tables_ready[c->device] = true;
+    return SWE_OK;
+}
+
+// Build the metric arrays in FP64 on the host and store them in precision T.
+template <class T>
+static int build_metric(swe_ctx *c, DevMetric<T> &dm)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t box = (size_t)(N + 1) * P;
+    // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1
+    const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1);
+    std::vector<T> h(n_el, T(0));
+    HostMetric my = host_metric(N, 0.5, 0.0), mx = host_metric(N, 0.0, 0.5), mxy = host_metric(N, 0.0, 0.0);
+    const double a = c->cfg.radius;
+    T *Q11y = h.data(), *iJy = Q11y + box, *Jy = iJy + box, *Q22x = Jy + box, *iJx = Q22x + box, *Jx = iJx + box,
+      *JQ12 = Jx + box, *iJa = JQ12 + box, *fJ2 = iJa + box, *qb = fJ2 + 6 * box, *qt = qb + (N + 1),
+      *ql = qt + (N + 1), *qr = ql + (N + 1);
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N; i++) {
+            size_t k = (size_t)(j - 1) * my.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            Q11y[o] = T(my.Q1[k]); iJy[o] = T(1.0 / my.J[k]); Jy[o] = T(my.J[k]);
+        }
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            size_t k = (size_t)(j - 1) * mx.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            Q22x[o] = T(mx.Q3[k]); iJx[o] = T(1.0 / mx.J[k]); Jx[o] = T(mx.J[k]);
+        }
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            size_t k = (size_t)(j - 1) * mxy.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            JQ12[o] = T(mxy.J[k] * mxy.Q2[k]);
+            iJa[o] = T(1.0 / (mxy.J[k] * a));
+            for (int p = 0; p < NPAN; p++) {
+                double f;
+                if (c->cfg.coriolis_constant) {
+                    f = c->cfg.omega;
+                } else {
+                    double r[3];
+                    vertex_r(N, p, i, j, r);
+                    const double *ax = c->cfg.rotation_axis;
+                    double pr = (ax[0] * r[0] + ax[1] * r[1] + ax[2] * r[2]) /
+                                std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                    f = 2 * c->cfg.omega * pr;
+                }
+                fJ2[p * box + o] = T(f * mxy.J[k] * mxy.J[k]);
+            }
+        }
+    std::vector<double> vb, vt, vl, vr;
+    sync_weights(N, vb, vt, vl, vr);
+    for (int i = 0; i <= N; i++) { qb[i] = T(vb[i]); qt[i] = T(vt[i]); ql[i] = T(vl[i]); qr[i] = T(vr[i]); }
+
+    T *d = nullptr;
+    if (cudaMalloc(&d, n_el * sizeof(T)) != cudaSuccess) return fail(c, SWE_ENOMEM, "metric allocation failed");
+    dm.base = d;
+    CU(c, cudaMemcpy(d, h.data(), n_el * sizeof(T), cudaMemcpyHostToDevice));
+    MetricView<T> &v = dm.v;
+    v.Q11y = d; v.iJy = d + box; v.Jy = d + 2 * box; v.Q22x = d + 3 * box; v.iJx = d + 4 * box; v.Jx = d + 5 * box;
+    v.JQ12 = d + 6 * box; v.iJa = d + 7 * box; v.fJ2 = d + 8 * box;
+    v.qb = d + 14 * box; v.qt = v.qb + (N + 1); v.ql = v.qt + (N + 1); v.qr = v.ql + (N + 1);
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    v.inv_hxa = T(1.0 / (hx * a));
+    v.inv_hx = T(1.0 / hx);
+    v.grav = T(c->cfg.grav);
+    return SWE_OK;
+}
+
+// SBP quadrature weights J hx hy Ax Ay (quadrature_factory_mod.f90:89-188) for xy, y, x meshes.
+static int build_quadrature(swe_ctx *c)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t box = (size_t)(N + 1) * P;
+    std::vector<double> h(3 * box, 0.0);
+    const double AI[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
+    const double AC[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
+    auto coeff = [&](int i, int n, bool iface) {
+        const double *e = iface ? AI : AC;
+        int ne = iface ? 5 : 4;
+        double A = 1.0;
+        if (i <= ne) A = e[i - 1];
+        if (i >= n - ne + 1) A = e[n - i];
+        return A;
+    };
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    HostMetric ms[3] = {host_metric(N, 0.0, 0.0), host_metric(N, 0.5, 0.0), host_metric(N, 0.0, 0.5)};
+    for (int q = 0; q < 3; q++) {
+        const HostMetric &m = ms[q];
+        for (int j = 1; j <= m.ny; j++)
+            for (int i = 1; i <= m.nx; i++) {
+                double Ax = coeff(i, m.nx, m.nx == N + 1), Ay = coeff(j, m.ny, m.ny == N + 1);
+                h[q * box + (size_t)(j - 1) * P + (i - 1)] = m.J[(size_t)(j - 1) * m.nx + (i - 1)] * hx * hx * Ax * Ay;
+            }
+    }
+    if (cudaMalloc(&c->qw, h.size() * sizeof(double)) != cudaSuccess)
+        return fail(c, SWE_ENOMEM, "quadrature allocation failed");
+    CU(c, cudaMemcpy(c->qw, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (cudaMalloc(&c->red, 4096 * sizeof(double)) != cudaSuccess)
+        return fail(c, SWE_ENOMEM, "reduction buffer allocation failed");
+    return SWE_OK;
+}
+
+extern "C" int swe_cfg_default(swe_cfg *cfg)
+{
+    if (!cfg) return SWE_EINVAL;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->N = 32;
+    cfg->precision = SWE_FP64;
+    cfg->n_members = 1;
+    cfg->operator_kind = SWE_OP_LINEAR;
+    cfg->radius = 0.6371229e7;
+    cfg->grav = 9.80616;
+    cfg->omega = 2.0 * 3.141592653589793238462643383279502884 / (23 * 60 * 60 + 56 * 60 + 4);
+    cfg->rotation_axis[0] = 0.0; cfg->rotation_axis[1] = 0.0; cfg->rotation_axis[2] = 1.0;
+    cfg->coriolis_constant = 0;
+    cfg->h_mean = 1000.0;
+    return SWE_OK;
+}
+
+static void free_ctx(swe_ctx *c)
+{
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm);
+    cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w);
+    cudaFree(c->qw); cudaFree(c->red);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+}
+
+static int alloc_box(swe_ctx *c, void **p)
+{
+    size_t bytes = c->box_elems * c->elem;
+    if (cudaMalloc(p, bytes) != cudaSuccess) return fail(c, SWE_ENOMEM, "device allocation of %zu bytes failed", bytes);
+    CU(c, cudaMemset(*p, 0, bytes));
+    return SWE_OK;
+}
+
+extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
+{
+    if (!cfg || !out) return SWE_EINVAL;
+    *out = nullptr;
+    if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
+        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
+        return SWE_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
+    swe_ctx *c = new swe_ctx();
+    c->cfg = *cfg;
+    cudaGetDevice(&c->device);
+    const int N = cfg->N;
+    c->dims.N = N;
+    c->dims.P = (N + 1 + 7) / 8 * 8;
+    c->dims.ps = (int64_t)(N + 1) * c->dims.P;
+    c->dims.fs = NPAN * c->dims.ps;
+    c->dims.ms = 3 * c->dims.fs;
+    c->elem = cfg->precision == SWE_FP64 ? 8 : 4;
+    c->box_elems = (size_t)c->dims.ms * cfg->n_members;
+    int rc = SWE_OK;
+    auto bail = [&](int code) { free_ctx(c); delete c; return code; };
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SWE_ECUDA);
+    c->stream = c->own_stream;
+    if ((rc = upload_tables(c)) != SWE_OK) return bail(rc);
+    if (cfg->precision == SWE_FP64) rc = build_metric<double>(c, c->m64);
+    else rc = build_metric<float>(c, c->m32);
+    if (rc != SWE_OK) return bail(rc);
+    if ((rc = build_quadrature(c)) != SWE_OK) return bail(rc);
+    c->Hhost.assign(cfg->n_members, cfg->h_mean);
+    if (cudaMalloc(&c->Hm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
+    if (cudaMemcpy(c->Hm, c->Hhost.data(), sizeof(double) * cfg->n_members, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(SWE_ECUDA);
+    if ((rc = alloc_box(c, &c->ya)) || (rc = alloc_box(c, &c->yb)) || (rc = alloc_box(c, &c->acc)) ||
+        (rc = alloc_box(c, &c->w)))
+        return bail(rc);
+    *out = c;
+    return SWE_OK;
+}
+
+extern "C" int swe_ctx_destroy(swe_ctx *c)
+{
+    if (!c) return SWE_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+    delete c;
+    return SWE_OK;
+}
+
+extern "C" const char *swe_last_error(const swe_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" int swe_set_stream(swe_ctx *c, void *s)
+{
+    if (!c) return SWE_EINVAL;
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    return SWE_OK;
+}
+
+extern "C" int swe_synchronize(swe_ctx *c)
+{
+    if (!c) return SWE_EINVAL;
+    CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+extern "C" long long swe_launch_count(const swe_ctx *c) { return c ? c->launches : -1; }
+
+extern "C" int swe_set_member_h_mean(swe_ctx *c, int member, double H)
+{
+    if (!c || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    c->Hhost[member] = H;
+    CU(c, cudaMemcpyAsync(c->Hm + member, &c->Hhost[member], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+extern "C" int swe_stvec_create(swe_ctx *c, swe_stvec **out)
+{
+    if (!c || !out) return SWE_EINVAL;
+    swe_stvec *v = new swe_stvec();
+    v->ctx = c;
+    int rc = alloc_box(c, &v->d);
+    if (rc) { delete v; return rc; }
+    *out = v;
+    return SWE_OK;
+}
+
+extern "C" int swe_stvec_destroy(swe_stvec *v)
+{
+    if (!v) return SWE_EINVAL;
+    cudaStreamSynchronize(v->ctx->stream);
+    cudaFree(v->d);
+    cudaFree(v->cmp);
+    delete v;
+    return SWE_OK;
+}
+
+// Packed host member (Fortran per-panel layout) <-> padded device box.
+template <class T>
+static void pack_member(const swe_ctx *c, const double *h, const double *u, const double *v, T *box)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t ps = c->dims.ps, fs = c->dims.fs;
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 0; j <= N; j++)
+            for (int i = 0; i <= N; i++) box[0 * fs + t * ps + (size_t)j * P + i] = T(*h++);
+        for (int j = 0; j <= N; j++)
+            for (int i = 0; i < N; i++) box[1 * fs + t * ps + (size_t)j * P + i] = T(*u++);
+        for (int j = 0; j < N; j++)
+            for (int i = 0; i <= N; i++) box[2 * fs + t * ps + (size_t)j * P + i] = T(*v++);
+    }
+}
+template <class T>
+static void unpack_member(const swe_ctx *c, const T *box, double *h, double *u, double *v)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t ps = c->dims.ps, fs = c->dims.fs;
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 0; j <= N; j++)
+            for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + (size_t)j * P + i]);
+        for (int j = 0; j <= N; j++)
+            for (int i = 0; i < N; i++) *u++ = double(box[1 * fs + t * ps + (size_t)j * P + i]);
+        for (int j = 0; j < N; j++)
+            for (int i = 0; i <= N; i++) *v++ = double(box[2 * fs + t * ps + (size_t)j * P + i]);
+    }
+}
+
+static size_t member_sizes(const swe_ctx *c, size_t *nh, size_t *nu)
+{
+    const size_t N = c->cfg.N;
+    *nh = NPAN * (N + 1) * (N + 1);
+    *nu = NPAN * N * (N + 1);
+    return *nh + 2 * *nu;
+}
+
+static int upload_range(swe_stvec *vec, int m0, int count, const double *h, const double *u, const double *v)
+{
+    swe_ctx *c = vec->ctx;
+    size_t nh, nu;
+    member_sizes(c, &nh, &nu);
+    const size_t mbytes = (size_t)c->dims.ms * c->elem;
+    std::vector<unsigned char> buf(mbytes * count, 0);
+    for (int k = 0; k < count; k++) {
+        if (c->elem == 8)
+            pack_member<double>(c, h + k * nh, u + k * nu, v + k * nu, (double *)(buf.data() + k * mbytes));
+        else
+            pack_member<float>(c, h + k * nh, u + k * nu, v + k * nu, (float *)(buf.data() + k * mbytes));
+    }
+    CU(c, cudaMemcpyAsync((char *)vec->d + m0 * mbytes, buf.data(), buf.size(), cudaMemcpyHostToDevice, c->stream));
+    if (vec->cmp) CU(c, cudaMemsetAsync((char *)vec->cmp + m0 * (size_t)c->dims.ms * 4, 0, (size_t)c->dims.ms * 4 * count, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+static int download_range(const swe_stvec *vec, int m0, int count, double *h, double *u, double *v)
+{
+    swe_ctx *c = vec->ctx;
+    size_t nh, nu;
+    member_sizes(c, &nh, &nu);
+    const size_t mbytes = (size_t)c->dims.ms * c->elem;
+    std::vector<unsigned char> buf(mbytes * count);
+    CU(c, cudaMemcpyAsync(buf.data(), (char *)vec->d + m0 * mbytes, buf.size(), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < count; k++) {
+        if (c->elem == 8)
+            unpack_member<double>(c, (const double *)(buf.data() + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
+        else
+            unpack_member<float>(c, (const float *)(buf.data() + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
+    }
+    return SWE_OK;
+}
+
+extern "C" int swe_stvec_upload(swe_stvec *vec, int member, const double *h, const double *u, const double *v)
+{
+    if (!vec || !h || !u || !v || member < 0 || member >= vec->ctx->cfg.n_members) return SWE_EINVAL;
+    return upload_range(vec, member, 1, h, u, v);
+}
+extern "C" int swe_stvec_download(const swe_stvec *vec, int member, double *h, double *u, double *v)
+{
+    if (!vec || !h || !u || !v || member < 0 || member >= vec->ctx->cfg.n_members) return SWE_EINVAL;
+    return download_range(vec, member, 1, h, u, v);
+}
+extern "C" int swe_stvec_upload_all(swe_stvec *vec, const double *h, const double *u, const double *v)
+{
+    if (!vec || !h || !u || !v) return SWE_EINVAL;
+    return upload_range(vec, 0, vec->ctx->cfg.n_members, h, u, v);
+}
+extern "C" int swe_stvec_download_all(const swe_stvec *vec, double *h, double *u, double *v)
+{
+    if (!vec || !h || !u || !v) return SWE_EINVAL;
+    return download_range(vec, 0, vec->ctx->cfg.n_members, h, u, v);
+}
+
+extern "C" int swe_stvec_device_view(const swe_stvec *vec, void **ptr, size_t *bytes, int *precision, int *pitch)
+{
+    if (!vec) return SWE_EINVAL;
+    if (ptr) *ptr = vec->d;
+    if (bytes) *bytes = vec->ctx->box_elems * vec->ctx->elem;
+    if (precision) *precision = vec->ctx->cfg.precision;
+    if (pitch) *pitch = vec->ctx->dims.P;
+    return SWE_OK;
+}
+
+static int launch_axpby(swe_ctx *c, void *y, const void *v1, const void *v2, double s1, double s2, int acc)
+{
+    const int64_t n = (int64_t)c->box_elems;
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    if (c->elem == 8)
+        k_axpby<double><<<blocks, 256, 0, c->stream>>>((double *)y, (const double *)v1, (const double *)v2, s1, s2, acc, n);
+    else
+        k_axpby<float><<<blocks, 256, 0, c->stream>>>((float *)y, (const float *)v1, (const float *)v2, s1, s2, acc, n);
+    c->launches++;
+    CU(c, cudaGetLastError());
+    return SWE_OK;
+}
+
+extern "C" int swe_stvec_assign(swe_stvec *y, double s1, const swe_stvec *v1, double s2, const swe_stvec *v2)
+{
+    if (!y || !v1 || y->ctx != v1->ctx || (v2 && v2->ctx != y->ctx)) return SWE_EINVAL;
+    return launch_axpby(y->ctx, y->d, v1->d, v2 ? v2->d : nullptr, s1, s2, 0);
+}
+extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, double s2, const swe_stvec *v2)
+{
+    if (!y || !v1 || y->ctx != v1->ctx || (v2 && v2->ctx != y->ctx)) return SWE_EINVAL;
+    return launch_axpby(y->ctx, y->d, v1->d, v2 ? v2->d : nullptr, s1, s2, 1);
+}
+
+// ---------------------------------------------------------------------------
+// operator application and RK4
+// ---------------------------------------------------------------------------
+static dim3 stage_block() { return dim3(32, 8, 1); }
+static dim3 stage_grid(const swe_ctx *c)
+{
+    const int n = c->cfg.N + 1;
+    return dim3((n + 31) / 32, (n + 7) / 8, NPAN * c->cfg.n_members);
+}
+
+template <class T>
+static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
+                          const MetricView<T> &mv)
+{
+    dim3 g = stage_grid(c), b = stage_block();
+    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    StageArgs a{mode, dt, c->Hm};
+    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims,
+                                      mv, a);
+    c->launches += 2;
+}
+
+static void enqueue_apply(swe_ctx *c, void *out, const void *in)
+{
+    if (c->elem == 8) enqueue_stage<double>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, c->m64.v);
+    else enqueue_stage<float>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, c->m32.v);
+}
+
+extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
+{
+    if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    enqueue_apply(c, vout->d, vin->d);
+    CU(c, cudaGetLastError());
+    return SWE_OK;
+}
+
+// One RK4 step as 8 launches: stage s reads yin and writes y1 (double-buffered).
+static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt)
+{
+    void *V = v0->d, *A = c->acc;
+    if (c->elem == 8) {
+        const MetricView<double> &m = c->m64.v;
+        enqueue_stage<double>(c, V, V, c->yb, A, nullptr, 1, dt, m);
+        enqueue_stage<double>(c, c->yb, V, c->ya, A, nullptr, 2, dt, m);
+        enqueue_stage<double>(c, c->ya, V, c->yb, A, nullptr, 3, dt, m);
+        enqueue_stage<double>(c, c->yb, V, nullptr, A, nullptr, 4, dt, m);
+    } else {
+        const MetricView<float> &m = c->m32.v;
+        enqueue_stage<float>(c, V, V, c->yb, A, v0->cmp, 1, dt, m);
+        enqueue_stage<float>(c, c->yb, V, c->ya, A, v0->cmp, 2, dt, m);
+        enqueue_stage<float>(c, c->ya, V, c->yb, A, v0->cmp, 3, dt, m);
+        enqueue_stage<float>(c, c->yb, V, nullptr, A, v0->cmp, 4, dt, m);
+    }
+}
+
+static int ensure_cmp(swe_stvec *v)
+{
+    swe_ctx *c = v->ctx;
+    if (c->elem == 4 && !v->cmp) {
+        size_t bytes = c->box_elems * 4;
+        if (cudaMalloc(&v->cmp, bytes) != cudaSuccess) return fail(c, SWE_ENOMEM, "compensation allocation failed");
+        CU(c, cudaMemsetAsync(v->cmp, 0, bytes, c->stream));
+    }
+    return SWE_OK;
+}
+
+extern "C" int swe_rk4_step(swe_ctx *c, swe_stvec *v0, double dt)
+{
+    if (!c || !v0 || v0->ctx != c) return SWE_EINVAL;
+    int rc = ensure_cmp(v0);
+    if (rc) return rc;
+    enqueue_rk4(c, v0, dt);
+    CU(c, cudaGetLastError());
+    return SWE_OK;
+}
+
+extern "C" int swe_rk4_steps(swe_ctx *c, swe_stvec *v0, double dt, int nsteps)
+{
+    if (!c || !v0 || v0->ctx != c || nsteps < 0) return SWE_EINVAL;
+    int rc = ensure_cmp(v0);
+    if (rc) return rc;
+    if (nsteps == 0) return SWE_OK;
+    if (!c->graph || c->graph_v0 != v0->d || c->graph_dt != dt) {
+        if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+        cudaGraph_t g;
+        long long before = c->launches;
+        CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_rk4(c, v0, dt);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+        c->graph_kernels = (int)(c->launches - before);
+        c->launches = before;
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        c->graph_v0 = v0->d;
+        c->graph_dt = dt;
+    }
+    for (int s = 0; s < nsteps; s++) {
+        CU(c, cudaGraphLaunch(c->graph, c->stream));
+        c->launches += c->graph_kernels;
+    }
+    return SWE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 integrals
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_quad(const T *__restrict__ y, const T *__restrict__ w, const double *__restrict__ qw, Dims d,
+                       double *partial)
+{
+    // blockIdx.x: slice of the rows, blockIdx.y: term (0 mass, 1 <h,h>, 2 <u,ut>, 3 <v,vt>)
+    const int term = blockIdx.y;
+    const int64_t box = (int64_t)(d.N + 1) * d.P;
+    const int64_t n = NPAN * box;
+    double acc = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t t = k / box, o = k % box;
+        int j = (int)(o / d.P) + 1, i = (int)(o % d.P) + 1;
+        const int N = d.N;
+        if (i > N + 1) continue;
+        if (term <= 1) {
+            double h = (double)y[0 * d.fs + t * d.ps + o];
+            acc += (term == 0 ? h : h * h) * qw[o];
+        } else if (term == 2) {
+            if (i > N) continue;
+            acc += (double)y[1 * d.fs + t * d.ps + o] * (double)w[1 * d.fs + t * d.ps + o] * qw[box + o];
+        } else {
+            if (j > N) continue;
+            acc += (double)y[2 * d.fs + t * d.ps + o] * (double)w[2 * d.fs + t * d.ps + o] * qw[2 * box + o];
+        }
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, double *mass, double *energy)
+{
+    if (!c || !vec || vec->ctx != c || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    const int nb = 256;
+    dim3 g(nb, 4), b(256);
+    // contravariant components of this member into the scratch, then the four sums
+    Dims d1 = c->dims;
+    dim3 gs(stage_grid(c).x, stage_grid(c).y, NPAN), bs = stage_block();
+    const size_t mo = (size_t)member * c->dims.ms;
+    if (c->elem == 8) {
+        k_co2contra<double><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
+        k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
+    } else {
+        k_co2contra<float><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
+        k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
+    }
+    c->launches += 2;
+    CU(c, cudaGetLastError());
+    std::vector<double> part(nb * 4);
+    CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    double s[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 4; q++)
+        for (int k = 0; k < nb; k++) s[q] += part[q * nb + k];
+    if (mass) *mass = s[0];
+    if (energy) *energy = 0.5 * c->Hhost[member] * (s[2] + s[3]) + 0.5 * c->cfg.grav * s[1];
+    return SWE_OK;
+}
+
+extern "C" int swe_edge_links(int *out)
+{
+    if (!out) return SWE_EINVAL;
+    Link L[NPAN][4];
+    compute_links(L);
+    for (int p = 0; p < NPAN; p++)
+        for (int s = 0; s < 4; s++) {
+            int *o = out + (p * 4 + s) * 5;
+            o[0] = L[p][s].nb; o[1] = L[p][s].nside; o[2] = L[p][s].rev; o[3] = L[p][s].sn; o[4] = L[p][s].st;
+        }
+    return SWE_OK;
+}

@@ -1,0 +1,68 @@
+// swe_common.cuh -- device-side layout, SBP stencil tables and cube-edge halo
+// reads shared by the shallow-water kernels.
+//
+// Layout in HBM (one allocation per state vector):
+//   [member][field h=0,u=1,v=2][panel 0..5][row j=1..N+1][pitch P >= N+1]
+// Every field uses the (N+1) x P box of the xy mesh: u (y mesh, i = 1..N,
+// j = 1..N+1) leaves column N+1 unused, v (x mesh, i = 1..N+1, j = 1..N)
+// leaves row N+1 unused.  Indices below are the reference's 1-based (i, j).
+#pragma once
+
+#include <cstdint>
+
+namespace chswe {
+
+constexpr int NPAN = 6;
+
+// Sides of a panel: 0 left (i = 1), 1 right (i = N+1), 2 bottom (j = 1), 3 top (j = N+1).
+enum { SIDE_L = 0, SIDE_R = 1, SIDE_B = 2, SIDE_T = 3 };
+
+// One-dimensional SBP 4-2 operators (src/differential_operators/sbp_operators/):
+//   OP_DI2C  difference, nodes -> centres   (sbp_diff_i2c_42_mod.f90)
+//   OP_DC2I  difference, centres -> nodes   (sbp_diff_c2i_42_mod.f90)
+//   OP_II2C  interpolation, nodes -> centres (sbp_interp_i2c_42_mod.f90)
+//   OP_IC2I  interpolation, centres -> nodes (sbp_interp_c2i_42_mod.f90)
+enum { OP_DI2C = 0, OP_DC2I = 1, OP_II2C = 2, OP_IC2I = 3 };
+
+// Each output row k (1..K) reads five consecutive inputs starting at `start`.
+// Rows 1..L use the left closure, rows K-L+1..K the right closure, the rest
+// the interior stencil.
+template <class T>
+struct OpTab {
+    int L;
+    int lstart[4];   // absolute start of left closure rows
+    int rstart[4];   // start = K + rstart[r] for row k = K - r
+    int ioff;        // interior start = k + ioff
+    T lw[4][5];
+    T rw[4][5];
+    T iw[5];
+};
+
+struct Dims {
+    int N;         // cells per panel edge
+    int P;         // row pitch in elements
+    int64_t ps;    // panel stride   = (N+1) * P
+    int64_t fs;    // field stride   = 6 * ps
+    int64_t ms;    // member stride  = 3 * fs
+};
+
+// Edge connectivity: neighbour panel, its side, reversed along-edge order,
+// sign of the normal and tangential covariant components across the edge.
+struct Link {
+    int nb, nside, rev, sn, st;
+};
+
+template <class T>
+struct MetricView {
+    const T *Q11y, *iJy, *Jy;     // y mesh (u points): Qi11, 1/J, J
+    const T *Q22x, *iJx, *Jx;     // x mesh (v points): Qi22, 1/J, J
+    const T *JQ12;                // xy mesh: J * Qi12
+    const T *iJa;                 // xy mesh: 1 / (J * a)
+    const T *fJ2;                 // xy mesh, per panel: f * J * J
+    const T *qb, *qt, *ql, *qr;   // covariant vector-sync weights along the four sides
+    T inv_hxa;                    // 1 / (hx * a)
+    T inv_hx;                     // 1 / hx   (hx == hy)
+    T grav;
+};
+
+}  // namespace chswe

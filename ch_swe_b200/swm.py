@@ -1,0 +1,275 @@
+"""Host-side mirror of the reference's operator_t / stvec_t / timescheme_t API for
+the shallow-water hot path, backed by libchswe.so.
+
+Names, arguments and error behaviour follow the reference (paths relative to the
+ch_swe source tree):
+
+* ``create_domain``        ~ create_domain            (src/domain/domain_factory_mod.f90:55-147)
+* ``create_stvec_swm``     ~ create_stvec_swm         (src/models/shallow_water/stvec/stvec_swm_factory_mod.f90:15-36)
+* ``StvecSwm.assign/update`` ~ stvec_t%assign/update  (src/stvec/stvec_flexible_mod.f90:196-306)
+* ``create_swm_operator``  ~ create_swm_operator      (src/models/shallow_water/operator/operator_swm_factory_mod.f90:14-57)
+* ``OperatorSwmLin.apply`` ~ operator_swm_lin_t%apply (.../operator_swm_lin_mod.f90:66-108)
+* ``create_timescheme``    ~ create_timescheme        (src/time_schemes/timescheme_factory_mod.f90:21-52)
+* ``Rk4.step``             ~ rk4_t%step               (src/time_schemes/rk4_mod.f90:20-42)
+
+Where the reference calls ``parcomm_global%abort`` these raise ``SweError``
+(device/library failures) or ``ValueError`` (unknown names, bad configuration).
+Host arrays use the packed per-panel Fortran layout documented in include/chswe.h.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import SweCfg, SweError, check, dptr
+
+EARTH_RADIUS = 0.6371229e7                                   # const_mod.f90:7
+EARTH_GRAV = 9.80616                                         # const_mod.f90:6
+EARTH_OMEGA = 2.0 * np.pi / (23 * 60 * 60 + 56 * 60 + 4)     # const_mod.f90:8-9
+
+# operator names accepted by the Ch / SBP 4-2 linear operator (gen_config_linear.sh:37-64)
+LINEAR_CH42_NAMES = {
+    "div_op_name": "div_ch_sbp_sat_42_proj",
+    "grad_op_name": "grad_ch_sbp_sat_42",
+    "coriolis_op_name": "coriolis_Ch_sbp42",
+    "co2contra_op_name": "co2contra_ch_sbp42",
+    "quadrature_name": "SBP_C42_quadrature",
+}
+
+
+def state_shapes(N: int, members: int | None = None):
+    """Packed host shapes of (h, u, v) for one member (or a batch of members)."""
+    sh = [(6, N + 1, N + 1), (6, N + 1, N), (6, N, N + 1)]
+    if members is None:
+        return tuple(sh)
+    return tuple((members,) + s for s in sh)
+
+
+@dataclass
+class Domain:
+    """Cubed-sphere domain with Ch staggering; owns the device context."""
+    N: int
+    precision: str = "fp64"
+    n_members: int = 1
+    planet_radius: float = EARTH_RADIUS
+    omega: float = EARTH_OMEGA
+    rotation_axis: tuple = (0.0, 0.0, 1.0)
+    coriolis_constant: bool = False
+    grav: float = EARTH_GRAV
+    h_mean: float = 1000.0
+    horizontal_staggering: str = "Ch"
+    _ctx: int = field(default=None, repr=False)
+
+    def __post_init__(self):
+        if self.horizontal_staggering != "Ch":
+            raise ValueError("domain_factory_mod, unsupported horizontal staggering: " + self.horizontal_staggering)
+        if self.precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        L = _lib.load()
+        cfg = SweCfg()
+        check(L.swe_cfg_default(ctypes.byref(cfg)))
+        cfg.N = int(self.N)
+        cfg.precision = _lib.SWE_FP64 if self.precision == "fp64" else _lib.SWE_FP32
+        cfg.n_members = int(self.n_members)
+        cfg.radius = float(self.planet_radius)
+        cfg.grav = float(self.grav)
+        cfg.omega = float(self.omega)
+        for d in range(3):
+            cfg.rotation_axis[d] = float(self.rotation_axis[d])
+        cfg.coriolis_constant = int(bool(self.coriolis_constant))
+        cfg.h_mean = float(self.h_mean)
+        ctx = ctypes.c_void_p()
+        check(L.swe_ctx_create(ctypes.byref(cfg), ctypes.byref(ctx)), None, "swe_ctx_create")
+        self._ctx = ctx.value
+
+    @property
+    def ctx(self):
+        if not self._ctx:
+            raise SweError("domain was destroyed")
+        return self._ctx
+
+    def synchronize(self):
+        check(_lib.load().swe_synchronize(self.ctx), self.ctx, "swe_synchronize")
+
+    def launch_count(self) -> int:
+        return int(_lib.load().swe_launch_count(self.ctx))
+
+    def set_stream(self, stream_ptr: int | None):
+        check(_lib.load().swe_set_stream(self.ctx, stream_ptr), self.ctx, "swe_set_stream")
+
+    def destroy(self):
+        if self._ctx:
+            _lib.load().swe_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def create_domain(N: int, **kw) -> Domain:
+    return Domain(N=N, **kw)
+
+
+class StvecSwm:
+    """stvec_swm_t on the device: fields h (xy), u (y), v (x) for every member."""
+
+    def __init__(self, domain: Domain):
+        self.domain = domain
+        p = ctypes.c_void_p()
+        check(_lib.load().swe_stvec_create(domain.ctx, ctypes.byref(p)), domain.ctx, "swe_stvec_create")
+        self._p = p.value
+
+    @property
+    def handle(self):
+        return self._p
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p and self.domain._ctx:
+            _lib.load().swe_stvec_destroy(p)
+            self._p = None
+
+    # -- transfers ------------------------------------------------------
+    def upload(self, h, u, v, member: int | None = 0):
+        N = self.domain.N
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        L = _lib.load()
+        if member is None:
+            for a, s in zip(arrs, state_shapes(N, self.domain.n_members)):
+                if a.shape != s:
+                    raise ValueError(f"expected shape {s}, got {a.shape}")
+            rc = L.swe_stvec_upload_all(self._p, *(dptr(a) for a in arrs))
+        else:
+            for a, s in zip(arrs, state_shapes(N)):
+                if a.shape != s:
+                    raise ValueError(f"expected shape {s}, got {a.shape}")
+            rc = L.swe_stvec_upload(self._p, int(member), *(dptr(a) for a in arrs))
+        check(rc, self.domain.ctx, "swe_stvec_upload")
+        return self
+
+    def download(self, member: int | None = 0):
+        N = self.domain.N
+        L = _lib.load()
+        if member is None:
+            out = [np.empty(s) for s in state_shapes(N, self.domain.n_members)]
+            rc = L.swe_stvec_download_all(self._p, *(dptr(a) for a in out))
+        else:
+            out = [np.empty(s) for s in state_shapes(N)]
+            rc = L.swe_stvec_download(self._p, int(member), *(dptr(a) for a in out))
+        check(rc, self.domain.ctx, "swe_stvec_download")
+        return tuple(out)
+
+    # -- stvec algebra (stvec_flexible_mod.f90:196-306) ------------------
+    def assign(self, s1, v1, s2=None, v2=None, domain=None):
+        self._check(v1, v2)
+        rc = _lib.load().swe_stvec_assign(self._p, float(s1), v1._p, float(s2 or 0.0), v2._p if v2 else None)
+        check(rc, self.domain.ctx, "stvec assign")
+        return self
+
+    def update(self, s1, v1, s2=None, v2=None, domain=None):
+        self._check(v1, v2)
+        rc = _lib.load().swe_stvec_update(self._p, float(s1), v1._p, float(s2 or 0.0), v2._p if v2 else None)
+        check(rc, self.domain.ctx, "stvec update")
+        return self
+
+    def create_similar(self) -> "StvecSwm":
+        return StvecSwm(self.domain)
+
+    def copy_to(self, dst: "StvecSwm", domain=None):
+        dst.assign(1.0, self)
+        return dst
+
+    def device_view(self):
+        ptr = ctypes.c_void_p()
+        nb = ctypes.c_size_t()
+        prec = ctypes.c_int()
+        pitch = ctypes.c_int()
+        check(_lib.load().swe_stvec_device_view(self._p, ctypes.byref(ptr), ctypes.byref(nb), ctypes.byref(prec),
+                                                ctypes.byref(pitch)), self.domain.ctx, "device_view")
+        return ptr.value, nb.value, prec.value, pitch.value
+
+    def _check(self, v1, v2):
+        for v in (v1, v2):
+            if v is not None and (not isinstance(v, StvecSwm) or v.domain is not self.domain):
+                raise ValueError("stvec algebra between different domains")
+
+
+def create_stvec_swm(domain: Domain, halo_width: int = 8, halo_width_z: int = 0) -> StvecSwm:
+    """Halo widths are accepted for interface parity; device states carry no halo."""
+    return StvecSwm(domain)
+
+
+class OperatorSwmLin:
+    """operator_swm_lin_t: linear SWE on the Ch grid with SBP 4-2 operators."""
+
+    def __init__(self, domain: Domain, h_mean: float, grav: float):
+        self.domain = domain
+        self.h_mean = float(h_mean)
+        self.grav = float(grav)
+        for m in range(domain.n_members):
+            check(_lib.load().swe_set_member_h_mean(domain.ctx, m, self.h_mean), domain.ctx, "h_mean")
+
+    def set_member_h_mean(self, member: int, h_mean: float):
+        check(_lib.load().swe_set_member_h_mean(self.domain.ctx, int(member), float(h_mean)),
+              self.domain.ctx, "h_mean")
+
+    def apply(self, vout: StvecSwm, vin: StvecSwm, domain: Domain | None = None):
+        if not isinstance(vout, StvecSwm):
+            raise ValueError("swm operator failure: vout of wrong type")
+        if not isinstance(vin, StvecSwm):
+            raise ValueError("swm operator failure: vin of wrong type")
+        check(_lib.load().swe_operator_apply(self.domain.ctx, vout.handle, vin.handle), self.domain.ctx,
+              "operator apply")
+
+    def integrals(self, state: StvecSwm, member: int = 0):
+        """FP64 SBP-quadrature mass and linear energy of one member."""
+        m = ctypes.c_double()
+        e = ctypes.c_double()
+        check(_lib.load().swe_integrals(self.domain.ctx, state.handle, int(member), ctypes.byref(m),
+                                        ctypes.byref(e)), self.domain.ctx, "integrals")
+        return m.value, e.value
+
+
+def create_swm_operator(grav: float, config: dict, domain: Domain, orography_generator=None):
+    kind = config.get("swm_operator_type")
+    if kind != "linear_swm_operator":
+        raise ValueError(f"unknown swm_op_type: {kind}")
+    if "h_mean" not in config:
+        raise ValueError("linear_swm_operator requires h_mean")
+    for key, want in LINEAR_CH42_NAMES.items():
+        got = config.get(key, want)
+        if got != want:
+            raise ValueError(f"unsupported {key}: {got} (this build implements {want})")
+    if abs(float(grav) - domain.grav) > 0.0:
+        raise ValueError(f"grav {grav} differs from the domain's {domain.grav}")
+    return OperatorSwmLin(domain, config["h_mean"], grav)
+
+
+class Rk4:
+    """rk4_t: classic RK4 with k1..k4 fused into per-stage device kernels."""
+
+    def step(self, v0: StvecSwm, operator: OperatorSwmLin, domain: Domain | None, dt: float):
+        check(_lib.load().swe_rk4_step(operator.domain.ctx, v0.handle, float(dt)), operator.domain.ctx, "rk4 step")
+
+    def steps(self, v0: StvecSwm, operator: OperatorSwmLin, domain: Domain | None, dt: float, nsteps: int):
+        check(_lib.load().swe_rk4_steps(operator.domain.ctx, v0.handle, float(dt), int(nsteps)),
+              operator.domain.ctx, "rk4 steps")
+
+
+def create_timescheme(state: StvecSwm, name: str):
+    if name != "rk4":
+        raise ValueError(f"unknown timescheme_name: {name}")
+    return Rk4()
+
+
+def edge_links() -> np.ndarray:
+    """Host-only connectivity table (6, 4, 5): nb, nside, rev, sn, st."""
+    out = (ctypes.c_int * 120)()
+    check(_lib.load().swe_edge_links(out))
+    return np.frombuffer(out, dtype=np.int32).reshape(6, 4, 5).copy()

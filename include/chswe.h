@@ -1,0 +1,123 @@
+/*
+ * chswe.h -- C ABI of the B200 shallow-water time step (ch_swe hot path).
+ *
+ * The entry points mirror the Fortran interfaces a GPU-backed subclass replaces
+ * (paths relative to the ch_swe source tree):
+ *
+ *   swe_stvec_*        <- stvec_t / stvec_swm_t            src/stvec/stvec_mod.f90:10-30,
+ *                                                            src/models/shallow_water/stvec/stvec_swm_mod.f90:10-42
+ *   swe_stvec_create   <- create_stvec_swm                  src/models/shallow_water/stvec/stvec_swm_factory_mod.f90:15-36
+ *   swe_stvec_assign   <- stvec_t%assign(s1, v1, s2, v2)    src/stvec/stvec_flexible_mod.f90:196-250
+ *   swe_stvec_update   <- stvec_t%update(s1, v1, s2, v2)    src/stvec/stvec_flexible_mod.f90:252-306
+ *   swe_ctx_create     <- create_domain + create_swm_operator("linear_swm_operator")
+ *                                                            src/domain/domain_factory_mod.f90:55-147,
+ *                                                            src/models/shallow_water/operator/operator_swm_factory_mod.f90:586-685
+ *   swe_operator_apply <- operator_swm_lin_t%apply(vout, vin, domain)
+ *                                                            src/models/shallow_water/operator/operator_swm_lin_mod.f90:66-108
+ *   swe_rk4_step       <- rk4_t%step(v0, operator, domain, dt)   src/time_schemes/rk4_mod.f90:20-42
+ *   swe_rk4_steps      <- nsteps x rk4_t%step (the driver loop  src/models/shallow_water/shallow_water_mod.f90:112-143)
+ *   swe_integrals      <- quadrature_t%mass / %dot           src/quadrature/abstract_quadrature_mod.f90:29-64
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative SWE_E* code on failure;
+ *    swe_last_error(ctx) gives the message.  The reference has no return codes:
+ *    it calls parcomm_global%abort (src/parallel/parcomm_mod.f90:73-90); a
+ *    Fortran shim maps a nonzero status to that call.
+ *  - Host state arrays use the reference's per-panel Fortran layout p(i,j) with
+ *    halos stripped, panels 1..6 outermost:
+ *       h : (N+1) x (N+1) per panel  (xy mesh)
+ *       u : N     x (N+1) per panel  (y mesh, i fastest: N values per row, N+1 rows)
+ *       v : (N+1) x N     per panel  (x mesh, N+1 values per row, N rows)
+ *    u, v are covariant wind components as in the reference ("covariant" v_components_type).
+ *  - A context owns one CUDA stream (or the one given by swe_set_stream) and
+ *    all device scratch; it is not thread-safe.  Calls are asynchronous on the
+ *    stream except upload/download/integrals, which synchronise it.
+ *  - A context holds n_members ensemble members of the same cube size; every
+ *    operation acts on all members at once.
+ */
+#ifndef CHSWE_H
+#define CHSWE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWE_OK 0
+#define SWE_EINVAL (-1)   /* bad argument or configuration */
+#define SWE_ECUDA (-2)    /* CUDA runtime failure (message holds the CUDA error) */
+#define SWE_ENOMEM (-3)   /* device allocation failed */
+#define SWE_ENODEV (-4)   /* no usable CUDA device (the library has no CPU fallback) */
+
+#define SWE_FP64 0
+#define SWE_FP32 1
+
+#define SWE_OP_LINEAR 0   /* operator_swm_lin_t, Ch staggering, SBP 4-2 */
+
+typedef struct swe_ctx swe_ctx;
+typedef struct swe_stvec swe_stvec;
+
+typedef struct swe_cfg {
+    int N;                    /* cells per panel edge (>= 8) */
+    int precision;            /* SWE_FP64 or SWE_FP32 (FP32 stencils, FP64 metric/reductions, Kahan state) */
+    int n_members;            /* ensemble members held by the context (>= 1) */
+    int operator_kind;        /* SWE_OP_LINEAR */
+    double radius;            /* planet radius, metric%scale        (default 6371229 m) */
+    double grav;              /* gravity                              (default 9.80616) */
+    double omega;             /* rotation rate, metric%omega          (default 2 pi / 86164 s) */
+    double rotation_axis[3];  /* metric%rotation_axis                 (default 0, 0, 1) */
+    int coriolis_constant;    /* metric%coriolis_const: f = omega instead of 2 omega sin(lat) */
+    double h_mean;            /* operator h_mean (H) for every member (default 1000 m) */
+} swe_cfg;
+
+/* Fill *cfg with the defaults listed above. */
+int swe_cfg_default(swe_cfg *cfg);
+
+int swe_ctx_create(const swe_cfg *cfg, swe_ctx **ctx);
+int swe_ctx_destroy(swe_ctx *ctx);
+const char *swe_last_error(const swe_ctx *ctx);
+/* Run the context's work on an existing CUDA stream (cudaStream_t); NULL restores the own stream. */
+int swe_set_stream(swe_ctx *ctx, void *cuda_stream);
+int swe_synchronize(swe_ctx *ctx);
+/* Per-member mean depth H (ensembles with different h_mean). */
+int swe_set_member_h_mean(swe_ctx *ctx, int member, double h_mean);
+
+int swe_stvec_create(swe_ctx *ctx, swe_stvec **vec);
+int swe_stvec_destroy(swe_stvec *vec);
+int swe_stvec_upload(swe_stvec *vec, int member, const double *h, const double *u, const double *v);
+int swe_stvec_download(const swe_stvec *vec, int member, double *h, double *u, double *v);
+/* Whole-batch transfers: arrays hold n_members consecutive member states. */
+int swe_stvec_upload_all(swe_stvec *vec, const double *h, const double *u, const double *v);
+int swe_stvec_download_all(const swe_stvec *vec, double *h, double *u, double *v);
+/* y = s1*v1 + s2*v2 ; v2 may be NULL (then y = s1*v1). */
+int swe_stvec_assign(swe_stvec *y, double s1, const swe_stvec *v1, double s2, const swe_stvec *v2);
+/* y = y + s1*v1 + s2*v2 ; v2 may be NULL. */
+int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, double s2, const swe_stvec *v2);
+/* Device storage of a state vector: element type (SWE_FP64/SWE_FP32), base pointer,
+   bytes, and the pitch/row layout [member][field h,u,v][panel][N+1 rows][pitch]. */
+int swe_stvec_device_view(const swe_stvec *vec, void **ptr, size_t *bytes, int *precision, int *pitch);
+
+/* vout = A(vin), A the linear shallow-water operator. */
+int swe_operator_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
+/* One classic RK4 step of size dt on v0 (in place). */
+int swe_rk4_step(swe_ctx *ctx, swe_stvec *v0, double dt);
+/* nsteps RK4 steps (captured into a CUDA graph after the first call with the same shape). */
+int swe_rk4_steps(swe_ctx *ctx, swe_stvec *v0, double dt, int nsteps);
+/* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
+int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
+
+/* Number of kernel launches issued on the context's stream since creation. */
+long long swe_launch_count(const swe_ctx *ctx);
+
+/* Panel-edge connectivity used by the device halo reads (host-only, no GPU needed):
+   for panel p (0..5) and side s (0 left i=1, 1 right i=N+1, 2 bottom j=1, 3 top j=N+1)
+   writes {neighbour panel, neighbour side, reversed along-edge order,
+           normal-component sign, tangential-component sign} to out[(p*4+s)*5 + 0..4]. */
+int swe_edge_links(int *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,180 @@
+"""ctypes wrapper of the CPU FP64 oracle (oracle/swe_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU legs of ``bench.py`` as the checker.  The product path never imports it.
+
+State arrays use the packed host layout of the drop-in boundary: for each of the
+six panels, Fortran order p(i, j) with i fastest and halos stripped:
+  h : xy mesh, (6, N+1, N+1)   [panel, j, i]
+  u : y  mesh, (6, N+1, N)     covariant alpha-component
+  v : x  mesh, (6, N,   N+1)   covariant beta-component
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+EARTH_RADIUS = 0.6371229e7       # const_mod.f90:7
+EARTH_GRAV = 9.80616             # const_mod.f90:6
+EARTH_OMEGA = 2.0 * np.pi / (23 * 60 * 60 + 56 * 60 + 4)   # const_mod.f90:8-9
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, _dp, ctypes.c_int]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_apply.argtypes = [ctypes.c_void_p] + [_dp] * 6
+        L.orc_rk4.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int]
+        L.orc_grad.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_co2contra.argtypes = [ctypes.c_void_p] + [_dp] * 4
+        L.orc_coriolis.argtypes = [ctypes.c_void_p] + [_dp] * 4
+        L.orc_div.argtypes = [ctypes.c_void_p] + [_dp] * 3
+        L.orc_integrals.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.orc_dot.restype = ctypes.c_double
+        L.orc_dot.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_init_gaussian.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, _dp, _dp, _dp]
+        L.orc_init_ts2.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int,
+                                   _dp, _dp, _dp]
+        L.orc_metric.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_sync_weights.argtypes = [ctypes.c_void_p] + [_dp] * 4
+        L.orc_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def shapes(N: int):
+    return (6, N + 1, N + 1), (6, N + 1, N), (6, N, N + 1)
+
+
+class Oracle:
+    """FP64 CPU restatement of the linear Ch/SBP42 shallow-water operator and RK4."""
+
+    def __init__(self, N: int, radius: float = EARTH_RADIUS, grav: float = EARTH_GRAV,
+                 omega: float = EARTH_OMEGA, h_mean: float = 1000.0, axis=(0.0, 0.0, 1.0),
+                 coriolis_constant: bool = False):
+        self.N = N
+        self.radius, self.grav, self.omega, self.h_mean = radius, grav, omega, h_mean
+        self.axis = np.ascontiguousarray(axis, dtype=np.float64)
+        self._c = lib().orc_create(N, radius, grav, omega, h_mean, _p(self.axis), int(coriolis_constant))
+        if not self._c:
+            raise ValueError(f"oracle: unsupported N={N} (need N >= 8)")
+
+    def __del__(self):
+        c = getattr(self, "_c", None)
+        if c:
+            lib().orc_destroy(c)
+            self._c = None
+
+    def zeros(self):
+        sh, su, sv = shapes(self.N)
+        return np.zeros(sh), np.zeros(su), np.zeros(sv)
+
+    def gaussian(self, lam0=np.pi, phi0=0.0, d0=0.25, amp=1.0):
+        h, u, v = self.zeros()
+        lib().orc_init_gaussian(self._c, lam0, phi0, d0, amp, _p(h), _p(u), _p(v))
+        return h, u, v
+
+    def ts2(self, u0, h_mean, axis=(0.0, 0.0, 1.0), linear_mode=False):
+        h, u, v = self.zeros()
+        ax = np.ascontiguousarray(axis, dtype=np.float64)
+        lib().orc_init_ts2(self._c, u0, h_mean, _p(ax), int(linear_mode), _p(h), _p(u), _p(v))
+        return h, u, v
+
+    def apply(self, h, u, v):
+        dh, du, dv = self.zeros()
+        lib().orc_apply(self._c, _p(np.ascontiguousarray(h)), _p(np.ascontiguousarray(u)),
+                        _p(np.ascontiguousarray(v)), _p(dh), _p(du), _p(dv))
+        return dh, du, dv
+
+    def rk4(self, h, u, v, dt, nsteps=1):
+        h, u, v = (np.array(x, dtype=np.float64, order="C") for x in (h, u, v))
+        lib().orc_rk4(self._c, _p(h), _p(u), _p(v), dt, int(nsteps))
+        return h, u, v
+
+    def grad(self, h):
+        _, gx, gy = self.zeros()
+        lib().orc_grad(self._c, _p(np.ascontiguousarray(h)), _p(gx), _p(gy))
+        return gx, gy
+
+    def co2contra(self, u, v):
+        _, ut, vt = self.zeros()
+        lib().orc_co2contra(self._c, _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)), _p(ut), _p(vt))
+        return ut, vt
+
+    def coriolis(self, ut, vt):
+        _, cu, cv = self.zeros()
+        lib().orc_coriolis(self._c, _p(np.ascontiguousarray(ut)), _p(np.ascontiguousarray(vt)), _p(cu), _p(cv))
+        return cu, cv
+
+    def div(self, ut, vt):
+        d, _, _ = self.zeros()
+        lib().orc_div(self._c, _p(np.ascontiguousarray(ut)), _p(np.ascontiguousarray(vt)), _p(d))
+        return d
+
+    def integrals(self, h, u, v):
+        m = ctypes.c_double()
+        e = ctypes.c_double()
+        lib().orc_integrals(self._c, _p(np.ascontiguousarray(h)), _p(np.ascontiguousarray(u)),
+                            _p(np.ascontiguousarray(v)), ctypes.byref(m), ctypes.byref(e))
+        return m.value, e.value
+
+    def dot(self, mesh: int, a, b=None):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if b is None:
+            return lib().orc_dot(self._c, mesh, _p(a), None)
+        return lib().orc_dot(self._c, mesh, _p(a), _p(np.ascontiguousarray(b, dtype=np.float64)))
+
+    def metric(self, mesh: int, what: int):
+        shp = shapes(self.N)[mesh]
+        out = np.empty(shp)
+        lib().orc_metric(self._c, mesh, what, _p(out))
+        return out
+
+    def sync_weights(self):
+        n = self.N + 1
+        qb, qt, ql, qr = (np.empty(n) for _ in range(4))
+        lib().orc_sync_weights(self._c, _p(qb), _p(qt), _p(ql), _p(qr))
+        return qb, qt, ql, qr
+
+    def halo_probe(self, kind: int, f, f2=None, w: int = 3):
+        """Run one reference exchange on packed field(s); return haloed arrays
+        (6, ny+2w, nx+2w) with NaN where nothing was written."""
+        N = self.N
+        if kind in (0, 1):
+            nx = ny = N + 1
+            nx2, ny2 = nx, ny
+        else:
+            nx, ny, nx2, ny2 = N, N + 1, N + 1, N
+        out = np.empty((6, ny + 2 * w, nx + 2 * w))
+        out2 = np.empty((6, ny2 + 2 * w, nx2 + 2 * w))
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        f2p = _p(np.ascontiguousarray(f2, dtype=np.float64)) if f2 is not None else None
+        lib().orc_halo_probe(self._c, kind, _p(f), f2p, w, _p(out), _p(out2))
+        return (out, out2) if kind != 0 else out
