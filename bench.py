@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: C192 linear shallow-water RK4 on the Ch-staggered cubed sphere.
+
+Workload (one bench step): one simulated day of C192 (6 x 192 x 192 cells),
+dt = 150 s, 576 RK4 steps, Gaussian hill (d0 = 0.15 rad, 1 m) centred on a cube
+corner with a seeded jitter <= 1e-3 rad, H = 1000 m, f = 2 Omega sin(lat).
+Metric: cell-updates/s = 6 N^2 * 576 / seconds (one cell advanced by one full
+RK4 step).  The headline ``value`` is the FP32 path (FP32 stencils, FP64 metric
+precompute and reductions, Kahan-compensated state); the FP64 path is reported
+beside it with the FP32-vs-FP64 relative L2/max errors after the day.
+
+Timing: W untimed warm-up integrations, then K timed integrations; each starts
+from the initial state restored on the device and after an L2 flush (a 512 MiB
+device write), bracketed by CUDA events on the library's stream; max over ranks.
+``--gpus N`` runs N independent replicas (one per GPU, weak scaling, no
+data-path collective).  ``--impl reference`` times the CPU restatement of the
+reference (the Fortran/MPI reference needs mpiifort, absent here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 192
+DT = 150.0
+NSTEPS = 576
+H_MEAN = 1000.0
+SEED = 20261203 + 1
+
+
+def workload_ic(N=N_CELLS, seed=SEED):
+    """Cube-corner Gaussian with seeded jitter (same generator as the test cases)."""
+    from ch_swe_b200 import testcases
+    rng = np.random.default_rng(seed)
+    lam0 = 0.25 * np.pi + rng.uniform(-1e-3, 1e-3)
+    phi0 = np.arcsin(1.0 / np.sqrt(3.0)) + rng.uniform(-1e-3, 1e-3)
+    return testcases.gaussian_hill(N, lam0=lam0, phi0=phi0, d0=0.15, amp=1.0), (lam0, phi0)
+
+
+def cells_per_step(N):
+    return 6 * N * N * NSTEPS
+
+
+def dof(N):
+    return 6 * (N + 1) ** 2 + 12 * N * (N + 1)
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU legs (the oracle): only here and in the reference arm
+# ----------------------------------------------------------------------------
+def _cpu_worker(args):
+    N, steps = args
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    (h, u, v), _ = workload_ic(N)
+    o = Oracle(N, h_mean=H_MEAN)
+    t0 = time.perf_counter()
+    o.rk4(h, u, v, DT, steps)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(steps=40):
+    """Oracle on one host core, bounded sample of the same workload."""
+    from oracle import oracle as orc
+    orc.build()
+    t = _cpu_worker((N_CELLS, steps))
+    return {"value": 6 * N_CELLS * N_CELLS * steps / t, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"C{N_CELLS}, {steps} RK4 steps of the same day (dt {DT:g} s), FP64 CPU restatement, 1 thread"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    from oracle import oracle as orc
+    orc.build()
+    cores = os.cpu_count() or 1
+    steps = 6
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(N_CELLS, steps)] * cores)
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                times.append(dt)
+    tot = sum(times)
+    value = cores * 6 * N_CELLS * N_CELLS * steps * len(times) / tot
+    line = {
+        "impl": "reference", "metric": "C192 RK4 cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"C{N_CELLS} linear SWE (Ch, SBP 4-2), dt {DT:g} s, bounded sample of {steps} "
+                               f"RK4 steps per process", "N": N_CELLS, "l2_between_steps": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} spawn processes x C{N_CELLS} x {steps} RK4 steps (FP64 CPU restatement; "
+                                   "the Fortran/MPI reference needs mpiifort, absent)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def profile_traffic(precision):
+    p = os.path.join(ROOT, "profiles", "k_stage_c192_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get(precision)
+        except Exception:
+            return None
+    return None
+
+
+def run_precision(precision, ic, args, torch, dist, world):
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    from ch_swe_b200 import _lib
+    dom = create_domain(N_CELLS, precision=precision, h_mean=H_MEAN)
+    stream = torch.cuda.current_stream()
+    dom.set_stream(stream.cuda_stream)
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
+    st = create_stvec_swm(dom)
+    ic_dev = create_stvec_swm(dom).upload(*ic)
+    rk = create_timescheme(st, "rk4")
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one():
+        st.assign(1.0, ic_dev)
+        rk.steps(st, op, dom, DT, NSTEPS)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    n0 = dom.launch_count()
+    for _ in range(args.steps):
+        st.assign(1.0, ic_dev)
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rk.steps(st, op, dom, DT, NSTEPS)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    launches = dom.launch_count() - n0
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms = float(t.item())
+    final = st.download()
+
+    # end-to-end through the public API: pinned host -> device, the day, device -> host
+    nbytes = st.device_view()[1]
+    e2e_s = 0.0
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st.upload(*ic)
+        rk.steps(st, op, dom, DT, NSTEPS)
+        st.download()
+        e2e_s += time.perf_counter() - t0
+    e2e_n = max(1, min(args.steps, 3))
+
+    # per-kernel durations (events around each launch, warm L2 as inside a day)
+    import ctypes
+    co = ctypes.c_double()
+    sg = ctypes.c_double()
+    st.assign(1.0, ic_dev)
+    _lib.check(_lib.load().swe_kernel_times(dom.ctx, st.handle, DT, 20, ctypes.byref(co), ctypes.byref(sg)),
+               dom.ctx, "kernel times")
+    return {
+        "total_ms": total_ms, "launches": launches, "final": final,
+        "e2e_value": cells_per_step(N_CELLS) * e2e_n / e2e_s, "e2e_bytes": nbytes,
+        "ms_co2contra": co.value, "ms_stage": sg.value, "dom": dom,
+    }
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu) else None
+    from ch_swe_b200 import build
+    build.build()
+    ic, (lam0, phi0) = workload_ic()
+    res = {}
+    stream = torch.cuda.Stream()   # a real (non-default) stream shared by torch events and the library
+    with ClockSampler(local) as clk, torch.cuda.stream(stream):
+        for prec in ("fp32", "fp64"):
+            res[prec] = run_precision(prec, ic, args, torch, dist, world)
+    clocks = clk.summary()
+
+    K = args.steps
+    r32, r64 = res["fp32"], res["fp64"]
+    v32 = world * cells_per_step(N_CELLS) * K / (r32["total_ms"] / 1e3)
+    v64 = world * cells_per_step(N_CELLS) * K / (r64["total_ms"] / 1e3)
+    errs = {}
+    for name, a, b in zip("huv", r32["final"], r64["final"]):
+        errs[name] = {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                      "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
+    peaks, src = measured_peaks()
+    D = dof(N_CELLS)
+    # algorithmic bytes of one fused stage launch: 16 state words per DOF per RK4
+    # step (S1 3, S2 5, S3 5, S4 3) + 2 Kahan words (FP32), i.e. 18/4 words of 4 B
+    alg_bytes_32 = D * 4 * (18 / 4)
+    achieved = alg_bytes_32 / (r32["ms_stage"] / 1e3) / 1e9
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    line = {
+        "metric": "C192 RK4 cell-updates/s", "value": v32, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": r32["total_ms"] / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"C{N_CELLS} linear SWE (Ch staggering, SBP 4-2), 1 simulated day = {NSTEPS} RK4 "
+                               f"steps of dt {DT:g} s per bench step, cube-corner Gaussian (seeded jitter)",
+                   "N": N_CELLS, "cells": 6 * N_CELLS ** 2, "dof": D, "dt": DT, "rk4_steps_per_step": NSTEPS,
+                   "h_mean": H_MEAN, "gaussian_centre": [lam0, phi0], "parallelism": f"replicas x{world}",
+                   "l2_between_steps": "flushed (512 MiB device write) before every timed step"},
+        "fp64": {"value": v64, "ms_per_step": r64["total_ms"] / K, "ms_stage_kernel": r64["ms_stage"],
+                 "ms_co2contra_kernel": r64["ms_co2contra"]},
+        "fp32_over_fp64": v32 / v64,
+        "fp32_vs_fp64_after_one_day": errs,
+        "e2e": {"value": r32["e2e_value"], "unit": "cell-updates/s", "h2d_bytes_per_step": r32["e2e_bytes"],
+                "d2h_bytes_per_step": r32["e2e_bytes"],
+                "path": "ch_swe_b200.swm -> libchswe.so C ABI: upload (pinned staging), 576 RK4 steps, download"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profile_traffic("fp32"), "kernel": "k_stage<float>",
+                     "peak_source": src, "ms_per_launch": r32["ms_stage"],
+                     "alg_bytes_per_launch": alg_bytes_32},
+        "gpu_launches": r32["launches"],
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for r in res.values():
+        r["dom"].destroy()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
+                    help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
+    args = ap.parse_args()
+    global NSTEPS
+    NSTEPS = args.rk4_steps
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

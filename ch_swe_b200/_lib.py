@@ -24,6 +24,7 @@ EXPORTED = [
     "swe_stvec_upload", "swe_stvec_download", "swe_stvec_upload_all", "swe_stvec_download_all",
     "swe_stvec_assign", "swe_stvec_update", "swe_stvec_device_view", "swe_operator_apply",
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
+    "swe_kernel_times",
 ]
 
 
@@ -84,6 +85,7 @@ def load(path: str = LIB_PATH):
     L.swe_launch_count.argtypes = [_vp]
     L.swe_launch_count.restype = ctypes.c_longlong
     L.swe_edge_links.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.swe_kernel_times.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, _dp, _dp]
     for name in EXPORTED:
         if not hasattr(L, name):
             raise SweError(f"libchswe.so does not export {name}")

@@ -304,6 +304,7 @@ struct swe_ctx {
     // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x meshes, [N+1][P]
     double *qw = nullptr;
     double *red = nullptr;           // reduction partials
+    unsigned char *pinned = nullptr; // pinned host staging for uploads/downloads (whole batch)
     // captured RK4 step
     cudaGraphExec_t graph = nullptr;
     const void *graph_v0 = nullptr;
@@ -480,6 +481,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w);
     cudaFree(c->qw); cudaFree(c->red);
+    if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
 
@@ -527,6 +529,9 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if ((rc = alloc_box(c, &c->ya)) || (rc = alloc_box(c, &c->yb)) || (rc = alloc_box(c, &c->acc)) ||
         (rc = alloc_box(c, &c->w)))
         return bail(rc);
+    if (cudaHostAlloc((void **)&c->pinned, c->box_elems * c->elem, cudaHostAllocDefault) != cudaSuccess)
+        return bail(SWE_ENOMEM);
+    std::memset(c->pinned, 0, c->box_elems * c->elem);
     *out = c;
     return SWE_OK;
 }
@@ -633,14 +638,15 @@ static int upload_range(swe_stvec *vec, int m0, int count, const double *h, cons
     size_t nh, nu;
     member_sizes(c, &nh, &nu);
     const size_t mbytes = (size_t)c->dims.ms * c->elem;
-    std::vector<unsigned char> buf(mbytes * count, 0);
+    CU(c, cudaStreamSynchronize(c->stream));   // the staging buffer may still feed an earlier copy
+    unsigned char *buf = c->pinned;
     for (int k = 0; k < count; k++) {
         if (c->elem == 8)
-            pack_member<double>(c, h + k * nh, u + k * nu, v + k * nu, (double *)(buf.data() + k * mbytes));
+            pack_member<double>(c, h + k * nh, u + k * nu, v + k * nu, (double *)(buf + k * mbytes));
         else
-            pack_member<float>(c, h + k * nh, u + k * nu, v + k * nu, (float *)(buf.data() + k * mbytes));
+            pack_member<float>(c, h + k * nh, u + k * nu, v + k * nu, (float *)(buf + k * mbytes));
     }
-    CU(c, cudaMemcpyAsync((char *)vec->d + m0 * mbytes, buf.data(), buf.size(), cudaMemcpyHostToDevice, c->stream));
+    CU(c, cudaMemcpyAsync((char *)vec->d + m0 * mbytes, buf, mbytes * count, cudaMemcpyHostToDevice, c->stream));
     if (vec->cmp) CU(c, cudaMemsetAsync((char *)vec->cmp + m0 * (size_t)c->dims.ms * 4, 0, (size_t)c->dims.ms * 4 * count, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
@@ -652,14 +658,14 @@ static int download_range(const swe_stvec *vec, int m0, int count, double *h, do
     size_t nh, nu;
     member_sizes(c, &nh, &nu);
     const size_t mbytes = (size_t)c->dims.ms * c->elem;
-    std::vector<unsigned char> buf(mbytes * count);
-    CU(c, cudaMemcpyAsync(buf.data(), (char *)vec->d + m0 * mbytes, buf.size(), cudaMemcpyDeviceToHost, c->stream));
+    unsigned char *buf = c->pinned;
+    CU(c, cudaMemcpyAsync(buf, (char *)vec->d + m0 * mbytes, mbytes * count, cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
     for (int k = 0; k < count; k++) {
         if (c->elem == 8)
-            unpack_member<double>(c, (const double *)(buf.data() + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
+            unpack_member<double>(c, (const double *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
         else
-            unpack_member<float>(c, (const float *)(buf.data() + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
+            unpack_member<float>(c, (const float *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
     }
     return SWE_OK;
 }
@@ -901,5 +907,56 @@ extern "C" int swe_edge_links(int *out)
             int *o = out + (p * 4 + s) * 5;
             o[0] = L[p][s].nb; o[1] = L[p][s].nside; o[2] = L[p][s].rev; o[3] = L[p][s].sn; o[4] = L[p][s].st;
         }
+    return SWE_OK;
+}
+
+// Diagnostic: run `nreps` RK4 steps launch by launch with CUDA events around every
+// kernel on the context's stream; returns the mean duration (ms) of the
+// contravariant kernel and of the fused stage kernel.
+extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps, double *ms_co2contra,
+                                double *ms_stage)
+{
+    if (!c || !v0 || v0->ctx != c || nreps < 1) return SWE_EINVAL;
+    int rc = ensure_cmp(v0);
+    if (rc) return rc;
+    const int nev = 16 * nreps + 1;
+    std::vector<cudaEvent_t> ev(nev);
+    for (auto &e : ev) CU(c, cudaEventCreate(&e));
+    dim3 g = stage_grid(c), b = stage_block();
+    int k = 0;
+    CU(c, cudaEventRecord(ev[k++], c->stream));
+    for (int r = 0; r < nreps; r++) {
+        void *bufs_in[4] = {v0->d, c->yb, c->ya, c->yb};
+        void *bufs_out[4] = {c->yb, c->ya, c->yb, nullptr};
+        for (int s = 0; s < 4; s++) {
+            StageArgs a{s + 1, dt, c->Hm};
+            if (c->elem == 8) {
+                k_co2contra<double><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (double *)c->w, c->dims, c->m64.v);
+                CU(c, cudaEventRecord(ev[k++], c->stream));
+                k_stage<double><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (const double *)c->w,
+                                                       (double *)v0->d, (double *)bufs_out[s], (double *)c->acc,
+                                                       nullptr, c->dims, c->m64.v, a);
+            } else {
+                k_co2contra<float><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (float *)c->w, c->dims, c->m32.v);
+                CU(c, cudaEventRecord(ev[k++], c->stream));
+                k_stage<float><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (const float *)c->w, (float *)v0->d,
+                                                      (float *)bufs_out[s], (float *)c->acc, v0->cmp, c->dims,
+                                                      c->m32.v, a);
+            }
+            CU(c, cudaEventRecord(ev[k++], c->stream));
+            c->launches += 2;
+        }
+    }
+    CU(c, cudaStreamSynchronize(c->stream));
+    double t_co = 0.0, t_st = 0.0;
+    for (int q = 0; q + 2 < k; q += 2) {
+        float a = 0.f, bms = 0.f;
+        cudaEventElapsedTime(&a, ev[q], ev[q + 1]);
+        cudaEventElapsedTime(&bms, ev[q + 1], ev[q + 2]);
+        t_co += a; t_st += bms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (ms_co2contra) *ms_co2contra = t_co / (4.0 * nreps);
+    if (ms_stage) *ms_stage = t_st / (4.0 * nreps);
     return SWE_OK;
 }
