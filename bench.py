@@ -113,14 +113,23 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 # CPU legs (the oracle): only here and in the reference arm
 # ----------------------------------------------------------------------------
-def _cpu_worker(args):
-    N, steps = args
+_WORKER = {}
+
+
+def _cpu_init(N):
     sys.path.insert(0, ROOT)
     from oracle.oracle import Oracle
-    (h, u, v), _ = workload_ic(N)
-    o = Oracle(N, h_mean=H_MEAN)
+    _WORKER["ic"] = workload_ic(N)[0]
+    _WORKER["o"] = Oracle(N, h_mean=H_MEAN)
+
+
+def _cpu_worker(args):
+    N, steps = args
+    if "o" not in _WORKER:
+        _cpu_init(N)
+    h, u, v = _WORKER["ic"]
     t0 = time.perf_counter()
-    o.rk4(h, u, v, DT, steps)
+    _WORKER["o"].rk4(h, u, v, DT, steps)
     return time.perf_counter() - t0
 
 
@@ -141,10 +150,10 @@ def run_reference(args):
     from oracle import oracle as orc
     orc.build()
     cores = os.cpu_count() or 1
-    steps = 6
+    steps = 12
     ctx = mp.get_context("spawn")
     times = []
-    with ctx.Pool(cores) as pool:
+    with ctx.Pool(cores, initializer=_cpu_init, initargs=(N_CELLS,)) as pool:
         for k in range(args.warmup + args.steps):
             t0 = time.perf_counter()
             pool.map(_cpu_worker, [(N_CELLS, steps)] * cores)
@@ -333,6 +342,7 @@ def run_ours(args):
 
 
 def main():
+    global NSTEPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -342,7 +352,6 @@ def main():
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
     args = ap.parse_args()
-    global NSTEPS
     NSTEPS = args.rk4_steps
     if args.warmup < 3:
         args.warmup = 3
