@@ -24,7 +24,7 @@ EXPORTED = [
     "swe_stvec_upload", "swe_stvec_download", "swe_stvec_upload_all", "swe_stvec_download_all",
     "swe_stvec_assign", "swe_stvec_update", "swe_stvec_device_view", "swe_operator_apply",
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
-    "swe_kernel_times",
+    "swe_kernel_times", "swe_operator_contravariant",
 ]
 
 
@@ -79,6 +79,7 @@ def load(path: str = LIB_PATH):
     L.swe_stvec_device_view.argtypes = [_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t),
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.swe_operator_apply.argtypes = [_vp, _vp, _vp]
+    L.swe_operator_contravariant.argtypes = [_vp, _vp, _vp]
     L.swe_rk4_step.argtypes = [_vp, _vp, ctypes.c_double]
     L.swe_rk4_steps.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int]
     L.swe_integrals.argtypes = [_vp, _vp, ctypes.c_int, _dp, _dp]

@@ -13,6 +13,7 @@
 #include "chswe.h"
 #include "swe_common.cuh"
 #include "swe_kernels.cuh"
+#include "swe_tiled.cuh"
 
 namespace chswe {
 
@@ -728,11 +729,12 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // ---------------------------------------------------------------------------
 // operator application and RK4
 // ---------------------------------------------------------------------------
-static dim3 stage_block() { return dim3(32, 8, 1); }
-static dim3 stage_grid(const swe_ctx *c)
+constexpr int TILE_X = 32, TILE_Y = 16;
+static dim3 stage_block() { return dim3(TILE_X, TILE_Y, 1); }
+static dim3 stage_grid(const swe_ctx *c, int members = -1)
 {
     const int n = c->cfg.N + 1;
-    return dim3((n + 31) / 32, (n + 7) / 8, NPAN * c->cfg.n_members);
+    return dim3((n + TILE_X - 1) / TILE_X, (n + TILE_Y - 1) / TILE_Y, NPAN * (members < 0 ? c->cfg.n_members : members));
 }
 
 template <class T>
@@ -740,9 +742,9 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     dim3 g = stage_grid(c), b = stage_block();
-    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    k_co2contra_t<T, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
     StageArgs a{mode, dt, c->Hm};
-    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims,
+    k_stage_t<T, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims,
                                       mv, a);
     c->launches += 2;
 }
@@ -757,6 +759,20 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     enqueue_apply(c, vout->d, vin->d);
+    CU(c, cudaGetLastError());
+    return SWE_OK;
+}
+
+// vout.u, vout.v = contravariant components of (vin.u, vin.v); vout.h is left as is.
+extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
+{
+    if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    dim3 g = stage_grid(c), b = stage_block();
+    if (c->elem == 8)
+        k_co2contra_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)vin->d, (double *)vout->d, c->dims, c->m64.v);
+    else
+        k_co2contra_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)vin->d, (float *)vout->d, c->dims, c->m32.v);
+    c->launches++;
     CU(c, cudaGetLastError());
     return SWE_OK;
 }
@@ -875,13 +891,13 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     dim3 g(nb, 4), b(256);
     // contravariant components of this member into the scratch, then the four sums
     Dims d1 = c->dims;
-    dim3 gs(stage_grid(c).x, stage_grid(c).y, NPAN), bs = stage_block();
+    dim3 gs = stage_grid(c, 1), bs = stage_block();
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        k_co2contra<double><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
+        k_co2contra_t<double, TILE_X, TILE_Y><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        k_co2contra<float><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
+        k_co2contra_t<float, TILE_X, TILE_Y><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
@@ -931,15 +947,15 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
         for (int s = 0; s < 4; s++) {
             StageArgs a{s + 1, dt, c->Hm};
             if (c->elem == 8) {
-                k_co2contra<double><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (double *)c->w, c->dims, c->m64.v);
+                k_co2contra_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (double *)c->w, c->dims, c->m64.v);
                 CU(c, cudaEventRecord(ev[k++], c->stream));
-                k_stage<double><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (const double *)c->w,
+                k_stage_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (const double *)c->w,
                                                        (double *)v0->d, (double *)bufs_out[s], (double *)c->acc,
                                                        nullptr, c->dims, c->m64.v, a);
             } else {
-                k_co2contra<float><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (float *)c->w, c->dims, c->m32.v);
+                k_co2contra_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (float *)c->w, c->dims, c->m32.v);
                 CU(c, cudaEventRecord(ev[k++], c->stream));
-                k_stage<float><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (const float *)c->w, (float *)v0->d,
+                k_stage_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (const float *)c->w, (float *)v0->d,
                                                       (float *)bufs_out[s], (float *)c->acc, v0->cmp, c->dims,
                                                       c->m32.v, a);
             }

@@ -1,13 +1,15 @@
 // swe_kernels.cuh -- sm_100a kernels of the linear shallow-water RK4 step on the
 // Ch-staggered equiangular cubed sphere (SBP 4-2), templated on the stencil type.
 //
-// One RK stage = two launches:
-//   k_co2contra : (u, v) of the stage input -> contravariant (ut, vt)
-//                 (co2contra_Ch_mod.f90:27-94)
-//   k_stage     : gradient + SAT, Coriolis with the ECS vector edge sync,
-//                 divergence + SAT with the Ah scalar edge sync, the linear
-//                 tendency (operator_swm_lin_mod.f90:66-108) and the RK4 update
-//                 (rk4_mod.f90:28-40) fused in one pass.
+// This header holds the global-memory building blocks (stencil tables, edge
+// links, the neighbour-panel values used at panel boundaries) and the small
+// elementwise kernels; the per-stage kernels are in swe_tiled.cuh:
+//   k_co2contra_t : (u, v) of the stage input -> contravariant (ut, vt)
+//                   (co2contra_Ch_mod.f90:27-94)
+//   k_stage_t     : gradient + SAT, Coriolis with the ECS vector edge sync,
+//                   divergence + SAT with the Ah scalar edge sync, the linear
+//                   tendency (operator_swm_lin_mod.f90:66-108) and the RK4 update
+//                   (rk4_mod.f90:28-40) fused in one pass.
 // The MPI halo exchange of the reference is replaced by index-mapped reads of
 // the neighbouring panel in the same allocation (`Link` table): panel-edge
 // threads recompute the neighbour's edge values they need instead of waiting
@@ -267,57 +269,6 @@ __device__ __forceinline__ T h_halo(const T *Y, const Dims &d, int t, int s, int
 // kernels
 // ---------------------------------------------------------------------------
 
-// Contravariant components (co2contra_Ch_mod.f90:27-94):
-//   ut = Qi11 u + J^-1 I_i2c,x( J Qi12 I_c2i,y(v) ),  vt = Qi22 v + J^-1 I_i2c,y( J Qi12 I_c2i,x(u) )
-// grid: x over i (N+1), y over j (N+1), z over member*6 + panel.
-template <class T>
-__global__ void __launch_bounds__(256) k_co2contra(const T *__restrict__ Y, T *__restrict__ W, Dims d,
-                                                   MetricView<T> m)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
-    const int N = d.N;
-    if (i > N + 1 || j > N + 1) return;
-    const T *y = Y + mem * d.ms;
-    T *w = W + mem * d.ms;
-    const T *wi, *wo;
-    if (i <= N) {
-        int s = sten<T>(OP_II2C, i, N, wo);
-        T acc = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            if (wo[q] == T(0)) continue;
-            int k = s + q;
-            int s2 = sten<T>(OP_IC2I, j, N + 1, wi);
-            T vq = 0;
-#pragma unroll
-            for (int r = 0; r < 5; r++)
-                if (wi[r] != T(0)) vq += wi[r] * ld(y, d, 2, t, k, s2 + r);
-            acc += wo[q] * (vq * __ldg(m.JQ12 + ofs(d, k, j)));
-        }
-        w[1 * d.fs + t * d.ps + ofs(d, i, j)] =
-            __ldg(m.Q11y + ofs(d, i, j)) * ld(y, d, 1, t, i, j) + acc * __ldg(m.iJy + ofs(d, i, j));
-    }
-    if (j <= N) {
-        int s = sten<T>(OP_II2C, j, N, wo);
-        T acc = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            if (wo[q] == T(0)) continue;
-            int l = s + q;
-            int s2 = sten<T>(OP_IC2I, i, N + 1, wi);
-            T uq = 0;
-#pragma unroll
-            for (int r = 0; r < 5; r++)
-                if (wi[r] != T(0)) uq += wi[r] * ld(y, d, 1, t, s2 + r, l);
-            acc += wo[q] * (uq * __ldg(m.JQ12 + ofs(d, i, l)));
-        }
-        w[2 * d.fs + t * d.ps + ofs(d, i, j)] =
-            __ldg(m.Q22x + ofs(d, i, j)) * ld(y, d, 2, t, i, j) + acc * __ldg(m.iJx + ofs(d, i, j));
-    }
-}
-
 // RK4 stage parameters.
 struct StageArgs {
     int mode;          // 0: write the tendency A(y) to out; 1..4: RK4 stage
@@ -332,116 +283,6 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float inc)
     float tk = s + yk;
     c = (tk - s) - yk;
     s = tk;
-}
-
-// Fused stage: tendency of the linear operator at the three staggered points of
-// xy box position (i, j) and the RK4 update.
-//   mode 1: Y1 = V0 + dt/2 k,  ACC = dt/6 k
-//   mode 2: Y1 = V0 + dt/2 k,  ACC += dt/3 k
-//   mode 3: Y1 = V0 + dt   k,  ACC += dt/3 k
-//   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
-template <class T>
-__global__ void __launch_bounds__(256) k_stage(const T *__restrict__ Yin, const T *__restrict__ W, T *V0, T *Y1,
-                                               T *ACC, T *CMP, Dims d, MetricView<T> m, StageArgs a)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
-    const int N = d.N;
-    if (i > N + 1 || j > N + 1) return;
-    const int64_t mo = mem * d.ms;
-    const T *y = Yin + mo;
-    const T *w = W + mo;
-    const T H = T(a.Hm[mem]);
-    const T *wo;
-
-    T kh, ku = 0, kv = 0;
-    kh = -H * div_sync(w, d, m, t, i, j);
-
-    if (i <= N) {
-        // gradient along x (grad_sbp_sat_mod.f90:42-76) with the SAT halo h(0), h(N+2)
-        int s = sten<T>(OP_DI2C, i, N, wo);
-        T gx = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++)
-            if (wo[q] != T(0)) gx += wo[q] * ld(y, d, 0, t, s + q, j);
-        if (i <= 3) gx += satc<T>(i - 1) * (ld(y, d, 0, t, 1, j) - h_halo(y, d, t, SIDE_L, j));
-        if (i >= N - 2) gx += satc<T>(N - i) * (h_halo(y, d, t, SIDE_R, j) - ld(y, d, 0, t, N + 1, j));
-        gx = gx * m.inv_hxa;
-        // Coriolis u-component: I_i2c,x of the synchronised vertex vector, / J
-        s = sten<T>(OP_II2C, i, N, wo);
-        T cu = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            if (wo[q] == T(0)) continue;
-            T ups, vps;
-            cor_sync(w, d, m, t, s + q, j, ups, vps);
-            cu += wo[q] * ups;
-        }
-        cu = cu * __ldg(m.iJy + ofs(d, i, j));
-        ku = -m.grav * gx + cu;
-    }
-    if (j <= N) {
-        int s = sten<T>(OP_DI2C, j, N, wo);
-        T gy = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++)
-            if (wo[q] != T(0)) gy += wo[q] * ld(y, d, 0, t, i, s + q);
-        if (j <= 3) gy += satc<T>(j - 1) * (ld(y, d, 0, t, i, 1) - h_halo(y, d, t, SIDE_B, i));
-        if (j >= N - 2) gy += satc<T>(N - j) * (h_halo(y, d, t, SIDE_T, i) - ld(y, d, 0, t, i, N + 1));
-        gy = gy * m.inv_hxa;
-        s = sten<T>(OP_II2C, j, N, wo);
-        T cv = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            if (wo[q] == T(0)) continue;
-            T ups, vps;
-            cor_sync(w, d, m, t, i, s + q, ups, vps);
-            cv += wo[q] * vps;
-        }
-        cv = cv * __ldg(m.iJx + ofs(d, i, j));
-        kv = -m.grav * gy + cv;
-    }
-
-    const int64_t base = mo + t * d.ps + ofs(d, i, j);
-    const int64_t ih = base, iu = base + d.fs, iv = base + 2 * d.fs;
-    const bool hu = (i <= N), hv = (j <= N);
-    if (a.mode == 0) {
-        Y1[ih] = kh;
-        if (hu) Y1[iu] = ku;
-        if (hv) Y1[iv] = kv;
-        return;
-    }
-    const T dt = T(a.dt);
-    if (a.mode <= 3) {
-        const T ca = (a.mode == 3) ? dt : T(0.5) * dt;
-        const T cb = (a.mode == 1) ? dt / T(6) : dt / T(3);
-        Y1[ih] = V0[ih] + ca * kh;
-        if (hu) Y1[iu] = V0[iu] + ca * ku;
-        if (hv) Y1[iv] = V0[iv] + ca * kv;
-        if (a.mode == 1) {
-            ACC[ih] = cb * kh;
-            if (hu) ACC[iu] = cb * ku;
-            if (hv) ACC[iv] = cb * kv;
-        } else {
-            ACC[ih] += cb * kh;
-            if (hu) ACC[iu] += cb * ku;
-            if (hv) ACC[iv] += cb * kv;
-        }
-        return;
-    }
-    const T cb = dt / T(6);
-    if constexpr (sizeof(T) == 4) {
-        float s0 = V0[ih], c0 = CMP[ih];
-        kahan_add(s0, c0, ACC[ih] + cb * kh);
-        V0[ih] = s0; CMP[ih] = c0;
-        if (hu) { float s1 = V0[iu], c1 = CMP[iu]; kahan_add(s1, c1, ACC[iu] + cb * ku); V0[iu] = s1; CMP[iu] = c1; }
-        if (hv) { float s2 = V0[iv], c2 = CMP[iv]; kahan_add(s2, c2, ACC[iv] + cb * kv); V0[iv] = s2; CMP[iv] = c2; }
-    } else {
-        V0[ih] = V0[ih] + (ACC[ih] + cb * kh);
-        if (hu) V0[iu] = V0[iu] + (ACC[iu] + cb * ku);
-        if (hv) V0[iv] = V0[iv] + (ACC[iv] + cb * kv);
-    }
 }
 
 // y = s1*v1 + s2*v2 (v2 may be null) or y += s1*v1 + s2*v2 over the whole box.

@@ -227,6 +227,11 @@ class OperatorSwmLin:
         check(_lib.load().swe_operator_apply(self.domain.ctx, vout.handle, vin.handle), self.domain.ctx,
               "operator apply")
 
+    def contravariant(self, vout: StvecSwm, vin: StvecSwm, domain: Domain | None = None):
+        """vout.u, vout.v = contravariant components of vin (co2contra_operator_t%transform)."""
+        check(_lib.load().swe_operator_contravariant(self.domain.ctx, vout.handle, vin.handle), self.domain.ctx,
+              "co2contra")
+
     def integrals(self, state: StvecSwm, member: int = 0):
         """FP64 SBP-quadrature mass and linear energy of one member."""
         m = ctypes.c_double()

@@ -100,6 +100,9 @@ int swe_stvec_device_view(const swe_stvec *vec, void **ptr, size_t *bytes, int *
 
 /* vout = A(vin), A the linear shallow-water operator. */
 int swe_operator_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
+/* vout.u, vout.v = contravariant components (ut, vt) of vin's covariant wind; vout.h unchanged.
+   Mirrors co2contra_operator_t%transform (co2contra_Ch_mod.f90:27-94). */
+int swe_operator_contravariant(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
 /* One classic RK4 step of size dt on v0 (in place). */
 int swe_rk4_step(swe_ctx *ctx, swe_stvec *v0, double dt);
 /* nsteps RK4 steps (captured into a CUDA graph after the first call with the same shape). */

@@ -35,7 +35,8 @@ def random_state(N, seed):
     return tuple(rng.standard_normal(s) for s in state_shapes(N))
 
 
-@pytest.mark.parametrize("N", [8, 12, 24, 33])
+# tile edges at 1 + 32k (x) and 1 + 16k (y): cover tiles that start at N-2 .. N+1
+@pytest.mark.parametrize("N", [8, 12, 15, 16, 17, 18, 24, 31, 32, 33, 34, 35, 47, 48])
 def test_apply_parity_fp64_random(N):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
     from oracle.oracle import Oracle
@@ -50,6 +51,22 @@ def test_apply_parity_fp64_random(N):
     got = y.download()
     for g, r, name in zip(got, ref, "huv"):
         assert rel(g, r) < FP64_RTOL, (name, rel(g, r))
+
+
+@pytest.mark.parametrize("N", [16, 33, 34])
+def test_contravariant_parity_fp64(N):
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
+    from oracle.oracle import Oracle
+    h, u, v = random_state(N, 200 + N)
+    ref = Oracle(N).co2contra(u, v)
+    dom = create_domain(N)
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
+    x = create_stvec_swm(dom).upload(h, u, v)
+    y = create_stvec_swm(dom).upload(h, u, v)
+    op.contravariant(y, x)
+    _, ut, vt = y.download()
+    assert rel(ut, ref[0]) < FP64_RTOL
+    assert rel(vt, ref[1]) < FP64_RTOL
 
 
 def test_apply_parity_coriolis_constant_tilted_axis():
