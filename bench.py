@@ -259,14 +259,15 @@ def run_precision(precision, ic, args, torch, dist, world):
     # per-kernel durations (events around each launch, warm L2 as inside a day)
     import ctypes
     co = ctypes.c_double()
+    ed = ctypes.c_double()
     sg = ctypes.c_double()
     st.assign(1.0, ic_dev)
-    _lib.check(_lib.load().swe_kernel_times(dom.ctx, st.handle, DT, 20, ctypes.byref(co), ctypes.byref(sg)),
+    _lib.check(_lib.load().swe_kernel_times(dom.ctx, st.handle, DT, 20, ctypes.byref(co), ctypes.byref(ed), ctypes.byref(sg)),
                dom.ctx, "kernel times")
     return {
         "total_ms": total_ms, "launches": launches, "final": final,
         "e2e_value": cells_per_step(N_CELLS) * e2e_n / e2e_s, "e2e_bytes": nbytes,
-        "ms_co2contra": co.value, "ms_stage": sg.value, "dom": dom,
+        "ms_co2contra": co.value, "ms_edge": ed.value, "ms_stage": sg.value, "dom": dom,
     }
 
 
@@ -317,7 +318,8 @@ def run_ours(args):
                    "h_mean": H_MEAN, "gaussian_centre": [lam0, phi0], "parallelism": f"replicas x{world}",
                    "l2_between_steps": "flushed (512 MiB device write) before every timed step"},
         "fp64": {"value": v64, "ms_per_step": r64["total_ms"] / K, "ms_stage_kernel": r64["ms_stage"],
-                 "ms_co2contra_kernel": r64["ms_co2contra"]},
+                 "ms_co2contra_kernel": r64["ms_co2contra"], "ms_edge_kernel": r64["ms_edge"]},
+        "fp32_kernel_ms": {"k_co2contra": r32["ms_co2contra"], "k_edge": r32["ms_edge"], "k_stage": r32["ms_stage"]},
         "fp32_over_fp64": v32 / v64,
         "fp32_vs_fp64_after_one_day": errs,
         "e2e": {"value": r32["e2e_value"], "unit": "cell-updates/s", "h2d_bytes_per_step": r32["e2e_bytes"],

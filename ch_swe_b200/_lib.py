@@ -86,7 +86,7 @@ def load(path: str = LIB_PATH):
     L.swe_launch_count.argtypes = [_vp]
     L.swe_launch_count.restype = ctypes.c_longlong
     L.swe_edge_links.argtypes = [ctypes.POINTER(ctypes.c_int)]
-    L.swe_kernel_times.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, _dp, _dp]
+    L.swe_kernel_times.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
     for name in EXPORTED:
         if not hasattr(L, name):
             raise SweError(f"libchswe.so does not export {name}")

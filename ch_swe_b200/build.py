@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchswe.so")
 SOURCES = ["swe_api.cu"]
-DEPS = ["swe_api.cu", "swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh"]
+DEPS = ["swe_api.cu", "swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

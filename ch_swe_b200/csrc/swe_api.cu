@@ -176,102 +176,6 @@ static void sync_weights(int N, std::vector<double> &qb, std::vector<double> &qt
     }
 }
 
-// ---------------------------------------------------------------------------
-// SBP 4-2 tables
-// ---------------------------------------------------------------------------
-template <class T>
-static void fill_tables(OpTab<T> op[4], T sat[8])
-{
-    auto set = [](T *w, double a, double b, double c, double d, double e) {
-        w[0] = T(a); w[1] = T(b); w[2] = T(c); w[3] = T(d); w[4] = T(e);
-    };
-    std::memset(op, 0, sizeof(OpTab<T>) * 4);
-    // difference nodes -> centres (sbp_diff_i2c_42_mod.f90:12-20)
-    {
-        const double q11 = -79.0 / 78.0, q12 = 27.0 / 26.0, q13 = -1.0 / 26.0, q14 = 1.0 / 78.0, q21 = 2.0 / 21.0,
-                     q22 = -9.0 / 7.0, q23 = 9.0 / 7.0, q24 = -2.0 / 21.0, q31 = 1.0 / 75.0, q33 = -27.0 / 25.0,
-                     q34 = 83.0 / 75.0, q35 = -1.0 / 25.0;
-        OpTab<T> &o = op[OP_DI2C];
-        o.L = 3;
-        o.lstart[0] = o.lstart[1] = o.lstart[2] = 1;
-        set(o.lw[0], q11, q12, q13, q14, 0);
-        set(o.lw[1], q21, q22, q23, q24, 0);
-        set(o.lw[2], q31, 0, q33, q34, q35);
-        o.rstart[0] = -2; set(o.rw[0], -q14, -q13, -q12, -q11, 0);
-        o.rstart[1] = -2; set(o.rw[1], -q24, -q23, -q22, -q21, 0);
-        o.rstart[2] = -3; set(o.rw[2], -q35, -q34, -q33, 0, -q31);
-        o.ioff = -1; set(o.iw, 1.0 / 24.0, -27.0 / 24.0, 27.0 / 24.0, -1.0 / 24.0, 0);
-    }
-    // difference centres -> nodes (sbp_diff_c2i_42_mod.f90:12-22)
-    {
-        const double q11 = -2.0, q12 = 3.0, q13 = -1.0, q21 = -1.0, q22 = 1.0, q31 = 1.0 / 24.0, q32 = -9.0 / 8.0,
-                     q33 = 9.0 / 8.0, q34 = -1.0 / 24.0, q41 = -1.0 / 71.0, q42 = 6.0 / 71.0, q43 = -83.0 / 71.0,
-                     q44 = 81.0 / 71.0, q45 = -3.0 / 71.0;
-        OpTab<T> &o = op[OP_DC2I];
-        o.L = 4;
-        o.lstart[0] = o.lstart[1] = o.lstart[2] = o.lstart[3] = 1;
-        set(o.lw[0], q11, q12, q13, 0, 0);
-        set(o.lw[1], q21, q22, 0, 0, 0);
-        set(o.lw[2], q31, q32, q33, q34, 0);
-        set(o.lw[3], q41, q42, q43, q44, q45);
-        o.rstart[0] = -3; set(o.rw[0], -q13, -q12, -q11, 0, 0);
-        o.rstart[1] = -2; set(o.rw[1], -q22, -q21, 0, 0, 0);
-        o.rstart[2] = -4; set(o.rw[2], -q34, -q33, -q32, -q31, 0);
-        o.rstart[3] = -5; set(o.rw[3], -q45, -q44, -q43, -q42, -q41);
-        o.ioff = -2; set(o.iw, 1.0 / 24.0, -27.0 / 24.0, 27.0 / 24.0, -1.0 / 24.0, 0);
-    }
-    const double c13 = 0.1264926207034815, c14 = -0.029892648949074313;
-    // interpolation nodes -> centres (sbp_interp_i2c_42_mod.f90:18-35)
-    {
-        const double q11 = 1.0 / 2.0 + c13 + 2.0 * c14, q12 = 1.0 / 2.0 - 2.0 * c13 - 3.0 * c14, q13 = c13, q14 = c14,
-                     q21 = -8.0 / 63.0 - 52.0 / 21.0 * c13 - 104.0 / 21.0 * c14,
-                     q22 = 29.0 / 42.0 + 104.0 / 21.0 * c13 + 52.0 / 7.0 * c14, q23 = -52.0 / 21.0 * c13 + 1.0 / 2.0,
-                     q24 = -52.0 / 21.0 * c14 - 4.0 / 63.0, q31 = 26.0 / 25.0 * c13 + 52.0 / 25.0 * c14 - 1.0 / 25.0,
-                     q32 = -1.0 / 50.0 - 52.0 / 25.0 * c13 - 78.0 / 25.0 * c14, q33 = 3.0 / 5.0 + 26.0 / 25.0 * c13,
-                     q34 = 13.0 / 25.0 + 26.0 / 25.0 * c14, q35 = -3.0 / 50.0;
-        OpTab<T> &o = op[OP_II2C];
-        o.L = 3;
-        o.lstart[0] = o.lstart[1] = o.lstart[2] = 1;
-        set(o.lw[0], q11, q12, q13, q14, 0);
-        set(o.lw[1], q21, q22, q23, q24, 0);
-        set(o.lw[2], q31, q32, q33, q34, q35);
-        o.rstart[0] = -2; set(o.rw[0], q14, q13, q12, q11, 0);
-        o.rstart[1] = -2; set(o.rw[1], q24, q23, q22, q21, 0);
-        o.rstart[2] = -3; set(o.rw[2], q35, q34, q33, q32, q31);
-        o.ioff = -1; set(o.iw, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0, 0);
-    }
-    // interpolation centres -> nodes (sbp_interp_c2i_42_mod.f90:13-27)
-    {
-        const double q11 = 39.0 / 28.0 + 39.0 / 14.0 * c13 + 39.0 / 7.0 * c14,
-                     q12 = -2.0 / 7.0 - 39.0 / 7.0 * c13 - 78.0 / 7.0 * c14,
-                     q13 = 39.0 / 14.0 * c13 + 39.0 / 7.0 * c14 - 3.0 / 28.0,
-                     q21 = 13.0 / 27.0 - 52.0 / 27.0 * c13 - 26.0 / 9.0 * c14,
-                     q22 = 29.0 / 54.0 + 104.0 / 27.0 * c13 + 52.0 / 9.0 * c14,
-                     q23 = -1.0 / 54.0 - 52.0 / 27.0 * c13 - 26.0 / 9.0 * c14, q31 = 13.0 / 12.0 * c13,
-                     q32 = -13.0 / 6.0 * c13 + 7.0 / 16.0, q33 = 5.0 / 8.0 + 13.0 / 12.0 * c13, q34 = -1.0 / 16.0,
-                     q41 = 78.0 / 71.0 * c14, q42 = -156.0 / 71.0 * c14 - 4.0 / 71.0,
-                     q43 = 39.0 / 71.0 + 78.0 / 71.0 * c14, q44 = 81.0 / 142.0, q45 = -9.0 / 142.0;
-        OpTab<T> &o = op[OP_IC2I];
-        o.L = 4;
-        o.lstart[0] = o.lstart[1] = o.lstart[2] = o.lstart[3] = 1;
-        set(o.lw[0], q11, q12, q13, 0, 0);
-        set(o.lw[1], q21, q22, q23, 0, 0);
-        set(o.lw[2], q31, q32, q33, q34, 0);
-        set(o.lw[3], q41, q42, q43, q44, q45);
-        o.rstart[0] = -3; set(o.rw[0], q13, q12, q11, 0, 0);
-        o.rstart[1] = -3; set(o.rw[1], q23, q22, q21, 0, 0);
-        o.rstart[2] = -4; set(o.rw[2], q34, q33, q32, q31, 0);
-        o.rstart[3] = -5; set(o.rw[3], q45, q44, q43, q42, q41);
-        o.ioff = -2; set(o.iw, -1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0, 0);
-    }
-    const double R11 = 15.0 / 8.0, R12 = -5.0 / 4.0, R13 = 3.0 / 8.0;
-    sat[0] = T(0.5 * R11 / (13.0 / 12.0));
-    sat[1] = T(0.5 * R12 / (7.0 / 8.0));
-    sat[2] = T(0.5 * R13 / (25.0 / 24.0));
-    sat[3] = T(0.5 / (7.0 / 18.0));
-    sat[4] = T(R11); sat[5] = T(R12); sat[6] = T(R13); sat[7] = T(0);
-}
-
 }  // namespace chswe
 
 using namespace chswe;
@@ -302,6 +206,7 @@ struct swe_ctx {
     std::vector<double> Hhost;
     // scratch (stage buffers and contravariant intermediates)
     void *ya = nullptr, *yb = nullptr, *acc = nullptr, *w = nullptr;
+    void *edge = nullptr;            // synchronised panel-boundary values of the current stage
     // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x meshes, [N+1][P]
     double *qw = nullptr;
     double *red = nullptr;           // reduction partials
@@ -340,21 +245,18 @@ static int fail(swe_ctx *c, int code, const char *fmt, ...)
 
 static bool g_tables_ready[64] = {false};
 
+// Balanced tiles of at most TILE_XM x TILE_YM points cover the N+1 box.
+static bool tiles_fit(int N)
+{
+    const int n = N + 1, nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
+    return (n + nbx - 1) / nbx <= TILE_XM && (n + nby - 1) / nby <= TILE_YM;
+}
+
 static int upload_tables(swe_ctx *c)
 {
     if (c->device >= 0 && c->device < 64 && g_tables_ready[c->device]) return SWE_OK;
-    OpTab<double> o64[4];
-    OpTab<float> o32[4];
-    double s64[8];
-    float s32[8];
-    fill_tables<double>(o64, s64);
-    fill_tables<float>(o32, s32);
     Link L[NPAN][4];
     compute_links(L);
-    CU(c, cudaMemcpyToSymbol(c_op64, o64, sizeof(o64)));
-    CU(c, cudaMemcpyToSymbol(c_op32, o32, sizeof(o32)));
-    CU(c, cudaMemcpyToSymbol(c_sat64, s64, sizeof(s64)));
-    CU(c, cudaMemcpyToSymbol(c_sat32, s32, sizeof(s32)));
     CU(c, cudaMemcpyToSymbol(c_link, L, sizeof(L)));
     if (c->device >= 0 && c->device < 64) g_tables_ready[c->device] = true;
     return SWE_OK;
@@ -480,7 +382,7 @@ static void free_ctx(swe_ctx *c)
 {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm);
-    cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w);
+    cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge);
     cudaFree(c->qw); cudaFree(c->red);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -498,7 +400,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
 {
     if (!cfg || !out) return SWE_EINVAL;
     *out = nullptr;
-    if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
+    if (cfg->N < 8 || !tiles_fit(cfg->N) || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
         cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
         return SWE_EINVAL;
     int ndev = 0;
@@ -530,6 +432,11 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if ((rc = alloc_box(c, &c->ya)) || (rc = alloc_box(c, &c->yb)) || (rc = alloc_box(c, &c->acc)) ||
         (rc = alloc_box(c, &c->w)))
         return bail(rc);
+    {
+        const size_t eb = (size_t)cfg->n_members * NPAN * 4 * (N + 1) * 3 * c->elem;
+        if (cudaMalloc(&c->edge, eb) != cudaSuccess) return bail(SWE_ENOMEM);
+        if (cudaMemset(c->edge, 0, eb) != cudaSuccess) return bail(SWE_ECUDA);
+    }
     if (cudaHostAlloc((void **)&c->pinned, c->box_elems * c->elem, cudaHostAllocDefault) != cudaSuccess)
         return bail(SWE_ENOMEM);
     std::memset(c->pinned, 0, c->box_elems * c->elem);
@@ -729,24 +636,29 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // ---------------------------------------------------------------------------
 // operator application and RK4
 // ---------------------------------------------------------------------------
-constexpr int TILE_X = 32, TILE_Y = 16;
-static dim3 stage_block() { return dim3(TILE_X, TILE_Y, 1); }
+static dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
+// Balanced tiles: ceil(N / nominal) tiles per direction, widths at most TILE_XM x TILE_YM.
 static dim3 stage_grid(const swe_ctx *c, int members = -1)
 {
-    const int n = c->cfg.N + 1;
-    return dim3((n + TILE_X - 1) / TILE_X, (n + TILE_Y - 1) / TILE_Y, NPAN * (members < 0 ? c->cfg.n_members : members));
+    const int N = c->cfg.N;
+    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
+    return dim3(nbx, nby, NPAN * (members < 0 ? c->cfg.n_members : members));
 }
+
+
+static dim3 edge_grid(const swe_ctx *c) { return dim3((c->cfg.N + 1 + 127) / 128, NPAN * 4, c->cfg.n_members); }
 
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const MetricView<T> &mv)
 {
     dim3 g = stage_grid(c), b = stage_block();
-    k_co2contra_t<T, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    k_edge<T><<<edge_grid(c), 128, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
     StageArgs a{mode, dt, c->Hm};
-    k_stage_t<T, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims,
-                                      mv, a);
-    c->launches += 2;
+    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+                                      (T *)cmp, c->dims, mv, a);
+    c->launches += 3;
 }
 
 static void enqueue_apply(swe_ctx *c, void *out, const void *in)
@@ -769,9 +681,9 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     dim3 g = stage_grid(c), b = stage_block();
     if (c->elem == 8)
-        k_co2contra_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)vin->d, (double *)vout->d, c->dims, c->m64.v);
+        k_co2contra<double><<<g, b, 0, c->stream>>>((const double *)vin->d, (double *)vout->d, c->dims, c->m64.v);
     else
-        k_co2contra_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)vin->d, (float *)vout->d, c->dims, c->m32.v);
+        k_co2contra<float><<<g, b, 0, c->stream>>>((const float *)vin->d, (float *)vout->d, c->dims, c->m32.v);
     c->launches++;
     CU(c, cudaGetLastError());
     return SWE_OK;
@@ -894,10 +806,10 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     dim3 gs = stage_grid(c, 1), bs = stage_block();
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        k_co2contra_t<double, TILE_X, TILE_Y><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
+        k_co2contra<double><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        k_co2contra_t<float, TILE_X, TILE_Y><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
+        k_co2contra<float><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
@@ -928,51 +840,56 @@ extern "C" int swe_edge_links(int *out)
 
 // Diagnostic: run `nreps` RK4 steps launch by launch with CUDA events around every
 // kernel on the context's stream; returns the mean duration (ms) of the
-// contravariant kernel and of the fused stage kernel.
-extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps, double *ms_co2contra,
+// contravariant kernel, the edge kernel and the fused stage kernel.
+template <class T>
+static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, void *v0, void *y1, float *cmp, int mode,
+                        double dt, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, cudaEvent_t e3)
+{
+    dim3 g = stage_grid(c), b = stage_block();
+    cudaEventRecord(e0, c->stream);
+    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    cudaEventRecord(e1, c->stream);
+    k_edge<T><<<edge_grid(c), 128, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
+    cudaEventRecord(e2, c->stream);
+    StageArgs a{mode, dt, c->Hm};
+    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1,
+                                      (T *)c->acc, (T *)cmp, c->dims, mv, a);
+    cudaEventRecord(e3, c->stream);
+    c->launches += 3;
+}
+
+extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps, double *ms_co2contra, double *ms_edge,
                                 double *ms_stage)
 {
     if (!c || !v0 || v0->ctx != c || nreps < 1) return SWE_EINVAL;
     int rc = ensure_cmp(v0);
     if (rc) return rc;
-    const int nev = 16 * nreps + 1;
-    std::vector<cudaEvent_t> ev(nev);
+    const int nst = 4 * nreps;
+    std::vector<cudaEvent_t> ev(4 * nst);
     for (auto &e : ev) CU(c, cudaEventCreate(&e));
-    dim3 g = stage_grid(c), b = stage_block();
-    int k = 0;
-    CU(c, cudaEventRecord(ev[k++], c->stream));
-    for (int r = 0; r < nreps; r++) {
-        void *bufs_in[4] = {v0->d, c->yb, c->ya, c->yb};
-        void *bufs_out[4] = {c->yb, c->ya, c->yb, nullptr};
+    void *bufs_in[4] = {v0->d, c->yb, c->ya, c->yb};
+    void *bufs_out[4] = {c->yb, c->ya, c->yb, nullptr};
+    for (int r = 0; r < nreps; r++)
         for (int s = 0; s < 4; s++) {
-            StageArgs a{s + 1, dt, c->Hm};
-            if (c->elem == 8) {
-                k_co2contra_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (double *)c->w, c->dims, c->m64.v);
-                CU(c, cudaEventRecord(ev[k++], c->stream));
-                k_stage_t<double, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const double *)bufs_in[s], (const double *)c->w,
-                                                       (double *)v0->d, (double *)bufs_out[s], (double *)c->acc,
-                                                       nullptr, c->dims, c->m64.v, a);
-            } else {
-                k_co2contra_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (float *)c->w, c->dims, c->m32.v);
-                CU(c, cudaEventRecord(ev[k++], c->stream));
-                k_stage_t<float, TILE_X, TILE_Y><<<g, b, 0, c->stream>>>((const float *)bufs_in[s], (const float *)c->w, (float *)v0->d,
-                                                      (float *)bufs_out[s], (float *)c->acc, v0->cmp, c->dims,
-                                                      c->m32.v, a);
-            }
-            CU(c, cudaEventRecord(ev[k++], c->stream));
-            c->launches += 2;
+            cudaEvent_t *e = &ev[4 * (4 * r + s)];
+            if (c->elem == 8)
+                timed_stage<double>(c, c->m64.v, bufs_in[s], v0->d, bufs_out[s], nullptr, s + 1, dt, e[0], e[1], e[2], e[3]);
+            else
+                timed_stage<float>(c, c->m32.v, bufs_in[s], v0->d, bufs_out[s], v0->cmp, s + 1, dt, e[0], e[1], e[2], e[3]);
         }
-    }
+    CU(c, cudaGetLastError());
     CU(c, cudaStreamSynchronize(c->stream));
-    double t_co = 0.0, t_st = 0.0;
-    for (int q = 0; q + 2 < k; q += 2) {
-        float a = 0.f, bms = 0.f;
-        cudaEventElapsedTime(&a, ev[q], ev[q + 1]);
-        cudaEventElapsedTime(&bms, ev[q + 1], ev[q + 2]);
-        t_co += a; t_st += bms;
+    double t_co = 0.0, t_ed = 0.0, t_st = 0.0;
+    for (int q = 0; q < nst; q++) {
+        float a = 0.f, b = 0.f, d = 0.f;
+        cudaEventElapsedTime(&a, ev[4 * q], ev[4 * q + 1]);
+        cudaEventElapsedTime(&b, ev[4 * q + 1], ev[4 * q + 2]);
+        cudaEventElapsedTime(&d, ev[4 * q + 2], ev[4 * q + 3]);
+        t_co += a; t_ed += b; t_st += d;
     }
     for (auto &e : ev) cudaEventDestroy(e);
-    if (ms_co2contra) *ms_co2contra = t_co / (4.0 * nreps);
-    if (ms_stage) *ms_stage = t_st / (4.0 * nreps);
+    if (ms_co2contra) *ms_co2contra = t_co / nst;
+    if (ms_edge) *ms_edge = t_ed / nst;
+    if (ms_stage) *ms_stage = t_st / nst;
     return SWE_OK;
 }

@@ -17,27 +17,6 @@ constexpr int NPAN = 6;
 // Sides of a panel: 0 left (i = 1), 1 right (i = N+1), 2 bottom (j = 1), 3 top (j = N+1).
 enum { SIDE_L = 0, SIDE_R = 1, SIDE_B = 2, SIDE_T = 3 };
 
-// One-dimensional SBP 4-2 operators (src/differential_operators/sbp_operators/):
-//   OP_DI2C  difference, nodes -> centres   (sbp_diff_i2c_42_mod.f90)
-//   OP_DC2I  difference, centres -> nodes   (sbp_diff_c2i_42_mod.f90)
-//   OP_II2C  interpolation, nodes -> centres (sbp_interp_i2c_42_mod.f90)
-//   OP_IC2I  interpolation, centres -> nodes (sbp_interp_c2i_42_mod.f90)
-enum { OP_DI2C = 0, OP_DC2I = 1, OP_II2C = 2, OP_IC2I = 3 };
-
-// Each output row k (1..K) reads five consecutive inputs starting at `start`.
-// Rows 1..L use the left closure, rows K-L+1..K the right closure, the rest
-// the interior stencil.
-template <class T>
-struct OpTab {
-    int L;
-    int lstart[4];   // absolute start of left closure rows
-    int rstart[4];   // start = K + rstart[r] for row k = K - r
-    int ioff;        // interior start = k + ioff
-    T lw[4][5];
-    T rw[4][5];
-    T iw[5];
-};
-
 struct Dims {
     int N;         // cells per panel edge
     int P;         // row pitch in elements

@@ -1,64 +1,47 @@
-// swe_kernels.cuh -- sm_100a kernels of the linear shallow-water RK4 step on the
-// Ch-staggered equiangular cubed sphere (SBP 4-2), templated on the stencil type.
-//
-// This header holds the global-memory building blocks (stencil tables, edge
-// links, the neighbour-panel values used at panel boundaries) and the small
-// elementwise kernels; the per-stage kernels are in swe_tiled.cuh:
-//   k_co2contra_t : (u, v) of the stage input -> contravariant (ut, vt)
-//                   (co2contra_Ch_mod.f90:27-94)
-//   k_stage_t     : gradient + SAT, Coriolis with the ECS vector edge sync,
-//                   divergence + SAT with the Ah scalar edge sync, the linear
-//                   tendency (operator_swm_lin_mod.f90:66-108) and the RK4 update
-//                   (rk4_mod.f90:28-40) fused in one pass.
-// The MPI halo exchange of the reference is replaced by index-mapped reads of
-// the neighbouring panel in the same allocation (`Link` table): panel-edge
-// threads recompute the neighbour's edge values they need instead of waiting
-// for an exchange.
+// swe_kernels.cuh -- device building blocks of the linear shallow-water RK4 step
+// on the Ch-staggered equiangular cubed sphere (SBP 4-2): global-memory panel
+// views, the cube-edge halo reads that replace the reference's MPI exchanges,
+// the edge synchronisations, and the elementwise kernels.  The per-stage
+// kernels are in swe_tiled.cuh:
+//   k_co2contra : (u, v) of the stage input -> contravariant (ut, vt)
+//                 (co2contra_Ch_mod.f90:27-94)
+//   k_stage     : gradient + SAT, Coriolis with the ECS vector edge sync,
+//                 divergence + SAT with the Ah scalar edge sync, the linear
+//                 tendency (operator_swm_lin_mod.f90:66-108) and the RK4 update
+//                 (rk4_mod.f90:28-40) fused in one pass.
+// Threads that own panel-boundary vertices read the neighbouring panel in the
+// same allocation through the `Link` table and recompute the few neighbour
+// edge values they need, instead of waiting for an exchange.
 #pragma once
 
 #include "swe_common.cuh"
+#include "swe_sbp.cuh"
 
 namespace chswe {
 
-// Tables filled once per device by the host (single translation unit).
-__constant__ OpTab<double> c_op64[4];
-__constant__ OpTab<float> c_op32[4];
+// Edge connectivity, filled once per device by the host.
 __constant__ Link c_link[NPAN][4];
-__constant__ double c_sat64[8];
-__constant__ float c_sat32[8];
 
-template <class T> __device__ __forceinline__ const OpTab<T> &optab(int op);
-template <> __device__ __forceinline__ const OpTab<double> &optab<double>(int op) { return c_op64[op]; }
-template <> __device__ __forceinline__ const OpTab<float> &optab<float>(int op) { return c_op32[op]; }
-template <class T> __device__ __forceinline__ T satc(int k);
-template <> __device__ __forceinline__ double satc<double>(int k) { return c_sat64[k]; }
-template <> __device__ __forceinline__ float satc<float>(int k) { return c_sat32[k]; }
-// SAT constants: [0..2] 0.5*R1r/hrr of the i2c difference, [3] 0.5/h11 of the
-// c2i difference, [4..6] R11, R12, R13.
-
-// Row k (1-based) of operator `op` with K outputs: returns the first input index
-// and the five weights.
+// Read-only view of one field of one panel: v(i, j) with the reference's 1-based indices.
 template <class T>
-__device__ __forceinline__ int sten(int op, int k, int K, const T *&w)
+struct GV {
+    const T *p;
+    int P;
+    __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (j - 1) * P + (i - 1)); }
+};
+
+template <class T>
+__device__ __forceinline__ GV<T> gview(const T *member_base, const Dims &d, int field, int panel)
 {
-    const OpTab<T> &o = optab<T>(op);
-    if (k <= o.L) { w = o.lw[k - 1]; return o.lstart[k - 1]; }
-    int r = K - k;
-    if (r < o.L) { w = o.rw[r]; return K + o.rstart[r]; }
-    w = o.iw;
-    return k + o.ioff;
+    return GV<T>{member_base + field * d.fs + panel * d.ps, d.P};
+}
+template <class T>
+__device__ __forceinline__ GV<T> mview(const T *p, const Dims &d)
+{
+    return GV<T>{p, d.P};
 }
 
-__device__ __forceinline__ int64_t ofs(const Dims &d, int i, int j) { return (int64_t)(j - 1) * d.P + (i - 1); }
-
-// Field accessors inside one member's block (base = member start).
-template <class T>
-__device__ __forceinline__ T ld(const T *base, const Dims &d, int f, int t, int i, int j)
-{
-    return __ldg(base + f * d.fs + t * d.ps + ofs(d, i, j));
-}
-
-// Vertex of side `s` at along-edge index a (1..N+1), `depth` nodes inward.
+// Vertex of side s at along-edge index a (1..N+1), `depth` nodes inward.
 __device__ __forceinline__ void side_vertex(int N, int s, int a, int depth, int &i, int &j)
 {
     switch (s) {
@@ -69,30 +52,17 @@ __device__ __forceinline__ void side_vertex(int N, int s, int a, int depth, int 
     }
 }
 
-// ---------------------------------------------------------------------------
-// building blocks reading global memory (used everywhere, and by panel-edge
-// threads for the neighbour's values)
-// ---------------------------------------------------------------------------
-
-// Raw Coriolis vertex vector (coriolis_Ch_mod.f90:97-120) at xy point (k, l):
-// up = fJ2 * I_c2i,y(vt), vp = -fJ2 * I_c2i,x(ut).
+// Raw Coriolis vertex vector (coriolis_Ch_mod.f90:97-120) at xy point (k, l) of
+// panel t: up = fJ2 I_c2i,y(vt), vp = -fJ2 I_c2i,x(ut).
 template <class T>
 __device__ __forceinline__ void cor_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l,
                                         T &up, T &vp)
 {
-    const int N = d.N;
-    const T *w;
-    int s = sten<T>(OP_IC2I, k, N + 1, w);
-    T ur = 0;
-#pragma unroll
-    for (int q = 0; q < 5; q++)
-        if (w[q] != T(0)) ur += w[q] * ld(W, d, 1, t, s + q, l);
-    s = sten<T>(OP_IC2I, l, N + 1, w);
-    T vr = 0;
-#pragma unroll
-    for (int q = 0; q < 5; q++)
-        if (w[q] != T(0)) vr += w[q] * ld(W, d, 2, t, k, s + q);
-    T f = __ldg(m.fJ2 + t * d.ps + ofs(d, k, l));
+    const int n = d.N + 1;
+    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t);
+    T ur = ic2i<T>(k, n, [&](int c) { return U(c, l); });
+    T vr = ic2i<T>(l, n, [&](int c) { return V(k, c); });
+    T f = mview(m.fJ2 + t * d.ps, d)(k, l);
     up = f * vr;
     vp = -f * ur;
 }
@@ -115,114 +85,99 @@ __device__ __forceinline__ void cor_halo(const T *W, const Dims &d, const Metric
     else { vph = T(L.sn) * nrm; uph = T(L.st) * tan; }
 }
 
-// Synchronised Coriolis vertex vector: the covariant ECS Ah vector sync
-// (ecs_Ah_vec_sync_mod.f90:62-125, called with (U, V) = (vp, up)).
+// Covariant ECS Ah vector sync (ecs_Ah_vec_sync_mod.f90:62-125, called with
+// (U, V) = (vp, up)) at a panel-boundary vertex (k, l): the synchronised up from
+// the own raw up (V), and the synchronised vp from the own raw vp (U).
 template <class T>
-__device__ __forceinline__ void cor_sync(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l,
-                                         T &ups, T &vps)
+__device__ __forceinline__ T sync_up(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, T V)
 {
     const int n = d.N + 1;
-    T V, U;
-    cor_raw(W, d, m, t, k, l, V, U);   // V = up, U = vp
-    bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
-    if (!(il || ir || ib || it)) { ups = V; vps = U; return; }
-    const T half = T(0.5);
-    T uh, vh, Uh1, Vh1, Uh2, Vh2;
-    if ((il || ir) && (ib || it)) {
-        // cube corner: own value + the two neighbours' copies
-        int sx = il ? SIDE_L : SIDE_R, sy = ib ? SIDE_B : SIDE_T;
-        cor_halo(W, d, m, t, sx, l, uh, vh); Uh1 = vh; Vh1 = uh;   // x-side halo (U, V)
-        cor_halo(W, d, m, t, sy, k, uh, vh); Uh2 = vh; Vh2 = uh;   // y-side halo
-        T qx = il ? __ldg(m.ql + l - 1) : __ldg(m.qr + l - 1);
-        T qy = ib ? __ldg(m.qb + k - 1) : __ldg(m.qt + k - 1);
-        T Un = (U + Uh1 + Uh2 + qy * Vh2) / T(3);
-        T Vn = (V + Vh1 + Vh2 + qx * Uh1) / T(3);
-        ups = Vn; vps = Un;
-        return;
-    }
+    const bool il = (k == 1), ir = (k == n), ib = (l == 1);
+    T uh, vh;
     if (il || ir) {
         cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh, vh);
-        T q = il ? __ldg(m.ql + l - 1) : __ldg(m.qr + l - 1);
-        T Un = half * (U + vh);
-        T Vn = half * (V + uh + q * vh);
-        ups = Vn; vps = Un;
-        return;
+        const T qx = __ldg((il ? m.ql : m.qr) + l - 1);
+        if (l == 1 || l == n) {
+            T uh2, vh2;
+            cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh2, vh2);
+            return (V + uh + uh2 + qx * vh) / T(3);
+        }
+        return T(0.5) * (V + uh + qx * vh);
     }
-    // bottom / top side: V <- (V + V_h)/2, U <- (U + U_h + q V_h)/2
     cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh, vh);
-    T q = ib ? __ldg(m.qb + k - 1) : __ldg(m.qt + k - 1);
-    T Vn = half * (V + uh);
-    T Un = half * (U + vh + q * uh);
-    ups = Vn; vps = Un;
+    return T(0.5) * (V + uh);
 }
 
-// J * (normal contravariant component) of the neighbour across side s, at
-// centre depth c = 1..3 and along-edge index a: the halo the Ch vector
-// exchange (exchange_halo_Ch_mod.f90) delivers for the divergence SAT.
+template <class T>
+__device__ __forceinline__ T sync_vp(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, T U)
+{
+    const int n = d.N + 1;
+    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
+    T uh, vh;
+    if (ib || it) {
+        cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh, vh);
+        const T qy = __ldg((ib ? m.qb : m.qt) + k - 1);
+        if (il || ir) {
+            T uh1, vh1;
+            cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh1, vh1);
+            return (U + vh1 + vh + qy * uh) / T(3);
+        }
+        return T(0.5) * (U + vh + qy * uh);
+    }
+    cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh, vh);
+    return T(0.5) * (U + vh);
+}
+
+// J * (normal contravariant component) of the neighbour across side s, at centre
+// depth c = 1..3 and along-edge index a: the halo the Ch vector exchange
+// (exchange_halo_Ch_mod.f90) delivers for the divergence SAT.
 template <class T>
 __device__ __forceinline__ T ju_halo(const T *W, const Dims &d, const MetricView<T> &m, int t, int s, int a, int c)
 {
     const Link L = c_link[t][s];
     const int N = d.N;
-    int ap = L.rev ? N + 2 - a : a;
+    const int ap = L.rev ? N + 2 - a : a;
+    const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
+    const GV<T> U = gview(W, d, 1, L.nb), V = gview(W, d, 2, L.nb);
     T val;
     switch (L.nside) {
-    case SIDE_L: val = __ldg(m.Jy + ofs(d, c, ap)) * ld(W, d, 1, L.nb, c, ap); break;
-    case SIDE_R: val = __ldg(m.Jy + ofs(d, N + 1 - c, ap)) * ld(W, d, 1, L.nb, N + 1 - c, ap); break;
-    case SIDE_B: val = __ldg(m.Jx + ofs(d, ap, c)) * ld(W, d, 2, L.nb, ap, c); break;
-    default: val = __ldg(m.Jx + ofs(d, ap, N + 1 - c)) * ld(W, d, 2, L.nb, ap, N + 1 - c); break;
+    case SIDE_L: val = Jy(c, ap) * U(c, ap); break;
+    case SIDE_R: val = Jy(N + 1 - c, ap) * U(N + 1 - c, ap); break;
+    case SIDE_B: val = Jx(ap, c) * V(ap, c); break;
+    default: val = Jx(ap, N + 1 - c) * V(ap, N + 1 - c); break;
     }
     return T(L.sn) * val;
 }
 
-// Divergence at xy point (k, l) before the Ah projection (div_sbp_sat_mod.f90:54-80).
+// Divergence at xy point (k, l) before the Ah projection (div_sbp_sat_mod.f90:54-80),
+// SAT terms (sbp_diff_c2i_42_mod.f90:195-251) included.
 template <class T>
 __device__ __forceinline__ T div_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l)
 {
+    using namespace sbp;
     const int N = d.N, n = N + 1;
-    const T *w;
-    int s = sten<T>(OP_DC2I, k, n, w);
-    T dx = 0;
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-        int i = s + q;
-        if (w[q] != T(0)) dx += w[q] * (__ldg(m.Jy + ofs(d, i, l)) * ld(W, d, 1, t, i, l));
-    }
-    const T c0 = satc<T>(3), R11 = satc<T>(4), R12 = satc<T>(5), R13 = satc<T>(6);
-    if (k == 1) {
-        T j1 = __ldg(m.Jy + ofs(d, 1, l)) * ld(W, d, 1, t, 1, l);
-        T j2 = __ldg(m.Jy + ofs(d, 2, l)) * ld(W, d, 1, t, 2, l);
-        T j3 = __ldg(m.Jy + ofs(d, 3, l)) * ld(W, d, 1, t, 3, l);
-        dx += c0 * (R11 * (j1 - ju_halo(W, d, m, t, SIDE_L, l, 1)) + R12 * (j2 - ju_halo(W, d, m, t, SIDE_L, l, 2)) +
-                    R13 * (j3 - ju_halo(W, d, m, t, SIDE_L, l, 3)));
-    } else if (k == n) {
-        T j1 = __ldg(m.Jy + ofs(d, N, l)) * ld(W, d, 1, t, N, l);
-        T j2 = __ldg(m.Jy + ofs(d, N - 1, l)) * ld(W, d, 1, t, N - 1, l);
-        T j3 = __ldg(m.Jy + ofs(d, N - 2, l)) * ld(W, d, 1, t, N - 2, l);
-        dx -= c0 * (R11 * (j1 - ju_halo(W, d, m, t, SIDE_R, l, 1)) + R12 * (j2 - ju_halo(W, d, m, t, SIDE_R, l, 2)) +
-                    R13 * (j3 - ju_halo(W, d, m, t, SIDE_R, l, 3)));
-    }
-    s = sten<T>(OP_DC2I, l, n, w);
-    T dy = 0;
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-        int j = s + q;
-        if (w[q] != T(0)) dy += w[q] * (__ldg(m.Jx + ofs(d, k, j)) * ld(W, d, 2, t, k, j));
-    }
-    if (l == 1) {
-        T j1 = __ldg(m.Jx + ofs(d, k, 1)) * ld(W, d, 2, t, k, 1);
-        T j2 = __ldg(m.Jx + ofs(d, k, 2)) * ld(W, d, 2, t, k, 2);
-        T j3 = __ldg(m.Jx + ofs(d, k, 3)) * ld(W, d, 2, t, k, 3);
-        dy += c0 * (R11 * (j1 - ju_halo(W, d, m, t, SIDE_B, k, 1)) + R12 * (j2 - ju_halo(W, d, m, t, SIDE_B, k, 2)) +
-                    R13 * (j3 - ju_halo(W, d, m, t, SIDE_B, k, 3)));
-    } else if (l == n) {
-        T j1 = __ldg(m.Jx + ofs(d, k, N)) * ld(W, d, 2, t, k, N);
-        T j2 = __ldg(m.Jx + ofs(d, k, N - 1)) * ld(W, d, 2, t, k, N - 1);
-        T j3 = __ldg(m.Jx + ofs(d, k, N - 2)) * ld(W, d, 2, t, k, N - 2);
-        dy -= c0 * (R11 * (j1 - ju_halo(W, d, m, t, SIDE_T, k, 1)) + R12 * (j2 - ju_halo(W, d, m, t, SIDE_T, k, 2)) +
-                    R13 * (j3 - ju_halo(W, d, m, t, SIDE_T, k, 3)));
-    }
-    return (dx * m.inv_hx + dy * m.inv_hx) * __ldg(m.iJa + ofs(d, k, l));
+    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t), Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
+    auto ju = [&](int c) { return Jy(c, l) * U(c, l); };
+    auto jv = [&](int c) { return Jx(k, c) * V(k, c); };
+    T dx = dc2i<T>(k, n, ju);
+    if (k == 1)
+        dx += T(SATC) * (T(R11) * (ju(1) - ju_halo(W, d, m, t, SIDE_L, l, 1)) +
+                         T(R12) * (ju(2) - ju_halo(W, d, m, t, SIDE_L, l, 2)) +
+                         T(R13) * (ju(3) - ju_halo(W, d, m, t, SIDE_L, l, 3)));
+    else if (k == n)
+        dx -= T(SATC) * (T(R11) * (ju(N) - ju_halo(W, d, m, t, SIDE_R, l, 1)) +
+                         T(R12) * (ju(N - 1) - ju_halo(W, d, m, t, SIDE_R, l, 2)) +
+                         T(R13) * (ju(N - 2) - ju_halo(W, d, m, t, SIDE_R, l, 3)));
+    T dy = dc2i<T>(l, n, jv);
+    if (l == 1)
+        dy += T(SATC) * (T(R11) * (jv(1) - ju_halo(W, d, m, t, SIDE_B, k, 1)) +
+                         T(R12) * (jv(2) - ju_halo(W, d, m, t, SIDE_B, k, 2)) +
+                         T(R13) * (jv(3) - ju_halo(W, d, m, t, SIDE_B, k, 3)));
+    else if (l == n)
+        dy -= T(SATC) * (T(R11) * (jv(N) - ju_halo(W, d, m, t, SIDE_T, k, 1)) +
+                         T(R12) * (jv(N - 1) - ju_halo(W, d, m, t, SIDE_T, k, 2)) +
+                         T(R13) * (jv(N - 2) - ju_halo(W, d, m, t, SIDE_T, k, 3)));
+    return (dx * m.inv_hx + dy * m.inv_hx) * mview(m.iJa, d)(k, l);
 }
 
 template <class T>
@@ -235,23 +190,21 @@ __device__ __forceinline__ T div_halo(const T *W, const Dims &d, const MetricVie
     return div_raw(W, d, m, L.nb, k, l);
 }
 
-// Divergence after the Ah scalar sync (halo_Ah_scalar_sync_mod.f90:43-98).
+// Divergence after the Ah scalar sync (halo_Ah_scalar_sync_mod.f90:43-98) at a
+// panel-boundary vertex.
 template <class T>
 __device__ __forceinline__ T div_sync(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l)
 {
     const int n = d.N + 1;
     T f = div_raw(W, d, m, t, k, l);
-    bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
-    if (!(il || ir || ib || it)) return f;
+    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
     if ((il || ir) && (ib || it)) {
         T fx = div_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l);
         T fy = div_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k);
         return (f + fx + fy) / T(3);
     }
-    if (il) return T(0.5) * (div_halo(W, d, m, t, SIDE_L, l) + f);
-    if (ir) return T(0.5) * (f + div_halo(W, d, m, t, SIDE_R, l));
-    if (ib) return T(0.5) * (f + div_halo(W, d, m, t, SIDE_B, k));
-    return T(0.5) * (f + div_halo(W, d, m, t, SIDE_T, k));
+    if (il || ir) return T(0.5) * (f + div_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l));
+    return T(0.5) * (f + div_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k));
 }
 
 // h at the neighbour's copy of the shared vertex (xy halo index 0 / N+2).
@@ -262,12 +215,48 @@ __device__ __forceinline__ T h_halo(const T *Y, const Dims &d, int t, int s, int
     int ap = L.rev ? d.N + 2 - a : a;
     int k, l;
     side_vertex(d.N, L.nside, ap, 0, k, l);
-    return ld(Y, d, 0, L.nb, k, l);
+    return gview(Y, d, 0, L.nb)(k, l);
 }
 
-// ---------------------------------------------------------------------------
-// kernels
-// ---------------------------------------------------------------------------
+// Edge buffer: for every member, panel, side and along-edge vertex a = 1..N+1
+// the synchronised (up, vp, div) of that panel-boundary vertex.
+__device__ __forceinline__ int64_t edge_index(int N, int mem, int t, int s, int a)
+{
+    return ((((int64_t)mem * NPAN + t) * 4 + s) * (N + 1) + (a - 1)) * 3;
+}
+
+// The panel-boundary vertices' synchronised Coriolis vector (ECS Ah vector sync)
+// and divergence (Ah scalar sync), computed once per stage: the work the
+// reference does with its 'cross' and 'full' exchanges before the edge loops.
+// grid: x over along-edge vertices, y over panel*4 + side, z over members.
+template <class T>
+__global__ void __launch_bounds__(128) k_edge(const T *__restrict__ Wc, T *__restrict__ E, Dims d, MetricView<T> m)
+{
+    const int N = d.N, n = N + 1;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (a > n) return;
+    const int t = blockIdx.y / 4, s = blockIdx.y % 4, mem = blockIdx.z;
+    const T *w = Wc + mem * d.ms;
+    int k, l;
+    side_vertex(N, s, a, 0, k, l);
+    T up, vp;
+    cor_raw(w, d, m, t, k, l, up, vp);
+    T *e = E + edge_index(N, mem, t, s, a);
+    e[0] = sync_up(w, d, m, t, k, l, up);
+    e[1] = sync_vp(w, d, m, t, k, l, vp);
+    e[2] = div_sync(w, d, m, t, k, l);
+}
+
+// Synchronised (up, vp, div) of panel-boundary vertex (k, l) from the edge buffer.
+template <class T>
+__device__ __forceinline__ const T *edge_entry(const T *E, int N, int mem, int t, int k, int l)
+{
+    const int n = N + 1;
+    if (k == 1) return E + edge_index(N, mem, t, SIDE_L, l);
+    if (k == n) return E + edge_index(N, mem, t, SIDE_R, l);
+    if (l == 1) return E + edge_index(N, mem, t, SIDE_B, k);
+    return E + edge_index(N, mem, t, SIDE_T, k);
+}
 
 // RK4 stage parameters.
 struct StageArgs {
@@ -276,7 +265,7 @@ struct StageArgs {
     const double *Hm;  // per-member mean depth
 };
 
-// Kahan-compensated state update for FP32 (v0 += inc with compensation c).
+// Kahan-compensated state update for FP32 (s += inc with compensation c).
 __device__ __forceinline__ void kahan_add(float &s, float &c, float inc)
 {
     float yk = inc - c;

@@ -1,0 +1,117 @@
+// swe_sbp.cuh -- the one-dimensional SBP 4-2 operators of the Ch grid as
+// device stencils over an accessor f(index) (1-based input index).
+//
+// Coefficients (src/differential_operators/sbp_operators/):
+//   difference nodes -> centres   sbp_diff_i2c_42_mod.f90:12-20,  stencil :29-160, SAT :162-274
+//   difference centres -> nodes   sbp_diff_c2i_42_mod.f90:12-22,  stencil :32-193, SAT :195-251
+//   interpolation nodes -> centres sbp_interp_i2c_42_mod.f90:18-35
+//   interpolation centres -> nodes sbp_interp_c2i_42_mod.f90:13-27
+// Interior rows use compile-time coefficients; closure rows (three or four at
+// each end) are selected by a branch that is warp-uniform away from panel edges.
+#pragma once
+
+namespace chswe {
+namespace sbp {
+
+// difference, nodes -> centres
+constexpr double DI11 = -79.0 / 78.0, DI12 = 27.0 / 26.0, DI13 = -1.0 / 26.0, DI14 = 1.0 / 78.0;
+constexpr double DI21 = 2.0 / 21.0, DI22 = -9.0 / 7.0, DI23 = 9.0 / 7.0, DI24 = -2.0 / 21.0;
+constexpr double DI31 = 1.0 / 75.0, DI33 = -27.0 / 25.0, DI34 = 83.0 / 75.0, DI35 = -1.0 / 25.0;
+// boundary projection and SAT weights 0.5 R1r / h_rr of the nodes -> centres difference
+constexpr double R11 = 15.0 / 8.0, R12 = -5.0 / 4.0, R13 = 3.0 / 8.0;
+constexpr double SATI1 = 0.5 * R11 / (13.0 / 12.0), SATI2 = 0.5 * R12 / (7.0 / 8.0), SATI3 = 0.5 * R13 / (25.0 / 24.0);
+// difference, centres -> nodes
+constexpr double DC11 = -2.0, DC12 = 3.0, DC13 = -1.0, DC21 = -1.0, DC22 = 1.0;
+constexpr double DC31 = 1.0 / 24.0, DC32 = -9.0 / 8.0, DC33 = 9.0 / 8.0, DC34 = -1.0 / 24.0;
+constexpr double DC41 = -1.0 / 71.0, DC42 = 6.0 / 71.0, DC43 = -83.0 / 71.0, DC44 = 81.0 / 71.0, DC45 = -3.0 / 71.0;
+constexpr double SATC = 0.5 / (7.0 / 18.0);
+// interpolation free parameters
+constexpr double C13 = 0.1264926207034815, C14 = -0.029892648949074313;
+// interpolation, nodes -> centres
+constexpr double II11 = 1.0 / 2.0 + C13 + 2.0 * C14, II12 = 1.0 / 2.0 - 2.0 * C13 - 3.0 * C14, II13 = C13, II14 = C14;
+constexpr double II21 = -8.0 / 63.0 - 52.0 / 21.0 * C13 - 104.0 / 21.0 * C14;
+constexpr double II22 = 29.0 / 42.0 + 104.0 / 21.0 * C13 + 52.0 / 7.0 * C14;
+constexpr double II23 = -52.0 / 21.0 * C13 + 1.0 / 2.0, II24 = -52.0 / 21.0 * C14 - 4.0 / 63.0;
+constexpr double II31 = 26.0 / 25.0 * C13 + 52.0 / 25.0 * C14 - 1.0 / 25.0;
+constexpr double II32 = -1.0 / 50.0 - 52.0 / 25.0 * C13 - 78.0 / 25.0 * C14;
+constexpr double II33 = 3.0 / 5.0 + 26.0 / 25.0 * C13, II34 = 13.0 / 25.0 + 26.0 / 25.0 * C14, II35 = -3.0 / 50.0;
+// interpolation, centres -> nodes
+constexpr double IC11 = 39.0 / 28.0 + 39.0 / 14.0 * C13 + 39.0 / 7.0 * C14;
+constexpr double IC12 = -2.0 / 7.0 - 39.0 / 7.0 * C13 - 78.0 / 7.0 * C14;
+constexpr double IC13 = 39.0 / 14.0 * C13 + 39.0 / 7.0 * C14 - 3.0 / 28.0;
+constexpr double IC21 = 13.0 / 27.0 - 52.0 / 27.0 * C13 - 26.0 / 9.0 * C14;
+constexpr double IC22 = 29.0 / 54.0 + 104.0 / 27.0 * C13 + 52.0 / 9.0 * C14;
+constexpr double IC23 = -1.0 / 54.0 - 52.0 / 27.0 * C13 - 26.0 / 9.0 * C14;
+constexpr double IC31 = 13.0 / 12.0 * C13, IC32 = -13.0 / 6.0 * C13 + 7.0 / 16.0, IC33 = 5.0 / 8.0 + 13.0 / 12.0 * C13,
+                 IC34 = -1.0 / 16.0;
+constexpr double IC41 = 78.0 / 71.0 * C14, IC42 = -156.0 / 71.0 * C14 - 4.0 / 71.0, IC43 = 39.0 / 71.0 + 78.0 / 71.0 * C14,
+                 IC44 = 81.0 / 142.0, IC45 = -9.0 / 142.0;
+
+}  // namespace sbp
+
+// Difference nodes -> centres at centre k of n (inputs nodes 1..n+1).
+template <class T, class F>
+__device__ __forceinline__ T di2c(int k, int n, const F &f)
+{
+    using namespace sbp;
+    if (k >= 4 && k <= n - 3) return (T(27) * (f(k + 1) - f(k)) - (f(k + 2) - f(k - 1))) * T(1.0 / 24.0);
+    if (k == 1) return T(DI11) * f(1) + T(DI12) * f(2) + T(DI13) * f(3) + T(DI14) * f(4);
+    if (k == 2) return T(DI21) * f(1) + T(DI22) * f(2) + T(DI23) * f(3) + T(DI24) * f(4);
+    if (k == 3) return T(DI31) * f(1) + T(DI33) * f(3) + T(DI34) * f(4) + T(DI35) * f(5);
+    if (k == n - 2) return -T(DI31) * f(n + 1) - T(DI33) * f(n - 1) - T(DI34) * f(n - 2) - T(DI35) * f(n - 3);
+    if (k == n - 1) return -T(DI21) * f(n + 1) - T(DI22) * f(n) - T(DI23) * f(n - 1) - T(DI24) * f(n - 2);
+    return -T(DI11) * f(n + 1) - T(DI12) * f(n) - T(DI13) * f(n - 1) - T(DI14) * f(n - 2);
+}
+
+// Difference centres -> nodes at node k of nx (inputs centres 1..nx-1).
+template <class T, class F>
+__device__ __forceinline__ T dc2i(int k, int nx, const F &f)
+{
+    using namespace sbp;
+    if (k >= 5 && k <= nx - 4) return (T(27) * (f(k) - f(k - 1)) - (f(k + 1) - f(k - 2))) * T(1.0 / 24.0);
+    if (k == 1) return T(DC11) * f(1) + T(DC12) * f(2) + T(DC13) * f(3);
+    if (k == 2) return T(DC21) * f(1) + T(DC22) * f(2);
+    if (k == 3) return T(DC31) * f(1) + T(DC32) * f(2) + T(DC33) * f(3) + T(DC34) * f(4);
+    if (k == 4) return T(DC41) * f(1) + T(DC42) * f(2) + T(DC43) * f(3) + T(DC44) * f(4) + T(DC45) * f(5);
+    if (k == nx - 3)
+        return -T(DC41) * f(nx - 1) - T(DC42) * f(nx - 2) - T(DC43) * f(nx - 3) - T(DC44) * f(nx - 4) -
+               T(DC45) * f(nx - 5);
+    if (k == nx - 2) return -T(DC31) * f(nx - 1) - T(DC32) * f(nx - 2) - T(DC33) * f(nx - 3) - T(DC34) * f(nx - 4);
+    if (k == nx - 1) return -T(DC21) * f(nx - 1) - T(DC22) * f(nx - 2);
+    return -T(DC11) * f(nx - 1) - T(DC12) * f(nx - 2) - T(DC13) * f(nx - 3);
+}
+
+// Interpolation nodes -> centres at centre k of n.
+template <class T, class F>
+__device__ __forceinline__ T ii2c(int k, int n, const F &f)
+{
+    using namespace sbp;
+    if (k >= 4 && k <= n - 3) return (T(9) * (f(k + 1) + f(k)) - (f(k + 2) + f(k - 1))) * T(0.0625);
+    if (k == 1) return T(II11) * f(1) + T(II12) * f(2) + T(II13) * f(3) + T(II14) * f(4);
+    if (k == 2) return T(II21) * f(1) + T(II22) * f(2) + T(II23) * f(3) + T(II24) * f(4);
+    if (k == 3) return T(II31) * f(1) + T(II32) * f(2) + T(II33) * f(3) + T(II34) * f(4) + T(II35) * f(5);
+    if (k == n - 2)
+        return T(II31) * f(n + 1) + T(II32) * f(n) + T(II33) * f(n - 1) + T(II34) * f(n - 2) + T(II35) * f(n - 3);
+    if (k == n - 1) return T(II21) * f(n + 1) + T(II22) * f(n) + T(II23) * f(n - 1) + T(II24) * f(n - 2);
+    return T(II11) * f(n + 1) + T(II12) * f(n) + T(II13) * f(n - 1) + T(II14) * f(n - 2);
+}
+
+// Interpolation centres -> nodes at node k of nx.
+template <class T, class F>
+__device__ __forceinline__ T ic2i(int k, int nx, const F &f)
+{
+    using namespace sbp;
+    if (k >= 5 && k <= nx - 4) return (T(9) * (f(k) + f(k - 1)) - (f(k + 1) + f(k - 2))) * T(0.0625);
+    if (k == 1) return T(IC11) * f(1) + T(IC12) * f(2) + T(IC13) * f(3);
+    if (k == 2) return T(IC21) * f(1) + T(IC22) * f(2) + T(IC23) * f(3);
+    if (k == 3) return T(IC31) * f(1) + T(IC32) * f(2) + T(IC33) * f(3) + T(IC34) * f(4);
+    if (k == 4) return T(IC41) * f(1) + T(IC42) * f(2) + T(IC43) * f(3) + T(IC44) * f(4) + T(IC45) * f(5);
+    if (k == nx - 3)
+        return T(IC41) * f(nx - 1) + T(IC42) * f(nx - 2) + T(IC43) * f(nx - 3) + T(IC44) * f(nx - 4) +
+               T(IC45) * f(nx - 5);
+    if (k == nx - 2) return T(IC31) * f(nx - 1) + T(IC32) * f(nx - 2) + T(IC33) * f(nx - 3) + T(IC34) * f(nx - 4);
+    if (k == nx - 1) return T(IC21) * f(nx - 1) + T(IC22) * f(nx - 2) + T(IC23) * f(nx - 3);
+    return T(IC11) * f(nx - 1) + T(IC12) * f(nx - 2) + T(IC13) * f(nx - 3);
+}
+
+}  // namespace chswe

@@ -115,8 +115,9 @@ long long swe_launch_count(const swe_ctx *ctx);
 
 /* Diagnostic: advance v0 by nreps RK4 steps launched kernel by kernel with CUDA
    events around each launch; returns the mean duration in ms of the
-   contravariant-component kernel and of the fused stage kernel. */
-int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *ms_co2contra, double *ms_stage);
+   contravariant-component kernel, the panel-edge kernel and the fused stage kernel. */
+int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *ms_co2contra, double *ms_edge,
+                     double *ms_stage);
 
 /* Panel-edge connectivity used by the device halo reads (host-only, no GPU needed):
    for panel p (0..5) and side s (0 left i=1, 1 right i=N+1, 2 bottom j=1, 3 top j=N+1)

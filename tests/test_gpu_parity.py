@@ -224,4 +224,4 @@ def test_launch_count_reported():
     n0 = dom.launch_count()
     create_timescheme(st, "rk4").steps(st, op, dom, 100.0, 4)
     dom.synchronize()
-    assert dom.launch_count() - n0 == 4 * 8
+    assert dom.launch_count() - n0 == 4 * 12
