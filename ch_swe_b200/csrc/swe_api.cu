@@ -267,7 +267,7 @@ template <class T>
 static int build_metric(swe_ctx *c, DevMetric<T> &dm)
 {
     const int N = c->cfg.N, P = c->dims.P;
-    const size_t box = (size_t)(N + 1) * P;
+    const size_t box = (size_t)c->dims.ps;
     // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1
     const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1);
     std::vector<T> h(n_el, T(0));
@@ -278,17 +278,17 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
       *ql = qt + (N + 1), *qr = ql + (N + 1);
     for (int j = 1; j <= N + 1; j++)
         for (int i = 1; i <= N; i++) {
-            size_t k = (size_t)(j - 1) * my.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            size_t k = (size_t)(j - 1) * my.nx + (i - 1), o = (size_t)box_off(P, i, j);
             Q11y[o] = T(my.Q1[k]); iJy[o] = T(1.0 / my.J[k]); Jy[o] = T(my.J[k]);
         }
     for (int j = 1; j <= N; j++)
         for (int i = 1; i <= N + 1; i++) {
-            size_t k = (size_t)(j - 1) * mx.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            size_t k = (size_t)(j - 1) * mx.nx + (i - 1), o = (size_t)box_off(P, i, j);
             Q22x[o] = T(mx.Q3[k]); iJx[o] = T(1.0 / mx.J[k]); Jx[o] = T(mx.J[k]);
         }
     for (int j = 1; j <= N + 1; j++)
         for (int i = 1; i <= N + 1; i++) {
-            size_t k = (size_t)(j - 1) * mxy.nx + (i - 1), o = (size_t)(j - 1) * P + (i - 1);
+            size_t k = (size_t)(j - 1) * mxy.nx + (i - 1), o = (size_t)box_off(P, i, j);
             JQ12[o] = T(mxy.J[k] * mxy.Q2[k]);
             iJa[o] = T(1.0 / (mxy.J[k] * a));
             for (int p = 0; p < NPAN; p++) {
@@ -330,7 +330,7 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
 static int build_quadrature(swe_ctx *c)
 {
     const int N = c->cfg.N, P = c->dims.P;
-    const size_t box = (size_t)(N + 1) * P;
+    const size_t box = (size_t)c->dims.ps;
     std::vector<double> h(3 * box, 0.0);
     const double AI[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
     const double AC[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
@@ -350,7 +350,7 @@ static int build_quadrature(swe_ctx *c)
         for (int j = 1; j <= m.ny; j++)
             for (int i = 1; i <= m.nx; i++) {
                 double Ax = coeff(i, m.nx, m.nx == N + 1), Ay = coeff(j, m.ny, m.ny == N + 1);
-                h[q * box + (size_t)(j - 1) * P + (i - 1)] = m.J[(size_t)(j - 1) * m.nx + (i - 1)] * hx * hx * Ax * Ay;
+                h[q * box + (size_t)box_off(P, i, j)] = m.J[(size_t)(j - 1) * m.nx + (i - 1)] * hx * hx * Ax * Ay;
             }
     }
     if (cudaMalloc(&c->qw, h.size() * sizeof(double)) != cudaSuccess)
@@ -410,8 +410,8 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     cudaGetDevice(&c->device);
     const int N = cfg->N;
     c->dims.N = N;
-    c->dims.P = (N + 1 + 7) / 8 * 8;
-    c->dims.ps = (int64_t)(N + 1) * c->dims.P;
+    c->dims.P = (N + 1 + 2 * MG + 7) / 8 * 8;
+    c->dims.ps = (int64_t)(N + 1 + 2 * MG) * c->dims.P;
     c->dims.fs = NPAN * c->dims.ps;
     c->dims.ms = 3 * c->dims.fs;
     c->elem = cfg->precision == SWE_FP64 ? 8 : 4;
@@ -510,11 +510,11 @@ static void pack_member(const swe_ctx *c, const double *h, const double *u, cons
     const size_t ps = c->dims.ps, fs = c->dims.fs;
     for (int t = 0; t < NPAN; t++) {
         for (int j = 0; j <= N; j++)
-            for (int i = 0; i <= N; i++) box[0 * fs + t * ps + (size_t)j * P + i] = T(*h++);
+            for (int i = 0; i <= N; i++) box[0 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*h++);
         for (int j = 0; j <= N; j++)
-            for (int i = 0; i < N; i++) box[1 * fs + t * ps + (size_t)j * P + i] = T(*u++);
+            for (int i = 0; i < N; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
         for (int j = 0; j < N; j++)
-            for (int i = 0; i <= N; i++) box[2 * fs + t * ps + (size_t)j * P + i] = T(*v++);
+            for (int i = 0; i <= N; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
     }
 }
 template <class T>
@@ -524,11 +524,11 @@ static void unpack_member(const swe_ctx *c, const T *box, double *h, double *u, 
     const size_t ps = c->dims.ps, fs = c->dims.fs;
     for (int t = 0; t < NPAN; t++) {
         for (int j = 0; j <= N; j++)
-            for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + (size_t)j * P + i]);
+            for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + box_off(P, i + 1, j + 1)]);
         for (int j = 0; j <= N; j++)
-            for (int i = 0; i < N; i++) *u++ = double(box[1 * fs + t * ps + (size_t)j * P + i]);
+            for (int i = 0; i < N; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
         for (int j = 0; j < N; j++)
-            for (int i = 0; i <= N; i++) *v++ = double(box[2 * fs + t * ps + (size_t)j * P + i]);
+            for (int i = 0; i <= N; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
     }
 }
 
@@ -636,7 +636,7 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // ---------------------------------------------------------------------------
 // operator application and RK4
 // ---------------------------------------------------------------------------
-static dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
+static dim3 stage_block() { return dim3(TB_X, TB_Y, 1); }
 // Balanced tiles: ceil(N / nominal) tiles per direction, widths at most TILE_XM x TILE_YM.
 static dim3 stage_grid(const swe_ctx *c, int members = -1)
 {
@@ -767,23 +767,22 @@ __global__ void k_quad(const T *__restrict__ y, const T *__restrict__ w, const d
 {
     // blockIdx.x: slice of the rows, blockIdx.y: term (0 mass, 1 <h,h>, 2 <u,ut>, 3 <v,vt>)
     const int term = blockIdx.y;
-    const int64_t box = (int64_t)(d.N + 1) * d.P;
-    const int64_t n = NPAN * box;
+    const int n = d.N + 1, N = d.N;
+    const int64_t npts = (int64_t)NPAN * n * n;
     double acc = 0.0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        int64_t t = k / box, o = k % box;
-        int j = (int)(o / d.P) + 1, i = (int)(o % d.P) + 1;
-        const int N = d.N;
-        if (i > N + 1) continue;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npts; k += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(k / ((int64_t)n * n)), r = (int)(k % ((int64_t)n * n));
+        const int j = r / n + 1, i = r % n + 1;
+        const int64_t o = box_off(d.P, i, j);
         if (term <= 1) {
             double h = (double)y[0 * d.fs + t * d.ps + o];
             acc += (term == 0 ? h : h * h) * qw[o];
         } else if (term == 2) {
             if (i > N) continue;
-            acc += (double)y[1 * d.fs + t * d.ps + o] * (double)w[1 * d.fs + t * d.ps + o] * qw[box + o];
+            acc += (double)y[1 * d.fs + t * d.ps + o] * (double)w[1 * d.fs + t * d.ps + o] * qw[d.ps + o];
         } else {
             if (j > N) continue;
-            acc += (double)y[2 * d.fs + t * d.ps + o] * (double)w[2 * d.fs + t * d.ps + o] * qw[2 * box + o];
+            acc += (double)y[2 * d.fs + t * d.ps + o] * (double)w[2 * d.fs + t * d.ps + o] * qw[2 * d.ps + o];
         }
     }
     __shared__ double sh[256];

@@ -17,10 +17,20 @@ constexpr int NPAN = 6;
 // Sides of a panel: 0 left (i = 1), 1 right (i = N+1), 2 bottom (j = 1), 3 top (j = N+1).
 enum { SIDE_L = 0, SIDE_R = 1, SIDE_B = 2, SIDE_T = 3 };
 
+// Zero margin around every panel box: point (i, j), 1 <= i, j <= N+1, lives at
+// row j - 1 + MG, column i - 1 + MG of an (N+1+2MG)-row box, so stencil windows
+// reaching up to MG points beyond the panel read zeros without bounds checks.
+constexpr int MG = 4;
+
+__host__ __device__ __forceinline__ int64_t box_off(int P, int i, int j)
+{
+    return (int64_t)(j - 1 + MG) * P + (i - 1 + MG);
+}
+
 struct Dims {
     int N;         // cells per panel edge
-    int P;         // row pitch in elements
-    int64_t ps;    // panel stride   = (N+1) * P
+    int P;         // row pitch in elements (>= N+1+2MG, multiple of 8)
+    int64_t ps;    // panel stride   = (N+1+2MG) * P
     int64_t fs;    // field stride   = 6 * ps
     int64_t ms;    // member stride  = 3 * fs
 };

@@ -27,7 +27,7 @@ template <class T>
 struct GV {
     const T *p;
     int P;
-    __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (j - 1) * P + (i - 1)); }
+    __device__ __forceinline__ T operator()(int i, int j) const { return __ldg(p + (j - 1 + MG) * P + (i - 1 + MG)); }
 };
 
 template <class T>

@@ -115,3 +115,50 @@ __device__ __forceinline__ T ic2i(int k, int nx, const F &f)
 }
 
 }  // namespace chswe
+
+namespace chswe {
+
+// Strided view of a line of inputs in shared memory: f(c) = p[c * s] (p points at
+// input index 0).  The *_s variants evaluate interior rows inline and send the
+// few closure rows to out-of-line copies, so interior points execute only the
+// four-tap formula.
+template <class T>
+struct Line {
+    const T *p;
+    int s;
+    __device__ __forceinline__ T operator()(int c) const { return p[c * s]; }
+};
+
+template <class T> __device__ __noinline__ T di2c_cl(int k, int n, Line<T> f) { return di2c<T>(k, n, f); }
+template <class T> __device__ __noinline__ T dc2i_cl(int k, int nx, Line<T> f) { return dc2i<T>(k, nx, f); }
+template <class T> __device__ __noinline__ T ii2c_cl(int k, int n, Line<T> f) { return ii2c<T>(k, n, f); }
+template <class T> __device__ __noinline__ T ic2i_cl(int k, int nx, Line<T> f) { return ic2i<T>(k, nx, f); }
+
+template <class T>
+__device__ __forceinline__ T di2c_s(int k, int n, Line<T> f)
+{
+    if (__builtin_expect(k >= 4 && k <= n - 3, 1))
+        return (T(27) * (f(k + 1) - f(k)) - (f(k + 2) - f(k - 1))) * T(1.0 / 24.0);
+    return di2c_cl<T>(k, n, f);
+}
+template <class T>
+__device__ __forceinline__ T dc2i_s(int k, int nx, Line<T> f)
+{
+    if (__builtin_expect(k >= 5 && k <= nx - 4, 1))
+        return (T(27) * (f(k) - f(k - 1)) - (f(k + 1) - f(k - 2))) * T(1.0 / 24.0);
+    return dc2i_cl<T>(k, nx, f);
+}
+template <class T>
+__device__ __forceinline__ T ii2c_s(int k, int n, Line<T> f)
+{
+    if (__builtin_expect(k >= 4 && k <= n - 3, 1)) return (T(9) * (f(k + 1) + f(k)) - (f(k + 2) + f(k - 1))) * T(0.0625);
+    return ii2c_cl<T>(k, n, f);
+}
+template <class T>
+__device__ __forceinline__ T ic2i_s(int k, int nx, Line<T> f)
+{
+    if (__builtin_expect(k >= 5 && k <= nx - 4, 1)) return (T(9) * (f(k) + f(k - 1)) - (f(k + 1) + f(k - 2))) * T(0.0625);
+    return ic2i_cl<T>(k, nx, f);
+}
+
+}  // namespace chswe

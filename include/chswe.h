@@ -95,7 +95,8 @@ int swe_stvec_assign(swe_stvec *y, double s1, const swe_stvec *v1, double s2, co
 /* y = y + s1*v1 + s2*v2 ; v2 may be NULL. */
 int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, double s2, const swe_stvec *v2);
 /* Device storage of a state vector: element type (SWE_FP64/SWE_FP32), base pointer,
-   bytes, and the pitch/row layout [member][field h,u,v][panel][N+1 rows][pitch]. */
+   bytes, and the row pitch of the layout [member][field h,u,v][panel][N+9 rows][pitch],
+   point (i, j) (1-based) at row j+3, column i+3; the 4-point margins hold zeros. */
 int swe_stvec_device_view(const swe_stvec *vec, void **ptr, size_t *bytes, int *precision, int *pitch);
 
 /* vout = A(vin), A the linear shallow-water operator. */
