@@ -236,11 +236,10 @@ def run_precision(precision, ic, args, torch, dist, world):
     torch.cuda.synchronize()
     launches = dom.launch_count() - n0
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        from ch_swe_b200 import replicas
+        total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
         dist.barrier()
-    total_ms = float(t.item())
     final = st.download()
 
     # end-to-end through the public API: pinned host -> device, the day, device -> host
@@ -279,9 +278,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        from ch_swe_b200 import replicas
+        dist = replicas.init("nccl", local)
     cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu) else None
     from ch_swe_b200 import build
     build.build()

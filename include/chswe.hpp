@@ -1,0 +1,102 @@
+// chswe.hpp -- C++ host mirror of the reference's operator_t / stvec_t /
+// timescheme_t interfaces (src/operator_mod.f90:11-41, src/stvec/stvec_mod.f90:10-30,
+// src/time_schemes/timescheme_mod.f90:9-24) over the C ABI in chswe.h.
+// Header-only; errors throw std::runtime_error carrying swe_last_error().
+#pragma once
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "chswe.h"
+
+namespace chswe_host {
+
+inline void check(int rc, const swe_ctx *ctx, const char *what)
+{
+    if (rc != SWE_OK)
+        throw std::runtime_error(std::string(what) + ": status " + std::to_string(rc) +
+                                 (ctx ? std::string(" (") + swe_last_error(ctx) + ")" : std::string()));
+}
+
+// domain + device context (create_domain, src/domain/domain_factory_mod.f90:55-147)
+class domain_gpu_t {
+  public:
+    explicit domain_gpu_t(const swe_cfg &cfg) : cfg_(cfg) { check(swe_ctx_create(&cfg_, &ctx_), nullptr, "swe_ctx_create"); }
+    ~domain_gpu_t() { if (ctx_) swe_ctx_destroy(ctx_); }
+    domain_gpu_t(const domain_gpu_t &) = delete;
+    domain_gpu_t &operator=(const domain_gpu_t &) = delete;
+    swe_ctx *ctx() const { return ctx_; }
+    const swe_cfg &cfg() const { return cfg_; }
+
+  private:
+    swe_cfg cfg_;
+    swe_ctx *ctx_ = nullptr;
+};
+
+// stvec_swm_t on the device (src/models/shallow_water/stvec/stvec_swm_mod.f90:10-42)
+class stvec_swm_gpu_t {
+  public:
+    explicit stvec_swm_gpu_t(const domain_gpu_t &d) : d_(d) { check(swe_stvec_create(d.ctx(), &v_), d.ctx(), "swe_stvec_create"); }
+    ~stvec_swm_gpu_t() { if (v_) swe_stvec_destroy(v_); }
+    stvec_swm_gpu_t(const stvec_swm_gpu_t &) = delete;
+    stvec_swm_gpu_t &operator=(const stvec_swm_gpu_t &) = delete;
+    swe_stvec *handle() const { return v_; }
+
+    // y = s1*v1 + s2*v2 / y = s1*v1 (stvec_flexible_mod.f90:196-250)
+    void assign(double s1, const stvec_swm_gpu_t &v1, double s2, const stvec_swm_gpu_t &v2)
+    {
+        check(swe_stvec_assign(v_, s1, v1.v_, s2, v2.v_), d_.ctx(), "assign");
+    }
+    void assign(double s1, const stvec_swm_gpu_t &v1) { check(swe_stvec_assign(v_, s1, v1.v_, 0.0, nullptr), d_.ctx(), "assign"); }
+    // y = y + s1*v1 + s2*v2 (stvec_flexible_mod.f90:252-306)
+    void update(double s1, const stvec_swm_gpu_t &v1, double s2, const stvec_swm_gpu_t &v2)
+    {
+        check(swe_stvec_update(v_, s1, v1.v_, s2, v2.v_), d_.ctx(), "update");
+    }
+    void upload(int member, const double *h, const double *u, const double *v)
+    {
+        check(swe_stvec_upload(v_, member, h, u, v), d_.ctx(), "upload");
+    }
+    void download(int member, double *h, double *u, double *v) const
+    {
+        check(swe_stvec_download(v_, member, h, u, v), d_.ctx(), "download");
+    }
+
+  private:
+    const domain_gpu_t &d_;
+    swe_stvec *v_ = nullptr;
+};
+
+// operator_swm_lin_t (src/models/shallow_water/operator/operator_swm_lin_mod.f90:66-108)
+class operator_swm_lin_gpu_t {
+  public:
+    explicit operator_swm_lin_gpu_t(const domain_gpu_t &d) : d_(d) {}
+    void apply(stvec_swm_gpu_t &vout, const stvec_swm_gpu_t &vin)
+    {
+        check(swe_operator_apply(d_.ctx(), vout.handle(), vin.handle()), d_.ctx(), "operator apply");
+    }
+    void integrals(const stvec_swm_gpu_t &s, int member, double &mass, double &energy) const
+    {
+        check(swe_integrals(d_.ctx(), s.handle(), member, &mass, &energy), d_.ctx(), "integrals");
+    }
+    const domain_gpu_t &domain() const { return d_; }
+
+  private:
+    const domain_gpu_t &d_;
+};
+
+// rk4_t (src/time_schemes/rk4_mod.f90:20-42)
+class rk4_gpu_t {
+  public:
+    void step(stvec_swm_gpu_t &v0, operator_swm_lin_gpu_t &op, double dt)
+    {
+        check(swe_rk4_step(op.domain().ctx(), v0.handle(), dt), op.domain().ctx(), "rk4 step");
+    }
+    void steps(stvec_swm_gpu_t &v0, operator_swm_lin_gpu_t &op, double dt, int nsteps)
+    {
+        check(swe_rk4_steps(op.domain().ctx(), v0.handle(), dt, nsteps), op.domain().ctx(), "rk4 steps");
+    }
+};
+
+}  // namespace chswe_host

@@ -60,6 +60,7 @@ def lib():
         L.orc_metric.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
         L.orc_sync_weights.argtypes = [ctypes.c_void_p] + [_dp] * 4
         L.orc_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
+        L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         _lib = L
     return _lib
 
@@ -178,3 +179,13 @@ class Oracle:
         f2p = _p(np.ascontiguousarray(f2, dtype=np.float64)) if f2 is not None else None
         lib().orc_halo_probe(self._c, kind, _p(f), f2p, w, _p(out), _p(out2))
         return (out, out2) if kind != 0 else out
+
+
+def sbp1d(op: int, n: int, x) -> np.ndarray:
+    """One-dimensional SBP 4-2 operator on one line (0 i2c diff, 1 c2i diff without SAT,
+    2 i2c interpolation, 3 c2i interpolation)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    nout = n if op in (0, 2) else n + 1
+    out = np.empty(nout)
+    lib().orc_sbp1d(op, n, _p(x), _p(out))
+    return out

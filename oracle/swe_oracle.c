@@ -1203,3 +1203,61 @@ void orc_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int
         ring_out(&a, w, out); ring_out(&b, w, out2); fld_free(&a); fld_free(&b);
     }
 }
+
+/* One-dimensional SBP 4-2 operator on a single line, for pinning the
+   coefficient tables: op 0 = i2c difference (in: n+1 nodes, out: n centres),
+   1 = c2i difference (in: n centres, out: n+1 nodes, no SAT), 2 = i2c
+   interpolation, 3 = c2i interpolation.  Halo inputs are taken as zero. */
+void orc_sbp1d(int op, int n, const double *in, double *out)
+{
+    init_coeffs();
+    int nin = (op == 0 || op == 2) ? n + 1 : n;
+    fld_t a, b;
+    fld_init(&a, nin, 1, 5);
+    fld_init(&b, (op == 0 || op == 2) ? n : n + 1, 1, 5);
+    for (int t = 0; t < NPAN; t++)
+        for (int i = -4; i <= nin + 5; i++) FA(&a, t, i, 1) = 0.0;
+    for (int i = 1; i <= nin; i++) FA(&a, 0, i, 1) = in[i - 1];
+    switch (op) {
+    case 0: {
+        /* apply_tile only (no SAT) */
+        int t = 0, dir = 0, l = 1;
+        fld_t *o = &b;
+        const fld_t *ii = &a;
+#define O2(k) FA(o, t, k, l)
+#define I2(k) FA(ii, t, k, l)
+        O2(1) = DI_q11 * I2(1) + DI_q12 * I2(2) + DI_q13 * I2(3) + DI_q14 * I2(4);
+        O2(2) = DI_q21 * I2(1) + DI_q22 * I2(2) + DI_q23 * I2(3) + DI_q24 * I2(4);
+        O2(3) = DI_q31 * I2(1) + DI_q33 * I2(3) + DI_q34 * I2(4) + DI_q35 * I2(5);
+        for (int k = 4; k <= n - 3; k++) O2(k) = (27.0 * (I2(k + 1) - I2(k)) - (I2(k + 2) - I2(k - 1))) / 24.0;
+        O2(n - 2) = -DI_q31 * I2(n + 1) - DI_q33 * I2(n - 1) - DI_q34 * I2(n - 2) - DI_q35 * I2(n - 3);
+        O2(n - 1) = -DI_q21 * I2(n + 1) - DI_q22 * I2(n) - DI_q23 * I2(n - 1) - DI_q24 * I2(n - 2);
+        O2(n) = -DI_q11 * I2(n + 1) - DI_q12 * I2(n) - DI_q13 * I2(n - 1) - DI_q14 * I2(n - 2);
+        (void)dir;
+        break;
+    }
+    case 1: {
+        int t = 0, l = 1, nx = n + 1;
+        fld_t *o = &b;
+        const fld_t *ii = &a;
+        O2(1) = DC_q11 * I2(1) + DC_q12 * I2(2) + DC_q13 * I2(3);
+        O2(2) = DC_q21 * I2(1) + DC_q22 * I2(2);
+        O2(3) = DC_q31 * I2(1) + DC_q32 * I2(2) + DC_q33 * I2(3) + DC_q34 * I2(4);
+        O2(4) = DC_q41 * I2(1) + DC_q42 * I2(2) + DC_q43 * I2(3) + DC_q44 * I2(4) + DC_q45 * I2(5);
+        for (int k = 5; k <= nx - 4; k++) O2(k) = (27.0 * (I2(k) - I2(k - 1)) - (I2(k + 1) - I2(k - 2))) / 24.0;
+        O2(nx - 3) = -DC_q41 * I2(nx - 1) - DC_q42 * I2(nx - 2) - DC_q43 * I2(nx - 3) - DC_q44 * I2(nx - 4) - DC_q45 * I2(nx - 5);
+        O2(nx - 2) = -DC_q31 * I2(nx - 1) - DC_q32 * I2(nx - 2) - DC_q33 * I2(nx - 3) - DC_q34 * I2(nx - 4);
+        O2(nx - 1) = -DC_q21 * I2(nx - 1) - DC_q22 * I2(nx - 2);
+        O2(nx) = -DC_q11 * I2(nx - 1) - DC_q12 * I2(nx - 2) - DC_q13 * I2(nx - 3);
+#undef O2
+#undef I2
+        break;
+    }
+    case 2: interp_i2c(&b, &a, 0, 0, n, 1, 1); break;
+    default: interp_c2i(&b, &a, 0, 0, n + 1, 1, 1); break;
+    }
+    int nout = (op == 0 || op == 2) ? n : n + 1;
+    for (int i = 1; i <= nout; i++) out[i - 1] = FA(&b, 0, i, 1);
+    fld_free(&a);
+    fld_free(&b);
+}

@@ -1,0 +1,81 @@
+"""The device path's panel-edge connectivity (a geometric derivation from the
+panel frames, swe_api.cu:compute_links) against the reference's exchange
+machinery as restated literally in the oracle (transform_index, tile
+intersections, pack order, signs).  CPU only: swe_edge_links needs no GPU."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+
+N = 12
+
+
+@pytest.fixture(scope="module")
+def links(lib_built, oracle_built):
+    from ch_swe_b200 import edge_links
+    return edge_links(), Oracle(N)
+
+
+def side_vertex(s, a, depth):
+    return [(1 + depth, a), (N + 1 - depth, a), (a, 1 + depth), (a, N + 1 - depth)][s]
+
+
+def test_links_form_a_cube(links):
+    L, _ = links
+    for p in range(6):
+        nbs = {int(L[p, s, 0]) for s in range(4)}
+        assert len(nbs) == 4 and p not in nbs
+        for s in range(4):
+            nb, ns = int(L[p, s, 0]), int(L[p, s, 1])
+            assert int(L[nb, ns, 0]) == p and int(L[nb, ns, 1]) == s   # symmetric
+
+
+def test_scalar_xy_halo_full_width3(links):
+    L, o = links
+    rng = np.random.default_rng(0)
+    h = rng.standard_normal((6, N + 1, N + 1))
+    w = 3
+    H = o.halo_probe(0, h, w=w)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, _, _ = L[t, s]
+            for a in range(1, N + 2):
+                ap = N + 2 - a if rev else a
+                for d in range(3):
+                    i, j = [(0 - d, a), (N + 2 + d, a), (a, 0 - d), (a, N + 2 + d)][s]
+                    k, l = side_vertex(ns, ap, d)
+                    assert H[t, j + w - 1, i + w - 1] == h[nb, l - 1, k - 1]
+
+
+def test_vector_xy_halo_cross_width1(links):
+    L, o = links
+    rng = np.random.default_rng(1)
+    up, vp = rng.standard_normal((6, N + 1, N + 1)), rng.standard_normal((6, N + 1, N + 1))
+    U, V = o.halo_probe(1, up, vp, w=1)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, sn, st = L[t, s]
+            for a in range(1, N + 2):
+                ap = N + 2 - a if rev else a
+                i, j = [(0, a), (N + 2, a), (a, 0), (a, N + 2)][s]
+                k, l = side_vertex(ns, ap, 0)
+                upn, vpn = up[nb, l - 1, k - 1], vp[nb, l - 1, k - 1]
+                nrm, tan = (upn, vpn) if ns <= 1 else (vpn, upn)
+                uh, vh = (sn * nrm, st * tan) if s <= 1 else (st * tan, sn * nrm)
+                assert U[t, j, i] == uh and V[t, j, i] == vh
+
+
+def test_ch_vector_halo_normal_component(links):
+    L, o = links
+    rng = np.random.default_rng(2)
+    ut, vt = rng.standard_normal((6, N + 1, N)), rng.standard_normal((6, N, N + 1))
+    A, B = o.halo_probe(2, ut, vt, w=3)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, sn, _ = L[t, s]
+            for a in range(1, N + 2):
+                ap = N + 2 - a if rev else a
+                for c in (1, 2, 3):
+                    val = [ut[nb, ap - 1, c - 1], ut[nb, ap - 1, N - c], vt[nb, c - 1, ap - 1], vt[nb, N - c, ap - 1]][ns]
+                    ref = [A[t, a + 2, 3 - c], A[t, a + 2, N + c + 2], B[t, 3 - c, a + 2], B[t, N + c + 2, a + 2]][s]
+                    assert ref == sn * val

@@ -1,0 +1,142 @@
+"""Pins the CPU oracle (oracle/swe_oracle.c) by known-answer properties of the
+reference's discretisation (no Fortran toolchain or golden vectors exist for
+this path, so these properties, not a binary, pin the restatement).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import EARTH_GRAV, EARTH_RADIUS, Oracle
+
+
+@pytest.fixture(scope="module")
+def o24(oracle_built):
+    return Oracle(24)
+
+
+def smooth_h(o, seed, k=5):
+    rng = np.random.default_rng(seed)
+    h = o.zeros()[0]
+    for _ in range(k):
+        h += o.gaussian(lam0=rng.uniform(0, 2 * np.pi), phi0=np.arcsin(rng.uniform(-1, 1)),
+                        d0=rng.uniform(0.2, 0.5), amp=rng.uniform(-1, 1))[0]
+    return h
+
+
+def test_gradient_of_constant_vanishes(o24):
+    gx, gy = o24.grad(np.full(o24.zeros()[0].shape, 3.7))
+    assert np.abs(gx).max() < 1e-18 and np.abs(gy).max() < 1e-18
+
+
+def test_co2contra_symmetric_in_sbp_norm(o24):
+    rng = np.random.default_rng(1)
+    _, u, v = o24.zeros()
+    a1, a2, b1, b2 = (rng.standard_normal(x.shape) for x in (u, v, u, v))
+    ta1, ta2 = o24.co2contra(a1, a2)
+    tb1, tb2 = o24.co2contra(b1, b2)
+    lhs = o24.dot(1, a1, tb1) + o24.dot(2, a2, tb2)
+    rhs = o24.dot(1, ta1, b1) + o24.dot(2, ta2, b2)
+    assert abs(lhs - rhs) < 1e-13 * abs(lhs)
+
+
+def test_sbp_adjointness_grad_div(o24):
+    """<grad h, u^c>_u + <h, div u^c>_h = 0 for h continuous across panel edges."""
+    rng = np.random.default_rng(2)
+    h = smooth_h(o24, 3)
+    _, u, v = o24.zeros()
+    ut, vt = o24.co2contra(rng.standard_normal(u.shape), rng.standard_normal(v.shape))
+    gx, gy = o24.grad(h)
+    a = o24.dot(1, gx, ut) + o24.dot(2, gy, vt)
+    b = o24.dot(0, h, o24.div(ut, vt))
+    assert abs(a + b) < 1e-12 * abs(a)
+
+
+def test_coriolis_energy_neutral(o24):
+    rng = np.random.default_rng(4)
+    _, u, v = o24.zeros()
+    ut, vt = o24.co2contra(rng.standard_normal(u.shape), rng.standard_normal(v.shape))
+    cu, cv = o24.coriolis(ut, vt)
+    s = o24.dot(1, np.abs(cu), np.abs(ut)) + o24.dot(2, np.abs(cv), np.abs(vt))
+    assert abs(o24.dot(1, cu, ut) + o24.dot(2, cv, vt)) < 1e-13 * s
+
+
+def test_semidiscrete_energy_and_mass_conserved(o24):
+    rng = np.random.default_rng(5)
+    h = smooth_h(o24, 6)
+    _, u, v = o24.zeros()
+    u, v = rng.standard_normal(u.shape), rng.standard_normal(v.shape)
+    dh, du, dv = o24.apply(h, u, v)
+    ut, vt = o24.co2contra(u, v)
+    terms = [o24.h_mean * o24.dot(1, du, ut), o24.h_mean * o24.dot(2, dv, vt), o24.grav * o24.dot(0, h, dh)]
+    assert abs(sum(terms)) < 1e-10 * sum(abs(t) for t in terms)
+    assert abs(o24.dot(0, dh)) < 1e-12 * o24.dot(0, np.abs(dh))
+
+
+def test_mass_conserved_over_rk4(o24):
+    h, u, v = o24.gaussian(lam0=1.0, phi0=0.3, d0=0.2)
+    m0, _ = o24.integrals(h, u, v)
+    h1, u1, v1 = o24.rk4(h, u, v, 900.0, 8)
+    m1, _ = o24.integrals(h1, u1, v1)
+    assert abs(m1 - m0) < 1e-13 * abs(m0)
+
+
+def test_linear_williamson2_steady_state_converges(oracle_built):
+    """Linear TS2 is an exact steady state; the error after 1/4 day falls at ~3rd order."""
+    errs = []
+    axis = (np.sin(0.7), 0.0, np.cos(0.7))
+    for N in (16, 32):
+        o = Oracle(N, h_mean=29400 / EARTH_GRAV, axis=axis)
+        u0 = 2 * np.pi * EARTH_RADIUS / (12 * 86400)
+        h, u, v = o.ts2(u0=u0, h_mean=29400 / EARTH_GRAV, axis=axis, linear_mode=True)
+        dt = 900.0 * 32 / N                      # CFL ~ 0.5 for c = sqrt(gH) ~ 171 m/s
+        nsteps = int(round(6 * 3600.0 / dt))
+        h1, _, _ = o.rk4(h, u, v, dt, nsteps)
+        errs.append(np.abs(h1 - h).max() / np.abs(h).max())
+    order = np.log2(errs[0] / errs[1])
+    assert order > 2.0, (errs, order)
+
+
+@pytest.mark.parametrize("deg", [0, 1, 2])
+def test_sbp42_polynomial_exactness(oracle_built, deg):
+    """SBP 4-2 including the closure rows: differences exact up to degree 2; the
+    interpolations up to degree 1 (their free closure parameters c13, c14 minimise
+    the degree-2 error instead, sbp_interp_i2c_42_mod.f90:12-19)."""
+    from oracle.oracle import sbp1d
+    n = 20
+    xn = np.arange(n + 1, dtype=float)          # nodes 0..n
+    xc = np.arange(n, dtype=float) + 0.5         # centres
+    f = lambda x: (0.3 + 1.7 * x - 0.05 * x ** 2) if deg == 2 else (0.3 + 1.7 * x if deg == 1 else 0.3 + 0 * x)
+    df = lambda x: (1.7 - 0.1 * x) if deg == 2 else (1.7 + 0 * x if deg == 1 else 0 * x)
+    if deg <= 1:
+        assert np.allclose(sbp1d(2, n, f(xn)), f(xc), atol=1e-12)
+        assert np.allclose(sbp1d(3, n, f(xc)), f(xn), atol=1e-12)
+    assert np.allclose(sbp1d(0, n, f(xn)), df(xc), atol=1e-12)
+    assert np.allclose(sbp1d(1, n, f(xc)), df(xn), atol=1e-12)
+
+
+def test_sbp42_interior_cubic_exactness(oracle_built):
+    from oracle.oracle import sbp1d
+    n = 24
+    xn = np.arange(n + 1, dtype=float)
+    xc = np.arange(n, dtype=float) + 0.5
+    f = lambda x: 0.01 * x ** 3 - 0.2 * x ** 2 + x
+    df = lambda x: 0.03 * x ** 2 - 0.4 * x + 1
+    inner_c, inner_n = slice(4, n - 4), slice(5, n - 4)
+    assert np.allclose(sbp1d(2, n, f(xn))[inner_c], f(xc)[inner_c], atol=1e-12)
+    assert np.allclose(sbp1d(3, n, f(xc))[inner_n], f(xn)[inner_n], atol=1e-12)
+    assert np.allclose(sbp1d(0, n, f(xn))[inner_c], df(xc)[inner_c], atol=1e-12)
+    assert np.allclose(sbp1d(1, n, f(xc))[inner_n], df(xn)[inner_n], atol=1e-12)
+
+
+def test_golden_fixtures_regression(oracle_built):
+    """Committed oracle outputs (tests/golden/make_golden.py): a regression pin of the
+    restatement itself, not reference output."""
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "oracle_c8.npz")
+    g = np.load(path)
+    o = Oracle(8, h_mean=float(g["h_mean"]))
+    out = o.apply(g["h"], g["u"], g["v"])
+    for a, b in zip(out, (g["dh"], g["du"], g["dv"])):
+        assert np.array_equal(a, b)
+    r = o.rk4(g["h"], g["u"], g["v"], float(g["dt"]), int(g["nsteps"]))
+    for a, b in zip(r, (g["h3"], g["u3"], g["v3"])):
+        assert np.array_equal(a, b)
