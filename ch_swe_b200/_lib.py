@@ -16,7 +16,10 @@ SWE_FP64 = 0
 SWE_FP32 = 1
 SWE_OP_LINEAR = 0
 
-ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "no CUDA device"}
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "no CUDA device",
+          -5: "cube size above SWE_NOALLOC_MAX_N"}
+SWE_ETOOBIG = -5
+SWE_NOALLOC_MAX_N = 64
 
 EXPORTED = [
     "swe_cfg_default", "swe_ctx_create", "swe_ctx_destroy", "swe_last_error", "swe_set_stream",
@@ -24,7 +27,7 @@ EXPORTED = [
     "swe_stvec_upload", "swe_stvec_download", "swe_stvec_upload_all", "swe_stvec_download_all",
     "swe_stvec_assign", "swe_stvec_update", "swe_stvec_device_view", "swe_operator_apply",
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
-    "swe_kernel_times", "swe_operator_contravariant",
+    "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
 ]
 
 
@@ -80,6 +83,7 @@ def load(path: str = LIB_PATH):
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.swe_operator_apply.argtypes = [_vp, _vp, _vp]
     L.swe_operator_contravariant.argtypes = [_vp, _vp, _vp]
+    L.swe_operator_apply_noalloc.argtypes = [ctypes.POINTER(SweCfg), _vp, _vp, _vp]
     L.swe_rk4_step.argtypes = [_vp, _vp, ctypes.c_double]
     L.swe_rk4_steps.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int]
     L.swe_integrals.argtypes = [_vp, _vp, ctypes.c_int, _dp, _dp]

@@ -892,3 +892,214 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
     if (ms_stage) *ms_stage = t_st / nst;
     return SWE_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free operator apply.
+//
+// For host programs that cannot allocate device memory themselves (a Fortran
+// model whose GPU memory is owned by another runtime or a fixed pool, or code
+// running where cudaMalloc is not permitted): everything the linear operator
+// needs besides the caller's input and output lives in one static device array
+// of this library, sized for cubes up to SWE_NOALLOC_MAX_N.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int NA_MAXN = SWE_NOALLOC_MAX_N;
+constexpr int NA_ROWS = NA_MAXN + 1 + 2 * MG;
+constexpr int NA_P = (NA_ROWS + 7) / 8 * 8;
+constexpr size_t NA_BOX = (size_t)NA_ROWS * NA_P;
+constexpr size_t NA_METRIC = 14 * NA_BOX + 4 * (size_t)(NA_MAXN + 1);
+constexpr size_t NA_W = 3 * (size_t)NPAN * NA_BOX;
+constexpr size_t NA_EDGE = (size_t)NPAN * 4 * (NA_MAXN + 1) * 3;
+constexpr size_t NA_TOTAL = NA_METRIC + NA_W + NA_EDGE + 8;
+
+struct Frames {
+    int ex[NPAN][3], ey[NPAN][3], nn[NPAN][3];
+};
+
+struct NoallocDevice {
+    bool ready = false;
+    double *base = nullptr;      // device address of g_noalloc_scratch on this device
+    bool metric_ok = false;
+    swe_cfg cached{};            // configuration the stored metric was computed for
+};
+NoallocDevice g_noalloc[64];
+}  // namespace
+
+// Metric, Coriolis weights and vector-sync weights: [0, NA_METRIC); contravariant
+// scratch W: [NA_METRIC, +NA_W); edge buffer: next NA_EDGE; the mean depth H: last slot.
+static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
+
+// FP64 metric of an N-cube into the scratch layout used by build_metric (same
+// formulas, evaluated on the device).
+__global__ void k_noalloc_metric(double *M, int N, int P, int64_t box, double a, double omega, double ax, double ay,
+                                 double az, int cc, Frames fr)
+{
+    const int n = N + 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    double *Q11y = M, *iJy = M + box, *Jy = M + 2 * box, *Q22x = M + 3 * box, *iJx = M + 4 * box, *Jx = M + 5 * box,
+           *JQ12 = M + 6 * box, *iJa = M + 7 * box, *fJ2 = M + 8 * box, *qv = M + 14 * box;
+    if (i <= n && j <= n) {
+        const int64_t o = box_off(P, i, j);
+        const double ta_n = tan(-0.25 * pi + (i - 1) * hx), tb_n = tan(-0.25 * pi + (j - 1) * hx);
+        const double ta_c = tan(-0.25 * pi + (i - 1 + 0.5) * hx), tb_c = tan(-0.25 * pi + (j - 1 + 0.5) * hx);
+        if (i <= N) {   // y mesh: centre in i, node in j
+            const double sg = sqrt(1.0 + ta_c * ta_c + tb_n * tb_n), s2 = sg * sg;
+            const double J = (1.0 + ta_c * ta_c) * (1.0 + tb_n * tb_n) / (sg * sg * sg);
+            Q11y[o] = s2 / (1.0 + ta_c * ta_c); Jy[o] = J; iJy[o] = 1.0 / J;
+        }
+        if (j <= N) {   // x mesh: node in i, centre in j
+            const double sg = sqrt(1.0 + ta_n * ta_n + tb_c * tb_c), s2 = sg * sg;
+            const double J = (1.0 + ta_n * ta_n) * (1.0 + tb_c * tb_c) / (sg * sg * sg);
+            Q22x[o] = s2 / (1.0 + tb_c * tb_c); Jx[o] = J; iJx[o] = 1.0 / J;
+        }
+        const double sg = sqrt(1.0 + ta_n * ta_n + tb_n * tb_n), s2 = sg * sg;
+        const double J = (1.0 + ta_n * ta_n) * (1.0 + tb_n * tb_n) / (sg * sg * sg);
+        JQ12[o] = J * (s2 * ta_n * tb_n / ((1 + ta_n * ta_n) * (1 + tb_n * tb_n)));
+        iJa[o] = 1.0 / (J * a);
+        const double rp[3] = {ta_n / sg, tb_n / sg, 1.0 / sg};
+        for (int p = 0; p < NPAN; p++) {
+            double f;
+            if (cc) {
+                f = omega;
+            } else {
+                double r[3];
+                for (int dd = 0; dd < 3; dd++) r[dd] = fr.ex[p][dd] * rp[0] + fr.ey[p][dd] * rp[1] - fr.nn[p][dd] * rp[2];
+                const double pr = (ax * r[0] + ay * r[1] + az * r[2]) / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                f = 2 * omega * pr;
+            }
+            fJ2[p * box + o] = f * J * J;
+        }
+    }
+    if (j == 1 && i <= n) {   // covariant vector-sync weights along the sides
+        const double q = 0.25 * pi, al = -0.25 * pi + (i - 1) * hx;
+        auto tb = [](double al_, double be_, double &ta, double &tbv) { ta = tan(al_); tbv = tan(be_); };
+        double ta, tbv;
+        // qb: a2(al, -q) . b1(al, q) rotated
+        {
+            tb(al, -q, ta, tbv);
+            double s = pow(1.0 + pow(ta, 2.0) + pow(tbv, 2.0), 1.5);
+            double a2[3] = {-ta * tbv * (1.0 + pow(tbv, 2.0)) / s, (1.0 + pow(ta, 2.0)) * (1.0 + pow(tbv, 2.0)) / s,
+                            -tbv * (1.0 + pow(tbv, 2.0)) / s};
+            tb(al, q, ta, tbv);
+            double sg2 = sqrt(1.0 + ta * ta + tbv * tbv);
+            double b1[3] = {(1.0 + tbv * tbv - (ta * tbv) * (ta * tbv) / (1.0 + ta * ta)) / sg2, 0.0,
+                            -ta * (1.0 + tbv * tbv / (1 + ta * ta)) / sg2};
+            qv[i - 1] = a2[0] * b1[0] + a2[1] * (-b1[2]) + a2[2] * b1[1];
+        }
+        // qt: a2(al, q) . b1(al, -q)
+        {
+            tb(al, q, ta, tbv);
+            double s = pow(1.0 + pow(ta, 2.0) + pow(tbv, 2.0), 1.5);
+            double a2[3] = {-ta * tbv * (1.0 + pow(tbv, 2.0)) / s, (1.0 + pow(ta, 2.0)) * (1.0 + pow(tbv, 2.0)) / s,
+                            -tbv * (1.0 + pow(tbv, 2.0)) / s};
+            tb(al, -q, ta, tbv);
+            double sg2 = sqrt(1.0 + ta * ta + tbv * tbv);
+            double b1[3] = {(1.0 + tbv * tbv - (ta * tbv) * (ta * tbv) / (1.0 + ta * ta)) / sg2, 0.0,
+                            -ta * (1.0 + tbv * tbv / (1 + ta * ta)) / sg2};
+            qv[n + i - 1] = a2[0] * b1[0] + a2[1] * b1[2] + a2[2] * (-b1[1]);
+        }
+        const double be = al;
+        // ql: a1(-q, be) . b2(q, be)
+        {
+            tb(-q, be, ta, tbv);
+            double s = pow(1.0 + pow(ta, 2.0) + pow(tbv, 2.0), 1.5);
+            double a1[3] = {(1.0 + pow(ta, 2.0)) * (1.0 + pow(tbv, 2.0)) / s, -ta * tbv * (1.0 + pow(ta, 2.0)) / s,
+                            -ta * (1.0 + pow(ta, 2.0)) / s};
+            tb(q, be, ta, tbv);
+            double sg2 = sqrt(1.0 + ta * ta + tbv * tbv);
+            double b2[3] = {0.0, ((1 + ta * ta) - (ta * tbv) * (ta * tbv) / (1 + tbv * tbv)) / sg2,
+                            -tbv * (ta * ta / (1 + tbv * tbv) + 1.0) / sg2};
+            qv[2 * n + i - 1] = a1[0] * (-b2[2]) + a1[1] * b2[1] + a1[2] * b2[0];
+        }
+        // qr: a1(q, be) . b2(-q, be)
+        {
+            tb(q, be, ta, tbv);
+            double s = pow(1.0 + pow(ta, 2.0) + pow(tbv, 2.0), 1.5);
+            double a1[3] = {(1.0 + pow(ta, 2.0)) * (1.0 + pow(tbv, 2.0)) / s, -ta * tbv * (1.0 + pow(ta, 2.0)) / s,
+                            -ta * (1.0 + pow(ta, 2.0)) / s};
+            tb(-q, be, ta, tbv);
+            double sg2 = sqrt(1.0 + ta * ta + tbv * tbv);
+            double b2[3] = {0.0, ((1 + ta * ta) - (ta * tbv) * (ta * tbv) / (1 + tbv * tbv)) / sg2,
+                            -tbv * (ta * ta / (1 + tbv * tbv) + 1.0) / sg2};
+            qv[3 * n + i - 1] = a1[0] * b2[2] + a1[1] * b2[1] + a1[2] * (-b2[0]);
+        }
+    }
+}
+
+__global__ void k_noalloc_set(double *p, double v) { *p = v; }
+
+static bool same_geometry(const swe_cfg &a, const swe_cfg &b)
+{
+    return a.N == b.N && a.radius == b.radius && a.grav == b.grav && a.omega == b.omega &&
+           a.rotation_axis[0] == b.rotation_axis[0] && a.rotation_axis[1] == b.rotation_axis[1] &&
+           a.rotation_axis[2] == b.rotation_axis[2] && a.coriolis_constant == b.coriolis_constant;
+}
+
+extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin, double *vout, void *cuda_stream)
+{
+    if (!cfg || !vin || !vout || vin == vout) return SWE_EINVAL;
+    if (cfg->N > NA_MAXN) {
+        fprintf(stderr, "swe_operator_apply_noalloc: N = %d exceeds the static scratch limit SWE_NOALLOC_MAX_N = %d\n",
+                cfg->N, NA_MAXN);
+        return SWE_ETOOBIG;
+    }
+    if (cfg->N < 8 || !tiles_fit(cfg->N) || cfg->precision != SWE_FP64 || cfg->n_members != 1 ||
+        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
+        return SWE_EINVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWE_ENODEV;
+    NoallocDevice &nd = g_noalloc[dev];
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    if (!nd.ready) {
+        // once per device, with the device current: the array's device address and the edge tables
+        if (cudaGetSymbolAddress((void **)&nd.base, g_noalloc_scratch) != cudaSuccess) return SWE_ECUDA;
+        Link L[NPAN][4];
+        compute_links(L);
+        if (cudaMemcpyToSymbol(c_link, L, sizeof(L)) != cudaSuccess) return SWE_ECUDA;
+        if (dev < 64) g_tables_ready[dev] = true;
+        nd.ready = true;
+    }
+    const int N = cfg->N, n = N + 1;
+    Dims dm;
+    dm.N = N;
+    dm.P = (N + 1 + 2 * MG + 7) / 8 * 8;
+    dm.ps = (int64_t)(N + 1 + 2 * MG) * dm.P;
+    dm.fs = NPAN * dm.ps;
+    dm.ms = 3 * dm.fs;
+    double *M = nd.base, *W = nd.base + NA_METRIC, *E = W + NA_W, *Hp = E + NA_EDGE;
+    const int64_t box = dm.ps;
+    if (!nd.metric_ok || !same_geometry(nd.cached, *cfg)) {
+        if (cudaMemsetAsync(M, 0, NA_METRIC * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
+        Frames fr;
+        for (int p = 0; p < NPAN; p++)
+            for (int dd = 0; dd < 3; dd++) { fr.ex[p][dd] = EX[p][dd]; fr.ey[p][dd] = EY[p][dd]; fr.nn[p][dd] = NRM[p][dd]; }
+        dim3 g((n + 15) / 16, (n + 15) / 16), b(16, 16);
+        k_noalloc_metric<<<g, b, 0, st>>>(M, N, dm.P, box, cfg->radius, cfg->omega, cfg->rotation_axis[0],
+                                          cfg->rotation_axis[1], cfg->rotation_axis[2], cfg->coriolis_constant, fr);
+        if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
+        nd.cached = *cfg;
+        nd.metric_ok = true;
+    }
+    MetricView<double> mv;
+    mv.Q11y = M; mv.iJy = M + box; mv.Jy = M + 2 * box; mv.Q22x = M + 3 * box; mv.iJx = M + 4 * box;
+    mv.Jx = M + 5 * box; mv.JQ12 = M + 6 * box; mv.iJa = M + 7 * box; mv.fJ2 = M + 8 * box;
+    mv.qb = M + 14 * box; mv.qt = mv.qb + n; mv.ql = mv.qt + n; mv.qr = mv.ql + n;
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    mv.inv_hxa = 1.0 / (hx * cfg->radius);
+    mv.inv_hx = 1.0 / hx;
+    mv.grav = cfg->grav;
+    // the contravariant scratch is read with its zero margins: clear what this size uses
+    if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
+    k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
+    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
+    dim3 g(nbx, nby, NPAN), b(TB_X, TB_Y, 1);
+    k_co2contra<double><<<g, b, 0, st>>>(vin, W, dm, mv);
+    k_edge<double><<<dim3((n + 127) / 128, NPAN * 4, 1), 128, 0, st>>>(W, E, dm, mv);
+    StageArgs a{0, 0.0, Hp};
+    k_stage<double><<<g, b, 0, st>>>(vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a);
+    if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
+    return SWE_OK;
+}

@@ -49,6 +49,7 @@ extern "C" {
 #define SWE_ECUDA (-2)    /* CUDA runtime failure (message holds the CUDA error) */
 #define SWE_ENOMEM (-3)   /* device allocation failed */
 #define SWE_ENODEV (-4)   /* no usable CUDA device (the library has no CPU fallback) */
+#define SWE_ETOOBIG (-5)  /* cube size above SWE_NOALLOC_MAX_N for swe_operator_apply_noalloc */
 
 #define SWE_FP64 0
 #define SWE_FP32 1
@@ -119,6 +120,30 @@ long long swe_launch_count(const swe_ctx *ctx);
    contravariant-component kernel, the panel-edge kernel and the fused stage kernel. */
 int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *ms_co2contra, double *ms_edge,
                      double *ms_stage);
+
+/* Largest cube size swe_operator_apply_noalloc accepts (its scratch is a static device
+   array of about 1.5 MB that every GPU using the library holds until the process exits). */
+#define SWE_NOALLOC_MAX_N 64
+
+/* vout = A(vin) for callers that cannot allocate device memory -- a host model whose
+   GPU memory belongs to another runtime or a fixed pool, or code that must not call
+   cudaMalloc.  This entry point allocates nothing and needs no context: the caller
+   passes device pointers to one FP64 state (input) and one FP64 state (output) in the
+   layout swe_stvec_device_view describes (one member, pitch = (N + 9) rounded up to a
+   multiple of 8, 4-point zero margins around every panel, margins of vin zero), and
+   every intermediate lives in one static device array of this library.  It has no
+   counterpart in the reference (there the operator owns allocatable work fields).
+   Limits and behaviour:
+   - cfg->N <= SWE_NOALLOC_MAX_N, else SWE_ETOOBIG (with a message on stderr);
+     cfg->precision SWE_FP64, cfg->n_members 1, SWE_OP_LINEAR.
+   - The first call on a device, with that device current, looks up the array's
+     device address and uploads the edge tables; make that first call before any
+     stream capture.  A call with a new geometry (N, radius, rotation) recomputes the
+     metric into the array.
+   - Work runs asynchronously on cuda_stream (NULL: the legacy default stream).
+   - All calls share the one array, which keeps the last call's contents; calls that
+     overlap on the GPU (other streams, other host threads) race on it.  Not thread-safe. */
+int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin, double *vout, void *cuda_stream);
 
 /* Panel-edge connectivity used by the device halo reads (host-only, no GPU needed):
    for panel p (0..5) and side s (0 left i=1, 1 right i=N+1, 2 bottom j=1, 3 top j=N+1)
