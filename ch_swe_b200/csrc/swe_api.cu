@@ -396,6 +396,9 @@ static int alloc_box(swe_ctx *c, void **p)
     return SWE_OK;
 }
 
+template <class T>
+static cudaError_t stage_smem_optin();
+
 extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
 {
     if (!cfg || !out) return SWE_EINVAL;
@@ -421,6 +424,8 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SWE_ECUDA);
     c->stream = c->own_stream;
     if ((rc = upload_tables(c)) != SWE_OK) return bail(rc);
+    if ((cfg->precision == SWE_FP64 ? stage_smem_optin<double>() : stage_smem_optin<float>()) != cudaSuccess)
+        return bail(SWE_ECUDA);
     if (cfg->precision == SWE_FP64) rc = build_metric<double>(c, c->m64);
     else rc = build_metric<float>(c, c->m32);
     if (rc != SWE_OK) return bail(rc);
@@ -636,28 +641,73 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // ---------------------------------------------------------------------------
 // operator application and RK4
 // ---------------------------------------------------------------------------
-static dim3 stage_block() { return dim3(TB_X, TB_Y, 1); }
+static dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
 // Balanced tiles: ceil(N / nominal) tiles per direction, widths at most TILE_XM x TILE_YM.
+static dim3 stage_grid(int N, int members)
+{
+    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
+    return dim3(nbx, nby, NPAN * members);
+}
 static dim3 stage_grid(const swe_ctx *c, int members = -1)
 {
-    const int N = c->cfg.N;
-    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
-    return dim3(nbx, nby, NPAN * (members < 0 ? c->cfg.n_members : members));
+    return stage_grid(c->cfg.N, members < 0 ? c->cfg.n_members : members);
+}
+
+// The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
+// device and element type (the attribute belongs to the device's context).
+template <class T>
+static cudaError_t stage_smem_optin()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_co2contra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T>::bytes());
+    const int sb = (int)StageLayout<T>::bytes();
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess && dev < 64) done[dev] = true;
+    return e;
+}
+
+template <class T>
+static void launch_co2contra(dim3 g, const T *y, T *w, const Dims &d, const MetricView<T> &m, cudaStream_t st)
+{
+    k_co2contra<T><<<g, stage_block(), Co2Layout<T>::bytes(), st>>>(y, w, d, m);
+}
+
+template <class T>
+static void launch_stage(dim3 g, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp, const Dims &d,
+                         const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+{
+    const size_t sb = StageLayout<T>::bytes();
+    switch (a.mode) {
+    case 0: k_stage<T, 0><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: k_stage<T, 1><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: k_stage<T, 2><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: k_stage<T, 3><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: k_stage<T, 4><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    }
 }
 
 
-static dim3 edge_grid(const swe_ctx *c) { return dim3((c->cfg.N + 1 + 127) / 128, NPAN * 4, c->cfg.n_members); }
+static dim3 edge_grid(int N, int members) { return dim3((N + 1 + EDGE_CHUNK - 1) / EDGE_CHUNK, NPAN * 4, members); }
+static dim3 edge_grid(const swe_ctx *c) { return edge_grid(c->cfg.N, c->cfg.n_members); }
 
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const MetricView<T> &mv)
 {
-    dim3 g = stage_grid(c), b = stage_block();
-    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
-    k_edge<T><<<edge_grid(c), 128, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
+    dim3 g = stage_grid(c);
+    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, c->dims, mv, c->stream);
+    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
     StageArgs a{mode, dt, c->Hm};
-    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
-                                      (T *)cmp, c->dims, mv, a);
+    launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
+                    c->dims, mv, a, c->stream);
     c->launches += 3;
 }
 
@@ -679,11 +729,11 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
-    dim3 g = stage_grid(c), b = stage_block();
+    dim3 g = stage_grid(c);
     if (c->elem == 8)
-        k_co2contra<double><<<g, b, 0, c->stream>>>((const double *)vin->d, (double *)vout->d, c->dims, c->m64.v);
+        launch_co2contra<double>(g, (const double *)vin->d, (double *)vout->d, c->dims, c->m64.v, c->stream);
     else
-        k_co2contra<float><<<g, b, 0, c->stream>>>((const float *)vin->d, (float *)vout->d, c->dims, c->m32.v);
+        launch_co2contra<float>(g, (const float *)vin->d, (float *)vout->d, c->dims, c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
     return SWE_OK;
@@ -802,13 +852,13 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     dim3 g(nb, 4), b(256);
     // contravariant components of this member into the scratch, then the four sums
     Dims d1 = c->dims;
-    dim3 gs = stage_grid(c, 1), bs = stage_block();
+    dim3 gs = stage_grid(c, 1);
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        k_co2contra<double><<<gs, bs, 0, c->stream>>>((const double *)vec->d + mo, (double *)c->w, d1, c->m64.v);
+        launch_co2contra<double>(gs, (const double *)vec->d + mo, (double *)c->w, d1, c->m64.v, c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        k_co2contra<float><<<gs, bs, 0, c->stream>>>((const float *)vec->d + mo, (float *)c->w, d1, c->m32.v);
+        launch_co2contra<float>(gs, (const float *)vec->d + mo, (float *)c->w, d1, c->m32.v, c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
@@ -844,15 +894,15 @@ template <class T>
 static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, void *v0, void *y1, float *cmp, int mode,
                         double dt, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, cudaEvent_t e3)
 {
-    dim3 g = stage_grid(c), b = stage_block();
+    dim3 g = stage_grid(c);
     cudaEventRecord(e0, c->stream);
-    k_co2contra<T><<<g, b, 0, c->stream>>>((const T *)yin, (T *)c->w, c->dims, mv);
+    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    k_edge<T><<<edge_grid(c), 128, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
+    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm};
-    k_stage<T><<<g, b, 0, c->stream>>>((const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1,
-                                      (T *)c->acc, (T *)cmp, c->dims, mv, a);
+    launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc, (T *)cmp,
+                    c->dims, mv, a, c->stream);
     cudaEventRecord(e3, c->stream);
     c->launches += 3;
 }
@@ -1058,6 +1108,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         Link L[NPAN][4];
         compute_links(L);
         if (cudaMemcpyToSymbol(c_link, L, sizeof(L)) != cudaSuccess) return SWE_ECUDA;
+        if (stage_smem_optin<double>() != cudaSuccess) return SWE_ECUDA;
         if (dev < 64) g_tables_ready[dev] = true;
         nd.ready = true;
     }
@@ -1094,12 +1145,11 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
-    dim3 g(nbx, nby, NPAN), b(TB_X, TB_Y, 1);
-    k_co2contra<double><<<g, b, 0, st>>>(vin, W, dm, mv);
-    k_edge<double><<<dim3((n + 127) / 128, NPAN * 4, 1), 128, 0, st>>>(W, E, dm, mv);
+    dim3 g = stage_grid(N, 1);
+    launch_co2contra<double>(g, vin, W, dm, mv, st);
+    k_edge<double><<<edge_grid(N, 1), EDGE_THREADS, 0, st>>>(W, E, dm, mv);
     StageArgs a{0, 0.0, Hp};
-    k_stage<double><<<g, b, 0, st>>>(vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a);
+    launch_stage<double>(g, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }

@@ -9,9 +9,10 @@
 //                 divergence + SAT with the Ah scalar edge sync, the linear
 //                 tendency (operator_swm_lin_mod.f90:66-108) and the RK4 update
 //                 (rk4_mod.f90:28-40) fused in one pass.
-// Threads that own panel-boundary vertices read the neighbouring panel in the
-// same allocation through the `Link` table and recompute the few neighbour
-// edge values they need, instead of waiting for an exchange.
+//   k_edge      : the synchronised Coriolis vector and divergence of every
+//                 panel-boundary vertex, once per stage, into the edge buffer.
+// Neighbouring panels live in the same allocation: threads read across a cube
+// edge through the `Link` table instead of waiting for an exchange.
 #pragma once
 
 #include "swe_common.cuh"
@@ -52,82 +53,6 @@ __device__ __forceinline__ void side_vertex(int N, int s, int a, int depth, int 
     }
 }
 
-// Raw Coriolis vertex vector (coriolis_Ch_mod.f90:97-120) at xy point (k, l) of
-// panel t: up = fJ2 I_c2i,y(vt), vp = -fJ2 I_c2i,x(ut).
-template <class T>
-__device__ __forceinline__ void cor_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l,
-                                        T &up, T &vp)
-{
-    const int n = d.N + 1;
-    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t);
-    T ur = ic2i<T>(k, n, [&](int c) { return U(c, l); });
-    T vr = ic2i<T>(l, n, [&](int c) { return V(k, c); });
-    T f = mview(m.fJ2 + t * d.ps, d)(k, l);
-    up = f * vr;
-    vp = -f * ur;
-}
-
-// Halo vector at side s, along-edge index a, as the reference's 'cross' vector
-// exchange delivers it: the neighbour's raw vertex vector in this panel's frame.
-template <class T>
-__device__ __forceinline__ void cor_halo(const T *W, const Dims &d, const MetricView<T> &m, int t, int s, int a,
-                                         T &uph, T &vph)
-{
-    const Link L = c_link[t][s];
-    int ap = L.rev ? d.N + 2 - a : a;
-    int k, l;
-    side_vertex(d.N, L.nside, ap, 0, k, l);
-    T upn, vpn;
-    cor_raw(W, d, m, L.nb, k, l, upn, vpn);
-    bool nlr = L.nside <= SIDE_R;
-    T nrm = nlr ? upn : vpn, tan = nlr ? vpn : upn;
-    if (s <= SIDE_R) { uph = T(L.sn) * nrm; vph = T(L.st) * tan; }
-    else { vph = T(L.sn) * nrm; uph = T(L.st) * tan; }
-}
-
-// Covariant ECS Ah vector sync (ecs_Ah_vec_sync_mod.f90:62-125, called with
-// (U, V) = (vp, up)) at a panel-boundary vertex (k, l): the synchronised up from
-// the own raw up (V), and the synchronised vp from the own raw vp (U).
-template <class T>
-__device__ __forceinline__ T sync_up(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, T V)
-{
-    const int n = d.N + 1;
-    const bool il = (k == 1), ir = (k == n), ib = (l == 1);
-    T uh, vh;
-    if (il || ir) {
-        cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh, vh);
-        const T qx = __ldg((il ? m.ql : m.qr) + l - 1);
-        if (l == 1 || l == n) {
-            T uh2, vh2;
-            cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh2, vh2);
-            return (V + uh + uh2 + qx * vh) / T(3);
-        }
-        return T(0.5) * (V + uh + qx * vh);
-    }
-    cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh, vh);
-    return T(0.5) * (V + uh);
-}
-
-template <class T>
-__device__ __forceinline__ T sync_vp(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, T U)
-{
-    const int n = d.N + 1;
-    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
-    T uh, vh;
-    if (ib || it) {
-        cor_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k, uh, vh);
-        const T qy = __ldg((ib ? m.qb : m.qt) + k - 1);
-        if (il || ir) {
-            T uh1, vh1;
-            cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh1, vh1);
-            return (U + vh1 + vh + qy * uh) / T(3);
-        }
-        return T(0.5) * (U + vh + qy * uh);
-    }
-    cor_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l, uh, vh);
-    return T(0.5) * (U + vh);
-}
-
 // J * (normal contravariant component) of the neighbour across side s, at centre
 // depth c = 1..3 and along-edge index a: the halo the Ch vector exchange
 // (exchange_halo_Ch_mod.f90) delivers for the divergence SAT.
@@ -149,64 +74,6 @@ __device__ __forceinline__ T ju_halo(const T *W, const Dims &d, const MetricView
     return T(L.sn) * val;
 }
 
-// Divergence at xy point (k, l) before the Ah projection (div_sbp_sat_mod.f90:54-80),
-// SAT terms (sbp_diff_c2i_42_mod.f90:195-251) included.
-template <class T>
-__device__ __forceinline__ T div_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l)
-{
-    using namespace sbp;
-    const int N = d.N, n = N + 1;
-    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t), Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
-    auto ju = [&](int c) { return Jy(c, l) * U(c, l); };
-    auto jv = [&](int c) { return Jx(k, c) * V(k, c); };
-    T dx = dc2i<T>(k, n, ju);
-    if (k == 1)
-        dx += T(SATC) * (T(R11) * (ju(1) - ju_halo(W, d, m, t, SIDE_L, l, 1)) +
-                         T(R12) * (ju(2) - ju_halo(W, d, m, t, SIDE_L, l, 2)) +
-                         T(R13) * (ju(3) - ju_halo(W, d, m, t, SIDE_L, l, 3)));
-    else if (k == n)
-        dx -= T(SATC) * (T(R11) * (ju(N) - ju_halo(W, d, m, t, SIDE_R, l, 1)) +
-                         T(R12) * (ju(N - 1) - ju_halo(W, d, m, t, SIDE_R, l, 2)) +
-                         T(R13) * (ju(N - 2) - ju_halo(W, d, m, t, SIDE_R, l, 3)));
-    T dy = dc2i<T>(l, n, jv);
-    if (l == 1)
-        dy += T(SATC) * (T(R11) * (jv(1) - ju_halo(W, d, m, t, SIDE_B, k, 1)) +
-                         T(R12) * (jv(2) - ju_halo(W, d, m, t, SIDE_B, k, 2)) +
-                         T(R13) * (jv(3) - ju_halo(W, d, m, t, SIDE_B, k, 3)));
-    else if (l == n)
-        dy -= T(SATC) * (T(R11) * (jv(N) - ju_halo(W, d, m, t, SIDE_T, k, 1)) +
-                         T(R12) * (jv(N - 1) - ju_halo(W, d, m, t, SIDE_T, k, 2)) +
-                         T(R13) * (jv(N - 2) - ju_halo(W, d, m, t, SIDE_T, k, 3)));
-    return (dx * m.inv_hx + dy * m.inv_hx) * mview(m.iJa, d)(k, l);
-}
-
-template <class T>
-__device__ __forceinline__ T div_halo(const T *W, const Dims &d, const MetricView<T> &m, int t, int s, int a)
-{
-    const Link L = c_link[t][s];
-    int ap = L.rev ? d.N + 2 - a : a;
-    int k, l;
-    side_vertex(d.N, L.nside, ap, 0, k, l);
-    return div_raw(W, d, m, L.nb, k, l);
-}
-
-// Divergence after the Ah scalar sync (halo_Ah_scalar_sync_mod.f90:43-98) at a
-// panel-boundary vertex.
-template <class T>
-__device__ __forceinline__ T div_sync(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l)
-{
-    const int n = d.N + 1;
-    T f = div_raw(W, d, m, t, k, l);
-    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
-    if ((il || ir) && (ib || it)) {
-        T fx = div_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l);
-        T fy = div_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k);
-        return (f + fx + fy) / T(3);
-    }
-    if (il || ir) return T(0.5) * (f + div_halo(W, d, m, t, il ? SIDE_L : SIDE_R, l));
-    return T(0.5) * (f + div_halo(W, d, m, t, ib ? SIDE_B : SIDE_T, k));
-}
-
 // h at the neighbour's copy of the shared vertex (xy halo index 0 / N+2).
 template <class T>
 __device__ __forceinline__ T h_halo(const T *Y, const Dims &d, int t, int s, int a)
@@ -225,26 +92,164 @@ __device__ __forceinline__ int64_t edge_index(int N, int mem, int t, int s, int 
     return ((((int64_t)mem * NPAN + t) * 4 + s) * (N + 1) + (a - 1)) * 3;
 }
 
-// The panel-boundary vertices' synchronised Coriolis vector (ECS Ah vector sync)
-// and divergence (Ah scalar sync), computed once per stage: the work the
-// reference does with its 'cross' and 'full' exchanges before the edge loops.
-// grid: x over along-edge vertices, y over panel*4 + side, z over members.
+// One raw quantity at boundary vertex (k, l) of panel t, before any edge sync:
+//   q = 0: up = fJ2 I_c2i,y(vt)      q = 1: vp = -fJ2 I_c2i,x(ut)
+//          (coriolis_Ch_mod.f90:97-120)
+//   q = 2: c2i x-difference of J ut  q = 3: c2i y-difference of J vt
+//          with the SAT terms of sbp_diff_c2i_42_mod.f90:195-251 on the panel edge
+//          (div_sbp_sat_mod.f90:54-80 before the 1/(hx J) scaling).
 template <class T>
-__global__ void __launch_bounds__(128) k_edge(const T *__restrict__ Wc, T *__restrict__ E, Dims d, MetricView<T> m)
+__device__ __forceinline__ T edge_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, int q)
 {
+    using namespace sbp;
     const int N = d.N, n = N + 1;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    if (a > n) return;
-    const int t = blockIdx.y / 4, s = blockIdx.y % 4, mem = blockIdx.z;
+    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t);
+    if (q == 0) return mview(m.fJ2 + t * d.ps, d)(k, l) * ic2i<T>(l, n, [&](int c) { return V(k, c); });
+    if (q == 1) return -mview(m.fJ2 + t * d.ps, d)(k, l) * ic2i<T>(k, n, [&](int c) { return U(c, l); });
+    const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
+    if (q == 2) {
+        auto ju = [&](int c) { return Jy(c, l) * U(c, l); };
+        T dx = dc2i<T>(k, n, ju);
+        if (k == 1)
+            dx += T(SATC) * (T(R11) * (ju(1) - ju_halo(W, d, m, t, SIDE_L, l, 1)) +
+                             T(R12) * (ju(2) - ju_halo(W, d, m, t, SIDE_L, l, 2)) +
+                             T(R13) * (ju(3) - ju_halo(W, d, m, t, SIDE_L, l, 3)));
+        else if (k == n)
+            dx -= T(SATC) * (T(R11) * (ju(N) - ju_halo(W, d, m, t, SIDE_R, l, 1)) +
+                             T(R12) * (ju(N - 1) - ju_halo(W, d, m, t, SIDE_R, l, 2)) +
+                             T(R13) * (ju(N - 2) - ju_halo(W, d, m, t, SIDE_R, l, 3)));
+        return dx;
+    }
+    auto jv = [&](int c) { return Jx(k, c) * V(k, c); };
+    T dy = dc2i<T>(l, n, jv);
+    if (l == 1)
+        dy += T(SATC) * (T(R11) * (jv(1) - ju_halo(W, d, m, t, SIDE_B, k, 1)) +
+                         T(R12) * (jv(2) - ju_halo(W, d, m, t, SIDE_B, k, 2)) +
+                         T(R13) * (jv(3) - ju_halo(W, d, m, t, SIDE_B, k, 3)));
+    else if (l == n)
+        dy -= T(SATC) * (T(R11) * (jv(N) - ju_halo(W, d, m, t, SIDE_T, k, 1)) +
+                         T(R12) * (jv(N - 1) - ju_halo(W, d, m, t, SIDE_T, k, 2)) +
+                         T(R13) * (jv(N - 2) - ju_halo(W, d, m, t, SIDE_T, k, 3)));
+    return dy;
+}
+
+// The neighbour's copy (panel nb, vertex (kk, ll)) of boundary vertex (k, l) of
+// panel t across side s.
+__device__ __forceinline__ void nb_vertex(int N, int t, int s, int k, int l, int &nb, int &kk, int &ll)
+{
+    const Link L = c_link[t][s];
+    const int a = s <= SIDE_R ? l : k;
+    nb = L.nb;
+    side_vertex(N, L.nside, L.rev ? N + 2 - a : a, 0, kk, ll);
+}
+
+// The neighbour's raw vertex vector (upn, vpn) in this panel's frame, as the
+// reference's 'cross' vector exchange delivers it across side s.
+template <class T>
+__device__ __forceinline__ void halo_vec(int t, int s, T upn, T vpn, T &uh, T &vh)
+{
+    const Link L = c_link[t][s];
+    const bool nlr = L.nside <= SIDE_R;
+    const T nrm = nlr ? upn : vpn, tan = nlr ? vpn : upn;
+    if (s <= SIDE_R) { uh = T(L.sn) * nrm; vh = T(L.st) * tan; }
+    else { vh = T(L.sn) * nrm; uh = T(L.st) * tan; }
+}
+
+constexpr int EDGE_CHUNK = 32;    // along-edge vertices per block (balanced split, at most 32)
+constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the third panel at corners
+
+// The panel-boundary vertices' synchronised Coriolis vector (ECS Ah covariant
+// vector sync, ecs_Ah_vec_sync_mod.f90:62-125 with (U, V) = (vp, up)) and
+// divergence (Ah scalar sync, halo_Ah_scalar_sync_mod.f90:43-98): the work the
+// reference does with its 'cross' and 'full' exchanges before the edge loops.
+// Block = (chunk of vertices along one side of one panel of one member).
+// Phase 1: every raw quantity the chunk needs is one thread's stencil: warp w < 8
+// takes quantity w % 4 for copy w / 4 (own vertex / neighbour across this side),
+// warp 8 the copy of the third panel at the two cube corners.  Phase 2 combines
+// the copies from shared memory.  Copies are stored by direction (x-neighbour
+// across L/R, y-neighbour across B/T), so the two sides that meet at a corner
+// compute bit-identical corner values.
+template <class T>
+__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ Wc, T *__restrict__ E, Dims d,
+                                                        MetricView<T> m)
+{
+    __shared__ T raw[3][4][EDGE_CHUNK];   // [own, x-neighbour, y-neighbour][quantity][vertex]
+    const int N = d.N, n = N + 1;
+    const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
+    const int a0 = 1 + (blockIdx.x * n) / gridDim.x, a1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
     const T *w = Wc + mem * d.ms;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool xs = s <= SIDE_R;
+    if (warp < 8) {
+        const int a = a0 + lane, q = warp & 3;
+        if (a < a1) {
+            int k, l;
+            side_vertex(N, s, a, 0, k, l);
+            if (warp < 4) {
+                raw[0][q][lane] = edge_raw(w, d, m, t, k, l, q);
+            } else {
+                int nb, kk, ll;
+                nb_vertex(N, t, s, k, l, nb, kk, ll);
+                raw[xs ? 1 : 2][q][lane] = edge_raw(w, d, m, nb, kk, ll, q);
+            }
+        }
+    } else if (lane < 8) {
+        // the other neighbour of the corner vertices a = 1 and a = N+1
+        const int a = lane < 4 ? 1 : n, q = lane & 3;
+        if (a >= a0 && a < a1) {
+            int k, l, nb, kk, ll;
+            side_vertex(N, s, a, 0, k, l);
+            const int s2 = xs ? (l == 1 ? SIDE_B : SIDE_T) : (k == 1 ? SIDE_L : SIDE_R);
+            nb_vertex(N, t, s2, k, l, nb, kk, ll);
+            raw[xs ? 2 : 1][q][a - a0] = edge_raw(w, d, m, nb, kk, ll, q);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x >= a1 - a0) return;
+    const int v = threadIdx.x, a = a0 + v;
     int k, l;
     side_vertex(N, s, a, 0, k, l);
-    T up, vp;
-    cor_raw(w, d, m, t, k, l, up, vp);
+    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
+    const bool cx = il || ir, cy = ib || it;
+    const GV<T> iJa = mview(m.iJa, d);
+    const T V = raw[0][0][v], U = raw[0][1][v];
+    const T f = (raw[0][2][v] * m.inv_hx + raw[0][3][v] * m.inv_hx) * iJa(k, l);
+    T uhx = 0, vhx = 0, fx = 0, uhy = 0, vhy = 0, fy = 0;
+    if (cx) {
+        const int sx = il ? SIDE_L : SIDE_R;
+        int nb, kk, ll;
+        nb_vertex(N, t, sx, k, l, nb, kk, ll);
+        halo_vec(t, sx, raw[1][0][v], raw[1][1][v], uhx, vhx);
+        fx = (raw[1][2][v] * m.inv_hx + raw[1][3][v] * m.inv_hx) * iJa(kk, ll);
+    }
+    if (cy) {
+        const int sy = ib ? SIDE_B : SIDE_T;
+        int nb, kk, ll;
+        nb_vertex(N, t, sy, k, l, nb, kk, ll);
+        halo_vec(t, sy, raw[2][0][v], raw[2][1][v], uhy, vhy);
+        fy = (raw[2][2][v] * m.inv_hx + raw[2][3][v] * m.inv_hx) * iJa(kk, ll);
+    }
+    T sup, svp, sdiv;
+    if (cx && cy) {
+        const T qx = __ldg((il ? m.ql : m.qr) + l - 1), qy = __ldg((ib ? m.qb : m.qt) + k - 1);
+        sup = (V + uhx + uhy + qx * vhx) / T(3);
+        svp = (U + vhx + vhy + qy * uhy) / T(3);
+        sdiv = (f + fx + fy) / T(3);
+    } else if (cx) {
+        const T qx = __ldg((il ? m.ql : m.qr) + l - 1);
+        sup = T(0.5) * (V + uhx + qx * vhx);
+        svp = T(0.5) * (U + vhx);
+        sdiv = T(0.5) * (f + fx);
+    } else {
+        const T qy = __ldg((ib ? m.qb : m.qt) + k - 1);
+        sup = T(0.5) * (V + uhy);
+        svp = T(0.5) * (U + vhy + qy * uhy);
+        sdiv = T(0.5) * (f + fy);
+    }
     T *e = E + edge_index(N, mem, t, s, a);
-    e[0] = sync_up(w, d, m, t, k, l, up);
-    e[1] = sync_vp(w, d, m, t, k, l, vp);
-    e[2] = div_sync(w, d, m, t, k, l);
+    e[0] = sup;
+    e[1] = svp;
+    e[2] = sdiv;
 }
 
 // Synchronised (up, vp, div) of panel-boundary vertex (k, l) from the edge buffer.

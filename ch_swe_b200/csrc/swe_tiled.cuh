@@ -1,15 +1,18 @@
 // swe_tiled.cuh -- the per-stage stencil kernels, shared-memory tiled.
 //
-// A block of 32 x 8 threads owns a tile [i0, i1) x [j0, j1) of the (N+1) x (N+1)
+// A block of 256 threads owns a tile [i0, i1) x [j0, j1) of the (N+1) x (N+1)
 // box of one panel of one member.  Tiles are balanced: gridDim.x tiles split the
-// N+1 columns into widths floor/ceil((N+1)/gridDim.x) <= TILE_XM, likewise rows
-// (<= TILE_YM), so N+1 = 32k+1 gives no one-column slivers.  The block copies the
-// windows it needs (tile plus stencil footprint) from the zero-margined panel
-// boxes into shared memory without bounds checks, then evaluates the SBP
-// stencils there.  Warps run along rows, so closure branches of y-direction
-// stencils are warp-uniform; x-direction closures diverge only in the warps
-// that touch a panel's left or right edge.  Panel-boundary vertices take their
-// synchronised values from the edge buffer written by k_edge.
+// N+1 columns into widths floor/ceil((N+1)/gridDim.x) <= TILE_XM, likewise rows,
+// so N+1 = 32k+1 gives no one-column slivers.  The block copies the windows it
+// needs (tile plus stencil footprint) from the zero-margined panel boxes into
+// shared memory without bounds checks and evaluates the SBP stencils there.
+//
+// Every stencil pass is laid out so that its closure branch is warp-uniform:
+// y-direction stencils run in row-major passes (consecutive lanes = consecutive
+// columns of one row), x-direction stencils in column-major passes (consecutive
+// lanes = consecutive rows of one column).  Shared-memory windows have odd
+// pitches, so column-major passes are free of bank conflicts.  Panel-boundary
+// vertices take their synchronised values from the edge buffer written by k_edge.
 //
 // Footprints: a nodes->centres stencil for outputs [a, b) reads inputs
 // [a-2, b+3); a centres->nodes stencil reads [a-3, b+2) (closure rows included).
@@ -20,12 +23,13 @@
 namespace chswe {
 
 constexpr int TILE_XN = 32;     // nominal tile width (tiles = ceil(N / TILE_XN))
-constexpr int TILE_YN = 16;     // nominal tile height
+constexpr int TILE_YN = 32;     // nominal tile height
 constexpr int TILE_XM = 33;     // maximal tile width  (balanced split of N+1 columns)
-constexpr int TILE_YM = 17;     // maximal tile height
-constexpr int TB_X = 32, TB_Y = 8;   // threads per block
-constexpr int STAGE_THREADS = TB_X * TB_Y;
-constexpr int WX = TILE_XM + 5, WY = TILE_YM + 5;   // window extents with stencil footprint
+constexpr int TILE_YM = 33;     // maximal tile height
+constexpr int STAGE_THREADS = 256;
+constexpr int PW = TILE_XM + 6;   // odd pitch of the (tile + 5)-wide windows
+constexpr int PT = TILE_XM;       // odd pitch of tile-wide windows
+constexpr int RW = TILE_YM + 5;   // rows of (tile + 5)-high windows
 
 __device__ __forceinline__ void tile_range(int n, int &i0, int &i1, int &j0, int &j1)
 {
@@ -35,23 +39,22 @@ __device__ __forceinline__ void tile_range(int n, int &i0, int &i1, int &j0, int
     j1 = 1 + ((blockIdx.y + 1) * n) / gridDim.y;
 }
 
-// Shared-memory window of NX x NY points with origin (x0, y0) (1-based indices).
-template <class T, int NX, int NY>
-struct Win {
-    T a[NX * NY];
-    __device__ __forceinline__ T &at(int x0, int y0, int i, int j) { return a[(j - y0) * NX + (i - x0)]; }
-    __device__ __forceinline__ Line<T> row(int x0, int y0, int j) const { return Line<T>{a + (j - y0) * NX - x0, 1}; }
-    __device__ __forceinline__ Line<T> col(int x0, int y0, int i) const { return Line<T>{a + (i - x0) - y0 * NX, NX}; }
-};
-
-// Copy the window [x0, x0+NX) x [y0, y0+NY) of a zero-margined panel box.
-template <class T, int NX, int NY>
-__device__ __forceinline__ void stage(Win<T, NX, NY> &w, const T *panel, int P, int x0, int y0)
+// q -> (a, b) with q = a * w + b, 0 <= b < w (q < 2^16, w <= 64): exact with a float reciprocal.
+__device__ __forceinline__ void split(int q, int w, float inv_w, int &a, int &b)
 {
-    const T *g = panel + box_off(P, x0, y0);
-    for (int r = threadIdx.y; r < NY; r += TB_Y)
-        for (int c = threadIdx.x; c < NX; c += TB_X) w.a[r * NX + c] = __ldg(g + r * P + c);
+    a = __float2int_rz(((float)q + 0.5f) * inv_w);
+    b = q - a * w;
 }
+
+// Shared-memory window of pitch NP with origin (x0, y0) (1-based indices).
+template <class T, int NP>
+struct SWin {
+    T *a;
+    int x0, y0;
+    __device__ __forceinline__ T &at(int i, int j) const { return a[(j - y0) * NP + (i - x0)]; }
+    __device__ __forceinline__ Line<T> row(int j) const { return Line<T>{a + (j - y0) * NP - x0, 1}; }
+    __device__ __forceinline__ Line<T> col(int i) const { return Line<T>{a + (i - x0) - y0 * NP, NP}; }
+};
 
 // Interior rows of the four operators (the closure rows go through the general
 // functions of swe_sbp.cuh).
@@ -71,85 +74,161 @@ template <class T> __device__ __forceinline__ T di2c_in(int k, const Line<T> &f)
 {
     return (T(27) * (f(k + 1) - f(k)) - (f(k + 2) - f(k - 1))) * T(1.0 / 24.0);
 }
-template <class T> __device__ __forceinline__ T ic2i_x(int k, int nx, const Line<T> &f)
+template <class T> __device__ __forceinline__ T ic2i_u(int k, int nx, const Line<T> &f)
 {
     return (k >= 5 && k <= nx - 4) ? ic2i_in<T>(k, f) : ic2i<T>(k, nx, f);
 }
-template <class T> __device__ __forceinline__ T ii2c_x(int k, int n, const Line<T> &f)
+template <class T> __device__ __forceinline__ T ii2c_u(int k, int n, const Line<T> &f)
 {
     return (k >= 4 && k <= n - 3) ? ii2c_in<T>(k, f) : ii2c<T>(k, n, f);
 }
-template <class T> __device__ __forceinline__ T dc2i_x(int k, int nx, const Line<T> &f)
+template <class T> __device__ __forceinline__ T dc2i_u(int k, int nx, const Line<T> &f)
 {
     return (k >= 5 && k <= nx - 4) ? dc2i_in<T>(k, f) : dc2i<T>(k, nx, f);
 }
-template <class T> __device__ __forceinline__ T di2c_x(int k, int n, const Line<T> &f)
+template <class T> __device__ __forceinline__ T di2c_u(int k, int n, const Line<T> &f)
 {
     return (k >= 4 && k <= n - 3) ? di2c_in<T>(k, f) : di2c<T>(k, n, f);
 }
+
+// Loop trip bounds of the flattened passes (256 threads): (tile+5)^2 windows,
+// (tile+5) x tile strips, tile^2.
+constexpr int IT_WIN = ((TILE_XM + 5) * (TILE_YM + 5) + STAGE_THREADS - 1) / STAGE_THREADS;
+constexpr int IT_STRIP = ((TILE_XM + 5) * TILE_YM + STAGE_THREADS - 1) / STAGE_THREADS;
+constexpr int IT_TILE = (TILE_XM * TILE_YM + STAGE_THREADS - 1) / STAGE_THREADS;
+static_assert(TILE_XM == TILE_YM, "strip bound assumes square maximal tiles");
+
+// Every global load of a pass is issued into registers before the first
+// shared-memory store or stencil of that pass (fixed-trip unrolled loops), so a
+// block pays one memory round trip per batch instead of one per loop iteration.
 
 // ---------------------------------------------------------------------------
 // contravariant components (co2contra_Ch_mod.f90:27-94)
 //   ut = Qi11 u + J^-1 I_i2c,x( J Qi12 I_c2i,y(v) ),  vt = Qi22 v + J^-1 I_i2c,y( J Qi12 I_c2i,x(u) )
 // ---------------------------------------------------------------------------
 template <class T>
-struct Co2Smem {
-    Win<T, WX, WY> v;              // origin (i0-2, j0-3)
-    Win<T, WX, WY> u;              // origin (i0-3, j0-2)
-    Win<T, WX, TILE_YM> vq;        // J Qi12 I_c2i,y(v) at xy, origin (i0-2, j0)
-    Win<T, TILE_XM, WY> uq;        // J Qi12 I_c2i,x(u) at xy, origin (i0, j0-2)
+struct Co2Layout {
+    static constexpr int V = 0, U = V + PW * RW, VQ = U + PW * RW, UQ = VQ + PW * TILE_YM, UX = UQ + PT * RW,
+                         TOTAL = UX + PT * TILE_YM;
+    static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
 
 template <class T>
-__global__ void __launch_bounds__(STAGE_THREADS) k_co2contra(const T *__restrict__ Y, T *__restrict__ W, Dims d,
+__global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W, Dims d,
                                                               MetricView<T> m)
 {
-    __shared__ Co2Smem<T> sm;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using L = Co2Layout<T>;
+    T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
     tile_range(n, i0, i1, j0, j1);
-    const int tw = i1 - i0, th = j1 - j0;
+    const int tw = i1 - i0, th = j1 - j0, w5 = tw + 5, h5 = th + 5;
+    const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
     const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
     const T *y = Y + mem * d.ms + t * d.ps;
     T *w = W + mem * d.ms + t * d.ps;
-    const int vx0 = i0 - 2, vy0 = j0 - 3, ux0 = i0 - 3, uy0 = j0 - 2;
+    const SWin<T, PW> sv{sm + L::V, i0 - 2, j0 - 3}, su{sm + L::U, i0 - 3, j0 - 2}, svq{sm + L::VQ, i0 - 2, j0};
+    const SWin<T, PT> suq{sm + L::UQ, i0, j0 - 2}, sux{sm + L::UX, i0, j0};
 
-    stage(sm.v, y + 2 * d.fs, P, vx0, vy0);
-    stage(sm.u, y + 1 * d.fs, P, ux0, uy0);
-    __syncthreads();
-    for (int r = threadIdx.y; r < th; r += TB_Y) {
-        const int l = j0 + r;
-        const bool inner = (l >= 5 && l <= n - 4);   // warp-uniform
-        for (int c = threadIdx.x; c < tw + 5; c += TB_X) {
-            const int k = vx0 + c;
-            const Line<T> f = sm.v.col(vx0, vy0, k);
-            const T q = inner ? ic2i_in<T>(l, f) : ic2i<T>(l, n, f);
-            sm.vq.a[r * WX + c] = q * __ldg(m.JQ12 + box_off(P, k, l));
+    // ---- batch 1: v and u windows, J Qi12 at both xy intermediates
+    T jq1[IT_STRIP], jq2[IT_STRIP];
+    {
+        const T *gv = y + 2 * d.fs + box_off(P, sv.x0, sv.y0), *gu = y + d.fs + box_off(P, su.x0, su.y0);
+        T rv[IT_WIN], ru[IT_WIN];
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            const bool ok = q < w5 * h5;
+            rv[it] = ok ? __ldg(gv + r * P + c) : T(0);
+            ru[it] = ok ? __ldg(gu + r * P + c) : T(0);
         }
-    }
-    for (int r = threadIdx.y; r < th + 5; r += TB_Y) {
-        const int l = uy0 + r;
-        const Line<T> f = sm.u.row(ux0, uy0, l);
-        for (int c = threadIdx.x; c < tw; c += TB_X) {
-            const int k = i0 + c;
-            sm.uq.a[r * TILE_XM + c] = ic2i_x<T>(k, n, f) * __ldg(m.JQ12 + box_off(P, k, l));
+#pragma unroll
+        for (int it = 0; it < IT_STRIP; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            jq1[it] = q < w5 * th ? __ldg(m.JQ12 + box_off(P, sv.x0 + c, j0 + r)) : T(0);
+            split(q, tw, iw, r, c);
+            jq2[it] = q < tw * h5 ? __ldg(m.JQ12 + box_off(P, i0 + c, suq.y0 + r)) : T(0);
         }
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < th; r += TB_Y) {
-        const int j = j0 + r;
-        const bool jin = (j >= 4 && j <= N - 3);   // warp-uniform
-        const Line<T> fq = sm.vq.row(vx0, j0, j);
-        for (int c = threadIdx.x; c < tw; c += TB_X) {
-            const int i = i0 + c;
-            const int64_t o = box_off(P, i, j);
-            if (i <= N)
-                w[d.fs + o] = __ldg(m.Q11y + o) * sm.u.at(ux0, uy0, i, j) + ii2c_x<T>(i, N, fq) * __ldg(m.iJy + o);
-            if (j <= N) {
-                const Line<T> g = sm.uq.col(i0, uy0, i);
-                const T acc = jin ? ii2c_in<T>(j, g) : ii2c<T>(j, N, g);
-                w[2 * d.fs + o] = __ldg(m.Q22x + o) * sm.v.at(vx0, vy0, i, j) + acc * __ldg(m.iJx + o);
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            if (q < w5 * h5) {
+                sv.a[r * PW + c] = rv[it];
+                su.a[r * PW + c] = ru[it];
             }
+        }
+    }
+    // ---- batch 2 (in flight during the passes): the output metric
+    T q11[IT_TILE], ijy[IT_TILE], q22[IT_TILE], ijx[IT_TILE];
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        const int64_t o = box_off(P, i, j);
+        const bool ok = q < tw * th;
+        q11[it] = ok && i <= N ? __ldg(m.Q11y + o) : T(0);
+        ijy[it] = ok && i <= N ? __ldg(m.iJy + o) : T(0);
+        q22[it] = ok && j <= N ? __ldg(m.Q22x + o) : T(0);
+        ijx[it] = ok && j <= N ? __ldg(m.iJx + o) : T(0);
+    }
+    __syncthreads();
+    // J Qi12 I_c2i,y(v) at xy nodes: row-major (y stencil, warp-uniform closure)
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, w5, iw5, r, c);
+        const int k = sv.x0 + c, l = j0 + r;
+        if (q < w5 * th) svq.at(k, l) = ic2i_u<T>(l, n, sv.col(k)) * jq1[it];
+    }
+    // I_c2i,x(u) at xy nodes: column-major (x stencil); the J Qi12 factor follows
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int c, r;
+        split(q, h5, ih5, c, r);
+        const int k = i0 + c, l = suq.y0 + r;
+        if (q < tw * h5) suq.at(k, l) = ic2i_u<T>(k, n, su.row(l));
+    }
+    __syncthreads();
+    // I_i2c,x of the first: column-major
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int c, r;
+        split(q, th, ih, c, r);
+        const int i = i0 + c, j = j0 + r;
+        if (q < tw * th && i <= N) sux.at(i, j) = ii2c_u<T>(i, N, svq.row(j));
+    }
+    // J Qi12 factor of the second: row-major, in place
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        if (q < tw * h5) suq.at(i0 + c, suq.y0 + r) *= jq2[it];
+    }
+    __syncthreads();
+    // outputs: row-major, I_i2c,y of the second (warp-uniform closure), coalesced stores
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        const int64_t o = box_off(P, i, j);
+        if (q < tw * th) {
+            if (i <= N) w[d.fs + o] = q11[it] * su.at(i, j) + sux.at(i, j) * ijy[it];
+            if (j <= N) w[2 * d.fs + o] = q22[it] * sv.at(i, j) + ii2c_u<T>(j, N, suq.col(i)) * ijx[it];
         }
     }
 }
@@ -158,194 +237,303 @@ __global__ void __launch_bounds__(STAGE_THREADS) k_co2contra(const T *__restrict
 // fused stage: tendency of the linear operator + RK4 update
 // ---------------------------------------------------------------------------
 template <class T>
-struct StageSmem {
-    Win<T, WX, WY> h;              // origin (i0-2, j0-2)
-    Win<T, WX, WY> ut;             // origin (i0-3, j0-2)
-    Win<T, WX, WY> vt;             // origin (i0-2, j0-3)
-    Win<T, WX, TILE_YM> ju;        // J ut on the tile rows, origin (i0-3, j0)
-    Win<T, TILE_XM, WY> jv;        // J vt on the tile columns, origin (i0, j0-3)
-    Win<T, WX, TILE_YM> up;        // synchronised up, origin (i0-2, j0)
-    Win<T, TILE_XM, WY> vp;        // synchronised vp, origin (i0, j0-2)
-    Win<T, TILE_XM, TILE_YM> dv;   // synchronised divergence, origin (i0, j0)
+struct StageLayout {
+    static constexpr int H = 0, UT = H + PW * RW, VT = UT + PW * RW, JU = VT + PW * RW, JV = JU + PW * TILE_YM,
+                         UP = JV + PT * RW, VP = UP + PW * TILE_YM, DX = VP + PT * RW, KX = DX + PT * TILE_YM,
+                         HL = KX + PT * TILE_YM, HR = HL + TILE_YM, HB = HR + TILE_YM, HT = HB + TILE_XM,
+                         TOTAL = HT + TILE_XM;
+    static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
+
+__device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1 || k == n || l == 1 || l == n; }
 
 //   mode 0: out = A(y)
 //   mode 1: Y1 = V0 + dt/2 k,  ACC = dt/6 k
 //   mode 2: Y1 = V0 + dt/2 k,  ACC += dt/3 k
 //   mode 3: Y1 = V0 + dt   k,  ACC += dt/3 k
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
-template <class T>
-__global__ void __launch_bounds__(STAGE_THREADS) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
+template <class T, int MODE>
+__global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
 {
     using namespace sbp;
-    __shared__ StageSmem<T> sm;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using L = StageLayout<T>;
+    T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
     tile_range(n, i0, i1, j0, j1);
     const int tw = i1 - i0, th = j1 - j0;
     const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
     const int64_t mo = mem * d.ms;
-    const T *y = Yin + mo;                 // member base (h_halo needs the other panels)
+    const T *y = Yin + mo;                 // member base (the h halos read the other panels)
     const T *w = Wc + mo;
     const T *yp = y + t * d.ps, *wp = w + t * d.ps;
-    const int hx0 = i0 - 2, hy0 = j0 - 2, ux0 = i0 - 3, uy0 = j0 - 2, vx0 = i0 - 2, vy0 = j0 - 3;
-
-    // ---- stage h, ut, vt and the J-weighted copies the divergence reads
-    stage(sm.h, yp, P, hx0, hy0);
-    {
-        const T *g = wp + d.fs + box_off(P, ux0, uy0), *gj = m.Jy + box_off(P, ux0, uy0);
-        for (int r = threadIdx.y; r < WY; r += TB_Y)
-            for (int c = threadIdx.x; c < WX; c += TB_X) {
-                const T v = __ldg(g + r * P + c);
-                sm.ut.a[r * WX + c] = v;
-                if (r >= 2 && r < TILE_YM + 2) sm.ju.a[(r - 2) * WX + c] = __ldg(gj + r * P + c) * v;
-            }
-    }
-    {
-        const T *g = wp + 2 * d.fs + box_off(P, vx0, vy0), *gj = m.Jx + box_off(P, vx0, vy0);
-        for (int r = threadIdx.y; r < WY; r += TB_Y)
-            for (int c = threadIdx.x; c < WX; c += TB_X) {
-                const T v = __ldg(g + r * P + c);
-                sm.vt.a[r * WX + c] = v;
-                if (c >= 2 && c < TILE_XM + 2) sm.jv.a[r * TILE_XM + (c - 2)] = __ldg(gj + r * P + c) * v;
-            }
-    }
-    __syncthreads();
-
-    // ---- Coriolis vertex vectors and divergence; panel-boundary vertices from the edge buffer
+    const SWin<T, PW> sh{sm + L::H, i0 - 2, j0 - 2}, sut{sm + L::UT, i0 - 3, j0 - 2}, svt{sm + L::VT, i0 - 2, j0 - 3},
+        sju{sm + L::JU, i0 - 3, j0}, sup{sm + L::UP, i0 - 2, j0};
+    const SWin<T, PT> sjv{sm + L::JV, i0, j0 - 3}, svp{sm + L::VP, i0, j0 - 2}, sdx{sm + L::DX, i0, j0},
+        skx{sm + L::KX, i0, j0};
+    T *hl = sm + L::HL, *hr = sm + L::HR, *hb = sm + L::HB, *ht = sm + L::HT;
+    const int w5 = tw + 5, h5 = th + 5;
+    const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
     const T *fJ2 = m.fJ2 + t * d.ps;
-    for (int r = threadIdx.y; r < th; r += TB_Y) {
-        const int l = j0 + r;
-        const bool inner = (l >= 5 && l <= n - 4);      // warp-uniform
-        const bool brow = (l == 1 || l == n);           // warp-uniform
-        for (int c = threadIdx.x; c < tw + 5; c += TB_X) {
-            const int k = vx0 + c;
-            T val;
-            if (brow || k == 1 || k == n) {
-                val = (k >= 1 && k <= n) ? edge_entry(E, N, mem, t, k, l)[0] : T(0);
-            } else {
-                const Line<T> f = sm.vt.col(vx0, vy0, k);
-                val = __ldg(fJ2 + box_off(P, k, l)) * (inner ? ic2i_in<T>(l, f) : ic2i<T>(l, n, f));
+    const bool sat_l = i0 <= 3, sat_r = i1 - 1 >= N - 2, sat_b = j0 <= 3, sat_t = j1 - 1 >= N - 2;
+
+    // ---- batch 1a: h and ut windows with J ut
+    {
+        const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0);
+        const T *gh = yp + oh, *gu = wp + d.fs + ou, *gjy = m.Jy + ou;
+        T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN];
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            const bool ok = q < w5 * h5;
+            const int go = r * P + c;
+            rh[it] = ok ? __ldg(gh + go) : T(0);
+            ru[it] = ok ? __ldg(gu + go) : T(0);
+            rjy[it] = ok && r >= 2 && r < th + 2 ? __ldg(gjy + go) : T(0);
+        }
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            if (q < w5 * h5) {
+                sh.a[r * PW + c] = rh[it];
+                sut.a[r * PW + c] = ru[it];
+                if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] = rjy[it] * ru[it];
             }
-            sm.up.a[r * WX + c] = val;
         }
     }
-    for (int r = threadIdx.y; r < th + 5; r += TB_Y) {
-        const int l = uy0 + r;
-        const bool lin = (l >= 1 && l <= n), brow = (l == 1 || l == n);
-        const Line<T> f = sm.ut.row(ux0, uy0, l);
-        for (int c = threadIdx.x; c < tw; c += TB_X) {
-            const int k = i0 + c;
-            T val;
-            if (lin && (brow || k == 1 || k == n))
-                val = edge_entry(E, N, mem, t, k, l)[1];
-            else
-                val = -__ldg(fJ2 + box_off(P, k, l)) * ic2i_x<T>(k, n, f);
-            sm.vp.a[r * TILE_XM + c] = val;
+    // ---- batch 1b: vt window with J vt, the h halos across the panel edges, and
+    // fJ2 (or the synchronised edge value) for the up / vp passes
+    T f1[IT_STRIP], f2[IT_STRIP];
+    {
+        const int64_t ov = box_off(P, svt.x0, svt.y0);
+        const T *gv = wp + 2 * d.fs + ov, *gjx = m.Jx + ov;
+        T rv[IT_WIN], rjx[IT_WIN];
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int q = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(q, w5, iw5, r, c);
+            const bool ok = q < w5 * h5;
+            const int go = r * P + c;
+            rv[it] = ok ? __ldg(gv + go) : T(0);
+            rjx[it] = ok && c >= 2 && c < tw + 2 ? __ldg(gjx + go) : T(0);
+        }
+        T hx0 = 0, hx1 = 0, hy0 = 0, hy1 = 0;
+        const int q = threadIdx.x;
+        if (q < th) {
+            if (sat_l) hx0 = h_halo(y, d, t, SIDE_L, j0 + q);
+            if (sat_r) hx1 = h_halo(y, d, t, SIDE_R, j0 + q);
+        }
+        if (q < tw) {
+            if (sat_b) hy0 = h_halo(y, d, t, SIDE_B, i0 + q);
+            if (sat_t) hy1 = h_halo(y, d, t, SIDE_T, i0 + q);
+        }
+#pragma unroll
+        for (int it = 0; it < IT_STRIP; it++) {
+            const int qq = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(qq, w5, iw5, r, c);
+            int k = sup.x0 + c, l = j0 + r;
+            if (qq >= w5 * th) f1[it] = T(0);
+            else if (on_boundary(k, l, n)) f1[it] = (k >= 1 && k <= n) ? edge_entry(E, N, mem, t, k, l)[0] : T(0);
+            else f1[it] = __ldg(fJ2 + box_off(P, k, l));
+            split(qq, tw, iw, r, c);
+            k = i0 + c;
+            l = svp.y0 + r;
+            if (qq >= tw * h5) f2[it] = T(0);
+            else if (l >= 1 && l <= n && on_boundary(k, l, n)) f2[it] = edge_entry(E, N, mem, t, k, l)[1];
+            else f2[it] = __ldg(fJ2 + box_off(P, k, l));
+        }
+#pragma unroll
+        for (int it = 0; it < IT_WIN; it++) {
+            const int qq = threadIdx.x + it * STAGE_THREADS;
+            int r, c;
+            split(qq, w5, iw5, r, c);
+            if (qq < w5 * h5) {
+                svt.a[r * PW + c] = rv[it];
+                if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] = rjx[it] * rv[it];
+            }
+        }
+        if (q < th) { hl[q] = hx0; hr[q] = hx1; }
+        if (q < tw) { hb[q] = hy0; ht[q] = hy1; }
+    }
+
+    // ---- batch 2 (in flight during the passes): the final pass's metric, or the
+    // synchronised divergence on the panel boundary
+    T mja[IT_TILE], mjy[IT_TILE], mjx[IT_TILE];
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        const int64_t o = box_off(P, i, j);
+        const bool ok = q < tw * th, hu = ok && i <= N, hv = ok && j <= N;
+        mja[it] = !ok ? T(0) : on_boundary(i, j, n) ? edge_entry(E, N, mem, t, i, j)[2] : __ldg(m.iJa + o);
+        mjy[it] = hu ? __ldg(m.iJy + o) : T(0);
+        mjx[it] = hv ? __ldg(m.iJx + o) : T(0);
+    }
+    __syncthreads();
+
+    // ---- P1 (row-major): up = fJ2 I_c2i,y(vt) on the tile rows, tile columns +- footprint
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, w5, iw5, r, c);
+        const int k = sup.x0 + c, l = j0 + r;
+        if (q < w5 * th) sup.at(k, l) = on_boundary(k, l, n) ? f1[it] : f1[it] * ic2i_u<T>(l, n, svt.col(k));
+    }
+    // ---- P2 (column-major): I_c2i,x(ut) on the tile columns, tile rows +- footprint
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int c, r;
+        split(q, h5, ih5, c, r);
+        const int k = i0 + c, l = svp.y0 + r;
+        if (q < tw * h5) svp.at(k, l) = ic2i_u<T>(k, n, sut.row(l));
+    }
+    // ---- P3 (column-major): x part of the divergence, c2i difference of J ut
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int c, r;
+        split(q, th, ih, c, r);
+        if (q < tw * th) sdx.at(i0 + c, j0 + r) = dc2i_u<T>(i0 + c, n, sju.row(j0 + r));
+    }
+    __syncthreads();
+    // ---- P4 (column-major): -g grad_x h (with SAT) and I_i2c,x(up); the second goes to the
+    // dead ut window and is scaled by 1/J in the final row-major pass
+    const SWin<T, PT> scx{sm + L::UT, i0, j0};
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int c, r;
+        split(q, th, ih, c, r);
+        const int i = i0 + c, j = j0 + r;
+        if (q < tw * th && i <= N) {
+            const Line<T> hrow = sh.row(j);
+            T gx = di2c_u<T>(i, N, hrow);
+            if (i <= 3) {
+                const T sat = i == 1 ? T(SATI1) : (i == 2 ? T(SATI2) : T(SATI3));
+                gx += sat * (hrow(1) - hl[r]);
+            }
+            if (i >= N - 2) {
+                const T sat = i == N ? T(SATI1) : (i == N - 1 ? T(SATI2) : T(SATI3));
+                gx += sat * (hr[r] - hrow(n));
+            }
+            skx.at(i, j) = -m.grav * (gx * m.inv_hxa);
+            scx.at(i, j) = ii2c_u<T>(i, N, sup.row(j));
         }
     }
-    for (int r = threadIdx.y; r < th; r += TB_Y) {
-        const int l = j0 + r;
-        const bool inner = (l >= 5 && l <= n - 4), brow = (l == 1 || l == n);
-        const Line<T> fx = sm.ju.row(ux0, j0, l);
-        for (int c = threadIdx.x; c < tw; c += TB_X) {
-            const int k = i0 + c;
-            T val;
-            if (brow || k == 1 || k == n) {
-                val = edge_entry(E, N, mem, t, k, l)[2];
-            } else {
-                const Line<T> fy = sm.jv.col(i0, vy0, k);
-                const T dx = dc2i_x<T>(k, n, fx);
-                const T dy = inner ? dc2i_in<T>(l, fy) : dc2i<T>(l, n, fy);
-                val = (dx * m.inv_hx + dy * m.inv_hx) * __ldg(m.iJa + box_off(P, k, l));
-            }
-            sm.dv.a[r * TILE_XM + c] = val;
+    // ---- P4b (row-major): vp = -fJ2 I_c2i,x(ut), synchronised values on the panel boundary
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int k = i0 + c, l = svp.y0 + r;
+        if (q < tw * h5) {
+            T &s = svp.at(k, l);
+            s = (l >= 1 && l <= n && on_boundary(k, l, n)) ? f2[it] : -f2[it] * s;
         }
     }
     __syncthreads();
 
-    // ---- tendencies and the RK4 update
+    // ---- P5 (row-major): divergence and v tendency of the thread's points, then the
+    // RK4 update with all its operand loads in one batch (coalesced)
     const T H = T(a.Hm[mem]);
-    const T dt = T(a.dt);
+    T kh[IT_TILE], ku[IT_TILE], kv[IT_TILE];
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        kh[it] = ku[it] = kv[it] = T(0);
+        if (q >= tw * th) continue;
+        T dvg;
+        if (on_boundary(i, j, n)) {
+            dvg = mja[it];
+        } else {
+            const T dy = dc2i_u<T>(j, n, sjv.col(i));
+            dvg = (sdx.at(i, j) * m.inv_hx + dy * m.inv_hx) * mja[it];
+        }
+        kh[it] = -H * dvg;
+        if (i <= N) ku[it] = skx.at(i, j) + scx.at(i, j) * mjy[it];
+        if (j <= N) {
+            const Line<T> hcol = sh.col(i);
+            T gy = di2c_u<T>(j, N, hcol);
+            if (j <= 3) {
+                const T sat = j == 1 ? T(SATI1) : (j == 2 ? T(SATI2) : T(SATI3));
+                gy += sat * (hcol(1) - hb[c]);
+            }
+            if (j >= N - 2) {
+                const T sat = j == N ? T(SATI1) : (j == N - 1 ? T(SATI2) : T(SATI3));
+                gy += sat * (ht[c] - hcol(n));
+            }
+            gy = gy * m.inv_hxa;
+            kv[it] = -m.grav * gy + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
+        }
+    }
+
     T *v0 = V0 + mo + t * d.ps, *y1 = Y1 + mo + t * d.ps, *acc = ACC + mo + t * d.ps;
     T *cmp = CMP ? CMP + mo + t * d.ps : nullptr;
     const int64_t fs = d.fs;
-    for (int r = threadIdx.y; r < th; r += TB_Y) {
-        const int j = j0 + r;
-        const bool jin = (j >= 4 && j <= N - 3);   // warp-uniform
-        const Line<T> hrow = sm.h.row(hx0, hy0, j), uprow = sm.up.row(vx0, j0, j);
-        for (int c = threadIdx.x; c < tw; c += TB_X) {
-            const int i = i0 + c;
-            const int64_t o = box_off(P, i, j);
-            const T kh = -H * sm.dv.a[r * TILE_XM + c];
-            T ku = 0, kv = 0;
-            if (i <= N) {
-                T gx = di2c_x<T>(i, N, hrow);
-                if (i <= 3) {
-                    const T sat = i == 1 ? T(SATI1) : (i == 2 ? T(SATI2) : T(SATI3));
-                    gx += sat * (hrow(1) - h_halo(y, d, t, SIDE_L, j));
-                }
-                if (i >= N - 2) {
-                    const T sat = i == N ? T(SATI1) : (i == N - 1 ? T(SATI2) : T(SATI3));
-                    gx += sat * (h_halo(y, d, t, SIDE_R, j) - hrow(n));
-                }
-                gx = gx * m.inv_hxa;
-                ku = -m.grav * gx + ii2c_x<T>(i, N, uprow) * __ldg(m.iJy + o);
-            }
-            if (j <= N) {
-                const Line<T> hcol = sm.h.col(hx0, hy0, i), vpcol = sm.vp.col(i0, uy0, i);
-                T gy = jin ? di2c_in<T>(j, hcol) : di2c<T>(j, N, hcol);
-                if (j <= 3) {
-                    const T sat = j == 1 ? T(SATI1) : (j == 2 ? T(SATI2) : T(SATI3));
-                    gy += sat * (hcol(1) - h_halo(y, d, t, SIDE_B, i));
-                }
-                if (j >= N - 2) {
-                    const T sat = j == N ? T(SATI1) : (j == N - 1 ? T(SATI2) : T(SATI3));
-                    gy += sat * (h_halo(y, d, t, SIDE_T, i) - hcol(n));
-                }
-                gy = gy * m.inv_hxa;
-                const T cv = jin ? ii2c_in<T>(j, vpcol) : ii2c<T>(j, N, vpcol);
-                kv = -m.grav * gy + cv * __ldg(m.iJx + o);
-            }
-
-            const int64_t oh = o, ou = o + fs, ov = o + 2 * fs;
-            const bool hu = (i <= N), hv = (j <= N);
-            if (a.mode == 0) {
-                y1[oh] = kh;
-                if (hu) y1[ou] = ku;
-                if (hv) y1[ov] = kv;
-                continue;
-            }
-            if (a.mode <= 3) {
-                const T ca = (a.mode == 3) ? dt : T(0.5) * dt;
-                const T cb = (a.mode == 1) ? dt / T(6) : dt / T(3);
-                y1[oh] = v0[oh] + ca * kh;
-                if (hu) y1[ou] = v0[ou] + ca * ku;
-                if (hv) y1[ov] = v0[ov] + ca * kv;
-                if (a.mode == 1) {
-                    acc[oh] = cb * kh;
-                    if (hu) acc[ou] = cb * ku;
-                    if (hv) acc[ov] = cb * kv;
-                } else {
-                    acc[oh] += cb * kh;
-                    if (hu) acc[ou] += cb * ku;
-                    if (hv) acc[ov] += cb * kv;
-                }
-                continue;
-            }
-            const T cb = dt / T(6);
-            if constexpr (sizeof(T) == 4) {
-                float s0 = v0[oh], c0 = cmp[oh];
-                kahan_add(s0, c0, acc[oh] + cb * kh);
-                v0[oh] = s0; cmp[oh] = c0;
-                if (hu) { float s1 = v0[ou], c1 = cmp[ou]; kahan_add(s1, c1, acc[ou] + cb * ku); v0[ou] = s1; cmp[ou] = c1; }
-                if (hv) { float s2 = v0[ov], c2 = cmp[ov]; kahan_add(s2, c2, acc[ov] + cb * kv); v0[ov] = s2; cmp[ov] = c2; }
+    const T dt = T(a.dt);
+    constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
+    T pv[3][IT_TILE], pa[3][IT_TILE], pc[3][IT_TILE];
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        const int64_t o = box_off(P, i, j);
+        const bool ok = q < tw * th;
+        const bool has[3] = {ok, ok && i <= N, ok && j <= N};
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            pv[f][it] = LV && has[f] ? v0[o + f * fs] : T(0);
+            pa[f][it] = LA && has[f] ? acc[o + f * fs] : T(0);
+            pc[f][it] = LC && has[f] ? cmp[o + f * fs] : T(0);
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < IT_TILE; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, tw, iw, r, c);
+        const int i = i0 + c, j = j0 + r;
+        const int64_t o = box_off(P, i, j);
+        const bool ok = q < tw * th;
+        const bool has[3] = {ok, ok && i <= N, ok && j <= N};
+        const T k3[3] = {kh[it], ku[it], kv[it]};
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            if (!has[f]) continue;
+            const int64_t of = o + f * fs;
+            if constexpr (MODE == 0) {
+                y1[of] = k3[f];
+            } else if constexpr (MODE <= 3) {
+                const T ca = (MODE == 3) ? dt : T(0.5) * dt;
+                const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
+                y1[of] = pv[f][it] + ca * k3[f];
+                acc[of] = (MODE == 1) ? cb * k3[f] : pa[f][it] + cb * k3[f];
+            } else if constexpr (sizeof(T) == 4) {
+                float sv = pv[f][it], cv = pc[f][it];
+                kahan_add(sv, cv, pa[f][it] + (dt / T(6)) * k3[f]);
+                v0[of] = sv;
+                cmp[of] = cv;
             } else {
-                v0[oh] = v0[oh] + (acc[oh] + cb * kh);
-                if (hu) v0[ou] = v0[ou] + (acc[ou] + cb * ku);
-                if (hv) v0[ov] = v0[ov] + (acc[ov] + cb * kv);
+                v0[of] = pv[f][it] + (pa[f][it] + (dt / T(6)) * k3[f]);
             }
         }
     }
