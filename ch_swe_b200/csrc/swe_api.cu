@@ -207,6 +207,7 @@ struct swe_ctx {
     // scratch (stage buffers and contravariant intermediates)
     void *ya = nullptr, *yb = nullptr, *acc = nullptr, *w = nullptr;
     void *edge = nullptr;            // synchronised panel-boundary values of the current stage
+    void *es = nullptr;              // edge strips of the current stage (k_co2contra -> k_edge)
     // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x meshes, [N+1][P]
     double *qw = nullptr;
     double *red = nullptr;           // reduction partials
@@ -268,8 +269,8 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t box = (size_t)c->dims.ps;
-    // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1
-    const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1);
+    // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1 + the edge tables (44 of N+1)
+    const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1) + 44 * (size_t)(N + 1);
     std::vector<T> h(n_el, T(0));
     HostMetric my = host_metric(N, 0.5, 0.0), mx = host_metric(N, 0.0, 0.5), mxy = host_metric(N, 0.0, 0.0);
     const double a = c->cfg.radius;
@@ -318,11 +319,16 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
     v.Q11y = d; v.iJy = d + box; v.Jy = d + 2 * box; v.Q22x = d + 3 * box; v.iJx = d + 4 * box; v.Jx = d + 5 * box;
     v.JQ12 = d + 6 * box; v.iJa = d + 7 * box; v.fJ2 = d + 8 * box;
     v.qb = d + 14 * box; v.qt = v.qb + (N + 1); v.ql = v.qt + (N + 1); v.qr = v.ql + (N + 1);
+    T *ej = d + 14 * box + 4 * (N + 1), *ef = ej + 16 * (N + 1), *ea = ef + 24 * (N + 1);
+    v.ej = ej; v.ef = ef; v.ea = ea;
     const double pi = 3.141592653589793238462643383279502884;
     const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
     v.inv_hxa = T(1.0 / (hx * a));
     v.inv_hx = T(1.0 / hx);
     v.grav = T(c->cfg.grav);
+    k_edge_tables<T><<<(N + 1 + 127) / 128, 128, 0, c->stream>>>(v, c->dims, ej, ef, ea);
+    CU(c, cudaGetLastError());
+    CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
 }
 
@@ -382,7 +388,7 @@ static void free_ctx(swe_ctx *c)
 {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm);
-    cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge);
+    cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
     cudaFree(c->qw); cudaFree(c->red);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -441,6 +447,9 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
         const size_t eb = (size_t)cfg->n_members * NPAN * 4 * (N + 1) * 3 * c->elem;
         if (cudaMalloc(&c->edge, eb) != cudaSuccess) return bail(SWE_ENOMEM);
         if (cudaMemset(c->edge, 0, eb) != cudaSuccess) return bail(SWE_ECUDA);
+        const size_t sb = (size_t)strip_member(N, cfg->n_members) * c->elem;
+        if (cudaMalloc(&c->es, sb) != cudaSuccess) return bail(SWE_ENOMEM);
+        if (cudaMemset(c->es, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
     }
     if (cudaHostAlloc((void **)&c->pinned, c->box_elems * c->elem, cudaHostAllocDefault) != cudaSuccess)
         return bail(SWE_ENOMEM);
@@ -675,9 +684,9 @@ static cudaError_t stage_smem_optin()
 }
 
 template <class T>
-static void launch_co2contra(dim3 g, const T *y, T *w, const Dims &d, const MetricView<T> &m, cudaStream_t st)
+static void launch_co2contra(dim3 g, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m, cudaStream_t st)
 {
-    k_co2contra<T><<<g, stage_block(), Co2Layout<T>::bytes(), st>>>(y, w, d, m);
+    k_co2contra<T><<<g, stage_block(), Co2Layout<T>::bytes(), st>>>(y, w, es, d, m);
 }
 
 template <class T>
@@ -703,8 +712,8 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     dim3 g = stage_grid(c);
-    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, c->dims, mv, c->stream);
-    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
+    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->es, (T *)c->edge, c->dims, mv);
     StageArgs a{mode, dt, c->Hm};
     launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
                     c->dims, mv, a, c->stream);
@@ -731,9 +740,10 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     dim3 g = stage_grid(c);
     if (c->elem == 8)
-        launch_co2contra<double>(g, (const double *)vin->d, (double *)vout->d, c->dims, c->m64.v, c->stream);
+        launch_co2contra<double>(g, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims, c->m64.v,
+                                 c->stream);
     else
-        launch_co2contra<float>(g, (const float *)vin->d, (float *)vout->d, c->dims, c->m32.v, c->stream);
+        launch_co2contra<float>(g, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims, c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
     return SWE_OK;
@@ -855,10 +865,10 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     dim3 gs = stage_grid(c, 1);
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(gs, (const double *)vec->d + mo, (double *)c->w, d1, c->m64.v, c->stream);
+        launch_co2contra<double>(gs, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v, c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(gs, (const float *)vec->d + mo, (float *)c->w, d1, c->m32.v, c->stream);
+        launch_co2contra<float>(gs, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v, c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
@@ -896,9 +906,9 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
 {
     dim3 g = stage_grid(c);
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, c->dims, mv, c->stream);
+    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->w, (T *)c->edge, c->dims, mv);
+    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->es, (T *)c->edge, c->dims, mv);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm};
     launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc, (T *)cmp,
@@ -957,10 +967,11 @@ constexpr int NA_MAXN = SWE_NOALLOC_MAX_N;
 constexpr int NA_ROWS = NA_MAXN + 1 + 2 * MG;
 constexpr int NA_P = (NA_ROWS + 7) / 8 * 8;
 constexpr size_t NA_BOX = (size_t)NA_ROWS * NA_P;
-constexpr size_t NA_METRIC = 14 * NA_BOX + 4 * (size_t)(NA_MAXN + 1);
+constexpr size_t NA_METRIC = 14 * NA_BOX + 48 * (size_t)(NA_MAXN + 1);
 constexpr size_t NA_W = 3 * (size_t)NPAN * NA_BOX;
 constexpr size_t NA_EDGE = (size_t)NPAN * 4 * (NA_MAXN + 1) * 3;
-constexpr size_t NA_TOTAL = NA_METRIC + NA_W + NA_EDGE + 8;
+constexpr size_t NA_STRIPS = (size_t)NPAN * 4 * STRIP_LINES * (NA_MAXN + 1);
+constexpr size_t NA_TOTAL = NA_METRIC + NA_W + NA_EDGE + NA_STRIPS + 8;
 
 struct Frames {
     int ex[NPAN][3], ey[NPAN][3], nn[NPAN][3];
@@ -975,8 +986,9 @@ struct NoallocDevice {
 NoallocDevice g_noalloc[64];
 }  // namespace
 
-// Metric, Coriolis weights and vector-sync weights: [0, NA_METRIC); contravariant
-// scratch W: [NA_METRIC, +NA_W); edge buffer: next NA_EDGE; the mean depth H: last slot.
+// Metric, Coriolis weights, vector-sync weights and edge tables: [0, NA_METRIC);
+// contravariant scratch W: [NA_METRIC, +NA_W); edge buffer: next NA_EDGE; edge
+// strips: next NA_STRIPS; the mean depth H: last slot.
 static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
 
 // FP64 metric of an N-cube into the scratch layout used by build_metric (same
@@ -1119,8 +1131,19 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     dm.ps = (int64_t)(N + 1 + 2 * MG) * dm.P;
     dm.fs = NPAN * dm.ps;
     dm.ms = 3 * dm.fs;
-    double *M = nd.base, *W = nd.base + NA_METRIC, *E = W + NA_W, *Hp = E + NA_EDGE;
+    double *M = nd.base, *W = nd.base + NA_METRIC, *E = W + NA_W, *ES = E + NA_EDGE, *Hp = ES + NA_STRIPS;
     const int64_t box = dm.ps;
+    MetricView<double> mv;
+    mv.Q11y = M; mv.iJy = M + box; mv.Jy = M + 2 * box; mv.Q22x = M + 3 * box; mv.iJx = M + 4 * box;
+    mv.Jx = M + 5 * box; mv.JQ12 = M + 6 * box; mv.iJa = M + 7 * box; mv.fJ2 = M + 8 * box;
+    mv.qb = M + 14 * box; mv.qt = mv.qb + n; mv.ql = mv.qt + n; mv.qr = mv.ql + n;
+    double *ej = M + 14 * box + 4 * n, *ef = ej + 16 * n, *ea = ef + 24 * n;
+    mv.ej = ej; mv.ef = ef; mv.ea = ea;
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
+    mv.inv_hxa = 1.0 / (hx * cfg->radius);
+    mv.inv_hx = 1.0 / hx;
+    mv.grav = cfg->grav;
     if (!nd.metric_ok || !same_geometry(nd.cached, *cfg)) {
         if (cudaMemsetAsync(M, 0, NA_METRIC * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
         Frames fr;
@@ -1129,25 +1152,17 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         dim3 g((n + 15) / 16, (n + 15) / 16), b(16, 16);
         k_noalloc_metric<<<g, b, 0, st>>>(M, N, dm.P, box, cfg->radius, cfg->omega, cfg->rotation_axis[0],
                                           cfg->rotation_axis[1], cfg->rotation_axis[2], cfg->coriolis_constant, fr);
+        k_edge_tables<double><<<(n + 127) / 128, 128, 0, st>>>(mv, dm, ej, ef, ea);
         if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
         nd.cached = *cfg;
         nd.metric_ok = true;
     }
-    MetricView<double> mv;
-    mv.Q11y = M; mv.iJy = M + box; mv.Jy = M + 2 * box; mv.Q22x = M + 3 * box; mv.iJx = M + 4 * box;
-    mv.Jx = M + 5 * box; mv.JQ12 = M + 6 * box; mv.iJa = M + 7 * box; mv.fJ2 = M + 8 * box;
-    mv.qb = M + 14 * box; mv.qt = mv.qb + n; mv.ql = mv.qt + n; mv.qr = mv.ql + n;
-    const double pi = 3.141592653589793238462643383279502884;
-    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
-    mv.inv_hxa = 1.0 / (hx * cfg->radius);
-    mv.inv_hx = 1.0 / hx;
-    mv.grav = cfg->grav;
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
     dim3 g = stage_grid(N, 1);
-    launch_co2contra<double>(g, vin, W, dm, mv, st);
-    k_edge<double><<<edge_grid(N, 1), EDGE_THREADS, 0, st>>>(W, E, dm, mv);
+    launch_co2contra<double>(g, vin, W, ES, dm, mv, st);
+    k_edge<double><<<edge_grid(N, 1), EDGE_THREADS, 0, st>>>(ES, E, dm, mv);
     StageArgs a{0, 0.0, Hp};
     launch_stage<double>(g, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;

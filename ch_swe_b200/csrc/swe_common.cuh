@@ -49,6 +49,7 @@ struct MetricView {
     const T *iJa;                 // xy mesh: 1 / (J * a)
     const T *fJ2;                 // xy mesh, per panel: f * J * J
     const T *qb, *qt, *ql, *qr;   // covariant vector-sync weights along the four sides
+    const T *ej, *ef, *ea;        // edge tables of k_edge_tables: J on the edge strips, fJ2 and 1/(J a) on the edges
     T inv_hxa;                    // 1 / (hx * a)
     T inv_hx;                     // 1 / hx   (hx == hy)
     T grav;

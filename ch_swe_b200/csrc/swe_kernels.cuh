@@ -53,27 +53,6 @@ __device__ __forceinline__ void side_vertex(int N, int s, int a, int depth, int 
     }
 }
 
-// J * (normal contravariant component) of the neighbour across side s, at centre
-// depth c = 1..3 and along-edge index a: the halo the Ch vector exchange
-// (exchange_halo_Ch_mod.f90) delivers for the divergence SAT.
-template <class T>
-__device__ __forceinline__ T ju_halo(const T *W, const Dims &d, const MetricView<T> &m, int t, int s, int a, int c)
-{
-    const Link L = c_link[t][s];
-    const int N = d.N;
-    const int ap = L.rev ? N + 2 - a : a;
-    const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
-    const GV<T> U = gview(W, d, 1, L.nb), V = gview(W, d, 2, L.nb);
-    T val;
-    switch (L.nside) {
-    case SIDE_L: val = Jy(c, ap) * U(c, ap); break;
-    case SIDE_R: val = Jy(N + 1 - c, ap) * U(N + 1 - c, ap); break;
-    case SIDE_B: val = Jx(ap, c) * V(ap, c); break;
-    default: val = Jx(ap, N + 1 - c) * V(ap, N + 1 - c); break;
-    }
-    return T(L.sn) * val;
-}
-
 // h at the neighbour's copy of the shared vertex (xy halo index 0 / N+2).
 template <class T>
 __device__ __forceinline__ T h_halo(const T *Y, const Dims &d, int t, int s, int a)
@@ -92,55 +71,84 @@ __device__ __forceinline__ int64_t edge_index(int N, int mem, int t, int s, int 
     return ((((int64_t)mem * NPAN + t) * 4 + s) * (N + 1) + (a - 1)) * 3;
 }
 
-// One raw quantity at boundary vertex (k, l) of panel t, before any edge sync:
+// Edge strips: for every member, panel and side, the contravariant components the
+// edge sync reads, contiguous along the side (written by k_co2contra):
+//   line 0..2: the normal component at depth 1..3 (centres), at along-edge node b = 1..N+1
+//   line 3   : the tangential component on the edge line, at along-edge centre c = 1..N
+// Normal/tangential: ut/vt on the L and R sides, vt/ut on B and T.  Depth counts
+// from the side (L: i = d, R: i = N+1-d, B: j = d, T: j = N+1-d).
+constexpr int STRIP_LINES = 4;
+
+__host__ __device__ __forceinline__ int64_t strip_member(int N, int mem) { return (int64_t)mem * NPAN * 4 * STRIP_LINES * (N + 1); }
+
+template <class T>
+struct Strips {
+    const T *es;   // member base
+    int n;         // N + 1
+    // 1-based line of panel p, side s
+    __device__ __forceinline__ const T *line(int p, int s, int k) const { return es + ((p * 4 + s) * STRIP_LINES + k) * n - 1; }
+};
+
+// Position of xy vertex (k, l) along side s (1..N+1).
+__device__ __forceinline__ int along(int s, int k, int l) { return s <= SIDE_R ? l : k; }
+
+// The neighbour's along-edge index of along index b on side s of panel p.
+__device__ __forceinline__ int nb_along(const Link &L, int n, int b) { return L.rev ? n + 1 - b : b; }
+
+// J * normal contravariant component of the neighbour across side s of panel p,
+// at depth dd and along index b of this side, with the orientation sign: the halo
+// the Ch vector exchange (exchange_halo_Ch_mod.f90) delivers for the divergence SAT.
+template <class T>
+__device__ __forceinline__ T sat_halo(const Strips<T> &S, const MetricView<T> &m, int p, int s, int b, int dd)
+{
+    const Link L = c_link[p][s];
+    const int n = S.n, bp = nb_along(L, n, b);
+    return T(L.sn) * (m.ej[(L.nside * 4 + dd - 1) * n + bp - 1] * S.line(L.nb, L.nside, dd - 1)[bp]);
+}
+
+// One raw quantity at along index b of side s of panel p, before any edge sync:
 //   q = 0: up = fJ2 I_c2i,y(vt)      q = 1: vp = -fJ2 I_c2i,x(ut)
 //          (coriolis_Ch_mod.f90:97-120)
 //   q = 2: c2i x-difference of J ut  q = 3: c2i y-difference of J vt
 //          with the SAT terms of sbp_diff_c2i_42_mod.f90:195-251 on the panel edge
 //          (div_sbp_sat_mod.f90:54-80 before the 1/(hx J) scaling).
+// Across the side the stencils are the first closure rows; along it the full
+// SBP stencils, with the second SAT at the cube corners.
 template <class T>
-__device__ __forceinline__ T edge_raw(const T *W, const Dims &d, const MetricView<T> &m, int t, int k, int l, int q)
+__device__ __forceinline__ T edge_raw(const Strips<T> &S, const MetricView<T> &m, int p, int s, int b, int q)
 {
     using namespace sbp;
-    const int N = d.N, n = N + 1;
-    const GV<T> U = gview(W, d, 1, t), V = gview(W, d, 2, t);
-    if (q == 0) return mview(m.fJ2 + t * d.ps, d)(k, l) * ic2i<T>(l, n, [&](int c) { return V(k, c); });
-    if (q == 1) return -mview(m.fJ2 + t * d.ps, d)(k, l) * ic2i<T>(k, n, [&](int c) { return U(c, l); });
-    const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d);
-    if (q == 2) {
-        auto ju = [&](int c) { return Jy(c, l) * U(c, l); };
-        T dx = dc2i<T>(k, n, ju);
-        if (k == 1)
-            dx += T(SATC) * (T(R11) * (ju(1) - ju_halo(W, d, m, t, SIDE_L, l, 1)) +
-                             T(R12) * (ju(2) - ju_halo(W, d, m, t, SIDE_L, l, 2)) +
-                             T(R13) * (ju(3) - ju_halo(W, d, m, t, SIDE_L, l, 3)));
-        else if (k == n)
-            dx -= T(SATC) * (T(R11) * (ju(N) - ju_halo(W, d, m, t, SIDE_R, l, 1)) +
-                             T(R12) * (ju(N - 1) - ju_halo(W, d, m, t, SIDE_R, l, 2)) +
-                             T(R13) * (ju(N - 2) - ju_halo(W, d, m, t, SIDE_R, l, 3)));
-        return dx;
+    const int n = S.n, N = n - 1;
+    const bool lr = s <= SIDE_R, lo = (s == SIDE_L || s == SIDE_B);
+    const T *n1 = S.line(p, s, 0), *n2 = S.line(p, s, 1), *n3 = S.line(p, s, 2), *tg = S.line(p, s, 3);
+    const T *jn = m.ej + s * 4 * n - 1, *jt = m.ej + (s * 4 + 3) * n - 1;
+    const bool across = lr ? (q == 1 || q == 2) : (q == 0 || q == 3);
+    if (q <= 1) {
+        const T f = m.ef[(p * 4 + s) * n + b - 1];
+        const T v = across ? T(IC11) * n1[b] + T(IC12) * n2[b] + T(IC13) * n3[b]
+                           : ic2i<T>(b, n, [&](int c) { return tg[c]; });
+        return q == 0 ? f * v : -f * v;
     }
-    auto jv = [&](int c) { return Jx(k, c) * V(k, c); };
-    T dy = dc2i<T>(l, n, jv);
-    if (l == 1)
-        dy += T(SATC) * (T(R11) * (jv(1) - ju_halo(W, d, m, t, SIDE_B, k, 1)) +
-                         T(R12) * (jv(2) - ju_halo(W, d, m, t, SIDE_B, k, 2)) +
-                         T(R13) * (jv(3) - ju_halo(W, d, m, t, SIDE_B, k, 3)));
-    else if (l == n)
-        dy -= T(SATC) * (T(R11) * (jv(N) - ju_halo(W, d, m, t, SIDE_T, k, 1)) +
-                         T(R12) * (jv(N - 1) - ju_halo(W, d, m, t, SIDE_T, k, 2)) +
-                         T(R13) * (jv(N - 2) - ju_halo(W, d, m, t, SIDE_T, k, 3)));
-    return dy;
-}
-
-// The neighbour's copy (panel nb, vertex (kk, ll)) of boundary vertex (k, l) of
-// panel t across side s.
-__device__ __forceinline__ void nb_vertex(int N, int t, int s, int k, int l, int &nb, int &kk, int &ll)
-{
-    const Link L = c_link[t][s];
-    const int a = s <= SIDE_R ? l : k;
-    nb = L.nb;
-    side_vertex(N, L.nside, L.rev ? N + 2 - a : a, 0, kk, ll);
+    if (across) {
+        const T j1 = jn[b] * n1[b], j2 = jn[n + b] * n2[b], j3 = jn[2 * n + b] * n3[b];
+        const T dd = lo ? T(DC11) * j1 + T(DC12) * j2 + T(DC13) * j3 : -T(DC11) * j1 - T(DC12) * j2 - T(DC13) * j3;
+        const T sat = T(SATC) * (T(R11) * (j1 - sat_halo(S, m, p, s, b, 1)) + T(R12) * (j2 - sat_halo(S, m, p, s, b, 2)) +
+                                 T(R13) * (j3 - sat_halo(S, m, p, s, b, 3)));
+        return lo ? dd + sat : dd - sat;
+    }
+    auto jtv = [&](int c) { return jt[c] * tg[c]; };
+    T dd = dc2i<T>(b, n, jtv);
+    if (b == 1 || b == n) {
+        // cube corner: the SAT across the other side through this vertex
+        const int s2 = lr ? (b == 1 ? SIDE_B : SIDE_T) : (b == 1 ? SIDE_L : SIDE_R);
+        const int b2 = lo ? 1 : n;
+        const int c1 = b == 1 ? 1 : N, c2 = b == 1 ? 2 : N - 1, c3 = b == 1 ? 3 : N - 2;
+        const T sat = T(SATC) * (T(R11) * (jtv(c1) - sat_halo(S, m, p, s2, b2, 1)) +
+                                 T(R12) * (jtv(c2) - sat_halo(S, m, p, s2, b2, 2)) +
+                                 T(R13) * (jtv(c3) - sat_halo(S, m, p, s2, b2, 3)));
+        dd = b == 1 ? dd + sat : dd - sat;
+    }
+    return dd;
 }
 
 // The neighbour's raw vertex vector (upn, vpn) in this panel's frame, as the
@@ -155,6 +163,46 @@ __device__ __forceinline__ void halo_vec(int t, int s, T upn, T vpn, T &uh, T &v
     else { vh = T(L.sn) * nrm; uh = T(L.st) * tan; }
 }
 
+// Metric on the panel edges, contiguous along each side, for the edge sync:
+//   ej[(s*4 + k)*(N+1) + b-1]: J at the normal component's depth k+1 (k < 3, node b)
+//                              and at the tangential component on the edge line (k = 3, centre b)
+//   ef[(p*4 + s)*(N+1) + b-1]: fJ2 of panel p at boundary vertex b of side s
+//   ea[s*(N+1) + b-1]        : 1/(J a) at boundary vertex b of side s
+template <class T>
+__global__ void k_edge_tables(MetricView<T> m, Dims d, T *ej, T *ef, T *ea)
+{
+    const int N = d.N, n = N + 1;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (b > n) return;
+    const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d), iJa = mview(m.iJa, d);
+    for (int s = 0; s < 4; s++) {
+        for (int k = 1; k <= 3; k++) {
+            T v;
+            switch (s) {
+            case SIDE_L: v = Jy(k, b); break;
+            case SIDE_R: v = Jy(n - k, b); break;
+            case SIDE_B: v = Jx(b, k); break;
+            default: v = Jx(b, n - k); break;
+            }
+            ej[(s * 4 + k - 1) * n + b - 1] = v;
+        }
+        T v = 0;
+        if (b <= N) {
+            switch (s) {
+            case SIDE_L: v = Jx(1, b); break;
+            case SIDE_R: v = Jx(n, b); break;
+            case SIDE_B: v = Jy(b, 1); break;
+            default: v = Jy(b, n); break;
+            }
+        }
+        ej[(s * 4 + 3) * n + b - 1] = v;
+        int k, l;
+        side_vertex(N, s, b, 0, k, l);
+        ea[s * n + b - 1] = iJa(k, l);
+        for (int p = 0; p < NPAN; p++) ef[(p * 4 + s) * n + b - 1] = mview(m.fJ2 + p * d.ps, d)(k, l);
+    }
+}
+
 constexpr int EDGE_CHUNK = 32;    // along-edge vertices per block (balanced split, at most 32)
 constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the third panel at corners
 
@@ -162,46 +210,43 @@ constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the th
 // vector sync, ecs_Ah_vec_sync_mod.f90:62-125 with (U, V) = (vp, up)) and
 // divergence (Ah scalar sync, halo_Ah_scalar_sync_mod.f90:43-98): the work the
 // reference does with its 'cross' and 'full' exchanges before the edge loops.
-// Block = (chunk of vertices along one side of one panel of one member).
+// Block = (chunk of vertices along one side of one panel of one member); every
+// read is from the edge strips and edge tables, contiguous along the side.
 // Phase 1: every raw quantity the chunk needs is one thread's stencil: warp w < 8
 // takes quantity w % 4 for copy w / 4 (own vertex / neighbour across this side),
 // warp 8 the copy of the third panel at the two cube corners.  Phase 2 combines
 // the copies from shared memory.  Copies are stored by direction (x-neighbour
-// across L/R, y-neighbour across B/T), so the two sides that meet at a corner
-// compute bit-identical corner values.
+// across L/R, y-neighbour across B/T).
 template <class T>
-__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ Wc, T *__restrict__ E, Dims d,
+__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, T *__restrict__ E, Dims d,
                                                         MetricView<T> m)
 {
     __shared__ T raw[3][4][EDGE_CHUNK];   // [own, x-neighbour, y-neighbour][quantity][vertex]
     const int N = d.N, n = N + 1;
     const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
     const int a0 = 1 + (blockIdx.x * n) / gridDim.x, a1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
-    const T *w = Wc + mem * d.ms;
+    const Strips<T> S{ES + strip_member(N, mem), n};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
     if (warp < 8) {
         const int a = a0 + lane, q = warp & 3;
         if (a < a1) {
-            int k, l;
-            side_vertex(N, s, a, 0, k, l);
             if (warp < 4) {
-                raw[0][q][lane] = edge_raw(w, d, m, t, k, l, q);
+                raw[0][q][lane] = edge_raw(S, m, t, s, a, q);
             } else {
-                int nb, kk, ll;
-                nb_vertex(N, t, s, k, l, nb, kk, ll);
-                raw[xs ? 1 : 2][q][lane] = edge_raw(w, d, m, nb, kk, ll, q);
+                const Link L = c_link[t][s];
+                raw[xs ? 1 : 2][q][lane] = edge_raw(S, m, L.nb, L.nside, nb_along(L, n, a), q);
             }
         }
     } else if (lane < 8) {
         // the other neighbour of the corner vertices a = 1 and a = N+1
         const int a = lane < 4 ? 1 : n, q = lane & 3;
         if (a >= a0 && a < a1) {
-            int k, l, nb, kk, ll;
+            int k, l;
             side_vertex(N, s, a, 0, k, l);
             const int s2 = xs ? (l == 1 ? SIDE_B : SIDE_T) : (k == 1 ? SIDE_L : SIDE_R);
-            nb_vertex(N, t, s2, k, l, nb, kk, ll);
-            raw[xs ? 2 : 1][q][a - a0] = edge_raw(w, d, m, nb, kk, ll, q);
+            const Link L2 = c_link[t][s2];
+            raw[xs ? 2 : 1][q][a - a0] = edge_raw(S, m, L2.nb, L2.nside, nb_along(L2, n, along(s2, k, l)), q);
         }
     }
     __syncthreads();
@@ -211,23 +256,20 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ Wc,
     side_vertex(N, s, a, 0, k, l);
     const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
     const bool cx = il || ir, cy = ib || it;
-    const GV<T> iJa = mview(m.iJa, d);
     const T V = raw[0][0][v], U = raw[0][1][v];
-    const T f = (raw[0][2][v] * m.inv_hx + raw[0][3][v] * m.inv_hx) * iJa(k, l);
+    const T f = (raw[0][2][v] * m.inv_hx + raw[0][3][v] * m.inv_hx) * m.ea[s * n + a - 1];
     T uhx = 0, vhx = 0, fx = 0, uhy = 0, vhy = 0, fy = 0;
     if (cx) {
         const int sx = il ? SIDE_L : SIDE_R;
-        int nb, kk, ll;
-        nb_vertex(N, t, sx, k, l, nb, kk, ll);
+        const Link L = c_link[t][sx];
         halo_vec(t, sx, raw[1][0][v], raw[1][1][v], uhx, vhx);
-        fx = (raw[1][2][v] * m.inv_hx + raw[1][3][v] * m.inv_hx) * iJa(kk, ll);
+        fx = (raw[1][2][v] * m.inv_hx + raw[1][3][v] * m.inv_hx) * m.ea[L.nside * n + nb_along(L, n, l) - 1];
     }
     if (cy) {
         const int sy = ib ? SIDE_B : SIDE_T;
-        int nb, kk, ll;
-        nb_vertex(N, t, sy, k, l, nb, kk, ll);
+        const Link L = c_link[t][sy];
         halo_vec(t, sy, raw[2][0][v], raw[2][1][v], uhy, vhy);
-        fy = (raw[2][2][v] * m.inv_hx + raw[2][3][v] * m.inv_hx) * iJa(kk, ll);
+        fy = (raw[2][2][v] * m.inv_hx + raw[2][3][v] * m.inv_hx) * m.ea[L.nside * n + nb_along(L, n, k) - 1];
     }
     T sup, svp, sdiv;
     if (cx && cy) {

@@ -114,8 +114,8 @@ struct Co2Layout {
 };
 
 template <class T>
-__global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W, Dims d,
-                                                              MetricView<T> m)
+__global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
+                                                                 T *__restrict__ ES, Dims d, MetricView<T> m)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = Co2Layout<T>;
@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
     const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
     const T *y = Y + mem * d.ms + t * d.ps;
     T *w = W + mem * d.ms + t * d.ps;
+    T *es = ES + strip_member(N, mem) + (int64_t)t * 4 * STRIP_LINES * n - 1;   // + (s*4 + line)*n + index
     const SWin<T, PW> sv{sm + L::V, i0 - 2, j0 - 3}, su{sm + L::U, i0 - 3, j0 - 2}, svq{sm + L::VQ, i0 - 2, j0};
     const SWin<T, PT> suq{sm + L::UQ, i0, j0 - 2}, sux{sm + L::UX, i0, j0};
 
@@ -227,8 +228,23 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
         const int i = i0 + c, j = j0 + r;
         const int64_t o = box_off(P, i, j);
         if (q < tw * th) {
-            if (i <= N) w[d.fs + o] = q11[it] * su.at(i, j) + sux.at(i, j) * ijy[it];
-            if (j <= N) w[2 * d.fs + o] = q22[it] * sv.at(i, j) + ii2c_u<T>(j, N, suq.col(i)) * ijx[it];
+            // the edge strips (k_edge reads them contiguous along each side)
+            if (i <= N) {
+                const T ut = q11[it] * su.at(i, j) + sux.at(i, j) * ijy[it];
+                w[d.fs + o] = ut;
+                if (i <= 3) es[(SIDE_L * 4 + i - 1) * n + j] = ut;
+                if (i >= N - 2) es[(SIDE_R * 4 + N - i) * n + j] = ut;
+                if (j == 1) es[(SIDE_B * 4 + 3) * n + i] = ut;
+                if (j == n) es[(SIDE_T * 4 + 3) * n + i] = ut;
+            }
+            if (j <= N) {
+                const T vt = q22[it] * sv.at(i, j) + ii2c_u<T>(j, N, suq.col(i)) * ijx[it];
+                w[2 * d.fs + o] = vt;
+                if (j <= 3) es[(SIDE_B * 4 + j - 1) * n + i] = vt;
+                if (j >= N - 2) es[(SIDE_T * 4 + N - j) * n + i] = vt;
+                if (i == 1) es[(SIDE_L * 4 + 3) * n + j] = vt;
+                if (i == n) es[(SIDE_R * 4 + 3) * n + j] = vt;
+            }
         }
     }
 }
