@@ -28,6 +28,7 @@ EXPORTED = [
     "swe_stvec_assign", "swe_stvec_update", "swe_stvec_device_view", "swe_operator_apply",
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
     "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
+    "swe_set_tile", "swe_get_tile", "swe_autotune",
 ]
 
 
@@ -91,6 +92,9 @@ def load(path: str = LIB_PATH):
     L.swe_launch_count.restype = ctypes.c_longlong
     L.swe_edge_links.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.swe_kernel_times.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+    L.swe_set_tile.argtypes = [_vp, ctypes.c_int]
+    L.swe_get_tile.argtypes = [_vp, ctypes.POINTER(ctypes.c_int)]
+    L.swe_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
     for name in EXPORTED:
         if not hasattr(L, name):
             raise SweError(f"libchswe.so does not export {name}")

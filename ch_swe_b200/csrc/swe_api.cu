@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -217,6 +218,7 @@ struct swe_ctx {
     const void *graph_v0 = nullptr;
     double graph_dt = 0.0;
     int graph_kernels = 0;
+    int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
 };
 
 struct swe_stvec {
@@ -246,12 +248,12 @@ static int fail(swe_ctx *c, int code, const char *fmt, ...)
 
 static bool g_tables_ready[64] = {false};
 
-// Balanced tiles of at most TILE_XM x TILE_YM points cover the N+1 box.
-static bool tiles_fit(int N)
-{
-    const int n = N + 1, nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
-    return (n + nbx - 1) / nbx <= TILE_XM && (n + nby - 1) / nby <= TILE_YM;
-}
+// Maximal tile sizes the stage kernels are built for; ceil(N / (TM - 1)) balanced
+// tiles per direction always fit, whatever N.
+static const int k_tiles[] = {17, 25, 33};
+static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
+// Default before autotuning: tiles of about 24 points for the smaller cubes.
+static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
 static int upload_tables(swe_ctx *c)
 {
@@ -409,7 +411,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
 {
     if (!cfg || !out) return SWE_EINVAL;
     *out = nullptr;
-    if (cfg->N < 8 || !tiles_fit(cfg->N) || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
+    if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
         cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
         return SWE_EINVAL;
     int ndev = 0;
@@ -424,6 +426,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     c->dims.fs = NPAN * c->dims.ps;
     c->dims.ms = 3 * c->dims.fs;
     c->elem = cfg->precision == SWE_FP64 ? 8 : 4;
+    c->tile = default_tile(N);
     c->box_elems = (size_t)c->dims.ms * cfg->n_members;
     int rc = SWE_OK;
     auto bail = [&](int code) { free_ctx(c); delete c; return code; };
@@ -651,19 +654,58 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // operator application and RK4
 // ---------------------------------------------------------------------------
 static dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
-// Balanced tiles: ceil(N / nominal) tiles per direction, widths at most TILE_XM x TILE_YM.
-static dim3 stage_grid(int N, int members)
+
+// The stage kernels are launched with programmatic stream serialization: each may
+// start (and load its metric) while its predecessor finishes, and waits for the
+// predecessor's results with griddepcontrol.wait.  CHSWE_PDL=0 in the environment
+// launches them plainly.
+static bool pdl_enabled()
 {
-    const int nbx = (N + TILE_XN - 1) / TILE_XN, nby = (N + TILE_YN - 1) / TILE_YN;
-    return dim3(nbx, nby, NPAN * members);
+    static const bool on = [] {
+        const char *e = std::getenv("CHSWE_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
-static dim3 stage_grid(const swe_ctx *c, int members = -1)
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kern)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t st, Args... args)
 {
-    return stage_grid(c->cfg.N, members < 0 ? c->cfg.n_members : members);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
+}
+// Balanced tiles: ceil(N / (TM - 1)) tiles per direction, widths at most TM.
+static dim3 stage_grid(int N, int members, int tm)
+{
+    const int nb = (N + tm - 2) / (tm - 1);
+    return dim3(nb, nb, NPAN * members);
 }
 
 // The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
 // device and element type (the attribute belongs to the device's context).
+template <class T, int TM>
+static cudaError_t stage_smem_optin_tm()
+{
+    cudaError_t e =
+        cudaFuncSetAttribute(k_co2contra<T, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T, TM>::bytes());
+    const int sb = (int)StageLayout<T, TM>::bytes();
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    return e;
+}
+
 template <class T>
 static cudaError_t stage_smem_optin()
 {
@@ -672,34 +714,55 @@ static cudaError_t stage_smem_optin()
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(k_co2contra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T>::bytes());
-    const int sb = (int)StageLayout<T>::bytes();
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    e = stage_smem_optin_tm<T, 17>();
+    if (e == cudaSuccess) e = stage_smem_optin_tm<T, 25>();
+    if (e == cudaSuccess) e = stage_smem_optin_tm<T, 33>();
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
-template <class T>
-static void launch_co2contra(dim3 g, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m, cudaStream_t st)
+template <class T, int TM>
+static void launch_co2contra_tm(int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
+                                cudaStream_t st)
 {
-    k_co2contra<T><<<g, stage_block(), Co2Layout<T>::bytes(), st>>>(y, w, es, d, m);
+    launch_k(k_co2contra<T, TM>, stage_grid(d.N, members, TM), stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es,
+             d, m);
 }
 
 template <class T>
-static void launch_stage(dim3 g, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp, const Dims &d,
-                         const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+static void launch_co2contra(int tm, int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
+                             cudaStream_t st)
 {
-    const size_t sb = StageLayout<T>::bytes();
+    switch (tm) {
+    case 17: launch_co2contra_tm<T, 17>(members, y, w, es, d, m, st); break;
+    case 25: launch_co2contra_tm<T, 25>(members, y, w, es, d, m, st); break;
+    default: launch_co2contra_tm<T, 33>(members, y, w, es, d, m, st); break;
+    }
+}
+
+template <class T, int TM>
+static void launch_stage_tm(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
+                            const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+{
+    const dim3 g = stage_grid(d.N, members, TM);
+    const size_t sb = StageLayout<T, TM>::bytes();
     switch (a.mode) {
-    case 0: k_stage<T, 0><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: k_stage<T, 1><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: k_stage<T, 2><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: k_stage<T, 3><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: k_stage<T, 4><<<g, stage_block(), sb, st>>>(y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 0: launch_k(k_stage<T, TM, 0>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: launch_k(k_stage<T, TM, 1>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: launch_k(k_stage<T, TM, 2>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: launch_k(k_stage<T, TM, 3>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: launch_k(k_stage<T, TM, 4>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    }
+}
+
+template <class T>
+static void launch_stage(int tm, int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
+                         const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+{
+    switch (tm) {
+    case 17: launch_stage_tm<T, 17>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 25: launch_stage_tm<T, 25>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    default: launch_stage_tm<T, 33>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
     }
 }
 
@@ -711,11 +774,11 @@ template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const MetricView<T> &mv)
 {
-    dim3 g = stage_grid(c);
-    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
-    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->es, (T *)c->edge, c->dims, mv);
+    const int M = c->cfg.n_members;
+    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv);
     StageArgs a{mode, dt, c->Hm};
-    launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
+    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
                     c->dims, mv, a, c->stream);
     c->launches += 3;
 }
@@ -738,12 +801,13 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
-    dim3 g = stage_grid(c);
+    const int M = c->cfg.n_members;
     if (c->elem == 8)
-        launch_co2contra<double>(g, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims, c->m64.v,
-                                 c->stream);
+        launch_co2contra<double>(c->tile, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
+                                 c->m64.v, c->stream);
     else
-        launch_co2contra<float>(g, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims, c->m32.v, c->stream);
+        launch_co2contra<float>(c->tile, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
+                                c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
     return SWE_OK;
@@ -862,13 +926,14 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     dim3 g(nb, 4), b(256);
     // contravariant components of this member into the scratch, then the four sums
     Dims d1 = c->dims;
-    dim3 gs = stage_grid(c, 1);
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(gs, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v, c->stream);
+        launch_co2contra<double>(c->tile, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
+                                 c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(gs, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v, c->stream);
+        launch_co2contra<float>(c->tile, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
+                                c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
@@ -904,14 +969,15 @@ template <class T>
 static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, void *v0, void *y1, float *cmp, int mode,
                         double dt, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, cudaEvent_t e3)
 {
-    dim3 g = stage_grid(c);
+    const int M = c->cfg.n_members;
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(g, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    k_edge<T><<<edge_grid(c), EDGE_THREADS, 0, c->stream>>>((const T *)c->es, (T *)c->edge, c->dims, mv);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm};
-    launch_stage<T>(g, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc, (T *)cmp,
+    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
+                    (T *)cmp,
                     c->dims, mv, a, c->stream);
     cudaEventRecord(e3, c->stream);
     c->launches += 3;
@@ -1107,7 +1173,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
                 cfg->N, NA_MAXN);
         return SWE_ETOOBIG;
     }
-    if (cfg->N < 8 || !tiles_fit(cfg->N) || cfg->precision != SWE_FP64 || cfg->n_members != 1 ||
+    if (cfg->N < 8 || cfg->precision != SWE_FP64 || cfg->n_members != 1 ||
         cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
         return SWE_EINVAL;
     int dev = 0;
@@ -1160,11 +1226,101 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    dim3 g = stage_grid(N, 1);
-    launch_co2contra<double>(g, vin, W, ES, dm, mv, st);
-    k_edge<double><<<edge_grid(N, 1), EDGE_THREADS, 0, st>>>(ES, E, dm, mv);
+    launch_co2contra<double>(33, 1, vin, W, ES, dm, mv, st);
+    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, E, dm, mv);
     StageArgs a{0, 0.0, Hp};
-    launch_stage<double>(g, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
+    launch_stage<double>(33, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
+    return SWE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tile size and its autotuner
+// ---------------------------------------------------------------------------
+static void drop_graph(swe_ctx *c)
+{
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+}
+
+extern "C" int swe_set_tile(swe_ctx *c, int tile)
+{
+    if (!c || !valid_tile(tile)) return SWE_EINVAL;
+    if (c->tile != tile) drop_graph(c);
+    c->tile = tile;
+    return SWE_OK;
+}
+
+extern "C" int swe_get_tile(const swe_ctx *c, int *tile)
+{
+    if (!c || !tile) return SWE_EINVAL;
+    *tile = c->tile;
+    return SWE_OK;
+}
+
+namespace {
+struct TuneKey {
+    int device, N, precision, members;
+    bool operator==(const TuneKey &o) const
+    {
+        return device == o.device && N == o.N && precision == o.precision && members == o.members;
+    }
+};
+struct TuneEntry {
+    TuneKey key;
+    int tile;
+    double ms[3];
+};
+std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
+}  // namespace
+
+// Time RK4 steps of a zero state for every built tile size and keep the fastest.
+// The state lives in a scratch vector of this context; the caller's states are
+// not touched.  Results are cached per (device, N, precision, members).
+extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_per_step)
+{
+    if (!c || nreps < 1) return SWE_EINVAL;
+    const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members};
+    for (const TuneEntry &e : g_tuned)
+        if (e.key == key) {
+            swe_set_tile(c, e.tile);
+            if (best_tile) *best_tile = e.tile;
+            if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = e.ms[k];
+            return SWE_OK;
+        }
+    swe_stvec *v = nullptr;
+    int rc = swe_stvec_create(c, &v);
+    if (rc) return rc;
+    const int keep = c->tile;
+    double ms[3];
+    int best = keep;
+    double best_ms = 1e300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    rc = SWE_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(c, SWE_ECUDA, "autotune events");
+    const double dt = 1.0;
+    for (int k = 0; k < 3 && rc == SWE_OK; k++) {
+        swe_set_tile(c, k_tiles[k]);
+        if ((rc = swe_rk4_steps(c, v, dt, 2)) != SWE_OK) break;
+        if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
+        if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
+        float t = 0.f;
+        if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+            rc = fail(c, SWE_ECUDA, "autotune timing");
+            break;
+        }
+        ms[k] = t / nreps;
+        if (ms[k] < best_ms) { best_ms = ms[k]; best = k_tiles[k]; }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    swe_stvec_destroy(v);
+    drop_graph(c);
+    if (rc != SWE_OK) { c->tile = keep; return rc; }
+    c->tile = best;
+    TuneEntry te{key, best, {ms[0], ms[1], ms[2]}};
+    g_tuned.push_back(te);
+    if (best_tile) *best_tile = best;
+    if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = ms[k];
     return SWE_OK;
 }

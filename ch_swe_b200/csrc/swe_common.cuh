@@ -55,4 +55,12 @@ struct MetricView {
     T grav;
 };
 
+// Programmatic dependent launch (sm_90+): a kernel launched with programmatic
+// stream serialization may start while its predecessor in the stream still runs;
+// pdl_wait() returns once the predecessor grid has completed and its writes are
+// visible, pdl_trigger() lets this grid's successor launch.  Both are no-ops for
+// a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace chswe

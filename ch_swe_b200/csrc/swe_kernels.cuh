@@ -228,6 +228,8 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
     const Strips<T> S{ES + strip_member(N, mem), n};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
+    pdl_trigger();
+    pdl_wait();
     if (warp < 8) {
         const int a = a0 + lane, q = warp & 3;
         if (a < a1) {

@@ -2,8 +2,9 @@
 //
 // A block of 256 threads owns a tile [i0, i1) x [j0, j1) of the (N+1) x (N+1)
 // box of one panel of one member.  Tiles are balanced: gridDim.x tiles split the
-// N+1 columns into widths floor/ceil((N+1)/gridDim.x) <= TILE_XM, likewise rows,
-// so N+1 = 32k+1 gives no one-column slivers.  The block copies the windows it
+// N+1 columns into widths floor/ceil((N+1)/gridDim.x) <= TM, likewise rows, so
+// N+1 = (TM-1)k+1 gives no one-column slivers.  TM (odd) is a template
+// parameter; the host picks it per cube size (autotuned).  The block copies the windows it
 // needs (tile plus stencil footprint) from the zero-margined panel boxes into
 // shared memory without bounds checks and evaluates the SBP stencils there.
 //
@@ -22,14 +23,26 @@
 
 namespace chswe {
 
-constexpr int TILE_XN = 32;     // nominal tile width (tiles = ceil(N / TILE_XN))
-constexpr int TILE_YN = 32;     // nominal tile height
-constexpr int TILE_XM = 33;     // maximal tile width  (balanced split of N+1 columns)
-constexpr int TILE_YM = 33;     // maximal tile height
 constexpr int STAGE_THREADS = 256;
-constexpr int PW = TILE_XM + 6;   // odd pitch of the (tile + 5)-wide windows
-constexpr int PT = TILE_XM;       // odd pitch of tile-wide windows
-constexpr int RW = TILE_YM + 5;   // rows of (tile + 5)-high windows
+
+// Tiles of at most TM x TM points, ceil(N / (TM - 1)) of them per direction.
+template <int TM>
+struct Tile {
+    static_assert(TM % 2 == 1, "odd shared-memory pitches need an odd maximal tile");
+    static constexpr int XN = TM - 1;   // nominal width
+    static constexpr int PW = TM + 6;   // odd pitch of (tile + 5)-wide windows
+    static constexpr int PT = TM;       // odd pitch of tile-wide windows
+    static constexpr int RW = TM + 5;   // rows of (tile + 5)-high windows
+    // trip bounds of the flattened passes: (tile+5)^2 windows, (tile+5) x tile strips, tile^2
+    static constexpr int IT_WIN = ((TM + 5) * (TM + 5) + STAGE_THREADS - 1) / STAGE_THREADS;
+    static constexpr int IT_STRIP = ((TM + 5) * TM + STAGE_THREADS - 1) / STAGE_THREADS;
+    static constexpr int IT_TILE = (TM * TM + STAGE_THREADS - 1) / STAGE_THREADS;
+};
+
+#define CHSWE_TILE_CONSTANTS(TM)                                                                           \
+    constexpr int PW = Tile<TM>::PW, PT = Tile<TM>::PT, RW = Tile<TM>::RW, IT_WIN = Tile<TM>::IT_WIN,      \
+                  IT_STRIP = Tile<TM>::IT_STRIP, IT_TILE = Tile<TM>::IT_TILE;                               \
+    (void)RW
 
 __device__ __forceinline__ void tile_range(int n, int &i0, int &i1, int &j0, int &j1)
 {
@@ -91,13 +104,6 @@ template <class T> __device__ __forceinline__ T di2c_u(int k, int n, const Line<
     return (k >= 4 && k <= n - 3) ? di2c_in<T>(k, f) : di2c<T>(k, n, f);
 }
 
-// Loop trip bounds of the flattened passes (256 threads): (tile+5)^2 windows,
-// (tile+5) x tile strips, tile^2.
-constexpr int IT_WIN = ((TILE_XM + 5) * (TILE_YM + 5) + STAGE_THREADS - 1) / STAGE_THREADS;
-constexpr int IT_STRIP = ((TILE_XM + 5) * TILE_YM + STAGE_THREADS - 1) / STAGE_THREADS;
-constexpr int IT_TILE = (TILE_XM * TILE_YM + STAGE_THREADS - 1) / STAGE_THREADS;
-static_assert(TILE_XM == TILE_YM, "strip bound assumes square maximal tiles");
-
 // Every global load of a pass is issued into registers before the first
 // shared-memory store or stencil of that pass (fixed-trip unrolled loops), so a
 // block pays one memory round trip per batch instead of one per loop iteration.
@@ -106,19 +112,21 @@ static_assert(TILE_XM == TILE_YM, "strip bound assumes square maximal tiles");
 // contravariant components (co2contra_Ch_mod.f90:27-94)
 //   ut = Qi11 u + J^-1 I_i2c,x( J Qi12 I_c2i,y(v) ),  vt = Qi22 v + J^-1 I_i2c,y( J Qi12 I_c2i,x(u) )
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, int TM>
 struct Co2Layout {
-    static constexpr int V = 0, U = V + PW * RW, VQ = U + PW * RW, UQ = VQ + PW * TILE_YM, UX = UQ + PT * RW,
-                         TOTAL = UX + PT * TILE_YM;
+    static constexpr int PW = Tile<TM>::PW, PT = Tile<TM>::PT, RW = Tile<TM>::RW;
+    static constexpr int V = 0, U = V + PW * RW, VQ = U + PW * RW, UQ = VQ + PW * TM, UX = UQ + PT * RW,
+                         TOTAL = UX + PT * TM;
     static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
 
-template <class T>
+template <class T, int TM>
 __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
                                                                  T *__restrict__ ES, Dims d, MetricView<T> m)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    using L = Co2Layout<T>;
+    using L = Co2Layout<T, TM>;
+    CHSWE_TILE_CONSTANTS(TM);
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -132,8 +140,20 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
     const SWin<T, PW> sv{sm + L::V, i0 - 2, j0 - 3}, su{sm + L::U, i0 - 3, j0 - 2}, svq{sm + L::VQ, i0 - 2, j0};
     const SWin<T, PT> suq{sm + L::UQ, i0, j0 - 2}, sux{sm + L::UX, i0, j0};
 
-    // ---- batch 1: v and u windows, J Qi12 at both xy intermediates
+    // ---- before the predecessor grid completes: J Qi12 at both xy intermediates (metric only)
+    pdl_trigger();
     T jq1[IT_STRIP], jq2[IT_STRIP];
+#pragma unroll
+    for (int it = 0; it < IT_STRIP; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, c;
+        split(q, w5, iw5, r, c);
+        jq1[it] = q < w5 * th ? __ldg(m.JQ12 + box_off(P, sv.x0 + c, j0 + r)) : T(0);
+        split(q, tw, iw, r, c);
+        jq2[it] = q < tw * h5 ? __ldg(m.JQ12 + box_off(P, i0 + c, suq.y0 + r)) : T(0);
+    }
+    pdl_wait();
+    // ---- batch 1: v and u windows
     {
         const T *gv = y + 2 * d.fs + box_off(P, sv.x0, sv.y0), *gu = y + d.fs + box_off(P, su.x0, su.y0);
         T rv[IT_WIN], ru[IT_WIN];
@@ -145,15 +165,6 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
             const bool ok = q < w5 * h5;
             rv[it] = ok ? __ldg(gv + r * P + c) : T(0);
             ru[it] = ok ? __ldg(gu + r * P + c) : T(0);
-        }
-#pragma unroll
-        for (int it = 0; it < IT_STRIP; it++) {
-            const int q = threadIdx.x + it * STAGE_THREADS;
-            int r, c;
-            split(q, w5, iw5, r, c);
-            jq1[it] = q < w5 * th ? __ldg(m.JQ12 + box_off(P, sv.x0 + c, j0 + r)) : T(0);
-            split(q, tw, iw, r, c);
-            jq2[it] = q < tw * h5 ? __ldg(m.JQ12 + box_off(P, i0 + c, suq.y0 + r)) : T(0);
         }
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
@@ -252,12 +263,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
 // ---------------------------------------------------------------------------
 // fused stage: tendency of the linear operator + RK4 update
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, int TM>
 struct StageLayout {
-    static constexpr int H = 0, UT = H + PW * RW, VT = UT + PW * RW, JU = VT + PW * RW, JV = JU + PW * TILE_YM,
-                         UP = JV + PT * RW, VP = UP + PW * TILE_YM, DX = VP + PT * RW, KX = DX + PT * TILE_YM,
-                         HL = KX + PT * TILE_YM, HR = HL + TILE_YM, HB = HR + TILE_YM, HT = HB + TILE_XM,
-                         TOTAL = HT + TILE_XM;
+    static constexpr int PW = Tile<TM>::PW, PT = Tile<TM>::PT, RW = Tile<TM>::RW;
+    static constexpr int H = 0, UT = H + PW * RW, VT = UT + PW * RW, JU = VT + PW * RW, JV = JU + PW * TM,
+                         UP = JV + PT * RW, VP = UP + PW * TM, DX = VP + PT * RW, KX = DX + PT * TM,
+                         HL = KX + PT * TM, HR = HL + TM, HB = HR + TM, HT = HB + TM, TOTAL = HT + TM;
     static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
 
@@ -268,14 +279,15 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 //   mode 2: Y1 = V0 + dt/2 k,  ACC += dt/3 k
 //   mode 3: Y1 = V0 + dt   k,  ACC += dt/3 k
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
-template <class T, int MODE>
+template <class T, int TM, int MODE>
 __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
 {
     using namespace sbp;
     extern __shared__ __align__(16) unsigned char smraw[];
-    using L = StageLayout<T>;
+    using L = StageLayout<T, TM>;
+    CHSWE_TILE_CONSTANTS(TM);
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -296,6 +308,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     const T *fJ2 = m.fJ2 + t * d.ps;
     const bool sat_l = i0 <= 3, sat_r = i1 - 1 >= N - 2, sat_b = j0 <= 3, sat_t = j1 - 1 >= N - 2;
 
+    pdl_trigger();
+    pdl_wait();
     // ---- batch 1a: h and ut windows with J ut
     {
         const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0);

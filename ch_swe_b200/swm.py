@@ -100,6 +100,26 @@ class Domain:
     def set_stream(self, stream_ptr: int | None):
         check(_lib.load().swe_set_stream(self.ctx, stream_ptr), self.ctx, "swe_set_stream")
 
+    # tile size of the stage kernels (17, 25 or 33) and its autotuner
+    TILES = (17, 25, 33)
+
+    @property
+    def tile(self) -> int:
+        t = ctypes.c_int()
+        check(_lib.load().swe_get_tile(self.ctx, ctypes.byref(t)), self.ctx, "swe_get_tile")
+        return t.value
+
+    @tile.setter
+    def tile(self, value: int):
+        check(_lib.load().swe_set_tile(self.ctx, int(value)), self.ctx, "swe_set_tile")
+
+    def autotune(self, nreps: int = 20) -> dict:
+        """Time RK4 steps for every tile size, keep the fastest; returns {tile: ms per step}."""
+        best = ctypes.c_int()
+        ms = (ctypes.c_double * 3)()
+        check(_lib.load().swe_autotune(self.ctx, int(nreps), ctypes.byref(best), ms), self.ctx, "swe_autotune")
+        return {t: ms[k] for k, t in enumerate(self.TILES)}
+
     def destroy(self):
         if self._ctx:
             _lib.load().swe_ctx_destroy(self._ctx)

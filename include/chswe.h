@@ -121,6 +121,19 @@ long long swe_launch_count(const swe_ctx *ctx);
 int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *ms_co2contra, double *ms_edge,
                      double *ms_stage);
 
+/* Tile size of the stage kernels: the maximal tile edge, 17, 25 or 33 points
+   (ceil(N / (tile - 1)) balanced tiles per panel direction).  Contexts start at 25
+   for N <= 96 and 33 above.  No reference counterpart: the reference's tiles are
+   MPI partitions of the panels (src/parallel/partition_mod.f90:83-129). */
+int swe_set_tile(swe_ctx *ctx, int tile);
+int swe_get_tile(const swe_ctx *ctx, int *tile);
+/* Autotuner: times nreps graph-replayed RK4 steps of a scratch state for each tile
+   size (17, 25, 33), keeps the fastest on the context and returns it; ms_per_step
+   (3 entries, may be NULL) receives each size's time per step.  Results are cached
+   for the process per (device, N, precision, members).  The caller's states are not
+   touched. */
+int swe_autotune(swe_ctx *ctx, int nreps, int *best_tile, double *ms_per_step);
+
 /* Largest cube size swe_operator_apply_noalloc accepts (its scratch is a static device
    array of about 1.5 MB that every GPU using the library holds until the process exits). */
 #define SWE_NOALLOC_MAX_N 64

@@ -53,6 +53,58 @@ def test_apply_parity_fp64_random(N):
         assert rel(g, r) < FP64_RTOL, (name, rel(g, r))
 
 
+# every tile size, with tile edges falling next to the closure rows
+@pytest.mark.parametrize("tile,N", [(17, 8), (17, 16), (17, 17), (17, 20), (17, 33), (17, 50),
+                                    (25, 24), (25, 25), (25, 26), (25, 49), (25, 50),
+                                    (33, 20), (33, 66)])
+def test_apply_parity_fp64_every_tile(tile, N):
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
+    from oracle.oracle import Oracle
+    h, u, v = random_state(N, 300 + N)
+    ref = Oracle(N, h_mean=1000.0).apply(h, u, v)
+    dom = create_domain(N, h_mean=1000.0)
+    dom.tile = tile
+    assert dom.tile == tile
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
+    x = create_stvec_swm(dom).upload(h, u, v)
+    y = create_stvec_swm(dom)
+    op.apply(y, x, dom)
+    for g, r, name in zip(y.download(), ref, "huv"):
+        assert rel(g, r) < FP64_RTOL, (tile, name, rel(g, r))
+
+
+@pytest.mark.parametrize("tile", [17, 25, 33])
+def test_rk4_every_tile_fp64(tile):
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    from oracle.oracle import Oracle
+    N, dt, nst = 24, 900.0, 6
+    o = Oracle(N, h_mean=1000.0)
+    h, u, v = o.gaussian(lam0=0.7, phi0=0.6, d0=0.2)
+    ref = o.rk4(h, u, v, dt, nst)
+    dom = create_domain(N, h_mean=1000.0)
+    dom.tile = tile
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
+    x = create_stvec_swm(dom).upload(h, u, v)
+    create_timescheme(x, "rk4").steps(x, op, dom, dt, nst)
+    for g, r, name in zip(x.download(), ref, "huv"):
+        assert rel(g, r) < FP64_RTOL, (tile, name, rel(g, r))
+
+
+def test_autotune_picks_a_built_tile_and_leaves_states_alone():
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    N = 32
+    dom = create_domain(N, precision="fp32")
+    h, u, v = random_state(N, 7)
+    x = create_stvec_swm(dom).upload(h, u, v)
+    times = dom.autotune(nreps=3)
+    assert set(times) == {17, 25, 33} and all(t > 0 for t in times.values())
+    assert dom.tile == min(times, key=times.get)
+    for g, r in zip(x.download(), (h, u, v)):
+        assert np.array_equal(g, r.astype(np.float32).astype(np.float64))
+    with pytest.raises(Exception):
+        dom.tile = 21
+
+
 @pytest.mark.parametrize("N", [16, 33, 34])
 def test_contravariant_parity_fp64(N):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
