@@ -12,6 +12,12 @@ beside it with the FP32-vs-FP64 relative L2/max errors after the day.
 Timing: W untimed warm-up integrations, then K timed integrations; each starts
 from the initial state restored on the device and after an L2 flush (a 512 MiB
 device write), bracketed by CUDA events on the library's stream; max over ranks.
+The stage kernels' tile size is autotuned per precision before the warm-up
+(``--tile`` fixes it instead).
+
+Also reported (same JSON line, ``ensemble``): the batched ensemble, 256 members
+of C48, dt 600 s, 144 RK4 steps, FP32, in one context, against the same 256
+members run one after another through a single-member context.
 ``--gpus N`` runs N independent replicas (one per GPU, weak scaling, no
 data-path collective).  ``--impl reference`` times the CPU restatement of the
 reference (the Fortran/MPI reference needs mpiifort, absent here).
@@ -200,12 +206,20 @@ def profile_traffic(precision):
     return None
 
 
+def set_tile(dom, args):
+    if args.tile == "auto":
+        return dom.autotune(nreps=10)
+    dom.tile = int(args.tile)
+    return None
+
+
 def run_precision(precision, ic, args, torch, dist, world):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
     from ch_swe_b200 import _lib
     dom = create_domain(N_CELLS, precision=precision, h_mean=H_MEAN)
     stream = torch.cuda.current_stream()
     dom.set_stream(stream.cuda_stream)
+    tune = set_tile(dom, args)
     op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
     st = create_stvec_swm(dom)
     ic_dev = create_stvec_swm(dom).upload(*ic)
@@ -267,7 +281,81 @@ def run_precision(precision, ic, args, torch, dist, world):
         "total_ms": total_ms, "launches": launches, "final": final,
         "e2e_value": cells_per_step(N_CELLS) * e2e_n / e2e_s, "e2e_bytes": nbytes,
         "ms_co2contra": co.value, "ms_edge": ed.value, "ms_stage": sg.value, "dom": dom,
+        "tile": dom.tile, "tune_ms_per_rk4_step": tune,
     }
+
+
+ENS_N, ENS_M, ENS_DT, ENS_STEPS, ENS_SEED = 48, 256, 600.0, 144, 20261203 + 4
+
+
+def run_ensemble(args, torch, dist, world):
+    """Batched ensemble (all members in one context) vs the same members one by one."""
+    from ch_swe_b200 import create_timescheme, ensemble, create_domain, create_stvec_swm, create_swm_operator
+    stream = torch.cuda.current_stream()
+    dom, op, st, params = ensemble.create_ensemble(ENS_N, ENS_M, ENS_SEED, precision="fp32")
+    dom.set_stream(stream.cuda_stream)
+    tune = set_tile(dom, args)
+    ic_dev = create_stvec_swm(dom)
+    ic_dev.assign(1.0, st)
+    rk = create_timescheme(st, "rk4")
+    for _ in range(max(1, args.warmup)):
+        st.assign(1.0, ic_dev)
+        rk.steps(st, op, dom, ENS_DT, ENS_STEPS)
+    torch.cuda.synchronize()
+    reps = 2
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    batched_ms = 0.0
+    for _ in range(reps):
+        st.assign(1.0, ic_dev)
+        a.record(stream)
+        rk.steps(st, op, dom, ENS_DT, ENS_STEPS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        batched_ms += a.elapsed_time(b)
+    batched_ms /= reps
+    # sequential: one single-member context, the members one after another
+    h0, u0, v0 = ensemble.initial_states(ENS_N, params)
+    d1 = create_domain(ENS_N, precision="fp32", h_mean=params[0][0])
+    d1.set_stream(stream.cuda_stream)
+    set_tile(d1, args)
+    op1 = create_swm_operator(d1.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": params[0][0]}, d1)
+    s1 = create_stvec_swm(d1)
+    rk1 = create_timescheme(s1, "rk4")
+    s1.upload(h0[0], u0[0], v0[0])
+    rk1.steps(s1, op1, d1, ENS_DT, ENS_STEPS)
+    torch.cuda.synchronize()
+    seq_ms = 0.0
+    for k in range(ENS_M):
+        s1.upload(h0[k], u0[k], v0[k])
+        op1.set_member_h_mean(0, params[k][0])
+        a.record(stream)
+        rk1.steps(s1, op1, d1, ENS_DT, ENS_STEPS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        seq_ms += a.elapsed_time(b)
+    # spot check: the last member alone equals its slot in the batch
+    st.assign(1.0, ic_dev)
+    rk.steps(st, op, dom, ENS_DT, ENS_STEPS)
+    got = st.download(member=ENS_M - 1)
+    alone = s1.download()
+    diff = max(float(np.abs(g - r).max() / max(np.abs(r).max(), 1e-30)) for g, r in zip(got, alone))
+    cells = 6 * ENS_N * ENS_N * ENS_STEPS * ENS_M
+    if world > 1:
+        from ch_swe_b200 import replicas
+        batched_ms = replicas.max_over_ranks(batched_ms, dist, device="cuda")
+        seq_ms = replicas.max_over_ranks(seq_ms, dist, device="cuda")
+    out = {
+        "workload": f"{ENS_M} members x C{ENS_N} linear SWE, dt {ENS_DT:g} s, {ENS_STEPS} RK4 steps, FP32 "
+                    "(FP64 metric and reductions, Kahan state), H ~ U[500,2000] m, 1-4 seeded Gaussians",
+        "value": world * cells / (batched_ms / 1e3), "unit": "cell-updates/s", "ms_batched": batched_ms,
+        "sequential_value": world * cells / (seq_ms / 1e3), "ms_sequential": seq_ms,
+        "batched_over_sequential": seq_ms / batched_ms, "tile": dom.tile, "tune_ms_per_rk4_step": tune,
+        "last_member_batched_vs_alone_rel_max": diff,
+    }
+    dom.destroy()
+    d1.destroy()
+    return out
 
 
 def run_ours(args):
@@ -289,6 +377,7 @@ def run_ours(args):
     with ClockSampler(local) as clk, torch.cuda.stream(stream):
         for prec in ("fp32", "fp64"):
             res[prec] = run_precision(prec, ic, args, torch, dist, world)
+        ens = None if args.no_ensemble else run_ensemble(args, torch, dist, world)
     clocks = clk.summary()
 
     K = args.steps
@@ -301,9 +390,11 @@ def run_ours(args):
                       "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
     peaks, src = measured_peaks()
     D = dof(N_CELLS)
-    # algorithmic bytes of one fused stage launch: 16 state words per DOF per RK4
-    # step (S1 3, S2 5, S3 5, S4 3) + 2 Kahan words (FP32), i.e. 18/4 words of 4 B
-    alg_bytes_32 = D * 4 * (18 / 4)
+    # algorithmic bytes of one fused stage launch, per DOF and RK4 step: S1 reads the
+    # state and writes Y1, ACC (3 words); S2, S3 read Y, V0, ACC and write Y, ACC (5
+    # each); S4 reads Y3, V0, ACC and writes V0 (4); FP32 adds the Kahan compensation
+    # read and write in S4 (2): 19 words of 4 B per step, 19/4 per launch
+    alg_bytes_32 = D * 4 * (19 / 4)
     achieved = alg_bytes_32 / (r32["ms_stage"] / 1e3) / 1e9
     peak = float(peaks.get("hbm_gbs", 6650.0))
     line = {
@@ -316,7 +407,9 @@ def run_ours(args):
                    "h_mean": H_MEAN, "gaussian_centre": [lam0, phi0], "parallelism": f"replicas x{world}",
                    "l2_between_steps": "flushed (512 MiB device write) before every timed step"},
         "fp64": {"value": v64, "ms_per_step": r64["total_ms"] / K, "ms_stage_kernel": r64["ms_stage"],
-                 "ms_co2contra_kernel": r64["ms_co2contra"], "ms_edge_kernel": r64["ms_edge"]},
+                 "ms_co2contra_kernel": r64["ms_co2contra"], "ms_edge_kernel": r64["ms_edge"], "tile": r64["tile"],
+                 "tune_ms_per_rk4_step": r64["tune_ms_per_rk4_step"]},
+        "fp32_tile": r32["tile"], "fp32_tune_ms_per_rk4_step": r32["tune_ms_per_rk4_step"],
         "fp32_kernel_ms": {"k_co2contra": r32["ms_co2contra"], "k_edge": r32["ms_edge"], "k_stage": r32["ms_stage"]},
         "fp32_over_fp64": v32 / v64,
         "fp32_vs_fp64_after_one_day": errs,
@@ -330,6 +423,8 @@ def run_ours(args):
         "gpu_launches": r32["launches"],
         "clocks": clocks,
     }
+    if ens is not None:
+        line["ensemble"] = ens
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -349,6 +444,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--tile", default="auto", choices=["auto", "17", "25", "33"],
+                    help="stage-kernel tile size (default: autotuned per precision)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
     args = ap.parse_args()
