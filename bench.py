@@ -17,7 +17,11 @@ The stage kernels' tile size is autotuned per precision before the warm-up
 
 Also reported (same JSON line, ``ensemble``): the batched ensemble, 256 members
 of C48, dt 600 s, 144 RK4 steps, FP32, in one context, against the same 256
-members run one after another through a single-member context.
+members run one after another through a single-member context.  And
+(``serving``): a seeded Poisson stream (200 requests/s) of linear integrations,
+N uniform over {24, 48, 96, 192, 384}, 24-576 RK4 steps, FP32/FP64 50/50,
+served with continuous batching under an HBM budget; p50/p99 latency,
+throughput, and the FP32 requests' errors against the same requests in FP64.
 ``--gpus N`` runs N independent replicas (one per GPU, weak scaling, no
 data-path collective).  ``--impl reference`` times the CPU restatement of the
 reference (the Fortran/MPI reference needs mpiifort, absent here).
@@ -286,6 +290,44 @@ def run_precision(precision, ic, args, torch, dist, world):
 
 
 ENS_N, ENS_M, ENS_DT, ENS_STEPS, ENS_SEED = 48, 256, 600.0, 144, 20261203 + 4
+SRV_REQUESTS, SRV_RATE, SRV_SEED, SRV_BUDGET = 120, 200.0, 20261203 + 5, 24 << 30
+
+
+def run_serving(args, torch):
+    """Config 5: continuous batching of a Poisson request stream."""
+    from ch_swe_b200 import serve
+    reqs = serve.poisson_stream(SRV_REQUESTS, rate=SRV_RATE, seed=SRV_SEED)
+    for r in reqs:
+        r.ic   # generate the initial states before the clock starts
+    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16)
+    stats = srv.run(reqs, realtime=True)
+    srv.close()
+    # FP32 requests against the same request in FP64 (the FP64 path is pinned to the
+    # oracle at 1e-12): a bounded sample of the smaller cubes
+    errs = []
+    for r in [r for r in reqs if r.precision == "fp32" and r.N <= 96][:8]:
+        import copy
+        r64 = copy.copy(r)
+        r64.precision = "fp64"
+        ref = serve.run_alone(r64)
+        errs.append({"rid": r.rid, "N": r.N, "steps": r.nsteps,
+                     **{f"{nm}_rel_l2": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                        for nm, a, b in zip("huv", r.result, ref)}})
+    by_size = {}
+    for N in serve.SIZES:
+        lat = [r.latency * 1e3 for r in reqs if r.N == N]
+        if lat:
+            by_size[f"C{N}"] = {"n": len(lat), "p50_ms": float(np.percentile(lat, 50)),
+                                "p99_ms": float(np.percentile(lat, 99))}
+    return {
+        "workload": f"{SRV_REQUESTS} requests, Poisson {SRV_RATE:g}/s (seed {SRV_SEED}), N in {list(serve.SIZES)}, "
+                    "24-576 RK4 steps, FP32/FP64 50/50, linear operator, 1-4 seeded Gaussians",
+        "requests": stats.n, "makespan_s": stats.makespan_s, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
+        "mean_ms": stats.mean_ms, "requests_per_s": stats.requests_per_s,
+        "cell_updates_per_s": stats.cell_updates_per_s, "hbm_budget_bytes": SRV_BUDGET,
+        "peak_pool_bytes": stats.peak_bytes, "pools": stats.pools, "latency_by_size": by_size,
+        "fp32_vs_fp64_sample": errs,
+    }
 
 
 def run_ensemble(args, torch, dist, world):
@@ -378,6 +420,7 @@ def run_ours(args):
         for prec in ("fp32", "fp64"):
             res[prec] = run_precision(prec, ic, args, torch, dist, world)
         ens = None if args.no_ensemble else run_ensemble(args, torch, dist, world)
+        srv = None if (args.no_serving or world > 1) else run_serving(args, torch)
     clocks = clk.summary()
 
     K = args.steps
@@ -425,6 +468,8 @@ def run_ours(args):
     }
     if ens is not None:
         line["ensemble"] = ens
+    if srv is not None:
+        line["serving"] = srv
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -445,6 +490,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-workload leg")
     ap.add_argument("--tile", default="auto", choices=["auto", "17", "25", "33"],
                     help="stage-kernel tile size (default: autotuned per precision)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,

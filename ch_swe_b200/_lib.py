@@ -28,7 +28,7 @@ EXPORTED = [
     "swe_stvec_assign", "swe_stvec_update", "swe_stvec_device_view", "swe_operator_apply",
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
     "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
-    "swe_set_tile", "swe_get_tile", "swe_autotune",
+    "swe_set_tile", "swe_get_tile", "swe_autotune", "swe_rk4_steps_members",
 ]
 
 
@@ -87,6 +87,7 @@ def load(path: str = LIB_PATH):
     L.swe_operator_apply_noalloc.argtypes = [ctypes.POINTER(SweCfg), _vp, _vp, _vp]
     L.swe_rk4_step.argtypes = [_vp, _vp, ctypes.c_double]
     L.swe_rk4_steps.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int]
+    L.swe_rk4_steps_members.argtypes = [_vp, _vp, _dp, ctypes.c_int]
     L.swe_integrals.argtypes = [_vp, _vp, ctypes.c_int, _dp, _dp]
     L.swe_launch_count.argtypes = [_vp]
     L.swe_launch_count.restype = ctypes.c_longlong

@@ -219,6 +219,8 @@ struct swe_ctx {
     double graph_dt = 0.0;
     int graph_kernels = 0;
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
+    bool graph_members = false;      // the cached graph uses the per-member time steps
+    double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
 };
 
 struct swe_stvec {
@@ -389,7 +391,7 @@ extern "C" int swe_cfg_default(swe_cfg *cfg)
 static void free_ctx(swe_ctx *c)
 {
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm);
+    cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
     cudaFree(c->qw); cudaFree(c->red);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -441,6 +443,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if ((rc = build_quadrature(c)) != SWE_OK) return bail(rc);
     c->Hhost.assign(cfg->n_members, cfg->h_mean);
     if (cudaMalloc(&c->Hm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
+    if (cudaMalloc(&c->dtm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
     if (cudaMemcpy(c->Hm, c->Hhost.data(), sizeof(double) * cfg->n_members, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(SWE_ECUDA);
     if ((rc = alloc_box(c, &c->ya)) || (rc = alloc_box(c, &c->yb)) || (rc = alloc_box(c, &c->acc)) ||
@@ -723,20 +726,20 @@ static cudaError_t stage_smem_optin()
 
 template <class T, int TM>
 static void launch_co2contra_tm(int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
-                                cudaStream_t st)
+                                cudaStream_t st, const double *dtm)
 {
     launch_k(k_co2contra<T, TM>, stage_grid(d.N, members, TM), stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es,
-             d, m);
+             d, m, dtm);
 }
 
 template <class T>
 static void launch_co2contra(int tm, int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
-                             cudaStream_t st)
+                             cudaStream_t st, const double *dtm = nullptr)
 {
     switch (tm) {
-    case 17: launch_co2contra_tm<T, 17>(members, y, w, es, d, m, st); break;
-    case 25: launch_co2contra_tm<T, 25>(members, y, w, es, d, m, st); break;
-    default: launch_co2contra_tm<T, 33>(members, y, w, es, d, m, st); break;
+    case 17: launch_co2contra_tm<T, 17>(members, y, w, es, d, m, st, dtm); break;
+    case 25: launch_co2contra_tm<T, 25>(members, y, w, es, d, m, st, dtm); break;
+    default: launch_co2contra_tm<T, 33>(members, y, w, es, d, m, st, dtm); break;
     }
 }
 
@@ -772,12 +775,14 @@ static dim3 edge_grid(const swe_ctx *c) { return edge_grid(c->cfg.N, c->cfg.n_me
 
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
+                          const double *dtm,
                           const MetricView<T> &mv)
 {
     const int M = c->cfg.n_members;
-    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv);
-    StageArgs a{mode, dt, c->Hm};
+    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv,
+             dtm);
+    StageArgs a{mode, dt, c->Hm, dtm};
     launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
                     c->dims, mv, a, c->stream);
     c->launches += 3;
@@ -785,8 +790,8 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
 
 static void enqueue_apply(swe_ctx *c, void *out, const void *in)
 {
-    if (c->elem == 8) enqueue_stage<double>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, c->m64.v);
-    else enqueue_stage<float>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, c->m32.v);
+    if (c->elem == 8) enqueue_stage<double>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, nullptr, c->m64.v);
+    else enqueue_stage<float>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, nullptr, c->m32.v);
 }
 
 extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
@@ -814,21 +819,21 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
 }
 
 // One RK4 step as 8 launches: stage s reads yin and writes y1 (double-buffered).
-static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt)
+static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt, const double *dtm = nullptr)
 {
     void *V = v0->d, *A = c->acc;
     if (c->elem == 8) {
         const MetricView<double> &m = c->m64.v;
-        enqueue_stage<double>(c, V, V, c->yb, A, nullptr, 1, dt, m);
-        enqueue_stage<double>(c, c->yb, V, c->ya, A, nullptr, 2, dt, m);
-        enqueue_stage<double>(c, c->ya, V, c->yb, A, nullptr, 3, dt, m);
-        enqueue_stage<double>(c, c->yb, V, nullptr, A, nullptr, 4, dt, m);
+        enqueue_stage<double>(c, V, V, c->yb, A, nullptr, 1, dt, dtm, m);
+        enqueue_stage<double>(c, c->yb, V, c->ya, A, nullptr, 2, dt, dtm, m);
+        enqueue_stage<double>(c, c->ya, V, c->yb, A, nullptr, 3, dt, dtm, m);
+        enqueue_stage<double>(c, c->yb, V, nullptr, A, nullptr, 4, dt, dtm, m);
     } else {
         const MetricView<float> &m = c->m32.v;
-        enqueue_stage<float>(c, V, V, c->yb, A, v0->cmp, 1, dt, m);
-        enqueue_stage<float>(c, c->yb, V, c->ya, A, v0->cmp, 2, dt, m);
-        enqueue_stage<float>(c, c->ya, V, c->yb, A, v0->cmp, 3, dt, m);
-        enqueue_stage<float>(c, c->yb, V, nullptr, A, v0->cmp, 4, dt, m);
+        enqueue_stage<float>(c, V, V, c->yb, A, v0->cmp, 1, dt, dtm, m);
+        enqueue_stage<float>(c, c->yb, V, c->ya, A, v0->cmp, 2, dt, dtm, m);
+        enqueue_stage<float>(c, c->ya, V, c->yb, A, v0->cmp, 3, dt, dtm, m);
+        enqueue_stage<float>(c, c->yb, V, nullptr, A, v0->cmp, 4, dt, dtm, m);
     }
 }
 
@@ -853,18 +858,19 @@ extern "C" int swe_rk4_step(swe_ctx *c, swe_stvec *v0, double dt)
     return SWE_OK;
 }
 
-extern "C" int swe_rk4_steps(swe_ctx *c, swe_stvec *v0, double dt, int nsteps)
+// nsteps replays of one captured RK4 step; members == true uses the per-member
+// time steps in c->dtm (captured by pointer, so new values need no new capture).
+static int run_steps(swe_ctx *c, swe_stvec *v0, double dt, bool members, int nsteps)
 {
-    if (!c || !v0 || v0->ctx != c || nsteps < 0) return SWE_EINVAL;
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     if (nsteps == 0) return SWE_OK;
-    if (!c->graph || c->graph_v0 != v0->d || c->graph_dt != dt) {
+    if (!c->graph || c->graph_v0 != v0->d || c->graph_members != members || (!members && c->graph_dt != dt)) {
         if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
         cudaGraph_t g;
         long long before = c->launches;
         CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_rk4(c, v0, dt);
+        enqueue_rk4(c, v0, dt, members ? c->dtm : nullptr);
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph capture: %s", cudaGetErrorString(e));
         c->graph_kernels = (int)(c->launches - before);
@@ -874,12 +880,31 @@ extern "C" int swe_rk4_steps(swe_ctx *c, swe_stvec *v0, double dt, int nsteps)
         if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
         c->graph_v0 = v0->d;
         c->graph_dt = dt;
+        c->graph_members = members;
     }
     for (int s = 0; s < nsteps; s++) {
         CU(c, cudaGraphLaunch(c->graph, c->stream));
         c->launches += c->graph_kernels;
     }
     return SWE_OK;
+}
+
+extern "C" int swe_rk4_steps(swe_ctx *c, swe_stvec *v0, double dt, int nsteps)
+{
+    if (!c || !v0 || v0->ctx != c || nsteps < 0) return SWE_EINVAL;
+    return run_steps(c, v0, dt, false, nsteps);
+}
+
+extern "C" int swe_rk4_steps_members(swe_ctx *c, swe_stvec *v0, const double *dt, int nsteps)
+{
+    if (!c || !v0 || v0->ctx != c || !dt || nsteps < 0) return SWE_EINVAL;
+    const int M = c->cfg.n_members;
+    for (int k = 0; k < M; k++)
+        if (!(dt[k] >= 0.0) || !std::isfinite(dt[k]))
+            return fail(c, SWE_EINVAL, "member %d: time step %g (need finite, >= 0)", k, dt[k]);
+    if (nsteps == 0) return SWE_OK;
+    CU(c, cudaMemcpyAsync(c->dtm, dt, sizeof(double) * M, cudaMemcpyHostToDevice, c->stream));
+    return run_steps(c, v0, 0.0, true, nsteps);
 }
 
 // ---------------------------------------------------------------------------
@@ -973,9 +998,10 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
     cudaEventRecord(e0, c->stream);
     launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv,
+             (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
-    StageArgs a{mode, dt, c->Hm};
+    StageArgs a{mode, dt, c->Hm, nullptr};
     launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
                     c->dims, mv, a, c->stream);
@@ -1227,8 +1253,9 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
     launch_co2contra<double>(33, 1, vin, W, ES, dm, mv, st);
-    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, E, dm, mv);
-    StageArgs a{0, 0.0, Hp};
+    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, E, dm, mv,
+             (const double *)nullptr);
+    StageArgs a{0, 0.0, Hp, nullptr};
     launch_stage<double>(33, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;

@@ -42,6 +42,9 @@ __device__ __forceinline__ GV<T> mview(const T *p, const Dims &d)
     return GV<T>{p, d.P};
 }
 
+// A member whose per-member time step is 0 is frozen: every block of it exits at once.
+__device__ __forceinline__ bool member_frozen(const double *dtm, int mem) { return dtm && dtm[mem] == 0.0; }
+
 // Vertex of side s at along-edge index a (1..N+1), `depth` nodes inward.
 __device__ __forceinline__ void side_vertex(int N, int s, int a, int depth, int &i, int &j)
 {
@@ -219,12 +222,13 @@ constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the th
 // across L/R, y-neighbour across B/T).
 template <class T>
 __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, T *__restrict__ E, Dims d,
-                                                        MetricView<T> m)
+                                                        MetricView<T> m, const double *__restrict__ dtm)
 {
     __shared__ T raw[3][4][EDGE_CHUNK];   // [own, x-neighbour, y-neighbour][quantity][vertex]
     const int N = d.N, n = N + 1;
     const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
     const int a0 = 1 + (blockIdx.x * n) / gridDim.x, a1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
+    if (member_frozen(dtm, mem)) return;
     const Strips<T> S{ES + strip_member(N, mem), n};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
@@ -312,6 +316,7 @@ struct StageArgs {
     int mode;          // 0: write the tendency A(y) to out; 1..4: RK4 stage
     double dt;
     const double *Hm;  // per-member mean depth
+    const double *dtm; // per-member time step (null: dt for all); 0 freezes a member
 };
 
 // Kahan-compensated state update for FP32 (s += inc with compensation c).

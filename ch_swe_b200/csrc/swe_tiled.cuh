@@ -122,7 +122,8 @@ struct Co2Layout {
 
 template <class T, int TM>
 __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
-                                                                 T *__restrict__ ES, Dims d, MetricView<T> m)
+                                                                 T *__restrict__ ES, Dims d, MetricView<T> m,
+                                                                 const double *__restrict__ dtm)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = Co2Layout<T, TM>;
@@ -134,6 +135,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restr
     const int tw = i1 - i0, th = j1 - j0, w5 = tw + 5, h5 = th + 5;
     const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
     const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
+    if (member_frozen(dtm, mem)) return;
     const T *y = Y + mem * d.ms + t * d.ps;
     T *w = W + mem * d.ms + t * d.ps;
     T *es = ES + strip_member(N, mem) + (int64_t)t * 4 * STRIP_LINES * n - 1;   // + (s*4 + line)*n + index
@@ -294,6 +296,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     tile_range(n, i0, i1, j0, j1);
     const int tw = i1 - i0, th = j1 - j0;
     const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
+    if (member_frozen(a.dtm, mem)) return;
     const int64_t mo = mem * d.ms;
     const T *y = Yin + mo;                 // member base (the h halos read the other panels)
     const T *w = Wc + mo;
@@ -517,7 +520,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     T *v0 = V0 + mo + t * d.ps, *y1 = Y1 + mo + t * d.ps, *acc = ACC + mo + t * d.ps;
     T *cmp = CMP ? CMP + mo + t * d.ps : nullptr;
     const int64_t fs = d.fs;
-    const T dt = T(a.dt);
+    const T dt = T(a.dtm ? a.dtm[mem] : a.dt);
     constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
     T pv[3][IT_TILE], pa[3][IT_TILE], pc[3][IT_TILE];
 #pragma unroll

@@ -1,0 +1,318 @@
+"""Served mixed workload: continuous batching of shallow-water integrations on one GPU.
+
+A request is one integration: cube size N, precision, number of RK4 steps, time
+step, mean depth and an initial state (h, u, v).  The server keeps one *pool*
+per (N, precision): a context with a fixed number of member slots, its own CUDA
+stream and its states resident in HBM.  A request occupies one slot from
+admission to completion.
+
+Continuous batching:
+- every pool advances all of its occupied slots together in *ticks* of at most
+  `max_tick` RK4 steps (one graph replay per step, `swe_rk4_steps_members`);
+  free slots have time step 0 and cost nothing (their blocks exit at once);
+- a tick is as long as the shortest remaining integration in the pool, so every
+  request stops exactly at its own step count;
+- between ticks, finished requests leave (their state is downloaded) and queued
+  requests of that pool are uploaded into the free slots;
+- pools run on separate streams, so the work of different cube sizes and
+  precisions overlaps on the device.
+
+Admission by HBM budget: a pool is created when a request needs one and its
+slots fit in the budget that other pools leave free (idle empty pools are
+released to make room); requests wait in the queue until a slot frees up.
+
+The reference has no server: it integrates one state per run
+(src/models/shallow_water/shallow_water_mod.f90:112-143).  Each served result
+is the same as the same request run alone (tests/test_gpu_serve.py).
+"""
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import ensemble, testcases
+
+SIZES = (24, 48, 96, 192, 384)
+MAX_SLOTS = {24: 64, 48: 64, 96: 32, 192: 16, 384: 8}
+
+
+def stable_dt(N: int) -> float:
+    """RK4 time step of the served linear runs: 150 s at C192, scaled with the grid spacing."""
+    return 150.0 * 192.0 / N
+
+
+def member_bytes(N: int, precision: str) -> int:
+    """Device bytes one member slot of a pool holds: the state, two stage buffers,
+    the RK accumulator, the contravariant scratch, the FP32 compensation, the edge
+    buffer and the edge strips (layout of swe_api.cu)."""
+    elem = 4 if precision == "fp32" else 8
+    rows = N + 9
+    pitch = (rows + 7) // 8 * 8
+    box = 3 * 6 * rows * pitch
+    words = 5 * box + 6 * 4 * (N + 1) * (3 + 4)
+    extra = box * 4 if precision == "fp32" else 0
+    return words * elem + extra
+
+
+@dataclass
+class Request:
+    rid: int
+    N: int
+    precision: str
+    nsteps: int
+    dt: float
+    h_mean: float
+    ic_params: tuple            # (centres, widths, amps) of the Gaussian bumps, or (h, u, v) arrays
+    arrival: float = 0.0
+    operator: str = "linear"
+    # filled by the server
+    admitted: float | None = None
+    finished: float | None = None
+    pool_tile: int | None = None
+    result: tuple | None = None
+
+    _ic: tuple | None = None
+
+    @property
+    def ic(self):
+        """Initial (h, u, v), FP64 host arrays (generated on first use)."""
+        if self._ic is None:
+            p = self.ic_params
+            if len(p) == 3 and isinstance(p[0], np.ndarray):
+                self._ic = p
+            else:
+                self._ic = testcases.gaussian_sum(self.N, *p)
+        return self._ic
+
+    @property
+    def cell_updates(self) -> int:
+        return 6 * self.N * self.N * self.nsteps
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.finished is None else self.finished - self.arrival
+
+
+def poisson_stream(n_requests: int, rate: float = 200.0, seed: int = 20261203 + 5, sizes=SIZES,
+                   steps=(24, 576), precisions=("fp32", "fp64")):
+    """Seeded Poisson arrivals (mean `rate` per second); N uniform over `sizes`, steps
+    uniform in `steps`, precision 50/50; each request one ensemble-style initial
+    state (H ~ U[500, 2000] m, 1-4 Gaussians)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for k in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        N = int(rng.choice(sizes))
+        nst = int(rng.integers(steps[0], steps[1] + 1))
+        prec = str(rng.choice(precisions))
+        H, centres, widths, amps = ensemble.member_params(1, int(rng.integers(1 << 31)))[0]
+        reqs.append(Request(k, N, prec, nst, stable_dt(N), H, (centres, widths, amps), arrival=t))
+    return reqs
+
+
+class Pool:
+    """Member slots of one (N, precision): one context on its own stream."""
+
+    def __init__(self, N: int, precision: str, capacity: int, torch, tile=None):
+        from .swm import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+        self.N, self.precision, self.capacity = N, precision, capacity
+        self.torch = torch
+        self.stream = torch.cuda.Stream()
+        self.dom = create_domain(N, precision=precision, n_members=capacity)
+        self.dom.set_stream(self.stream.cuda_stream)
+        if tile is None:
+            with torch.cuda.stream(self.stream):
+                self.dom.autotune(nreps=4)
+        else:
+            self.dom.tile = tile
+        self.op = create_swm_operator(self.dom.grav, {"swm_operator_type": "linear_swm_operator",
+                                                      "h_mean": 1000.0}, self.dom)
+        self.state = create_stvec_swm(self.dom)
+        self.rk = create_timescheme(self.state, "rk4")
+        self.slots: list[Request | None] = [None] * capacity
+        self.remaining = [0] * capacity
+        self.event = None
+        self.tick_len = 0
+        self.bytes = capacity * member_bytes(N, precision)
+
+    @property
+    def busy(self) -> bool:
+        return self.event is not None
+
+    @property
+    def occupied(self) -> int:
+        return sum(r is not None for r in self.slots)
+
+    def free_slot(self):
+        for k, r in enumerate(self.slots):
+            if r is None:
+                return k
+        return None
+
+    def admit(self, req: Request, now: float):
+        k = self.free_slot()
+        self.state.upload(*req.ic, member=k)
+        self.op.set_member_h_mean(k, req.h_mean)
+        self.slots[k] = req
+        self.remaining[k] = req.nsteps
+        req.admitted = now
+        req.pool_tile = self.dom.tile
+
+    def launch_tick(self, max_tick: int):
+        active = [k for k, r in enumerate(self.slots) if r is not None and self.remaining[k] > 0]
+        if not active:
+            return False
+        L = min(max_tick, min(self.remaining[k] for k in active))
+        dts = np.zeros(self.capacity)
+        for k in active:
+            dts[k] = self.slots[k].dt
+        with self.torch.cuda.stream(self.stream):
+            self.rk.steps_members(self.state, self.op, dts, L)
+            self.event = self.torch.cuda.Event()
+            self.event.record(self.stream)
+        self.tick_len = L
+        return True
+
+    def poll(self, now_fn):
+        """If the tick in flight has finished: account it, retire finished requests."""
+        if self.event is None or not self.event.query():
+            return []
+        self.event = None
+        done = []
+        for k, r in enumerate(self.slots):
+            if r is None or self.remaining[k] <= 0:
+                continue
+            self.remaining[k] -= self.tick_len
+            if self.remaining[k] == 0:
+                r.result = self.state.download(member=k)
+                r.finished = now_fn()
+                self.slots[k] = None
+                done.append(r)
+        return done
+
+    def destroy(self):
+        self.dom.destroy()
+
+
+@dataclass
+class ServeStats:
+    n: int
+    makespan_s: float
+    p50_ms: float
+    p99_ms: float
+    mean_ms: float
+    requests_per_s: float
+    cell_updates_per_s: float
+    pools: dict = field(default_factory=dict)
+    peak_bytes: int = 0
+
+
+class Server:
+    def __init__(self, hbm_budget_bytes: int = 16 << 30, max_tick: int = 16, max_slots=None, tiles=None):
+        import torch
+        self.torch = torch
+        self.budget = int(hbm_budget_bytes)
+        self.max_tick = int(max_tick)
+        self.max_slots = dict(MAX_SLOTS if max_slots is None else max_slots)
+        self.tiles = dict(tiles or {})
+        self.pools: dict[tuple, Pool] = {}
+        self.peak = 0
+
+    def used_bytes(self) -> int:
+        return sum(p.bytes for p in self.pools.values())
+
+    def _pool_for(self, req: Request):
+        if req.operator != "linear":
+            raise ValueError(f"request {req.rid}: operator {req.operator!r} is not served")
+        key = (req.N, req.precision)
+        if key in self.pools:
+            return self.pools[key]
+        per = member_bytes(req.N, req.precision)
+        want = self.max_slots.get(req.N, 4)
+        free = self.budget - self.used_bytes()
+        if free < per:
+            # release idle, empty pools of other keys
+            for k2, p in list(self.pools.items()):
+                if not p.busy and p.occupied == 0:
+                    p.destroy()
+                    del self.pools[k2]
+            free = self.budget - self.used_bytes()
+        cap = min(want, free // per)
+        if cap < 1:
+            return None
+        pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key))
+        self.pools[key] = pool
+        self.peak = max(self.peak, self.used_bytes())
+        return pool
+
+    def run(self, requests, realtime: bool = True) -> ServeStats:
+        """Serve `requests` (arrival times in seconds from the start); realtime=False
+        admits every request at once in arrival order (for tests)."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        queue: collections.deque[Request] = collections.deque()
+        t0 = time.perf_counter()
+        now = (lambda: time.perf_counter() - t0) if realtime else (lambda: 0.0)
+        if not realtime:
+            for r in pending:
+                r.arrival = 0.0
+        done = []
+        total = len(pending)
+        while len(done) < total:
+            progressed = False
+            t = now()
+            while pending and pending[0].arrival <= t:
+                queue.append(pending.popleft())
+                progressed = True
+            for p in list(self.pools.values()):
+                fin = p.poll(now)
+                if fin:
+                    done.extend(fin)
+                    progressed = True
+            # admission into free slots of idle pools, in arrival order
+            waiting = collections.deque()
+            while queue:
+                r = queue.popleft()
+                p = self._pool_for(r)
+                if p is not None and not p.busy and p.free_slot() is not None:
+                    p.admit(r, now())
+                    progressed = True
+                else:
+                    waiting.append(r)
+            queue = waiting
+            for p in self.pools.values():
+                if not p.busy and p.launch_tick(self.max_tick):
+                    progressed = True
+            if not progressed:
+                time.sleep(20e-6)
+        makespan = max(r.finished for r in done) - min(r.arrival for r in done) if realtime else time.perf_counter() - t0
+        lat = np.array([r.latency for r in done]) * 1e3 if realtime else np.array([0.0])
+        cells = sum(r.cell_updates for r in done)
+        return ServeStats(
+            n=len(done), makespan_s=makespan, p50_ms=float(np.percentile(lat, 50)),
+            p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
+            requests_per_s=len(done) / makespan, cell_updates_per_s=cells / makespan,
+            pools={f"C{k[0]}/{k[1]}": {"slots": p.capacity, "tile": p.dom.tile} for k, p in self.pools.items()},
+            peak_bytes=self.peak)
+
+    def close(self):
+        for p in self.pools.values():
+            p.destroy()
+        self.pools.clear()
+
+
+def run_alone(req: Request, tile=None):
+    """The same integration in its own single-member context (the comparison arm)."""
+    from .swm import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    dom = create_domain(req.N, precision=req.precision, h_mean=req.h_mean)
+    if tile is not None:
+        dom.tile = tile
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": req.h_mean}, dom)
+    st = create_stvec_swm(dom).upload(*req.ic)
+    create_timescheme(st, "rk4").steps_members(st, op, [req.dt], req.nsteps)
+    out = st.download()
+    dom.destroy()
+    return out

@@ -286,6 +286,14 @@ class Rk4:
         check(_lib.load().swe_rk4_steps(operator.domain.ctx, v0.handle, float(dt), int(nsteps)),
               operator.domain.ctx, "rk4 steps")
 
+    def steps_members(self, v0: StvecSwm, operator: OperatorSwmLin, dt_per_member, nsteps: int):
+        """nsteps steps with one dt per member; dt 0 freezes a member (continuous batching)."""
+        dts = np.ascontiguousarray(dt_per_member, dtype=np.float64)
+        if dts.shape != (operator.domain.n_members,):
+            raise ValueError(f"need {operator.domain.n_members} time steps, got shape {dts.shape}")
+        check(_lib.load().swe_rk4_steps_members(operator.domain.ctx, v0.handle, dptr(dts), int(nsteps)),
+              operator.domain.ctx, "rk4 steps (members)")
+
 
 def create_timescheme(state: StvecSwm, name: str):
     if name != "rk4":

@@ -109,6 +109,12 @@ int swe_operator_contravariant(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *v
 int swe_rk4_step(swe_ctx *ctx, swe_stvec *v0, double dt);
 /* nsteps RK4 steps (captured into a CUDA graph after the first call with the same shape). */
 int swe_rk4_steps(swe_ctx *ctx, swe_stvec *v0, double dt, int nsteps);
+/* nsteps RK4 steps with a time step per member (dt[0..n_members-1]); a member with
+   dt 0 is frozen: its state is left untouched and its blocks exit at once.  This is
+   the step of continuous batching (one context = one pool of member slots).  No
+   reference counterpart: the reference advances one state per timescheme%step
+   (src/time_schemes/rk4_mod.f90:20-42). */
+int swe_rk4_steps_members(swe_ctx *ctx, swe_stvec *v0, const double *dt, int nsteps);
 /* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
 int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
 

@@ -1,0 +1,72 @@
+"""Served mixed workload (continuous batching): every result equals the same
+request run alone, the HBM budget bounds the pools, latencies are reported."""
+import numpy as np
+import pytest
+
+from tests.conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu(lib_built):
+    if not gpu_available():
+        pytest.fail("no CUDA device: the -m gpu tests need a B200")
+
+
+def _stream(n, seed, sizes=(24, 48), steps=(24, 64)):
+    from ch_swe_b200.serve import poisson_stream
+    return poisson_stream(n, rate=2000.0, seed=seed, sizes=sizes, steps=steps)
+
+
+def test_mixed_results_equal_alone_bitwise():
+    """Same tile alone and in the mix: bit-identical states (both precisions)."""
+    from ch_swe_b200.serve import Server, run_alone
+    reqs = _stream(20, 11)
+    srv = Server(hbm_budget_bytes=2 << 30, max_tick=8, max_slots={24: 6, 48: 4})
+    stats = srv.run(reqs, realtime=False)
+    srv.close()
+    assert stats.n == len(reqs)
+    for r in reqs:
+        alone = run_alone(r, tile=r.pool_tile)
+        for a, b, name in zip(r.result, alone, "huv"):
+            assert np.array_equal(a, b), (r.rid, r.N, r.precision, name, np.abs(a - b).max())
+
+
+def test_mixed_fp64_matches_oracle():
+    from ch_swe_b200.serve import Server
+    from oracle.oracle import Oracle
+    reqs = [r for r in _stream(12, 12, sizes=(24,), steps=(24, 40)) if r.precision == "fp64"][:3]
+    assert reqs
+    srv = Server(hbm_budget_bytes=1 << 30, max_tick=16)
+    srv.run(reqs, realtime=False)
+    srv.close()
+    for r in reqs:
+        o = Oracle(r.N, h_mean=r.h_mean)
+        ref = o.rk4(*r.ic, r.dt, r.nsteps)
+        for a, b, name in zip(r.result, ref, "huv"):
+            assert np.abs(a - b).max() / np.abs(b).max() < 1e-12, (r.rid, name)
+
+
+def test_budget_bounds_pools_and_all_requests_finish():
+    from ch_swe_b200.serve import Server, member_bytes
+    reqs = _stream(16, 13, sizes=(24, 48))
+    budget = 3 * member_bytes(48, "fp64") + 2 * member_bytes(24, "fp64")
+    srv = Server(hbm_budget_bytes=budget, max_tick=8)
+    stats = srv.run(reqs, realtime=False)
+    srv.close()
+    assert stats.n == len(reqs)
+    assert stats.peak_bytes <= budget
+    assert all(r.result is not None for r in reqs)
+
+
+def test_realtime_latencies_reported():
+    from ch_swe_b200.serve import Server
+    reqs = _stream(10, 14)
+    srv = Server(hbm_budget_bytes=1 << 30, max_tick=16)
+    stats = srv.run(reqs, realtime=True)
+    srv.close()
+    assert stats.n == 10
+    assert all(r.latency > 0 for r in reqs)
+    assert stats.p99_ms >= stats.p50_ms > 0
+    assert stats.cell_updates_per_s > 0

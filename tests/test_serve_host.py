@@ -1,0 +1,29 @@
+"""Host-side pieces of the serving loop (no GPU): the seeded request stream and
+the per-slot memory model."""
+import numpy as np
+
+
+def test_poisson_stream_is_seeded_and_in_range():
+    from ch_swe_b200.serve import poisson_stream, SIZES
+    a = poisson_stream(200, rate=200.0, seed=5)
+    b = poisson_stream(200, rate=200.0, seed=5)
+    assert [(r.N, r.nsteps, r.precision, r.arrival) for r in a] == [(r.N, r.nsteps, r.precision, r.arrival) for r in b]
+    assert all(r.N in SIZES and 24 <= r.nsteps <= 576 and r.precision in ("fp32", "fp64") for r in a)
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) > 0)
+    rate = len(arr) / arr[-1]
+    assert 150 < rate < 260
+    assert 0.35 < np.mean([r.precision == "fp32" for r in a]) < 0.65
+    h, u, v = a[0].ic
+    assert h.shape == (6, a[0].N + 1, a[0].N + 1) and not u.any() and not v.any()
+
+
+def test_member_bytes_and_dt():
+    from ch_swe_b200.serve import member_bytes, stable_dt
+    assert member_bytes(48, "fp64") > member_bytes(48, "fp32") > member_bytes(24, "fp32")
+    # five FP64 boxes of 3 fields x 6 panels x (N+9) x pitch dominate
+    N = 192
+    rows = N + 9
+    pitch = (rows + 7) // 8 * 8
+    assert member_bytes(N, "fp64") >= 5 * 18 * rows * pitch * 8
+    assert stable_dt(192) == 150.0 and stable_dt(384) == 75.0
