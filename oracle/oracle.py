@@ -61,6 +61,7 @@ def lib():
         L.orc_sync_weights.argtypes = [ctypes.c_void_p] + [_dp] * 4
         L.orc_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_set_operator.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -77,15 +78,21 @@ def shapes(N: int):
 class Oracle:
     """FP64 CPU restatement of the linear Ch/SBP42 shallow-water operator and RK4."""
 
+    OPERATORS = {"linear": 0, "advective": 1}
+
     def __init__(self, N: int, radius: float = EARTH_RADIUS, grav: float = EARTH_GRAV,
                  omega: float = EARTH_OMEGA, h_mean: float = 1000.0, axis=(0.0, 0.0, 1.0),
-                 coriolis_constant: bool = False):
+                 coriolis_constant: bool = False, operator: str = "linear"):
+        """operator: 'linear' (linear_swm_operator) or 'advective' (advective_swm_operator,
+        covariant Ch branch: up4 mass flux and up4 vector advection)."""
         self.N = N
         self.radius, self.grav, self.omega, self.h_mean = radius, grav, omega, h_mean
         self.axis = np.ascontiguousarray(axis, dtype=np.float64)
         self._c = lib().orc_create(N, radius, grav, omega, h_mean, _p(self.axis), int(coriolis_constant))
         if not self._c:
             raise ValueError(f"oracle: unsupported N={N} (need N >= 8)")
+        self.operator = operator
+        lib().orc_set_operator(self._c, self.OPERATORS[operator])
 
     def __del__(self):
         c = getattr(self, "_c", None)

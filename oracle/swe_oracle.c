@@ -31,6 +31,22 @@
  *   ECS Ah vector sync .. src/equiang_cs/ecs_Ah_vec_sync_mod.f90:34-125,
  *                         ecs_Ah_vec_sync_factory_mod.f90:97-158
  *   linear operator ..... src/models/shallow_water/operator/operator_swm_lin_mod.f90:66-108
+ *   advective operator .. src/models/shallow_water/operator/operator_adv_swm_mod.f90:62-126
+ *                         (covariant branch: co2contra_ch_sbp42, massflux_ch_up4,
+ *                         div_ch_sbp_sat_42_proj, grad_ch_sbp_sat_42, coriolis_Ch_sbp42,
+ *                         vector_advection_Ch_up4_cov)
+ *   up4 mass flux ....... .../horizontal/massflux/massflux_ch_mod.f90:61-121
+ *   ECS_xy scalar halo .. src/equiang_cs/ecs_halo_factory_mod.f90:70-114,190-270,
+ *                         ecs_halo_xy_mod.f90:66-235
+ *   vector advection .... .../horizontal/vec_advection/vector_advection_Ch_mod.f90:33-115,
+ *                         vector_advection_factory_mod.f90:154-200,
+ *                         .../v_dot_nabla/v_nabla_mod.f90:105-146,
+ *                         .../Christofel/hor_Christofel_shallow_mod.f90:92-164,
+ *                         hor_Christofel_factory_mod.f90:100-134,
+ *                         src/metric/metric_2d_ecs_mod.f90:270-335
+ *   ECS Ch vector halo .. src/equiang_cs/ecs_halo_vec_Ch_mod.f90:29-150,
+ *                         ecs_halo_vec_Ch_factory_mod.f90:21-270,
+ *                         src/particles/interpolations/bicubic_interp_mod.f90:27-115
  *   RK4 ................. src/time_schemes/rk4_mod.f90:20-42
  *   stvec algebra ....... src/grid_field_mod.f90:442-534
  *   quadrature .......... src/quadrature/sbp_quadrature_mod.f90:22-62,
@@ -673,6 +689,10 @@ typedef struct orc_ctx {
     fld_t h, u, v, du, dv, dh;
     fld_t gx, gy, ut, vt, uq, vq, up, vp, Ju, Jv, Dx, Dy, div;
     fld_t k[4][3], y[3];
+    /* advective operator */
+    int nonlinear;
+    exch_t ex_xy5_full_s, ex_ch1c_u, ex_ch1c_v;
+    fld_t htot, hu, hv, cu, cv, uh, vh, vau, uav, uhal, vhal;
 } orc_ctx;
 
 static void coriolis_parameter(orc_ctx *c)
@@ -743,10 +763,13 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     build_xy_exchange(&c->ex_xy1_cross_v, N, 1, 1, PK_VEC);
     build_ch_exchange(&c->ex_ch3_u, N, 3, 0, 1);
     build_ch_exchange(&c->ex_ch3_v, N, 3, 0, 0);
+    build_xy_exchange(&c->ex_xy5_full_s, N, 5, 0, PK_SCALAR);
+    build_ch_exchange(&c->ex_ch1c_u, N, 1, 1, 1);
+    build_ch_exchange(&c->ex_ch1c_v, N, 1, 1, 0);
     int hw = 5;
-    fld_t *xy[] = {&c->h, &c->dh, &c->uq, &c->vq, &c->up, &c->vp, &c->Dx, &c->Dy, &c->div};
-    fld_t *yy[] = {&c->u, &c->du, &c->gx, &c->ut, &c->Ju};
-    fld_t *xx[] = {&c->v, &c->dv, &c->gy, &c->vt, &c->Jv};
+    fld_t *xy[] = {&c->h, &c->dh, &c->uq, &c->vq, &c->up, &c->vp, &c->Dx, &c->Dy, &c->div, &c->htot, &c->uh, &c->vh};
+    fld_t *yy[] = {&c->u, &c->du, &c->gx, &c->ut, &c->Ju, &c->hu, &c->cu, &c->vau, &c->uhal};
+    fld_t *xx[] = {&c->v, &c->dv, &c->gy, &c->vt, &c->Jv, &c->hv, &c->cv, &c->uav, &c->vhal};
     for (unsigned q = 0; q < sizeof(xy) / sizeof(xy[0]); q++) fld_init(xy[q], N + 1, N + 1, hw);
     for (unsigned q = 0; q < sizeof(yy) / sizeof(yy[0]); q++) fld_init(yy[q], N, N + 1, hw);
     for (unsigned q = 0; q < sizeof(xx) / sizeof(xx[0]); q++) fld_init(xx[q], N + 1, N, hw);
@@ -768,7 +791,8 @@ void orc_destroy(orc_ctx *c)
     free(c->fJ2); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
-                    &c->y[0], &c->y[1], &c->y[2]};
+                    &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
+                    &c->vh, &c->vau, &c->uav, &c->uhal, &c->vhal};
     for (unsigned q = 0; q < sizeof(all) / sizeof(all[0]); q++) fld_free(all[q]);
     for (int s = 0; s < 4; s++) for (int f = 0; f < 3; f++) fld_free(&c->k[s][f]);
     free(c);
@@ -938,7 +962,7 @@ static void op_div(orc_ctx *c, fld_t *div, fld_t *ut, fld_t *vt)
 }
 
 /* operator_swm_lin_t%apply (operator_swm_lin_mod.f90:66-108) */
-static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
+static void op_apply_lin(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
 {
     int N = c->N;
     op_grad(c, &c->gx, &c->gy, h);
@@ -960,6 +984,394 @@ static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= N + 1; j++)
             for (int i = 1; i <= N + 1; i++) FA(dh, t, i, j) = -c->H * FA(&c->div, t, i, j);
+}
+
+
+/* ================================================================== */
+/* advective operator, covariant Ch branch                              */
+/* ================================================================== */
+
+/* Point of a mesh at any (also halo) index: position on the sphere and the
+   covariant basis a1 / a2 (set_curvilinear_mesh, metric_2d_ecs_mod.f90:338-411);
+   same expressions as mesh_build. */
+static void mesh_point(const mesh_t *m, int t, int i, int j, double r[3], double a1[3], double a2[3])
+{
+    double alpha = -0.25 * PI_ + (i - 1 + m->shift_i) * m->hx, beta = -0.25 * PI_ + (j - 1 + m->shift_j) * m->hy;
+    double ta = tan(alpha), tb = tan(beta);
+    double sigm = sqrt(1.0 + ta * ta + tb * tb);
+    double rp[3] = {ta / sigm, tb / sigm, 1.0 / sigm};
+    proto2real(t, rp, r);
+    double s15 = pow(1.0 + pow(ta, 2.0) + pow(tb, 2.0), 1.5);
+    double a1p[3] = {(1.0 + pow(ta, 2.0)) * (1.0 + pow(tb, 2.0)) / s15, -ta * tb * (1.0 + pow(ta, 2.0)) / s15,
+                     -ta * (1.0 + pow(ta, 2.0)) / s15};
+    double a2p[3] = {-ta * tb * (1.0 + pow(tb, 2.0)) / s15, (1.0 + pow(ta, 2.0)) * (1.0 + pow(tb, 2.0)) / s15,
+                     -tb * (1.0 + pow(tb, 2.0)) / s15};
+    proto2real(t, a1p, a1);
+    proto2real(t, a2p, a2);
+}
+
+/* transform_cartesian_to_native_ecs (metric_2d_ecs_mod.f90:310-335): the panel with
+   the largest projection of r on its outer normal, and (alpha, beta) there. */
+static void cart_to_native(const double r[3], int *panel, double *alpha, double *beta)
+{
+    int p = 0;
+    double best = 0.0;
+    for (int q = 0; q < NPAN; q++) {
+        double d = -(r[0] * T_N[q][0] + r[1] * T_N[q][1] + r[2] * T_N[q][2]);
+        if (d > best) { p = q; best = d; }
+    }
+    *panel = p;
+    *alpha = atan((T_EX[p][0] * r[0] + T_EX[p][1] * r[1] + T_EX[p][2] * r[2]) / best);
+    *beta = atan((T_EY[p][0] * r[0] + T_EY[p][1] * r[1] + T_EY[p][2] * r[2]) / best);
+}
+
+/* ---- ECS_xy scalar halo (massflux_factory_mod.f90:59-64: width 3) ---- */
+
+/* init_halo_xy_interp (ecs_halo_factory_mod.f90:236-270): cubic Lagrange weights
+   along the source face's grid line for target index i at halo row j. */
+static void halo_xy_weights(int n, double dxa, int i, int j, double w[4], int *ind)
+{
+    double zb = 0.25 * PI_ + j * dxa;
+    double za = -0.25 * PI_ + (i - 1.0) * dxa;
+    double zx = tan(za);
+    double zz = tan(zb);
+    zx = zx / zz;
+    za = atan(zx);
+    int k = (int)floor((za + 0.25 * PI_) / dxa) + 1;
+    k = imin(imax(2, k), n - 2);
+    double zxi = (za + 0.25 * PI_) / dxa - (k - 1.0);
+    w[0] = -(zxi * (zxi - 1.0) * (zxi - 2.0) / 6.0);
+    w[1] = (zxi + 1.0) * (zxi - 1.0) * (zxi - 2.0) / 2.0;
+    w[2] = -((zxi + 1.0) * zxi * (zxi - 2.0) / 2.0);
+    w[3] = (zxi + 1.0) * zxi * (zxi - 1.0) / 6.0;
+    *ind = k;
+}
+
+/* ecs_ext_halo_1e: interpolate one line (values zf[b] at b = 1..n) */
+static double halo_xy_line(int n, double dxa, int i, int j, const double *zf)
+{
+    double w[4];
+    int ii;
+    halo_xy_weights(n, dxa, i, j, w, &ii);
+    return w[0] * zf[ii - 1] + w[1] * zf[ii] + w[2] * zf[ii + 1] + w[3] * zf[ii + 2];
+}
+
+/* get_ecs_halo + ext_ecs_tile_halo (ecs_halo_xy_mod.f90:66-235) on the whole panel
+   (one tile per panel): the exchange, then corner diagonals and the averaging of
+   the duplicated vertices, then rows / columns of interpolated virtual points.
+   Modifies the interior edge and corner values of f, as the reference does. */
+static void ecs_xy_halo(orc_ctx *c, fld_t *f, int hw)
+{
+    int n = c->N + 1;
+    double dxa = c->mxy.hx;
+    exch_do(&c->ex_xy5_full_s, f, NULL);
+    double *zb = malloc(sizeof(double) * (n + 2 * hw + 8));
+    double *zl = zb + hw + 2;   /* zl[b], b = 1 - hw - 2 .. n + hw + 4 */
+    for (int t = 0; t < NPAN; t++) {
+        /* corners */
+        FA(f, t, 1, 1) = (FA(f, t, 1, 1) + FA(f, t, 1, 0) + FA(f, t, 0, 1)) / 3.0;
+        for (int j = 1; j <= hw; j++) {
+            FA(f, t, 1 - j, 1 - j) = 0.5 * (FA(f, t, -j, 1) + FA(f, t, 1, -j));
+            FA(f, t, -j, 1) = FA(f, t, 1 - j, 1 - j);
+            FA(f, t, 1, -j) = FA(f, t, 1 - j, 1 - j);
+        }
+        FA(f, t, n, 1) = (FA(f, t, n, 1) + FA(f, t, n, 0) + FA(f, t, n + 1, 1)) / 3.0;
+        for (int j = 1; j <= hw; j++) {
+            FA(f, t, n + j, 1 - j) = 0.5 * (FA(f, t, n + j + 1, 1) + FA(f, t, n, -j));
+            FA(f, t, n + j + 1, 1) = FA(f, t, n + j, 1 - j);
+            FA(f, t, n, -j) = FA(f, t, n + j, 1 - j);
+        }
+        FA(f, t, n, n) = (FA(f, t, n, n) + FA(f, t, n, n + 1) + FA(f, t, n + 1, n)) / 3.0;
+        for (int j = 1; j <= hw; j++) {
+            FA(f, t, n + j, n + j) = 0.5 * (FA(f, t, n + j + 1, n) + FA(f, t, n, n + j + 1));
+            FA(f, t, n + j + 1, n) = FA(f, t, n + j, n + j);
+            FA(f, t, n, n + j + 1) = FA(f, t, n + j, n + j);
+        }
+        FA(f, t, 1, n) = (FA(f, t, 1, n) + FA(f, t, 0, n) + FA(f, t, 1, n + 1)) / 3.0;
+        for (int j = 1; j <= hw; j++) {
+            FA(f, t, 1 - j, n + j) = 0.5 * (FA(f, t, 1, n + j + 1) + FA(f, t, -j, n));
+            FA(f, t, 1, n + j + 1) = FA(f, t, 1 - j, n + j);
+            FA(f, t, -j, n) = FA(f, t, 1 - j, n + j);
+        }
+        /* edge 1 (j = 1) */
+        for (int i = 2; i <= n - 1; i++) FA(f, t, i, 1) = 0.5 * (FA(f, t, i, 1) + FA(f, t, i, 0));
+        for (int j = 1; j <= hw; j++) {
+            for (int b = 1; b <= n; b++) zl[b] = FA(f, t, b, -j);
+            for (int i = 2 - j; i <= n + j - 1; i++) FA(f, t, i, 1 - j) = halo_xy_line(n, dxa, i, j, zl);
+        }
+        /* edge 2 (j = n) */
+        for (int i = 2; i <= n - 1; i++) FA(f, t, i, n) = 0.5 * (FA(f, t, i, n) + FA(f, t, i, n + 1));
+        for (int j = 1; j <= hw; j++) {
+            for (int b = 1; b <= n; b++) zl[b] = FA(f, t, b, n + j + 1);
+            for (int i = 2 - j; i <= n + j - 1; i++) FA(f, t, i, n + j) = halo_xy_line(n, dxa, i, j, zl);
+        }
+        /* edge 3 (i = 1) */
+        for (int j = 2; j <= n - 1; j++) FA(f, t, 1, j) = 0.5 * (FA(f, t, 1, j) + FA(f, t, 0, j));
+        for (int i = 1; i <= hw; i++) {
+            for (int b = 1; b <= n; b++) zl[b] = FA(f, t, -i, b);
+            for (int j = 2 - i; j <= n + i - 1; j++) FA(f, t, 1 - i, j) = halo_xy_line(n, dxa, j, i, zl);
+        }
+        /* edge 4 (i = n) */
+        for (int j = 2; j <= n - 1; j++) FA(f, t, n, j) = 0.5 * (FA(f, t, n, j) + FA(f, t, n + 1, j));
+        for (int i = 1; i <= hw; i++) {
+            for (int b = 1; b <= n; b++) zl[b] = FA(f, t, n + i + 1, b);
+            for (int j = 2 - i; j <= n + i - 1; j++) FA(f, t, n + i, j) = halo_xy_line(n, dxa, j, i, zl);
+        }
+    }
+    free(zb);
+}
+
+/* calc_ch_up4_massflux (massflux_ch_mod.f90:61-121): fx on the y mesh, fy on the x mesh */
+static void op_massflux_up4(orc_ctx *c, fld_t *fx, fld_t *fy, fld_t *f, fld_t *u, fld_t *v)
+{
+    int N = c->N;
+    ecs_xy_halo(c, f, 3);
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) {
+                double uu = FA(u, t, i, j);
+                double zl = 0.5 + copysign(0.5, uu), zr = 1.0 - zl;
+                FA(fx, t, i, j) = uu * (zl * (5.0 * FA(f, t, i + 1, j) + 15.0 * FA(f, t, i, j) - 5.0 * FA(f, t, i - 1, j) +
+                                              FA(f, t, i - 2, j)) +
+                                        zr * (5.0 * FA(f, t, i, j) + 15.0 * FA(f, t, i + 1, j) - 5.0 * FA(f, t, i + 2, j) +
+                                              FA(f, t, i + 3, j))) /
+                                  16.0;
+            }
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) {
+                double vv = FA(v, t, i, j);
+                double zl = 0.5 + copysign(0.5, vv), zr = 1.0 - zl;
+                FA(fy, t, i, j) = vv * (zl * (5.0 * FA(f, t, i, j + 1) + 15.0 * FA(f, t, i, j) - 5.0 * FA(f, t, i, j - 1) +
+                                              FA(f, t, i, j - 2)) +
+                                        zr * (5.0 * FA(f, t, i, j) + 15.0 * FA(f, t, i, j + 1) - 5.0 * FA(f, t, i, j + 2) +
+                                              FA(f, t, i, j + 3))) /
+                                  16.0;
+            }
+    }
+}
+
+/* ---- ECS Ch covariant vector halo (ecs_halo_vec_Ch, width 3) ---- */
+
+/* calc_w of bicubic_interp_t (bicubic_interp_mod.f90:27-84) on a mesh of the source face */
+static void bicubic_w(const mesh_t *m, double alpha, double beta, int *ix, int *iy, double wx[4], double wy[4])
+{
+    double dx = (alpha - (-0.25 * PI_)) / m->hx + 1 - m->shift_i;
+    double dy = (beta - (-0.25 * PI_)) / m->hy + 1 - m->shift_j;
+    *ix = imin(imax(2, (int)dx), m->nx - 2);
+    *iy = imin(imax(2, (int)dy), m->ny - 2);
+    dx = dx - *ix;
+    dy = dy - *iy;
+    double p1 = dx + 1.0, p2 = dx, p3 = dx - 1.0, p4 = dx - 2.0;
+    wx[0] = -p2 * p3 * p4 / 6.0; wx[1] = p1 * p3 * p4 / 2.0; wx[2] = -p1 * p2 * p4 / 2.0; wx[3] = p1 * p2 * p3 / 6.0;
+    p1 = dy + 1.0; p2 = dy; p3 = dy - 1.0; p4 = dy - 2.0;
+    wy[0] = -p2 * p3 * p4 / 6.0; wy[1] = p1 * p3 * p4 / 2.0; wy[2] = -p1 * p2 * p4 / 2.0; wy[3] = p1 * p2 * p3 / 6.0;
+}
+
+/* interp_2d_levs (bicubic_interp_mod.f90:86-113) */
+static double bicubic_v(const fld_t *f, int t, int ix, int iy, const double wx[4], const double wy[4])
+{
+    double r = 0.0;
+    for (int j1 = -1; j1 <= 2; j1++) {
+        double p = 0.0;
+        for (int i1 = -1; i1 <= 2; i1++) p = p + wx[i1 + 1] * FA(f, t, ix + i1, iy + j1);
+        r = r + wy[j1 + 1] * p;
+    }
+    return r;
+}
+
+/* The covariant component along the target basis vector a of the wind at halo
+   point r, interpolated from the source face's u (y mesh) and v (x mesh) and
+   projected with a.b1, a.b2 (ecs_halo_vec_Ch_factory_mod.f90:238-266). */
+static double vec_halo_value(orc_ctx *c, const fld_t *u, const fld_t *v, const double r[3], const double a[3])
+{
+    int p, ixu, iyu, ixv, iyv;
+    double al, be, wxu[4], wyu[4], wxv[4], wyv[4], bp[3], b1[3], b2[3];
+    cart_to_native(r, &p, &al, &be);
+    bicubic_w(&c->my, al, be, &ixu, &iyu, wxu, wyu);
+    bicubic_w(&c->mx, al, be, &ixv, &iyv, wxv, wyv);
+    b1_proto(al, be, bp); proto2real(p, bp, b1);
+    b2_proto(al, be, bp); proto2real(p, bp, b2);
+    double wu = a[0] * b1[0] + a[1] * b1[1] + a[2] * b1[2];
+    double wv = a[0] * b2[0] + a[1] * b2[1] + a[2] * b2[2];
+    double vu = bicubic_v(u, p, ixu, iyu, wxu, wyu), vv = bicubic_v(v, p, ixv, iyv, wxv, wyv);
+    return wu * vu + wv * vv;
+}
+
+/* get_halo_vector (ecs_halo_vec_Ch_mod.f90:29-150): every side-strip halo point of
+   u (y mesh) and v (x mesh) up to depth hw, from the interior of the source faces */
+static void ecs_vec_halo(orc_ctx *c, fld_t *u, fld_t *v, int hw)
+{
+    int N = c->N;
+    exch_do(&c->ex_ch3_u, u, v);
+    exch_do(&c->ex_ch3_v, u, v);
+    /* all values first (the reference interpolates every particle, then assembles) */
+    size_t cnt = (size_t)NPAN * hw * (2 * N + 2 * (N + 1)) * 2;
+    double *val = malloc(sizeof(double) * cnt);
+    double r[3], a1[3], a2[3];
+    for (int pass = 0; pass < 2; pass++) {
+        size_t q = 0;   /* both passes walk the points in the same order */
+        for (int t = 0; t < NPAN; t++)
+            for (int d = 1; d <= hw; d++) {
+                /* u: rows beyond south / north, columns beyond west / east */
+                for (int i = 1; i <= N; i++) {
+                    int jj[2] = {1 - d, N + 1 + d};
+                    for (int s = 0; s < 2; s++, q++) {
+                        if (pass == 0) { mesh_point(&c->my, t, i, jj[s], r, a1, a2); val[q] = vec_halo_value(c, u, v, r, a1); }
+                        else FA(u, t, i, jj[s]) = val[q];
+                    }
+                }
+                for (int j = 1; j <= N + 1; j++) {
+                    int ii[2] = {1 - d, N + d};
+                    for (int s = 0; s < 2; s++, q++) {
+                        if (pass == 0) { mesh_point(&c->my, t, ii[s], j, r, a1, a2); val[q] = vec_halo_value(c, u, v, r, a1); }
+                        else FA(u, t, ii[s], j) = val[q];
+                    }
+                }
+                /* v: columns beyond west / east, rows beyond south / north */
+                for (int j = 1; j <= N; j++) {
+                    int ii[2] = {1 - d, N + 1 + d};
+                    for (int s = 0; s < 2; s++, q++) {
+                        if (pass == 0) { mesh_point(&c->mx, t, ii[s], j, r, a1, a2); val[q] = vec_halo_value(c, u, v, r, a2); }
+                        else FA(v, t, ii[s], j) = val[q];
+                    }
+                }
+                for (int i = 1; i <= N + 1; i++) {
+                    int jj[2] = {1 - d, N + d};
+                    for (int s = 0; s < 2; s++, q++) {
+                        if (pass == 0) { mesh_point(&c->mx, t, i, jj[s], r, a1, a2); val[q] = vec_halo_value(c, u, v, r, a2); }
+                        else FA(v, t, i, jj[s]) = val[q];
+                    }
+                }
+            }
+    }
+    free(val);
+}
+
+/* calc_v_nabla_up4_tile (v_nabla_mod.f90:105-146) on nx x ny points of one panel */
+static void v_nabla_up4(fld_t *tend, const fld_t *f, const fld_t *ut, const fld_t *vt, int t, int nx, int ny, double hx,
+                        double scale)
+{
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            double a = FA(ut, t, i, j), b = FA(vt, t, i, j);
+            double zl = 0.5 + copysign(0.5, a), zr = 1.0 - zl;
+            double dx = (zl * (3.0 * FA(f, t, i + 1, j) + 10.0 * FA(f, t, i, j) - 18.0 * FA(f, t, i - 1, j) +
+                               6.0 * FA(f, t, i - 2, j) - FA(f, t, i - 3, j)) -
+                         zr * (3.0 * FA(f, t, i - 1, j) + 10.0 * FA(f, t, i, j) - 18.0 * FA(f, t, i + 1, j) +
+                               6.0 * FA(f, t, i + 2, j) - FA(f, t, i + 3, j))) /
+                        12.0;
+            zl = 0.5 + copysign(0.5, b);
+            zr = 1.0 - zl;
+            double dy = (zl * (3.0 * FA(f, t, i, j + 1) + 10.0 * FA(f, t, i, j) - 18.0 * FA(f, t, i, j - 1) +
+                               6.0 * FA(f, t, i, j - 2) - FA(f, t, i, j - 3)) -
+                         zr * (3.0 * FA(f, t, i, j - 1) + 10.0 * FA(f, t, i, j) - 18.0 * FA(f, t, i, j + 1) +
+                               6.0 * FA(f, t, i, j + 2) - FA(f, t, i, j + 3))) /
+                        12.0;
+            FA(tend, t, i, j) = -(a * dx + b * dy) / (hx * scale);
+        }
+}
+
+/* calculate_ecs_S (metric_2d_ecs_mod.f90:270-291): Christoffel symbols of the first kind */
+static void christoffel_S(double alpha, double beta, double S[3][2])
+{
+    double x = tan(alpha), y = tan(beta);
+    double x2 = x * x, y2 = y * y;
+    double sigma = 1.0 + x2 + y2;
+    double s3 = sigma * sigma * sigma;
+    S[0][0] = 2.0 * x * y2 * ((1.0 + x2) * (1.0 + x2)) * (1.0 + y2) / s3;
+    S[1][0] = -0.5 * y * (1.0 + y2) * (1.0 + x2) * (-(x2 * x2) + 3.0 * x2 * y2 + y2 + 1.0) / s3;
+    S[2][0] = x * (1.0 + x2) * ((1.0 + y2) * (1.0 + y2)) * (-x2 + y2 - 1.0) / s3;
+    S[0][1] = y * (1.0 + y2) * ((1.0 + x2) * (1.0 + x2)) * (-y2 + x2 - 1.0) / s3;
+    S[1][1] = -0.5 * x * (1.0 + x2) * (1.0 + y2) * (-(y2 * y2) + 3.0 * y2 * x2 + x2 + 1.0) / s3;
+    S[2][1] = 2.0 * y * x2 * ((1.0 + y2) * (1.0 + y2)) * (1.0 + x2) / s3;
+}
+
+/* add_cov_wind_advection (hor_Christofel_shallow_mod.f90:92-122,149-164), comp 0 = u, 1 = v */
+static void christoffel_add(fld_t *tend, const fld_t *ut, const fld_t *vt, const mesh_t *m, int t, int comp, double a)
+{
+    double scale = -a;
+    for (int j = 1; j <= m->ny; j++)
+        for (int i = 1; i <= m->nx; i++) {
+            double alpha = -0.25 * PI_ + (i - 1 + m->shift_i) * m->hx, beta = -0.25 * PI_ + (j - 1 + m->shift_j) * m->hy;
+            double S[3][2];
+            christoffel_S(alpha, beta, S);
+            double g11 = S[0][comp], g21 = S[1][comp], g22 = S[2][comp];
+            double uu = FA(ut, t, i, j), vv = FA(vt, t, i, j);
+            FA(tend, t, i, j) = FA(tend, t, i, j) - (uu * uu * g11 + 2.0 * uu * vv * g21 + vv * vv * g22) / scale;
+        }
+}
+
+/* calc_vec_advection (vector_advection_Ch_mod.f90:33-62) */
+static void op_vec_adv(orc_ctx *c, fld_t *utd, fld_t *vtd, fld_t *u, fld_t *v, fld_t *ut, fld_t *vt)
+{
+    int N = c->N;
+    /* interp2d_uv2pvec_Ch_sbp42: uh = I_c2i,x(ut), vh = I_c2i,y(vt) on xy */
+    exch_do(&c->ex_ch3_u, ut, vt);
+    exch_do(&c->ex_ch3_v, ut, vt);
+    for (int t = 0; t < NPAN; t++) {
+        interp_c2i(&c->uh, ut, t, 0, N + 1, 1, N + 1);
+        interp_c2i(&c->vh, vt, t, 1, N + 1, 1, N + 1);
+    }
+    /* interp2d_pvec2uv_Ch_sbp42 on (vh, uh): v_at_u = I_i2c,x(vh), u_at_v = I_i2c,y(uh)
+       (its xy exchange fills halos that the SBP interpolation does not read) */
+    for (int t = 0; t < NPAN; t++) {
+        interp_i2c(&c->vau, &c->vh, t, 0, N, 1, N + 1);
+        interp_i2c(&c->uav, &c->uh, t, 1, N, 1, N + 1);
+    }
+    /* u_halo = u, v_halo = v, then the ECS Ch vector halo of width 3 */
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) FA(&c->uhal, t, i, j) = FA(u, t, i, j);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) FA(&c->vhal, t, i, j) = FA(v, t, i, j);
+    }
+    ecs_vec_halo(c, &c->uhal, &c->vhal, 3);
+    for (int t = 0; t < NPAN; t++) {
+        v_nabla_up4(utd, &c->uhal, ut, &c->vau, t, N, N + 1, c->my.hx, c->a);
+        v_nabla_up4(vtd, &c->vhal, &c->uav, vt, t, N + 1, N, c->mx.hx, c->a);
+        christoffel_add(utd, ut, &c->vau, &c->my, t, 0, c->a);
+        christoffel_add(vtd, &c->uav, vt, &c->mx, t, 1, c->a);
+    }
+    /* CH_uv_exchange ('cross', width 1) and sync_ch_cov (vector_advection_Ch_mod.f90:73-115) */
+    exch_do(&c->ex_ch1c_u, utd, vtd);
+    exch_do(&c->ex_ch1c_v, utd, vtd);
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N; j++) FA(vtd, t, 1, j) = 0.5 * (FA(vtd, t, 1, j) + FA(vtd, t, 0, j));
+        for (int j = 1; j <= N; j++) FA(vtd, t, N + 1, j) = 0.5 * (FA(vtd, t, N + 2, j) + FA(vtd, t, N + 1, j));
+        for (int i = 1; i <= N; i++) FA(utd, t, i, 1) = 0.5 * (FA(utd, t, i, 1) + FA(utd, t, i, 0));
+        for (int i = 1; i <= N; i++) FA(utd, t, i, N + 1) = 0.5 * (FA(utd, t, i, N + 2) + FA(utd, t, i, N + 1));
+    }
+}
+
+/* operator_adv_swm_t%apply, covariant branch (operator_adv_swm_mod.f90:62-96); no orography */
+static void op_apply_nl(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
+{
+    int N = c->N;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N + 1; i++) FA(&c->htot, t, i, j) = 1.0 * FA(h, t, i, j) + 1.0 * 0.0;
+    op_co2contra(c, &c->ut, &c->vt, u, v);
+    op_massflux_up4(c, &c->hu, &c->hv, h, &c->ut, &c->vt);
+    op_div(c, &c->div, &c->hu, &c->hv);
+    op_grad(c, &c->gx, &c->gy, &c->htot);
+    op_coriolis(c, &c->cu, &c->cv, &c->ut, &c->vt);
+    op_vec_adv(c, du, dv, u, v, &c->ut, &c->vt);
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++)
+                FA(du, t, i, j) = FA(du, t, i, j) + (-c->g) * FA(&c->gx, t, i, j) + 1.0 * FA(&c->cu, t, i, j);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++)
+                FA(dv, t, i, j) = FA(dv, t, i, j) + (-c->g) * FA(&c->gy, t, i, j) + 1.0 * FA(&c->cv, t, i, j);
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N + 1; i++) FA(dh, t, i, j) = -1.0 * FA(&c->div, t, i, j);
+    }
+}
+
+static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
+{
+    if (c->nonlinear) op_apply_nl(c, dh, du, dv, h, u, v);
+    else op_apply_lin(c, dh, du, dv, h, u, v);
 }
 
 /* stvec assign/update over interior points (grid_field_mod.f90:442-534) */
@@ -1031,6 +1443,9 @@ static void store_state(orc_ctx *c, double *h, double *u, double *v)
 }
 
 int orc_N(const orc_ctx *c) { return c->N; }
+
+/* operator kind: 0 linear_swm_operator, 1 advective_swm_operator (covariant Ch) */
+void orc_set_operator(orc_ctx *c, int kind) { c->nonlinear = kind == 1; }
 
 void orc_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv)
 {
