@@ -15,6 +15,7 @@ SWE_OK = 0
 SWE_FP64 = 0
 SWE_FP32 = 1
 SWE_OP_LINEAR = 0
+SWE_OP_ADVECTIVE = 1
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "no CUDA device",
           -5: "cube size above SWE_NOALLOC_MAX_N"}

@@ -191,6 +191,14 @@ struct DevMetric {
     MetricView<T> v{};
 };
 
+// Static tables of the advective operator on the device.
+template <class T>
+struct DevAdv {
+    T *base = nullptr;
+    int *ibase = nullptr;
+    AdvView<T> v{};
+};
+
 struct swe_ctx {
     swe_cfg cfg{};
     Dims dims{};
@@ -221,6 +229,15 @@ struct swe_ctx {
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
+    // advective operator (cfg.operator_kind == SWE_OP_ADVECTIVE)
+    bool adv = false;
+    DevAdv<double> a64;
+    DevAdv<float> a32;
+    void *fl = nullptr, *adt = nullptr, *ph = nullptr;   // mass flux, advective tendencies, uh/vh (state boxes)
+    void *fs = nullptr;              // mass-flux edge strips
+    void *vh = nullptr;              // covariant wind at the virtual points beyond the panel edges
+    void *hb = nullptr;              // panel-boundary h before the in-place averaging
+    double *ones = nullptr;          // per-member depth factor 1 (dh = -div F)
 };
 
 struct swe_stvec {
@@ -257,12 +274,17 @@ static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
 // Default before autotuning: tiles of about 24 points for the smaller cubes.
 static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
+static void cube_edges(int out[12][2]);
+
 static int upload_tables(swe_ctx *c)
 {
     if (c->device >= 0 && c->device < 64 && g_tables_ready[c->device]) return SWE_OK;
     Link L[NPAN][4];
     compute_links(L);
     CU(c, cudaMemcpyToSymbol(c_link, L, sizeof(L)));
+    int ce[12][2];
+    cube_edges(ce);
+    CU(c, cudaMemcpyToSymbol(c_cube_edge, ce, sizeof(ce)));
     if (c->device >= 0 && c->device < 64) g_tables_ready[c->device] = true;
     return SWE_OK;
 }
@@ -336,6 +358,229 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
     return SWE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// advective operator: static tables, FP64 on the host (same expressions as the
+// reference's setup code), stored in the context's precision
+// ---------------------------------------------------------------------------
+static void p2r(int p, const double rp[3], double r[3])
+{
+    for (int d = 0; d < 3; d++) r[d] = EX[p][d] * rp[0] + EY[p][d] * rp[1] - NRM[p][d] * rp[2];
+}
+
+struct MeshGeom {
+    int nx, ny;
+    double shi, shj, hx, hy;
+};
+static MeshGeom mesh_geom(int N, double shi, double shj)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    MeshGeom g;
+    g.nx = shi == 0.0 ? N + 1 : N;
+    g.ny = shj == 0.0 ? N + 1 : N;
+    g.shi = shi;
+    g.shj = shj;
+    const double a0 = -0.25 * pi, a1 = 0.25 * pi;
+    g.hx = (a1 - a0) / ((double)g.nx - 1 + 2.0 * shi);
+    g.hy = (a1 - a0) / ((double)g.ny - 1 + 2.0 * shj);
+    return g;
+}
+static void mesh_ab(const MeshGeom &g, int i, int j, double &alpha, double &beta)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    alpha = -0.25 * pi + (i - 1 + g.shi) * g.hx;
+    beta = -0.25 * pi + (j - 1 + g.shj) * g.hy;
+}
+
+// Position and covariant basis of a mesh point at any index (set_curvilinear_mesh,
+// metric_2d_ecs_mod.f90:338-411).
+static void mesh_point(const MeshGeom &g, int p, int i, int j, double r[3], double a1[3], double a2[3])
+{
+    double alpha, beta;
+    mesh_ab(g, i, j, alpha, beta);
+    const double ta = std::tan(alpha), tb = std::tan(beta);
+    const double sigm = std::sqrt(1.0 + ta * ta + tb * tb);
+    const double rp[3] = {ta / sigm, tb / sigm, 1.0 / sigm};
+    p2r(p, rp, r);
+    double q[3];
+    a1p(alpha, beta, q);
+    p2r(p, q, a1);
+    a2p(alpha, beta, q);
+    p2r(p, q, a2);
+}
+
+// transform_cartesian_to_native_ecs (metric_2d_ecs_mod.f90:310-335)
+static void cart_to_native(const double r[3], int &panel, double &alpha, double &beta)
+{
+    int p = 0;
+    double best = 0.0;
+    for (int q = 0; q < NPAN; q++) {
+        const double d = -(r[0] * NRM[q][0] + r[1] * NRM[q][1] + r[2] * NRM[q][2]);
+        if (d > best) { p = q; best = d; }
+    }
+    panel = p;
+    alpha = std::atan((EX[p][0] * r[0] + EX[p][1] * r[1] + EX[p][2] * r[2]) / best);
+    beta = std::atan((EY[p][0] * r[0] + EY[p][1] * r[1] + EY[p][2] * r[2]) / best);
+}
+
+// bicubic_interp_t%calc_w (bicubic_interp_mod.f90:27-84)
+static void bicubic_w(const MeshGeom &g, double alpha, double beta, int &ix, int &iy, double wx[4], double wy[4])
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    double dx = (alpha - (-0.25 * pi)) / g.hx + 1 - g.shi;
+    double dy = (beta - (-0.25 * pi)) / g.hy + 1 - g.shj;
+    ix = std::min(std::max(2, (int)dx), g.nx - 2);
+    iy = std::min(std::max(2, (int)dy), g.ny - 2);
+    dx = dx - ix;
+    dy = dy - iy;
+    double p1 = dx + 1.0, p2 = dx, p3 = dx - 1.0, p4 = dx - 2.0;
+    wx[0] = -p2 * p3 * p4 / 6.0; wx[1] = p1 * p3 * p4 / 2.0; wx[2] = -p1 * p2 * p4 / 2.0; wx[3] = p1 * p2 * p3 / 6.0;
+    p1 = dy + 1.0; p2 = dy; p3 = dy - 1.0; p4 = dy - 2.0;
+    wy[0] = -p2 * p3 * p4 / 6.0; wy[1] = p1 * p3 * p4 / 2.0; wy[2] = -p1 * p2 * p4 / 2.0; wy[3] = p1 * p2 * p3 / 6.0;
+}
+
+// init_halo_xy_interp (ecs_halo_factory_mod.f90:236-270): target index i at halo row j
+static void halo_xy_weights(int n, double dxa, int i, int j, double w[4], int &ind)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    const double zb = 0.25 * pi + j * dxa;
+    double za = -0.25 * pi + (i - 1.0) * dxa;
+    double zx = std::tan(za);
+    const double zz = std::tan(zb);
+    zx = zx / zz;
+    za = std::atan(zx);
+    int k = (int)std::floor((za + 0.25 * pi) / dxa) + 1;
+    k = std::min(std::max(2, k), n - 2);
+    const double zxi = (za + 0.25 * pi) / dxa - (k - 1.0);
+    w[0] = -(zxi * (zxi - 1.0) * (zxi - 2.0) / 6.0);
+    w[1] = (zxi + 1.0) * (zxi - 1.0) * (zxi - 2.0) / 2.0;
+    w[2] = -((zxi + 1.0) * zxi * (zxi - 2.0) / 2.0);
+    w[3] = (zxi + 1.0) * zxi * (zxi - 1.0) / 6.0;
+    ind = k;
+}
+
+// calculate_ecs_S (metric_2d_ecs_mod.f90:270-291)
+static void christoffel_S(double alpha, double beta, double S[3][2])
+{
+    const double x = std::tan(alpha), y = std::tan(beta);
+    const double x2 = x * x, y2 = y * y;
+    const double sigma = 1.0 + x2 + y2;
+    const double s3 = sigma * sigma * sigma;
+    S[0][0] = 2.0 * x * y2 * ((1.0 + x2) * (1.0 + x2)) * (1.0 + y2) / s3;
+    S[1][0] = -0.5 * y * (1.0 + y2) * (1.0 + x2) * (-(x2 * x2) + 3.0 * x2 * y2 + y2 + 1.0) / s3;
+    S[2][0] = x * (1.0 + x2) * ((1.0 + y2) * (1.0 + y2)) * (-x2 + y2 - 1.0) / s3;
+    S[0][1] = y * (1.0 + y2) * ((1.0 + x2) * (1.0 + x2)) * (-y2 + x2 - 1.0) / s3;
+    S[1][1] = -0.5 * x * (1.0 + x2) * (1.0 + y2) * (-(y2 * y2) + 3.0 * y2 * x2 + x2 + 1.0) / s3;
+    S[2][1] = 2.0 * y * x2 * ((1.0 + y2) * (1.0 + y2)) * (1.0 + x2) / s3;
+}
+
+// One virtual point of the covariant vector halo (ecs_halo_vec_Ch_factory_mod.f90:21-270):
+// source panel, bicubic stencils on its y (u) and x (v) meshes, projections a.b1, a.b2.
+static void vec_halo_entry(int N, const MeshGeom &gm, int t, int i, int j, bool comp_u, int &src, int ix[4], double w[18])
+{
+    double r[3], a1[3], a2[3], al, be, bp[3], b1[3], b2[3];
+    mesh_point(gm, t, i, j, r, a1, a2);
+    const double *a = comp_u ? a1 : a2;
+    cart_to_native(r, src, al, be);
+    bicubic_w(mesh_geom(N, 0.5, 0.0), al, be, ix[0], ix[1], w, w + 4);
+    bicubic_w(mesh_geom(N, 0.0, 0.5), al, be, ix[2], ix[3], w + 8, w + 12);
+    b1p(al, be, bp);
+    p2r(src, bp, b1);
+    b2p(al, be, bp);
+    p2r(src, bp, b2);
+    w[16] = a[0] * b1[0] + a[1] * b1[1] + a[2] * b1[2];
+    w[17] = a[0] * b2[0] + a[1] * b2[1] + a[2] * b2[2];
+}
+
+template <class T>
+static int build_adv_tables(swe_ctx *c, DevAdv<T> &da)
+{
+    const int N = c->cfg.N, n = N + 1, P = c->dims.P, hp = vh_points(N);
+    const size_t box = (size_t)c->dims.ps;
+    // layout: xyw [2][n][4] | hw [6][hp][18] | S [6 boxes]
+    const size_t o_hw = 8 * (size_t)n, o_S = o_hw + (size_t)NPAN * hp * 18, n_el = o_S + 6 * box;
+    // ints: xyind [2][n] | hsrc [6][hp] | hidx [6][hp][4]
+    const size_t i_src = 2 * (size_t)n, i_idx = i_src + (size_t)NPAN * hp, n_int = i_idx + (size_t)NPAN * hp * 4;
+    std::vector<T> h(n_el, T(0));
+    std::vector<int> hi(n_int, 0);
+    const MeshGeom gxy = mesh_geom(N, 0.0, 0.0), gy = mesh_geom(N, 0.5, 0.0), gx = mesh_geom(N, 0.0, 0.5);
+    for (int d = 1; d <= 2; d++)
+        for (int a = 1; a <= n; a++) {
+            double w[4];
+            int ind;
+            halo_xy_weights(n, gxy.hx, a, d, w, ind);
+            for (int k = 0; k < 4; k++) h[((size_t)(d - 1) * n + (a - 1)) * 4 + k] = T(w[k]);
+            hi[(size_t)(d - 1) * n + (a - 1)] = ind;
+        }
+    for (int t = 0; t < NPAN; t++) {
+        auto put = [&](int k, const MeshGeom &g, int i, int j, bool cu) {
+            int src, ix[4];
+            double w[18];
+            vec_halo_entry(N, g, t, i, j, cu, src, ix, w);
+            const size_t q = (size_t)t * hp + k;
+            hi[i_src + q] = src;
+            for (int e = 0; e < 4; e++) hi[i_idx + 4 * q + e] = ix[e];
+            for (int e = 0; e < 18; e++) h[o_hw + 18 * q + e] = T(w[e]);
+        };
+        for (int d = 1; d <= 3; d++) {
+            for (int i = 1; i <= N; i++) {
+                put(vh_u_s(N) + (d - 1) * N + (i - 1), gy, i, 1 - d, true);
+                put(vh_u_n(N) + (d - 1) * N + (i - 1), gy, i, N + 1 + d, true);
+            }
+            for (int j = 1; j <= N + 1; j++) {
+                put(vh_u_w(N) + (d - 1) * (N + 1) + (j - 1), gy, 1 - d, j, true);
+                put(vh_u_e(N) + (d - 1) * (N + 1) + (j - 1), gy, N + d, j, true);
+            }
+            for (int j = 1; j <= N; j++) {
+                put(vh_v_w(N) + (d - 1) * N + (j - 1), gx, 1 - d, j, false);
+                put(vh_v_e(N) + (d - 1) * N + (j - 1), gx, N + 1 + d, j, false);
+            }
+            for (int i = 1; i <= N + 1; i++) {
+                put(vh_v_s(N) + (d - 1) * (N + 1) + (i - 1), gx, i, 1 - d, false);
+                put(vh_v_n(N) + (d - 1) * (N + 1) + (i - 1), gx, i, N + d, false);
+            }
+        }
+    }
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N; i++) {
+            double al, be, S[3][2];
+            mesh_ab(gy, i, j, al, be);
+            christoffel_S(al, be, S);
+            for (int k = 0; k < 3; k++) h[o_S + k * box + box_off(P, i, j)] = T(S[k][0]);
+        }
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            double al, be, S[3][2];
+            mesh_ab(gx, i, j, al, be);
+            christoffel_S(al, be, S);
+            for (int k = 0; k < 3; k++) h[o_S + (3 + k) * box + box_off(P, i, j)] = T(S[k][1]);
+        }
+    if (cudaMalloc(&da.base, n_el * sizeof(T)) != cudaSuccess || cudaMalloc(&da.ibase, n_int * sizeof(int)) != cudaSuccess)
+        return fail(c, SWE_ENOMEM, "advective tables allocation failed");
+    CU(c, cudaMemcpy(da.base, h.data(), n_el * sizeof(T), cudaMemcpyHostToDevice));
+    CU(c, cudaMemcpy(da.ibase, hi.data(), n_int * sizeof(int), cudaMemcpyHostToDevice));
+    AdvView<T> &v = da.v;
+    v.xyw = da.base;
+    v.hw = da.base + o_hw;
+    v.S = da.base + o_S;
+    v.xyind = da.ibase;
+    v.hsrc = da.ibase + i_src;
+    v.hidx = da.ibase + i_idx;
+    v.neg_radius = T(-c->cfg.radius);
+    v.hp = hp;
+    return SWE_OK;
+}
+
+// Cube edges as (panel, side) with (panel*4 + side) below the neighbour's.
+static void cube_edges(int out[12][2])
+{
+    Link L[NPAN][4];
+    compute_links(L);
+    int k = 0;
+    for (int p = 0; p < NPAN; p++)
+        for (int s = 0; s < 4; s++)
+            if (p * 4 + s < L[p][s].nb * 4 + L[p][s].nside && k < 12) { out[k][0] = p; out[k][1] = s; k++; }
+}
+
 // SBP quadrature weights J hx hy Ax Ay (quadrature_factory_mod.f90:89-188) for xy, y, x meshes.
 static int build_quadrature(swe_ctx *c)
 {
@@ -394,6 +639,8 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
     cudaFree(c->qw); cudaFree(c->red);
+    cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
+    cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -414,7 +661,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (!cfg || !out) return SWE_EINVAL;
     *out = nullptr;
     if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
-        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
+        (cfg->operator_kind != SWE_OP_LINEAR && cfg->operator_kind != SWE_OP_ADVECTIVE) || !(cfg->radius > 0.0))
         return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
@@ -456,6 +703,24 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
         const size_t sb = (size_t)strip_member(N, cfg->n_members) * c->elem;
         if (cudaMalloc(&c->es, sb) != cudaSuccess) return bail(SWE_ENOMEM);
         if (cudaMemset(c->es, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
+        if (cfg->operator_kind == SWE_OP_ADVECTIVE) {
+            c->adv = true;
+            if ((rc = alloc_box(c, &c->fl)) || (rc = alloc_box(c, &c->adt)) || (rc = alloc_box(c, &c->ph))) return bail(rc);
+            if (cudaMalloc(&c->fs, sb) != cudaSuccess) return bail(SWE_ENOMEM);
+            if (cudaMemset(c->fs, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
+            const size_t vb = (size_t)cfg->n_members * NPAN * vh_points(N) * c->elem;
+            if (cudaMalloc(&c->vh, vb) != cudaSuccess) return bail(SWE_ENOMEM);
+            if (cudaMemset(c->vh, 0, vb) != cudaSuccess) return bail(SWE_ECUDA);
+            const size_t hbb = (size_t)cfg->n_members * NPAN * 4 * (N + 1) * c->elem;
+            if (cudaMalloc(&c->hb, hbb) != cudaSuccess) return bail(SWE_ENOMEM);
+            if (cudaMemset(c->hb, 0, hbb) != cudaSuccess) return bail(SWE_ECUDA);
+            std::vector<double> one(cfg->n_members, 1.0);
+            if (cudaMalloc(&c->ones, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
+            if (cudaMemcpy(c->ones, one.data(), sizeof(double) * cfg->n_members, cudaMemcpyHostToDevice) != cudaSuccess)
+                return bail(SWE_ECUDA);
+            rc = cfg->precision == SWE_FP64 ? build_adv_tables<double>(c, c->a64) : build_adv_tables<float>(c, c->a32);
+            if (rc != SWE_OK) return bail(rc);
+        }
     }
     if (cudaHostAlloc((void **)&c->pinned, c->box_elems * c->elem, cudaHostAllocDefault) != cudaSuccess)
         return bail(SWE_ENOMEM);
@@ -773,6 +1038,10 @@ static void launch_stage(int tm, int members, const T *y, const T *w, const T *e
 static dim3 edge_grid(int N, int members) { return dim3((N + 1 + EDGE_CHUNK - 1) / EDGE_CHUNK, NPAN * 4, members); }
 static dim3 edge_grid(const swe_ctx *c) { return edge_grid(c->cfg.N, c->cfg.n_members); }
 
+template <class T> static const AdvView<T> &adv_view(const swe_ctx *c);
+template <> const AdvView<double> &adv_view<double>(const swe_ctx *c) { return c->a64.v; }
+template <> const AdvView<float> &adv_view<float>(const swe_ctx *c) { return c->a32.v; }
+
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const double *dtm,
@@ -780,12 +1049,34 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
 {
     const int M = c->cfg.n_members;
     launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv,
-             dtm);
-    StageArgs a{mode, dt, c->Hm, dtm};
-    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp,
-                    c->dims, mv, a, c->stream);
-    c->launches += 3;
+    if (!c->adv) {
+        launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+                 (T *)c->edge, c->dims, mv, dtm);
+        StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
+        launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+                        (T *)cmp, c->dims, mv, a, c->stream);
+        c->launches += 3;
+        return;
+    }
+    // advective operator (operator_adv_swm_mod.f90:81-96); the averaging of the
+    // duplicated h vertices acts on the stage input in place, as in the reference
+    const AdvView<T> &av = adv_view<T>(c);
+    const int N = c->cfg.N, n = N + 1;
+    const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
+    launch_k(k_havg<T>, dim3(M), dim3(256), 0, c->stream, (T *)yin, (T *)c->hb, c->dims, dtm);
+    launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
+             (T *)c->edge, c->dims, mv, dtm);
+    launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
+    const long long nvh = (long long)NPAN * av.hp * M;
+    launch_k(k_vhalo<T>, dim3((unsigned)((nvh + 255) / 256)), dim3(256), 0, c->stream, (const T *)yin, (T *)c->vh,
+             c->dims, av, M, dtm);
+    launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
+             (T *)c->adt, c->dims, av, mv, dtm);
+    StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
+    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+                    (T *)cmp, c->dims, mv, a, c->stream);
+    c->launches += 8;
 }
 
 static void enqueue_apply(swe_ctx *c, void *out, const void *in)
@@ -998,10 +1289,10 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
     cudaEventRecord(e0, c->stream);
     launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (T *)c->edge, c->dims, mv,
-             (const double *)nullptr);
+    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+             (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
-    StageArgs a{mode, dt, c->Hm, nullptr};
+    StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
     launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
                     c->dims, mv, a, c->stream);
@@ -1013,6 +1304,7 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
                                 double *ms_stage)
 {
     if (!c || !v0 || v0->ctx != c || nreps < 1) return SWE_EINVAL;
+    if (c->adv) return fail(c, SWE_EINVAL, "swe_kernel_times times the linear operator's three kernels");
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     const int nst = 4 * nreps;
@@ -1253,9 +1545,9 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
     launch_co2contra<double>(33, 1, vin, W, ES, dm, mv, st);
-    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, E, dm, mv,
-             (const double *)nullptr);
-    StageArgs a{0, 0.0, Hp, nullptr};
+    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
+             mv, (const double *)nullptr);
+    StageArgs a{0, 0.0, Hp, nullptr, nullptr, nullptr, nullptr};
     launch_stage<double>(33, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;

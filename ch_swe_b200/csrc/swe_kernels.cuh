@@ -221,15 +221,18 @@ constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the th
 // the copies from shared memory.  Copies are stored by direction (x-neighbour
 // across L/R, y-neighbour across B/T).
 template <class T>
-__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, T *__restrict__ E, Dims d,
-                                                        MetricView<T> m, const double *__restrict__ dtm)
+__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, const T *__restrict__ ESd,
+                                                        T *__restrict__ E, Dims d, MetricView<T> m,
+                                                        const double *__restrict__ dtm)
 {
     __shared__ T raw[3][4][EDGE_CHUNK];   // [own, x-neighbour, y-neighbour][quantity][vertex]
     const int N = d.N, n = N + 1;
     const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
     const int a0 = 1 + (blockIdx.x * n) / gridDim.x, a1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
     if (member_frozen(dtm, mem)) return;
-    const Strips<T> S{ES + strip_member(N, mem), n};
+    // Coriolis parts (q 0, 1) from the ut/vt strips, divergence parts (q 2, 3) from
+    // the strips of the field whose divergence is taken (ut/vt, or the mass flux)
+    const Strips<T> Sc{ES + strip_member(N, mem), n}, Sd{ESd + strip_member(N, mem), n};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
     pdl_trigger();
@@ -237,6 +240,7 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
     if (warp < 8) {
         const int a = a0 + lane, q = warp & 3;
         if (a < a1) {
+            const Strips<T> &S = q < 2 ? Sc : Sd;
             if (warp < 4) {
                 raw[0][q][lane] = edge_raw(S, m, t, s, a, q);
             } else {
@@ -252,7 +256,7 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
             side_vertex(N, s, a, 0, k, l);
             const int s2 = xs ? (l == 1 ? SIDE_B : SIDE_T) : (k == 1 ? SIDE_L : SIDE_R);
             const Link L2 = c_link[t][s2];
-            raw[xs ? 2 : 1][q][a - a0] = edge_raw(S, m, L2.nb, L2.nside, nb_along(L2, n, along(s2, k, l)), q);
+            raw[xs ? 2 : 1][q][a - a0] = edge_raw(q < 2 ? Sc : Sd, m, L2.nb, L2.nside, nb_along(L2, n, along(s2, k, l)), q);
         }
     }
     __syncthreads();
@@ -317,6 +321,11 @@ struct StageArgs {
     double dt;
     const double *Hm;  // per-member mean depth
     const double *dtm; // per-member time step (null: dt for all); 0 freezes a member
+    // advective operator only (null for the linear one): the mass flux (fields 1, 2
+    // of a state box) whose divergence gives dh, and the advective wind tendencies
+    const void *F;
+    const void *A;
+    const void *HB;    // panel-boundary h before the in-place averaging (the gradient's input)
 };
 
 // Kahan-compensated state update for FP32 (s += inc with compensation c).

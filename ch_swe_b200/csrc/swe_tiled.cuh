@@ -20,6 +20,7 @@
 #pragma once
 
 #include "swe_kernels.cuh"
+#include "swe_advective.cuh"
 
 namespace chswe {
 
@@ -317,7 +318,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     {
         const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0);
         const T *gh = yp + oh, *gu = wp + d.fs + ou, *gjy = m.Jy + ou;
-        T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN];
+        // the field whose divergence is taken: ut, or the mass flux of the advective operator
+        const T *gf = a.F ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
+        T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN], rfu[IT_WIN];
+        const T *hpre = (const T *)a.HB;
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
@@ -325,9 +329,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             split(q, w5, iw5, r, c);
             const bool ok = q < w5 * h5;
             const int go = r * P + c;
+            const bool jr = ok && r >= 2 && r < th + 2;
             rh[it] = ok ? __ldg(gh + go) : T(0);
+            if (hpre && ok) {
+                // advective operator: the gradient reads h as it was before the averaging
+                const int hi = sh.x0 + c, hj = sh.y0 + r;
+                if (hi >= 1 && hi <= n && hj >= 1 && hj <= n && (hi == 1 || hi == n || hj == 1 || hj == n))
+                    rh[it] = __ldg(hpre + (hi == 1 || hi == n ? hb_index(N, mem, t, hi == 1 ? SIDE_L : SIDE_R, hj)
+                                                           : hb_index(N, mem, t, hj == 1 ? SIDE_B : SIDE_T, hi)));
+            }
             ru[it] = ok ? __ldg(gu + go) : T(0);
-            rjy[it] = ok && r >= 2 && r < th + 2 ? __ldg(gjy + go) : T(0);
+            rjy[it] = jr ? __ldg(gjy + go) : T(0);
+            rfu[it] = gf && jr ? __ldg(gf + go) : ru[it];
         }
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
@@ -337,7 +350,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             if (q < w5 * h5) {
                 sh.a[r * PW + c] = rh[it];
                 sut.a[r * PW + c] = ru[it];
-                if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] = rjy[it] * ru[it];
+                if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] = rjy[it] * rfu[it];
             }
         }
     }
@@ -347,7 +360,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     {
         const int64_t ov = box_off(P, svt.x0, svt.y0);
         const T *gv = wp + 2 * d.fs + ov, *gjx = m.Jx + ov;
-        T rv[IT_WIN], rjx[IT_WIN];
+        const T *gf = a.F ? (const T *)a.F + mo + t * d.ps + 2 * d.fs + ov : nullptr;
+        T rv[IT_WIN], rjx[IT_WIN], rfv[IT_WIN];
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
@@ -355,18 +369,26 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             split(q, w5, iw5, r, c);
             const bool ok = q < w5 * h5;
             const int go = r * P + c;
+            const bool jc = ok && c >= 2 && c < tw + 2;
             rv[it] = ok ? __ldg(gv + go) : T(0);
-            rjx[it] = ok && c >= 2 && c < tw + 2 ? __ldg(gjx + go) : T(0);
+            rjx[it] = jc ? __ldg(gjx + go) : T(0);
+            rfv[it] = gf && jc ? __ldg(gf + go) : rv[it];
         }
         T hx0 = 0, hx1 = 0, hy0 = 0, hy1 = 0;
         const int q = threadIdx.x;
+        const T *hpre = (const T *)a.HB;
+        auto halo = [&](int s, int along) {
+            if (!hpre) return h_halo(y, d, t, s, along);
+            const Link L = c_link[t][s];
+            return __ldg(hpre + hb_index(N, mem, L.nb, L.nside, nb_along(L, n, along)));
+        };
         if (q < th) {
-            if (sat_l) hx0 = h_halo(y, d, t, SIDE_L, j0 + q);
-            if (sat_r) hx1 = h_halo(y, d, t, SIDE_R, j0 + q);
+            if (sat_l) hx0 = halo(SIDE_L, j0 + q);
+            if (sat_r) hx1 = halo(SIDE_R, j0 + q);
         }
         if (q < tw) {
-            if (sat_b) hy0 = h_halo(y, d, t, SIDE_B, i0 + q);
-            if (sat_t) hy1 = h_halo(y, d, t, SIDE_T, i0 + q);
+            if (sat_b) hy0 = halo(SIDE_B, i0 + q);
+            if (sat_t) hy1 = halo(SIDE_T, i0 + q);
         }
 #pragma unroll
         for (int it = 0; it < IT_STRIP; it++) {
@@ -391,7 +413,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             split(qq, w5, iw5, r, c);
             if (qq < w5 * h5) {
                 svt.a[r * PW + c] = rv[it];
-                if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] = rjx[it] * rv[it];
+                if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] = rjx[it] * rfv[it];
             }
         }
         if (q < th) { hl[q] = hx0; hr[q] = hx1; }
@@ -500,7 +522,17 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             dvg = (sdx.at(i, j) * m.inv_hx + dy * m.inv_hx) * mja[it];
         }
         kh[it] = -H * dvg;
-        if (i <= N) ku[it] = skx.at(i, j) + scx.at(i, j) * mjy[it];
+        const T *Aa = (const T *)a.A;
+        if (i <= N) {
+            if (Aa) {
+                // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
+                T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
+                if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
+                ku[it] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it];
+            } else {
+                ku[it] = skx.at(i, j) + scx.at(i, j) * mjy[it];
+            }
+        }
         if (j <= N) {
             const Line<T> hcol = sh.col(i);
             T gy = di2c_u<T>(j, N, hcol);
@@ -513,7 +545,13 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
                 gy += sat * (ht[c] - hcol(n));
             }
             gy = gy * m.inv_hxa;
-            kv[it] = -m.grav * gy + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
+            if (Aa) {
+                T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
+                if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
+                kv[it] = (av + -m.grav * gy) + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
+            } else {
+                kv[it] = -m.grav * gy + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
+            }
         }
     }
 

@@ -38,6 +38,10 @@ LINEAR_CH42_NAMES = {
     "co2contra_op_name": "co2contra_ch_sbp42",
     "quadrature_name": "SBP_C42_quadrature",
 }
+# advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4)
+ADVECTIVE_CH42_NAMES = dict(LINEAR_CH42_NAMES, vector_advection_op_name="vector_advection_Ch_up4_cov",
+                            massflux_op_name="massflux_ch_up4")
+OPERATORS = {"linear": _lib.SWE_OP_LINEAR, "advective": _lib.SWE_OP_ADVECTIVE}
 
 
 def state_shapes(N: int, members: int | None = None):
@@ -61,6 +65,7 @@ class Domain:
     grav: float = EARTH_GRAV
     h_mean: float = 1000.0
     horizontal_staggering: str = "Ch"
+    operator: str = "linear"          # the operator the context runs: 'linear' or 'advective'
     _ctx: int = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -68,6 +73,8 @@ class Domain:
             raise ValueError("domain_factory_mod, unsupported horizontal staggering: " + self.horizontal_staggering)
         if self.precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
+        if self.operator not in OPERATORS:
+            raise ValueError(f"operator must be one of {sorted(OPERATORS)}")
         L = _lib.load()
         cfg = SweCfg()
         check(L.swe_cfg_default(ctypes.byref(cfg)))
@@ -81,6 +88,7 @@ class Domain:
             cfg.rotation_axis[d] = float(self.rotation_axis[d])
         cfg.coriolis_constant = int(bool(self.coriolis_constant))
         cfg.h_mean = float(self.h_mean)
+        cfg.operator_kind = OPERATORS[self.operator]
         ctx = ctypes.c_void_p()
         check(L.swe_ctx_create(ctypes.byref(cfg), ctypes.byref(ctx)), None, "swe_ctx_create")
         self._ctx = ctx.value
@@ -262,18 +270,45 @@ class OperatorSwmLin:
 
 
 def create_swm_operator(grav: float, config: dict, domain: Domain, orography_generator=None):
+    """operator_swm_factory_mod.f90:33-55: 'linear_swm_operator' or 'advective_swm_operator'
+    (covariant Ch, up4 mass flux and vector advection).  The operator kind is fixed
+    when the domain's device context is created (create_domain(..., operator=...))."""
     kind = config.get("swm_operator_type")
-    if kind != "linear_swm_operator":
+    if kind == "linear_swm_operator":
+        if "h_mean" not in config:
+            raise ValueError("linear_swm_operator requires h_mean")
+        names, want_op = LINEAR_CH42_NAMES, "linear"
+    elif kind == "advective_swm_operator":
+        if config.get("v_components_type", "covariant") != "covariant":
+            raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
+        if orography_generator is not None:
+            raise ValueError("advective_swm_operator: orography is not supported")
+        names, want_op = ADVECTIVE_CH42_NAMES, "advective"
+    else:
         raise ValueError(f"unknown swm_op_type: {kind}")
-    if "h_mean" not in config:
-        raise ValueError("linear_swm_operator requires h_mean")
-    for key, want in LINEAR_CH42_NAMES.items():
+    for key, want in names.items():
         got = config.get(key, want)
         if got != want:
             raise ValueError(f"unsupported {key}: {got} (this build implements {want})")
+    if domain.operator != want_op:
+        raise ValueError(f"{kind} needs a domain created with operator='{want_op}' (got '{domain.operator}')")
     if abs(float(grav) - domain.grav) > 0.0:
         raise ValueError(f"grav {grav} differs from the domain's {domain.grav}")
+    if want_op == "advective":
+        return OperatorSwmAdv(domain, grav)
     return OperatorSwmLin(domain, config["h_mean"], grav)
+
+
+class OperatorSwmAdv(OperatorSwmLin):
+    """operator_adv_swm_t, covariant Ch branch: h is the full depth (no mean depth)."""
+
+    def __init__(self, domain: Domain, grav: float):
+        self.domain = domain
+        self.h_mean = None
+        self.grav = float(grav)
+
+    def set_member_h_mean(self, member: int, h_mean: float):
+        raise ValueError("the advective operator has no mean depth")
 
 
 class Rk4:

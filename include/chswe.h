@@ -55,6 +55,9 @@ extern "C" {
 #define SWE_FP32 1
 
 #define SWE_OP_LINEAR 0   /* operator_swm_lin_t, Ch staggering, SBP 4-2 */
+#define SWE_OP_ADVECTIVE 1 /* operator_adv_swm_t, covariant Ch branch (massflux_ch_up4,
+                              vector_advection_Ch_up4_cov; operator_adv_swm_mod.f90:62-96);
+                              h is the full depth, h_mean is not used, no orography */
 
 typedef struct swe_ctx swe_ctx;
 typedef struct swe_stvec swe_stvec;

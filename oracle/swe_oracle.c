@@ -1611,10 +1611,12 @@ void orc_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int
         exch_do(&c->ex_xy1_cross_v, &a, &b);
         ring_out(&a, w, out); ring_out(&b, w, out2); fld_free(&a); fld_free(&b);
     } else {
+        /* kind 2: Ch 'full' exchange of width 3; kind 4: Ch 'cross' exchange of width 1
+           (the tendency exchange of vector_advection_Ch_mod.f90:56) */
         fld_t a, b; fld_init(&a, c->N, c->N + 1, 5); fld_init(&b, c->N + 1, c->N, 5);
         fld_from_packed(&a, f); fld_from_packed(&b, f2);
-        exch_do(&c->ex_ch3_u, &a, &b);
-        exch_do(&c->ex_ch3_v, &a, &b);
+        exch_do(kind == 4 ? &c->ex_ch1c_u : &c->ex_ch3_u, &a, &b);
+        exch_do(kind == 4 ? &c->ex_ch1c_v : &c->ex_ch3_v, &a, &b);
         ring_out(&a, w, out); ring_out(&b, w, out2); fld_free(&a); fld_free(&b);
     }
 }

@@ -79,3 +79,26 @@ def test_ch_vector_halo_normal_component(links):
                     val = [ut[nb, ap - 1, c - 1], ut[nb, ap - 1, N - c], vt[nb, c - 1, ap - 1], vt[nb, N - c, ap - 1]][ns]
                     ref = [A[t, a + 2, 3 - c], A[t, a + 2, N + c + 2], B[t, 3 - c, a + 2], B[t, N + c + 2, a + 2]][s]
                     assert ref == sn * val
+
+
+def test_ch_tendency_exchange_cross_width1(links):
+    """The width-1 'cross' Ch exchange behind the advective tendency edge sync
+    (vector_advection_Ch_mod.f90:56): the halo row/column next to a duplicated
+    edge holds the neighbour's tangential component there, with the tangential
+    sign (swe_advective.cuh:adv_edge_sync)."""
+    L, o = links
+    rng = np.random.default_rng(3)
+    u, v = rng.standard_normal((6, N + 1, N)), rng.standard_normal((6, N, N + 1))
+    w = 2
+    U, V = o.halo_probe(4, u, v, w=w)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, sn, st = L[t, s]
+            for c in range(1, N + 1):
+                cp = N + 1 - c if rev else c
+                nbv = u[nb, 0 if ns == 2 else N, cp - 1] if ns >= 2 else v[nb, cp - 1, 0 if ns == 0 else N]
+                if s >= 2:
+                    got = U[t, (0 if s == 2 else N + 2) + w - 1, c + w - 1]
+                else:
+                    got = V[t, c + w - 1, (0 if s == 0 else N + 2) + w - 1]
+                assert got == st * nbv
