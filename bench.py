@@ -15,7 +15,9 @@ device write), bracketed by CUDA events on the library's stream; max over ranks.
 The stage kernels' tile size is autotuned per precision before the warm-up
 (``--tile`` fixes it instead).
 
-Also reported (same JSON line, ``ensemble``): the batched ensemble, 256 members
+Also reported (``nonlinear``): C384 nonlinear Williamson test 2 with a tilted
+axis, dt 75 s, 1152 RK4 steps, advective operator, FP32 and FP64, with errors
+against the steady state.  And (``ensemble``): the batched ensemble, 256 members
 of C48, dt 600 s, 144 RK4 steps, FP32, in one context, against the same 256
 members run one after another through a single-member context.  And
 (``serving``): a seeded Poisson stream (200 requests/s) of linear integrations,
@@ -291,6 +293,58 @@ def run_precision(precision, ic, args, torch, dist, world):
 
 ENS_N, ENS_M, ENS_DT, ENS_STEPS, ENS_SEED = 48, 256, 600.0, 144, 20261203 + 4
 SRV_REQUESTS, SRV_RATE, SRV_SEED, SRV_BUDGET = 120, 200.0, 20261203 + 5, 24 << 30
+NL_N, NL_DT, NL_STEPS, NL_SEED = 384, 75.0, 1152, 20261203 + 3
+
+
+def run_nonlinear(args, torch, dist, world):
+    """Config 3: nonlinear Williamson test 2 (steady zonal flow about a tilted axis) at
+    C384, dt 75 s, 1152 RK4 steps, advective operator; FP32 and FP64; errors against
+    the analytic steady state (the initial state) and FP32 against FP64."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme, testcases
+    from ch_swe_b200.testcases import EARTH_GRAV, EARTH_RADIUS
+    rng = np.random.default_rng(NL_SEED)
+    theta = float(rng.uniform(0.0, 0.5 * np.pi))
+    axis = (np.sin(theta), 0.0, np.cos(theta))
+    u0 = 2.0 * np.pi * EARTH_RADIUS / (12.0 * 86400.0)
+    hm = 2.94e4 / EARTH_GRAV
+    ic = testcases.williamson2(NL_N, u0=u0, h_mean=hm, axis=axis)
+    stream = torch.cuda.current_stream()
+    out, final = {}, {}
+    for prec in ("fp32", "fp64"):
+        dom = create_domain(NL_N, precision=prec, operator="advective", rotation_axis=axis)
+        dom.set_stream(stream.cuda_stream)
+        tune = set_tile(dom, args)
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
+        x = create_stvec_swm(dom).upload(*ic)
+        rk = create_timescheme(x, "rk4")
+        rk.steps(x, op, dom, NL_DT, 4)
+        x.upload(*ic)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rk.steps(x, op, dom, NL_DT, NL_STEPS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        if world > 1:
+            from ch_swe_b200 import replicas
+            ms = replicas.max_over_ranks(ms, dist, device="cuda")
+        final[prec] = x.download()
+        errs = {nm: {"rel_l2": float(np.linalg.norm(f - r) / np.linalg.norm(r)),
+                     "rel_max": float(np.abs(f - r).max() / np.abs(r).max())}
+                for nm, f, r in zip("huv", final[prec], ic)}
+        out[prec] = {"value": world * 6 * NL_N ** 2 * NL_STEPS / (ms / 1e3), "ms_total": ms, "tile": dom.tile,
+                     "tune_ms_per_rk4_step": tune, "error_vs_steady_state": errs}
+        dom.destroy()
+    out["fp32_vs_fp64"] = {nm: {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                                "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
+                           for nm, a, b in zip("huv", final["fp32"], final["fp64"])}
+    out["workload"] = (f"C{NL_N} nonlinear SWE (advective operator, covariant Ch, up4 flux and advection), "
+                       f"Williamson test 2, u0 = 2 pi a / 12 days, axis tilted by {theta:.4f} rad (seed {NL_SEED}), "
+                       f"g h0 = 2.94e4 m2/s2, dt {NL_DT:g} s, {NL_STEPS} RK4 steps")
+    out["unit"] = "cell-updates/s"
+    return out
 
 
 def run_serving(args, torch):
@@ -310,7 +364,7 @@ def run_serving(args, torch):
         r64 = copy.copy(r)
         r64.precision = "fp64"
         ref = serve.run_alone(r64)
-        errs.append({"rid": r.rid, "N": r.N, "steps": r.nsteps,
+        errs.append({"rid": r.rid, "N": r.N, "steps": r.nsteps, "operator": r.operator,
                      **{f"{nm}_rel_l2": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
                         for nm, a, b in zip("huv", r.result, ref)}})
     by_size = {}
@@ -321,7 +375,7 @@ def run_serving(args, torch):
                                 "p99_ms": float(np.percentile(lat, 99))}
     return {
         "workload": f"{SRV_REQUESTS} requests, Poisson {SRV_RATE:g}/s (seed {SRV_SEED}), N in {list(serve.SIZES)}, "
-                    "24-576 RK4 steps, FP32/FP64 50/50, linear operator, 1-4 seeded Gaussians",
+                    "24-576 RK4 steps, FP32/FP64 50/50, linear/advective operator 50/50, 1-4 seeded Gaussians",
         "requests": stats.n, "makespan_s": stats.makespan_s, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
         "mean_ms": stats.mean_ms, "requests_per_s": stats.requests_per_s,
         "cell_updates_per_s": stats.cell_updates_per_s, "hbm_budget_bytes": SRV_BUDGET,
@@ -421,6 +475,7 @@ def run_ours(args):
             res[prec] = run_precision(prec, ic, args, torch, dist, world)
         ens = None if args.no_ensemble else run_ensemble(args, torch, dist, world)
         srv = None if (args.no_serving or world > 1) else run_serving(args, torch)
+        nl = None if args.no_nonlinear else run_nonlinear(args, torch, dist, world)
     clocks = clk.summary()
 
     K = args.steps
@@ -470,6 +525,8 @@ def run_ours(args):
         line["ensemble"] = ens
     if srv is not None:
         line["serving"] = srv
+    if nl is not None:
+        line["nonlinear"] = nl
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -491,6 +548,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-workload leg")
+    ap.add_argument("--no-nonlinear", action="store_true", help="skip the nonlinear (C384 Williamson 2) leg")
     ap.add_argument("--tile", default="auto", choices=["auto", "17", "25", "33"],
                     help="stage-kernel tile size (default: autotuned per precision)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,

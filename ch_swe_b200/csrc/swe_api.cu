@@ -960,17 +960,25 @@ static dim3 stage_grid(int N, int members, int tm)
 
 // The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
 // device and element type (the attribute belongs to the device's context).
+template <class T, int TM, bool ADV>
+static cudaError_t stage_smem_optin_modes()
+{
+    const int sb = (int)StageLayout<T, TM>::bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, 0, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 1, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 2, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 3, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 4, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    return e;
+}
+
 template <class T, int TM>
 static cudaError_t stage_smem_optin_tm()
 {
     cudaError_t e =
         cudaFuncSetAttribute(k_co2contra<T, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T, TM>::bytes());
-    const int sb = (int)StageLayout<T, TM>::bytes();
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, false>();
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, true>();
     return e;
 }
 
@@ -1008,19 +1016,27 @@ static void launch_co2contra(int tm, int members, const T *y, T *w, T *es, const
     }
 }
 
-template <class T, int TM>
-static void launch_stage_tm(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
-                            const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+template <class T, int TM, bool ADV>
+static void launch_stage_modes(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
+                               const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
     const dim3 g = stage_grid(d.N, members, TM);
     const size_t sb = StageLayout<T, TM>::bytes();
     switch (a.mode) {
-    case 0: launch_k(k_stage<T, TM, 0>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: launch_k(k_stage<T, TM, 1>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: launch_k(k_stage<T, TM, 2>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: launch_k(k_stage<T, TM, 3>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: launch_k(k_stage<T, TM, 4>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 0: launch_k(k_stage<T, TM, 0, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: launch_k(k_stage<T, TM, 1, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: launch_k(k_stage<T, TM, 2, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: launch_k(k_stage<T, TM, 3, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: launch_k(k_stage<T, TM, 4, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
     }
+}
+
+template <class T, int TM>
+static void launch_stage_tm(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
+                            const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+{
+    if (a.A) launch_stage_modes<T, TM, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
+    else launch_stage_modes<T, TM, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
 }
 
 template <class T>

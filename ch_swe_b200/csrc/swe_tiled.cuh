@@ -282,8 +282,10 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 //   mode 2: Y1 = V0 + dt/2 k,  ACC += dt/3 k
 //   mode 3: Y1 = V0 + dt   k,  ACC += dt/3 k
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
-template <class T, int TM, int MODE>
-__global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
+// ADV: the advective operator (divergence of the mass flux a.F, tendencies a.A,
+// gradient of the pre-averaging boundary h a.HB); false: the linear operator.
+template <class T, int TM, int MODE, bool ADV>
+__global__ void __launch_bounds__(STAGE_THREADS, TM <= 17 ? 3 : 2) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
 {
@@ -319,9 +321,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
         const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0);
         const T *gh = yp + oh, *gu = wp + d.fs + ou, *gjy = m.Jy + ou;
         // the field whose divergence is taken: ut, or the mass flux of the advective operator
-        const T *gf = a.F ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
+        const T *gf = ADV ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
         T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN], rfu[IT_WIN];
-        const T *hpre = (const T *)a.HB;
+        const T *hpre = ADV ? (const T *)a.HB : nullptr;
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             const int go = r * P + c;
             const bool jr = ok && r >= 2 && r < th + 2;
             rh[it] = ok ? __ldg(gh + go) : T(0);
-            if (hpre && ok) {
+            if (ADV && ok) {
                 // advective operator: the gradient reads h as it was before the averaging
                 const int hi = sh.x0 + c, hj = sh.y0 + r;
                 if (hi >= 1 && hi <= n && hj >= 1 && hj <= n && (hi == 1 || hi == n || hj == 1 || hj == n))
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             }
             ru[it] = ok ? __ldg(gu + go) : T(0);
             rjy[it] = jr ? __ldg(gjy + go) : T(0);
-            rfu[it] = gf && jr ? __ldg(gf + go) : ru[it];
+            rfu[it] = ADV && jr ? __ldg(gf + go) : ru[it];
         }
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
     {
         const int64_t ov = box_off(P, svt.x0, svt.y0);
         const T *gv = wp + 2 * d.fs + ov, *gjx = m.Jx + ov;
-        const T *gf = a.F ? (const T *)a.F + mo + t * d.ps + 2 * d.fs + ov : nullptr;
+        const T *gf = ADV ? (const T *)a.F + mo + t * d.ps + 2 * d.fs + ov : nullptr;
         T rv[IT_WIN], rjx[IT_WIN], rfv[IT_WIN];
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
@@ -372,13 +374,13 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
             const bool jc = ok && c >= 2 && c < tw + 2;
             rv[it] = ok ? __ldg(gv + go) : T(0);
             rjx[it] = jc ? __ldg(gjx + go) : T(0);
-            rfv[it] = gf && jc ? __ldg(gf + go) : rv[it];
+            rfv[it] = ADV && jc ? __ldg(gf + go) : rv[it];
         }
         T hx0 = 0, hx1 = 0, hy0 = 0, hy1 = 0;
         const int q = threadIdx.x;
-        const T *hpre = (const T *)a.HB;
+        const T *hpre = ADV ? (const T *)a.HB : nullptr;
         auto halo = [&](int s, int along) {
-            if (!hpre) return h_halo(y, d, t, s, along);
+            if (!ADV) return h_halo(y, d, t, s, along);
             const Link L = c_link[t][s];
             return __ldg(hpre + hb_index(N, mem, L.nb, L.nside, nb_along(L, n, along)));
         };
@@ -524,7 +526,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
         kh[it] = -H * dvg;
         const T *Aa = (const T *)a.A;
         if (i <= N) {
-            if (Aa) {
+            if constexpr (ADV) {
                 // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
                 T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
                 if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(const T *__restrict_
                 gy += sat * (ht[c] - hcol(n));
             }
             gy = gy * m.inv_hxa;
-            if (Aa) {
+            if constexpr (ADV) {
                 T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
                 if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
                 kv[it] = (av + -m.grav * gy) + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];

@@ -1,9 +1,9 @@
 """Served mixed workload: continuous batching of shallow-water integrations on one GPU.
 
-A request is one integration: cube size N, precision, number of RK4 steps, time
-step, mean depth and an initial state (h, u, v).  The server keeps one *pool*
-per (N, precision): a context with a fixed number of member slots, its own CUDA
-stream and its states resident in HBM.  A request occupies one slot from
+A request is one integration: operator (linear or advective), cube size N,
+precision, number of RK4 steps, time step, depth and an initial state (h, u, v).
+The server keeps one *pool* per (operator, N, precision): a context with a fixed
+number of member slots, its own CUDA stream and its states resident in HBM.  A request occupies one slot from
 admission to completion.
 
 Continuous batching:
@@ -44,15 +44,19 @@ def stable_dt(N: int) -> float:
     return 150.0 * 192.0 / N
 
 
-def member_bytes(N: int, precision: str) -> int:
+def member_bytes(N: int, precision: str, operator: str = "linear") -> int:
     """Device bytes one member slot of a pool holds: the state, two stage buffers,
     the RK accumulator, the contravariant scratch, the FP32 compensation, the edge
-    buffer and the edge strips (layout of swe_api.cu)."""
+    buffer and the edge strips (layout of swe_api.cu); the advective operator adds
+    the mass flux, the advective tendencies, uh/vh, the flux strips, the virtual
+    wind points and the boundary h."""
     elem = 4 if precision == "fp32" else 8
     rows = N + 9
     pitch = (rows + 7) // 8 * 8
     box = 3 * 6 * rows * pitch
     words = 5 * box + 6 * 4 * (N + 1) * (3 + 4)
+    if operator == "advective":
+        words += 3 * box + 6 * 4 * (N + 1) * (4 + 1) + 6 * (24 * N + 12)
     extra = box * 4 if precision == "fp32" else 0
     return words * elem + extra
 
@@ -87,6 +91,12 @@ class Request:
                 self._ic = testcases.gaussian_sum(self.N, *p)
         return self._ic
 
+    def initial_state(self):
+        """(h, u, v) as uploaded: the linear operator integrates the perturbation of
+        the mean depth h_mean, the advective one the full depth h_mean + bumps."""
+        h, u, v = self.ic
+        return (h + self.h_mean, u, v) if self.operator == "advective" else (h, u, v)
+
     @property
     def cell_updates(self) -> int:
         return 6 * self.N * self.N * self.nsteps
@@ -97,10 +107,10 @@ class Request:
 
 
 def poisson_stream(n_requests: int, rate: float = 200.0, seed: int = 20261203 + 5, sizes=SIZES,
-                   steps=(24, 576), precisions=("fp32", "fp64")):
+                   steps=(24, 576), precisions=("fp32", "fp64"), operators=("linear", "advective")):
     """Seeded Poisson arrivals (mean `rate` per second); N uniform over `sizes`, steps
-    uniform in `steps`, precision 50/50; each request one ensemble-style initial
-    state (H ~ U[500, 2000] m, 1-4 Gaussians)."""
+    uniform in `steps`, precision and operator 50/50; each request one ensemble-style
+    initial state (H ~ U[500, 2000] m, 1-4 Gaussians, at rest)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     reqs = []
@@ -109,35 +119,42 @@ def poisson_stream(n_requests: int, rate: float = 200.0, seed: int = 20261203 + 
         N = int(rng.choice(sizes))
         nst = int(rng.integers(steps[0], steps[1] + 1))
         prec = str(rng.choice(precisions))
+        op = str(rng.choice(operators))
         H, centres, widths, amps = ensemble.member_params(1, int(rng.integers(1 << 31)))[0]
-        reqs.append(Request(k, N, prec, nst, stable_dt(N), H, (centres, widths, amps), arrival=t))
+        reqs.append(Request(k, N, prec, nst, stable_dt(N), H, (centres, widths, amps), arrival=t, operator=op))
     return reqs
 
 
-class Pool:
-    """Member slots of one (N, precision): one context on its own stream."""
+def _operator(dom, operator: str):
+    from .swm import create_swm_operator
+    if operator == "advective":
+        return create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
+    return create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
 
-    def __init__(self, N: int, precision: str, capacity: int, torch, tile=None):
-        from .swm import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
-        self.N, self.precision, self.capacity = N, precision, capacity
+
+class Pool:
+    """Member slots of one (operator, N, precision): one context on its own stream."""
+
+    def __init__(self, N: int, precision: str, capacity: int, torch, tile=None, operator: str = "linear"):
+        from .swm import create_domain, create_stvec_swm, create_timescheme
+        self.N, self.precision, self.capacity, self.operator = N, precision, capacity, operator
         self.torch = torch
         self.stream = torch.cuda.Stream()
-        self.dom = create_domain(N, precision=precision, n_members=capacity)
+        self.dom = create_domain(N, precision=precision, n_members=capacity, operator=operator)
         self.dom.set_stream(self.stream.cuda_stream)
         if tile is None:
             with torch.cuda.stream(self.stream):
                 self.dom.autotune(nreps=4)
         else:
             self.dom.tile = tile
-        self.op = create_swm_operator(self.dom.grav, {"swm_operator_type": "linear_swm_operator",
-                                                      "h_mean": 1000.0}, self.dom)
+        self.op = _operator(self.dom, operator)
         self.state = create_stvec_swm(self.dom)
         self.rk = create_timescheme(self.state, "rk4")
         self.slots: list[Request | None] = [None] * capacity
         self.remaining = [0] * capacity
         self.event = None
         self.tick_len = 0
-        self.bytes = capacity * member_bytes(N, precision)
+        self.bytes = capacity * member_bytes(N, precision, operator)
 
     @property
     def busy(self) -> bool:
@@ -155,8 +172,9 @@ class Pool:
 
     def admit(self, req: Request, now: float):
         k = self.free_slot()
-        self.state.upload(*req.ic, member=k)
-        self.op.set_member_h_mean(k, req.h_mean)
+        self.state.upload(*req.initial_state(), member=k)
+        if req.operator == "linear":
+            self.op.set_member_h_mean(k, req.h_mean)
         self.slots[k] = req
         self.remaining[k] = req.nsteps
         req.admitted = now
@@ -226,12 +244,12 @@ class Server:
         return sum(p.bytes for p in self.pools.values())
 
     def _pool_for(self, req: Request):
-        if req.operator != "linear":
+        if req.operator not in ("linear", "advective"):
             raise ValueError(f"request {req.rid}: operator {req.operator!r} is not served")
-        key = (req.N, req.precision)
+        key = (req.N, req.precision, req.operator)
         if key in self.pools:
             return self.pools[key]
-        per = member_bytes(req.N, req.precision)
+        per = member_bytes(req.N, req.precision, req.operator)
         want = self.max_slots.get(req.N, 4)
         free = self.budget - self.used_bytes()
         if free < per:
@@ -244,7 +262,7 @@ class Server:
         cap = min(want, free // per)
         if cap < 1:
             return None
-        pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key))
+        pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key), operator=req.operator)
         self.pools[key] = pool
         self.peak = max(self.peak, self.used_bytes())
         return pool
@@ -295,7 +313,7 @@ class Server:
             n=len(done), makespan_s=makespan, p50_ms=float(np.percentile(lat, 50)),
             p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
             requests_per_s=len(done) / makespan, cell_updates_per_s=cells / makespan,
-            pools={f"C{k[0]}/{k[1]}": {"slots": p.capacity, "tile": p.dom.tile} for k, p in self.pools.items()},
+            pools={f"{k[2]}/C{k[0]}/{k[1]}": {"slots": p.capacity, "tile": p.dom.tile} for k, p in self.pools.items()},
             peak_bytes=self.peak)
 
     def close(self):
@@ -306,12 +324,14 @@ class Server:
 
 def run_alone(req: Request, tile=None):
     """The same integration in its own single-member context (the comparison arm)."""
-    from .swm import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
-    dom = create_domain(req.N, precision=req.precision, h_mean=req.h_mean)
+    from .swm import create_domain, create_stvec_swm, create_timescheme
+    dom = create_domain(req.N, precision=req.precision, operator=req.operator)
     if tile is not None:
         dom.tile = tile
-    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": req.h_mean}, dom)
-    st = create_stvec_swm(dom).upload(*req.ic)
+    op = _operator(dom, req.operator)
+    if req.operator == "linear":
+        op.set_member_h_mean(0, req.h_mean)
+    st = create_stvec_swm(dom).upload(*req.initial_state())
     create_timescheme(st, "rk4").steps_members(st, op, [req.dt], req.nsteps)
     out = st.download()
     dom.destroy()

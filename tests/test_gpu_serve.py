@@ -20,13 +20,14 @@ def _stream(n, seed, sizes=(24, 48), steps=(24, 64)):
 
 
 def test_mixed_results_equal_alone_bitwise():
-    """Same tile alone and in the mix: bit-identical states (both precisions)."""
+    """Same tile alone and in the mix: bit-identical states (both precisions, both operators)."""
     from ch_swe_b200.serve import Server, run_alone
     reqs = _stream(20, 11)
     srv = Server(hbm_budget_bytes=2 << 30, max_tick=8, max_slots={24: 6, 48: 4})
     stats = srv.run(reqs, realtime=False)
     srv.close()
     assert stats.n == len(reqs)
+    assert {r.operator for r in reqs} == {"linear", "advective"}
     for r in reqs:
         alone = run_alone(r, tile=r.pool_tile)
         for a, b, name in zip(r.result, alone, "huv"):
@@ -36,22 +37,28 @@ def test_mixed_results_equal_alone_bitwise():
 def test_mixed_fp64_matches_oracle():
     from ch_swe_b200.serve import Server
     from oracle.oracle import Oracle
-    reqs = [r for r in _stream(12, 12, sizes=(24,), steps=(24, 40)) if r.precision == "fp64"][:3]
-    assert reqs
+    reqs = [r for r in _stream(16, 12, sizes=(24,), steps=(24, 40)) if r.precision == "fp64"][:4]
+    assert {r.operator for r in reqs} == {"linear", "advective"}
     srv = Server(hbm_budget_bytes=1 << 30, max_tick=16)
     srv.run(reqs, realtime=False)
     srv.close()
     for r in reqs:
-        o = Oracle(r.N, h_mean=r.h_mean)
-        ref = o.rk4(*r.ic, r.dt, r.nsteps)
+        o = Oracle(r.N, h_mean=r.h_mean, operator=r.operator)
+        ref = o.rk4(*r.initial_state(), r.dt, r.nsteps)
         for a, b, name in zip(r.result, ref, "huv"):
-            assert np.abs(a - b).max() / np.abs(b).max() < 1e-12, (r.rid, name)
+            # 1e-12 of the field's scale; a wind that starts at rest is measured against
+            # the gravity-wave speed sqrt(g H) (rounding in the gradient of the full
+            # depth h ~ H is what separates the two FP64 results)
+            scale = np.abs(b).max()
+            if name != "h":
+                scale = max(scale, np.sqrt(9.80616 * r.h_mean))
+            assert np.abs(a - b).max() / scale < 1e-12, (r.rid, r.operator, name)
 
 
 def test_budget_bounds_pools_and_all_requests_finish():
     from ch_swe_b200.serve import Server, member_bytes
     reqs = _stream(16, 13, sizes=(24, 48))
-    budget = 3 * member_bytes(48, "fp64") + 2 * member_bytes(24, "fp64")
+    budget = 3 * member_bytes(48, "fp64", "advective") + 2 * member_bytes(24, "fp64", "advective")
     srv = Server(hbm_budget_bytes=budget, max_tick=8)
     stats = srv.run(reqs, realtime=False)
     srv.close()

@@ -14,6 +14,7 @@ def test_poisson_stream_is_seeded_and_in_range():
     rate = len(arr) / arr[-1]
     assert 150 < rate < 260
     assert 0.35 < np.mean([r.precision == "fp32" for r in a]) < 0.65
+    assert 0.35 < np.mean([r.operator == "advective" for r in a]) < 0.65
     h, u, v = a[0].ic
     assert h.shape == (6, a[0].N + 1, a[0].N + 1) and not u.any() and not v.any()
 
@@ -21,6 +22,7 @@ def test_poisson_stream_is_seeded_and_in_range():
 def test_member_bytes_and_dt():
     from ch_swe_b200.serve import member_bytes, stable_dt
     assert member_bytes(48, "fp64") > member_bytes(48, "fp32") > member_bytes(24, "fp32")
+    assert member_bytes(48, "fp32", "advective") > member_bytes(48, "fp32", "linear")
     # five FP64 boxes of 3 fields x 6 panels x (N+9) x pitch dominate
     N = 192
     rows = N + 9
