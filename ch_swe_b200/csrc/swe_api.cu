@@ -222,10 +222,11 @@ struct swe_ctx {
     double *red = nullptr;           // reduction partials
     unsigned char *pinned = nullptr; // pinned host staging for uploads/downloads (whole batch)
     // captured RK4 step
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;   // one RK4 step
+    cudaGraphExec_t graphk = nullptr;  // GRAPH_STEPS RK4 steps
     const void *graph_v0 = nullptr;
     double graph_dt = 0.0;
-    int graph_kernels = 0;
+    int graph_kernels = 0, graphk_kernels = 0;
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
@@ -636,6 +637,7 @@ extern "C" int swe_cfg_default(swe_cfg *cfg)
 static void free_ctx(swe_ctx *c)
 {
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->graphk) cudaGraphExecDestroy(c->graphk);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
     cudaFree(c->qw); cudaFree(c->red);
@@ -745,6 +747,7 @@ extern "C" int swe_set_stream(swe_ctx *c, void *s)
     if (!c) return SWE_EINVAL;
     c->stream = s ? (cudaStream_t)s : c->own_stream;
     if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
     return SWE_OK;
 }
 
@@ -781,6 +784,14 @@ extern "C" int swe_stvec_destroy(swe_stvec *v)
 {
     if (!v) return SWE_EINVAL;
     cudaStreamSynchronize(v->ctx->stream);
+    swe_ctx *c = v->ctx;
+    if (c->graph_v0 == v->d) {
+        // the cached graphs hold this vector's pointers: a later vector at the same
+        // address must capture its own
+        if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+        if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
+        c->graph_v0 = nullptr;
+    }
     cudaFree(v->d);
     cudaFree(v->cmp);
     delete v;
@@ -1165,31 +1176,51 @@ extern "C" int swe_rk4_step(swe_ctx *c, swe_stvec *v0, double dt)
     return SWE_OK;
 }
 
-// nsteps replays of one captured RK4 step; members == true uses the per-member
-// time steps in c->dtm (captured by pointer, so new values need no new capture).
+// RK4 steps per replay of the long graph: enough to hide the gaps between graph
+// launches, small enough that a remainder costs little.
+constexpr int GRAPH_STEPS = 8;
+
+static int capture_steps(swe_ctx *c, swe_stvec *v0, double dt, bool members, int steps, cudaGraphExec_t *out,
+                         int *kernels)
+{
+    cudaGraph_t g;
+    long long before = c->launches;
+    CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < steps; s++) enqueue_rk4(c, v0, dt, members ? c->dtm : nullptr);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+    *kernels = (int)(c->launches - before);
+    c->launches = before;
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return SWE_OK;
+}
+
+// nsteps replays of captured RK4 steps (GRAPH_STEPS per replay, then single steps);
+// members == true uses the per-member time steps in c->dtm (captured by pointer,
+// so new values need no new capture).
 static int run_steps(swe_ctx *c, swe_stvec *v0, double dt, bool members, int nsteps)
 {
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     if (nsteps == 0) return SWE_OK;
-    if (!c->graph || c->graph_v0 != v0->d || c->graph_members != members || (!members && c->graph_dt != dt)) {
+    if (c->graph_v0 != v0->d || c->graph_members != members || (!members && c->graph_dt != dt)) {
         if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
-        cudaGraph_t g;
-        long long before = c->launches;
-        CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_rk4(c, v0, dt, members ? c->dtm : nullptr);
-        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-        if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph capture: %s", cudaGetErrorString(e));
-        c->graph_kernels = (int)(c->launches - before);
-        c->launches = before;
-        e = cudaGraphInstantiate(&c->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
         c->graph_v0 = v0->d;
         c->graph_dt = dt;
         c->graph_members = members;
     }
-    for (int s = 0; s < nsteps; s++) {
+    const int full = nsteps / GRAPH_STEPS, rest = nsteps % GRAPH_STEPS;
+    if (full > 0 && !c->graphk && (rc = capture_steps(c, v0, dt, members, GRAPH_STEPS, &c->graphk, &c->graphk_kernels)))
+        return rc;
+    if (rest > 0 && !c->graph && (rc = capture_steps(c, v0, dt, members, 1, &c->graph, &c->graph_kernels))) return rc;
+    for (int s = 0; s < full; s++) {
+        CU(c, cudaGraphLaunch(c->graphk, c->stream));
+        c->launches += c->graphk_kernels;
+    }
+    for (int s = 0; s < rest; s++) {
         CU(c, cudaGraphLaunch(c->graph, c->stream));
         c->launches += c->graph_kernels;
     }
@@ -1575,6 +1606,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
 static void drop_graph(swe_ctx *c)
 {
     if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
 }
 
 extern "C" int swe_set_tile(swe_ctx *c, int tile)
