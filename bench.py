@@ -538,6 +538,37 @@ def run_ours(args):
     return 0
 
 
+def run_profile_leg(args):
+    """A few RK4 steps of one workload and nothing else: the command the ncu
+    summaries under profiles/ are taken from (never a bench value)."""
+    import torch
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme, ensemble, testcases
+    tile = None if args.tile == "auto" else int(args.tile)
+    if args.profile_leg == "ensemble":
+        dom, op, st, _ = ensemble.create_ensemble(ENS_N, ENS_M, ENS_SEED, precision="fp32")
+        dt = ENS_DT
+    elif args.profile_leg == "nonlinear":
+        axis = (np.sin(0.7), 0.0, np.cos(0.7))
+        dom = create_domain(NL_N, precision="fp32", operator="advective", rotation_axis=axis)
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
+        st = create_stvec_swm(dom).upload(*testcases.williamson2(NL_N, axis=axis))
+        dt = NL_DT
+    else:
+        dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN)
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
+        st = create_stvec_swm(dom).upload(*workload_ic()[0])
+        dt = DT
+    if tile:
+        dom.tile = tile
+    rk = create_timescheme(st, "rk4")
+    for _ in range(args.rk4_steps):
+        rk.step(st, op, dom, dt)
+    torch.cuda.synchronize()
+    dom.destroy()
+    print(f"profile leg {args.profile_leg}: {args.rk4_steps} RK4 steps, tile {tile or 'default'}", flush=True)
+    return 0
+
+
 def main():
     global NSTEPS
     ap = argparse.ArgumentParser()
@@ -553,7 +584,11 @@ def main():
                     help="stage-kernel tile size (default: autotuned per precision)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
+    ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear"], default=None,
+                    help="run --rk4-steps steps of one workload only (for ncu captures; prints no bench line)")
     args = ap.parse_args()
+    if args.profile_leg:
+        return run_profile_leg(args)
     NSTEPS = args.rk4_steps
     if args.warmup < 3:
         args.warmup = 3
