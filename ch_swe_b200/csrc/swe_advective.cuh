@@ -70,13 +70,17 @@ __device__ __forceinline__ int64_t hb_index(int N, int mem, int t, int s, int a)
 // their three copies (in each panel's own order), other edge vertices the mean of
 // their two copies.  The values before the averaging go to HB: the reference's
 // gradient reads its copy h_total taken before (operator_adv_swm_mod.f90:77).
-// One block per member; corner reads precede all corner writes.
+// Grid (1 + edge blocks, members): block 0 of a member takes the 24 corners (all
+// corner reads precede its corner writes), the others one vertex pair each per
+// thread (edge pairs never touch a corner).
 // ---------------------------------------------------------------------------
+constexpr int HAVG_THREADS = 256;
+
 template <class T>
-__global__ void __launch_bounds__(256) k_havg(T *__restrict__ Y, T *__restrict__ HB, Dims d,
-                                              const double *__restrict__ dtm)
+__global__ void __launch_bounds__(HAVG_THREADS) k_havg(T *__restrict__ Y, T *__restrict__ HB, Dims d,
+                                                       const double *__restrict__ dtm)
 {
-    const int mem = blockIdx.x;
+    const int mem = blockIdx.y;
     if (member_frozen(dtm, mem)) return;
     pdl_trigger();
     pdl_wait();
@@ -85,6 +89,22 @@ __global__ void __launch_bounds__(256) k_havg(T *__restrict__ Y, T *__restrict__
     auto at = [&](int t, int i, int j) -> T & { return h[t * d.ps + (j - 1 + MG) * d.P + (i - 1 + MG)]; };
     __shared__ T cval[NPAN * 4];
     const int q = threadIdx.x;
+    if (blockIdx.x > 0) {
+        const int e = (blockIdx.x - 1) * HAVG_THREADS + q;
+        if (e >= 12 * (N - 1)) return;
+        const int ce = e / (N - 1), a = 2 + e % (N - 1);
+        const int t = c_cube_edge[ce][0], s = c_cube_edge[ce][1];
+        int k, l, nb, kk, ll;
+        side_vertex(N, s, a, 0, k, l);
+        nb_copy(N, t, s, k, l, nb, kk, ll);
+        const T x = at(t, k, l), y = at(nb, kk, ll);
+        const T avg = T(0.5) * (x + y);
+        HB[hb_index(N, mem, t, s, a)] = x;
+        HB[hb_index(N, mem, nb, c_link[t][s].nside, nb_along(c_link[t][s], n, a))] = y;
+        at(t, k, l) = avg;
+        at(nb, kk, ll) = avg;
+        return;
+    }
     if (q < NPAN * 4) {
         const int t = q >> 2, c = q & 3;
         const int k0 = (c == 0 || c == 3) ? 1 : n, l0 = (c < 2) ? 1 : n;
@@ -106,19 +126,6 @@ __global__ void __launch_bounds__(256) k_havg(T *__restrict__ Y, T *__restrict__
     if (q < NPAN * 4) {
         const int t = q >> 2, c = q & 3;
         at(t, (c == 0 || c == 3) ? 1 : n, (c < 2) ? 1 : n) = cval[q];
-    }
-    for (int e = q; e < 12 * (N - 1); e += blockDim.x) {
-        const int ce = e / (N - 1), a = 2 + e % (N - 1);
-        const int t = c_cube_edge[ce][0], s = c_cube_edge[ce][1];
-        int k, l, nb, kk, ll;
-        side_vertex(N, s, a, 0, k, l);
-        nb_copy(N, t, s, k, l, nb, kk, ll);
-        const T x = at(t, k, l), y = at(nb, kk, ll);
-        const T avg = T(0.5) * (x + y);
-        HB[hb_index(N, mem, t, s, a)] = x;
-        HB[hb_index(N, mem, nb, c_link[t][s].nside, nb_along(c_link[t][s], n, a))] = y;
-        at(t, k, l) = avg;
-        at(nb, kk, ll) = avg;
     }
 }
 
@@ -181,10 +188,14 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
     const int64_t o = box_off(d.P, i, j);
     const int64_t po = mem * d.ms + t * d.ps;
     T *fs = FS + strip_member(N, mem) + (int64_t)t * 4 * STRIP_LINES * n - 1;
+    const T *hr = h + t * d.ps + (j - 1 + MG) * d.P + (i - 1 + MG);   // h(i, j); the box has 4-point margins
     if (i <= N) {
         const T c = __ldg(W + po + d.fs + o);
-        const T fx = up4_flux(c, h_ext(h, d, av, t, i - 2, j), h_ext(h, d, av, t, i - 1, j), h_ext(h, d, av, t, i, j),
-                              h_ext(h, d, av, t, i + 1, j), h_ext(h, d, av, t, i + 2, j), h_ext(h, d, av, t, i + 3, j));
+        // the six points i-2 .. i+3 lie in the panel for 3 <= i <= N-2
+        const T fx = (i >= 3 && i <= N - 2)
+                         ? up4_flux(c, __ldg(hr - 2), __ldg(hr - 1), __ldg(hr), __ldg(hr + 1), __ldg(hr + 2), __ldg(hr + 3))
+                         : up4_flux(c, h_ext(h, d, av, t, i - 2, j), h_ext(h, d, av, t, i - 1, j), h_ext(h, d, av, t, i, j),
+                                    h_ext(h, d, av, t, i + 1, j), h_ext(h, d, av, t, i + 2, j), h_ext(h, d, av, t, i + 3, j));
         F[po + d.fs + o] = fx;
         if (i <= 3) fs[(SIDE_L * 4 + i - 1) * n + j] = fx;
         if (i >= N - 2) fs[(SIDE_R * 4 + N - i) * n + j] = fx;
@@ -193,8 +204,12 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
     }
     if (j <= N) {
         const T c = __ldg(W + po + 2 * d.fs + o);
-        const T fy = up4_flux(c, h_ext(h, d, av, t, i, j - 2), h_ext(h, d, av, t, i, j - 1), h_ext(h, d, av, t, i, j),
-                              h_ext(h, d, av, t, i, j + 1), h_ext(h, d, av, t, i, j + 2), h_ext(h, d, av, t, i, j + 3));
+        const int P = d.P;
+        const T fy = (j >= 3 && j <= N - 2)
+                         ? up4_flux(c, __ldg(hr - 2 * P), __ldg(hr - P), __ldg(hr), __ldg(hr + P), __ldg(hr + 2 * P),
+                                    __ldg(hr + 3 * P))
+                         : up4_flux(c, h_ext(h, d, av, t, i, j - 2), h_ext(h, d, av, t, i, j - 1), h_ext(h, d, av, t, i, j),
+                                    h_ext(h, d, av, t, i, j + 1), h_ext(h, d, av, t, i, j + 2), h_ext(h, d, av, t, i, j + 3));
         F[po + 2 * d.fs + o] = fy;
         if (j <= 3) fs[(SIDE_B * 4 + j - 1) * n + i] = fy;
         if (j >= N - 2) fs[(SIDE_T * 4 + N - j) * n + i] = fy;
@@ -322,10 +337,20 @@ __global__ void __launch_bounds__(256) k_adv(const T *__restrict__ Y, const T *_
         const GV<T> VHp{PH + po + 2 * d.fs, d.P};
         const T b = ii2c<T>(i, N, [&](int c) { return VHp(c, j); });
         T fx[7], fy[7];
+        const T *ur = y + t * d.ps + d.fs + (j - 1 + MG) * d.P + (i - 1 + MG);   // u(i, j)
+        if (i >= 4 && i <= N - 3) {
 #pragma unroll
-        for (int k = 0; k < 7; k++) {
-            fx[k] = u_ext(y, vh, d, av.hp, t, i - 3 + k, j);
-            fy[k] = u_ext(y, vh, d, av.hp, t, i, j - 3 + k);
+            for (int k = 0; k < 7; k++) fx[k] = __ldg(ur + (k - 3));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fx[k] = u_ext(y, vh, d, av.hp, t, i - 3 + k, j);
+        }
+        if (j >= 4 && j <= N - 2) {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fy[k] = __ldg(ur + (k - 3) * d.P);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fy[k] = u_ext(y, vh, d, av.hp, t, i, j - 3 + k);
         }
         const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
         T tend = -(a * dx + b * dy) * m.inv_hxa;
@@ -339,10 +364,20 @@ __global__ void __launch_bounds__(256) k_adv(const T *__restrict__ Y, const T *_
         const GV<T> UHp{PH + po + d.fs, d.P};
         const T a = ii2c<T>(j, N, [&](int c) { return UHp(i, c); });
         T fx[7], fy[7];
+        const T *vr = y + t * d.ps + 2 * d.fs + (j - 1 + MG) * d.P + (i - 1 + MG);   // v(i, j)
+        if (i >= 4 && i <= N - 2) {
 #pragma unroll
-        for (int k = 0; k < 7; k++) {
-            fx[k] = v_ext(y, vh, d, av.hp, t, i - 3 + k, j);
-            fy[k] = v_ext(y, vh, d, av.hp, t, i, j - 3 + k);
+            for (int k = 0; k < 7; k++) fx[k] = __ldg(vr + (k - 3));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fx[k] = v_ext(y, vh, d, av.hp, t, i - 3 + k, j);
+        }
+        if (j >= 4 && j <= N - 3) {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fy[k] = __ldg(vr + (k - 3) * d.P);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; k++) fy[k] = v_ext(y, vh, d, av.hp, t, i, j - 3 + k);
         }
         const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
         T tend = -(a * dx + b * dy) * m.inv_hxa;

@@ -1090,7 +1090,8 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     const AdvView<T> &av = adv_view<T>(c);
     const int N = c->cfg.N, n = N + 1;
     const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
-    launch_k(k_havg<T>, dim3(M), dim3(256), 0, c->stream, (T *)yin, (T *)c->hb, c->dims, dtm);
+    launch_k(k_havg<T>, dim3(1 + (12 * (N - 1) + HAVG_THREADS - 1) / HAVG_THREADS, M), dim3(HAVG_THREADS), 0, c->stream,
+             (T *)yin, (T *)c->hb, c->dims, dtm);
     launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
     launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
              (T *)c->edge, c->dims, mv, dtm);

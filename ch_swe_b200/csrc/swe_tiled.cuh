@@ -324,6 +324,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, TM <= 17 ? 3 : 2) k_stage(const
         const T *gf = ADV ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
         T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN], rfu[IT_WIN];
         const T *hpre = ADV ? (const T *)a.HB : nullptr;
+        // only windows that reach a panel-boundary vertex read the pre-averaging values
+        const bool etile = i0 <= 3 || i1 + 2 >= n || j0 <= 3 || j1 + 2 >= n;
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, TM <= 17 ? 3 : 2) k_stage(const
             const int go = r * P + c;
             const bool jr = ok && r >= 2 && r < th + 2;
             rh[it] = ok ? __ldg(gh + go) : T(0);
-            if (ADV && ok) {
+            if (ADV && etile && ok) {
                 // advective operator: the gradient reads h as it was before the averaging
                 const int hi = sh.x0 + c, hj = sh.y0 + r;
                 if (hi >= 1 && hi <= n && hj >= 1 && hj <= n && (hi == 1 || hi == n || hj == 1 || hj == n))
