@@ -228,6 +228,7 @@ struct swe_ctx {
     double graph_dt = 0.0;
     int graph_kernels = 0, graphk_kernels = 0;
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
+    int occ = 2;                     // resident blocks per SM of the stage kernels' register cap
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
     // advective operator (cfg.operator_kind == SWE_OP_ADVECTIVE)
@@ -270,8 +271,22 @@ static bool g_tables_ready[64] = {false};
 
 // Maximal tile sizes the stage kernels are built for; ceil(N / (TM - 1)) balanced
 // tiles per direction always fit, whatever N.
-static const int k_tiles[] = {17, 25, 33};
 static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
+// Kernel configurations the stage kernels are built for: (maximal tile edge,
+// resident blocks per SM the register allocation is capped for).  The advective
+// operator's stage kernel is built for the first configuration of each tile only.
+struct KernelCfg {
+    int tile, occ;
+};
+static const KernelCfg k_cfgs[] = {{17, 3}, {17, 4}, {25, 2}, {25, 3}, {25, 4}, {33, 2}, {33, 3}};
+static const int N_CFGS = sizeof(k_cfgs) / sizeof(k_cfgs[0]);
+static int default_occ(int tm) { return tm == 17 ? 3 : 2; }
+static bool valid_cfg(int tm, int occ)
+{
+    for (const KernelCfg &k : k_cfgs)
+        if (k.tile == tm && k.occ == occ) return true;
+    return false;
+}
 // Default before autotuning: tiles of about 24 points for the smaller cubes.
 static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
@@ -678,6 +693,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     c->dims.ms = 3 * c->dims.fs;
     c->elem = cfg->precision == SWE_FP64 ? 8 : 4;
     c->tile = default_tile(N);
+    c->occ = default_occ(c->tile);
     c->box_elems = (size_t)c->dims.ms * cfg->n_members;
     int rc = SWE_OK;
     auto bail = [&](int code) { free_ctx(c); delete c; return code; };
@@ -971,25 +987,25 @@ static dim3 stage_grid(int N, int members, int tm)
 
 // The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
 // device and element type (the attribute belongs to the device's context).
-template <class T, int TM, bool ADV>
+template <class T, int TM, int OCC, bool ADV>
 static cudaError_t stage_smem_optin_modes()
 {
     const int sb = (int)StageLayout<T, TM>::bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, 0, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 1, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 2, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 3, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, 4, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     return e;
 }
 
-template <class T, int TM>
-static cudaError_t stage_smem_optin_tm()
+template <class T, int TM, int OCC>
+static cudaError_t stage_smem_optin_cfg()
 {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_co2contra<T, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T, TM>::bytes());
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, false>();
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, true>();
+    cudaError_t e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Co2Layout<T, TM>::bytes());
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false>();
+    if (e == cudaSuccess && OCC == (TM == 17 ? 3 : 2)) e = stage_smem_optin_modes<T, TM, OCC, true>();
     return e;
 }
 
@@ -1001,63 +1017,76 @@ static cudaError_t stage_smem_optin()
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && done[dev]) return cudaSuccess;
-    e = stage_smem_optin_tm<T, 17>();
-    if (e == cudaSuccess) e = stage_smem_optin_tm<T, 25>();
-    if (e == cudaSuccess) e = stage_smem_optin_tm<T, 33>();
+    e = stage_smem_optin_cfg<T, 17, 3>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 17, 4>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 2>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 3>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 4>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 33, 2>();
+    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 33, 3>();
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
-template <class T, int TM>
-static void launch_co2contra_tm(int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
-                                cudaStream_t st, const double *dtm)
+template <class T, int TM, int OCC>
+static void launch_co2contra_cfg(int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
+                                 cudaStream_t st, const double *dtm)
 {
-    launch_k(k_co2contra<T, TM>, stage_grid(d.N, members, TM), stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es,
-             d, m, dtm);
+    launch_k(k_co2contra<T, TM, OCC>, stage_grid(d.N, members, TM), stage_block(), Co2Layout<T, TM>::bytes(), st, y, w,
+             es, d, m, dtm);
 }
 
 template <class T>
-static void launch_co2contra(int tm, int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
-                             cudaStream_t st, const double *dtm = nullptr)
+static void launch_co2contra(int tm, int occ, int members, const T *y, T *w, T *es, const Dims &d,
+                             const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
-    switch (tm) {
-    case 17: launch_co2contra_tm<T, 17>(members, y, w, es, d, m, st, dtm); break;
-    case 25: launch_co2contra_tm<T, 25>(members, y, w, es, d, m, st, dtm); break;
-    default: launch_co2contra_tm<T, 33>(members, y, w, es, d, m, st, dtm); break;
+    switch (tm * 10 + occ) {
+    case 173: launch_co2contra_cfg<T, 17, 3>(members, y, w, es, d, m, st, dtm); break;
+    case 174: launch_co2contra_cfg<T, 17, 4>(members, y, w, es, d, m, st, dtm); break;
+    case 252: launch_co2contra_cfg<T, 25, 2>(members, y, w, es, d, m, st, dtm); break;
+    case 253: launch_co2contra_cfg<T, 25, 3>(members, y, w, es, d, m, st, dtm); break;
+    case 254: launch_co2contra_cfg<T, 25, 4>(members, y, w, es, d, m, st, dtm); break;
+    case 333: launch_co2contra_cfg<T, 33, 3>(members, y, w, es, d, m, st, dtm); break;
+    default: launch_co2contra_cfg<T, 33, 2>(members, y, w, es, d, m, st, dtm); break;
     }
 }
 
-template <class T, int TM, bool ADV>
+template <class T, int TM, int OCC, bool ADV>
 static void launch_stage_modes(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
                                const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
     const dim3 g = stage_grid(d.N, members, TM);
     const size_t sb = StageLayout<T, TM>::bytes();
     switch (a.mode) {
-    case 0: launch_k(k_stage<T, TM, 0, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: launch_k(k_stage<T, TM, 1, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: launch_k(k_stage<T, TM, 2, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: launch_k(k_stage<T, TM, 3, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: launch_k(k_stage<T, TM, 4, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: launch_k(k_stage<T, TM, OCC, 4, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
     }
 }
 
-template <class T, int TM>
-static void launch_stage_tm(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
-                            const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
-{
-    if (a.A) launch_stage_modes<T, TM, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
-    else launch_stage_modes<T, TM, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
-}
-
+// The advective variant exists for the first configuration of each tile only.
 template <class T>
-static void launch_stage(int tm, int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
+static void launch_stage(int tm, int occ, int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
                          const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
-    switch (tm) {
-    case 17: launch_stage_tm<T, 17>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 25: launch_stage_tm<T, 25>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    default: launch_stage_tm<T, 33>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    if (a.A) {
+        switch (tm) {
+        case 17: launch_stage_modes<T, 17, 3, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+        case 25: launch_stage_modes<T, 25, 2, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+        default: launch_stage_modes<T, 33, 2, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+        }
+        return;
+    }
+    switch (tm * 10 + occ) {
+    case 173: launch_stage_modes<T, 17, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 174: launch_stage_modes<T, 17, 4, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 252: launch_stage_modes<T, 25, 2, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 253: launch_stage_modes<T, 25, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 254: launch_stage_modes<T, 25, 4, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 333: launch_stage_modes<T, 33, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    default: launch_stage_modes<T, 33, 2, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
     }
 }
 
@@ -1075,12 +1104,12 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     const int M = c->cfg.n_members;
-    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
+    launch_co2contra<T>(c->tile, c->occ, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
         launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
-        launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+        launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                         (T *)cmp, c->dims, mv, a, c->stream);
         c->launches += 3;
         return;
@@ -1102,7 +1131,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
              (T *)c->adt, c->dims, av, mv, dtm);
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
-    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+    launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                     (T *)cmp, c->dims, mv, a, c->stream);
     c->launches += 8;
 }
@@ -1127,10 +1156,10 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     const int M = c->cfg.n_members;
     if (c->elem == 8)
-        launch_co2contra<double>(c->tile, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
+        launch_co2contra<double>(c->tile, c->occ, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
                                  c->m64.v, c->stream);
     else
-        launch_co2contra<float>(c->tile, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
+        launch_co2contra<float>(c->tile, c->occ, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
                                 c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
@@ -1292,11 +1321,11 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     Dims d1 = c->dims;
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
+        launch_co2contra<double>(c->tile, c->occ, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
                                  c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(c->tile, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
+        launch_co2contra<float>(c->tile, c->occ, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
                                 c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
@@ -1335,13 +1364,13 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
 {
     const int M = c->cfg.n_members;
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(c->tile, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    launch_co2contra<T>(c->tile, c->occ, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
     launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
              (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<T>(c->tile, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
+    launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
                     c->dims, mv, a, c->stream);
     cudaEventRecord(e3, c->stream);
@@ -1592,11 +1621,11 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    launch_co2contra<double>(33, 1, vin, W, ES, dm, mv, st);
+    launch_co2contra<double>(33, 2, 1, vin, W, ES, dm, mv, st);
     launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
              mv, (const double *)nullptr);
     StageArgs a{0, 0.0, Hp, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<double>(33, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
+    launch_stage<double>(33, 2, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }
@@ -1610,11 +1639,17 @@ static void drop_graph(swe_ctx *c)
     if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
 }
 
+static void set_cfg(swe_ctx *c, int tile, int occ)
+{
+    if (c->tile != tile || c->occ != occ) drop_graph(c);
+    c->tile = tile;
+    c->occ = occ;
+}
+
 extern "C" int swe_set_tile(swe_ctx *c, int tile)
 {
     if (!c || !valid_tile(tile)) return SWE_EINVAL;
-    if (c->tile != tile) drop_graph(c);
-    c->tile = tile;
+    set_cfg(c, tile, default_occ(tile));
     return SWE_OK;
 }
 
@@ -1625,32 +1660,50 @@ extern "C" int swe_get_tile(const swe_ctx *c, int *tile)
     return SWE_OK;
 }
 
+extern "C" int swe_set_kernel_config(swe_ctx *c, int tile, int blocks_per_sm)
+{
+    if (!c || !valid_cfg(tile, blocks_per_sm)) return SWE_EINVAL;
+    set_cfg(c, tile, blocks_per_sm);
+    return SWE_OK;
+}
+
+extern "C" int swe_get_kernel_config(const swe_ctx *c, int *tile, int *blocks_per_sm)
+{
+    if (!c || !tile || !blocks_per_sm) return SWE_EINVAL;
+    *tile = c->tile;
+    *blocks_per_sm = c->occ;
+    return SWE_OK;
+}
+
 namespace {
 struct TuneKey {
-    int device, N, precision, members;
+    int device, N, precision, members, op;
     bool operator==(const TuneKey &o) const
     {
-        return device == o.device && N == o.N && precision == o.precision && members == o.members;
+        return device == o.device && N == o.N && precision == o.precision && members == o.members && op == o.op;
     }
 };
 struct TuneEntry {
     TuneKey key;
-    int tile;
+    int tile, occ;
     double ms[3];
 };
 std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
 }  // namespace
 
-// Time RK4 steps of a zero state for every built tile size and keep the fastest.
-// The state lives in a scratch vector of this context; the caller's states are
-// not touched.  Results are cached per (device, N, precision, members).
+// Time RK4 steps of a zero state for every built kernel configuration (tile edge
+// and blocks per SM; the advective operator's stage kernel exists for one
+// configuration per tile) and keep the fastest.  The state lives in a scratch
+// vector of this context; the caller's states are not touched.  ms_per_step gets
+// the best time of each tile edge.  Results are cached per (device, N, precision,
+// members, operator).
 extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_per_step)
 {
     if (!c || nreps < 1) return SWE_EINVAL;
-    const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members};
+    const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind};
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {
-            swe_set_tile(c, e.tile);
+            set_cfg(c, e.tile, e.occ);
             if (best_tile) *best_tile = e.tile;
             if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = e.ms[k];
             return SWE_OK;
@@ -1658,16 +1711,18 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     swe_stvec *v = nullptr;
     int rc = swe_stvec_create(c, &v);
     if (rc) return rc;
-    const int keep = c->tile;
-    double ms[3];
-    int best = keep;
+    const int keep_tile = c->tile, keep_occ = c->occ;
+    double ms[3] = {1e300, 1e300, 1e300};
+    int best_t = keep_tile, best_o = keep_occ;
     double best_ms = 1e300;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     rc = SWE_OK;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(c, SWE_ECUDA, "autotune events");
     const double dt = 1.0;
-    for (int k = 0; k < 3 && rc == SWE_OK; k++) {
-        swe_set_tile(c, k_tiles[k]);
+    for (int k = 0; k < N_CFGS && rc == SWE_OK; k++) {
+        const KernelCfg kc = k_cfgs[k];
+        if (c->adv && kc.occ != default_occ(kc.tile)) continue;
+        set_cfg(c, kc.tile, kc.occ);
         if ((rc = swe_rk4_steps(c, v, dt, 2)) != SWE_OK) break;
         if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
         if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
@@ -1677,18 +1732,20 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
             rc = fail(c, SWE_ECUDA, "autotune timing");
             break;
         }
-        ms[k] = t / nreps;
-        if (ms[k] < best_ms) { best_ms = ms[k]; best = k_tiles[k]; }
+        const double m = t / nreps;
+        const int ti = kc.tile == 17 ? 0 : (kc.tile == 25 ? 1 : 2);
+        ms[ti] = std::min(ms[ti], m);
+        if (m < best_ms) { best_ms = m; best_t = kc.tile; best_o = kc.occ; }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     swe_stvec_destroy(v);
     drop_graph(c);
-    if (rc != SWE_OK) { c->tile = keep; return rc; }
-    c->tile = best;
-    TuneEntry te{key, best, {ms[0], ms[1], ms[2]}};
+    if (rc != SWE_OK) { set_cfg(c, keep_tile, keep_occ); return rc; }
+    set_cfg(c, best_t, best_o);
+    TuneEntry te{key, best_t, best_o, {ms[0], ms[1], ms[2]}};
     g_tuned.push_back(te);
-    if (best_tile) *best_tile = best;
+    if (best_tile) *best_tile = best_t;
     if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = ms[k];
     return SWE_OK;
 }

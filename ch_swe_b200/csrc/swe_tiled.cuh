@@ -121,8 +121,9 @@ struct Co2Layout {
     static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
 
-template <class T, int TM>
-__global__ void __launch_bounds__(STAGE_THREADS, 2) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
+// OCC: resident blocks per SM the register allocation is capped for (autotuned).
+template <class T, int TM, int OCC>
+__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
                                                                  T *__restrict__ ES, Dims d, MetricView<T> m,
                                                                  const double *__restrict__ dtm)
 {
@@ -284,8 +285,8 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
 // ADV: the advective operator (divergence of the mass flux a.F, tendencies a.A,
 // gradient of the pre-averaging boundary h a.HB); false: the linear operator.
-template <class T, int TM, int MODE, bool ADV>
-__global__ void __launch_bounds__(STAGE_THREADS, TM <= 17 ? 3 : 2) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
+template <class T, int TM, int OCC, int MODE, bool ADV>
+__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
 {

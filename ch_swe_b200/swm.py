@@ -121,6 +121,19 @@ class Domain:
     def tile(self, value: int):
         check(_lib.load().swe_set_tile(self.ctx, int(value)), self.ctx, "swe_set_tile")
 
+    @property
+    def kernel_config(self) -> tuple:
+        """(tile edge, resident blocks per SM) of the stage kernels."""
+        t, o = ctypes.c_int(), ctypes.c_int()
+        check(_lib.load().swe_get_kernel_config(self.ctx, ctypes.byref(t), ctypes.byref(o)), self.ctx,
+              "swe_get_kernel_config")
+        return t.value, o.value
+
+    @kernel_config.setter
+    def kernel_config(self, value):
+        check(_lib.load().swe_set_kernel_config(self.ctx, int(value[0]), int(value[1])), self.ctx,
+              "swe_set_kernel_config")
+
     def autotune(self, nreps: int = 20) -> dict:
         """Time RK4 steps for every tile size, keep the fastest; returns {tile: ms per step}."""
         best = ctypes.c_int()

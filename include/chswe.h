@@ -136,11 +136,18 @@ int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *
    MPI partitions of the panels (src/parallel/partition_mod.f90:83-129). */
 int swe_set_tile(swe_ctx *ctx, int tile);
 int swe_get_tile(const swe_ctx *ctx, int *tile);
-/* Autotuner: times nreps graph-replayed RK4 steps of a scratch state for each tile
-   size (17, 25, 33), keeps the fastest on the context and returns it; ms_per_step
-   (3 entries, may be NULL) receives each size's time per step.  Results are cached
-   for the process per (device, N, precision, members).  The caller's states are not
-   touched. */
+/* Kernel configuration: tile edge and the resident blocks per SM that the stage
+   kernels' register allocation is capped for.  Built pairs: (17, 3), (17, 4), (25, 2),
+   (25, 3), (25, 4), (33, 2), (33, 3); swe_set_tile picks (17, 3), (25, 2) or (33, 2).
+   The advective operator's stage kernel always uses the tile's first pair.  No
+   reference counterpart. */
+int swe_set_kernel_config(swe_ctx *ctx, int tile, int blocks_per_sm);
+int swe_get_kernel_config(const swe_ctx *ctx, int *tile, int *blocks_per_sm);
+/* Autotuner: times nreps graph-replayed RK4 steps of a scratch state for each built
+   kernel configuration, keeps the fastest on the context and returns its tile;
+   ms_per_step (3 entries, may be NULL) receives the best time per step of tiles 17,
+   25 and 33.  Results are cached for the process per (device, N, precision, members,
+   operator).  The caller's states are not touched. */
 int swe_autotune(swe_ctx *ctx, int nreps, int *best_tile, double *ms_per_step);
 
 /* Largest cube size swe_operator_apply_noalloc accepts (its scratch is a static device

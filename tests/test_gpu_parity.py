@@ -73,6 +73,28 @@ def test_apply_parity_fp64_every_tile(tile, N):
         assert rel(g, r) < FP64_RTOL, (tile, name, rel(g, r))
 
 
+@pytest.mark.parametrize("cfg", [(17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2), (33, 3)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_every_kernel_config_matches_oracle(cfg, precision):
+    """Every built (tile, blocks-per-SM) configuration: one apply against the oracle."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
+    from oracle.oracle import Oracle
+    N = 26
+    h, u, v = random_state(N, 77)
+    ref = Oracle(N, h_mean=1000.0).apply(h, u, v)
+    dom = create_domain(N, precision=precision, h_mean=1000.0)
+    dom.kernel_config = cfg
+    assert dom.kernel_config == cfg
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
+    x = create_stvec_swm(dom).upload(h, u, v)
+    y = create_stvec_swm(dom)
+    op.apply(y, x, dom)
+    tol = FP64_RTOL if precision == "fp64" else 1e-5
+    for g, r, name in zip(y.download(), ref, "huv"):
+        assert rel(g, r) < tol, (cfg, precision, name, rel(g, r))
+    dom.destroy()
+
+
 @pytest.mark.parametrize("tile", [17, 25, 33])
 def test_rk4_every_tile_fp64(tile):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
