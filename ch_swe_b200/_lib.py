@@ -98,8 +98,9 @@ def load(path: str = LIB_PATH):
     L.swe_set_tile.argtypes = [_vp, ctypes.c_int]
     L.swe_get_tile.argtypes = [_vp, ctypes.POINTER(ctypes.c_int)]
     L.swe_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
-    L.swe_set_kernel_config.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
-    L.swe_get_kernel_config.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.swe_set_kernel_config.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.swe_get_kernel_config.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
     for name in EXPORTED:
         if not hasattr(L, name):
             raise SweError(f"libchswe.so does not export {name}")

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchswe.so")
 SOURCES = ["swe_api.cu"]
-DEPS = ["swe_api.cu", "swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh"]
+DEPS = ["swe_api.cu", "swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh", "swe_advective.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,7 +33,10 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+    # the device code is one large translation unit of templated kernels: let nvcc
+    # optimise its kernels in parallel on the host's cores
+    split = ["--split-compile", str(max(1, min(8, os.cpu_count() or 1)))]
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", *split, "-Xcompiler", "-fPIC", "-shared",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", LIB + ".tmp",
            *[os.path.join(CSRC, s) for s in SOURCES]]
     if verbose:

@@ -229,6 +229,7 @@ struct swe_ctx {
     int graph_kernels = 0, graphk_kernels = 0;
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
     int occ = 2;                     // resident blocks per SM of the stage kernels' register cap
+    int runs = 0;                    // 1: stencil runs of several outputs per thread
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
     // advective operator (cfg.operator_kind == SWE_OP_ADVECTIVE)
@@ -273,20 +274,28 @@ static bool g_tables_ready[64] = {false};
 // tiles per direction always fit, whatever N.
 static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
 // Kernel configurations the stage kernels are built for: (maximal tile edge,
-// resident blocks per SM the register allocation is capped for).  The advective
-// operator's stage kernel is built for the first configuration of each tile only.
+// resident blocks per SM the register allocation is capped for, stencil runs of
+// several outputs per thread or one).  The advective operator's stage kernel is
+// built for the first blocks-per-SM value of each tile only.
+#define CHSWE_LINEAR_CFGS(X)                                                                                  \
+    X(17, 3, 0) X(17, 4, 0) X(25, 2, 0) X(25, 3, 0) X(25, 4, 0) X(33, 2, 0) X(33, 3, 0) X(17, 3, 1) X(17, 4, 1) \
+        X(25, 2, 1) X(25, 3, 1) X(25, 4, 1) X(33, 2, 1) X(33, 3, 1)
+#define CHSWE_ADV_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0) X(17, 3, 1) X(25, 2, 1) X(33, 2, 1)
 struct KernelCfg {
-    int tile, occ;
+    int tile, occ, runs;
 };
-static const KernelCfg k_cfgs[] = {{17, 3}, {17, 4}, {25, 2}, {25, 3}, {25, 4}, {33, 2}, {33, 3}};
+#define CHSWE_CFG_ENTRY(TM, OCC, RUNS) {TM, OCC, RUNS},
+static const KernelCfg k_cfgs[] = {CHSWE_LINEAR_CFGS(CHSWE_CFG_ENTRY)};
+#undef CHSWE_CFG_ENTRY
 static const int N_CFGS = sizeof(k_cfgs) / sizeof(k_cfgs[0]);
 static int default_occ(int tm) { return tm == 17 ? 3 : 2; }
-static bool valid_cfg(int tm, int occ)
+static bool valid_cfg(int tm, int occ, int runs)
 {
     for (const KernelCfg &k : k_cfgs)
-        if (k.tile == tm && k.occ == occ) return true;
+        if (k.tile == tm && k.occ == occ && k.runs == runs) return true;
     return false;
 }
+static constexpr int cfg_code(int tm, int occ, int runs) { return tm * 100 + occ * 10 + runs; }
 // Default before autotuning: tiles of about 24 points for the smaller cubes.
 static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
@@ -987,25 +996,15 @@ static dim3 stage_grid(int N, int members, int tm)
 
 // The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
 // device and element type (the attribute belongs to the device's context).
-template <class T, int TM, int OCC, bool ADV>
+template <class T, int TM, int OCC, bool ADV, bool RUNS>
 static cudaError_t stage_smem_optin_modes()
 {
     const int sb = (int)StageLayout<T, TM>::bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    return e;
-}
-
-template <class T, int TM, int OCC>
-static cudaError_t stage_smem_optin_cfg()
-{
-    cudaError_t e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Co2Layout<T, TM>::bytes());
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false>();
-    if (e == cudaSuccess && OCC == (TM == 17 ? 3 : 2)) e = stage_smem_optin_modes<T, TM, OCC, true>();
+    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     return e;
 }
 
@@ -1017,76 +1016,73 @@ static cudaError_t stage_smem_optin()
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && done[dev]) return cudaSuccess;
-    e = stage_smem_optin_cfg<T, 17, 3>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 17, 4>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 2>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 3>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 25, 4>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 33, 2>();
-    if (e == cudaSuccess) e = stage_smem_optin_cfg<T, 33, 3>();
+#define CHSWE_OPTIN_LIN(TM, OCC, RUNS)                                                                        \
+    if (e == cudaSuccess)                                                                                     \
+        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)Co2Layout<T, TM>::bytes());                                            \
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS>();
+#define CHSWE_OPTIN_ADV(TM, OCC, RUNS) \
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, true, RUNS>();
+    CHSWE_LINEAR_CFGS(CHSWE_OPTIN_LIN)
+    CHSWE_ADV_CFGS(CHSWE_OPTIN_ADV)
+#undef CHSWE_OPTIN_LIN
+#undef CHSWE_OPTIN_ADV
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
-template <class T, int TM, int OCC>
-static void launch_co2contra_cfg(int members, const T *y, T *w, T *es, const Dims &d, const MetricView<T> &m,
-                                 cudaStream_t st, const double *dtm)
-{
-    launch_k(k_co2contra<T, TM, OCC>, stage_grid(d.N, members, TM), stage_block(), Co2Layout<T, TM>::bytes(), st, y, w,
-             es, d, m, dtm);
-}
-
 template <class T>
-static void launch_co2contra(int tm, int occ, int members, const T *y, T *w, T *es, const Dims &d,
+static void launch_co2contra(int tm, int occ, int runs, int members, const T *y, T *w, T *es, const Dims &d,
                              const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
-    switch (tm * 10 + occ) {
-    case 173: launch_co2contra_cfg<T, 17, 3>(members, y, w, es, d, m, st, dtm); break;
-    case 174: launch_co2contra_cfg<T, 17, 4>(members, y, w, es, d, m, st, dtm); break;
-    case 252: launch_co2contra_cfg<T, 25, 2>(members, y, w, es, d, m, st, dtm); break;
-    case 253: launch_co2contra_cfg<T, 25, 3>(members, y, w, es, d, m, st, dtm); break;
-    case 254: launch_co2contra_cfg<T, 25, 4>(members, y, w, es, d, m, st, dtm); break;
-    case 333: launch_co2contra_cfg<T, 33, 3>(members, y, w, es, d, m, st, dtm); break;
-    default: launch_co2contra_cfg<T, 33, 2>(members, y, w, es, d, m, st, dtm); break;
+    const dim3 g = stage_grid(d.N, members, tm);
+    switch (cfg_code(tm, occ, runs)) {
+#define CHSWE_CO2_CASE(TM, OCC, RUNS)                                                                             \
+    case cfg_code(TM, OCC, RUNS):                                                                             \
+        launch_k(k_co2contra<T, TM, OCC, RUNS>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
+                 dtm);                                                                                        \
+        break;
+        CHSWE_LINEAR_CFGS(CHSWE_CO2_CASE)
+#undef CHSWE_CO2_CASE
+    default: break;   // configurations are validated when set
     }
 }
 
-template <class T, int TM, int OCC, bool ADV>
+template <class T, int TM, int OCC, bool ADV, bool RUNS>
 static void launch_stage_modes(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
                                const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
     const dim3 g = stage_grid(d.N, members, TM);
     const size_t sb = StageLayout<T, TM>::bytes();
     switch (a.mode) {
-    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: launch_k(k_stage<T, TM, OCC, 4, ADV>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: launch_k(k_stage<T, TM, OCC, 4, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
     }
 }
 
-// The advective variant exists for the first configuration of each tile only.
+// The advective variant exists for the first blocks-per-SM value of each tile only.
 template <class T>
-static void launch_stage(int tm, int occ, int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
-                         const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+static void launch_stage(int tm, int occ, int runs, int members, const T *y, const T *w, const T *e, T *v0, T *y1,
+                         T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
-    if (a.A) {
-        switch (tm) {
-        case 17: launch_stage_modes<T, 17, 3, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-        case 25: launch_stage_modes<T, 25, 2, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-        default: launch_stage_modes<T, 33, 2, true>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-        }
-        return;
-    }
-    switch (tm * 10 + occ) {
-    case 173: launch_stage_modes<T, 17, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 174: launch_stage_modes<T, 17, 4, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 252: launch_stage_modes<T, 25, 2, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 253: launch_stage_modes<T, 25, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 254: launch_stage_modes<T, 25, 4, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 333: launch_stage_modes<T, 33, 3, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    default: launch_stage_modes<T, 33, 2, false>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    if (a.A) occ = default_occ(tm);
+    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0)) {
+#define CHSWE_STAGE_CASE(TM, OCC, RUNS)                                                                        \
+    case cfg_code(TM, OCC, RUNS):                                                                          \
+        launch_stage_modes<T, TM, OCC, false, RUNS>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);      \
+        break;
+#define CHSWE_STAGE_CASE_ADV(TM, OCC, RUNS)                                                                    \
+    case 10000 + cfg_code(TM, OCC, RUNS):                                                                  \
+        launch_stage_modes<T, TM, OCC, true, RUNS>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);       \
+        break;
+        CHSWE_LINEAR_CFGS(CHSWE_STAGE_CASE)
+        CHSWE_ADV_CFGS(CHSWE_STAGE_CASE_ADV)
+#undef CHSWE_STAGE_CASE
+#undef CHSWE_STAGE_CASE_ADV
+    default: break;   // configurations are validated when set
     }
 }
 
@@ -1104,12 +1100,12 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     const int M = c->cfg.n_members;
-    launch_co2contra<T>(c->tile, c->occ, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
+    launch_co2contra<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
         launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
-        launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+        launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                         (T *)cmp, c->dims, mv, a, c->stream);
         c->launches += 3;
         return;
@@ -1131,7 +1127,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
              (T *)c->adt, c->dims, av, mv, dtm);
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
-    launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+    launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                     (T *)cmp, c->dims, mv, a, c->stream);
     c->launches += 8;
 }
@@ -1156,10 +1152,10 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     const int M = c->cfg.n_members;
     if (c->elem == 8)
-        launch_co2contra<double>(c->tile, c->occ, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
+        launch_co2contra<double>(c->tile, c->occ, c->runs, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
                                  c->m64.v, c->stream);
     else
-        launch_co2contra<float>(c->tile, c->occ, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
+        launch_co2contra<float>(c->tile, c->occ, c->runs, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
                                 c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
@@ -1321,11 +1317,11 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     Dims d1 = c->dims;
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, c->occ, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
+        launch_co2contra<double>(c->tile, c->occ, c->runs, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
                                  c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(c->tile, c->occ, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
+        launch_co2contra<float>(c->tile, c->occ, c->runs, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
                                 c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
@@ -1364,13 +1360,13 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
 {
     const int M = c->cfg.n_members;
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(c->tile, c->occ, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    launch_co2contra<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
     launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
              (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<T>(c->tile, c->occ, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
+    launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
                     c->dims, mv, a, c->stream);
     cudaEventRecord(e3, c->stream);
@@ -1621,11 +1617,11 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    launch_co2contra<double>(33, 2, 1, vin, W, ES, dm, mv, st);
+    launch_co2contra<double>(33, 2, 0, 1, vin, W, ES, dm, mv, st);
     launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
              mv, (const double *)nullptr);
     StageArgs a{0, 0.0, Hp, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<double>(33, 2, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
+    launch_stage<double>(33, 2, 0, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }
@@ -1639,17 +1635,18 @@ static void drop_graph(swe_ctx *c)
     if (c->graphk) { cudaGraphExecDestroy(c->graphk); c->graphk = nullptr; }
 }
 
-static void set_cfg(swe_ctx *c, int tile, int occ)
+static void set_cfg(swe_ctx *c, int tile, int occ, int runs)
 {
-    if (c->tile != tile || c->occ != occ) drop_graph(c);
+    if (c->tile != tile || c->occ != occ || c->runs != runs) drop_graph(c);
     c->tile = tile;
     c->occ = occ;
+    c->runs = runs;
 }
 
 extern "C" int swe_set_tile(swe_ctx *c, int tile)
 {
     if (!c || !valid_tile(tile)) return SWE_EINVAL;
-    set_cfg(c, tile, default_occ(tile));
+    set_cfg(c, tile, default_occ(tile), 0);
     return SWE_OK;
 }
 
@@ -1660,18 +1657,19 @@ extern "C" int swe_get_tile(const swe_ctx *c, int *tile)
     return SWE_OK;
 }
 
-extern "C" int swe_set_kernel_config(swe_ctx *c, int tile, int blocks_per_sm)
+extern "C" int swe_set_kernel_config(swe_ctx *c, int tile, int blocks_per_sm, int runs)
 {
-    if (!c || !valid_cfg(tile, blocks_per_sm)) return SWE_EINVAL;
-    set_cfg(c, tile, blocks_per_sm);
+    if (!c || !valid_cfg(tile, blocks_per_sm, runs)) return SWE_EINVAL;
+    set_cfg(c, tile, blocks_per_sm, runs);
     return SWE_OK;
 }
 
-extern "C" int swe_get_kernel_config(const swe_ctx *c, int *tile, int *blocks_per_sm)
+extern "C" int swe_get_kernel_config(const swe_ctx *c, int *tile, int *blocks_per_sm, int *runs)
 {
-    if (!c || !tile || !blocks_per_sm) return SWE_EINVAL;
+    if (!c || !tile || !blocks_per_sm || !runs) return SWE_EINVAL;
     *tile = c->tile;
     *blocks_per_sm = c->occ;
+    *runs = c->runs;
     return SWE_OK;
 }
 
@@ -1685,7 +1683,7 @@ struct TuneKey {
 };
 struct TuneEntry {
     TuneKey key;
-    int tile, occ;
+    int tile, occ, runs;
     double ms[3];
 };
 std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
@@ -1703,7 +1701,7 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind};
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {
-            set_cfg(c, e.tile, e.occ);
+            set_cfg(c, e.tile, e.occ, e.runs);
             if (best_tile) *best_tile = e.tile;
             if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = e.ms[k];
             return SWE_OK;
@@ -1711,9 +1709,9 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     swe_stvec *v = nullptr;
     int rc = swe_stvec_create(c, &v);
     if (rc) return rc;
-    const int keep_tile = c->tile, keep_occ = c->occ;
+    const int keep_tile = c->tile, keep_occ = c->occ, keep_runs = c->runs;
     double ms[3] = {1e300, 1e300, 1e300};
-    int best_t = keep_tile, best_o = keep_occ;
+    int best_t = keep_tile, best_o = keep_occ, best_r = keep_runs;
     double best_ms = 1e300;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     rc = SWE_OK;
@@ -1722,7 +1720,7 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     for (int k = 0; k < N_CFGS && rc == SWE_OK; k++) {
         const KernelCfg kc = k_cfgs[k];
         if (c->adv && kc.occ != default_occ(kc.tile)) continue;
-        set_cfg(c, kc.tile, kc.occ);
+        set_cfg(c, kc.tile, kc.occ, kc.runs);
         if ((rc = swe_rk4_steps(c, v, dt, 2)) != SWE_OK) break;
         if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
         if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
@@ -1735,15 +1733,15 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
         const double m = t / nreps;
         const int ti = kc.tile == 17 ? 0 : (kc.tile == 25 ? 1 : 2);
         ms[ti] = std::min(ms[ti], m);
-        if (m < best_ms) { best_ms = m; best_t = kc.tile; best_o = kc.occ; }
+        if (m < best_ms) { best_ms = m; best_t = kc.tile; best_o = kc.occ; best_r = kc.runs; }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     swe_stvec_destroy(v);
     drop_graph(c);
-    if (rc != SWE_OK) { set_cfg(c, keep_tile, keep_occ); return rc; }
-    set_cfg(c, best_t, best_o);
-    TuneEntry te{key, best_t, best_o, {ms[0], ms[1], ms[2]}};
+    if (rc != SWE_OK) { set_cfg(c, keep_tile, keep_occ, keep_runs); return rc; }
+    set_cfg(c, best_t, best_o, best_r);
+    TuneEntry te{key, best_t, best_o, best_r, {ms[0], ms[1], ms[2]}};
     g_tuned.push_back(te);
     if (best_tile) *best_tile = best_t;
     if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = ms[k];

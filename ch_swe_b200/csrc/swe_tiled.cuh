@@ -38,11 +38,20 @@ struct Tile {
     static constexpr int IT_WIN = ((TM + 5) * (TM + 5) + STAGE_THREADS - 1) / STAGE_THREADS;
     static constexpr int IT_STRIP = ((TM + 5) * TM + STAGE_THREADS - 1) / STAGE_THREADS;
     static constexpr int IT_TILE = (TM * TM + STAGE_THREADS - 1) / STAGE_THREADS;
+    // run-blocked kernel variant: runs of RBW (passes over tile + 5 cross lines) or RBT
+    // (tile cross lines) outputs along the stencil direction, the longest runs that
+    // keep every pass within one item per thread
+    static constexpr int RBW = TM == 17 ? 2 : (TM == 25 ? 4 : 6);
+    static constexpr int RBT = TM == 17 ? 2 : (TM == 25 ? 3 : 5);
 };
 
-#define CHSWE_TILE_CONSTANTS(TM)                                                                           \
+// RUNS = false gives runs of one output: the flat element-per-thread passes.
+#define CHSWE_TILE_CONSTANTS(TM, RUNS)                                                                     \
     constexpr int PW = Tile<TM>::PW, PT = Tile<TM>::PT, RW = Tile<TM>::RW, IT_WIN = Tile<TM>::IT_WIN,      \
-                  IT_STRIP = Tile<TM>::IT_STRIP, IT_TILE = Tile<TM>::IT_TILE;                               \
+                  IT_STRIP = Tile<TM>::IT_STRIP, RBW = (RUNS) ? Tile<TM>::RBW : 1,                          \
+                  RBT = (RUNS) ? Tile<TM>::RBT : 1,                                                         \
+                  IT_RW = ((TM + 5) * ((TM + RBW - 1) / RBW) + STAGE_THREADS - 1) / STAGE_THREADS,          \
+                  IT_RT = (TM * ((TM + RBT - 1) / RBT) + STAGE_THREADS - 1) / STAGE_THREADS;                \
     (void)RW
 
 __device__ __forceinline__ void tile_range(int n, int &i0, int &i1, int &j0, int &j1)
@@ -105,6 +114,32 @@ template <class T> __device__ __forceinline__ T di2c_u(int k, int n, const Line<
     return (k >= 4 && k <= n - 3) ? di2c_in<T>(k, f) : di2c<T>(k, n, f);
 }
 
+// Stencil runs.  A pass gives every thread whole runs of RB consecutive outputs
+// along the stencil direction at one cross index; lanes take consecutive cross
+// indices, so shared-memory accesses are conflict-free (odd pitches) and the closure
+// tests are warp-uniform.  A run clear of the SBP closures loads its RB + 3 inputs
+// once and evaluates the interior rows on registers; other runs (closures, or
+// shorter than RB at the end of a tile) go output by output.  RB = 1 is the flat
+// one-output-per-element form.
+// v[m] = f(k0 + O + m): O = -2 for the centres->nodes rows (taps k-2..k+1), O = -1
+// for the nodes->centres rows (taps k-1..k+2); the interior formulas then coincide.
+template <class T, int RB, int O>
+__device__ __forceinline__ void run_load(const Line<T> &f, int k0, T (&v)[RB + 3])
+{
+#pragma unroll
+    for (int m = 0; m < RB + 3; m++) v[m] = f(k0 + O + m);
+}
+template <class T, int RB>
+__device__ __forceinline__ T run_interp(const T (&v)[RB + 3], int m)
+{
+    return (T(9) * (v[m + 2] + v[m + 1]) - (v[m + 3] + v[m])) * T(0.0625);
+}
+template <class T, int RB>
+__device__ __forceinline__ T run_diff(const T (&v)[RB + 3], int m)
+{
+    return (T(27) * (v[m + 2] - v[m + 1]) - (v[m + 3] - v[m])) * T(1.0 / 24.0);
+}
+
 // Every global load of a pass is issued into registers before the first
 // shared-memory store or stencil of that pass (fixed-trip unrolled loops), so a
 // block pays one memory round trip per batch instead of one per loop iteration.
@@ -121,15 +156,16 @@ struct Co2Layout {
     static constexpr size_t bytes() { return sizeof(T) * TOTAL; }
 };
 
-// OCC: resident blocks per SM the register allocation is capped for (autotuned).
-template <class T, int TM, int OCC>
+// OCC: resident blocks per SM the register allocation is capped for; RUNS: stencil
+// runs of several outputs per thread (both autotuned).
+template <class T, int TM, int OCC, bool RUNS>
 __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
                                                                  T *__restrict__ ES, Dims d, MetricView<T> m,
                                                                  const double *__restrict__ dtm)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = Co2Layout<T, TM>;
-    CHSWE_TILE_CONSTANTS(TM);
+    CHSWE_TILE_CONSTANTS(TM, RUNS);
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -144,15 +180,27 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
     const SWin<T, PW> sv{sm + L::V, i0 - 2, j0 - 3}, su{sm + L::U, i0 - 3, j0 - 2}, svq{sm + L::VQ, i0 - 2, j0};
     const SWin<T, PT> suq{sm + L::UQ, i0, j0 - 2}, sux{sm + L::UX, i0, j0};
 
+    // runs along the tile width / height: window passes (RBW), tile passes (RBT)
+    const int nww = (tw + RBW - 1) / RBW, nhw = (th + RBW - 1) / RBW, nwt = (tw + RBT - 1) / RBT,
+              nht = (th + RBT - 1) / RBT;
+
     // ---- before the predecessor grid completes: J Qi12 at both xy intermediates (metric only)
     pdl_trigger();
-    T jq1[IT_STRIP], jq2[IT_STRIP];
+    T jq1[IT_RW][RBW], jq2[IT_STRIP];
+#pragma unroll
+    for (int it = 0; it < IT_RW; it++) {
+        const int q = threadIdx.x + it * STAGE_THREADS;
+        int r, x;
+        split(q, w5, iw5, r, x);
+        const int l0 = j0 + r * RBW;
+#pragma unroll
+        for (int mm = 0; mm < RBW; mm++)
+            jq1[it][mm] = q < w5 * nhw && l0 + mm < j1 ? __ldg(m.JQ12 + box_off(P, sv.x0 + x, l0 + mm)) : T(0);
+    }
 #pragma unroll
     for (int it = 0; it < IT_STRIP; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
         int r, c;
-        split(q, w5, iw5, r, c);
-        jq1[it] = q < w5 * th ? __ldg(m.JQ12 + box_off(P, sv.x0 + c, j0 + r)) : T(0);
         split(q, tw, iw, r, c);
         jq2[it] = q < tw * h5 ? __ldg(m.JQ12 + box_off(P, i0 + c, suq.y0 + r)) : T(0);
     }
@@ -181,49 +229,91 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
             }
         }
     }
-    // ---- batch 2 (in flight during the passes): the output metric
-    T q11[IT_TILE], ijy[IT_TILE], q22[IT_TILE], ijx[IT_TILE];
+    // ---- batch 2 (in flight during the passes): the output metric, by output run
+    T q11[IT_RT][RBT], ijy[IT_RT][RBT], q22[IT_RT][RBT], ijx[IT_RT][RBT];
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        const int64_t o = box_off(P, i, j);
-        const bool ok = q < tw * th;
-        q11[it] = ok && i <= N ? __ldg(m.Q11y + o) : T(0);
-        ijy[it] = ok && i <= N ? __ldg(m.iJy + o) : T(0);
-        q22[it] = ok && j <= N ? __ldg(m.Q22x + o) : T(0);
-        ijx[it] = ok && j <= N ? __ldg(m.iJx + o) : T(0);
+        int r, x;
+        split(q, tw, iw, r, x);
+        const int i = i0 + x, jr = j0 + r * RBT;
+#pragma unroll
+        for (int mm = 0; mm < RBT; mm++) {
+            const int j = jr + mm;
+            const int64_t o = box_off(P, i, j);
+            const bool ok = q < tw * nht && j < j1;
+            q11[it][mm] = ok && i <= N ? __ldg(m.Q11y + o) : T(0);
+            ijy[it][mm] = ok && i <= N ? __ldg(m.iJy + o) : T(0);
+            q22[it][mm] = ok && j <= N ? __ldg(m.Q22x + o) : T(0);
+            ijx[it][mm] = ok && j <= N ? __ldg(m.iJx + o) : T(0);
+        }
     }
     __syncthreads();
-    // J Qi12 I_c2i,y(v) at xy nodes: row-major (y stencil, warp-uniform closure)
+    // J Qi12 I_c2i,y(v) at xy nodes: columns of the window, runs along the tile rows
 #pragma unroll
-    for (int it = 0; it < IT_STRIP; it++) {
+    for (int it = 0; it < IT_RW; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, w5, iw5, r, c);
-        const int k = sv.x0 + c, l = j0 + r;
-        if (q < w5 * th) svq.at(k, l) = ic2i_u<T>(l, n, sv.col(k)) * jq1[it];
+        int r, x;
+        split(q, w5, iw5, r, x);
+        if (q >= w5 * nhw) continue;
+        const int k = sv.x0 + x, l0 = j0 + r * RBW, cnt = min(RBW, j1 - l0);
+        const Line<T> col = sv.col(k);
+        T *o = &svq.at(k, l0);
+        if (cnt == RBW && l0 >= 5 && l0 + RBW - 1 <= n - 4) {
+            T v[RBW + 3];
+            run_load<T, RBW, -2>(col, l0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = run_interp<T, RBW>(v, mm) * jq1[it][mm];
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++)
+                if (mm < cnt) o[mm * PW] = ic2i_u<T>(l0 + mm, n, col) * jq1[it][mm];
+        }
     }
-    // I_c2i,x(u) at xy nodes: column-major (x stencil); the J Qi12 factor follows
+    // I_c2i,x(u) at xy nodes: rows of the window, runs along the tile columns; the
+    // J Qi12 factor follows
 #pragma unroll
-    for (int it = 0; it < IT_STRIP; it++) {
+    for (int it = 0; it < IT_RW; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int c, r;
-        split(q, h5, ih5, c, r);
-        const int k = i0 + c, l = suq.y0 + r;
-        if (q < tw * h5) suq.at(k, l) = ic2i_u<T>(k, n, su.row(l));
+        int r, x;
+        split(q, h5, ih5, r, x);
+        if (q >= h5 * nww) continue;
+        const int l = suq.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
+        const Line<T> row = su.row(l);
+        T *o = &suq.at(k0, l);
+        if (cnt == RBW && k0 >= 5 && k0 + RBW - 1 <= n - 4) {
+            T v[RBW + 3];
+            run_load<T, RBW, -2>(row, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++)
+                if (mm < cnt) o[mm] = ic2i_u<T>(k0 + mm, n, row);
+        }
     }
     __syncthreads();
-    // I_i2c,x of the first: column-major
+    // I_i2c,x of the first: tile rows, runs along the tile columns (u points, i <= N)
+    const int iu1 = min(i1, n);
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int c, r;
-        split(q, th, ih, c, r);
-        const int i = i0 + c, j = j0 + r;
-        if (q < tw * th && i <= N) sux.at(i, j) = ii2c_u<T>(i, N, svq.row(j));
+        int r, x;
+        split(q, th, ih, r, x);
+        if (q >= th * nwt) continue;
+        const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
+        const Line<T> row = svq.row(j);
+        T *o = &sux.at(k0, j);
+        if (cnt == RBT && k0 >= 4 && k0 + RBT - 1 <= N - 3) {
+            T v[RBT + 3];
+            run_load<T, RBT, -1>(row, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) o[mm] = run_interp<T, RBT>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++)
+                if (mm < cnt) o[mm] = ii2c_u<T>(k0 + mm, N, row);
+        }
     }
     // J Qi12 factor of the second: row-major, in place
 #pragma unroll
@@ -234,18 +324,34 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         if (q < tw * h5) suq.at(i0 + c, suq.y0 + r) *= jq2[it];
     }
     __syncthreads();
-    // outputs: row-major, I_i2c,y of the second (warp-uniform closure), coalesced stores
+    // outputs: tile columns, runs along the tile rows (I_i2c,y of the second); lanes
+    // store consecutive columns of a row (coalesced)
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        const int64_t o = box_off(P, i, j);
-        if (q < tw * th) {
+        int r, x;
+        split(q, tw, iw, r, x);
+        if (q >= tw * nht) continue;
+        const int i = i0 + x, jr = j0 + r * RBT, cnt = min(RBT, j1 - jr);
+        const Line<T> col = suq.col(i);
+        T vi[RBT];
+        if (cnt == RBT && jr >= 4 && jr + RBT - 1 <= N - 3) {
+            T v[RBT + 3];
+            run_load<T, RBT, -1>(col, jr, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) vi[mm] = run_interp<T, RBT>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) vi[mm] = (mm < cnt && jr + mm <= N) ? ii2c_u<T>(jr + mm, N, col) : T(0);
+        }
+#pragma unroll
+        for (int mm = 0; mm < RBT; mm++) {
+            if (mm >= cnt) continue;
+            const int j = jr + mm;
+            const int64_t o = box_off(P, i, j);
             // the edge strips (k_edge reads them contiguous along each side)
             if (i <= N) {
-                const T ut = q11[it] * su.at(i, j) + sux.at(i, j) * ijy[it];
+                const T ut = q11[it][mm] * su.at(i, j) + sux.at(i, j) * ijy[it][mm];
                 w[d.fs + o] = ut;
                 if (i <= 3) es[(SIDE_L * 4 + i - 1) * n + j] = ut;
                 if (i >= N - 2) es[(SIDE_R * 4 + N - i) * n + j] = ut;
@@ -253,7 +359,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
                 if (j == n) es[(SIDE_T * 4 + 3) * n + i] = ut;
             }
             if (j <= N) {
-                const T vt = q22[it] * sv.at(i, j) + ii2c_u<T>(j, N, suq.col(i)) * ijx[it];
+                const T vt = q22[it][mm] * sv.at(i, j) + vi[mm] * ijx[it][mm];
                 w[2 * d.fs + o] = vt;
                 if (j <= 3) es[(SIDE_B * 4 + j - 1) * n + i] = vt;
                 if (j >= N - 2) es[(SIDE_T * 4 + N - j) * n + i] = vt;
@@ -285,7 +391,7 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
 // ADV: the advective operator (divergence of the mass flux a.F, tendencies a.A,
 // gradient of the pre-averaging boundary h a.HB); false: the linear operator.
-template <class T, int TM, int OCC, int MODE, bool ADV>
+template <class T, int TM, int OCC, int MODE, bool ADV, bool RUNS>
 __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
@@ -293,7 +399,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     using namespace sbp;
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = StageLayout<T, TM>;
-    CHSWE_TILE_CONSTANTS(TM);
+    CHSWE_TILE_CONSTANTS(TM, RUNS);
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -314,6 +420,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
     const T *fJ2 = m.fJ2 + t * d.ps;
     const bool sat_l = i0 <= 3, sat_r = i1 - 1 >= N - 2, sat_b = j0 <= 3, sat_t = j1 - 1 >= N - 2;
+    // runs along the tile width / height: window passes (RBW), tile passes (RBT)
+    const int nww = (tw + RBW - 1) / RBW, nhw = (th + RBW - 1) / RBW, nwt = (tw + RBT - 1) / RBT,
+              nht = (th + RBT - 1) / RBT;
 
     pdl_trigger();
     pdl_wait();
@@ -361,7 +470,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     }
     // ---- batch 1b: vt window with J vt, the h halos across the panel edges, and
     // fJ2 (or the synchronised edge value) for the up / vp passes
-    T f1[IT_STRIP], f2[IT_STRIP];
+    T f1[IT_RW][RBW], f2[IT_STRIP];
     {
         const int64_t ov = box_off(P, svt.x0, svt.y0);
         const T *gv = wp + 2 * d.fs + ov, *gjx = m.Jx + ov;
@@ -396,17 +505,25 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             if (sat_t) hy1 = halo(SIDE_T, i0 + q);
         }
 #pragma unroll
+        for (int it = 0; it < IT_RW; it++) {
+            const int qq = threadIdx.x + it * STAGE_THREADS;
+            int r, x;
+            split(qq, w5, iw5, r, x);
+            const int k = sup.x0 + x, l0 = j0 + r * RBW;
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) {
+                const int l = l0 + mm;
+                if (qq >= w5 * nhw || l >= j1) f1[it][mm] = T(0);
+                else if (on_boundary(k, l, n)) f1[it][mm] = (k >= 1 && k <= n) ? edge_entry(E, N, mem, t, k, l)[0] : T(0);
+                else f1[it][mm] = __ldg(fJ2 + box_off(P, k, l));
+            }
+        }
+#pragma unroll
         for (int it = 0; it < IT_STRIP; it++) {
             const int qq = threadIdx.x + it * STAGE_THREADS;
             int r, c;
-            split(qq, w5, iw5, r, c);
-            int k = sup.x0 + c, l = j0 + r;
-            if (qq >= w5 * th) f1[it] = T(0);
-            else if (on_boundary(k, l, n)) f1[it] = (k >= 1 && k <= n) ? edge_entry(E, N, mem, t, k, l)[0] : T(0);
-            else f1[it] = __ldg(fJ2 + box_off(P, k, l));
             split(qq, tw, iw, r, c);
-            k = i0 + c;
-            l = svp.y0 + r;
+            const int k = i0 + c, l = svp.y0 + r;
             if (qq >= tw * h5) f2[it] = T(0);
             else if (l >= 1 && l <= n && on_boundary(k, l, n)) f2[it] = edge_entry(E, N, mem, t, k, l)[1];
             else f2[it] = __ldg(fJ2 + box_off(P, k, l));
@@ -426,71 +543,136 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     }
 
     // ---- batch 2 (in flight during the passes): the final pass's metric, or the
-    // synchronised divergence on the panel boundary
-    T mja[IT_TILE], mjy[IT_TILE], mjx[IT_TILE];
+    // synchronised divergence on the panel boundary, by output run
+    T mja[IT_RT][RBT], mjy[IT_RT][RBT], mjx[IT_RT][RBT];
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        const int64_t o = box_off(P, i, j);
-        const bool ok = q < tw * th, hu = ok && i <= N, hv = ok && j <= N;
-        mja[it] = !ok ? T(0) : on_boundary(i, j, n) ? edge_entry(E, N, mem, t, i, j)[2] : __ldg(m.iJa + o);
-        mjy[it] = hu ? __ldg(m.iJy + o) : T(0);
-        mjx[it] = hv ? __ldg(m.iJx + o) : T(0);
+        int r, x;
+        split(q, tw, iw, r, x);
+        const int i = i0 + x, jr = j0 + r * RBT;
+#pragma unroll
+        for (int mm = 0; mm < RBT; mm++) {
+            const int j = jr + mm;
+            const int64_t o = box_off(P, i, j);
+            const bool ok = q < tw * nht && j < j1, hu = ok && i <= N, hv = ok && j <= N;
+            mja[it][mm] = !ok ? T(0) : on_boundary(i, j, n) ? edge_entry(E, N, mem, t, i, j)[2] : __ldg(m.iJa + o);
+            mjy[it][mm] = hu ? __ldg(m.iJy + o) : T(0);
+            mjx[it][mm] = hv ? __ldg(m.iJx + o) : T(0);
+        }
     }
     __syncthreads();
 
-    // ---- P1 (row-major): up = fJ2 I_c2i,y(vt) on the tile rows, tile columns +- footprint
+    // ---- P1: up = fJ2 I_c2i,y(vt): columns of the up window, runs along the tile rows
 #pragma unroll
-    for (int it = 0; it < IT_STRIP; it++) {
+    for (int it = 0; it < IT_RW; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, w5, iw5, r, c);
-        const int k = sup.x0 + c, l = j0 + r;
-        if (q < w5 * th) sup.at(k, l) = on_boundary(k, l, n) ? f1[it] : f1[it] * ic2i_u<T>(l, n, svt.col(k));
+        int r, x;
+        split(q, w5, iw5, r, x);
+        if (q >= w5 * nhw) continue;
+        const int k = sup.x0 + x, l0 = j0 + r * RBW, cnt = min(RBW, j1 - l0);
+        const Line<T> col = svt.col(k);
+        T *o = &sup.at(k, l0);
+        if (k == 1 || k == n) {
+            // panel-boundary column: the synchronised values
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++)
+                if (mm < cnt) o[mm * PW] = f1[it][mm];
+        } else if (cnt == RBW && l0 >= 5 && l0 + RBW - 1 <= n - 4) {
+            T v[RBW + 3];
+            run_load<T, RBW, -2>(col, l0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = f1[it][mm] * run_interp<T, RBW>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) {
+                const int l = l0 + mm;
+                if (mm < cnt) o[mm * PW] = on_boundary(k, l, n) ? f1[it][mm] : f1[it][mm] * ic2i_u<T>(l, n, col);
+            }
+        }
     }
-    // ---- P2 (column-major): I_c2i,x(ut) on the tile columns, tile rows +- footprint
+    // ---- P2: I_c2i,x(ut): rows of the vp window, runs along the tile columns
 #pragma unroll
-    for (int it = 0; it < IT_STRIP; it++) {
+    for (int it = 0; it < IT_RW; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int c, r;
-        split(q, h5, ih5, c, r);
-        const int k = i0 + c, l = svp.y0 + r;
-        if (q < tw * h5) svp.at(k, l) = ic2i_u<T>(k, n, sut.row(l));
+        int r, x;
+        split(q, h5, ih5, r, x);
+        if (q >= h5 * nww) continue;
+        const int l = svp.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
+        const Line<T> row = sut.row(l);
+        T *o = &svp.at(k0, l);
+        if (cnt == RBW && k0 >= 5 && k0 + RBW - 1 <= n - 4) {
+            T v[RBW + 3];
+            run_load<T, RBW, -2>(row, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBW; mm++)
+                if (mm < cnt) o[mm] = ic2i_u<T>(k0 + mm, n, row);
+        }
     }
-    // ---- P3 (column-major): x part of the divergence, c2i difference of J ut
+    // ---- P3: x part of the divergence, c2i difference of J ut: tile rows, runs along columns
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int c, r;
-        split(q, th, ih, c, r);
-        if (q < tw * th) sdx.at(i0 + c, j0 + r) = dc2i_u<T>(i0 + c, n, sju.row(j0 + r));
+        int r, x;
+        split(q, th, ih, r, x);
+        if (q >= th * nwt) continue;
+        const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, i1 - k0);
+        const Line<T> row = sju.row(j);
+        T *o = &sdx.at(k0, j);
+        if (cnt == RBT && k0 >= 5 && k0 + RBT - 1 <= n - 4) {
+            T v[RBT + 3];
+            run_load<T, RBT, -2>(row, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) o[mm] = run_diff<T, RBT>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++)
+                if (mm < cnt) o[mm] = dc2i_u<T>(k0 + mm, n, row);
+        }
     }
     __syncthreads();
-    // ---- P4 (column-major): -g grad_x h (with SAT) and I_i2c,x(up); the second goes to the
-    // dead ut window and is scaled by 1/J in the final row-major pass
+    // ---- P4: -g grad_x h (with SAT) and I_i2c,x(up) on the u points: tile rows, runs
+    // along the columns; the second goes to the dead ut window and is scaled by 1/J
+    // in the final pass
     const SWin<T, PT> scx{sm + L::UT, i0, j0};
+    const int iu1 = min(i1, n);
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int c, r;
-        split(q, th, ih, c, r);
-        const int i = i0 + c, j = j0 + r;
-        if (q < tw * th && i <= N) {
-            const Line<T> hrow = sh.row(j);
-            T gx = di2c_u<T>(i, N, hrow);
-            if (i <= 3) {
-                const T sat = i == 1 ? T(SATI1) : (i == 2 ? T(SATI2) : T(SATI3));
-                gx += sat * (hrow(1) - hl[r]);
+        int r, x;
+        split(q, th, ih, r, x);
+        if (q >= th * nwt) continue;
+        const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
+        const Line<T> hrow = sh.row(j), prow = sup.row(j);
+        T *og = &skx.at(k0, j), *oc = &scx.at(k0, j);
+        if (cnt == RBT && k0 >= 4 && k0 + RBT - 1 <= N - 3) {
+            T v[RBT + 3];
+            run_load<T, RBT, -1>(hrow, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) og[mm] = -m.grav * (run_diff<T, RBT>(v, mm) * m.inv_hxa);
+            run_load<T, RBT, -1>(prow, k0, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) oc[mm] = run_interp<T, RBT>(v, mm);
+        } else {
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) {
+                if (mm >= cnt) continue;
+                const int i = k0 + mm;
+                T gx = di2c_u<T>(i, N, hrow);
+                if (i <= 3) {
+                    const T sat = i == 1 ? T(SATI1) : (i == 2 ? T(SATI2) : T(SATI3));
+                    gx += sat * (hrow(1) - hl[x]);
+                }
+                if (i >= N - 2) {
+                    const T sat = i == N ? T(SATI1) : (i == N - 1 ? T(SATI2) : T(SATI3));
+                    gx += sat * (hr[x] - hrow(n));
+                }
+                og[mm] = -m.grav * (gx * m.inv_hxa);
+                oc[mm] = ii2c_u<T>(i, N, prow);
             }
-            if (i >= N - 2) {
-                const T sat = i == N ? T(SATI1) : (i == N - 1 ? T(SATI2) : T(SATI3));
-                gx += sat * (hr[r] - hrow(n));
-            }
-            skx.at(i, j) = -m.grav * (gx * m.inv_hxa);
-            scx.at(i, j) = ii2c_u<T>(i, N, sup.row(j));
         }
     }
     // ---- P4b (row-major): vp = -fJ2 I_c2i,x(ut), synchronised values on the panel boundary
@@ -507,109 +689,166 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     }
     __syncthreads();
 
-    // ---- P5 (row-major): divergence and v tendency of the thread's points, then the
-    // RK4 update with all its operand loads in one batch (coalesced)
+    // ---- P5: divergence and the tendencies of the thread's points (tile columns, runs
+    // along the rows; lanes take consecutive columns, so the global accesses of the
+    // RK4 update below are coalesced row by row)
     const T H = T(a.Hm[mem]);
-    T kh[IT_TILE], ku[IT_TILE], kv[IT_TILE];
+    T kh[IT_RT][RBT], ku[IT_RT][RBT], kv[IT_RT][RBT];
+    const T *Aa = (const T *)a.A;
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        kh[it] = ku[it] = kv[it] = T(0);
-        if (q >= tw * th) continue;
-        T dvg;
-        if (on_boundary(i, j, n)) {
-            dvg = mja[it];
-        } else {
-            const T dy = dc2i_u<T>(j, n, sjv.col(i));
-            dvg = (sdx.at(i, j) * m.inv_hx + dy * m.inv_hx) * mja[it];
+        int r, x;
+        split(q, tw, iw, r, x);
+        const int i = i0 + x, jr = j0 + r * RBT, cnt = q < tw * nht ? min(RBT, j1 - jr) : 0;
+#pragma unroll
+        for (int mm = 0; mm < RBT; mm++) kh[it][mm] = ku[it][mm] = kv[it][mm] = T(0);
+        if (cnt <= 0) continue;
+        const Line<T> dcol = sjv.col(i), hcol = sh.col(i), pcol = svp.col(i);
+        if (cnt == RBT && jr >= 5 && jr + RBT - 1 <= N - 3) {
+            // rows clear of the closures, the SAT terms and the panel-boundary rows
+            const bool bcol = (i == 1 || i == n), hasu = i <= N;
+            T v[RBT + 3];
+            run_load<T, RBT, -2>(dcol, jr, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) {
+                const T dvg = bcol ? mja[it][mm]
+                                   : (sdx.at(i, jr + mm) * m.inv_hx + run_diff<T, RBT>(v, mm) * m.inv_hx) * mja[it][mm];
+                kh[it][mm] = -H * dvg;
+            }
+            if (hasu) {
+#pragma unroll
+                for (int mm = 0; mm < RBT; mm++) {
+                    const int j = jr + mm;
+                    if constexpr (ADV) {
+                        const T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
+                        ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
+                    } else {
+                        ku[it][mm] = skx.at(i, j) + scx.at(i, j) * mjy[it][mm];
+                    }
+                }
+            }
+            run_load<T, RBT, -1>(hcol, jr, v);
+            T gy[RBT];
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) gy[mm] = run_diff<T, RBT>(v, mm) * m.inv_hxa;
+            run_load<T, RBT, -1>(pcol, jr, v);
+#pragma unroll
+            for (int mm = 0; mm < RBT; mm++) {
+                if constexpr (ADV) {
+                    const int j = jr + mm;
+                    T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
+                    if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
+                    kv[it][mm] = (av + -m.grav * gy[mm]) + run_interp<T, RBT>(v, mm) * mjx[it][mm];
+                } else {
+                    kv[it][mm] = -m.grav * gy[mm] + run_interp<T, RBT>(v, mm) * mjx[it][mm];
+                }
+            }
+            continue;
         }
-        kh[it] = -H * dvg;
-        const T *Aa = (const T *)a.A;
-        if (i <= N) {
-            if constexpr (ADV) {
-                // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
-                T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
-                if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
-                ku[it] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it];
+#pragma unroll
+        for (int mm = 0; mm < RBT; mm++) {
+            if (mm >= cnt) continue;
+            const int j = jr + mm;
+            T dvg;
+            if (on_boundary(i, j, n)) {
+                dvg = mja[it][mm];
             } else {
-                ku[it] = skx.at(i, j) + scx.at(i, j) * mjy[it];
+                const T dy = dc2i_u<T>(j, n, dcol);
+                dvg = (sdx.at(i, j) * m.inv_hx + dy * m.inv_hx) * mja[it][mm];
             }
-        }
-        if (j <= N) {
-            const Line<T> hcol = sh.col(i);
-            T gy = di2c_u<T>(j, N, hcol);
-            if (j <= 3) {
-                const T sat = j == 1 ? T(SATI1) : (j == 2 ? T(SATI2) : T(SATI3));
-                gy += sat * (hcol(1) - hb[c]);
+            kh[it][mm] = -H * dvg;
+            if (i <= N) {
+                if constexpr (ADV) {
+                    // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
+                    T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
+                    if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
+                    ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
+                } else {
+                    ku[it][mm] = skx.at(i, j) + scx.at(i, j) * mjy[it][mm];
+                }
             }
-            if (j >= N - 2) {
-                const T sat = j == N ? T(SATI1) : (j == N - 1 ? T(SATI2) : T(SATI3));
-                gy += sat * (ht[c] - hcol(n));
-            }
-            gy = gy * m.inv_hxa;
-            if constexpr (ADV) {
-                T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
-                if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
-                kv[it] = (av + -m.grav * gy) + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
-            } else {
-                kv[it] = -m.grav * gy + ii2c_u<T>(j, N, svp.col(i)) * mjx[it];
+            if (j <= N) {
+                T gy = di2c_u<T>(j, N, hcol);
+                if (j <= 3) {
+                    const T sat = j == 1 ? T(SATI1) : (j == 2 ? T(SATI2) : T(SATI3));
+                    gy += sat * (hcol(1) - hb[x]);
+                }
+                if (j >= N - 2) {
+                    const T sat = j == N ? T(SATI1) : (j == N - 1 ? T(SATI2) : T(SATI3));
+                    gy += sat * (ht[x] - hcol(n));
+                }
+                gy = gy * m.inv_hxa;
+                if constexpr (ADV) {
+                    T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
+                    if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
+                    kv[it][mm] = (av + -m.grav * gy) + ii2c_u<T>(j, N, pcol) * mjx[it][mm];
+                } else {
+                    kv[it][mm] = -m.grav * gy + ii2c_u<T>(j, N, pcol) * mjx[it][mm];
+                }
             }
         }
     }
 
+    // ---- RK4 update, all operand loads of the thread in one batch
     T *v0 = V0 + mo + t * d.ps, *y1 = Y1 + mo + t * d.ps, *acc = ACC + mo + t * d.ps;
     T *cmp = CMP ? CMP + mo + t * d.ps : nullptr;
     const int64_t fs = d.fs;
     const T dt = T(a.dtm ? a.dtm[mem] : a.dt);
     constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
-    T pv[3][IT_TILE], pa[3][IT_TILE], pc[3][IT_TILE];
+    T pv[3][IT_RT][RBT], pa[3][IT_RT][RBT], pc[3][IT_RT][RBT];
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        const int64_t o = box_off(P, i, j);
-        const bool ok = q < tw * th;
-        const bool has[3] = {ok, ok && i <= N, ok && j <= N};
+        int r, x;
+        split(q, tw, iw, r, x);
+        const int i = i0 + x, jr = j0 + r * RBT, cnt = q < tw * nht ? min(RBT, j1 - jr) : 0;
 #pragma unroll
-        for (int f = 0; f < 3; f++) {
-            pv[f][it] = LV && has[f] ? v0[o + f * fs] : T(0);
-            pa[f][it] = LA && has[f] ? acc[o + f * fs] : T(0);
-            pc[f][it] = LC && has[f] ? cmp[o + f * fs] : T(0);
+        for (int mm = 0; mm < RBT; mm++) {
+            const int j = jr + mm;
+            const int64_t o = box_off(P, i, j);
+            const bool ok = mm < cnt;
+            const bool has[3] = {ok, ok && i <= N, ok && j <= N};
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                pv[f][it][mm] = LV && has[f] ? v0[o + f * fs] : T(0);
+                pa[f][it][mm] = LA && has[f] ? acc[o + f * fs] : T(0);
+                pc[f][it][mm] = LC && has[f] ? cmp[o + f * fs] : T(0);
+            }
         }
     }
 #pragma unroll
-    for (int it = 0; it < IT_TILE; it++) {
+    for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
-        int r, c;
-        split(q, tw, iw, r, c);
-        const int i = i0 + c, j = j0 + r;
-        const int64_t o = box_off(P, i, j);
-        const bool ok = q < tw * th;
-        const bool has[3] = {ok, ok && i <= N, ok && j <= N};
-        const T k3[3] = {kh[it], ku[it], kv[it]};
+        int r, x;
+        split(q, tw, iw, r, x);
+        const int i = i0 + x, jr = j0 + r * RBT, cnt = q < tw * nht ? min(RBT, j1 - jr) : 0;
 #pragma unroll
-        for (int f = 0; f < 3; f++) {
-            if (!has[f]) continue;
-            const int64_t of = o + f * fs;
-            if constexpr (MODE == 0) {
-                y1[of] = k3[f];
-            } else if constexpr (MODE <= 3) {
-                const T ca = (MODE == 3) ? dt : T(0.5) * dt;
-                const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
-                y1[of] = pv[f][it] + ca * k3[f];
-                acc[of] = (MODE == 1) ? cb * k3[f] : pa[f][it] + cb * k3[f];
-            } else if constexpr (sizeof(T) == 4) {
-                float sv = pv[f][it], cv = pc[f][it];
-                kahan_add(sv, cv, pa[f][it] + (dt / T(6)) * k3[f]);
-                v0[of] = sv;
-                cmp[of] = cv;
-            } else {
-                v0[of] = pv[f][it] + (pa[f][it] + (dt / T(6)) * k3[f]);
+        for (int mm = 0; mm < RBT; mm++) {
+            const int j = jr + mm;
+            const int64_t o = box_off(P, i, j);
+            const bool ok = mm < cnt;
+            const bool has[3] = {ok, ok && i <= N, ok && j <= N};
+            const T k3[3] = {kh[it][mm], ku[it][mm], kv[it][mm]};
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (!has[f]) continue;
+                const int64_t of = o + f * fs;
+                if constexpr (MODE == 0) {
+                    y1[of] = k3[f];
+                } else if constexpr (MODE <= 3) {
+                    const T ca = (MODE == 3) ? dt : T(0.5) * dt;
+                    const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
+                    y1[of] = pv[f][it][mm] + ca * k3[f];
+                    acc[of] = (MODE == 1) ? cb * k3[f] : pa[f][it][mm] + cb * k3[f];
+                } else if constexpr (sizeof(T) == 4) {
+                    float sv = pv[f][it][mm], cv = pc[f][it][mm];
+                    kahan_add(sv, cv, pa[f][it][mm] + (dt / T(6)) * k3[f]);
+                    v0[of] = sv;
+                    cmp[of] = cv;
+                } else {
+                    v0[of] = pv[f][it][mm] + (pa[f][it][mm] + (dt / T(6)) * k3[f]);
+                }
             }
         }
     }

@@ -121,17 +121,24 @@ class Domain:
     def tile(self, value: int):
         check(_lib.load().swe_set_tile(self.ctx, int(value)), self.ctx, "swe_set_tile")
 
+    # built stage-kernel configurations: (tile edge, resident blocks per SM, runs)
+    KERNEL_CONFIGS = tuple((t, o, r) for r in (0, 1)
+                           for t, o in ((17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2), (33, 3)))
+
     @property
     def kernel_config(self) -> tuple:
-        """(tile edge, resident blocks per SM) of the stage kernels."""
-        t, o = ctypes.c_int(), ctypes.c_int()
-        check(_lib.load().swe_get_kernel_config(self.ctx, ctypes.byref(t), ctypes.byref(o)), self.ctx,
-              "swe_get_kernel_config")
-        return t.value, o.value
+        """(tile edge, resident blocks per SM, runs) of the stage kernels; runs 1: each
+        thread evaluates runs of consecutive outputs along a stencil."""
+        t, o, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(_lib.load().swe_get_kernel_config(self.ctx, ctypes.byref(t), ctypes.byref(o), ctypes.byref(r)),
+              self.ctx, "swe_get_kernel_config")
+        return t.value, o.value, r.value
 
     @kernel_config.setter
     def kernel_config(self, value):
-        check(_lib.load().swe_set_kernel_config(self.ctx, int(value[0]), int(value[1])), self.ctx,
+        """(tile, blocks per SM) or (tile, blocks per SM, runs); runs defaults to 0."""
+        runs = int(value[2]) if len(value) > 2 else 0
+        check(_lib.load().swe_set_kernel_config(self.ctx, int(value[0]), int(value[1]), runs), self.ctx,
               "swe_set_kernel_config")
 
     def autotune(self, nreps: int = 20) -> dict:

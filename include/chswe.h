@@ -136,13 +136,15 @@ int swe_kernel_times(swe_ctx *ctx, swe_stvec *v0, double dt, int nreps, double *
    MPI partitions of the panels (src/parallel/partition_mod.f90:83-129). */
 int swe_set_tile(swe_ctx *ctx, int tile);
 int swe_get_tile(const swe_ctx *ctx, int *tile);
-/* Kernel configuration: tile edge and the resident blocks per SM that the stage
-   kernels' register allocation is capped for.  Built pairs: (17, 3), (17, 4), (25, 2),
-   (25, 3), (25, 4), (33, 2), (33, 3); swe_set_tile picks (17, 3), (25, 2) or (33, 2).
-   The advective operator's stage kernel always uses the tile's first pair.  No
-   reference counterpart. */
-int swe_set_kernel_config(swe_ctx *ctx, int tile, int blocks_per_sm);
-int swe_get_kernel_config(const swe_ctx *ctx, int *tile, int *blocks_per_sm);
+/* Kernel configuration: tile edge, the resident blocks per SM that the stage
+   kernels' register allocation is capped for, and runs (1: each thread evaluates
+   runs of several consecutive outputs along a stencil, 0: one output per element).
+   Built (tile, blocks) pairs: (17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2),
+   (33, 3), each with runs 0 and 1; swe_set_tile picks (17, 3, 0), (25, 2, 0) or
+   (33, 2, 0).  The advective operator's stage kernel always uses the tile's first
+   blocks-per-SM value.  No reference counterpart. */
+int swe_set_kernel_config(swe_ctx *ctx, int tile, int blocks_per_sm, int runs);
+int swe_get_kernel_config(const swe_ctx *ctx, int *tile, int *blocks_per_sm, int *runs);
 /* Autotuner: times nreps graph-replayed RK4 steps of a scratch state for each built
    kernel configuration, keeps the fastest on the context and returns its tile;
    ms_per_step (3 entries, may be NULL) receives the best time per step of tiles 17,

@@ -41,11 +41,11 @@ def smooth_state(o, seed):
     return h, u, v
 
 
-def gpu_apply(N, state, precision="fp64", tile=None, axis=(0.0, 0.0, 1.0)):
+def gpu_apply(N, state, precision="fp64", tile=None, axis=(0.0, 0.0, 1.0), runs=0):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
     dom = create_domain(N, precision=precision, operator="advective", rotation_axis=axis)
     if tile:
-        dom.tile = tile
+        dom.kernel_config = (tile, 3 if tile == 17 else 2, runs)
     op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
     x = create_stvec_swm(dom).upload(*state)
     y = create_stvec_swm(dom)
@@ -65,16 +65,18 @@ def test_apply_parity_fp64_random(N):
         assert rel(g, r) < FP64_RTOL, (N, name, rel(g, r))
 
 
+@pytest.mark.parametrize("runs", [0, 1])
 @pytest.mark.parametrize("tile", [17, 25, 33])
-def test_apply_parity_fp64_smooth_every_tile(tile):
+def test_apply_parity_fp64_smooth_every_tile(tile, runs):
+    """Every built advective stage configuration (tile, with and without stencil runs)."""
     from oracle.oracle import Oracle
     N = 26
     o = Oracle(N, h_mean=H0, operator="advective")
     st = smooth_state(o, 7)
     ref = o.apply(*st)
-    got = gpu_apply(N, st, tile=tile)
+    got = gpu_apply(N, st, tile=tile, runs=runs)
     for g, r, name in zip(got, ref, "huv"):
-        assert rel(g, r) < FP64_RTOL, (tile, name, rel(g, r))
+        assert rel(g, r) < FP64_RTOL, (tile, runs, name, rel(g, r))
 
 
 def test_rk4_williamson2_tilted_fp64_matches_oracle():

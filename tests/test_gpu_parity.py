@@ -73,10 +73,14 @@ def test_apply_parity_fp64_every_tile(tile, N):
         assert rel(g, r) < FP64_RTOL, (tile, name, rel(g, r))
 
 
-@pytest.mark.parametrize("cfg", [(17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2), (33, 3)])
+KERNEL_CONFIGS = [(t, o, r) for r in (0, 1)
+                  for t, o in ((17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2), (33, 3))]
+
+
+@pytest.mark.parametrize("cfg", KERNEL_CONFIGS)
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_every_kernel_config_matches_oracle(cfg, precision):
-    """Every built (tile, blocks-per-SM) configuration: one apply against the oracle."""
+    """Every built (tile, blocks-per-SM, runs) configuration: one apply against the oracle."""
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
     from oracle.oracle import Oracle
     N = 26
