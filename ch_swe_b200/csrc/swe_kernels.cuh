@@ -236,69 +236,86 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
     pdl_trigger();
-    pdl_wait();
+    // phase-1 task of this thread: raw quantity rq of the copy of panel rp, side rs,
+    // along index rb (one call site keeps the kernel's code small: every block runs
+    // once per SM on a cold instruction cache)
+    int rp = -1, rs = 0, rb = 0, rq = 0, dst = 0;
     if (warp < 8) {
-        const int a = a0 + lane, q = warp & 3;
+        const int a = a0 + lane;
+        rq = warp & 3;
         if (a < a1) {
-            const Strips<T> &S = q < 2 ? Sc : Sd;
             if (warp < 4) {
-                raw[0][q][lane] = edge_raw(S, m, t, s, a, q);
+                rp = t; rs = s; rb = a;
+                dst = rq * EDGE_CHUNK + lane;
             } else {
                 const Link L = c_link[t][s];
-                raw[xs ? 1 : 2][q][lane] = edge_raw(S, m, L.nb, L.nside, nb_along(L, n, a), q);
+                rp = L.nb; rs = L.nside; rb = nb_along(L, n, a);
+                dst = ((xs ? 1 : 2) * 4 + rq) * EDGE_CHUNK + lane;
             }
         }
     } else if (lane < 8) {
         // the other neighbour of the corner vertices a = 1 and a = N+1
-        const int a = lane < 4 ? 1 : n, q = lane & 3;
+        const int a = lane < 4 ? 1 : n;
+        rq = lane & 3;
         if (a >= a0 && a < a1) {
             int k, l;
             side_vertex(N, s, a, 0, k, l);
             const int s2 = xs ? (l == 1 ? SIDE_B : SIDE_T) : (k == 1 ? SIDE_L : SIDE_R);
             const Link L2 = c_link[t][s2];
-            raw[xs ? 2 : 1][q][a - a0] = edge_raw(q < 2 ? Sc : Sd, m, L2.nb, L2.nside, nb_along(L2, n, along(s2, k, l)), q);
+            rp = L2.nb; rs = L2.nside; rb = nb_along(L2, n, along(s2, k, l));
+            dst = ((xs ? 2 : 1) * 4 + rq) * EDGE_CHUNK + (a - a0);
         }
     }
-    __syncthreads();
-    if (threadIdx.x >= a1 - a0) return;
-    const int v = threadIdx.x, a = a0 + v;
-    int k, l;
-    side_vertex(N, s, a, 0, k, l);
-    const bool il = (k == 1), ir = (k == n), ib = (l == 1), it = (l == n);
+    // phase-2 metric of this thread's vertex, before the predecessor grid completes
+    const int v = threadIdx.x, av = a0 + v;
+    int kv = 1, lv = 1;
+    if (av < a1) side_vertex(N, s, av, 0, kv, lv);
+    const bool il = (kv == 1), ir = (kv == n), ib = (lv == 1), it = (lv == n);
     const bool cx = il || ir, cy = ib || it;
+    T ea0 = 0, eax = 0, eay = 0, qx = 0, qy = 0;
+    if (av < a1) {
+        ea0 = m.ea[s * n + av - 1];
+        if (cx) {
+            const Link L = c_link[t][il ? SIDE_L : SIDE_R];
+            eax = m.ea[L.nside * n + nb_along(L, n, lv) - 1];
+            qx = __ldg((il ? m.ql : m.qr) + lv - 1);
+        }
+        if (cy) {
+            const Link L = c_link[t][ib ? SIDE_B : SIDE_T];
+            eay = m.ea[L.nside * n + nb_along(L, n, kv) - 1];
+            qy = __ldg((ib ? m.qb : m.qt) + kv - 1);
+        }
+    }
+    pdl_wait();
+    if (rp >= 0) (&raw[0][0][0])[dst] = edge_raw(rq < 2 ? Sc : Sd, m, rp, rs, rb, rq);
+    __syncthreads();
+    if (av >= a1) return;
     const T V = raw[0][0][v], U = raw[0][1][v];
-    const T f = (raw[0][2][v] * m.inv_hx + raw[0][3][v] * m.inv_hx) * m.ea[s * n + a - 1];
+    const T f = (raw[0][2][v] * m.inv_hx + raw[0][3][v] * m.inv_hx) * ea0;
     T uhx = 0, vhx = 0, fx = 0, uhy = 0, vhy = 0, fy = 0;
     if (cx) {
-        const int sx = il ? SIDE_L : SIDE_R;
-        const Link L = c_link[t][sx];
-        halo_vec(t, sx, raw[1][0][v], raw[1][1][v], uhx, vhx);
-        fx = (raw[1][2][v] * m.inv_hx + raw[1][3][v] * m.inv_hx) * m.ea[L.nside * n + nb_along(L, n, l) - 1];
+        halo_vec(t, il ? SIDE_L : SIDE_R, raw[1][0][v], raw[1][1][v], uhx, vhx);
+        fx = (raw[1][2][v] * m.inv_hx + raw[1][3][v] * m.inv_hx) * eax;
     }
     if (cy) {
-        const int sy = ib ? SIDE_B : SIDE_T;
-        const Link L = c_link[t][sy];
-        halo_vec(t, sy, raw[2][0][v], raw[2][1][v], uhy, vhy);
-        fy = (raw[2][2][v] * m.inv_hx + raw[2][3][v] * m.inv_hx) * m.ea[L.nside * n + nb_along(L, n, k) - 1];
+        halo_vec(t, ib ? SIDE_B : SIDE_T, raw[2][0][v], raw[2][1][v], uhy, vhy);
+        fy = (raw[2][2][v] * m.inv_hx + raw[2][3][v] * m.inv_hx) * eay;
     }
     T sup, svp, sdiv;
     if (cx && cy) {
-        const T qx = __ldg((il ? m.ql : m.qr) + l - 1), qy = __ldg((ib ? m.qb : m.qt) + k - 1);
         sup = (V + uhx + uhy + qx * vhx) / T(3);
         svp = (U + vhx + vhy + qy * uhy) / T(3);
         sdiv = (f + fx + fy) / T(3);
     } else if (cx) {
-        const T qx = __ldg((il ? m.ql : m.qr) + l - 1);
         sup = T(0.5) * (V + uhx + qx * vhx);
         svp = T(0.5) * (U + vhx);
         sdiv = T(0.5) * (f + fx);
     } else {
-        const T qy = __ldg((ib ? m.qb : m.qt) + k - 1);
         sup = T(0.5) * (V + uhy);
         svp = T(0.5) * (U + vhy + qy * uhy);
         sdiv = T(0.5) * (f + fy);
     }
-    T *e = E + edge_index(N, mem, t, s, a);
+    T *e = E + edge_index(N, mem, t, s, av);
     e[0] = sup;
     e[1] = svp;
     e[2] = sdiv;
