@@ -26,6 +26,9 @@ __host__ __device__ __forceinline__ int64_t box_off(int P, int i, int j)
 {
     return (int64_t)(j - 1 + MG) * P + (i - 1 + MG);
 }
+// The same offset in 32 bits, for device code indexing within one member's
+// state (three fields of six panel boxes stay far below 2^31 elements).
+__device__ __forceinline__ int box_off32(int P, int i, int j) { return (j - 1 + MG) * P + (i - 1 + MG); }
 
 struct Dims {
     int N;         // cells per panel edge

@@ -695,6 +695,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     const T H = T(a.Hm[mem]);
     T kh[IT_RT][RBT], ku[IT_RT][RBT], kv[IT_RT][RBT];
     const T *Aa = (const T *)a.A;
+    // advective tendencies of this panel (u, v fields), indexed in 32 bits
+    const T *Au = ADV ? Aa + mo + t * d.ps + d.fs : nullptr, *Av = ADV ? Aa + mo + t * d.ps + 2 * d.fs : nullptr;
 #pragma unroll
     for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
@@ -721,7 +723,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                 for (int mm = 0; mm < RBT; mm++) {
                     const int j = jr + mm;
                     if constexpr (ADV) {
-                        const T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
+                        const T au = __ldg(Au + box_off32(P, i, j));
                         ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
                     } else {
                         ku[it][mm] = skx.at(i, j) + scx.at(i, j) * mjy[it][mm];
@@ -737,7 +739,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             for (int mm = 0; mm < RBT; mm++) {
                 if constexpr (ADV) {
                     const int j = jr + mm;
-                    T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
+                    T av = __ldg(Av + box_off32(P, i, j));
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
                     kv[it][mm] = (av + -m.grav * gy[mm]) + run_interp<T, RBT>(v, mm) * mjx[it][mm];
                 } else {
@@ -761,7 +763,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             if (i <= N) {
                 if constexpr (ADV) {
                     // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
-                    T au = __ldg(Aa + mo + t * d.ps + d.fs + box_off(P, i, j));
+                    T au = __ldg(Au + box_off32(P, i, j));
                     if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
                     ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
                 } else {
@@ -780,7 +782,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                 }
                 gy = gy * m.inv_hxa;
                 if constexpr (ADV) {
-                    T av = __ldg(Aa + mo + t * d.ps + 2 * d.fs + box_off(P, i, j));
+                    T av = __ldg(Av + box_off32(P, i, j));
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
                     kv[it][mm] = (av + -m.grav * gy) + ii2c_u<T>(j, N, pcol) * mjx[it][mm];
                 } else {
