@@ -213,6 +213,9 @@ def profile_traffic(precision):
 
 
 def set_tile(dom, args):
+    if args.kernel_config:
+        dom.kernel_config = tuple(int(x) for x in args.kernel_config.split(","))
+        return None
     if args.tile == "auto":
         return dom.autotune(nreps=10)
     dom.tile = int(args.tile)
@@ -287,7 +290,7 @@ def run_precision(precision, ic, args, torch, dist, world):
         "total_ms": total_ms, "launches": launches, "final": final,
         "e2e_value": cells_per_step(N_CELLS) * e2e_n / e2e_s, "e2e_bytes": nbytes,
         "ms_co2contra": co.value, "ms_edge": ed.value, "ms_stage": sg.value, "dom": dom,
-        "tile": dom.tile, "tune_ms_per_rk4_step": tune,
+        "tile": dom.tile, "kernel_config": list(dom.kernel_config), "tune_ms_per_rk4_step": tune,
     }
 
 
@@ -507,7 +510,8 @@ def run_ours(args):
         "fp64": {"value": v64, "ms_per_step": r64["total_ms"] / K, "ms_stage_kernel": r64["ms_stage"],
                  "ms_co2contra_kernel": r64["ms_co2contra"], "ms_edge_kernel": r64["ms_edge"], "tile": r64["tile"],
                  "tune_ms_per_rk4_step": r64["tune_ms_per_rk4_step"]},
-        "fp32_tile": r32["tile"], "fp32_tune_ms_per_rk4_step": r32["tune_ms_per_rk4_step"],
+        "fp32_tile": r32["tile"], "fp32_kernel_config": r32["kernel_config"],
+        "fp64_kernel_config": r64["kernel_config"], "fp32_tune_ms_per_rk4_step": r32["tune_ms_per_rk4_step"],
         "fp32_kernel_ms": {"k_co2contra": r32["ms_co2contra"], "k_edge": r32["ms_edge"], "k_stage": r32["ms_stage"]},
         "fp32_over_fp64": v32 / v64,
         "fp32_vs_fp64_after_one_day": errs,
@@ -558,14 +562,17 @@ def run_profile_leg(args):
         op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
         st = create_stvec_swm(dom).upload(*workload_ic()[0])
         dt = DT
-    if tile:
+    if args.kernel_config:
+        dom.kernel_config = tuple(int(x) for x in args.kernel_config.split(","))
+    elif tile:
         dom.tile = tile
     rk = create_timescheme(st, "rk4")
     for _ in range(args.rk4_steps):
         rk.step(st, op, dom, dt)
     torch.cuda.synchronize()
+    dom_cfg = dom.kernel_config
     dom.destroy()
-    print(f"profile leg {args.profile_leg}: {args.rk4_steps} RK4 steps, tile {tile or 'default'}", flush=True)
+    print(f"profile leg {args.profile_leg}: {args.rk4_steps} RK4 steps, kernel config {dom_cfg}", flush=True)
     return 0
 
 
@@ -582,6 +589,8 @@ def main():
     ap.add_argument("--no-nonlinear", action="store_true", help="skip the nonlinear (C384 Williamson 2) leg")
     ap.add_argument("--tile", default="auto", choices=["auto", "17", "25", "33"],
                     help="stage-kernel tile size (default: autotuned per precision)")
+    ap.add_argument("--kernel-config", default=None,
+                    help="stage-kernel configuration 'tile,blocks_per_sm,runs' (overrides --tile and autotuning)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
     ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear"], default=None,
