@@ -46,6 +46,7 @@ class SweCfg(ctypes.Structure):
         ("rotation_axis", ctypes.c_double * 3),
         ("coriolis_constant", ctypes.c_int),
         ("h_mean", ctypes.c_double),
+        ("sbp_order", ctypes.c_int),
     ]
 
 

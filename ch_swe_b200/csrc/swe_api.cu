@@ -230,6 +230,7 @@ struct swe_ctx {
     int tile = 33;                   // maximal tile edge of the stage kernels (17, 25 or 33)
     int occ = 2;                     // resident blocks per SM of the stage kernels' register cap
     int runs = 0;                    // 1: stencil runs of several outputs per thread
+    int ord = 42;                    // SBP order of the Ch operators (42 or 21)
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
     // advective operator (cfg.operator_kind == SWE_OP_ADVECTIVE)
@@ -281,18 +282,31 @@ static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
     X(17, 3, 0) X(17, 4, 0) X(25, 2, 0) X(25, 3, 0) X(25, 4, 0) X(33, 2, 0) X(33, 3, 0) X(17, 3, 1) X(17, 4, 1) \
         X(25, 2, 1) X(25, 3, 1) X(25, 4, 1) X(33, 2, 1) X(33, 3, 1)
 #define CHSWE_ADV_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0) X(17, 3, 1) X(25, 2, 1) X(33, 2, 1)
+// SBP 2-1 stage kernels (linear operator): the first blocks-per-SM value of each
+// tile, one output per element.
+#define CHSWE_LINEAR21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 struct KernelCfg {
     int tile, occ, runs;
 };
 #define CHSWE_CFG_ENTRY(TM, OCC, RUNS) {TM, OCC, RUNS},
 static const KernelCfg k_cfgs[] = {CHSWE_LINEAR_CFGS(CHSWE_CFG_ENTRY)};
+static const KernelCfg k_cfgs21[] = {CHSWE_LINEAR21_CFGS(CHSWE_CFG_ENTRY)};
 #undef CHSWE_CFG_ENTRY
 static const int N_CFGS = sizeof(k_cfgs) / sizeof(k_cfgs[0]);
+static const int N_CFGS21 = sizeof(k_cfgs21) / sizeof(k_cfgs21[0]);
 static int default_occ(int tm) { return tm == 17 ? 3 : 2; }
-static bool valid_cfg(int tm, int occ, int runs)
+// the configurations built for SBP order ord
+static const KernelCfg *cfgs_of(int ord, int *count)
 {
-    for (const KernelCfg &k : k_cfgs)
-        if (k.tile == tm && k.occ == occ && k.runs == runs) return true;
+    *count = ord == 21 ? N_CFGS21 : N_CFGS;
+    return ord == 21 ? k_cfgs21 : k_cfgs;
+}
+static bool valid_cfg(int ord, int tm, int occ, int runs)
+{
+    int nc = 0;
+    const KernelCfg *cs = cfgs_of(ord, &nc);
+    for (int k = 0; k < nc; k++)
+        if (cs[k].tile == tm && cs[k].occ == occ && cs[k].runs == runs) return true;
     return false;
 }
 static constexpr int cfg_code(int tm, int occ, int runs) { return tm * 100 + occ * 10 + runs; }
@@ -612,11 +626,15 @@ static int build_quadrature(swe_ctx *c)
     const int N = c->cfg.N, P = c->dims.P;
     const size_t box = (size_t)c->dims.ps;
     std::vector<double> h(3 * box, 0.0);
-    const double AI[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
-    const double AC[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
+    // edge weights of the SBP norms: D42_A_interfaces / D42_A_centers, or D21_*
+    // (sbp_operators_collection_mod.f90:169-170,196-197)
+    const double AI42[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
+    const double AC42[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
+    const double AI21[2] = {0.5, 1.0}, AC21[2] = {1.0, 1.0};
+    const bool o21 = c->ord == 21;
     auto coeff = [&](int i, int n, bool iface) {
-        const double *e = iface ? AI : AC;
-        int ne = iface ? 5 : 4;
+        const double *e = iface ? (o21 ? AI21 : AI42) : (o21 ? AC21 : AC42);
+        int ne = o21 ? 2 : (iface ? 5 : 4);
         double A = 1.0;
         if (i <= ne) A = e[i - 1];
         if (i >= n - ne + 1) A = e[n - i];
@@ -655,6 +673,7 @@ extern "C" int swe_cfg_default(swe_cfg *cfg)
     cfg->rotation_axis[0] = 0.0; cfg->rotation_axis[1] = 0.0; cfg->rotation_axis[2] = 1.0;
     cfg->coriolis_constant = 0;
     cfg->h_mean = 1000.0;
+    cfg->sbp_order = 42;
     return SWE_OK;
 }
 
@@ -689,10 +708,15 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
         (cfg->operator_kind != SWE_OP_LINEAR && cfg->operator_kind != SWE_OP_ADVECTIVE) || !(cfg->radius > 0.0))
         return SWE_EINVAL;
+    // SBP order: 4-2 (0 selects it too) or 2-1, the latter for the linear operator
+    const int ord = cfg->sbp_order == 0 ? 42 : cfg->sbp_order;
+    if ((ord != 42 && ord != 21) || (ord == 21 && cfg->operator_kind != SWE_OP_LINEAR)) return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
     swe_ctx *c = new swe_ctx();
     c->cfg = *cfg;
+    c->cfg.sbp_order = ord;
+    c->ord = ord;
     cudaGetDevice(&c->device);
     const int N = cfg->N;
     c->dims.N = N;
@@ -703,6 +727,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     c->elem = cfg->precision == SWE_FP64 ? 8 : 4;
     c->tile = default_tile(N);
     c->occ = default_occ(c->tile);
+    c->runs = 0;
     c->box_elems = (size_t)c->dims.ms * cfg->n_members;
     int rc = SWE_OK;
     auto bail = [&](int code) { free_ctx(c); delete c; return code; };
@@ -996,15 +1021,15 @@ static dim3 stage_grid(int N, int members, int tm)
 
 // The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
 // device and element type (the attribute belongs to the device's context).
-template <class T, int TM, int OCC, bool ADV, bool RUNS>
+template <class T, int TM, int OCC, bool ADV, bool RUNS, int ORD>
 static cudaError_t stage_smem_optin_modes()
 {
     const int sb = (int)StageLayout<T, TM>::bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     return e;
 }
 
@@ -1016,72 +1041,94 @@ static cudaError_t stage_smem_optin()
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && done[dev]) return cudaSuccess;
-#define CHSWE_OPTIN_LIN(TM, OCC, RUNS)                                                                        \
-    if (e == cudaSuccess)                                                                                     \
-        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)Co2Layout<T, TM>::bytes());                                            \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS>();
+#define CHSWE_OPTIN_LIN(TM, OCC, RUNS)                                                                            \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 42>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)Co2Layout<T, TM>::bytes());                                                \
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 42>();
+#define CHSWE_OPTIN_LIN21(TM, OCC, RUNS)                                                                          \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 21>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)Co2Layout<T, TM>::bytes());                                                \
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 21>();
 #define CHSWE_OPTIN_ADV(TM, OCC, RUNS) \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, true, RUNS>();
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, true, RUNS, 42>();
     CHSWE_LINEAR_CFGS(CHSWE_OPTIN_LIN)
+    CHSWE_LINEAR21_CFGS(CHSWE_OPTIN_LIN21)
     CHSWE_ADV_CFGS(CHSWE_OPTIN_ADV)
 #undef CHSWE_OPTIN_LIN
+#undef CHSWE_OPTIN_LIN21
 #undef CHSWE_OPTIN_ADV
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
+// ord: SBP order (42 or 21); codes of order 21 are offset by 100000.
 template <class T>
-static void launch_co2contra(int tm, int occ, int runs, int members, const T *y, T *w, T *es, const Dims &d,
+static void launch_co2contra(int tm, int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                              const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
     const dim3 g = stage_grid(d.N, members, tm);
-    switch (cfg_code(tm, occ, runs)) {
-#define CHSWE_CO2_CASE(TM, OCC, RUNS)                                                                             \
-    case cfg_code(TM, OCC, RUNS):                                                                             \
-        launch_k(k_co2contra<T, TM, OCC, RUNS>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
-                 dtm);                                                                                        \
+    switch (cfg_code(tm, occ, runs) + (ord == 21 ? 100000 : 0)) {
+#define CHSWE_CO2_CASE(TM, OCC, RUNS)                                                                                 \
+    case cfg_code(TM, OCC, RUNS):                                                                                 \
+        launch_k(k_co2contra<T, TM, OCC, RUNS, 42>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
+                 dtm);                                                                                            \
+        break;
+#define CHSWE_CO2_CASE21(TM, OCC, RUNS)                                                                               \
+    case 100000 + cfg_code(TM, OCC, RUNS):                                                                        \
+        launch_k(k_co2contra<T, TM, OCC, RUNS, 21>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
+                 dtm);                                                                                            \
         break;
         CHSWE_LINEAR_CFGS(CHSWE_CO2_CASE)
+        CHSWE_LINEAR21_CFGS(CHSWE_CO2_CASE21)
 #undef CHSWE_CO2_CASE
+#undef CHSWE_CO2_CASE21
     default: break;   // configurations are validated when set
     }
 }
 
-template <class T, int TM, int OCC, bool ADV, bool RUNS>
+template <class T, int TM, int OCC, bool ADV, bool RUNS, int ORD>
 static void launch_stage_modes(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
                                const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
 {
     const dim3 g = stage_grid(d.N, members, TM);
     const size_t sb = StageLayout<T, TM>::bytes();
     switch (a.mode) {
-    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: launch_k(k_stage<T, TM, OCC, 4, ADV, RUNS>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    default: launch_k(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
     }
 }
 
 // The advective variant exists for the first blocks-per-SM value of each tile only.
 template <class T>
-static void launch_stage(int tm, int occ, int runs, int members, const T *y, const T *w, const T *e, T *v0, T *y1,
-                         T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
+static void launch_stage(int tm, int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0,
+                         T *y1, T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a,
+                         cudaStream_t st)
 {
     if (a.A) occ = default_occ(tm);
-    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0)) {
+    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0) + (ord == 21 ? 100000 : 0)) {
 #define CHSWE_STAGE_CASE(TM, OCC, RUNS)                                                                        \
     case cfg_code(TM, OCC, RUNS):                                                                          \
-        launch_stage_modes<T, TM, OCC, false, RUNS>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);      \
+        launch_stage_modes<T, TM, OCC, false, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
+        break;
+#define CHSWE_STAGE_CASE21(TM, OCC, RUNS)                                                                      \
+    case 100000 + cfg_code(TM, OCC, RUNS):                                                                 \
+        launch_stage_modes<T, TM, OCC, false, RUNS, 21>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
         break;
 #define CHSWE_STAGE_CASE_ADV(TM, OCC, RUNS)                                                                    \
     case 10000 + cfg_code(TM, OCC, RUNS):                                                                  \
-        launch_stage_modes<T, TM, OCC, true, RUNS>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);       \
+        launch_stage_modes<T, TM, OCC, true, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);   \
         break;
         CHSWE_LINEAR_CFGS(CHSWE_STAGE_CASE)
         CHSWE_ADV_CFGS(CHSWE_STAGE_CASE_ADV)
+        CHSWE_LINEAR21_CFGS(CHSWE_STAGE_CASE21)
 #undef CHSWE_STAGE_CASE
 #undef CHSWE_STAGE_CASE_ADV
+#undef CHSWE_STAGE_CASE21
     default: break;   // configurations are validated when set
     }
 }
@@ -1100,12 +1147,12 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     const int M = c->cfg.n_members;
-    launch_co2contra<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
+    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
-        launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+        launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
-        launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+        launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                         (T *)cmp, c->dims, mv, a, c->stream);
         c->launches += 3;
         return;
@@ -1118,7 +1165,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     launch_k(k_havg<T>, dim3(1 + (12 * (N - 1) + HAVG_THREADS - 1) / HAVG_THREADS, M), dim3(HAVG_THREADS), 0, c->stream,
              (T *)yin, (T *)c->hb, c->dims, dtm);
     launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
+    launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
              (T *)c->edge, c->dims, mv, dtm);
     launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
     const long long nvh = (long long)NPAN * av.hp * M;
@@ -1127,7 +1174,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
              (T *)c->adt, c->dims, av, mv, dtm);
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
-    launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                     (T *)cmp, c->dims, mv, a, c->stream);
     c->launches += 8;
 }
@@ -1152,10 +1199,10 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     const int M = c->cfg.n_members;
     if (c->elem == 8)
-        launch_co2contra<double>(c->tile, c->occ, c->runs, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
+        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
                                  c->m64.v, c->stream);
     else
-        launch_co2contra<float>(c->tile, c->occ, c->runs, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
+        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
                                 c->m32.v, c->stream);
     c->launches++;
     CU(c, cudaGetLastError());
@@ -1317,11 +1364,11 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     Dims d1 = c->dims;
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, c->occ, c->runs, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
+        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
                                  c->stream);
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(c->tile, c->occ, c->runs, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
+        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
                                 c->stream);
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
@@ -1360,13 +1407,13 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
 {
     const int M = c->cfg.n_members;
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    launch_k(k_edge<T>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+    launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
              (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<T>(c->tile, c->occ, c->runs, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
+    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
                     c->dims, mv, a, c->stream);
     cudaEventRecord(e3, c->stream);
@@ -1565,7 +1612,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         return SWE_ETOOBIG;
     }
     if (cfg->N < 8 || cfg->precision != SWE_FP64 || cfg->n_members != 1 ||
-        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0))
+        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0) || (cfg->sbp_order != 0 && cfg->sbp_order != 42))
         return SWE_EINVAL;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWE_ENODEV;
@@ -1617,11 +1664,11 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     // the contravariant scratch is read with its zero margins: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    launch_co2contra<double>(33, 2, 0, 1, vin, W, ES, dm, mv, st);
-    launch_k(k_edge<double>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
+    launch_co2contra<double>(33, 2, 0, 42, 1, vin, W, ES, dm, mv, st);
+    launch_k(k_edge<double, 42>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
              mv, (const double *)nullptr);
     StageArgs a{0, 0.0, Hp, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<double>(33, 2, 0, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
+    launch_stage<double>(33, 2, 0, 42, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }
@@ -1659,7 +1706,7 @@ extern "C" int swe_get_tile(const swe_ctx *c, int *tile)
 
 extern "C" int swe_set_kernel_config(swe_ctx *c, int tile, int blocks_per_sm, int runs)
 {
-    if (!c || !valid_cfg(tile, blocks_per_sm, runs)) return SWE_EINVAL;
+    if (!c || !valid_cfg(c->ord, tile, blocks_per_sm, runs)) return SWE_EINVAL;
     set_cfg(c, tile, blocks_per_sm, runs);
     return SWE_OK;
 }
@@ -1675,10 +1722,11 @@ extern "C" int swe_get_kernel_config(const swe_ctx *c, int *tile, int *blocks_pe
 
 namespace {
 struct TuneKey {
-    int device, N, precision, members, op;
+    int device, N, precision, members, op, ord;
     bool operator==(const TuneKey &o) const
     {
-        return device == o.device && N == o.N && precision == o.precision && members == o.members && op == o.op;
+        return device == o.device && N == o.N && precision == o.precision && members == o.members && op == o.op &&
+               ord == o.ord;
     }
 };
 struct TuneEntry {
@@ -1698,7 +1746,7 @@ std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
 extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_per_step)
 {
     if (!c || nreps < 1) return SWE_EINVAL;
-    const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind};
+    const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind, c->ord};
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {
             set_cfg(c, e.tile, e.occ, e.runs);
@@ -1717,8 +1765,10 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     rc = SWE_OK;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(c, SWE_ECUDA, "autotune events");
     const double dt = 1.0;
-    for (int k = 0; k < N_CFGS && rc == SWE_OK; k++) {
-        const KernelCfg kc = k_cfgs[k];
+    int ncfg = 0;
+    const KernelCfg *cfgs = cfgs_of(c->ord, &ncfg);
+    for (int k = 0; k < ncfg && rc == SWE_OK; k++) {
+        const KernelCfg kc = cfgs[k];
         if (c->adv && kc.occ != default_occ(kc.tile)) continue;
         set_cfg(c, kc.tile, kc.occ, kc.runs);
         if ((rc = swe_rk4_steps(c, v, dt, 2)) != SWE_OK) break;

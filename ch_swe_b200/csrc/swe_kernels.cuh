@@ -113,14 +113,15 @@ __device__ __forceinline__ T sat_halo(const Strips<T> &S, const MetricView<T> &m
 //   q = 0: up = fJ2 I_c2i,y(vt)      q = 1: vp = -fJ2 I_c2i,x(ut)
 //          (coriolis_Ch_mod.f90:97-120)
 //   q = 2: c2i x-difference of J ut  q = 3: c2i y-difference of J vt
-//          with the SAT terms of sbp_diff_c2i_42_mod.f90:195-251 on the panel edge
+//          with the SAT terms of sbp_diff_c2i_42_mod.f90:195-251 (sbp_diff_c2i_21_mod.f90:100-146
+//          for ORD 21) on the panel edge
 //          (div_sbp_sat_mod.f90:54-80 before the 1/(hx J) scaling).
 // Across the side the stencils are the first closure rows; along it the full
 // SBP stencils, with the second SAT at the cube corners.
-template <class T>
+template <class T, int ORD = 42>
 __device__ __forceinline__ T edge_raw(const Strips<T> &S, const MetricView<T> &m, int p, int s, int b, int q)
 {
-    using namespace sbp;
+    using SB = SbpOrder<ORD>;
     const int n = S.n, N = n - 1;
     const bool lr = s <= SIDE_R, lo = (s == SIDE_L || s == SIDE_B);
     const T *n1 = S.line(p, s, 0), *n2 = S.line(p, s, 1), *n3 = S.line(p, s, 2), *tg = S.line(p, s, 3);
@@ -128,27 +129,27 @@ __device__ __forceinline__ T edge_raw(const Strips<T> &S, const MetricView<T> &m
     const bool across = lr ? (q == 1 || q == 2) : (q == 0 || q == 3);
     if (q <= 1) {
         const T f = m.ef[(p * 4 + s) * n + b - 1];
-        const T v = across ? T(IC11) * n1[b] + T(IC12) * n2[b] + T(IC13) * n3[b]
-                           : ic2i<T>(b, n, [&](int c) { return tg[c]; });
+        const T v = across ? T(SB::IC1) * n1[b] + T(SB::IC2) * n2[b] + T(SB::IC3) * n3[b]
+                           : SB::template ic2i<T>(b, n, [&](int c) { return tg[c]; });
         return q == 0 ? f * v : -f * v;
     }
     if (across) {
         const T j1 = jn[b] * n1[b], j2 = jn[n + b] * n2[b], j3 = jn[2 * n + b] * n3[b];
-        const T dd = lo ? T(DC11) * j1 + T(DC12) * j2 + T(DC13) * j3 : -T(DC11) * j1 - T(DC12) * j2 - T(DC13) * j3;
-        const T sat = T(SATC) * (T(R11) * (j1 - sat_halo(S, m, p, s, b, 1)) + T(R12) * (j2 - sat_halo(S, m, p, s, b, 2)) +
-                                 T(R13) * (j3 - sat_halo(S, m, p, s, b, 3)));
+        const T dd = lo ? T(SB::DC1) * j1 + T(SB::DC2) * j2 + T(SB::DC3) * j3 : -T(SB::DC1) * j1 - T(SB::DC2) * j2 - T(SB::DC3) * j3;
+        const T sat = T(SB::SATC) * (T(SB::R1) * (j1 - sat_halo(S, m, p, s, b, 1)) + T(SB::R2) * (j2 - sat_halo(S, m, p, s, b, 2)) +
+                                 T(SB::R3) * (j3 - sat_halo(S, m, p, s, b, 3)));
         return lo ? dd + sat : dd - sat;
     }
     auto jtv = [&](int c) { return jt[c] * tg[c]; };
-    T dd = dc2i<T>(b, n, jtv);
+    T dd = SB::template dc2i<T>(b, n, jtv);
     if (b == 1 || b == n) {
         // cube corner: the SAT across the other side through this vertex
         const int s2 = lr ? (b == 1 ? SIDE_B : SIDE_T) : (b == 1 ? SIDE_L : SIDE_R);
         const int b2 = lo ? 1 : n;
         const int c1 = b == 1 ? 1 : N, c2 = b == 1 ? 2 : N - 1, c3 = b == 1 ? 3 : N - 2;
-        const T sat = T(SATC) * (T(R11) * (jtv(c1) - sat_halo(S, m, p, s2, b2, 1)) +
-                                 T(R12) * (jtv(c2) - sat_halo(S, m, p, s2, b2, 2)) +
-                                 T(R13) * (jtv(c3) - sat_halo(S, m, p, s2, b2, 3)));
+        const T sat = T(SB::SATC) * (T(SB::R1) * (jtv(c1) - sat_halo(S, m, p, s2, b2, 1)) +
+                                 T(SB::R2) * (jtv(c2) - sat_halo(S, m, p, s2, b2, 2)) +
+                                 T(SB::R3) * (jtv(c3) - sat_halo(S, m, p, s2, b2, 3)));
         dd = b == 1 ? dd + sat : dd - sat;
     }
     return dd;
@@ -220,7 +221,7 @@ constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the th
 // warp 8 the copy of the third panel at the two cube corners.  Phase 2 combines
 // the copies from shared memory.  Copies are stored by direction (x-neighbour
 // across L/R, y-neighbour across B/T).
-template <class T>
+template <class T, int ORD>
 __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, const T *__restrict__ ESd,
                                                         T *__restrict__ E, Dims d, MetricView<T> m,
                                                         const double *__restrict__ dtm)
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
         }
     }
     pdl_wait();
-    if (rp >= 0) (&raw[0][0][0])[dst] = edge_raw(rq < 2 ? Sc : Sd, m, rp, rs, rb, rq);
+    if (rp >= 0) (&raw[0][0][0])[dst] = edge_raw<T, ORD>(rq < 2 ? Sc : Sd, m, rp, rs, rb, rq);
     __syncthreads();
     if (av >= a1) return;
     const T V = raw[0][0][v], U = raw[0][1][v];

@@ -114,6 +114,82 @@ __device__ __forceinline__ T ic2i(int k, int nx, const F &f)
     return T(IC11) * f(nx - 1) + T(IC12) * f(nx - 2) + T(IC13) * f(nx - 3);
 }
 
+// SBP 2-1 operators (sbp_diff_i2c_21_mod.f90:33-41, sbp_diff_c2i_21_mod.f90:32-42,
+// sbp_interp_i2c_21_mod.f90:25-31, sbp_interp_c2i_21_mod.f90:25-35): two-point
+// interior rows, one-sided first and last rows of the centres->nodes operators.
+template <class T, class F>
+__device__ __forceinline__ T di2c21(int k, int, const F &f) { return f(k + 1) - f(k); }
+template <class T, class F>
+__device__ __forceinline__ T dc2i21(int k, int nx, const F &f)
+{
+    if (k == 1) return f(2) - f(1);
+    if (k == nx) return f(nx - 1) - f(nx - 2);
+    return f(k) - f(k - 1);
+}
+template <class T, class F>
+__device__ __forceinline__ T ii2c21(int k, int, const F &f) { return T(0.5) * (f(k + 1) + f(k)); }
+template <class T, class F>
+__device__ __forceinline__ T ic2i21(int k, int nx, const F &f)
+{
+    if (k == 1) return f(1);
+    if (k == nx) return f(nx - 1);
+    return T(0.5) * (f(k) + f(k - 1));
+}
+
+// The order-dependent parts of the Ch operators, by SBP order (42 or 21):
+//   C2I_LO/HI: nodes k in [C2I_LO, nx - C2I_HI] use the interior c2i rows;
+//   I2C_LO/HI: centres k in [I2C_LO, n - I2C_HI] use the interior i2c rows;
+//   GRAD_LO/HI: centres with the interior i2c difference and no gradient SAT;
+//   U_LO/HI: u-point columns [U_LO, N - U_HI] clear of both (the grad_x + I_i2c,x pass);
+//   V_LO/HI: rows [V_LO, N - V_HI] clear of the c2i and i2c closures, the gradient SAT
+//            and the panel-boundary rows (the final pass);
+//   SAT1..3: gradient SAT weights 0.5 R1k / h_kk of rows 1..3 (and mirrored);
+//   IC1..3, DC1..3: first c2i interpolation / difference rows (a panel edge node);
+//   SATC, R1..3: divergence SAT 0.5 / h11 and the boundary projection.
+template <int ORD>
+struct SbpOrder;
+
+template <>
+struct SbpOrder<42> {
+    static constexpr int C2I_LO = 5, C2I_HI = 4, I2C_LO = 4, I2C_HI = 3, GRAD_LO = 4, GRAD_HI = 3;
+    static constexpr int U_LO = 4, U_HI = 3, V_LO = 5, V_HI = 3;
+    static constexpr double SAT1 = sbp::SATI1, SAT2 = sbp::SATI2, SAT3 = sbp::SATI3;
+    static constexpr double IC1 = sbp::IC11, IC2 = sbp::IC12, IC3 = sbp::IC13;
+    static constexpr double DC1 = sbp::DC11, DC2 = sbp::DC12, DC3 = sbp::DC13;
+    static constexpr double SATC = sbp::SATC, R1 = sbp::R11, R2 = sbp::R12, R3 = sbp::R13;
+    template <class T, class F> static __device__ __forceinline__ T di2c(int k, int n, const F &f) { return chswe::di2c<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T dc2i(int k, int nx, const F &f) { return chswe::dc2i<T>(k, nx, f); }
+    template <class T, class F> static __device__ __forceinline__ T ii2c(int k, int n, const F &f) { return chswe::ii2c<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T ic2i(int k, int nx, const F &f) { return chswe::ic2i<T>(k, nx, f); }
+    // interior rows on four consecutive inputs: c2i rows take v0..v3 = f(k-2..k+1),
+    // i2c rows v0..v3 = f(k-1..k+2)
+    template <class T> static __device__ __forceinline__ T interp4(T v0, T v1, T v2, T v3)
+    {
+        return (T(9) * (v2 + v1) - (v3 + v0)) * T(0.0625);
+    }
+    template <class T> static __device__ __forceinline__ T diff4(T v0, T v1, T v2, T v3)
+    {
+        return (T(27) * (v2 - v1) - (v3 - v0)) * T(1.0 / 24.0);
+    }
+};
+
+template <>
+struct SbpOrder<21> {
+    static constexpr int C2I_LO = 2, C2I_HI = 1, I2C_LO = 1, I2C_HI = 0, GRAD_LO = 3, GRAD_HI = 2;
+    static constexpr int U_LO = 3, U_HI = 2, V_LO = 3, V_HI = 2;
+    // h11 = h22 = 1 (i2c), h11 = 1/2 (c2i), R11 = 3/2, R12 = -1/2
+    static constexpr double SAT1 = 0.5 * 1.5, SAT2 = 0.5 * -0.5, SAT3 = 0.0;
+    static constexpr double IC1 = 1.0, IC2 = 0.0, IC3 = 0.0;
+    static constexpr double DC1 = -1.0, DC2 = 1.0, DC3 = 0.0;
+    static constexpr double SATC = 0.5 / 0.5, R1 = 1.5, R2 = -0.5, R3 = 0.0;
+    template <class T, class F> static __device__ __forceinline__ T di2c(int k, int n, const F &f) { return di2c21<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T dc2i(int k, int nx, const F &f) { return dc2i21<T>(k, nx, f); }
+    template <class T, class F> static __device__ __forceinline__ T ii2c(int k, int n, const F &f) { return ii2c21<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T ic2i(int k, int nx, const F &f) { return ic2i21<T>(k, nx, f); }
+    template <class T> static __device__ __forceinline__ T interp4(T, T v1, T v2, T) { return T(0.5) * (v2 + v1); }
+    template <class T> static __device__ __forceinline__ T diff4(T, T v1, T v2, T) { return v2 - v1; }
+};
+
 }  // namespace chswe
 
 namespace chswe {

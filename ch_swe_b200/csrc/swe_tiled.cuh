@@ -79,39 +79,31 @@ struct SWin {
     __device__ __forceinline__ Line<T> col(int i) const { return Line<T>{a + (i - x0) - y0 * NP, NP}; }
 };
 
-// Interior rows of the four operators (the closure rows go through the general
-// functions of swe_sbp.cuh).
-template <class T> __device__ __forceinline__ T ic2i_in(int k, const Line<T> &f)
+// The four operators at one output: the interior rows inline, the closure rows
+// through the general functions of swe_sbp.cuh (SbpOrder<ORD>).
+template <class T, int ORD = 42> __device__ __forceinline__ T ic2i_u(int k, int nx, const Line<T> &f)
 {
-    return (T(9) * (f(k) + f(k - 1)) - (f(k + 1) + f(k - 2))) * T(0.0625);
+    using S = SbpOrder<ORD>;
+    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template interp4<T>(f(k - 2), f(k - 1), f(k), f(k + 1))
+                                                   : S::template ic2i<T>(k, nx, f);
 }
-template <class T> __device__ __forceinline__ T ii2c_in(int k, const Line<T> &f)
+template <class T, int ORD = 42> __device__ __forceinline__ T ii2c_u(int k, int n, const Line<T> &f)
 {
-    return (T(9) * (f(k + 1) + f(k)) - (f(k + 2) + f(k - 1))) * T(0.0625);
+    using S = SbpOrder<ORD>;
+    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template interp4<T>(f(k - 1), f(k), f(k + 1), f(k + 2))
+                                                  : S::template ii2c<T>(k, n, f);
 }
-template <class T> __device__ __forceinline__ T dc2i_in(int k, const Line<T> &f)
+template <class T, int ORD = 42> __device__ __forceinline__ T dc2i_u(int k, int nx, const Line<T> &f)
 {
-    return (T(27) * (f(k) - f(k - 1)) - (f(k + 1) - f(k - 2))) * T(1.0 / 24.0);
+    using S = SbpOrder<ORD>;
+    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template diff4<T>(f(k - 2), f(k - 1), f(k), f(k + 1))
+                                                   : S::template dc2i<T>(k, nx, f);
 }
-template <class T> __device__ __forceinline__ T di2c_in(int k, const Line<T> &f)
+template <class T, int ORD = 42> __device__ __forceinline__ T di2c_u(int k, int n, const Line<T> &f)
 {
-    return (T(27) * (f(k + 1) - f(k)) - (f(k + 2) - f(k - 1))) * T(1.0 / 24.0);
-}
-template <class T> __device__ __forceinline__ T ic2i_u(int k, int nx, const Line<T> &f)
-{
-    return (k >= 5 && k <= nx - 4) ? ic2i_in<T>(k, f) : ic2i<T>(k, nx, f);
-}
-template <class T> __device__ __forceinline__ T ii2c_u(int k, int n, const Line<T> &f)
-{
-    return (k >= 4 && k <= n - 3) ? ii2c_in<T>(k, f) : ii2c<T>(k, n, f);
-}
-template <class T> __device__ __forceinline__ T dc2i_u(int k, int nx, const Line<T> &f)
-{
-    return (k >= 5 && k <= nx - 4) ? dc2i_in<T>(k, f) : dc2i<T>(k, nx, f);
-}
-template <class T> __device__ __forceinline__ T di2c_u(int k, int n, const Line<T> &f)
-{
-    return (k >= 4 && k <= n - 3) ? di2c_in<T>(k, f) : di2c<T>(k, n, f);
+    using S = SbpOrder<ORD>;
+    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template diff4<T>(f(k - 1), f(k), f(k + 1), f(k + 2))
+                                                  : S::template di2c<T>(k, n, f);
 }
 
 // Stencil runs.  A pass gives every thread whole runs of RB consecutive outputs
@@ -129,15 +121,15 @@ __device__ __forceinline__ void run_load(const Line<T> &f, int k0, T (&v)[RB + 3
 #pragma unroll
     for (int m = 0; m < RB + 3; m++) v[m] = f(k0 + O + m);
 }
-template <class T, int RB>
+template <class T, int RB, int ORD>
 __device__ __forceinline__ T run_interp(const T (&v)[RB + 3], int m)
 {
-    return (T(9) * (v[m + 2] + v[m + 1]) - (v[m + 3] + v[m])) * T(0.0625);
+    return SbpOrder<ORD>::template interp4<T>(v[m], v[m + 1], v[m + 2], v[m + 3]);
 }
-template <class T, int RB>
+template <class T, int RB, int ORD>
 __device__ __forceinline__ T run_diff(const T (&v)[RB + 3], int m)
 {
-    return (T(27) * (v[m + 2] - v[m + 1]) - (v[m + 3] - v[m])) * T(1.0 / 24.0);
+    return SbpOrder<ORD>::template diff4<T>(v[m], v[m + 1], v[m + 2], v[m + 3]);
 }
 
 // Every global load of a pass is issued into registers before the first
@@ -158,7 +150,7 @@ struct Co2Layout {
 
 // OCC: resident blocks per SM the register allocation is capped for; RUNS: stencil
 // runs of several outputs per thread (both autotuned).
-template <class T, int TM, int OCC, bool RUNS>
+template <class T, int TM, int OCC, bool RUNS, int ORD>
 __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
                                                                  T *__restrict__ ES, Dims d, MetricView<T> m,
                                                                  const double *__restrict__ dtm)
@@ -166,6 +158,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = Co2Layout<T, TM>;
     CHSWE_TILE_CONSTANTS(TM, RUNS);
+    using SB = SbpOrder<ORD>;
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -259,15 +252,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int k = sv.x0 + x, l0 = j0 + r * RBW, cnt = min(RBW, j1 - l0);
         const Line<T> col = sv.col(k);
         T *o = &svq.at(k, l0);
-        if (cnt == RBW && l0 >= 5 && l0 + RBW - 1 <= n - 4) {
+        if (cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(col, l0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = run_interp<T, RBW>(v, mm) * jq1[it][mm];
+            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = run_interp<T, RBW, ORD>(v, mm) * jq1[it][mm];
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++)
-                if (mm < cnt) o[mm * PW] = ic2i_u<T>(l0 + mm, n, col) * jq1[it][mm];
+                if (mm < cnt) o[mm * PW] = ic2i_u<T, ORD>(l0 + mm, n, col) * jq1[it][mm];
         }
     }
     // I_c2i,x(u) at xy nodes: rows of the window, runs along the tile columns; the
@@ -281,15 +274,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int l = suq.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
         const Line<T> row = su.row(l);
         T *o = &suq.at(k0, l);
-        if (cnt == RBW && k0 >= 5 && k0 + RBW - 1 <= n - 4) {
+        if (cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(row, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW>(v, mm);
+            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++)
-                if (mm < cnt) o[mm] = ic2i_u<T>(k0 + mm, n, row);
+                if (mm < cnt) o[mm] = ic2i_u<T, ORD>(k0 + mm, n, row);
         }
     }
     __syncthreads();
@@ -304,15 +297,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
         const Line<T> row = svq.row(j);
         T *o = &sux.at(k0, j);
-        if (cnt == RBT && k0 >= 4 && k0 + RBT - 1 <= N - 3) {
+        if (cnt == RBT && k0 >= SB::I2C_LO && k0 + RBT - 1 <= N - SB::I2C_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(row, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) o[mm] = run_interp<T, RBT>(v, mm);
+            for (int mm = 0; mm < RBT; mm++) o[mm] = run_interp<T, RBT, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBT; mm++)
-                if (mm < cnt) o[mm] = ii2c_u<T>(k0 + mm, N, row);
+                if (mm < cnt) o[mm] = ii2c_u<T, ORD>(k0 + mm, N, row);
         }
     }
     // J Qi12 factor of the second: row-major, in place
@@ -335,14 +328,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int i = i0 + x, jr = j0 + r * RBT, cnt = min(RBT, j1 - jr);
         const Line<T> col = suq.col(i);
         T vi[RBT];
-        if (cnt == RBT && jr >= 4 && jr + RBT - 1 <= N - 3) {
+        if (cnt == RBT && jr >= SB::I2C_LO && jr + RBT - 1 <= N - SB::I2C_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(col, jr, v);
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) vi[mm] = run_interp<T, RBT>(v, mm);
+            for (int mm = 0; mm < RBT; mm++) vi[mm] = run_interp<T, RBT, ORD>(v, mm);
         } else {
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) vi[mm] = (mm < cnt && jr + mm <= N) ? ii2c_u<T>(jr + mm, N, col) : T(0);
+            for (int mm = 0; mm < RBT; mm++) vi[mm] = (mm < cnt && jr + mm <= N) ? ii2c_u<T, ORD>(jr + mm, N, col) : T(0);
         }
 #pragma unroll
         for (int mm = 0; mm < RBT; mm++) {
@@ -391,7 +384,7 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 //   mode 4: V0 += ACC + dt/6 k          (FP32: Kahan with compensation CMP)
 // ADV: the advective operator (divergence of the mass flux a.F, tendencies a.A,
 // gradient of the pre-averaging boundary h a.HB); false: the linear operator.
-template <class T, int TM, int OCC, int MODE, bool ADV, bool RUNS>
+template <class T, int TM, int OCC, int MODE, bool ADV, bool RUNS, int ORD>
 __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
                                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
                                                           Dims d, MetricView<T> m, StageArgs a)
@@ -400,6 +393,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = StageLayout<T, TM>;
     CHSWE_TILE_CONSTANTS(TM, RUNS);
+    using SB = SbpOrder<ORD>;
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
@@ -578,16 +572,16 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++)
                 if (mm < cnt) o[mm * PW] = f1[it][mm];
-        } else if (cnt == RBW && l0 >= 5 && l0 + RBW - 1 <= n - 4) {
+        } else if (cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(col, l0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = f1[it][mm] * run_interp<T, RBW>(v, mm);
+            for (int mm = 0; mm < RBW; mm++) o[mm * PW] = f1[it][mm] * run_interp<T, RBW, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++) {
                 const int l = l0 + mm;
-                if (mm < cnt) o[mm * PW] = on_boundary(k, l, n) ? f1[it][mm] : f1[it][mm] * ic2i_u<T>(l, n, col);
+                if (mm < cnt) o[mm * PW] = on_boundary(k, l, n) ? f1[it][mm] : f1[it][mm] * ic2i_u<T, ORD>(l, n, col);
             }
         }
     }
@@ -601,15 +595,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int l = svp.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
         const Line<T> row = sut.row(l);
         T *o = &svp.at(k0, l);
-        if (cnt == RBW && k0 >= 5 && k0 + RBW - 1 <= n - 4) {
+        if (cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(row, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW>(v, mm);
+            for (int mm = 0; mm < RBW; mm++) o[mm] = run_interp<T, RBW, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++)
-                if (mm < cnt) o[mm] = ic2i_u<T>(k0 + mm, n, row);
+                if (mm < cnt) o[mm] = ic2i_u<T, ORD>(k0 + mm, n, row);
         }
     }
     // ---- P3: x part of the divergence, c2i difference of J ut: tile rows, runs along columns
@@ -622,15 +616,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, i1 - k0);
         const Line<T> row = sju.row(j);
         T *o = &sdx.at(k0, j);
-        if (cnt == RBT && k0 >= 5 && k0 + RBT - 1 <= n - 4) {
+        if (cnt == RBT && k0 >= SB::C2I_LO && k0 + RBT - 1 <= n - SB::C2I_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -2>(row, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) o[mm] = run_diff<T, RBT>(v, mm);
+            for (int mm = 0; mm < RBT; mm++) o[mm] = run_diff<T, RBT, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBT; mm++)
-                if (mm < cnt) o[mm] = dc2i_u<T>(k0 + mm, n, row);
+                if (mm < cnt) o[mm] = dc2i_u<T, ORD>(k0 + mm, n, row);
         }
     }
     __syncthreads();
@@ -648,30 +642,30 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
         const Line<T> hrow = sh.row(j), prow = sup.row(j);
         T *og = &skx.at(k0, j), *oc = &scx.at(k0, j);
-        if (cnt == RBT && k0 >= 4 && k0 + RBT - 1 <= N - 3) {
+        if (cnt == RBT && k0 >= SB::U_LO && k0 + RBT - 1 <= N - SB::U_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(hrow, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) og[mm] = -m.grav * (run_diff<T, RBT>(v, mm) * m.inv_hxa);
+            for (int mm = 0; mm < RBT; mm++) og[mm] = -m.grav * (run_diff<T, RBT, ORD>(v, mm) * m.inv_hxa);
             run_load<T, RBT, -1>(prow, k0, v);
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) oc[mm] = run_interp<T, RBT>(v, mm);
+            for (int mm = 0; mm < RBT; mm++) oc[mm] = run_interp<T, RBT, ORD>(v, mm);
         } else {
 #pragma unroll
             for (int mm = 0; mm < RBT; mm++) {
                 if (mm >= cnt) continue;
                 const int i = k0 + mm;
-                T gx = di2c_u<T>(i, N, hrow);
+                T gx = di2c_u<T, ORD>(i, N, hrow);
                 if (i <= 3) {
-                    const T sat = i == 1 ? T(SATI1) : (i == 2 ? T(SATI2) : T(SATI3));
+                    const T sat = i == 1 ? T(SB::SAT1) : (i == 2 ? T(SB::SAT2) : T(SB::SAT3));
                     gx += sat * (hrow(1) - hl[x]);
                 }
                 if (i >= N - 2) {
-                    const T sat = i == N ? T(SATI1) : (i == N - 1 ? T(SATI2) : T(SATI3));
+                    const T sat = i == N ? T(SB::SAT1) : (i == N - 1 ? T(SB::SAT2) : T(SB::SAT3));
                     gx += sat * (hr[x] - hrow(n));
                 }
                 og[mm] = -m.grav * (gx * m.inv_hxa);
-                oc[mm] = ii2c_u<T>(i, N, prow);
+                oc[mm] = ii2c_u<T, ORD>(i, N, prow);
             }
         }
     }
@@ -707,7 +701,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         for (int mm = 0; mm < RBT; mm++) kh[it][mm] = ku[it][mm] = kv[it][mm] = T(0);
         if (cnt <= 0) continue;
         const Line<T> dcol = sjv.col(i), hcol = sh.col(i), pcol = svp.col(i);
-        if (cnt == RBT && jr >= 5 && jr + RBT - 1 <= N - 3) {
+        if (cnt == RBT && jr >= SB::V_LO && jr + RBT - 1 <= N - SB::V_HI) {
             // rows clear of the closures, the SAT terms and the panel-boundary rows
             const bool bcol = (i == 1 || i == n), hasu = i <= N;
             T v[RBT + 3];
@@ -715,7 +709,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
 #pragma unroll
             for (int mm = 0; mm < RBT; mm++) {
                 const T dvg = bcol ? mja[it][mm]
-                                   : (sdx.at(i, jr + mm) * m.inv_hx + run_diff<T, RBT>(v, mm) * m.inv_hx) * mja[it][mm];
+                                   : (sdx.at(i, jr + mm) * m.inv_hx + run_diff<T, RBT, ORD>(v, mm) * m.inv_hx) * mja[it][mm];
                 kh[it][mm] = -H * dvg;
             }
             if (hasu) {
@@ -733,7 +727,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             run_load<T, RBT, -1>(hcol, jr, v);
             T gy[RBT];
 #pragma unroll
-            for (int mm = 0; mm < RBT; mm++) gy[mm] = run_diff<T, RBT>(v, mm) * m.inv_hxa;
+            for (int mm = 0; mm < RBT; mm++) gy[mm] = run_diff<T, RBT, ORD>(v, mm) * m.inv_hxa;
             run_load<T, RBT, -1>(pcol, jr, v);
 #pragma unroll
             for (int mm = 0; mm < RBT; mm++) {
@@ -741,9 +735,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                     const int j = jr + mm;
                     T av = __ldg(Av + box_off32(P, i, j));
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
-                    kv[it][mm] = (av + -m.grav * gy[mm]) + run_interp<T, RBT>(v, mm) * mjx[it][mm];
+                    kv[it][mm] = (av + -m.grav * gy[mm]) + run_interp<T, RBT, ORD>(v, mm) * mjx[it][mm];
                 } else {
-                    kv[it][mm] = -m.grav * gy[mm] + run_interp<T, RBT>(v, mm) * mjx[it][mm];
+                    kv[it][mm] = -m.grav * gy[mm] + run_interp<T, RBT, ORD>(v, mm) * mjx[it][mm];
                 }
             }
             continue;
@@ -756,7 +750,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             if (on_boundary(i, j, n)) {
                 dvg = mja[it][mm];
             } else {
-                const T dy = dc2i_u<T>(j, n, dcol);
+                const T dy = dc2i_u<T, ORD>(j, n, dcol);
                 dvg = (sdx.at(i, j) * m.inv_hx + dy * m.inv_hx) * mja[it][mm];
             }
             kh[it][mm] = -H * dvg;
@@ -771,22 +765,22 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                 }
             }
             if (j <= N) {
-                T gy = di2c_u<T>(j, N, hcol);
+                T gy = di2c_u<T, ORD>(j, N, hcol);
                 if (j <= 3) {
-                    const T sat = j == 1 ? T(SATI1) : (j == 2 ? T(SATI2) : T(SATI3));
+                    const T sat = j == 1 ? T(SB::SAT1) : (j == 2 ? T(SB::SAT2) : T(SB::SAT3));
                     gy += sat * (hcol(1) - hb[x]);
                 }
                 if (j >= N - 2) {
-                    const T sat = j == N ? T(SATI1) : (j == N - 1 ? T(SATI2) : T(SATI3));
+                    const T sat = j == N ? T(SB::SAT1) : (j == N - 1 ? T(SB::SAT2) : T(SB::SAT3));
                     gy += sat * (ht[x] - hcol(n));
                 }
                 gy = gy * m.inv_hxa;
                 if constexpr (ADV) {
                     T av = __ldg(Av + box_off32(P, i, j));
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
-                    kv[it][mm] = (av + -m.grav * gy) + ii2c_u<T>(j, N, pcol) * mjx[it][mm];
+                    kv[it][mm] = (av + -m.grav * gy) + ii2c_u<T, ORD>(j, N, pcol) * mjx[it][mm];
                 } else {
-                    kv[it][mm] = -m.grav * gy + ii2c_u<T>(j, N, pcol) * mjx[it][mm];
+                    kv[it][mm] = -m.grav * gy + ii2c_u<T, ORD>(j, N, pcol) * mjx[it][mm];
                 }
             }
         }

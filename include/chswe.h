@@ -73,6 +73,10 @@ typedef struct swe_cfg {
     double rotation_axis[3];  /* metric%rotation_axis                 (default 0, 0, 1) */
     int coriolis_constant;    /* metric%coriolis_const: f = omega instead of 2 omega sin(lat) */
     double h_mean;            /* operator h_mean (H) for every member (default 1000 m) */
+    int sbp_order;            /* SBP order of the Ch operators: 42 (default; 0 also selects it) or
+                                 21 (linear operator only): the _sbp_sat_42 / _sbp_sat_21 names of
+                                 grad_factory_mod.f90, div_factory_mod.f90, co2contra_factory_mod.f90,
+                                 coriolis_factory_mod.f90 and the SBP_C42/C21 quadratures */
 } swe_cfg;
 
 /* Fill *cfg with the defaults listed above. */
@@ -166,7 +170,7 @@ int swe_autotune(swe_ctx *ctx, int nreps, int *best_tile, double *ms_per_step);
    counterpart in the reference (there the operator owns allocatable work fields).
    Limits and behaviour:
    - cfg->N <= SWE_NOALLOC_MAX_N, else SWE_ETOOBIG (with a message on stderr);
-     cfg->precision SWE_FP64, cfg->n_members 1, SWE_OP_LINEAR.
+     cfg->precision SWE_FP64, cfg->n_members 1, SWE_OP_LINEAR, SBP order 4-2.
    - The first call on a device, with that device current, looks up the array's
      device address and uploads the edge tables; make that first call before any
      stream capture.  A call with a new geometry (N, radius, rotation) recomputes the

@@ -62,6 +62,8 @@ def lib():
         L.orc_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_set_operator.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_sbp_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         _lib = L
     return _lib
 
@@ -76,15 +78,17 @@ def shapes(N: int):
 
 
 class Oracle:
-    """FP64 CPU restatement of the linear Ch/SBP42 shallow-water operator and RK4."""
+    """FP64 CPU restatement of the linear Ch shallow-water operator (SBP 4-2 or 2-1) and RK4."""
 
     OPERATORS = {"linear": 0, "advective": 1}
 
     def __init__(self, N: int, radius: float = EARTH_RADIUS, grav: float = EARTH_GRAV,
                  omega: float = EARTH_OMEGA, h_mean: float = 1000.0, axis=(0.0, 0.0, 1.0),
-                 coriolis_constant: bool = False, operator: str = "linear"):
+                 coriolis_constant: bool = False, operator: str = "linear", sbp_order: int = 42):
         """operator: 'linear' (linear_swm_operator) or 'advective' (advective_swm_operator,
-        covariant Ch branch: up4 mass flux and up4 vector advection)."""
+        covariant Ch branch: up4 mass flux and up4 vector advection).  sbp_order: 42 or
+        21, the order of the Ch difference, interpolation and quadrature operators (the
+        _sbp_sat_42 / _sbp_sat_21 operator names of the reference's factories)."""
         self.N = N
         self.radius, self.grav, self.omega, self.h_mean = radius, grav, omega, h_mean
         self.axis = np.ascontiguousarray(axis, dtype=np.float64)
@@ -93,6 +97,9 @@ class Oracle:
             raise ValueError(f"oracle: unsupported N={N} (need N >= 8)")
         self.operator = operator
         lib().orc_set_operator(self._c, self.OPERATORS[operator])
+        self.sbp_order = int(sbp_order)
+        if lib().orc_set_sbp_order(self._c, self.sbp_order) != 0:
+            raise ValueError(f"oracle: unsupported SBP order {sbp_order} (21 or 42)")
 
     def __del__(self):
         c = getattr(self, "_c", None)
@@ -188,11 +195,11 @@ class Oracle:
         return (out, out2) if kind != 0 else out
 
 
-def sbp1d(op: int, n: int, x) -> np.ndarray:
-    """One-dimensional SBP 4-2 operator on one line (0 i2c diff, 1 c2i diff without SAT,
-    2 i2c interpolation, 3 c2i interpolation)."""
+def sbp1d(op: int, n: int, x, order: int = 42) -> np.ndarray:
+    """One-dimensional SBP operator (order 42 or 21) on one line (0 i2c diff, 1 c2i diff,
+    both without SAT, 2 i2c interpolation, 3 c2i interpolation)."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     nout = n if op in (0, 2) else n + 1
     out = np.empty(nout)
-    lib().orc_sbp1d(op, n, _p(x), _p(out))
+    lib().orc_sbp1d_ord(int(order), op, n, _p(x), _p(out))
     return out

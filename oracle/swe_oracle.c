@@ -482,6 +482,18 @@ static void mass_coeffs(double *A, int n, const double *edge, int nedge)
 
 static const double A42_I[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
 static const double A42_C[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
+/* D21_A_interfaces, D21_A_centers (sbp_operators_collection_mod.f90:169-170) */
+static const double A21_I[2] = {0.5, 1.0};
+static const double A21_C[2] = {1.0, 1.0};
+
+/* quadrature edge weights of the mesh's two directions for SBP order ord */
+static void mesh_mass(mesh_t *m, int ord)
+{
+    const double *ei = ord == 21 ? A21_I : A42_I, *ec = ord == 21 ? A21_C : A42_C;
+    const int ni = ord == 21 ? 2 : 5, nc = ord == 21 ? 2 : 4;
+    mass_coeffs(m->Ax, m->nx, m->shift_i == 0.0 ? ei : ec, m->shift_i == 0.0 ? ni : nc);
+    mass_coeffs(m->Ay, m->ny, m->shift_j == 0.0 ? ei : ec, m->shift_j == 0.0 ? ni : nc);
+}
 
 static void mesh_build(mesh_t *m, int N, double shift_i, double shift_j)
 {
@@ -524,8 +536,7 @@ static void mesh_build(mesh_t *m, int N, double shift_i, double shift_j)
         }
     m->Ax = malloc(sizeof(double) * m->nx);
     m->Ay = malloc(sizeof(double) * m->ny);
-    mass_coeffs(m->Ax, m->nx, shift_i == 0.0 ? A42_I : A42_C, shift_i == 0.0 ? 5 : 4);
-    mass_coeffs(m->Ay, m->ny, shift_j == 0.0 ? A42_I : A42_C, shift_j == 0.0 ? 5 : 4);
+    mesh_mass(m, 42);
 }
 
 static void mesh_free(mesh_t *m)
@@ -549,6 +560,11 @@ static const double DC_q11 = -2.0, DC_q12 = 3.0, DC_q13 = -1.0, DC_q21 = -1.0, D
                     DC_q31 = 1.0 / 24.0, DC_q32 = -9.0 / 8.0, DC_q33 = 9.0 / 8.0, DC_q34 = -1.0 / 24.0,
                     DC_q41 = -1.0 / 71.0, DC_q42 = 6.0 / 71.0, DC_q43 = -83.0 / 71.0, DC_q44 = 81.0 / 71.0,
                     DC_q45 = -3.0 / 71.0;
+/* SBP 2-1 (sbp_diff_i2c_21_mod.f90:12-15, sbp_diff_c2i_21_mod.f90:12-15): norms of the
+   i2c difference (h11 = h22 = 1) and of the c2i difference (h11 = 1/2), boundary
+   projection R11, R12 */
+static const double S21_DI_h11 = 1.0, S21_DI_h22 = 1.0, S21_DC_h11 = 0.5;
+static const double S21_R11 = 3.0 / 2.0, S21_R12 = -1.0 / 2.0;
 /* interpolation free parameters */
 static const double C13 = 0.1264926207034815, C14 = -0.029892648949074313;
 static double II_q[15], IC_q[15];
@@ -594,12 +610,24 @@ static void init_coeffs(void)
    dir 1 = y (i = l, j = k). */
 #define L(f, t, dir, k, l) ((dir) == 0 ? FA(f, t, k, l) : FA(f, t, l, k))
 
-/* sbp_diff_i2c_42_t%apply_tile + add_SAT_correction along dir; out has n = nodes-1 rows */
-static void diff_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le)
+/* sbp_diff_i2c_42_t%apply_tile + add_SAT_correction along dir; out has n = nodes-1 rows.
+   ord 21: sbp_diff_i2c_21_t (sbp_diff_i2c_21_mod.f90:25-146). */
+static void diff_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le, int ord)
 {
-    for (int l = ls; l <= le; l++) {
 #define O(k) (*((dir) == 0 ? &FA(out, t, k, l) : &FA(out, t, l, k)))
 #define I(k) L(in, t, dir, k, l)
+    if (ord == 21) {
+        for (int l = ls; l <= le; l++)
+            for (int k = 1; k <= n; k++) O(k) = I(k + 1) - I(k);
+        for (int l = ls; l <= le; l++) {
+            O(1) = O(1) + 0.5 * S21_R11 / S21_DI_h11 * (I(1) - I(0));
+            O(2) = O(2) + 0.5 * S21_R12 / S21_DI_h22 * (I(1) - I(0));
+            O(n) = O(n) + 0.5 * S21_R11 / S21_DI_h11 * (I(n + 2) - I(n + 1));
+            O(n - 1) = O(n - 1) + 0.5 * S21_R12 / S21_DI_h22 * (I(n + 2) - I(n + 1));
+        }
+        return;
+    }
+    for (int l = ls; l <= le; l++) {
         O(1) = DI_q11 * I(1) + DI_q12 * I(2) + DI_q13 * I(3) + DI_q14 * I(4);
         O(2) = DI_q21 * I(1) + DI_q22 * I(2) + DI_q23 * I(3) + DI_q24 * I(4);
         O(3) = DI_q31 * I(1) + DI_q33 * I(3) + DI_q34 * I(4) + DI_q35 * I(5);
@@ -619,9 +647,22 @@ static void diff_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls,
     }
 }
 
-/* sbp_diff_c2i_42_t%apply_tile + add_SAT_correction; out has nx = centres+1 rows */
-static void diff_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le)
+/* sbp_diff_c2i_42_t%apply_tile + add_SAT_correction; out has nx = centres+1 rows.
+   ord 21: sbp_diff_c2i_21_t (sbp_diff_c2i_21_mod.f90:24-146). */
+static void diff_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le, int ord)
 {
+    if (ord == 21) {
+        for (int l = ls; l <= le; l++) {
+            O(1) = I(2) - I(1);
+            for (int k = 2; k <= nx - 1; k++) O(k) = I(k) - I(k - 1);
+            O(nx) = I(nx - 1) - I(nx - 2);
+        }
+        for (int l = ls; l <= le; l++) {
+            O(1) = O(1) + 0.5 / S21_DC_h11 * (S21_R11 * (I(1) - I(0)) + S21_R12 * (I(2) - I(-1)));
+            O(nx) = O(nx) - 0.5 / S21_DC_h11 * (S21_R11 * (I(nx - 1) - I(nx)) + S21_R12 * (I(nx - 2) - I(nx + 1)));
+        }
+        return;
+    }
     for (int l = ls; l <= le; l++) {
         O(1) = DC_q11 * I(1) + DC_q12 * I(2) + DC_q13 * I(3);
         O(2) = DC_q21 * I(1) + DC_q22 * I(2);
@@ -639,9 +680,15 @@ static void diff_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls
     }
 }
 
-/* sbp_interp_i2c_42_t%apply_tile; out has n centres */
-static void interp_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le)
+/* sbp_interp_i2c_42_t%apply_tile; out has n centres.
+   ord 21: sbp_interp_i2c_21_t (sbp_interp_i2c_21_mod.f90:17-56). */
+static void interp_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le, int ord)
 {
+    if (ord == 21) {
+        for (int l = ls; l <= le; l++)
+            for (int k = 1; k <= n; k++) O(k) = 0.5 * (I(k + 1) + I(k));
+        return;
+    }
     const double *q = II_q;
     for (int l = ls; l <= le; l++) {
         O(1) = q[0] * I(1) + q[1] * I(2) + q[2] * I(3) + q[3] * I(4);
@@ -654,9 +701,18 @@ static void interp_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int l
     }
 }
 
-/* sbp_interp_c2i_42_t%apply_tile; out has nx = centres+1 nodes */
-static void interp_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le)
+/* sbp_interp_c2i_42_t%apply_tile; out has nx = centres+1 nodes.
+   ord 21: sbp_interp_c2i_21_t (sbp_interp_c2i_21_mod.f90:17-84). */
+static void interp_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le, int ord)
 {
+    if (ord == 21) {
+        for (int l = ls; l <= le; l++) {
+            O(1) = I(1);
+            for (int k = 2; k <= nx - 1; k++) O(k) = 0.5 * (I(k) + I(k - 1));
+            O(nx) = I(nx - 1);
+        }
+        return;
+    }
     const double *q = IC_q;
     for (int l = ls; l <= le; l++) {
         O(1) = q[0] * I(1) + q[1] * I(2) + q[2] * I(3);
@@ -678,6 +734,7 @@ static void interp_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int 
 /* ------------------------------------------------------------------ */
 typedef struct orc_ctx {
     int N;
+    int ord;                     /* SBP order of the Ch operators: 42 (default) or 21 */
     double a, g, omega, H, axis[3];
     int coriolis_const;
     mesh_t mxy, mx, my;          /* xy (h), x (v), y (u) */
@@ -752,6 +809,7 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     c->N = N; c->a = radius; c->g = grav; c->omega = omega; c->H = h_mean;
     c->axis[0] = axis ? axis[0] : 0.0; c->axis[1] = axis ? axis[1] : 0.0; c->axis[2] = axis ? axis[2] : 1.0;
     c->coriolis_const = coriolis_const;
+    c->ord = 42;
     mesh_build(&c->mxy, N, 0.0, 0.0);
     mesh_build(&c->mx, N, 0.0, 0.5);
     mesh_build(&c->my, N, 0.5, 0.0);
@@ -808,10 +866,10 @@ static void op_grad(orc_ctx *c, fld_t *gx, fld_t *gy, fld_t *h)
     int N = c->N;
     exch_do(&c->ex_xy3_full_s, h, NULL);
     for (int t = 0; t < NPAN; t++) {
-        diff_i2c(gx, h, t, 0, N, 1, N + 1);
+        diff_i2c(gx, h, t, 0, N, 1, N + 1, c->ord);
         for (int j = 1; j <= N + 1; j++)
             for (int i = 1; i <= N; i++) FA(gx, t, i, j) = FA(gx, t, i, j) / (c->my.hx * c->a);
-        diff_i2c(gy, h, t, 1, N, 1, N + 1);
+        diff_i2c(gy, h, t, 1, N, 1, N + 1, c->ord);
         for (int j = 1; j <= N; j++)
             for (int i = 1; i <= N + 1; i++) FA(gy, t, i, j) = FA(gy, t, i, j) / (c->mx.hy * c->a);
     }
@@ -825,8 +883,8 @@ static void op_co2contra(orc_ctx *c, fld_t *ut, fld_t *vt, fld_t *u, fld_t *v)
     exch_do(&c->ex_ch3_u, u, v);
     exch_do(&c->ex_ch3_v, u, v);
     for (int t = 0; t < NPAN; t++) {
-        interp_c2i(&c->uq, u, t, 0, N + 1, 1, N + 1);
-        interp_c2i(&c->vq, v, t, 1, N + 1, 1, N + 1);
+        interp_c2i(&c->uq, u, t, 0, N + 1, 1, N + 1, c->ord);
+        interp_c2i(&c->vq, v, t, 1, N + 1, 1, N + 1, c->ord);
     }
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= N + 1; j++)
@@ -840,8 +898,8 @@ static void op_co2contra(orc_ctx *c, fld_t *ut, fld_t *vt, fld_t *u, fld_t *v)
     /* interp_pvec2uv_Ch (interpolator_p2uv_mod.f90:71-99) */
     exch_do(&c->ex_xy3_full_v, &c->uq, &c->vq);
     for (int t = 0; t < NPAN; t++) {
-        interp_i2c(ut, &c->uq, t, 0, N, 1, N + 1);
-        interp_i2c(vt, &c->vq, t, 1, N, 1, N + 1);
+        interp_i2c(ut, &c->uq, t, 0, N, 1, N + 1, c->ord);
+        interp_i2c(vt, &c->vq, t, 1, N, 1, N + 1, c->ord);
     }
     for (int t = 0; t < NPAN; t++) {
         for (int j = 1; j <= N + 1; j++)
@@ -897,8 +955,8 @@ static void op_coriolis(orc_ctx *c, fld_t *cu, fld_t *cv, fld_t *ut, fld_t *vt)
     exch_do(&c->ex_ch3_u, ut, vt);
     exch_do(&c->ex_ch3_v, ut, vt);
     for (int t = 0; t < NPAN; t++) {
-        interp_c2i(&c->up, ut, t, 0, N + 1, 1, N + 1);
-        interp_c2i(&c->vp, vt, t, 1, N + 1, 1, N + 1);
+        interp_c2i(&c->up, ut, t, 0, N + 1, 1, N + 1, c->ord);
+        interp_c2i(&c->vp, vt, t, 1, N + 1, 1, N + 1, c->ord);
     }
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= N + 1; j++)
@@ -914,8 +972,8 @@ static void op_coriolis(orc_ctx *c, fld_t *cu, fld_t *cv, fld_t *ut, fld_t *vt)
     for (int t = 0; t < NPAN; t++) sync_grad_on_edges(c, &c->vp, &c->up, t);
     exch_do(&c->ex_xy3_full_v, &c->up, &c->vp);
     for (int t = 0; t < NPAN; t++) {
-        interp_i2c(cu, &c->up, t, 0, N, 1, N + 1);
-        interp_i2c(cv, &c->vp, t, 1, N, 1, N + 1);
+        interp_i2c(cu, &c->up, t, 0, N, 1, N + 1, c->ord);
+        interp_i2c(cv, &c->vp, t, 1, N, 1, N + 1, c->ord);
         for (int j = 1; j <= N + 1; j++)
             for (int i = 1; i <= N; i++) FA(cu, t, i, j) = FA(cu, t, i, j) / c->my.J[MI(&c->my, t, i, j)];
         for (int j = 1; j <= N; j++)
@@ -950,8 +1008,8 @@ static void op_div(orc_ctx *c, fld_t *div, fld_t *ut, fld_t *vt)
     exch_do(&c->ex_ch3_u, &c->Ju, &c->Jv);
     exch_do(&c->ex_ch3_v, &c->Ju, &c->Jv);
     for (int t = 0; t < NPAN; t++) {
-        diff_c2i(&c->Dx, &c->Ju, t, 0, N + 1, 1, N + 1);
-        diff_c2i(&c->Dy, &c->Jv, t, 1, N + 1, 1, N + 1);
+        diff_c2i(&c->Dx, &c->Ju, t, 0, N + 1, 1, N + 1, c->ord);
+        diff_c2i(&c->Dy, &c->Jv, t, 1, N + 1, 1, N + 1, c->ord);
         for (int j = 1; j <= N + 1; j++)
             for (int i = 1; i <= N + 1; i++)
                 FA(div, t, i, j) = (FA(&c->Dx, t, i, j) / c->mxy.hx + FA(&c->Dy, t, i, j) / c->mxy.hy) /
@@ -1309,14 +1367,14 @@ static void op_vec_adv(orc_ctx *c, fld_t *utd, fld_t *vtd, fld_t *u, fld_t *v, f
     exch_do(&c->ex_ch3_u, ut, vt);
     exch_do(&c->ex_ch3_v, ut, vt);
     for (int t = 0; t < NPAN; t++) {
-        interp_c2i(&c->uh, ut, t, 0, N + 1, 1, N + 1);
-        interp_c2i(&c->vh, vt, t, 1, N + 1, 1, N + 1);
+        interp_c2i(&c->uh, ut, t, 0, N + 1, 1, N + 1, c->ord);
+        interp_c2i(&c->vh, vt, t, 1, N + 1, 1, N + 1, c->ord);
     }
     /* interp2d_pvec2uv_Ch_sbp42 on (vh, uh): v_at_u = I_i2c,x(vh), u_at_v = I_i2c,y(uh)
        (its xy exchange fills halos that the SBP interpolation does not read) */
     for (int t = 0; t < NPAN; t++) {
-        interp_i2c(&c->vau, &c->vh, t, 0, N, 1, N + 1);
-        interp_i2c(&c->uav, &c->uh, t, 1, N, 1, N + 1);
+        interp_i2c(&c->vau, &c->vh, t, 0, N, 1, N + 1, c->ord);
+        interp_i2c(&c->uav, &c->uh, t, 1, N, 1, N + 1, c->ord);
     }
     /* u_halo = u, v_halo = v, then the ECS Ch vector halo of width 3 */
     for (int t = 0; t < NPAN; t++) {
@@ -1446,6 +1504,19 @@ int orc_N(const orc_ctx *c) { return c->N; }
 
 /* operator kind: 0 linear_swm_operator, 1 advective_swm_operator (covariant Ch) */
 void orc_set_operator(orc_ctx *c, int kind) { c->nonlinear = kind == 1; }
+
+/* SBP order of the Ch operators (the _21 / _42 operator names of the reference's
+   factories: grad_ch_sbp_sat_*, div_ch_sbp_sat_*_proj, co2contra_ch_sbp*,
+   coriolis_Ch_sbp*, SBP_C*_quadrature); returns 0, or -1 for an unknown order. */
+int orc_set_sbp_order(orc_ctx *c, int ord)
+{
+    if (ord != 21 && ord != 42) return -1;
+    c->ord = ord;
+    mesh_mass(&c->mxy, ord);
+    mesh_mass(&c->mx, ord);
+    mesh_mass(&c->my, ord);
+    return 0;
+}
 
 void orc_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv)
 {
@@ -1625,6 +1696,32 @@ void orc_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int
    coefficient tables: op 0 = i2c difference (in: n+1 nodes, out: n centres),
    1 = c2i difference (in: n centres, out: n+1 nodes, no SAT), 2 = i2c
    interpolation, 3 = c2i interpolation.  Halo inputs are taken as zero. */
+void orc_sbp1d(int op, int n, const double *in, double *out);
+
+/* The same probe for SBP order ord (21 or 42); the 2-1 stencils restate
+   sbp_diff_i2c_21_mod.f90:33-41, sbp_diff_c2i_21_mod.f90:32-42,
+   sbp_interp_i2c_21_mod.f90:25-31 and sbp_interp_c2i_21_mod.f90:25-35 (no SAT). */
+void orc_sbp1d_ord(int ord, int op, int n, const double *in, double *out)
+{
+    if (ord != 21) { orc_sbp1d(op, n, in, out); return; }
+#define X(k) in[(k) - 1]
+    switch (op) {
+    case 0: for (int k = 1; k <= n; k++) out[k - 1] = X(k + 1) - X(k); break;
+    case 1:
+        out[0] = X(2) - X(1);
+        for (int k = 2; k <= n; k++) out[k - 1] = X(k) - X(k - 1);
+        out[n] = X(n) - X(n - 1);
+        break;
+    case 2: for (int k = 1; k <= n; k++) out[k - 1] = 0.5 * (X(k + 1) + X(k)); break;
+    default:
+        out[0] = X(1);
+        for (int k = 2; k <= n; k++) out[k - 1] = 0.5 * (X(k) + X(k - 1));
+        out[n] = X(n);
+        break;
+    }
+#undef X
+}
+
 void orc_sbp1d(int op, int n, const double *in, double *out)
 {
     init_coeffs();
@@ -1670,8 +1767,8 @@ void orc_sbp1d(int op, int n, const double *in, double *out)
 #undef I2
         break;
     }
-    case 2: interp_i2c(&b, &a, 0, 0, n, 1, 1); break;
-    default: interp_c2i(&b, &a, 0, 0, n + 1, 1, 1); break;
+    case 2: interp_i2c(&b, &a, 0, 0, n, 1, 1, 42); break;
+    default: interp_c2i(&b, &a, 0, 0, n + 1, 1, 1, 42); break;
     }
     int nout = (op == 0 || op == 2) ? n : n + 1;
     for (int i = 1; i <= nout; i++) out[i - 1] = FA(&b, 0, i, 1);
