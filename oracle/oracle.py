@@ -78,7 +78,7 @@ def shapes(N: int):
 
 
 class Oracle:
-    """FP64 CPU restatement of the linear Ch shallow-water operator (SBP 4-2 or 2-1) and RK4."""
+    """FP64 CPU restatement of the linear Ch shallow-water operator (SBP 4-2, 2-1 or 6-3) and RK4."""
 
     OPERATORS = {"linear": 0, "advective": 1}
 
@@ -86,9 +86,10 @@ class Oracle:
                  omega: float = EARTH_OMEGA, h_mean: float = 1000.0, axis=(0.0, 0.0, 1.0),
                  coriolis_constant: bool = False, operator: str = "linear", sbp_order: int = 42):
         """operator: 'linear' (linear_swm_operator) or 'advective' (advective_swm_operator,
-        covariant Ch branch: up4 mass flux and up4 vector advection).  sbp_order: 42 or
-        21, the order of the Ch difference, interpolation and quadrature operators (the
-        _sbp_sat_42 / _sbp_sat_21 operator names of the reference's factories)."""
+        covariant Ch branch: up4 mass flux and up4 vector advection).  sbp_order: 42, 21
+        or 63 (N >= 16), the order of the Ch difference, interpolation and quadrature
+        operators (the _sbp_sat_42 / _21 / _63 operator names of the reference's
+        factories)."""
         self.N = N
         self.radius, self.grav, self.omega, self.h_mean = radius, grav, omega, h_mean
         self.axis = np.ascontiguousarray(axis, dtype=np.float64)
@@ -99,7 +100,7 @@ class Oracle:
         lib().orc_set_operator(self._c, self.OPERATORS[operator])
         self.sbp_order = int(sbp_order)
         if lib().orc_set_sbp_order(self._c, self.sbp_order) != 0:
-            raise ValueError(f"oracle: unsupported SBP order {sbp_order} (21 or 42)")
+            raise ValueError(f"oracle: unsupported SBP order {sbp_order} (21, 42, or 63 with N >= 16)")
 
     def __del__(self):
         c = getattr(self, "_c", None)
@@ -196,7 +197,7 @@ class Oracle:
 
 
 def sbp1d(op: int, n: int, x, order: int = 42) -> np.ndarray:
-    """One-dimensional SBP operator (order 42 or 21) on one line (0 i2c diff, 1 c2i diff,
+    """One-dimensional SBP operator (order 42, 21 or 63) on one line (0 i2c diff, 1 c2i diff,
     both without SAT, 2 i2c interpolation, 3 c2i interpolation)."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     nout = n if op in (0, 2) else n + 1

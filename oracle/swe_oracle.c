@@ -67,6 +67,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include "sbp63.h"
 
 #define NPAN 6
 
@@ -489,8 +490,10 @@ static const double A21_C[2] = {1.0, 1.0};
 /* quadrature edge weights of the mesh's two directions for SBP order ord */
 static void mesh_mass(mesh_t *m, int ord)
 {
-    const double *ei = ord == 21 ? A21_I : A42_I, *ec = ord == 21 ? A21_C : A42_C;
-    const int ni = ord == 21 ? 2 : 5, nc = ord == 21 ? 2 : 4;
+    /* D63_A_interfaces / D63_A_centers (sbp_operators_collection_mod.f90:199-200) */
+    const double *ei = ord == 21 ? A21_I : (ord == 63 ? SBP63_H_I : A42_I);
+    const double *ec = ord == 21 ? A21_C : (ord == 63 ? SBP63_H_C : A42_C);
+    const int ni = ord == 21 ? 2 : 5, nc = ord == 21 ? 2 : (ord == 63 ? 6 : 4);
     mass_coeffs(m->Ax, m->nx, m->shift_i == 0.0 ? ei : ec, m->shift_i == 0.0 ? ni : nc);
     mass_coeffs(m->Ay, m->ny, m->shift_j == 0.0 ? ei : ec, m->shift_j == 0.0 ? ni : nc);
 }
@@ -565,6 +568,10 @@ static const double DC_q11 = -2.0, DC_q12 = 3.0, DC_q13 = -1.0, DC_q21 = -1.0, D
    projection R11, R12 */
 static const double S21_DI_h11 = 1.0, S21_DI_h22 = 1.0, S21_DC_h11 = 0.5;
 static const double S21_R11 = 3.0 / 2.0, S21_R12 = -1.0 / 2.0;
+/* SBP 6-3: coefficient tables (sbp63.h) and closure-row widths of the i2c and c2i
+   operators (sbp_diff_i2c_63_mod.f90:84-134, sbp_diff_c2i_63_mod.f90:82-124) */
+static const int S63_WI[6] = {5, 5, 6, 7, 8, 9};
+static const int S63_WC[5] = {6, 6, 6, 6, 7};
 /* interpolation free parameters */
 static const double C13 = 0.1264926207034815, C14 = -0.029892648949074313;
 static double II_q[15], IC_q[15];
@@ -616,6 +623,29 @@ static void diff_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls,
 {
 #define O(k) (*((dir) == 0 ? &FA(out, t, k, l) : &FA(out, t, l, k)))
 #define I(k) L(in, t, dir, k, l)
+    if (ord == 63) {
+        /* sbp_diff_i2c_63_mod.f90:84-134 (rows), :335-395 (SAT on rows 1..4) */
+        const double *C = SBP63_DI_C;
+        for (int l = ls; l <= le; l++) {
+            for (int r = 1; r <= 6; r++) {
+                double a = 0.0, b = 0.0;
+                for (int j = 0; j < S63_WI[r - 1]; j++) {
+                    a += SBP63_DI_Q[r - 1][j] * I(j + 1);
+                    b -= SBP63_DI_Q[r - 1][j] * I(n + 1 - j);
+                }
+                O(r) = a;
+                O(n + 1 - r) = b;
+            }
+            for (int k = 7; k <= n - 6; k++)
+                O(k) = C[0] * (I(k + 1) - I(k)) + C[1] * (I(k + 2) - I(k - 1)) + C[2] * (I(k + 3) - I(k - 2));
+        }
+        for (int l = ls; l <= le; l++)
+            for (int r = 1; r <= 4; r++) {
+                O(r) = O(r) + 0.5 * SBP63_R[r - 1] / SBP63_H_C[r - 1] * (I(1) - I(0));
+                O(n + 1 - r) = O(n + 1 - r) + 0.5 * SBP63_R[r - 1] / SBP63_H_C[r - 1] * (I(n + 2) - I(n + 1));
+            }
+        return;
+    }
     if (ord == 21) {
         for (int l = ls; l <= le; l++)
             for (int k = 1; k <= n; k++) O(k) = I(k + 1) - I(k);
@@ -651,6 +681,33 @@ static void diff_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls,
    ord 21: sbp_diff_c2i_21_t (sbp_diff_c2i_21_mod.f90:24-146). */
 static void diff_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le, int ord)
 {
+    if (ord == 63) {
+        /* sbp_diff_c2i_63_mod.f90:82-124 (rows), :267-327 (SAT) */
+        const double *C = SBP63_DC_C;
+        for (int l = ls; l <= le; l++) {
+            for (int r = 1; r <= 5; r++) {
+                double a = 0.0, b = 0.0;
+                for (int j = 0; j < S63_WC[r - 1]; j++) {
+                    a += SBP63_DC_Q[r - 1][j] * I(j + 1);
+                    b -= SBP63_DC_Q[r - 1][j] * I(nx - 1 - j);
+                }
+                O(r) = a;
+                O(nx + 1 - r) = b;
+            }
+            for (int k = 6; k <= nx - 5; k++)
+                O(k) = C[0] * (I(k) - I(k - 1)) + C[1] * (I(k + 1) - I(k - 2)) + C[2] * (I(k + 2) - I(k - 3));
+        }
+        for (int l = ls; l <= le; l++) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int k = 1; k <= 4; k++) {
+                s1 += SBP63_R[k - 1] * (I(k) - I(1 - k));
+                s2 += SBP63_R[k - 1] * (I(nx - 1 + k) - I(nx - k));
+            }
+            O(1) = O(1) + 0.5 / SBP63_H_I[0] * s1;
+            O(nx) = O(nx) + 0.5 / SBP63_H_I[0] * s2;
+        }
+        return;
+    }
     if (ord == 21) {
         for (int l = ls; l <= le; l++) {
             O(1) = I(2) - I(1);
@@ -684,6 +741,24 @@ static void diff_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls
    ord 21: sbp_interp_i2c_21_t (sbp_interp_i2c_21_mod.f90:17-56). */
 static void interp_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le, int ord)
 {
+    if (ord == 63) {
+        /* sbp_interp_i2c_63_mod.f90:82-130 */
+        const double *C = SBP63_II_C;
+        for (int l = ls; l <= le; l++) {
+            for (int r = 1; r <= 6; r++) {
+                double a = 0.0, b = 0.0;
+                for (int j = 0; j < S63_WI[r - 1]; j++) {
+                    a += SBP63_II_Q[r - 1][j] * I(j + 1);
+                    b += SBP63_II_Q[r - 1][j] * I(n + 1 - j);
+                }
+                O(r) = a;
+                O(n + 1 - r) = b;
+            }
+            for (int k = 7; k <= n - 6; k++)
+                O(k) = C[0] * (I(k + 1) + I(k)) + C[1] * (I(k + 2) + I(k - 1)) + C[2] * (I(k + 3) + I(k - 2));
+        }
+        return;
+    }
     if (ord == 21) {
         for (int l = ls; l <= le; l++)
             for (int k = 1; k <= n; k++) O(k) = 0.5 * (I(k + 1) + I(k));
@@ -705,6 +780,24 @@ static void interp_i2c(fld_t *out, const fld_t *in, int t, int dir, int n, int l
    ord 21: sbp_interp_c2i_21_t (sbp_interp_c2i_21_mod.f90:17-84). */
 static void interp_c2i(fld_t *out, const fld_t *in, int t, int dir, int nx, int ls, int le, int ord)
 {
+    if (ord == 63) {
+        /* sbp_interp_c2i_63_mod.f90:70-112 */
+        const double *C = SBP63_IC_C;
+        for (int l = ls; l <= le; l++) {
+            for (int r = 1; r <= 5; r++) {
+                double a = 0.0, b = 0.0;
+                for (int j = 0; j < S63_WC[r - 1]; j++) {
+                    a += SBP63_IC_Q[r - 1][j] * I(j + 1);
+                    b += SBP63_IC_Q[r - 1][j] * I(nx - 1 - j);
+                }
+                O(r) = a;
+                O(nx + 1 - r) = b;
+            }
+            for (int k = 6; k <= nx - 5; k++)
+                O(k) = C[0] * (I(k) + I(k - 1)) + C[1] * (I(k + 1) + I(k - 2)) + C[2] * (I(k + 2) + I(k - 3));
+        }
+        return;
+    }
     if (ord == 21) {
         for (int l = ls; l <= le; l++) {
             O(1) = I(1);
@@ -742,6 +835,7 @@ typedef struct orc_ctx {
     double *qb, *qt, *ql, *qr;   /* covariant ECS Ah sync weights, length N+1 */
     exch_t ex_xy3_full_s, ex_xy3_full_v, ex_xy1_full_s, ex_xy1_cross_v;
     exch_t ex_ch3_u, ex_ch3_v;   /* Ch: fills x-mesh field / y-mesh field */
+    exch_t ex_ch4_u, ex_ch4_v;   /* width 4: the SBP 6-3 divergence SAT reads four halo depths */
     /* work fields */
     fld_t h, u, v, du, dv, dh;
     fld_t gx, gy, ut, vt, uq, vq, up, vp, Ju, Jv, Dx, Dy, div;
@@ -821,6 +915,8 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     build_xy_exchange(&c->ex_xy1_cross_v, N, 1, 1, PK_VEC);
     build_ch_exchange(&c->ex_ch3_u, N, 3, 0, 1);
     build_ch_exchange(&c->ex_ch3_v, N, 3, 0, 0);
+    build_ch_exchange(&c->ex_ch4_u, N, 4, 0, 1);
+    build_ch_exchange(&c->ex_ch4_v, N, 4, 0, 0);
     build_xy_exchange(&c->ex_xy5_full_s, N, 5, 0, PK_SCALAR);
     build_ch_exchange(&c->ex_ch1c_u, N, 1, 1, 1);
     build_ch_exchange(&c->ex_ch1c_v, N, 1, 1, 0);
@@ -1005,8 +1101,8 @@ static void op_div(orc_ctx *c, fld_t *div, fld_t *ut, fld_t *vt)
         for (int j = 1; j <= N; j++)
             for (int i = 1; i <= N + 1; i++) FA(&c->Jv, t, i, j) = FA(vt, t, i, j) * c->mx.J[MI(&c->mx, t, i, j)];
     }
-    exch_do(&c->ex_ch3_u, &c->Ju, &c->Jv);
-    exch_do(&c->ex_ch3_v, &c->Ju, &c->Jv);
+    exch_do(c->ord == 63 ? &c->ex_ch4_u : &c->ex_ch3_u, &c->Ju, &c->Jv);
+    exch_do(c->ord == 63 ? &c->ex_ch4_v : &c->ex_ch3_v, &c->Ju, &c->Jv);
     for (int t = 0; t < NPAN; t++) {
         diff_c2i(&c->Dx, &c->Ju, t, 0, N + 1, 1, N + 1, c->ord);
         diff_c2i(&c->Dy, &c->Jv, t, 1, N + 1, 1, N + 1, c->ord);
@@ -1505,12 +1601,13 @@ int orc_N(const orc_ctx *c) { return c->N; }
 /* operator kind: 0 linear_swm_operator, 1 advective_swm_operator (covariant Ch) */
 void orc_set_operator(orc_ctx *c, int kind) { c->nonlinear = kind == 1; }
 
-/* SBP order of the Ch operators (the _21 / _42 operator names of the reference's
+/* SBP order of the Ch operators (the _21 / _42 / _63 operator names of the reference's
    factories: grad_ch_sbp_sat_*, div_ch_sbp_sat_*_proj, co2contra_ch_sbp*,
    coriolis_Ch_sbp*, SBP_C*_quadrature); returns 0, or -1 for an unknown order. */
 int orc_set_sbp_order(orc_ctx *c, int ord)
 {
-    if (ord != 21 && ord != 42) return -1;
+    if (ord != 21 && ord != 42 && ord != 63) return -1;
+    if (ord == 63 && c->N < 16) return -1;
     c->ord = ord;
     mesh_mass(&c->mxy, ord);
     mesh_mass(&c->mx, ord);
@@ -1703,6 +1800,42 @@ void orc_sbp1d(int op, int n, const double *in, double *out);
    sbp_interp_i2c_21_mod.f90:25-31 and sbp_interp_c2i_21_mod.f90:25-35 (no SAT). */
 void orc_sbp1d_ord(int ord, int op, int n, const double *in, double *out)
 {
+    if (ord == 63) {
+        /* rows of the 6-3 operators on one line, zero halo, without SAT */
+        const int nin = (op == 0 || op == 2) ? n + 1 : n;
+        fld_t a, b;
+        fld_init(&a, nin, 1, 5);
+        fld_init(&b, (op == 0 || op == 2) ? n : n + 1, 1, 5);
+        for (int t = 0; t < NPAN; t++)
+            for (int i = -4; i <= nin + 5; i++) FA(&a, t, i, 1) = 0.0;
+        for (int i = 1; i <= nin; i++) FA(&a, 0, i, 1) = in[i - 1];
+        if (op == 0) {
+            diff_i2c(&b, &a, 0, 0, n, 1, 1, 63);
+            /* undo the SAT: the halo is zero, so row r carries 0.5 R_r/h_r f(1) */
+            for (int r = 1; r <= 4; r++) {
+                FA(&b, 0, r, 1) -= 0.5 * SBP63_R[r - 1] / SBP63_H_C[r - 1] * FA(&a, 0, 1, 1);
+                FA(&b, 0, n + 1 - r, 1) -= 0.5 * SBP63_R[r - 1] / SBP63_H_C[r - 1] * (0.0 - FA(&a, 0, n + 1, 1));
+            }
+        } else if (op == 1) {
+            diff_c2i(&b, &a, 0, 0, n + 1, 1, 1, 63);
+            double s1 = 0.0, s2 = 0.0;
+            for (int k = 1; k <= 4; k++) {
+                s1 += SBP63_R[k - 1] * (FA(&a, 0, k, 1) - FA(&a, 0, 1 - k, 1));
+                s2 += SBP63_R[k - 1] * (FA(&a, 0, n + k, 1) - FA(&a, 0, n + 1 - k, 1));
+            }
+            FA(&b, 0, 1, 1) -= 0.5 / SBP63_H_I[0] * s1;
+            FA(&b, 0, n + 1, 1) -= 0.5 / SBP63_H_I[0] * s2;
+        } else if (op == 2) {
+            interp_i2c(&b, &a, 0, 0, n, 1, 1, 63);
+        } else {
+            interp_c2i(&b, &a, 0, 0, n + 1, 1, 1, 63);
+        }
+        const int nout = (op == 0 || op == 2) ? n : n + 1;
+        for (int i = 1; i <= nout; i++) out[i - 1] = FA(&b, 0, i, 1);
+        fld_free(&a);
+        fld_free(&b);
+        return;
+    }
     if (ord != 21) { orc_sbp1d(op, n, in, out); return; }
 #define X(k) in[(k) - 1]
     switch (op) {

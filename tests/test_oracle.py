@@ -8,9 +8,9 @@ import pytest
 from oracle.oracle import EARTH_GRAV, EARTH_RADIUS, Oracle
 
 
-@pytest.fixture(scope="module", params=[42, 21], ids=["sbp42", "sbp21"])
+@pytest.fixture(scope="module", params=[42, 21, 63], ids=["sbp42", "sbp21", "sbp63"])
 def o24(oracle_built, request):
-    """C24 oracle with the SBP 4-2 and the SBP 2-1 Ch operators."""
+    """C24 oracle with the SBP 4-2, 2-1 and 6-3 Ch operators."""
     return Oracle(24, sbp_order=request.param)
 
 
@@ -111,6 +111,46 @@ def test_linear_williamson2_steady_state_converges_sbp21(oracle_built):
         errs.append(np.abs(h1 - h).max() / np.abs(h).max())
     order = np.log2(errs[0] / errs[1])
     assert order > 1.0, (errs, order)
+
+
+def test_linear_williamson2_steady_state_converges_sbp63(oracle_built):
+    """SBP 6-3 (sixth order inside, third at the panel edges): the TS2 error after
+    1/4 day falls at better than third order and below the 4-2 error at C32."""
+    errs = []
+    axis = (np.sin(0.7), 0.0, np.cos(0.7))
+    for N in (16, 32):
+        o = Oracle(N, h_mean=29400 / EARTH_GRAV, axis=axis, sbp_order=63)
+        u0 = 2 * np.pi * EARTH_RADIUS / (12 * 86400)
+        h, u, v = o.ts2(u0=u0, h_mean=29400 / EARTH_GRAV, axis=axis, linear_mode=True)
+        dt = 900.0 * 32 / N
+        nsteps = int(round(6 * 3600.0 / dt))
+        h1, _, _ = o.rk4(h, u, v, dt, nsteps)
+        errs.append(np.abs(h1 - h).max() / np.abs(h).max())
+    order = np.log2(errs[0] / errs[1])
+    assert order > 3.0, (errs, order)
+
+
+@pytest.mark.parametrize("deg", [0, 1, 2, 3])
+def test_sbp63_polynomial_exactness(oracle_built, deg):
+    """The 6-3 differences are exact for polynomials of degree <= 3, the
+    interpolations for degree <= 2 (third-order closures); interior rows exact to
+    degree 5."""
+    from oracle.oracle import sbp1d
+    n = 30
+    xn = np.linspace(0.0, 1.0, n + 1)
+    xc = 0.5 * (xn[:-1] + xn[1:])
+    hx = xn[1] - xn[0]
+    f = lambda x: x ** deg
+    df = lambda x: deg * x ** (deg - 1) if deg else 0 * x
+    assert np.allclose(sbp1d(0, n, f(xn), order=63) / hx, df(xc), atol=1e-11)
+    assert np.allclose(sbp1d(1, n, f(xc), order=63) / hx, df(xn), atol=1e-11)
+    if deg <= 2:
+        assert np.allclose(sbp1d(2, n, f(xn), order=63), f(xc), atol=1e-12)
+        assert np.allclose(sbp1d(3, n, f(xc), order=63), f(xn), atol=1e-12)
+    g = lambda x: x ** 5
+    inner = slice(8, n - 8)
+    assert np.allclose(sbp1d(0, n, g(xn), order=63)[inner] / hx, 5 * xc[inner] ** 4, atol=1e-9)
+    assert np.allclose(sbp1d(3, n, g(xc), order=63)[inner], g(xn)[inner], atol=1e-12)
 
 
 @pytest.mark.parametrize("deg", [0, 1])
