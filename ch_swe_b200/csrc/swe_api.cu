@@ -285,21 +285,25 @@ static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
 // SBP 2-1 stage kernels (linear operator): the first blocks-per-SM value of each
 // tile, one output per element.
 #define CHSWE_LINEAR21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
+// SBP 6-3 stage kernels: the same configurations
+#define CHSWE_LINEAR63_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 struct KernelCfg {
     int tile, occ, runs;
 };
 #define CHSWE_CFG_ENTRY(TM, OCC, RUNS) {TM, OCC, RUNS},
 static const KernelCfg k_cfgs[] = {CHSWE_LINEAR_CFGS(CHSWE_CFG_ENTRY)};
 static const KernelCfg k_cfgs21[] = {CHSWE_LINEAR21_CFGS(CHSWE_CFG_ENTRY)};
+static const KernelCfg k_cfgs63[] = {CHSWE_LINEAR63_CFGS(CHSWE_CFG_ENTRY)};
 #undef CHSWE_CFG_ENTRY
 static const int N_CFGS = sizeof(k_cfgs) / sizeof(k_cfgs[0]);
 static const int N_CFGS21 = sizeof(k_cfgs21) / sizeof(k_cfgs21[0]);
+static const int N_CFGS63 = sizeof(k_cfgs63) / sizeof(k_cfgs63[0]);
 static int default_occ(int tm) { return tm == 17 ? 3 : 2; }
 // the configurations built for SBP order ord
 static const KernelCfg *cfgs_of(int ord, int *count)
 {
-    *count = ord == 21 ? N_CFGS21 : N_CFGS;
-    return ord == 21 ? k_cfgs21 : k_cfgs;
+    *count = ord == 21 ? N_CFGS21 : (ord == 63 ? N_CFGS63 : N_CFGS);
+    return ord == 21 ? k_cfgs21 : (ord == 63 ? k_cfgs63 : k_cfgs);
 }
 static bool valid_cfg(int ord, int tm, int occ, int runs)
 {
@@ -310,6 +314,8 @@ static bool valid_cfg(int ord, int tm, int occ, int runs)
     return false;
 }
 static constexpr int cfg_code(int tm, int occ, int runs) { return tm * 100 + occ * 10 + runs; }
+// edge-strip lines per panel side for SBP order ord
+static int ord_strip_lines(int ord) { return ord == 63 ? strip_lines<63>() : strip_lines<42>(); }
 // Default before autotuning: tiles of about 24 points for the smaller cubes.
 static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
@@ -334,8 +340,9 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t box = (size_t)c->dims.ps;
-    // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1 + the edge tables (44 of N+1)
-    const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1) + 44 * (size_t)(N + 1);
+    // 8 panel-independent boxes + fJ2 (6 boxes) + 4 edge vectors of N+1 + the edge tables
+    // (ej: 4 sides x up to 7 lines, ef: 24, ea: 4, each of N+1)
+    const size_t n_el = 8 * box + 6 * box + 4 * (size_t)(N + 1) + 56 * (size_t)(N + 1);
     std::vector<T> h(n_el, T(0));
     HostMetric my = host_metric(N, 0.5, 0.0), mx = host_metric(N, 0.0, 0.5), mxy = host_metric(N, 0.0, 0.0);
     const double a = c->cfg.radius;
@@ -384,14 +391,14 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
     v.Q11y = d; v.iJy = d + box; v.Jy = d + 2 * box; v.Q22x = d + 3 * box; v.iJx = d + 4 * box; v.Jx = d + 5 * box;
     v.JQ12 = d + 6 * box; v.iJa = d + 7 * box; v.fJ2 = d + 8 * box;
     v.qb = d + 14 * box; v.qt = v.qb + (N + 1); v.ql = v.qt + (N + 1); v.qr = v.ql + (N + 1);
-    T *ej = d + 14 * box + 4 * (N + 1), *ef = ej + 16 * (N + 1), *ea = ef + 24 * (N + 1);
+    T *ej = d + 14 * box + 4 * (N + 1), *ef = ej + 28 * (N + 1), *ea = ef + 24 * (N + 1);
     v.ej = ej; v.ef = ef; v.ea = ea;
     const double pi = 3.141592653589793238462643383279502884;
     const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
     v.inv_hxa = T(1.0 / (hx * a));
     v.inv_hx = T(1.0 / hx);
     v.grav = T(c->cfg.grav);
-    k_edge_tables<T><<<(N + 1 + 127) / 128, 128, 0, c->stream>>>(v, c->dims, ej, ef, ea);
+    k_edge_tables<T><<<(N + 1 + 127) / 128, 128, 0, c->stream>>>(v, c->dims, ej, ef, ea, ord_strip_lines(c->ord));
     CU(c, cudaGetLastError());
     CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
@@ -631,10 +638,11 @@ static int build_quadrature(swe_ctx *c)
     const double AI42[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
     const double AC42[4] = {13.0 / 12.0, 7.0 / 8.0, 25.0 / 24.0, 1.0};
     const double AI21[2] = {0.5, 1.0}, AC21[2] = {1.0, 1.0};
-    const bool o21 = c->ord == 21;
+    // D63_A_interfaces / D63_A_centers: the 6-3 norms (sbp_operators_collection_mod.f90:199-200)
+    const bool o21 = c->ord == 21, o63 = c->ord == 63;
     auto coeff = [&](int i, int n, bool iface) {
-        const double *e = iface ? (o21 ? AI21 : AI42) : (o21 ? AC21 : AC42);
-        int ne = o21 ? 2 : (iface ? 5 : 4);
+        const double *e = iface ? (o21 ? AI21 : (o63 ? SBP63_H_I : AI42)) : (o21 ? AC21 : (o63 ? SBP63_H_C : AC42));
+        int ne = o21 ? 2 : (o63 ? (iface ? 5 : 6) : (iface ? 5 : 4));
         double A = 1.0;
         if (i <= ne) A = e[i - 1];
         if (i >= n - ne + 1) A = e[n - i];
@@ -708,9 +716,11 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
         (cfg->operator_kind != SWE_OP_LINEAR && cfg->operator_kind != SWE_OP_ADVECTIVE) || !(cfg->radius > 0.0))
         return SWE_EINVAL;
-    // SBP order: 4-2 (0 selects it too) or 2-1, the latter for the linear operator
+    // SBP order: 4-2 (0 selects it too), 2-1 or 6-3 (N >= 16), the last two for the linear operator
     const int ord = cfg->sbp_order == 0 ? 42 : cfg->sbp_order;
-    if ((ord != 42 && ord != 21) || (ord == 21 && cfg->operator_kind != SWE_OP_LINEAR)) return SWE_EINVAL;
+    if ((ord != 42 && ord != 21 && ord != 63) || (ord != 42 && cfg->operator_kind != SWE_OP_LINEAR) ||
+        (ord == 63 && cfg->N < 16))
+        return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
     swe_ctx *c = new swe_ctx();
@@ -752,7 +762,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
         const size_t eb = (size_t)cfg->n_members * NPAN * 4 * (N + 1) * 3 * c->elem;
         if (cudaMalloc(&c->edge, eb) != cudaSuccess) return bail(SWE_ENOMEM);
         if (cudaMemset(c->edge, 0, eb) != cudaSuccess) return bail(SWE_ECUDA);
-        const size_t sb = (size_t)strip_member(N, cfg->n_members) * c->elem;
+        const size_t sb = (size_t)strip_member(N, cfg->n_members, ord_strip_lines(ord)) * c->elem;
         if (cudaMalloc(&c->es, sb) != cudaSuccess) return bail(SWE_ENOMEM);
         if (cudaMemset(c->es, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
         if (cfg->operator_kind == SWE_OP_ADVECTIVE) {
@@ -1051,25 +1061,32 @@ static cudaError_t stage_smem_optin()
         e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 21>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                  (int)Co2Layout<T, TM>::bytes());                                                \
     if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 21>();
+#define CHSWE_OPTIN_LIN63(TM, OCC, RUNS)                                                                          \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 63>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)Co2Layout<T, TM>::bytes());                                                \
+    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 63>();
 #define CHSWE_OPTIN_ADV(TM, OCC, RUNS) \
     if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, true, RUNS, 42>();
     CHSWE_LINEAR_CFGS(CHSWE_OPTIN_LIN)
     CHSWE_LINEAR21_CFGS(CHSWE_OPTIN_LIN21)
+    CHSWE_LINEAR63_CFGS(CHSWE_OPTIN_LIN63)
     CHSWE_ADV_CFGS(CHSWE_OPTIN_ADV)
 #undef CHSWE_OPTIN_LIN
 #undef CHSWE_OPTIN_LIN21
+#undef CHSWE_OPTIN_LIN63
 #undef CHSWE_OPTIN_ADV
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
-// ord: SBP order (42 or 21); codes of order 21 are offset by 100000.
+// ord: SBP order (42, 21 or 63); codes of order 21 are offset by 100000, of 63 by 200000.
 template <class T>
 static void launch_co2contra(int tm, int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                              const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
     const dim3 g = stage_grid(d.N, members, tm);
-    switch (cfg_code(tm, occ, runs) + (ord == 21 ? 100000 : 0)) {
+    switch (cfg_code(tm, occ, runs) + (ord == 21 ? 100000 : (ord == 63 ? 200000 : 0))) {
 #define CHSWE_CO2_CASE(TM, OCC, RUNS)                                                                                 \
     case cfg_code(TM, OCC, RUNS):                                                                                 \
         launch_k(k_co2contra<T, TM, OCC, RUNS, 42>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
@@ -1081,9 +1098,16 @@ static void launch_co2contra(int tm, int occ, int runs, int ord, int members, co
                  dtm);                                                                                            \
         break;
         CHSWE_LINEAR_CFGS(CHSWE_CO2_CASE)
+#define CHSWE_CO2_CASE63(TM, OCC, RUNS)                                                                               \
+    case 200000 + cfg_code(TM, OCC, RUNS):                                                                        \
+        launch_k(k_co2contra<T, TM, OCC, RUNS, 63>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
+                 dtm);                                                                                            \
+        break;
         CHSWE_LINEAR21_CFGS(CHSWE_CO2_CASE21)
+        CHSWE_LINEAR63_CFGS(CHSWE_CO2_CASE63)
 #undef CHSWE_CO2_CASE
 #undef CHSWE_CO2_CASE21
+#undef CHSWE_CO2_CASE63
     default: break;   // configurations are validated when set
     }
 }
@@ -1110,7 +1134,7 @@ static void launch_stage(int tm, int occ, int runs, int ord, int members, const 
                          cudaStream_t st)
 {
     if (a.A) occ = default_occ(tm);
-    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0) + (ord == 21 ? 100000 : 0)) {
+    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0) + (ord == 21 ? 100000 : (ord == 63 ? 200000 : 0))) {
 #define CHSWE_STAGE_CASE(TM, OCC, RUNS)                                                                        \
     case cfg_code(TM, OCC, RUNS):                                                                          \
         launch_stage_modes<T, TM, OCC, false, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
@@ -1119,6 +1143,10 @@ static void launch_stage(int tm, int occ, int runs, int ord, int members, const 
     case 100000 + cfg_code(TM, OCC, RUNS):                                                                 \
         launch_stage_modes<T, TM, OCC, false, RUNS, 21>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
         break;
+#define CHSWE_STAGE_CASE63(TM, OCC, RUNS)                                                                      \
+    case 200000 + cfg_code(TM, OCC, RUNS):                                                                 \
+        launch_stage_modes<T, TM, OCC, false, RUNS, 63>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
+        break;
 #define CHSWE_STAGE_CASE_ADV(TM, OCC, RUNS)                                                                    \
     case 10000 + cfg_code(TM, OCC, RUNS):                                                                  \
         launch_stage_modes<T, TM, OCC, true, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);   \
@@ -1126,9 +1154,11 @@ static void launch_stage(int tm, int occ, int runs, int ord, int members, const 
         CHSWE_LINEAR_CFGS(CHSWE_STAGE_CASE)
         CHSWE_ADV_CFGS(CHSWE_STAGE_CASE_ADV)
         CHSWE_LINEAR21_CFGS(CHSWE_STAGE_CASE21)
+        CHSWE_LINEAR63_CFGS(CHSWE_STAGE_CASE63)
 #undef CHSWE_STAGE_CASE
 #undef CHSWE_STAGE_CASE_ADV
 #undef CHSWE_STAGE_CASE21
+#undef CHSWE_STAGE_CASE63
     default: break;   // configurations are validated when set
     }
 }
@@ -1149,7 +1179,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     const int M = c->cfg.n_members;
     launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
-        launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+        launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
         launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
@@ -1165,7 +1195,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     launch_k(k_havg<T>, dim3(1 + (12 * (N - 1) + HAVG_THREADS - 1) / HAVG_THREADS, M), dim3(HAVG_THREADS), 0, c->stream,
              (T *)yin, (T *)c->hb, c->dims, dtm);
     launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
-    launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
+    launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
              (T *)c->edge, c->dims, mv, dtm);
     launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
     const long long nvh = (long long)NPAN * av.hp * M;
@@ -1409,7 +1439,7 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
     cudaEventRecord(e0, c->stream);
     launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
     cudaEventRecord(e1, c->stream);
-    launch_k(c->ord == 21 ? k_edge<T, 21> : k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+    launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
              (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
@@ -1656,7 +1686,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         dim3 g((n + 15) / 16, (n + 15) / 16), b(16, 16);
         k_noalloc_metric<<<g, b, 0, st>>>(M, N, dm.P, box, cfg->radius, cfg->omega, cfg->rotation_axis[0],
                                           cfg->rotation_axis[1], cfg->rotation_axis[2], cfg->coriolis_constant, fr);
-        k_edge_tables<double><<<(n + 127) / 128, 128, 0, st>>>(mv, dm, ej, ef, ea);
+        k_edge_tables<double><<<(n + 127) / 128, 128, 0, st>>>(mv, dm, ej, ef, ea, STRIP_LINES);
         if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
         nd.cached = *cfg;
         nd.metric_ok = true;

@@ -80,16 +80,22 @@ __device__ __forceinline__ int64_t edge_index(int N, int mem, int t, int s, int 
 //   line 3   : the tangential component on the edge line, at along-edge centre c = 1..N
 // Normal/tangential: ut/vt on the L and R sides, vt/ut on B and T.  Depth counts
 // from the side (L: i = d, R: i = N+1-d, B: j = d, T: j = N+1-d).
+// The lines per side are NDEP + 1 of the SBP order (4 for 4-2 and 2-1, 7 for 6-3).
 constexpr int STRIP_LINES = 4;
+template <int ORD> __host__ __device__ constexpr int strip_lines() { return SbpOrder<ORD>::NDEP + 1; }
 
-__host__ __device__ __forceinline__ int64_t strip_member(int N, int mem) { return (int64_t)mem * NPAN * 4 * STRIP_LINES * (N + 1); }
+__host__ __device__ __forceinline__ int64_t strip_member(int N, int mem, int nl = STRIP_LINES)
+{
+    return (int64_t)mem * NPAN * 4 * nl * (N + 1);
+}
 
 template <class T>
 struct Strips {
     const T *es;   // member base
     int n;         // N + 1
+    int nl;        // lines per side: normal depths 1..nl-1, then the tangential line
     // 1-based line of panel p, side s
-    __device__ __forceinline__ const T *line(int p, int s, int k) const { return es + ((p * 4 + s) * STRIP_LINES + k) * n - 1; }
+    __device__ __forceinline__ const T *line(int p, int s, int k) const { return es + ((p * 4 + s) * nl + k) * n - 1; }
 };
 
 // Position of xy vertex (k, l) along side s (1..N+1).
@@ -106,7 +112,7 @@ __device__ __forceinline__ T sat_halo(const Strips<T> &S, const MetricView<T> &m
 {
     const Link L = c_link[p][s];
     const int n = S.n, bp = nb_along(L, n, b);
-    return T(L.sn) * (m.ej[(L.nside * 4 + dd - 1) * n + bp - 1] * S.line(L.nb, L.nside, dd - 1)[bp]);
+    return T(L.sn) * (m.ej[(L.nside * S.nl + dd - 1) * n + bp - 1] * S.line(L.nb, L.nside, dd - 1)[bp]);
 }
 
 // One raw quantity at along index b of side s of panel p, before any edge sync:
@@ -122,22 +128,37 @@ template <class T, int ORD = 42>
 __device__ __forceinline__ T edge_raw(const Strips<T> &S, const MetricView<T> &m, int p, int s, int b, int q)
 {
     using SB = SbpOrder<ORD>;
-    const int n = S.n, N = n - 1;
+    const int n = S.n, N = n - 1, nl = S.nl;
     const bool lr = s <= SIDE_R, lo = (s == SIDE_L || s == SIDE_B);
-    const T *n1 = S.line(p, s, 0), *n2 = S.line(p, s, 1), *n3 = S.line(p, s, 2), *tg = S.line(p, s, 3);
-    const T *jn = m.ej + s * 4 * n - 1, *jt = m.ej + (s * 4 + 3) * n - 1;
+    const T *tg = S.line(p, s, nl - 1);
+    const T *jn = m.ej + s * nl * n - 1, *jt = m.ej + (s * nl + nl - 1) * n - 1;
     const bool across = lr ? (q == 1 || q == 2) : (q == 0 || q == 3);
     if (q <= 1) {
         const T f = m.ef[(p * 4 + s) * n + b - 1];
-        const T v = across ? T(SB::IC1) * n1[b] + T(SB::IC2) * n2[b] + T(SB::IC3) * n3[b]
-                           : SB::template ic2i<T>(b, n, [&](int c) { return tg[c]; });
+        T v;
+        if (across) {
+            // first c2i interpolation row on the normal lines at depths 1..NDEP
+            v = T(SB::ic1(1)) * S.line(p, s, 0)[b];
+#pragma unroll
+            for (int dd = 2; dd <= SB::NDEP; dd++) v += T(SB::ic1(dd)) * S.line(p, s, dd - 1)[b];
+        } else {
+            v = SB::template ic2i<T>(b, n, [&](int c) { return tg[c]; });
+        }
         return q == 0 ? f * v : -f * v;
     }
     if (across) {
-        const T j1 = jn[b] * n1[b], j2 = jn[n + b] * n2[b], j3 = jn[2 * n + b] * n3[b];
-        const T dd = lo ? T(SB::DC1) * j1 + T(SB::DC2) * j2 + T(SB::DC3) * j3 : -T(SB::DC1) * j1 - T(SB::DC2) * j2 - T(SB::DC3) * j3;
-        const T sat = T(SB::SATC) * (T(SB::R1) * (j1 - sat_halo(S, m, p, s, b, 1)) + T(SB::R2) * (j2 - sat_halo(S, m, p, s, b, 2)) +
-                                 T(SB::R3) * (j3 - sat_halo(S, m, p, s, b, 3)));
+        // J * normal component at depths 1..NDEP; first c2i difference row and the SAT
+        T jd[SB::NDEP];
+#pragma unroll
+        for (int dd = 1; dd <= SB::NDEP; dd++) jd[dd - 1] = jn[(dd - 1) * n + b] * S.line(p, s, dd - 1)[b];
+        T dd = T(SB::dc1(1)) * jd[0];
+#pragma unroll
+        for (int k = 2; k <= SB::NDEP; k++) dd += T(SB::dc1(k)) * jd[k - 1];
+        if (!lo) dd = -dd;
+        T ssum = T(SB::r1(1)) * (jd[0] - sat_halo(S, m, p, s, b, 1));
+#pragma unroll
+        for (int k = 2; k <= SB::NR; k++) ssum += T(SB::r1(k)) * (jd[k - 1] - sat_halo(S, m, p, s, b, k));
+        const T sat = T(SB::SATC) * ssum;
         return lo ? dd + sat : dd - sat;
     }
     auto jtv = [&](int c) { return jt[c] * tg[c]; };
@@ -146,10 +167,10 @@ __device__ __forceinline__ T edge_raw(const Strips<T> &S, const MetricView<T> &m
         // cube corner: the SAT across the other side through this vertex
         const int s2 = lr ? (b == 1 ? SIDE_B : SIDE_T) : (b == 1 ? SIDE_L : SIDE_R);
         const int b2 = lo ? 1 : n;
-        const int c1 = b == 1 ? 1 : N, c2 = b == 1 ? 2 : N - 1, c3 = b == 1 ? 3 : N - 2;
-        const T sat = T(SB::SATC) * (T(SB::R1) * (jtv(c1) - sat_halo(S, m, p, s2, b2, 1)) +
-                                 T(SB::R2) * (jtv(c2) - sat_halo(S, m, p, s2, b2, 2)) +
-                                 T(SB::R3) * (jtv(c3) - sat_halo(S, m, p, s2, b2, 3)));
+        T ssum = T(SB::r1(1)) * (jtv(b == 1 ? 1 : N) - sat_halo(S, m, p, s2, b2, 1));
+#pragma unroll
+        for (int k = 2; k <= SB::NR; k++) ssum += T(SB::r1(k)) * (jtv(b == 1 ? k : N + 1 - k) - sat_halo(S, m, p, s2, b2, k));
+        const T sat = T(SB::SATC) * ssum;
         dd = b == 1 ? dd + sat : dd - sat;
     }
     return dd;
@@ -168,19 +189,20 @@ __device__ __forceinline__ void halo_vec(int t, int s, T upn, T vpn, T &uh, T &v
 }
 
 // Metric on the panel edges, contiguous along each side, for the edge sync:
-//   ej[(s*4 + k)*(N+1) + b-1]: J at the normal component's depth k+1 (k < 3, node b)
-//                              and at the tangential component on the edge line (k = 3, centre b)
+//   ej[(s*nl + k)*(N+1) + b-1]: J at the normal component's depth k+1 (k < nl-1, node b)
+//                               and at the tangential component on the edge line (k = nl-1, centre b)
+//   (nl: the strip lines per side of the SBP order)
 //   ef[(p*4 + s)*(N+1) + b-1]: fJ2 of panel p at boundary vertex b of side s
 //   ea[s*(N+1) + b-1]        : 1/(J a) at boundary vertex b of side s
 template <class T>
-__global__ void k_edge_tables(MetricView<T> m, Dims d, T *ej, T *ef, T *ea)
+__global__ void k_edge_tables(MetricView<T> m, Dims d, T *ej, T *ef, T *ea, int nl)
 {
     const int N = d.N, n = N + 1;
     const int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (b > n) return;
     const GV<T> Jy = mview(m.Jy, d), Jx = mview(m.Jx, d), iJa = mview(m.iJa, d);
     for (int s = 0; s < 4; s++) {
-        for (int k = 1; k <= 3; k++) {
+        for (int k = 1; k <= nl - 1; k++) {
             T v;
             switch (s) {
             case SIDE_L: v = Jy(k, b); break;
@@ -188,7 +210,7 @@ __global__ void k_edge_tables(MetricView<T> m, Dims d, T *ej, T *ef, T *ea)
             case SIDE_B: v = Jx(b, k); break;
             default: v = Jx(b, n - k); break;
             }
-            ej[(s * 4 + k - 1) * n + b - 1] = v;
+            ej[(s * nl + k - 1) * n + b - 1] = v;
         }
         T v = 0;
         if (b <= N) {
@@ -199,7 +221,7 @@ __global__ void k_edge_tables(MetricView<T> m, Dims d, T *ej, T *ef, T *ea)
             default: v = Jy(b, n); break;
             }
         }
-        ej[(s * 4 + 3) * n + b - 1] = v;
+        ej[(s * nl + nl - 1) * n + b - 1] = v;
         int k, l;
         side_vertex(N, s, b, 0, k, l);
         ea[s * n + b - 1] = iJa(k, l);
@@ -233,7 +255,8 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
     if (member_frozen(dtm, mem)) return;
     // Coriolis parts (q 0, 1) from the ut/vt strips, divergence parts (q 2, 3) from
     // the strips of the field whose divergence is taken (ut/vt, or the mass flux)
-    const Strips<T> Sc{ES + strip_member(N, mem), n}, Sd{ESd + strip_member(N, mem), n};
+    constexpr int NL = strip_lines<ORD>();
+    const Strips<T> Sc{ES + strip_member(N, mem, NL), n, NL}, Sd{ESd + strip_member(N, mem, NL), n, NL};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool xs = s <= SIDE_R;
     pdl_trigger();

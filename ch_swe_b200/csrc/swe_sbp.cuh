@@ -10,6 +10,8 @@
 // each end) are selected by a branch that is warp-uniform away from panel edges.
 #pragma once
 
+#include "sbp63.h"
+
 namespace chswe {
 namespace sbp {
 
@@ -136,16 +138,74 @@ __device__ __forceinline__ T ic2i21(int k, int nx, const F &f)
     return T(0.5) * (f(k) + f(k - 1));
 }
 
-// The order-dependent parts of the Ch operators, by SBP order (42 or 21):
+// SBP 6-3 operators (sbp_diff_i2c_63_mod.f90:84-134, sbp_diff_c2i_63_mod.f90:82-124,
+// sbp_interp_i2c_63_mod.f90:82-130, sbp_interp_c2i_63_mod.f90:70-112): six-point
+// interior rows, table-driven closure rows (sbp63.h), mirrored at the far end.
+template <class T, class F>
+__device__ __forceinline__ T di2c63(int k, int n, const F &f)
+{
+    const double *C = D_SBP63_DI_C;
+    if (k >= 7 && k <= n - 6)
+        return T(C[0]) * (f(k + 1) - f(k)) + T(C[1]) * (f(k + 2) - f(k - 1)) + T(C[2]) * (f(k + 3) - f(k - 2));
+    const int w[6] = {5, 5, 6, 7, 8, 9};
+    const bool lo = k <= 6;
+    const int r = lo ? k : n + 1 - k;
+    T a = T(0);
+    for (int j = 0; j < w[r - 1]; j++) a += T(D_SBP63_DI_Q[r - 1][j]) * (lo ? f(j + 1) : f(n + 1 - j));
+    return lo ? a : -a;
+}
+template <class T, class F>
+__device__ __forceinline__ T dc2i63(int k, int nx, const F &f)
+{
+    const double *C = D_SBP63_DC_C;
+    if (k >= 6 && k <= nx - 5)
+        return T(C[0]) * (f(k) - f(k - 1)) + T(C[1]) * (f(k + 1) - f(k - 2)) + T(C[2]) * (f(k + 2) - f(k - 3));
+    const int w[5] = {6, 6, 6, 6, 7};
+    const bool lo = k <= 5;
+    const int r = lo ? k : nx + 1 - k;
+    T a = T(0);
+    for (int j = 0; j < w[r - 1]; j++) a += T(D_SBP63_DC_Q[r - 1][j]) * (lo ? f(j + 1) : f(nx - 1 - j));
+    return lo ? a : -a;
+}
+template <class T, class F>
+__device__ __forceinline__ T ii2c63(int k, int n, const F &f)
+{
+    const double *C = D_SBP63_II_C;
+    if (k >= 7 && k <= n - 6)
+        return T(C[0]) * (f(k + 1) + f(k)) + T(C[1]) * (f(k + 2) + f(k - 1)) + T(C[2]) * (f(k + 3) + f(k - 2));
+    const int w[6] = {5, 5, 6, 7, 8, 9};
+    const bool lo = k <= 6;
+    const int r = lo ? k : n + 1 - k;
+    T a = T(0);
+    for (int j = 0; j < w[r - 1]; j++) a += T(D_SBP63_II_Q[r - 1][j]) * (lo ? f(j + 1) : f(n + 1 - j));
+    return a;
+}
+template <class T, class F>
+__device__ __forceinline__ T ic2i63(int k, int nx, const F &f)
+{
+    const double *C = D_SBP63_IC_C;
+    if (k >= 6 && k <= nx - 5)
+        return T(C[0]) * (f(k) + f(k - 1)) + T(C[1]) * (f(k + 1) + f(k - 2)) + T(C[2]) * (f(k + 2) + f(k - 3));
+    const int w[5] = {6, 6, 6, 6, 7};
+    const bool lo = k <= 5;
+    const int r = lo ? k : nx + 1 - k;
+    T a = T(0);
+    for (int j = 0; j < w[r - 1]; j++) a += T(D_SBP63_IC_Q[r - 1][j]) * (lo ? f(j + 1) : f(nx - 1 - j));
+    return a;
+}
+
+// The order-dependent parts of the Ch operators, by SBP order (42, 21 or 63):
 //   C2I_LO/HI: nodes k in [C2I_LO, nx - C2I_HI] use the interior c2i rows;
 //   I2C_LO/HI: centres k in [I2C_LO, n - I2C_HI] use the interior i2c rows;
 //   GRAD_LO/HI: centres with the interior i2c difference and no gradient SAT;
 //   U_LO/HI: u-point columns [U_LO, N - U_HI] clear of both (the grad_x + I_i2c,x pass);
 //   V_LO/HI: rows [V_LO, N - V_HI] clear of the c2i and i2c closures, the gradient SAT
 //            and the panel-boundary rows (the final pass);
-//   SAT1..3: gradient SAT weights 0.5 R1k / h_kk of rows 1..3 (and mirrored);
-//   IC1..3, DC1..3: first c2i interpolation / difference rows (a panel edge node);
-//   SATC, R1..3: divergence SAT 0.5 / h11 and the boundary projection.
+//   RUN_OK: the interior rows read four consecutive inputs (the stencil runs);
+//   NSAT, satw(r): gradient SAT weights 0.5 R1r / h_rr of rows r = 1..NSAT (mirrored);
+//   NDEP: inputs of the first c2i rows; the edge strips hold NDEP normal lines;
+//   ic1(d), dc1(d): first c2i interpolation / difference row, input d = 1..NDEP;
+//   NR, r1(d), SATC: divergence SAT 0.5 / h11 * sum_d R1d (f(d) - f(1 - d)), d <= NR.
 template <int ORD>
 struct SbpOrder;
 
@@ -153,10 +213,13 @@ template <>
 struct SbpOrder<42> {
     static constexpr int C2I_LO = 5, C2I_HI = 4, I2C_LO = 4, I2C_HI = 3, GRAD_LO = 4, GRAD_HI = 3;
     static constexpr int U_LO = 4, U_HI = 3, V_LO = 5, V_HI = 3;
-    static constexpr double SAT1 = sbp::SATI1, SAT2 = sbp::SATI2, SAT3 = sbp::SATI3;
-    static constexpr double IC1 = sbp::IC11, IC2 = sbp::IC12, IC3 = sbp::IC13;
-    static constexpr double DC1 = sbp::DC11, DC2 = sbp::DC12, DC3 = sbp::DC13;
-    static constexpr double SATC = sbp::SATC, R1 = sbp::R11, R2 = sbp::R12, R3 = sbp::R13;
+    static constexpr bool RUN_OK = true;
+    static constexpr int NSAT = 3, NDEP = 3, NR = 3;
+    static constexpr double SATC = sbp::SATC;
+    static __device__ __forceinline__ double satw(int r) { return r == 1 ? sbp::SATI1 : (r == 2 ? sbp::SATI2 : sbp::SATI3); }
+    static __device__ __forceinline__ double ic1(int d) { return d == 1 ? sbp::IC11 : (d == 2 ? sbp::IC12 : sbp::IC13); }
+    static __device__ __forceinline__ double dc1(int d) { return d == 1 ? sbp::DC11 : (d == 2 ? sbp::DC12 : sbp::DC13); }
+    static __device__ __forceinline__ double r1(int d) { return d == 1 ? sbp::R11 : (d == 2 ? sbp::R12 : sbp::R13); }
     template <class T, class F> static __device__ __forceinline__ T di2c(int k, int n, const F &f) { return chswe::di2c<T>(k, n, f); }
     template <class T, class F> static __device__ __forceinline__ T dc2i(int k, int nx, const F &f) { return chswe::dc2i<T>(k, nx, f); }
     template <class T, class F> static __device__ __forceinline__ T ii2c(int k, int n, const F &f) { return chswe::ii2c<T>(k, n, f); }
@@ -171,23 +234,74 @@ struct SbpOrder<42> {
     {
         return (T(27) * (v2 - v1) - (v3 - v0)) * T(1.0 / 24.0);
     }
+    template <class T, class F> static __device__ __forceinline__ T ic2i_in(int k, const F &f) { return interp4<T>(f(k - 2), f(k - 1), f(k), f(k + 1)); }
+    template <class T, class F> static __device__ __forceinline__ T dc2i_in(int k, const F &f) { return diff4<T>(f(k - 2), f(k - 1), f(k), f(k + 1)); }
+    template <class T, class F> static __device__ __forceinline__ T ii2c_in(int k, const F &f) { return interp4<T>(f(k - 1), f(k), f(k + 1), f(k + 2)); }
+    template <class T, class F> static __device__ __forceinline__ T di2c_in(int k, const F &f) { return diff4<T>(f(k - 1), f(k), f(k + 1), f(k + 2)); }
 };
 
 template <>
 struct SbpOrder<21> {
     static constexpr int C2I_LO = 2, C2I_HI = 1, I2C_LO = 1, I2C_HI = 0, GRAD_LO = 3, GRAD_HI = 2;
     static constexpr int U_LO = 3, U_HI = 2, V_LO = 3, V_HI = 2;
+    static constexpr bool RUN_OK = true;
     // h11 = h22 = 1 (i2c), h11 = 1/2 (c2i), R11 = 3/2, R12 = -1/2
-    static constexpr double SAT1 = 0.5 * 1.5, SAT2 = 0.5 * -0.5, SAT3 = 0.0;
-    static constexpr double IC1 = 1.0, IC2 = 0.0, IC3 = 0.0;
-    static constexpr double DC1 = -1.0, DC2 = 1.0, DC3 = 0.0;
-    static constexpr double SATC = 0.5 / 0.5, R1 = 1.5, R2 = -0.5, R3 = 0.0;
+    static constexpr int NSAT = 2, NDEP = 3, NR = 2;
+    static constexpr double SATC = 0.5 / 0.5;
+    static __device__ __forceinline__ double satw(int r) { return r == 1 ? 0.5 * 1.5 : 0.5 * -0.5; }
+    static __device__ __forceinline__ double ic1(int d) { return d == 1 ? 1.0 : 0.0; }
+    static __device__ __forceinline__ double dc1(int d) { return d == 1 ? -1.0 : (d == 2 ? 1.0 : 0.0); }
+    static __device__ __forceinline__ double r1(int d) { return d == 1 ? 1.5 : -0.5; }
     template <class T, class F> static __device__ __forceinline__ T di2c(int k, int n, const F &f) { return di2c21<T>(k, n, f); }
     template <class T, class F> static __device__ __forceinline__ T dc2i(int k, int nx, const F &f) { return dc2i21<T>(k, nx, f); }
     template <class T, class F> static __device__ __forceinline__ T ii2c(int k, int n, const F &f) { return ii2c21<T>(k, n, f); }
     template <class T, class F> static __device__ __forceinline__ T ic2i(int k, int nx, const F &f) { return ic2i21<T>(k, nx, f); }
     template <class T> static __device__ __forceinline__ T interp4(T, T v1, T v2, T) { return T(0.5) * (v2 + v1); }
     template <class T> static __device__ __forceinline__ T diff4(T, T v1, T v2, T) { return v2 - v1; }
+    template <class T, class F> static __device__ __forceinline__ T ic2i_in(int k, const F &f) { return T(0.5) * (f(k) + f(k - 1)); }
+    template <class T, class F> static __device__ __forceinline__ T dc2i_in(int k, const F &f) { return f(k) - f(k - 1); }
+    template <class T, class F> static __device__ __forceinline__ T ii2c_in(int k, const F &f) { return T(0.5) * (f(k + 1) + f(k)); }
+    template <class T, class F> static __device__ __forceinline__ T di2c_in(int k, const F &f) { return f(k + 1) - f(k); }
+};
+
+template <>
+struct SbpOrder<63> {
+    static constexpr int C2I_LO = 6, C2I_HI = 5, I2C_LO = 7, I2C_HI = 6, GRAD_LO = 7, GRAD_HI = 6;
+    static constexpr int U_LO = 7, U_HI = 6, V_LO = 7, V_HI = 6;
+    static constexpr bool RUN_OK = false;   // six-point interior rows: evaluated per output
+    static constexpr int NSAT = 4, NDEP = 6, NR = 4;
+    static constexpr double SATC = 0.5 / (95.0 / 288.0);   // 0.5 / h11 of sbp_diff_c2i_63_mod.f90:12
+    static __device__ __forceinline__ double satw(int r) { return 0.5 * D_SBP63_R[r - 1] / D_SBP63_H_C[r - 1]; }
+    static __device__ __forceinline__ double ic1(int d) { return D_SBP63_IC_Q[0][d - 1]; }
+    static __device__ __forceinline__ double dc1(int d) { return D_SBP63_DC_Q[0][d - 1]; }
+    static __device__ __forceinline__ double r1(int d) { return D_SBP63_R[d - 1]; }
+    template <class T, class F> static __device__ __forceinline__ T di2c(int k, int n, const F &f) { return di2c63<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T dc2i(int k, int nx, const F &f) { return dc2i63<T>(k, nx, f); }
+    template <class T, class F> static __device__ __forceinline__ T ii2c(int k, int n, const F &f) { return ii2c63<T>(k, n, f); }
+    template <class T, class F> static __device__ __forceinline__ T ic2i(int k, int nx, const F &f) { return ic2i63<T>(k, nx, f); }
+    // the stencil runs are not built for 6-3 (RUN_OK): placeholders
+    template <class T> static __device__ __forceinline__ T interp4(T, T, T, T) { return T(0); }
+    template <class T> static __device__ __forceinline__ T diff4(T, T, T, T) { return T(0); }
+    template <class T, class F> static __device__ __forceinline__ T ic2i_in(int k, const F &f)
+    {
+        const double *C = D_SBP63_IC_C;
+        return T(C[0]) * (f(k) + f(k - 1)) + T(C[1]) * (f(k + 1) + f(k - 2)) + T(C[2]) * (f(k + 2) + f(k - 3));
+    }
+    template <class T, class F> static __device__ __forceinline__ T dc2i_in(int k, const F &f)
+    {
+        const double *C = D_SBP63_DC_C;
+        return T(C[0]) * (f(k) - f(k - 1)) + T(C[1]) * (f(k + 1) - f(k - 2)) + T(C[2]) * (f(k + 2) - f(k - 3));
+    }
+    template <class T, class F> static __device__ __forceinline__ T ii2c_in(int k, const F &f)
+    {
+        const double *C = D_SBP63_II_C;
+        return T(C[0]) * (f(k + 1) + f(k)) + T(C[1]) * (f(k + 2) + f(k - 1)) + T(C[2]) * (f(k + 3) + f(k - 2));
+    }
+    template <class T, class F> static __device__ __forceinline__ T di2c_in(int k, const F &f)
+    {
+        const double *C = D_SBP63_DI_C;
+        return T(C[0]) * (f(k + 1) - f(k)) + T(C[1]) * (f(k + 2) - f(k - 1)) + T(C[2]) * (f(k + 3) - f(k - 2));
+    }
 };
 
 }  // namespace chswe

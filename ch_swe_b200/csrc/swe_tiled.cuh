@@ -84,26 +84,22 @@ struct SWin {
 template <class T, int ORD = 42> __device__ __forceinline__ T ic2i_u(int k, int nx, const Line<T> &f)
 {
     using S = SbpOrder<ORD>;
-    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template interp4<T>(f(k - 2), f(k - 1), f(k), f(k + 1))
-                                                   : S::template ic2i<T>(k, nx, f);
+    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template ic2i_in<T>(k, f) : S::template ic2i<T>(k, nx, f);
 }
 template <class T, int ORD = 42> __device__ __forceinline__ T ii2c_u(int k, int n, const Line<T> &f)
 {
     using S = SbpOrder<ORD>;
-    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template interp4<T>(f(k - 1), f(k), f(k + 1), f(k + 2))
-                                                  : S::template ii2c<T>(k, n, f);
+    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template ii2c_in<T>(k, f) : S::template ii2c<T>(k, n, f);
 }
 template <class T, int ORD = 42> __device__ __forceinline__ T dc2i_u(int k, int nx, const Line<T> &f)
 {
     using S = SbpOrder<ORD>;
-    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template diff4<T>(f(k - 2), f(k - 1), f(k), f(k + 1))
-                                                   : S::template dc2i<T>(k, nx, f);
+    return (k >= S::C2I_LO && k <= nx - S::C2I_HI) ? S::template dc2i_in<T>(k, f) : S::template dc2i<T>(k, nx, f);
 }
 template <class T, int ORD = 42> __device__ __forceinline__ T di2c_u(int k, int n, const Line<T> &f)
 {
     using S = SbpOrder<ORD>;
-    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template diff4<T>(f(k - 1), f(k), f(k + 1), f(k + 2))
-                                                  : S::template di2c<T>(k, n, f);
+    return (k >= S::I2C_LO && k <= n - S::I2C_HI) ? S::template di2c_in<T>(k, f) : S::template di2c<T>(k, n, f);
 }
 
 // Stencil runs.  A pass gives every thread whole runs of RB consecutive outputs
@@ -169,7 +165,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
     if (member_frozen(dtm, mem)) return;
     const T *y = Y + mem * d.ms + t * d.ps;
     T *w = W + mem * d.ms + t * d.ps;
-    T *es = ES + strip_member(N, mem) + (int64_t)t * 4 * STRIP_LINES * n - 1;   // + (s*4 + line)*n + index
+    constexpr int NDEP = SB::NDEP, NL = NDEP + 1;   // normal depths and lines per side of the strips
+    T *es = ES + strip_member(N, mem, NL) + (int64_t)t * 4 * NL * n - 1;   // + (s*NL + line)*n + index
     const SWin<T, PW> sv{sm + L::V, i0 - 2, j0 - 3}, su{sm + L::U, i0 - 3, j0 - 2}, svq{sm + L::VQ, i0 - 2, j0};
     const SWin<T, PT> suq{sm + L::UQ, i0, j0 - 2}, sux{sm + L::UX, i0, j0};
 
@@ -252,7 +249,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int k = sv.x0 + x, l0 = j0 + r * RBW, cnt = min(RBW, j1 - l0);
         const Line<T> col = sv.col(k);
         T *o = &svq.at(k, l0);
-        if (cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
+        if (SB::RUN_OK && cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(col, l0, v);
 #pragma unroll
@@ -274,7 +271,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int l = suq.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
         const Line<T> row = su.row(l);
         T *o = &suq.at(k0, l);
-        if (cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
+        if (SB::RUN_OK && cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(row, k0, v);
 #pragma unroll
@@ -297,7 +294,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
         const Line<T> row = svq.row(j);
         T *o = &sux.at(k0, j);
-        if (cnt == RBT && k0 >= SB::I2C_LO && k0 + RBT - 1 <= N - SB::I2C_HI) {
+        if (SB::RUN_OK && cnt == RBT && k0 >= SB::I2C_LO && k0 + RBT - 1 <= N - SB::I2C_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(row, k0, v);
 #pragma unroll
@@ -328,7 +325,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
         const int i = i0 + x, jr = j0 + r * RBT, cnt = min(RBT, j1 - jr);
         const Line<T> col = suq.col(i);
         T vi[RBT];
-        if (cnt == RBT && jr >= SB::I2C_LO && jr + RBT - 1 <= N - SB::I2C_HI) {
+        if (SB::RUN_OK && cnt == RBT && jr >= SB::I2C_LO && jr + RBT - 1 <= N - SB::I2C_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(col, jr, v);
 #pragma unroll
@@ -346,18 +343,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
             if (i <= N) {
                 const T ut = q11[it][mm] * su.at(i, j) + sux.at(i, j) * ijy[it][mm];
                 w[d.fs + o] = ut;
-                if (i <= 3) es[(SIDE_L * 4 + i - 1) * n + j] = ut;
-                if (i >= N - 2) es[(SIDE_R * 4 + N - i) * n + j] = ut;
-                if (j == 1) es[(SIDE_B * 4 + 3) * n + i] = ut;
-                if (j == n) es[(SIDE_T * 4 + 3) * n + i] = ut;
+                if (i <= NDEP) es[(SIDE_L * NL + i - 1) * n + j] = ut;
+                if (i >= N + 1 - NDEP) es[(SIDE_R * NL + N - i) * n + j] = ut;
+                if (j == 1) es[(SIDE_B * NL + NL - 1) * n + i] = ut;
+                if (j == n) es[(SIDE_T * NL + NL - 1) * n + i] = ut;
             }
             if (j <= N) {
                 const T vt = q22[it][mm] * sv.at(i, j) + vi[mm] * ijx[it][mm];
                 w[2 * d.fs + o] = vt;
-                if (j <= 3) es[(SIDE_B * 4 + j - 1) * n + i] = vt;
-                if (j >= N - 2) es[(SIDE_T * 4 + N - j) * n + i] = vt;
-                if (i == 1) es[(SIDE_L * 4 + 3) * n + j] = vt;
-                if (i == n) es[(SIDE_R * 4 + 3) * n + j] = vt;
+                if (j <= NDEP) es[(SIDE_B * NL + j - 1) * n + i] = vt;
+                if (j >= N + 1 - NDEP) es[(SIDE_T * NL + N - j) * n + i] = vt;
+                if (i == 1) es[(SIDE_L * NL + NL - 1) * n + j] = vt;
+                if (i == n) es[(SIDE_R * NL + NL - 1) * n + j] = vt;
             }
         }
     }
@@ -413,7 +410,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     const int w5 = tw + 5, h5 = th + 5;
     const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
     const T *fJ2 = m.fJ2 + t * d.ps;
-    const bool sat_l = i0 <= 3, sat_r = i1 - 1 >= N - 2, sat_b = j0 <= 3, sat_t = j1 - 1 >= N - 2;
+    const bool sat_l = i0 <= SB::NSAT, sat_r = i1 - 1 >= N + 1 - SB::NSAT, sat_b = j0 <= SB::NSAT,
+               sat_t = j1 - 1 >= N + 1 - SB::NSAT;
     // runs along the tile width / height: window passes (RBW), tile passes (RBT)
     const int nww = (tw + RBW - 1) / RBW, nhw = (th + RBW - 1) / RBW, nwt = (tw + RBT - 1) / RBT,
               nht = (th + RBT - 1) / RBT;
@@ -572,7 +570,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
 #pragma unroll
             for (int mm = 0; mm < RBW; mm++)
                 if (mm < cnt) o[mm * PW] = f1[it][mm];
-        } else if (cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
+        } else if (SB::RUN_OK && cnt == RBW && l0 >= SB::C2I_LO && l0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(col, l0, v);
 #pragma unroll
@@ -595,7 +593,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int l = svp.y0 + x, k0 = i0 + r * RBW, cnt = min(RBW, i1 - k0);
         const Line<T> row = sut.row(l);
         T *o = &svp.at(k0, l);
-        if (cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
+        if (SB::RUN_OK && cnt == RBW && k0 >= SB::C2I_LO && k0 + RBW - 1 <= n - SB::C2I_HI) {
             T v[RBW + 3];
             run_load<T, RBW, -2>(row, k0, v);
 #pragma unroll
@@ -616,7 +614,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, i1 - k0);
         const Line<T> row = sju.row(j);
         T *o = &sdx.at(k0, j);
-        if (cnt == RBT && k0 >= SB::C2I_LO && k0 + RBT - 1 <= n - SB::C2I_HI) {
+        if (SB::RUN_OK && cnt == RBT && k0 >= SB::C2I_LO && k0 + RBT - 1 <= n - SB::C2I_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -2>(row, k0, v);
 #pragma unroll
@@ -642,7 +640,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         const int j = j0 + x, k0 = i0 + r * RBT, cnt = min(RBT, iu1 - k0);
         const Line<T> hrow = sh.row(j), prow = sup.row(j);
         T *og = &skx.at(k0, j), *oc = &scx.at(k0, j);
-        if (cnt == RBT && k0 >= SB::U_LO && k0 + RBT - 1 <= N - SB::U_HI) {
+        if (SB::RUN_OK && cnt == RBT && k0 >= SB::U_LO && k0 + RBT - 1 <= N - SB::U_HI) {
             T v[RBT + 3];
             run_load<T, RBT, -1>(hrow, k0, v);
 #pragma unroll
@@ -656,14 +654,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                 if (mm >= cnt) continue;
                 const int i = k0 + mm;
                 T gx = di2c_u<T, ORD>(i, N, hrow);
-                if (i <= 3) {
-                    const T sat = i == 1 ? T(SB::SAT1) : (i == 2 ? T(SB::SAT2) : T(SB::SAT3));
-                    gx += sat * (hrow(1) - hl[x]);
-                }
-                if (i >= N - 2) {
-                    const T sat = i == N ? T(SB::SAT1) : (i == N - 1 ? T(SB::SAT2) : T(SB::SAT3));
-                    gx += sat * (hr[x] - hrow(n));
-                }
+                if (i <= SB::NSAT) gx += T(SB::satw(i)) * (hrow(1) - hl[x]);
+                if (i >= N + 1 - SB::NSAT) gx += T(SB::satw(N + 1 - i)) * (hr[x] - hrow(n));
                 og[mm] = -m.grav * (gx * m.inv_hxa);
                 oc[mm] = ii2c_u<T, ORD>(i, N, prow);
             }
@@ -701,7 +693,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         for (int mm = 0; mm < RBT; mm++) kh[it][mm] = ku[it][mm] = kv[it][mm] = T(0);
         if (cnt <= 0) continue;
         const Line<T> dcol = sjv.col(i), hcol = sh.col(i), pcol = svp.col(i);
-        if (cnt == RBT && jr >= SB::V_LO && jr + RBT - 1 <= N - SB::V_HI) {
+        if (SB::RUN_OK && cnt == RBT && jr >= SB::V_LO && jr + RBT - 1 <= N - SB::V_HI) {
             // rows clear of the closures, the SAT terms and the panel-boundary rows
             const bool bcol = (i == 1 || i == n), hasu = i <= N;
             T v[RBT + 3];
@@ -766,14 +758,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             }
             if (j <= N) {
                 T gy = di2c_u<T, ORD>(j, N, hcol);
-                if (j <= 3) {
-                    const T sat = j == 1 ? T(SB::SAT1) : (j == 2 ? T(SB::SAT2) : T(SB::SAT3));
-                    gy += sat * (hcol(1) - hb[x]);
-                }
-                if (j >= N - 2) {
-                    const T sat = j == N ? T(SB::SAT1) : (j == N - 1 ? T(SB::SAT2) : T(SB::SAT3));
-                    gy += sat * (ht[x] - hcol(n));
-                }
+                if (j <= SB::NSAT) gy += T(SB::satw(j)) * (hcol(1) - hb[x]);
+                if (j >= N + 1 - SB::NSAT) gy += T(SB::satw(N + 1 - j)) * (ht[x] - hcol(n));
                 gy = gy * m.inv_hxa;
                 if constexpr (ADV) {
                     T av = __ldg(Av + box_off32(P, i, j));

@@ -46,6 +46,15 @@ LINEAR_CH21_NAMES = {
     "co2contra_op_name": "co2contra_ch_sbp21",
     "quadrature_name": "SBP_C21_quadrature",
 }
+# ... and with the SBP 6-3 Ch operators (the _63 names)
+LINEAR_CH63_NAMES = {
+    "div_op_name": "div_ch_sbp_sat_63_proj",
+    "grad_op_name": "grad_ch_sbp_sat_63",
+    "coriolis_op_name": "coriolis_Ch_sbp63",
+    "co2contra_op_name": "co2contra_ch_sbp63",
+    "quadrature_name": "SBP_C63_quadrature",
+}
+LINEAR_NAMES_BY_ORDER = {42: LINEAR_CH42_NAMES, 21: LINEAR_CH21_NAMES, 63: LINEAR_CH63_NAMES}
 # advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4)
 ADVECTIVE_CH42_NAMES = dict(LINEAR_CH42_NAMES, vector_advection_op_name="vector_advection_Ch_up4_cov",
                             massflux_op_name="massflux_ch_up4")
@@ -74,7 +83,7 @@ class Domain:
     h_mean: float = 1000.0
     horizontal_staggering: str = "Ch"
     operator: str = "linear"          # the operator the context runs: 'linear' or 'advective'
-    sbp_order: int = 42               # SBP order of the Ch operators: 42, or 21 (linear operator)
+    sbp_order: int = 42               # SBP order of the Ch operators: 42, or 21 / 63 (linear operator)
     _ctx: int = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -84,8 +93,10 @@ class Domain:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if self.operator not in OPERATORS:
             raise ValueError(f"operator must be one of {sorted(OPERATORS)}")
-        if self.sbp_order not in (42, 21) or (self.sbp_order == 21 and self.operator != "linear"):
-            raise ValueError("sbp_order must be 42, or 21 with the linear operator")
+        if self.sbp_order not in (42, 21, 63) or (self.sbp_order != 42 and self.operator != "linear"):
+            raise ValueError("sbp_order must be 42, or 21 / 63 with the linear operator")
+        if self.sbp_order == 63 and self.N < 16:
+            raise ValueError("SBP 6-3 needs N >= 16")
         L = _lib.load()
         cfg = SweCfg()
         check(L.swe_cfg_default(ctypes.byref(cfg)))
@@ -309,7 +320,7 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     if kind == "linear_swm_operator":
         if "h_mean" not in config:
             raise ValueError("linear_swm_operator requires h_mean")
-        names, want_op = (LINEAR_CH21_NAMES if domain.sbp_order == 21 else LINEAR_CH42_NAMES), "linear"
+        names, want_op = LINEAR_NAMES_BY_ORDER[domain.sbp_order], "linear"
     elif kind == "advective_swm_operator":
         if config.get("v_components_type", "covariant") != "covariant":
             raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
@@ -321,10 +332,9 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     for key, want in names.items():
         got = config.get(key, want)
         if got != want:
-            other = LINEAR_CH21_NAMES if domain.sbp_order != 21 else LINEAR_CH42_NAMES
-            if want_op == "linear" and got == other.get(key):
-                raise ValueError(f"{key} = {got} needs a domain created with sbp_order="
-                                 f"{21 if domain.sbp_order != 21 else 42}")
+            for order, other in LINEAR_NAMES_BY_ORDER.items():
+                if want_op == "linear" and got == other.get(key):
+                    raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")
             raise ValueError(f"unsupported {key}: {got} (this build implements {want})")
     if domain.operator != want_op:
         raise ValueError(f"{kind} needs a domain created with operator='{want_op}' (got '{domain.operator}')")

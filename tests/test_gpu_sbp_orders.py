@@ -1,5 +1,6 @@
-"""GPU parity of the SBP 2-1 Ch linear operator (the _sbp_sat_21 / _sbp21 names of
-the reference's factories) against the CPU FP64 oracle with the same order.
+"""GPU parity of the SBP 2-1 and 6-3 Ch linear operators (the _sbp_sat_21 / _21 and
+_63 names of the reference's factories) against the CPU FP64 oracle with the same
+order.
 
 Tolerances as for SBP 4-2: FP64 within 1e-12 relative (max-norm of the
 difference over the max-norm of the oracle field), FP32 within 1e-5.
@@ -32,9 +33,9 @@ def random_state(N, seed):
     return tuple(rng.standard_normal(s) for s in state_shapes(N))
 
 
-def gpu_apply(N, state, precision="fp64", tile=None):
+def gpu_apply(N, state, order, precision="fp64", tile=None):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
-    dom = create_domain(N, precision=precision, h_mean=1000.0, sbp_order=21)
+    dom = create_domain(N, precision=precision, h_mean=1000.0, sbp_order=order)
     if tile:
         dom.tile = tile
     op = create_swm_operator(dom.grav, LIN, dom)
@@ -46,42 +47,51 @@ def gpu_apply(N, state, precision="fp64", tile=None):
     return out
 
 
+ORDERS = [21, 63]
+
+
+@pytest.mark.parametrize("order", ORDERS)
 @pytest.mark.parametrize("N", [8, 12, 16, 17, 24, 33, 48])
-def test_apply_parity_fp64_random(N):
+def test_apply_parity_fp64_random(order, N):
     from oracle.oracle import Oracle
+    if order == 63 and N < 16:
+        pytest.skip("SBP 6-3 needs N >= 16")
     st = random_state(N, 700 + N)
-    ref = Oracle(N, h_mean=1000.0, sbp_order=21).apply(*st)
-    for g, r, name in zip(gpu_apply(N, st), ref, "huv"):
-        assert rel(g, r) < FP64_RTOL, (N, name, rel(g, r))
+    ref = Oracle(N, h_mean=1000.0, sbp_order=order).apply(*st)
+    for g, r, name in zip(gpu_apply(N, st, order), ref, "huv"):
+        assert rel(g, r) < FP64_RTOL, (order, N, name, rel(g, r))
 
 
+@pytest.mark.parametrize("order", ORDERS)
 @pytest.mark.parametrize("tile,N", [(17, 16), (17, 33), (25, 24), (25, 49), (33, 32), (33, 65)])
-def test_apply_parity_fp64_every_tile(tile, N):
+def test_apply_parity_fp64_every_tile(order, tile, N):
     from oracle.oracle import Oracle
     st = random_state(N, 800 + N)
-    ref = Oracle(N, h_mean=1000.0, sbp_order=21).apply(*st)
-    for g, r, name in zip(gpu_apply(N, st, tile=tile), ref, "huv"):
-        assert rel(g, r) < FP64_RTOL, (tile, N, name, rel(g, r))
+    ref = Oracle(N, h_mean=1000.0, sbp_order=order).apply(*st)
+    for g, r, name in zip(gpu_apply(N, st, order, tile=tile), ref, "huv"):
+        assert rel(g, r) < FP64_RTOL, (order, tile, N, name, rel(g, r))
 
 
-def test_apply_fp32_within_bound():
+@pytest.mark.parametrize("order", ORDERS)
+def test_apply_fp32_within_bound(order):
     from oracle.oracle import Oracle
     N = 26
-    o = Oracle(N, h_mean=1000.0, sbp_order=21)
+    o = Oracle(N, h_mean=1000.0, sbp_order=order)
     st = o.gaussian(lam0=0.9, phi0=0.4, d0=0.25)
     ref = o.apply(*st)
-    for g, r, name in zip(gpu_apply(N, st, precision="fp32"), ref, "huv"):
-        assert rel(g, r) < 1e-5, (name, rel(g, r))
+    for g, r, name in zip(gpu_apply(N, st, order, precision="fp32"), ref, "huv"):
+        assert rel(g, r) < 1e-5, (order, name, rel(g, r))
 
 
-def test_rk4_fp64_matches_oracle_and_conserves_mass():
+@pytest.mark.parametrize("order", ORDERS)
+def test_rk4_fp64_matches_oracle_and_conserves_mass(order):
     from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
     from oracle.oracle import Oracle
     N, dt, nst = 24, 900.0, 8
-    o = Oracle(N, h_mean=1000.0, sbp_order=21)
+    o = Oracle(N, h_mean=1000.0, sbp_order=order)
     h, u, v = o.gaussian(lam0=0.7, phi0=0.6, d0=0.2)
     ref = o.rk4(h, u, v, dt, nst)
-    dom = create_domain(N, h_mean=1000.0, sbp_order=21)
+    dom = create_domain(N, h_mean=1000.0, sbp_order=order)
     op = create_swm_operator(dom.grav, LIN, dom)
     x = create_stvec_swm(dom).upload(h, u, v)
     m0, e0 = op.integrals(x)
@@ -95,8 +105,9 @@ def test_rk4_fp64_matches_oracle_and_conserves_mass():
     dom.destroy()
 
 
-def test_orders_differ_and_configs_are_checked():
-    """The two orders give different tendencies on the same state; the 2-1 context
+@pytest.mark.parametrize("order", ORDERS)
+def test_orders_differ_and_configs_are_checked(order):
+    """The orders give different tendencies on the same state; a 2-1 or 6-3 context
     accepts only its built kernel configurations and the linear operator."""
     from ch_swe_b200 import create_domain, create_swm_operator
     from ch_swe_b200._lib import SweError
@@ -104,8 +115,8 @@ def test_orders_differ_and_configs_are_checked():
     N = 16
     st = random_state(N, 5)
     ref42 = Oracle(N, h_mean=1000.0).apply(*st)
-    assert rel(gpu_apply(N, st)[0], ref42[0]) > 1e-3
-    dom = create_domain(N, h_mean=1000.0, sbp_order=21)
+    assert rel(gpu_apply(N, st, order)[0], ref42[0]) > 1e-3
+    dom = create_domain(N, h_mean=1000.0, sbp_order=order)
     with pytest.raises(SweError):
         dom.kernel_config = (25, 4, 1)
     dom.kernel_config = (25, 2, 0)
@@ -116,4 +127,4 @@ def test_orders_differ_and_configs_are_checked():
         create_swm_operator(dom.grav, dict(LIN, div_op_name="div_ch_sbp_sat_42_proj"), dom)
     dom.destroy()
     with pytest.raises(ValueError):
-        create_domain(N, operator="advective", sbp_order=21)
+        create_domain(N, operator="advective", sbp_order=order)
