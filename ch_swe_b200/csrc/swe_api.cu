@@ -1415,6 +1415,83 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     return SWE_OK;
 }
 
+// Extrema for the diagnostics (swm_output_diag_mod.f90:110-154, :160-171).  Per
+// block: term 0 max h, 1 min h (xy mesh), 2 max |(cx ut) u| (y mesh),
+// 3 max |(cy vt) v| (x mesh); w holds (ut, vt).  FP64 arithmetic.
+template <class T>
+__global__ void k_extrema(const T *__restrict__ y, const T *__restrict__ w, Dims d, double cx, double cy,
+                          double *partial)
+{
+    const int term = blockIdx.y;
+    const int n = d.N + 1, N = d.N;
+    const int64_t npts = (int64_t)NPAN * n * n;
+    double acc = term == 1 ? INFINITY : (term == 0 ? -INFINITY : 0.0);
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npts; k += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(k / ((int64_t)n * n)), r = (int)(k % ((int64_t)n * n));
+        const int j = r / n + 1, i = r % n + 1;
+        const int64_t o = box_off(d.P, i, j) + t * d.ps;
+        if (term <= 1) {
+            const double h = (double)y[o];
+            acc = term == 0 ? fmax(acc, h) : fmin(acc, h);
+        } else if (term == 2) {
+            if (i > N) continue;
+            acc = fmax(acc, fabs(cx * (double)w[d.fs + o] * (double)y[d.fs + o]));
+        } else {
+            if (j > N) continue;
+            acc = fmax(acc, fabs(cy * (double)w[2 * d.fs + o] * (double)y[2 * d.fs + o]));
+        }
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            sh[threadIdx.x] = term == 1 ? fmin(sh[threadIdx.x], sh[threadIdx.x + s]) : fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+extern "C" int swe_diag(swe_ctx *c, const swe_stvec *vec, int member, double dt, double *out)
+{
+    if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    const int nb = 256;
+    dim3 g(nb, 4), b(256);
+    Dims d1 = c->dims;
+    const size_t mo = (size_t)member * c->dims.ms;
+    const double pi = 3.141592653589793238462643383279502884;
+    const double dx = c->cfg.radius * (0.5 * pi / c->cfg.N);   // dx = dy on the xy mesh
+    const double cxy = 1.0 / (dx * dx);
+    if (c->elem == 8) {
+        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
+                                 (double *)c->es, d1, c->m64.v, c->stream);
+        k_extrema<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, d1, cxy, cxy, c->red);
+    } else {
+        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
+                                (float *)c->es, d1, c->m32.v, c->stream);
+        k_extrema<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, d1, cxy, cxy, c->red);
+    }
+    c->launches += 2;
+    CU(c, cudaGetLastError());
+    std::vector<double> part(nb * 4);
+    CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    double hmax = -INFINITY, hmin = INFINITY, umax = 0.0, vmax = 0.0;
+    for (int k = 0; k < nb; k++) {
+        hmax = std::max(hmax, part[k]);
+        hmin = std::min(hmin, part[nb + k]);
+        umax = std::max(umax, part[2 * nb + k]);
+        vmax = std::max(vmax, part[3 * nb + k]);
+    }
+    out[0] = hmin;
+    out[1] = hmax;
+    // the reference scales with its constant Earth_grav; this uses the context's g
+    out[2] = std::sqrt((c->cfg.grav / (dx * dx)) * hmax) * dt;
+    out[3] = std::sqrt(umax) * dt;
+    out[4] = std::sqrt(vmax) * dt;
+    return SWE_OK;
+}
+
 extern "C" int swe_edge_links(int *out)
 {
     if (!out) return SWE_EINVAL;

@@ -1,0 +1,58 @@
+"""Diagnostics and output of a shallow-water state: the swm_output_diag_t checks
+(CFL numbers, h extrema, mass) and the paneled single-precision writer
+(src/models/shallow_water/output_and_diag/swm_output_diag_mod.f90,
+src/outputer/master_paneled_outputer_mod.f90)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+class SwmOutputDiag:
+    """swm_output_diag_t for a device state: print_CFL_diag and the h extrema and
+    mass of print_integrals_diag (swm_output_diag_mod.f90:110-171)."""
+
+    def __init__(self, domain):
+        self.domain = domain
+
+    def diagnostics(self, state, dt: float, member: int = 0) -> dict:
+        """h_min, h_max, the gravity-wave CFL and the advective CFL numbers (x, y)."""
+        out = (ctypes.c_double * 5)()
+        check(_lib.load().swe_diag(self.domain.ctx, state.handle, int(member), float(dt), out), self.domain.ctx,
+              "swe_diag")
+        return {"h_min": out[0], "h_max": out[1], "cfl_gravity": out[2], "cfl_adv_x": out[3], "cfl_adv_y": out[4]}
+
+    def print_cfl_diag(self, state, dt: float, member: int = 0) -> str:
+        d = self.diagnostics(state, dt, member)
+        line = (f"Gravity waves CFL-max = {d['cfl_gravity']:15.7f}, Advective CFL-max (x,y) = "
+                f"{d['cfl_adv_x']:15.7f}{d['cfl_adv_y']:15.7f}")
+        print(line)
+        return line
+
+
+def write_paneled(path: str, field: np.ndarray, rec: int = 1) -> None:
+    """master_paneled_outputer_t%write for one level: record rec (1-based) of a
+    direct-access file holds the six panels of the field as real*4, i fastest, then j,
+    then panel (master_paneled_outputer_mod.f90:32-77).  field: (6, ny, nx)."""
+    a = np.ascontiguousarray(field, dtype="<f4")
+    if a.ndim != 3 or a.shape[0] != 6:
+        raise ValueError("expected a (6, ny, nx) panel field")
+    reclen = a.nbytes
+    mode = "r+b" if os.path.exists(path) else "wb"
+    with open(path, mode) as f:
+        f.seek((int(rec) - 1) * reclen)
+        f.write(a.tobytes())
+
+
+def read_paneled(path: str, shape, rec: int = 1) -> np.ndarray:
+    """Record rec of a file written by write_paneled (or by the reference's writer)."""
+    shape = tuple(shape)
+    n = int(np.prod(shape))
+    with open(path, "rb") as f:
+        f.seek((int(rec) - 1) * n * 4)
+        return np.frombuffer(f.read(n * 4), dtype="<f4").reshape(shape).copy()

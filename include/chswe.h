@@ -126,6 +126,13 @@ int swe_rk4_steps_members(swe_ctx *ctx, swe_stvec *v0, const double *dt, int nst
 /* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
 int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
 
+/* Diagnostics of swm_output_diag_t for one member (print_CFL_diag and the extrema
+   of print_integrals_diag, swm_output_diag_mod.f90:110-171): out[0..4] = h_min,
+   h_max, the gravity-wave CFL sqrt(max (g / dx^2) h) dt and the advective CFL
+   numbers sqrt(max |ut u| / dx^2) dt and sqrt(max |vt v| / dy^2) dt, with (ut, vt)
+   the contravariant components and dx = dy = a (pi/2) / N.  Synchronous. */
+int swe_diag(swe_ctx *ctx, const swe_stvec *vec, int member, double dt, double *out);
+
 /* Number of kernel launches issued on the context's stream since creation. */
 long long swe_launch_count(const swe_ctx *ctx);
 

@@ -63,6 +63,7 @@ def lib():
         L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_set_operator.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_sbp_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_diag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, _dp]
         L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         _lib = L
     return _lib
@@ -111,6 +112,13 @@ class Oracle:
     def zeros(self):
         sh, su, sv = shapes(self.N)
         return np.zeros(sh), np.zeros(su), np.zeros(sv)
+
+    def diag(self, h, u, v, dt: float):
+        """(h_min, h_max, gravity-wave CFL, advective CFL x, y) of swm_output_diag_t."""
+        out = np.zeros(5)
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        lib().orc_diag(self._c, _p(a[0]), _p(a[1]), _p(a[2]), float(dt), _p(out))
+        return tuple(out)
 
     def gaussian(self, lam0=np.pi, phi0=0.0, d0=0.25, amp=1.0):
         h, u, v = self.zeros()

@@ -1669,6 +1669,46 @@ void orc_integrals(orc_ctx *c, const double *h, const double *u, const double *v
     if (energy) *energy = 0.5 * c->H * (eu + ev) + 0.5 * c->g * eh;
 }
 
+/* swm_output_diag_t diagnostics (swm_output_diag_mod.f90:110-154 print_CFL_diag,
+   :160-171 the extrema of print_integrals_diag): out = {h_min, h_max, CFL of the
+   gravity waves, advective CFL in x, in y}.  The CFL numbers are
+   sqrt(max (g / min(dx,dy)^2) h) dt and sqrt(maxabs (1/dx^2) ut u) dt (likewise y),
+   with (ut, vt) = co2contra(u, v) and dx = a hx on the xy mesh. */
+void orc_diag(orc_ctx *c, const double *h, const double *u, const double *v, double dt, double *out)
+{
+    load_state(c, h, u, v);
+    op_co2contra(c, &c->ut, &c->vt, &c->u, &c->v);
+    const int N = c->N;
+    const double dx = c->a * c->mxy.hx, dy = c->a * c->mxy.hy, dm = dx < dy ? dx : dy;
+    const double cg = c->g / (dm * dm), cx = 1.0 / (dx * dx), cy = 1.0 / (dy * dy);
+    double hmin = INFINITY, hmax = -INFINITY, gmax = -INFINITY, umax = 0.0, vmax = 0.0;
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N + 1; i++) {
+                const double hv = FA(&c->h, t, i, j);
+                hmin = hv < hmin ? hv : hmin;
+                hmax = hv > hmax ? hv : hmax;
+                const double gv = cg * hv;
+                gmax = gv > gmax ? gv : gmax;
+            }
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) {
+                const double p = fabs(cx * FA(&c->ut, t, i, j) * FA(&c->u, t, i, j));
+                umax = p > umax ? p : umax;
+            }
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) {
+                const double p = fabs(cy * FA(&c->vt, t, i, j) * FA(&c->v, t, i, j));
+                vmax = p > vmax ? p : vmax;
+            }
+    }
+    out[0] = hmin;
+    out[1] = hmax;
+    out[2] = sqrt(gmax) * dt;
+    out[3] = sqrt(umax) * dt;
+    out[4] = sqrt(vmax) * dt;
+}
+
 /* SBP-weighted inner product on mesh 0 = xy (h), 1 = y (u), 2 = x (v) */
 double orc_dot(orc_ctx *c, int mesh, const double *a, const double *b)
 {
