@@ -5,13 +5,21 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchswe.so")
-SOURCES = ["swe_api.cu"]
-DEPS = ["swe_api.cu", "swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh", "swe_advective.cuh"]
+OBJDIR = os.path.join(HERE, "_build")
+# the C ABI (edge sync, advective fluxes, quadrature, diagnostics) and one translation
+# unit per precision and maximal tile for the stage and contravariant kernels: small
+# device modules, compiled in parallel
+STAGE_SOURCES = [f"stage_{p}{tm}.cu" for p in ("f", "d") for tm in (17, 25, 33)]
+SOURCES = ["swe_api.cu", *STAGE_SOURCES]
+HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh",
+           "swe_launch.cuh", "swe_stage_tu.cuh"]
+DEPS = SOURCES + HEADERS
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,19 +38,30 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    # the device code is one large translation unit of templated kernels: let nvcc
-    # optimise its kernels in parallel on the host's cores
-    split = ["--split-compile", str(max(1, min(8, os.cpu_count() or 1)))]
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", *split, "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", LIB + ".tmp",
-           *[os.path.join(CSRC, s) for s in SOURCES]]
+def _compile(src: str, verbose: bool, force: bool = False) -> str:
+    obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+    deps = [os.path.join(CSRC, d) for d in [src, *HEADERS]] + [os.path.join(ROOT, "include", "chswe.h")]
+    if not force and os.path.exists(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in deps):
+        return obj
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-c",
+           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", obj, os.path.join(CSRC, src)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    # every unit is compiled whole: no --split-compile, whose partition of a unit's
+    # kernels (and with it the generated code) varies from one run to the next
+    with ThreadPoolExecutor(jobs) as pool:
+        objs = list(pool.map(lambda src: _compile(src, verbose, force), SOURCES))
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,5 @@
+// stage_d33.cu -- the FP64 stage and contravariant kernels for tiles of at most
+// 33 x 33 points (every blocks-per-SM, runs, SBP-order and operator variant).
+#include "swe_stage_tu.cuh"
+
+template struct chswe::StageTU<double, 33>;

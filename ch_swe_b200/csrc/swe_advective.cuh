@@ -23,7 +23,7 @@
 namespace chswe {
 
 // Cube edges (panel, side) with (panel*4 + side) below its neighbour's, filled by the host.
-__constant__ int c_cube_edge[12][2];
+static __constant__ int c_cube_edge[12][2];
 
 // Static tables of the advective operator (host-computed in FP64, stored in T).
 template <class T>

@@ -13,8 +13,9 @@
 
 #include "chswe.h"
 #include "swe_common.cuh"
+#include "swe_advective.cuh"
 #include "swe_kernels.cuh"
-#include "swe_tiled.cuh"
+#include "swe_launch.cuh"
 
 namespace chswe {
 
@@ -217,8 +218,11 @@ struct swe_ctx {
     void *ya = nullptr, *yb = nullptr, *acc = nullptr, *w = nullptr;
     void *edge = nullptr;            // synchronised panel-boundary values of the current stage
     void *es = nullptr;              // edge strips of the current stage (k_co2contra -> k_edge)
-    // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x meshes, [N+1][P]
+    // FP64 quadrature weights (J hx hy Ax Ay) on xy, y, x and o (cell-centre) meshes, [N+1][P]
     double *qw = nullptr;
+    // FP64 tables of the curl and enstrophy on the o mesh (built on first use): J a
+    // (one box), the Coriolis parameter f (one box per panel); then 6 N^2 curl values
+    double *otab = nullptr;
     double *red = nullptr;           // reduction partials
     unsigned char *pinned = nullptr; // pinned host staging for uploads/downloads (whole batch)
     // captured RK4 step
@@ -274,19 +278,6 @@ static bool g_tables_ready[64] = {false};
 // Maximal tile sizes the stage kernels are built for; ceil(N / (TM - 1)) balanced
 // tiles per direction always fit, whatever N.
 static bool valid_tile(int tm) { return tm == 17 || tm == 25 || tm == 33; }
-// Kernel configurations the stage kernels are built for: (maximal tile edge,
-// resident blocks per SM the register allocation is capped for, stencil runs of
-// several outputs per thread or one).  The advective operator's stage kernel is
-// built for the first blocks-per-SM value of each tile only.
-#define CHSWE_LINEAR_CFGS(X)                                                                                  \
-    X(17, 3, 0) X(17, 4, 0) X(25, 2, 0) X(25, 3, 0) X(25, 4, 0) X(33, 2, 0) X(33, 3, 0) X(17, 3, 1) X(17, 4, 1) \
-        X(25, 2, 1) X(25, 3, 1) X(25, 4, 1) X(33, 2, 1) X(33, 3, 1)
-#define CHSWE_ADV_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0) X(17, 3, 1) X(25, 2, 1) X(33, 2, 1)
-// SBP 2-1 stage kernels (linear operator): the first blocks-per-SM value of each
-// tile, one output per element.
-#define CHSWE_LINEAR21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
-// SBP 6-3 stage kernels: the same configurations
-#define CHSWE_LINEAR63_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 struct KernelCfg {
     int tile, occ, runs;
 };
@@ -313,7 +304,6 @@ static bool valid_cfg(int ord, int tm, int occ, int runs)
         if (cs[k].tile == tm && cs[k].occ == occ && cs[k].runs == runs) return true;
     return false;
 }
-static constexpr int cfg_code(int tm, int occ, int runs) { return tm * 100 + occ * 10 + runs; }
 // edge-strip lines per panel side for SBP order ord
 static int ord_strip_lines(int ord) { return ord == 63 ? strip_lines<63>() : strip_lines<42>(); }
 // Default before autotuning: tiles of about 24 points for the smaller cubes.
@@ -321,15 +311,31 @@ static int default_tile(int N) { return N <= 96 ? 25 : 33; }
 
 static void cube_edges(int out[12][2]);
 
+// The panel links and cube edges into the constant memory of this unit and of every
+// stage translation unit (each holds its own copy), on the current device.
+static cudaError_t upload_link_tables()
+{
+    Link L[NPAN][4];
+    compute_links(L);
+    int ce[12][2];
+    cube_edges(ce);
+    const Link *l = &L[0][0];
+    const int *q = &ce[0][0];
+    cudaError_t e = cudaMemcpyToSymbol(c_link, L, sizeof(L));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cube_edge, ce, sizeof(ce));
+    if (e == cudaSuccess) e = StageTU<float, 17>::upload_tables(l, q);
+    if (e == cudaSuccess) e = StageTU<float, 25>::upload_tables(l, q);
+    if (e == cudaSuccess) e = StageTU<float, 33>::upload_tables(l, q);
+    if (e == cudaSuccess) e = StageTU<double, 17>::upload_tables(l, q);
+    if (e == cudaSuccess) e = StageTU<double, 25>::upload_tables(l, q);
+    if (e == cudaSuccess) e = StageTU<double, 33>::upload_tables(l, q);
+    return e;
+}
+
 static int upload_tables(swe_ctx *c)
 {
     if (c->device >= 0 && c->device < 64 && g_tables_ready[c->device]) return SWE_OK;
-    Link L[NPAN][4];
-    compute_links(L);
-    CU(c, cudaMemcpyToSymbol(c_link, L, sizeof(L)));
-    int ce[12][2];
-    cube_edges(ce);
-    CU(c, cudaMemcpyToSymbol(c_cube_edge, ce, sizeof(ce)));
+    CU(c, upload_link_tables());
     if (c->device >= 0 && c->device < 64) g_tables_ready[c->device] = true;
     return SWE_OK;
 }
@@ -627,12 +633,13 @@ static void cube_edges(int out[12][2])
             if (p * 4 + s < L[p][s].nb * 4 + L[p][s].nside && k < 12) { out[k][0] = p; out[k][1] = s; k++; }
 }
 
-// SBP quadrature weights J hx hy Ax Ay (quadrature_factory_mod.f90:89-188) for xy, y, x meshes.
+// SBP quadrature weights J hx hy Ax Ay (quadrature_factory_mod.f90:89-188) for xy, y, x
+// and o (cell centres, the Ch q mesh of the enstrophy) meshes.
 static int build_quadrature(swe_ctx *c)
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t box = (size_t)c->dims.ps;
-    std::vector<double> h(3 * box, 0.0);
+    std::vector<double> h(4 * box, 0.0);
     // edge weights of the SBP norms: D42_A_interfaces / D42_A_centers, or D21_*
     // (sbp_operators_collection_mod.f90:169-170,196-197)
     const double AI42[5] = {7.0 / 18.0, 9.0 / 8.0, 1.0, 71.0 / 72.0, 1.0};
@@ -650,8 +657,9 @@ static int build_quadrature(swe_ctx *c)
     };
     const double pi = 3.141592653589793238462643383279502884;
     const double hx = (0.25 * pi - (-0.25 * pi)) / (double)N;
-    HostMetric ms[3] = {host_metric(N, 0.0, 0.0), host_metric(N, 0.5, 0.0), host_metric(N, 0.0, 0.5)};
-    for (int q = 0; q < 3; q++) {
+    HostMetric ms[4] = {host_metric(N, 0.0, 0.0), host_metric(N, 0.5, 0.0), host_metric(N, 0.0, 0.5),
+                        host_metric(N, 0.5, 0.5)};
+    for (int q = 0; q < 4; q++) {
         const HostMetric &m = ms[q];
         for (int j = 1; j <= m.ny; j++)
             for (int i = 1; i <= m.nx; i++) {
@@ -691,7 +699,7 @@ static void free_ctx(swe_ctx *c)
     if (c->graphk) cudaGraphExecDestroy(c->graphk);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
-    cudaFree(c->qw); cudaFree(c->red);
+    cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -992,57 +1000,9 @@ extern "C" int swe_stvec_update(swe_stvec *y, double s1, const swe_stvec *v1, do
 // ---------------------------------------------------------------------------
 // operator application and RK4
 // ---------------------------------------------------------------------------
-static dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
-
-// The stage kernels are launched with programmatic stream serialization: each may
-// start (and load its metric) while its predecessor finishes, and waits for the
-// predecessor's results with griddepcontrol.wait.  CHSWE_PDL=0 in the environment
-// launches them plainly.
-static bool pdl_enabled()
-{
-    static const bool on = [] {
-        const char *e = std::getenv("CHSWE_PDL");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
-
-template <typename... KArgs, typename... Args>
-static void launch_k(void (*kern)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t st, Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = g;
-    cfg.blockDim = b;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
-}
-// Balanced tiles: ceil(N / (TM - 1)) tiles per direction, widths at most TM.
-static dim3 stage_grid(int N, int members, int tm)
-{
-    const int nb = (N + tm - 2) / (tm - 1);
-    return dim3(nb, nb, NPAN * members);
-}
-
-// The tiled kernels use more than 48 KB of dynamic shared memory: opt in once per
-// device and element type (the attribute belongs to the device's context).
-template <class T, int TM, int OCC, bool ADV, bool RUNS, int ORD>
-static cudaError_t stage_smem_optin_modes()
-{
-    const int sb = (int)StageLayout<T, TM>::bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 0, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 1, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-    return e;
-}
-
+// Dispatch to the stage translation units (stage_*.cu) by tile size.  The tiled
+// kernels use more than 48 KB of dynamic shared memory: opt in once per device and
+// element type (the attribute belongs to the device's context).
 template <class T>
 static cudaError_t stage_smem_optin()
 {
@@ -1051,79 +1011,22 @@ static cudaError_t stage_smem_optin()
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && done[dev]) return cudaSuccess;
-#define CHSWE_OPTIN_LIN(TM, OCC, RUNS)                                                                            \
-    if (e == cudaSuccess)                                                                                         \
-        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 42>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)Co2Layout<T, TM>::bytes());                                                \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 42>();
-#define CHSWE_OPTIN_LIN21(TM, OCC, RUNS)                                                                          \
-    if (e == cudaSuccess)                                                                                         \
-        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 21>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)Co2Layout<T, TM>::bytes());                                                \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 21>();
-#define CHSWE_OPTIN_LIN63(TM, OCC, RUNS)                                                                          \
-    if (e == cudaSuccess)                                                                                         \
-        e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, 63>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)Co2Layout<T, TM>::bytes());                                                \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, false, RUNS, 63>();
-#define CHSWE_OPTIN_ADV(TM, OCC, RUNS) \
-    if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, true, RUNS, 42>();
-    CHSWE_LINEAR_CFGS(CHSWE_OPTIN_LIN)
-    CHSWE_LINEAR21_CFGS(CHSWE_OPTIN_LIN21)
-    CHSWE_LINEAR63_CFGS(CHSWE_OPTIN_LIN63)
-    CHSWE_ADV_CFGS(CHSWE_OPTIN_ADV)
-#undef CHSWE_OPTIN_LIN
-#undef CHSWE_OPTIN_LIN21
-#undef CHSWE_OPTIN_LIN63
-#undef CHSWE_OPTIN_ADV
+    e = StageTU<T, 17>::optin();
+    if (e == cudaSuccess) e = StageTU<T, 25>::optin();
+    if (e == cudaSuccess) e = StageTU<T, 33>::optin();
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
-// ord: SBP order (42, 21 or 63); codes of order 21 are offset by 100000, of 63 by 200000.
+// ord: SBP order (42, 21 or 63).  Configurations are validated when set.
 template <class T>
 static void launch_co2contra(int tm, int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                              const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
-    const dim3 g = stage_grid(d.N, members, tm);
-    switch (cfg_code(tm, occ, runs) + (ord == 21 ? 100000 : (ord == 63 ? 200000 : 0))) {
-#define CHSWE_CO2_CASE(TM, OCC, RUNS)                                                                                 \
-    case cfg_code(TM, OCC, RUNS):                                                                                 \
-        launch_k(k_co2contra<T, TM, OCC, RUNS, 42>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
-                 dtm);                                                                                            \
-        break;
-#define CHSWE_CO2_CASE21(TM, OCC, RUNS)                                                                               \
-    case 100000 + cfg_code(TM, OCC, RUNS):                                                                        \
-        launch_k(k_co2contra<T, TM, OCC, RUNS, 21>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
-                 dtm);                                                                                            \
-        break;
-        CHSWE_LINEAR_CFGS(CHSWE_CO2_CASE)
-#define CHSWE_CO2_CASE63(TM, OCC, RUNS)                                                                               \
-    case 200000 + cfg_code(TM, OCC, RUNS):                                                                        \
-        launch_k(k_co2contra<T, TM, OCC, RUNS, 63>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w, es, d, m, \
-                 dtm);                                                                                            \
-        break;
-        CHSWE_LINEAR21_CFGS(CHSWE_CO2_CASE21)
-        CHSWE_LINEAR63_CFGS(CHSWE_CO2_CASE63)
-#undef CHSWE_CO2_CASE
-#undef CHSWE_CO2_CASE21
-#undef CHSWE_CO2_CASE63
-    default: break;   // configurations are validated when set
-    }
-}
-
-template <class T, int TM, int OCC, bool ADV, bool RUNS, int ORD>
-static void launch_stage_modes(int members, const T *y, const T *w, const T *e, T *v0, T *y1, T *acc, T *cmp,
-                               const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st)
-{
-    const dim3 g = stage_grid(d.N, members, TM);
-    const size_t sb = StageLayout<T, TM>::bytes();
-    switch (a.mode) {
-    case 0: launch_k(k_stage<T, TM, OCC, 0, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 1: launch_k(k_stage<T, TM, OCC, 1, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 2: launch_k(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    case 3: launch_k(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
-    default: launch_k(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>, g, stage_block(), sb, st, y, w, e, v0, y1, acc, cmp, d, m, a); break;
+    switch (tm) {
+    case 17: StageTU<T, 17>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
+    case 25: StageTU<T, 25>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
+    default: StageTU<T, 33>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
     }
 }
 
@@ -1134,32 +1037,10 @@ static void launch_stage(int tm, int occ, int runs, int ord, int members, const 
                          cudaStream_t st)
 {
     if (a.A) occ = default_occ(tm);
-    switch (cfg_code(tm, occ, runs) + (a.A ? 10000 : 0) + (ord == 21 ? 100000 : (ord == 63 ? 200000 : 0))) {
-#define CHSWE_STAGE_CASE(TM, OCC, RUNS)                                                                        \
-    case cfg_code(TM, OCC, RUNS):                                                                          \
-        launch_stage_modes<T, TM, OCC, false, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
-        break;
-#define CHSWE_STAGE_CASE21(TM, OCC, RUNS)                                                                      \
-    case 100000 + cfg_code(TM, OCC, RUNS):                                                                 \
-        launch_stage_modes<T, TM, OCC, false, RUNS, 21>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
-        break;
-#define CHSWE_STAGE_CASE63(TM, OCC, RUNS)                                                                      \
-    case 200000 + cfg_code(TM, OCC, RUNS):                                                                 \
-        launch_stage_modes<T, TM, OCC, false, RUNS, 63>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);  \
-        break;
-#define CHSWE_STAGE_CASE_ADV(TM, OCC, RUNS)                                                                    \
-    case 10000 + cfg_code(TM, OCC, RUNS):                                                                  \
-        launch_stage_modes<T, TM, OCC, true, RUNS, 42>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);   \
-        break;
-        CHSWE_LINEAR_CFGS(CHSWE_STAGE_CASE)
-        CHSWE_ADV_CFGS(CHSWE_STAGE_CASE_ADV)
-        CHSWE_LINEAR21_CFGS(CHSWE_STAGE_CASE21)
-        CHSWE_LINEAR63_CFGS(CHSWE_STAGE_CASE63)
-#undef CHSWE_STAGE_CASE
-#undef CHSWE_STAGE_CASE_ADV
-#undef CHSWE_STAGE_CASE21
-#undef CHSWE_STAGE_CASE63
-    default: break;   // configurations are validated when set
+    switch (tm) {
+    case 17: StageTU<T, 17>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 25: StageTU<T, 25>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    default: StageTU<T, 33>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
     }
 }
 
@@ -1492,6 +1373,221 @@ extern "C" int swe_diag(swe_ctx *c, const swe_stvec *vec, int member, double dt,
     return SWE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Curl, energies and potential enstrophy (swm_output_diag_t%calc_energies)
+// ---------------------------------------------------------------------------
+// The neighbour's copy of the tangential covariant component on side s of panel t,
+// at along-edge centre c (1..N): u on its B and T sides, v on L and R, with the
+// orientation sign.  It is the halo value (index 0 / N+2) that the Ch vector
+// exchange (exchange_halo_Ch_mod.f90) gives the curl SAT.
+template <class T>
+__device__ __forceinline__ double tan_halo(const T *Y, const Dims &d, int t, int s, int c)
+{
+    const Link L = c_link[t][s];
+    const int N = d.N, cp = L.rev ? N + 1 - c : c;
+    double x;
+    switch (L.nside) {
+    case SIDE_L: x = (double)gview(Y, d, 2, L.nb)(1, cp); break;
+    case SIDE_R: x = (double)gview(Y, d, 2, L.nb)(N + 1, cp); break;
+    case SIDE_B: x = (double)gview(Y, d, 1, L.nb)(cp, 1); break;
+    default: x = (double)gview(Y, d, 1, L.nb)(cp, N + 1); break;
+    }
+    return L.st * x;
+}
+
+// curl_sbp_sat_t%calc_curl_tile for curl_ch_sbp_sat_{21,42,63} (curl_sbp_sat_mod.f90:48-74):
+// at cell centre (i, j) of panel t, the i2c differences of the covariant u along y
+// and v along x with their SAT terms, (Dx / hx - Dy / hy) / (J a).  FP64.
+template <class T, int ORD>
+__device__ double curl_at(const T *Y, const Dims &d, int t, int i, int j, double hx, double Ja)
+{
+    using SB = SbpOrder<ORD>;
+    const int N = d.N;
+    const GV<T> U = gview(Y, d, 1, t), V = gview(Y, d, 2, t);
+    double dy = SB::template di2c<double>(j, N, [&](int k) { return (double)U(i, k); });
+    double dx = SB::template di2c<double>(i, N, [&](int k) { return (double)V(k, j); });
+    if (j <= SB::NSAT) dy += SB::satw(j) * ((double)U(i, 1) - tan_halo(Y, d, t, SIDE_B, i));
+    if (j >= N + 1 - SB::NSAT) dy += SB::satw(N + 1 - j) * (tan_halo(Y, d, t, SIDE_T, i) - (double)U(i, N + 1));
+    if (i <= SB::NSAT) dx += SB::satw(i) * ((double)V(1, j) - tan_halo(Y, d, t, SIDE_L, j));
+    if (i >= N + 1 - SB::NSAT) dx += SB::satw(N + 1 - i) * (tan_halo(Y, d, t, SIDE_R, j) - (double)V(N + 1, j));
+    return (dx / hx - dy / hx) / Ja;
+}
+
+// The curl of one member on the cell centres, packed [panel][j][i] in FP64.
+template <class T, int ORD>
+__global__ void k_curl(const T *__restrict__ y, const double *__restrict__ otab, Dims d, double hx,
+                       double *__restrict__ out)
+{
+    const int N = d.N;
+    const int64_t npts = (int64_t)NPAN * N * N;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npts; k += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(k / ((int64_t)N * N)), r = (int)(k % ((int64_t)N * N));
+        const int j = r / N + 1, i = r % N + 1;
+        out[k] = curl_at<T, ORD>(y, d, t, i, j, hx, otab[box_off(d.P, i, j)]);
+    }
+}
+
+// The four sums of calc_energies (swm_output_diag_mod.f90:186-234), per block:
+// term 0 <h h>_xy, 1 <hu ut u / 2>_y, 2 <hv vt v / 2>_x with hu, hv = I_i2c(h),
+// 3 <(curl + f)^2 / (2 hq)>_o with hq = (I_i2c,y(hu) + I_i2c,x(hv)) / 2.
+// w holds (ut, vt) in its fields 1 and 2.  FP64 arithmetic.
+template <class T, int ORD>
+__global__ void k_energies(const T *__restrict__ y, const T *__restrict__ w, const double *__restrict__ qw,
+                           const double *__restrict__ otab, Dims d, double hx, double *partial)
+{
+    using SB = SbpOrder<ORD>;
+    const int term = blockIdx.y;
+    const int n = d.N + 1, N = d.N;
+    const int64_t npts = (int64_t)NPAN * n * n;
+    double acc = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npts; k += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(k / ((int64_t)n * n)), r = (int)(k % ((int64_t)n * n));
+        const int j = r / n + 1, i = r % n + 1;
+        const int64_t o = box_off(d.P, i, j);
+        const GV<T> H = gview(y, d, 0, t);
+        if (term == 0) {
+            const double h = (double)H(i, j);
+            acc += h * h * qw[o];
+        } else if (term == 1) {
+            if (i > N) continue;
+            const double hu = SB::template ii2c<double>(i, N, [&](int q) { return (double)H(q, j); });
+            acc += 0.5 * (hu * (double)w[1 * d.fs + t * d.ps + o]) * (double)y[1 * d.fs + t * d.ps + o] * qw[d.ps + o];
+        } else if (term == 2) {
+            if (j > N) continue;
+            const double hv = SB::template ii2c<double>(j, N, [&](int q) { return (double)H(i, q); });
+            acc += 0.5 * (hv * (double)w[2 * d.fs + t * d.ps + o]) * (double)y[2 * d.fs + t * d.ps + o] *
+                   qw[2 * d.ps + o];
+        } else {
+            if (i > N || j > N) continue;
+            const double hqu = SB::template ii2c<double>(j, N, [&](int q) {
+                return SB::template ii2c<double>(i, N, [&](int p) { return (double)H(p, q); });
+            });
+            const double hqv = SB::template ii2c<double>(i, N, [&](int q) {
+                return SB::template ii2c<double>(j, N, [&](int p) { return (double)H(q, p); });
+            });
+            const double hq = 0.5 * hqu + 0.5 * hqv;
+            const double c = curl_at<T, ORD>(y, d, t, i, j, hx, otab[o]) + otab[(1 + t) * d.ps + o];
+            acc += 0.5 * c * c / hq * qw[3 * d.ps + o];
+        }
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+// J a and the Coriolis parameter (calc_coriolis_parameter, coriolis_factory_mod.f90:239-280)
+// on the cell centres, and room for one member's curl: built on first use.
+static int ensure_otab(swe_ctx *c)
+{
+    if (c->otab) return SWE_OK;
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t box = (size_t)c->dims.ps;
+    std::vector<double> h(7 * box, 0.0);
+    const HostMetric m = host_metric(N, 0.5, 0.5);
+    const MeshGeom g = mesh_geom(N, 0.5, 0.5);
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N; i++) {
+            const size_t k = (size_t)(j - 1) * m.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            h[o] = m.J[k] * c->cfg.radius;
+            for (int p = 0; p < NPAN; p++) {
+                double f = c->cfg.omega;
+                if (!c->cfg.coriolis_constant) {
+                    double r[3], a1[3], a2[3];
+                    mesh_point(g, p, i, j, r, a1, a2);
+                    const double *ax = c->cfg.rotation_axis;
+                    f = 2 * c->cfg.omega * (ax[0] * r[0] + ax[1] * r[1] + ax[2] * r[2]) /
+                        std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                }
+                h[(1 + p) * box + o] = f;
+            }
+        }
+    const size_t ncurl = (size_t)NPAN * N * N;
+    if (cudaMalloc(&c->otab, (h.size() + ncurl) * sizeof(double)) != cudaSuccess) {
+        c->otab = nullptr;
+        return fail(c, SWE_ENOMEM, "diagnostic table allocation failed");
+    }
+    CU(c, cudaMemcpy(c->otab, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return SWE_OK;
+}
+
+template <class T>
+static void launch_curl(swe_ctx *c, const T *y, const Dims &d, double hx, double *out)
+{
+    const int64_t npts = (int64_t)NPAN * d.N * d.N;
+    const dim3 g((unsigned)std::min<int64_t>((npts + 255) / 256, 4096)), b(256);
+    if (c->ord == 21) k_curl<T, 21><<<g, b, 0, c->stream>>>(y, c->otab, d, hx, out);
+    else if (c->ord == 63) k_curl<T, 63><<<g, b, 0, c->stream>>>(y, c->otab, d, hx, out);
+    else k_curl<T, 42><<<g, b, 0, c->stream>>>(y, c->otab, d, hx, out);
+}
+
+template <class T>
+static void launch_energies(swe_ctx *c, const T *y, const Dims &d, double hx, int nb)
+{
+    const dim3 g(nb, 4), b(256);
+    const T *w = (const T *)c->w;
+    if (c->ord == 21) k_energies<T, 21><<<g, b, 0, c->stream>>>(y, w, c->qw, c->otab, d, hx, c->red);
+    else if (c->ord == 63) k_energies<T, 63><<<g, b, 0, c->stream>>>(y, w, c->qw, c->otab, d, hx, c->red);
+    else k_energies<T, 42><<<g, b, 0, c->stream>>>(y, w, c->qw, c->otab, d, hx, c->red);
+}
+
+extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *out)
+{
+    if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    int rc = ensure_otab(c);
+    if (rc != SWE_OK) return rc;
+    const size_t mo = (size_t)member * c->dims.ms, box = (size_t)c->dims.ps;
+    const size_t ncurl = (size_t)NPAN * c->cfg.N * c->cfg.N;
+    const double hx = 0.5 * 3.141592653589793238462643383279502884 / c->cfg.N;
+    double *dcurl = c->otab + 7 * box;
+    if (c->elem == 8) launch_curl<double>(c, (const double *)vec->d + mo, c->dims, hx, dcurl);
+    else launch_curl<float>(c, (const float *)vec->d + mo, c->dims, hx, dcurl);
+    c->launches += 1;
+    CU(c, cudaGetLastError());
+    CU(c, cudaMemcpyAsync(out, dcurl, ncurl * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+extern "C" int swe_energies(swe_ctx *c, const swe_stvec *vec, int member, double *out)
+{
+    if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    int rc = ensure_otab(c);
+    if (rc != SWE_OK) return rc;
+    const int nb = 256;
+    const size_t mo = (size_t)member * c->dims.ms;
+    const double hx = 0.5 * 3.141592653589793238462643383279502884 / c->cfg.N;
+    Dims d1 = c->dims;
+    if (c->elem == 8) {
+        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
+                                 (double *)c->es, d1, c->m64.v, c->stream);
+        launch_energies<double>(c, (const double *)vec->d + mo, d1, hx, nb);
+    } else {
+        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
+                                (float *)c->es, d1, c->m32.v, c->stream);
+        launch_energies<float>(c, (const float *)vec->d + mo, d1, hx, nb);
+    }
+    c->launches += 2;
+    CU(c, cudaGetLastError());
+    std::vector<double> part(nb * 4);
+    CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    double sum[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 4; q++)
+        for (int k = 0; k < nb; k++) sum[q] += part[q * nb + k];
+    // the reference scales the potential energy with its constant Earth_grav; this uses the context's g
+    const double pe = 0.5 * c->cfg.grav * sum[0], ke = sum[1] + sum[2];
+    out[0] = ke + pe;
+    out[1] = ke;
+    out[2] = pe;
+    out[3] = sum[3];
+    return SWE_OK;
+}
+
 extern "C" int swe_edge_links(int *out)
 {
     if (!out) return SWE_EINVAL;
@@ -1728,9 +1824,7 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
     if (!nd.ready) {
         // once per device, with the device current: the array's device address and the edge tables
         if (cudaGetSymbolAddress((void **)&nd.base, g_noalloc_scratch) != cudaSuccess) return SWE_ECUDA;
-        Link L[NPAN][4];
-        compute_links(L);
-        if (cudaMemcpyToSymbol(c_link, L, sizeof(L)) != cudaSuccess) return SWE_ECUDA;
+        if (upload_link_tables() != cudaSuccess) return SWE_ECUDA;
         if (stage_smem_optin<double>() != cudaSuccess) return SWE_ECUDA;
         if (dev < 64) g_tables_ready[dev] = true;
         nd.ready = true;

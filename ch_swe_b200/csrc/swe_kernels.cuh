@@ -21,7 +21,7 @@
 namespace chswe {
 
 // Edge connectivity, filled once per device by the host.
-__constant__ Link c_link[NPAN][4];
+static __constant__ Link c_link[NPAN][4];
 
 // Read-only view of one field of one panel: v(i, j) with the reference's 1-based indices.
 template <class T>
@@ -355,6 +355,9 @@ __device__ __forceinline__ const T *edge_entry(const T *E, int N, int mem, int t
     if (l == 1) return E + edge_index(N, mem, t, SIDE_B, k);
     return E + edge_index(N, mem, t, SIDE_T, k);
 }
+
+// threads of a stage / contravariant tile block
+constexpr int STAGE_THREADS = 256;
 
 // RK4 stage parameters.
 struct StageArgs {

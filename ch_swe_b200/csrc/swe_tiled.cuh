@@ -26,8 +26,6 @@
 
 namespace chswe {
 
-constexpr int STAGE_THREADS = 256;
-
 // Tiles of at most TM x TM points, ceil(N / (TM - 1)) of them per direction.
 template <int TM>
 struct Tile {

@@ -27,12 +27,49 @@ class SwmOutputDiag:
               "swe_diag")
         return {"h_min": out[0], "h_max": out[1], "cfl_gravity": out[2], "cfl_adv_x": out[3], "cfl_adv_y": out[4]}
 
+    def calc_energies(self, state, member: int = 0) -> dict:
+        """TE, KE, PE and the potential enstrophy of calc_energies (swm_output_diag_mod.f90:186-234)
+        for covariant (u, v), computed on the device in FP64."""
+        out = (ctypes.c_double * 4)()
+        check(_lib.load().swe_energies(self.domain.ctx, state.handle, int(member), out), self.domain.ctx,
+              "swe_energies")
+        return {"te": out[0], "ke": out[1], "pe": out[2], "enstrophy": out[3]}
+
+    def curl(self, state, member: int = 0) -> np.ndarray:
+        """Curl of the covariant (u, v) on the cell centres (curl_ch_sbp_sat_*): (6, N, N), FP64."""
+        N = self.domain.N
+        out = np.empty((6, N, N))
+        check(_lib.load().swe_curl(self.domain.ctx, state.handle, int(member),
+                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), self.domain.ctx, "swe_curl")
+        return out
+
+    def print_integrals_diag(self, state, member: int = 0) -> str:
+        """The line of print_integrals_diag (swm_output_diag_mod.f90:155-183): h extrema, mass,
+        TE, KE, PE and enstrophy."""
+        d = self.diagnostics(state, 0.0, member)
+        mass, _ = state_integrals(self.domain, state, member)
+        e = self.calc_energies(state, member)
+        vals = [("hmin = ", d["h_min"]), (" hmax = ", d["h_max"]), (" mass = ", mass), (" TE = ", e["te"]),
+                (" KE = ", e["ke"]), (" PE = ", e["pe"]), (" Enstrophy = ", e["enstrophy"])]
+        line = "".join(f"{k}{v:24.16E}" for k, v in vals)
+        print(line)
+        return line
+
     def print_cfl_diag(self, state, dt: float, member: int = 0) -> str:
         d = self.diagnostics(state, dt, member)
         line = (f"Gravity waves CFL-max = {d['cfl_gravity']:15.7f}, Advective CFL-max (x,y) = "
                 f"{d['cfl_adv_x']:15.7f}{d['cfl_adv_y']:15.7f}")
         print(line)
         return line
+
+
+def state_integrals(domain, state, member: int = 0):
+    """(mass, linear energy) of swe_integrals for one member."""
+    m = ctypes.c_double()
+    e = ctypes.c_double()
+    check(_lib.load().swe_integrals(domain.ctx, state.handle, int(member), ctypes.byref(m), ctypes.byref(e)),
+          domain.ctx, "swe_integrals")
+    return m.value, e.value
 
 
 def write_paneled(path: str, field: np.ndarray, rec: int = 1) -> None:

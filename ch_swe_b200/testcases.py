@@ -35,9 +35,9 @@ def _to_real(p: int, v: np.ndarray) -> np.ndarray:
 
 
 def mesh_geometry(N: int, mesh: str):
-    """Unit position vectors r and tangent vectors a1, a2 of a mesh ('xy', 'y' or 'x'),
-    each (6, ny, nx, 3)."""
-    si, sj = {"xy": (0.0, 0.0), "y": (0.5, 0.0), "x": (0.0, 0.5)}[mesh]
+    """Unit position vectors r and tangent vectors a1, a2 of a mesh ('xy', 'y', 'x' or 'o',
+    the cell centres), each (6, ny, nx, 3)."""
+    si, sj = {"xy": (0.0, 0.0), "y": (0.5, 0.0), "x": (0.0, 0.5), "o": (0.5, 0.5)}[mesh]
     nx = N + 1 if si == 0.0 else N
     ny = N + 1 if sj == 0.0 else N
     ta = np.tan(_angles(N, nx, si))[None, :]

@@ -133,6 +133,22 @@ int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, 
    the contravariant components and dx = dy = a (pi/2) / N.  Synchronous. */
 int swe_diag(swe_ctx *ctx, const swe_stvec *vec, int member, double dt, double *out);
 
+/* Energies and potential enstrophy of swm_output_diag_t%calc_energies for one member
+   with covariant (u, v) (swm_output_diag_mod.f90:186-234, with the operators of the Ch
+   diagnostics configuration: co2contra_ch_sbp*, curl_ch_sbp_sat_*, interp2d_p2uv_Ch_sbp*,
+   interp2d_uv2qvec_Ch_sbp*, SBP_C*_quadrature; gen_config_linear.sh:53-63):
+   out[0..3] = TE, KE, PE, enstrophy with
+     KE = <hu ut u>_u / 2 + <hv vt v>_v / 2   (hu, hv: h interpolated to the u, v points)
+     PE = g/2 <h h>_h                          (no orography)
+     enstrophy = <(curl + f)^2 / (2 hq)>_q     (q: cell centres; hq: the mean of the two
+                                               interpolations of hu, hv to the centres)
+   in the context's SBP order, FP64 arithmetic.  Synchronous. */
+int swe_energies(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
+
+/* Curl of the covariant (u, v) of one member on the cell centres (curl_ch_sbp_sat_{21,42,63},
+   curl_sbp_sat_mod.f90:27-76): out[6][N][N] in FP64, i fastest.  Synchronous. */
+int swe_curl(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
+
 /* Number of kernel launches issued on the context's stream since creation. */
 long long swe_launch_count(const swe_ctx *ctx);
 

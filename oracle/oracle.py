@@ -65,6 +65,9 @@ def lib():
         L.orc_set_sbp_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_diag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, _dp]
         L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_curl.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_energies.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+        L.orc_latlon_xy.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
         _lib = L
     return _lib
 
@@ -118,6 +121,29 @@ class Oracle:
         out = np.zeros(5)
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
         lib().orc_diag(self._c, _p(a[0]), _p(a[1]), _p(a[2]), float(dt), _p(out))
+        return tuple(out)
+
+    def curl(self, u, v):
+        """Curl of the covariant (u, v) on the cell centres (curl_ch_sbp_sat_*): shape (6, N, N)."""
+        out = np.zeros((6, self.N, self.N))
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v)]
+        lib().orc_curl(self._c, _p(a[0]), _p(a[1]), _p(out))
+        return out
+
+    def latlon(self, f, nlat=None, nlon=None):
+        """Cubic lat-lon regrid of an xy field (latlon_outputer_t, default grid 2N+1 x 4N):
+        shape (nlat, nlon)."""
+        nlat = 2 * self.N + 1 if nlat is None else int(nlat)
+        nlon = 4 * self.N if nlon is None else int(nlon)
+        out = np.zeros((nlat, nlon))
+        lib().orc_latlon_xy(self._c, _p(np.ascontiguousarray(f, dtype=np.float64)), nlat, nlon, _p(out))
+        return out
+
+    def energies(self, h, u, v):
+        """(TE, KE, PE, enstrophy) of swm_output_diag_t%calc_energies (covariant u, v)."""
+        out = np.zeros(4)
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        lib().orc_energies(self._c, _p(a[0]), _p(a[1]), _p(a[2]), _p(out))
         return tuple(out)
 
     def gaussian(self, lam0=np.pi, phi0=0.0, d0=0.25, amp=1.0):
@@ -176,7 +202,9 @@ class Oracle:
         return lib().orc_dot(self._c, mesh, _p(a), _p(np.ascontiguousarray(b, dtype=np.float64)))
 
     def metric(self, mesh: int, what: int):
-        shp = shapes(self.N)[mesh]
+        """mesh 0 xy, 1 y (u), 2 x (v), 3 o (centres); what 0 J, 1-3 Q1-Q3, 4 f J^2 (f on o),
+        5-7 the unit position vector's x, y, z."""
+        shp = (6, self.N, self.N) if mesh == 3 else shapes(self.N)[mesh]
         out = np.empty(shp)
         lib().orc_metric(self._c, mesh, what, _p(out))
         return out

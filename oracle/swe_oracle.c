@@ -844,28 +844,35 @@ typedef struct orc_ctx {
     int nonlinear;
     exch_t ex_xy5_full_s, ex_ch1c_u, ex_ch1c_v;
     fld_t htot, hu, hv, cu, cv, uh, vh, vau, uav, uhal, vhal;
+    /* energies and enstrophy of swm_output_diag_t: mesh o (cell centres, the Ch q mesh) */
+    mesh_t mo;
+    double *fo;                  /* Coriolis parameter on o, [t][j][i] */
+    fld_t oDx, oDy, curl, hqu, hqv, ehu, ehv;
 } orc_ctx;
+
+/* calc_coriolis_parameter (coriolis_factory_mod.f90:239-280) at point k of mesh m */
+static double coriolis_f(const orc_ctx *c, const mesh_t *m, size_t k)
+{
+    if (c->coriolis_const) return c->omega;
+    double nv[3] = {m->rx[k], m->ry[k], m->rz[k]};
+    double pr = (c->axis[0] * nv[0] + c->axis[1] * nv[1] + c->axis[2] * nv[2]) /
+                sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+    return 2 * c->omega * pr;
+}
 
 static void coriolis_parameter(orc_ctx *c)
 {
     mesh_t *m = &c->mxy;
     size_t n = (size_t)NPAN * m->nx * m->ny;
     c->fJ2 = malloc(sizeof(double) * n);
-    for (int t = 0; t < NPAN; t++)
-        for (int j = 1; j <= m->ny; j++)
-            for (int i = 1; i <= m->nx; i++) {
-                size_t k = MI(m, t, i, j);
-                double f;
-                if (c->coriolis_const) f = c->omega;
-                else {
-                    double nv[3] = {m->rx[k], m->ry[k], m->rz[k]};
-                    double pr = (c->axis[0] * nv[0] + c->axis[1] * nv[1] + c->axis[2] * nv[2]) /
-                                sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-                    f = 2 * c->omega * pr;
-                }
-                /* multiply_by_J_self applied twice (coriolis_factory_mod.f90:188-193) */
-                c->fJ2[k] = f * m->J[k] * m->J[k];
-            }
+    for (size_t k = 0; k < n; k++) {
+        /* multiply_by_J_self applied twice (coriolis_factory_mod.f90:188-193) */
+        c->fJ2[k] = coriolis_f(c, m, k) * m->J[k] * m->J[k];
+    }
+    const mesh_t *o = &c->mo;
+    const size_t no = (size_t)NPAN * o->nx * o->ny;
+    c->fo = malloc(sizeof(double) * no);
+    for (size_t k = 0; k < no; k++) c->fo[k] = coriolis_f(c, o, k);
 }
 
 static void sync_weights(orc_ctx *c)
@@ -907,6 +914,7 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     mesh_build(&c->mxy, N, 0.0, 0.0);
     mesh_build(&c->mx, N, 0.0, 0.5);
     mesh_build(&c->my, N, 0.5, 0.0);
+    mesh_build(&c->mo, N, 0.5, 0.5);
     coriolis_parameter(c);
     sync_weights(c);
     build_xy_exchange(&c->ex_xy3_full_s, N, 3, 0, PK_SCALAR);
@@ -935,18 +943,23 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     fld_init(&c->y[0], N + 1, N + 1, hw);
     fld_init(&c->y[1], N, N + 1, hw);
     fld_init(&c->y[2], N + 1, N, hw);
+    fld_t *oo[] = {&c->oDx, &c->oDy, &c->curl, &c->hqu, &c->hqv};
+    for (unsigned q = 0; q < sizeof(oo) / sizeof(oo[0]); q++) fld_init(oo[q], N, N, hw);
+    fld_init(&c->ehu, N, N + 1, hw);
+    fld_init(&c->ehv, N + 1, N, hw);
     return c;
 }
 
 void orc_destroy(orc_ctx *c)
 {
     if (!c) return;
-    mesh_free(&c->mxy); mesh_free(&c->mx); mesh_free(&c->my);
-    free(c->fJ2); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
+    mesh_free(&c->mxy); mesh_free(&c->mx); mesh_free(&c->my); mesh_free(&c->mo);
+    free(c->fJ2); free(c->fo); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
                     &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
-                    &c->vh, &c->vau, &c->uav, &c->uhal, &c->vhal};
+                    &c->vh, &c->vau, &c->uav, &c->uhal, &c->vhal, &c->oDx, &c->oDy, &c->curl,
+                    &c->hqu, &c->hqv, &c->ehu, &c->ehv};
     for (unsigned q = 0; q < sizeof(all) / sizeof(all[0]); q++) fld_free(all[q]);
     for (int s = 0; s < 4; s++) for (int f = 0; f < 3; f++) fld_free(&c->k[s][f]);
     free(c);
@@ -1584,6 +1597,72 @@ static double q_dot(const mesh_t *m, const fld_t *f1, const fld_t *f2)
     return out;
 }
 
+/* curl_sbp_sat_t%calc_curl for curl_ch_sbp_sat_{21,42,63} (curl_sbp_sat_mod.f90:27-76,
+   curl_factory_mod.f90:89-97,113-117): the i2c difference of the covariant u in y
+   and of v in x, each with its SAT correction against the neighbour's copy of the
+   tangential component on the panel edge (the Ch vector exchange puts it at halo
+   index 0 / N+2), on mesh o:
+       curl = (Dx(v) / hx - Dy(u) / hy) / (J a)                                     */
+static void op_curl(orc_ctx *c, fld_t *curl, fld_t *u, fld_t *v)
+{
+    int N = c->N;
+    exch_do(&c->ex_ch3_u, u, v);
+    exch_do(&c->ex_ch3_v, u, v);
+    const mesh_t *m = &c->mo;
+    for (int t = 0; t < NPAN; t++) {
+        diff_i2c(&c->oDy, u, t, 1, N, 1, N, c->ord);
+        diff_i2c(&c->oDx, v, t, 0, N, 1, N, c->ord);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++)
+                FA(curl, t, i, j) = (FA(&c->oDx, t, i, j) / m->hx - FA(&c->oDy, t, i, j) / m->hy) /
+                                    (m->J[MI(m, t, i, j)] * c->a);
+    }
+}
+
+/* swm_output_diag_t%calc_energies for covariant (u, v) on Ch (swm_output_diag_mod.f90:186-234;
+   operators of the Ch diagnostics configuration: co2contra_ch_sbp*, curl_ch_sbp_sat_*,
+   interp2d_p2uv_Ch_sbp*, interp2d_uv2qvec_Ch_sbp*, SBP_C*_quadrature):
+     KE = <hu ut u>_u / 2 + <hv vt v>_v / 2,  hu, hv = I_i2c(h) along x, y
+     PE = g/2 <h h>_xy  (no orography)
+     enstrophy = < (curl + f)^2 / (2 hq) >_o,  hq = (I_i2c,y(hu) + I_i2c,x(hv)) / 2
+   out = {TE, KE, PE, enstrophy} */
+static void op_energies(orc_ctx *c, double *out, fld_t *h, fld_t *u, fld_t *v)
+{
+    int N = c->N;
+    op_co2contra(c, &c->ut, &c->vt, u, v);
+    op_curl(c, &c->curl, u, v);
+    for (int t = 0; t < NPAN; t++) {
+        interp_i2c(&c->ehu, h, t, 0, N, 1, N + 1, c->ord);
+        interp_i2c(&c->ehv, h, t, 1, N, 1, N + 1, c->ord);
+    }
+    for (int t = 0; t < NPAN; t++) {
+        interp_i2c(&c->hqu, &c->ehu, t, 1, N, 1, N, c->ord);
+        interp_i2c(&c->hqv, &c->ehv, t, 0, N, 1, N, c->ord);
+    }
+    const mesh_t *m = &c->mo;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++) {
+                const double hq = 0.5 * FA(&c->hqu, t, i, j) + 0.5 * FA(&c->hqv, t, i, j);
+                const double w = FA(&c->curl, t, i, j) + c->fo[MI(m, t, i, j)];
+                FA(&c->hqu, t, i, j) = 0.5 * w * w / hq;
+            }
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++)
+                FA(&c->ehu, t, i, j) = 0.5 * (FA(&c->ehu, t, i, j) * FA(&c->ut, t, i, j)) * FA(u, t, i, j);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++)
+                FA(&c->ehv, t, i, j) = 0.5 * (FA(&c->ehv, t, i, j) * FA(&c->vt, t, i, j)) * FA(v, t, i, j);
+    }
+    const double ke = q_dot(&c->my, &c->ehu, NULL) + q_dot(&c->mx, &c->ehv, NULL);
+    const double pe = 0.5 * c->g * q_dot(&c->mxy, h, h);
+    out[0] = ke + pe;
+    out[1] = ke;
+    out[2] = pe;
+    out[3] = q_dot(m, &c->hqu, NULL);
+}
+
 /* ------------------------------------------------------------------ */
 /* exported API (ctypes)                                               */
 /* ------------------------------------------------------------------ */
@@ -1612,6 +1691,7 @@ int orc_set_sbp_order(orc_ctx *c, int ord)
     mesh_mass(&c->mxy, ord);
     mesh_mass(&c->mx, ord);
     mesh_mass(&c->my, ord);
+    mesh_mass(&c->mo, ord);
     return 0;
 }
 
@@ -1709,6 +1789,65 @@ void orc_diag(orc_ctx *c, const double *h, const double *u, const double *v, dou
     out[4] = sqrt(vmax) * dt;
 }
 
+/* latlon_regrid_t%do_regrid of an xy scalar with cubic interpolation (latlon_outputer_mod.f90:30-53,
+   regrid_factory_mod.f90:25-70,165-262 distribute_latlon_points_to_cubsphere,
+   latlon_regrid_mod.f90:286-365 init_interpolation / interpolate,
+   latlon_grid_generator_mod.f90 init / get_cartesian_coords): the field gets an ECS_xy
+   halo of width 2 (on a copy), every point of the nlat x nlon grid
+   (phi_j = -pi/2 + (j-1) pi/(nlat-1), lam_i = (i-1) 2pi/nlon) is located on its panel,
+   and the 4 x 4 cubic Lagrange stencil around it is summed.  out[j][i], i fastest. */
+void orc_latlon_xy(orc_ctx *c, const double *f, int nlat, int nlon, double *out)
+{
+    fld_t *b = &c->htot;
+    fld_from_packed(b, f);
+    ecs_xy_halo(c, b, 2);
+    const mesh_t *m = &c->mxy;
+    const double alpha0 = -0.25 * PI_, beta0 = -0.25 * PI_;
+    for (int j = 1; j <= nlat; j++) {
+        const double phi = -0.5 * PI_ + (j - 1) * PI_ / (nlat - 1.0);
+        for (int i = 1; i <= nlon; i++) {
+            const double lam = (i - 1) * 2.0 * PI_ / nlon;
+            const double r[3] = {cos(phi) * cos(lam), cos(phi) * sin(lam), sin(phi)};
+            int t;
+            double alpha, beta;
+            cart_to_native(r, &t, &alpha, &beta);
+            double zdx = (alpha - alpha0) / m->hx + 1 - m->shift_i;
+            double zdy = (beta - beta0) / m->hy + 1 - m->shift_j;
+            const int xi = (int)zdx, yi = (int)zdy;
+            zdx = zdx - xi;
+            zdy = zdy - yi;
+            double wx[4], wy[4];
+            wx[0] = -zdx * (zdx - 1.0) * (zdx - 2.0) / 6.0;
+            wx[1] = (zdx + 1.0) * (zdx - 1.0) * (zdx - 2.0) / 2.0;
+            wx[2] = -(zdx + 1.0) * zdx * (zdx - 2.0) / 2.0;
+            wx[3] = (zdx + 1.0) * zdx * (zdx - 1.0) / 6.0;
+            wy[0] = -zdy * (zdy - 1.0) * (zdy - 2.0) / 6.0;
+            wy[1] = (zdy + 1.0) * (zdy - 1.0) * (zdy - 2.0) / 2.0;
+            wy[2] = -(zdy + 1.0) * zdy * (zdy - 2.0) / 2.0;
+            wy[3] = (zdy + 1.0) * zdy * (zdy - 1.0) / 6.0;
+            double acc = 0.0;
+            for (int q = -1; q <= 2; q++)
+                for (int p = -1; p <= 2; p++) acc = acc + wx[p + 1] * wy[q + 1] * FA(b, t, xi + p, yi + q);
+            out[(size_t)(j - 1) * nlon + (i - 1)] = acc;
+        }
+    }
+}
+
+/* curl of the covariant (u, v) on mesh o (N x N per panel, packed [t][j][i]) */
+void orc_curl(orc_ctx *c, const double *u, const double *v, double *out)
+{
+    fld_from_packed(&c->u, u); fld_from_packed(&c->v, v);
+    op_curl(c, &c->curl, &c->u, &c->v);
+    fld_to_packed(&c->curl, out);
+}
+
+/* out = {TE, KE, PE, enstrophy} of swm_output_diag_t%calc_energies */
+void orc_energies(orc_ctx *c, const double *h, const double *u, const double *v, double *out)
+{
+    load_state(c, h, u, v);
+    op_energies(c, out, &c->h, &c->u, &c->v);
+}
+
 /* SBP-weighted inner product on mesh 0 = xy (h), 1 = y (u), 2 = x (v) */
 double orc_dot(orc_ctx *c, int mesh, const double *a, const double *b)
 {
@@ -1783,9 +1922,11 @@ void orc_init_ts2(orc_ctx *c, double u0, double h_mean, const double *axis_in, i
    what 0 = J, 1..3 = Qi, 4 = fJ^2 (xy only) */
 void orc_metric(orc_ctx *c, int mesh, int what, double *out)
 {
-    const mesh_t *m = mesh == 0 ? &c->mxy : (mesh == 1 ? &c->my : &c->mx);
+    const mesh_t *m = mesh == 0 ? &c->mxy : (mesh == 1 ? &c->my : (mesh == 2 ? &c->mx : &c->mo));
     size_t n = (size_t)NPAN * m->nx * m->ny;
-    const double *src = what == 0 ? m->J : what == 1 ? m->Q1 : what == 2 ? m->Q2 : what == 3 ? m->Q3 : c->fJ2;
+    /* what: 0 J, 1-3 Q1-Q3, 4 f J^2 (xy) or f (o), 5-7 the unit position vector */
+    const double *src = what == 0 ? m->J : what == 1 ? m->Q1 : what == 2 ? m->Q2 : what == 3 ? m->Q3
+                      : what == 5 ? m->rx : what == 6 ? m->ry : what == 7 ? m->rz : (mesh == 3 ? c->fo : c->fJ2);
     memcpy(out, src, sizeof(double) * n);
 }
 void orc_sync_weights(orc_ctx *c, double *qb, double *qt, double *ql, double *qr)

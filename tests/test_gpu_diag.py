@@ -35,3 +35,82 @@ def test_diag_matches_oracle(precision, tol):
     d0 = SwmOutputDiag(dom).diagnostics(st, dt, member=0)
     assert d0["h_max"] == 0.0 and d0["cfl_adv_x"] == 0.0
     dom.destroy()
+
+
+def _energy_state(o, seed):
+    """A state with h > 0 everywhere (the enstrophy divides by h on the cell centres) and
+    a rotated wind, plus seeded noise on every field so that the duplicated panel-edge
+    copies disagree and the curl SAT terms matter."""
+    rng = np.random.default_rng(seed)
+    h, u, v = o.ts2(u0=30.0, h_mean=3000.0, axis=(0.3, 0.0, 0.95))
+    h = h + o.gaussian(lam0=0.4, phi0=0.3, d0=0.3, amp=50.0)[0]
+    return h + rng.standard_normal(h.shape), u + rng.standard_normal(u.shape), v + rng.standard_normal(v.shape)
+
+
+def _gpu_diag(N, precision, order, state, operator="linear"):
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import SwmOutputDiag
+    dom = create_domain(N, precision=precision, h_mean=1000.0, n_members=2, sbp_order=order, operator=operator)
+    st = create_stvec_swm(dom)
+    st.upload(*state, member=1)
+    st.upload(*(x * 0 + 1.0 for x in state), member=0)
+    diag = SwmOutputDiag(dom)
+    e = diag.calc_energies(st, member=1)
+    curl = diag.curl(st, member=1)
+    e0 = diag.calc_energies(st, member=0)
+    dom.destroy()
+    return (e["te"], e["ke"], e["pe"], e["enstrophy"]), curl, e0
+
+
+@pytest.mark.parametrize("order", [42, 21, 63])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_energies_and_curl_match_oracle(order, precision, tol):
+    """swe_energies / swe_curl against the oracle's calc_energies / curl_ch_sbp_sat_*:
+    relative to each quantity (the curl in the max norm over the field's max)."""
+    from oracle.oracle import Oracle
+    N = 24
+    o = Oracle(N, h_mean=1000.0, axis=(0.0, 0.0, 1.0), sbp_order=order)
+    st = _energy_state(o, 40 + order)
+    ref = o.energies(*st)
+    ref_curl = o.curl(st[1], st[2])
+    got, curl, e0 = _gpu_diag(N, precision, order, st)
+    for g, r, name in zip(got, ref, ("te", "ke", "pe", "enstrophy")):
+        assert abs(g - r) <= tol * abs(r), (order, precision, name, g, r)
+    err = np.abs(curl - ref_curl).max() / np.abs(ref_curl).max()
+    assert err < tol, (order, precision, err)
+    # member 0 holds constant fields (h = u = v = 1): each member is read on its own
+    ref0 = o.energies(*(np.ones_like(x) for x in st))
+    for g, r, name in zip((e0["te"], e0["ke"], e0["pe"], e0["enstrophy"]), ref0, ("te", "ke", "pe", "enstrophy")):
+        assert abs(g - r) <= tol * abs(r), ("member 0", name, g, r)
+
+
+def test_energies_advective_domain_fp64():
+    """The diagnostics of an advective-operator context (SBP 4-2)."""
+    from oracle.oracle import Oracle
+    N = 20
+    o = Oracle(N, h_mean=1000.0)
+    st = _energy_state(o, 7)
+    ref = o.energies(*st)
+    got, curl, _ = _gpu_diag(N, "fp64", 42, st, operator="advective")
+    for g, r in zip(got, ref):
+        assert abs(g - r) <= 1e-12 * abs(r)
+    assert np.abs(curl - o.curl(st[1], st[2])).max() <= 1e-12 * np.abs(curl).max()
+
+
+def test_curl_solid_body_rotation_large_cube():
+    """At C192 (beyond the oracle's sizes): the curl of a solid-body rotation about a
+    tilted axis is 2 u0 / a (r . axis) on the cell centres up to the SBP 4-2
+    truncation error (about 2e-5 of its maximum at this size)."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import SwmOutputDiag
+    from ch_swe_b200.testcases import mesh_geometry, williamson2
+    N, u0, H = 192, 20.0, 1000.0
+    axis = np.array([np.sin(0.7), 0.0, np.cos(0.7)])
+    dom = create_domain(N, precision="fp64", h_mean=H, rotation_axis=tuple(axis))
+    st = create_stvec_swm(dom)
+    st.upload(*williamson2(N, u0=u0, h_mean=H, axis=axis))
+    curl = SwmOutputDiag(dom).curl(st)
+    r, _, _ = mesh_geometry(N, "o")
+    exact = 2 * u0 / dom.planet_radius * (r @ axis)
+    assert np.abs(curl - exact).max() < 1e-4 * np.abs(exact).max()
+    dom.destroy()

@@ -215,3 +215,50 @@ def test_golden_fixtures_regression(oracle_built):
     r = o.rk4(g["h"], g["u"], g["v"], float(g["dt"]), int(g["nsteps"]))
     for a, b in zip(r, (g["h3"], g["u3"], g["v3"])):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("order", [42, 21, 63])
+def test_curl_of_gradient_vanishes(order):
+    """curl_ch_sbp_sat_* of the covariant gradient of a smooth field is zero to
+    rounding: the i2c differences along x and y commute and the SAT terms vanish
+    because both panels hold the same tangential derivative on a shared edge, which
+    pins the exchange's orientation signs."""
+    o = Oracle(20, sbp_order=order)
+    h = o.gaussian(lam0=1.0, phi0=0.4, d0=0.5, amp=1.0)[0]
+    gx, gy = o.grad(h)
+    c = o.curl(gx, gy)
+    scale = max(np.abs(gx).max(), np.abs(gy).max()) / EARTH_RADIUS
+    assert np.abs(c).max() < 1e-11 * scale
+
+
+@pytest.mark.parametrize("order,expect", [(42, 1.8), (21, 1.8), (63, 2.4)])
+def test_curl_solid_body_rotation_converges(order, expect):
+    """The curl of a solid-body rotation about a tilted axis converges to
+    2 u0 / a (r . axis) in the max norm (order 2 with the 4-2 and 2-1 closures, near 3
+    with 6-3)."""
+    ax = np.array([np.sin(0.7), 0.0, np.cos(0.7)])
+    errs = []
+    for N in (16, 32, 64):
+        o = Oracle(N, sbp_order=order)
+        _, u, v = o.ts2(u0=20.0, h_mean=1000.0, axis=ax)
+        z = o.curl(u, v)
+        r = np.stack([o.metric(3, w) for w in (5, 6, 7)])
+        ex = 2 * 20.0 / EARTH_RADIUS * np.tensordot(ax, r, 1)
+        errs.append(np.abs(z - ex).max() / np.abs(ex).max())
+    rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert rates.min() > expect, (errs, rates)
+
+
+def test_energies_consistent_across_orders():
+    """calc_energies of a smooth state agrees between the SBP orders to their
+    truncation error, and PE is g/2 <h, h>."""
+    ax = (0.3, 0.0, 0.95)
+    vals = {}
+    for order in (21, 42, 63):
+        o = Oracle(48, h_mean=3000.0, axis=ax, sbp_order=order)
+        h, u, v = o.ts2(u0=30.0, h_mean=3000.0, axis=ax)
+        vals[order] = np.array(o.energies(h, u, v))
+        assert abs(vals[order][2] - 0.5 * EARTH_GRAV * o.dot(0, h, h)) < 1e-13 * vals[order][2]
+        assert abs(vals[order][0] - vals[order][1] - vals[order][2]) < 1e-13 * vals[order][0]
+    assert np.all(np.abs(vals[42] - vals[63]) < 1e-5 * np.abs(vals[63]))
+    assert np.all(np.abs(vals[21] - vals[63]) < 1e-3 * np.abs(vals[63]))
