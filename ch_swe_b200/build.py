@@ -40,7 +40,9 @@ def up_to_date() -> bool:
 
 def _compile(src: str, verbose: bool, force: bool = False) -> str:
     obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
-    deps = [os.path.join(CSRC, d) for d in [src, *HEADERS]] + [os.path.join(ROOT, "include", "chswe.h")]
+    deps = [os.path.join(CSRC, d) for d in [src, *HEADERS]]
+    if src == "swe_api.cu":   # the only unit that includes the C header
+        deps.append(os.path.join(ROOT, "include", "chswe.h"))
     if not force and os.path.exists(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in deps):
         return obj
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-c",

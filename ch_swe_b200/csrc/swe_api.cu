@@ -223,6 +223,12 @@ struct swe_ctx {
     // FP64 tables of the curl and enstrophy on the o mesh (built on first use): J a
     // (one box), the Coriolis parameter f (one box per panel); then 6 N^2 curl values
     double *otab = nullptr;
+    // lat-lon regrid of h (swe_regrid_latlon), built on first use for a grid size:
+    // ints = per point (panel, x index, y index), then the ECS halo line indices;
+    // reals = per point (wx[4], wy[4]), the ECS halo weights, the extended field, the output
+    int ll_nlat = 0, ll_nlon = 0;
+    int *ll_i = nullptr;
+    double *ll_d = nullptr;
     double *red = nullptr;           // reduction partials
     unsigned char *pinned = nullptr; // pinned host staging for uploads/downloads (whole batch)
     // captured RK4 step
@@ -699,7 +705,7 @@ static void free_ctx(swe_ctx *c)
     if (c->graphk) cudaGraphExecDestroy(c->graphk);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
-    cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab);
+    cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     if (c->pinned) cudaFreeHost(c->pinned);
@@ -1585,6 +1591,196 @@ extern "C" int swe_energies(swe_ctx *c, const swe_stvec *vec, int member, double
     out[1] = ke;
     out[2] = pe;
     out[3] = sum[3];
+    return SWE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lat-lon regrid of h (latlon_outputer_t with the cubic latlon_regrid_t)
+// ---------------------------------------------------------------------------
+// Width of the ECS_xy halo the cubic stencil reads (init_halo_for_interp,
+// regrid_factory_mod.f90:273-276), and the pitch of the extended panel.
+constexpr int LL_HW = 2;
+__host__ __device__ __forceinline__ int ll_pitch(int N) { return N + 1 + 2 * LL_HW; }
+
+// h of the neighbour across side s of panel t, `depth` nodes inside the neighbour,
+// at along index a (1..N+1) of this side: the xy 'full' exchange's halo value at
+// index -depth (L, B) or N+2+depth (R, T).
+template <class T>
+__device__ __forceinline__ double xy_nb(const T *Y, const Dims &d, int t, int s, int depth, int a)
+{
+    const Link L = c_link[t][s];
+    const int ap = L.rev ? d.N + 2 - a : a;
+    int k, l;
+    side_vertex(d.N, L.nside, ap, depth, k, l);
+    return (double)gview(Y, d, 0, L.nb)(k, l);
+}
+
+// get_ecs_halo + ext_ecs_tile_halo on one panel (ecs_halo_xy_mod.f90:66-235), evaluated
+// point by point: the extended panel (indices 1-LL_HW .. N+1+LL_HW) with the averaged
+// duplicated vertices, the corner diagonals and the rows / columns of virtual points
+// interpolated along the neighbours' grid lines (cubic Lagrange, weights wt / lines kt
+// per depth and along index).  FP64 into ext[panel][j][i].
+template <class T>
+__global__ void k_ecs_xy_ext(const T *__restrict__ y, Dims d, const int *__restrict__ kt,
+                             const double *__restrict__ wt, double *__restrict__ ext)
+{
+    const int N = d.N, n = N + 1, E = ll_pitch(N);
+    const int64_t npts = (int64_t)NPAN * E * E;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(q / ((int64_t)E * E)), r = (int)(q % ((int64_t)E * E));
+        const int j = r / E + 1 - LL_HW, i = r % E + 1 - LL_HW;
+        auto X = [&](int s, int depth, int a) { return xy_nb(y, d, t, s, depth, a); };
+        // corner diagonals at offset m (1..LL_HW) from the four corner vertices
+        auto DBL = [&](int m) { return 0.5 * (X(SIDE_L, m, 1) + X(SIDE_B, m, 1)); };
+        auto DBR = [&](int m) { return 0.5 * (X(SIDE_R, m, 1) + X(SIDE_B, m, n)); };
+        auto DTR = [&](int m) { return 0.5 * (X(SIDE_R, m, n) + X(SIDE_T, m, n)); };
+        auto DTL = [&](int m) { return 0.5 * (X(SIDE_T, m, 1) + X(SIDE_L, m, n)); };
+        // the neighbour's grid line at depth m along side s, its ends replaced by the diagonals
+        auto line = [&](int s, int m, int b) {
+            if (b == 1) return s == SIDE_R ? DBR(m) : (s == SIDE_T ? DTL(m) : DBL(m));
+            if (b == n) return s == SIDE_L ? DTL(m) : (s == SIDE_B ? DBR(m) : DTR(m));
+            return X(s, m, b);
+        };
+        auto virt = [&](int s, int m, int a) {
+            const int row = (m - 1) * (n + 2) + a;   // a in 2-m .. n+m-1, i.e. 0 .. n+1
+            const int k = kt[row];
+            const double *w = wt + 4 * row;
+            return w[0] * line(s, m, k - 1) + w[1] * line(s, m, k) + w[2] * line(s, m, k + 1) + w[3] * line(s, m, k + 2);
+        };
+        double v;
+        if (i >= 1 && i <= n && j >= 1 && j <= n) {
+            const double raw = (double)gview(y, d, 0, t)(i, j);
+            const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
+            if (il && jb) v = (raw + X(SIDE_B, 0, 1) + X(SIDE_L, 0, 1)) / 3.0;
+            else if (ir && jb) v = (raw + X(SIDE_B, 0, n) + X(SIDE_R, 0, 1)) / 3.0;
+            else if (ir && jt) v = (raw + X(SIDE_T, 0, n) + X(SIDE_R, 0, n)) / 3.0;
+            else if (il && jt) v = (raw + X(SIDE_L, 0, n) + X(SIDE_T, 0, 1)) / 3.0;
+            else if (jb) v = 0.5 * (raw + X(SIDE_B, 0, i));
+            else if (jt) v = 0.5 * (raw + X(SIDE_T, 0, i));
+            else if (il) v = 0.5 * (raw + X(SIDE_L, 0, j));
+            else if (ir) v = 0.5 * (raw + X(SIDE_R, 0, j));
+            else v = raw;
+        } else if (j < 1 && i >= 2 - (1 - j) && i <= n + (1 - j) - 1) {
+            v = virt(SIDE_B, 1 - j, i);
+        } else if (j > n && i >= 2 - (j - n) && i <= n + (j - n) - 1) {
+            v = virt(SIDE_T, j - n, i);
+        } else if (i < 1 && j >= 2 - (1 - i) && j <= n + (1 - i) - 1) {
+            v = virt(SIDE_L, 1 - i, j);
+        } else if (i > n && j >= 2 - (i - n) && j <= n + (i - n) - 1) {
+            v = virt(SIDE_R, i - n, j);
+        } else if (i < 1) {
+            v = j < 1 ? DBL(1 - i) : DTL(1 - i);
+        } else {
+            v = j < 1 ? DBR(i - n) : DTR(i - n);
+        }
+        ext[q] = v;
+    }
+}
+
+// interp_t%interpolate (latlon_regrid_mod.f90:338-365): the 4 x 4 cubic stencil of
+// every lat-lon point on the extended panel, FP64.
+__global__ void k_latlon(const double *__restrict__ ext, const int *__restrict__ idx, const double *__restrict__ w,
+                         int N, int64_t npts, double *__restrict__ out)
+{
+    const int E = ll_pitch(N);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
+        const int t = idx[3 * q], xi = idx[3 * q + 1], yi = idx[3 * q + 2];
+        const double *wx = w + 8 * q, *wy = wx + 4;
+        const double *e = ext + ((int64_t)t * E + (yi + LL_HW - 1)) * E + (xi + LL_HW - 1);
+        double acc = 0.0;
+        for (int b = -1; b <= 2; b++)
+            for (int a = -1; a <= 2; a++) acc = acc + wx[a + 1] * wy[b + 1] * e[b * E + a];
+        out[q] = acc;
+    }
+}
+
+// Point location and cubic weights (distribute_latlon_points_to_cubsphere,
+// regrid_factory_mod.f90:165-262; init_interpolation, latlon_regrid_mod.f90:286-336;
+// latlon_grid_generator_t%init / get_cartesian_coords) and the ECS_xy halo weights
+// (init_halo_xy_interp, ecs_halo_factory_mod.f90:236-270), built on the host in FP64.
+static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
+{
+    if (c->ll_i && c->ll_nlat == nlat && c->ll_nlon == nlon) return SWE_OK;
+    cudaFree(c->ll_i); cudaFree(c->ll_d);
+    c->ll_i = nullptr; c->ll_d = nullptr; c->ll_nlat = c->ll_nlon = 0;
+    const int N = c->cfg.N, n = N + 1, E = ll_pitch(N);
+    const size_t np = (size_t)nlat * nlon, nrow = (size_t)LL_HW * (n + 2);
+    std::vector<int> hi(3 * np + nrow, 0);
+    std::vector<double> hd(8 * np + 4 * nrow, 0.0);
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = 0.5 * pi / N, a0 = -0.25 * pi;
+    for (int j = 1; j <= nlat; j++) {
+        const double phi = -0.5 * pi + (j - 1) * pi / (nlat - 1.0);
+        for (int i = 1; i <= nlon; i++) {
+            const double lam = (i - 1) * 2.0 * pi / nlon;
+            const double r[3] = {std::cos(phi) * std::cos(lam), std::cos(phi) * std::sin(lam), std::sin(phi)};
+            int t;
+            double alpha, beta;
+            cart_to_native(r, t, alpha, beta);
+            double zdx = (alpha - a0) / hx + 1 - 0.0, zdy = (beta - a0) / hx + 1 - 0.0;
+            const int xi = (int)zdx, yi = (int)zdy;
+            zdx = zdx - xi;
+            zdy = zdy - yi;
+            const size_t q = (size_t)(j - 1) * nlon + (i - 1);
+            hi[3 * q] = t; hi[3 * q + 1] = xi; hi[3 * q + 2] = yi;
+            double *wx = &hd[8 * q], *wy = wx + 4;
+            wx[0] = -zdx * (zdx - 1.0) * (zdx - 2.0) / 6.0;
+            wx[1] = (zdx + 1.0) * (zdx - 1.0) * (zdx - 2.0) / 2.0;
+            wx[2] = -(zdx + 1.0) * zdx * (zdx - 2.0) / 2.0;
+            wx[3] = (zdx + 1.0) * zdx * (zdx - 1.0) / 6.0;
+            wy[0] = -zdy * (zdy - 1.0) * (zdy - 2.0) / 6.0;
+            wy[1] = (zdy + 1.0) * (zdy - 1.0) * (zdy - 2.0) / 2.0;
+            wy[2] = -(zdy + 1.0) * zdy * (zdy - 2.0) / 2.0;
+            wy[3] = (zdy + 1.0) * zdy * (zdy - 1.0) / 6.0;
+            // the stencil (indices xi-1 .. xi+2) stays inside the extended panel
+            if (t < 0 || t >= NPAN || xi < 0 || xi > n || yi < 0 || yi > n)
+                return fail(c, SWE_EINVAL, "lat-lon point (%d, %d) outside the cube panels", i, j);
+        }
+    }
+    for (int m = 1; m <= LL_HW; m++)
+        for (int a = 2 - m; a <= n + m - 1; a++) {
+            const size_t row = (size_t)(m - 1) * (n + 2) + a;
+            halo_xy_weights(n, hx, a, m, &hd[8 * np + 4 * row], hi[3 * np + row]);
+        }
+    const size_t nd = hd.size() + (size_t)NPAN * E * E + np;
+    if (cudaMalloc(&c->ll_i, hi.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->ll_d, nd * sizeof(double)) != cudaSuccess) {
+        cudaFree(c->ll_i); c->ll_i = nullptr; c->ll_d = nullptr;
+        return fail(c, SWE_ENOMEM, "lat-lon regrid allocation failed");
+    }
+    CU(c, cudaMemcpy(c->ll_i, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(c, cudaMemcpy(c->ll_d, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->ll_nlat = nlat;
+    c->ll_nlon = nlon;
+    return SWE_OK;
+}
+
+extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, int field, int nlat, int nlon,
+                                 double *out)
+{
+    if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    if (field != 0) return fail(c, SWE_EINVAL, "lat-lon regrid: only field 0 (h, xy points) is supported");
+    if (nlat < 2 || nlon < 1 || (int64_t)nlat * nlon > (1 << 28))
+        return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
+    int rc = ensure_latlon(c, nlat, nlon);
+    if (rc != SWE_OK) return rc;
+    const int N = c->cfg.N, n = N + 1, E = ll_pitch(N);
+    const int64_t np = (int64_t)nlat * nlon;
+    const size_t nrow = (size_t)LL_HW * (n + 2);
+    const int *kt = c->ll_i + 3 * np;
+    const double *wt = c->ll_d + 8 * np;
+    double *ext = c->ll_d + 8 * np + 4 * nrow, *dout = ext + (size_t)NPAN * E * E;
+    const size_t mo = (size_t)member * c->dims.ms;
+    const int64_t next = (int64_t)NPAN * E * E;
+    const dim3 b(256), g1((unsigned)std::min<int64_t>((next + 255) / 256, 8192)),
+        g2((unsigned)std::min<int64_t>((np + 255) / 256, 8192));
+    if (c->elem == 8) k_ecs_xy_ext<double><<<g1, b, 0, c->stream>>>((const double *)vec->d + mo, c->dims, kt, wt, ext);
+    else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)vec->d + mo, c->dims, kt, wt, ext);
+    k_latlon<<<g2, b, 0, c->stream>>>(ext, c->ll_i, c->ll_d, N, np, dout);
+    c->launches += 2;
+    CU(c, cudaGetLastError());
+    CU(c, cudaMemcpyAsync(out, dout, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
 }
 

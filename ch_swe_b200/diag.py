@@ -1,7 +1,8 @@
 """Diagnostics and output of a shallow-water state: the swm_output_diag_t checks
-(CFL numbers, h extrema, mass) and the paneled single-precision writer
+(CFL numbers, h extrema, mass, energies, enstrophy, curl), the lat-lon outputer of h
+and the paneled single-precision writer
 (src/models/shallow_water/output_and_diag/swm_output_diag_mod.f90,
-src/outputer/master_paneled_outputer_mod.f90)."""
+src/outputer/latlon_outputer_mod.f90, src/outputer/master_paneled_outputer_mod.f90)."""
 from __future__ import annotations
 
 import ctypes
@@ -70,6 +71,43 @@ def state_integrals(domain, state, member: int = 0):
     check(_lib.load().swe_integrals(domain.ctx, state.handle, int(member), ctypes.byref(m), ctypes.byref(e)),
           domain.ctx, "swe_integrals")
     return m.value, e.value
+
+
+class LatlonOutputer:
+    """latlon_outputer_t for h (latlon_outputer_mod.f90:30-53): the cubic regrid on the
+    device (swe_regrid_latlon) onto nlat x nlon points (default 2N+1 x 4N, as
+    create_swm_output_diag sets them) and one real*4 direct-access record per write."""
+
+    def __init__(self, domain, nlat: int | None = None, nlon: int | None = None):
+        self.domain = domain
+        self.nlat = 2 * domain.N + 1 if nlat is None else int(nlat)
+        self.nlon = 4 * domain.N if nlon is None else int(nlon)
+
+    def regrid(self, state, member: int = 0) -> np.ndarray:
+        """h on the lat-lon grid, (nlat, nlon) in FP64, longitude fastest."""
+        out = np.empty((self.nlat, self.nlon))
+        check(_lib.load().swe_regrid_latlon(self.domain.ctx, state.handle, int(member), 0, self.nlat, self.nlon,
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self.domain.ctx, "swe_regrid_latlon")
+        return out
+
+    def write(self, state, path: str, rec: int = 1, member: int = 0) -> np.ndarray:
+        """Record rec (1-based) of `path`: the regridded h as real*4, longitude fastest."""
+        f = self.regrid(state, member)
+        write_latlon(path, f, rec)
+        return f
+
+
+def write_latlon(path: str, field: np.ndarray, rec: int = 1) -> None:
+    """One record of latlon_outputer_t%write: real(f_latlon, 4) with f_latlon(Nlon, Nlat),
+    longitude fastest, record length nlat * nlon values.  field: (nlat, nlon)."""
+    a = np.ascontiguousarray(field, dtype="<f4")
+    if a.ndim != 2:
+        raise ValueError("expected a (nlat, nlon) field")
+    mode = "r+b" if os.path.exists(path) else "wb"
+    with open(path, mode) as f:
+        f.seek((int(rec) - 1) * a.nbytes)
+        f.write(a.tobytes())
 
 
 def write_paneled(path: str, field: np.ndarray, rec: int = 1) -> None:

@@ -149,6 +149,16 @@ int swe_energies(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
    curl_sbp_sat_mod.f90:27-76): out[6][N][N] in FP64, i fastest.  Synchronous. */
 int swe_curl(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
 
+/* Cubic lat-lon regrid of h (field 0, xy points) of one member, the values that
+   latlon_outputer_t%write puts in a record (latlon_outputer_mod.f90:30-53,
+   latlon_regrid_mod.f90:75-365, regrid_factory_mod.f90:25-70,165-276): h gets an
+   ECS_xy halo of width 2, the points phi_j = -pi/2 + (j-1) pi / (nlat-1),
+   lam_i = (i-1) 2 pi / nlon are located on their panels and the 4 x 4 cubic Lagrange
+   stencil is summed.  out[nlat][nlon] in FP64, longitude fastest (the reference's
+   outputer uses nlat = 2N+1, nlon = 4N).  Other fields give SWE_EINVAL.  Synchronous. */
+int swe_regrid_latlon(swe_ctx *ctx, const swe_stvec *vec, int member, int field, int nlat, int nlon,
+                      double *out);
+
 /* Number of kernel launches issued on the context's stream since creation. */
 long long swe_launch_count(const swe_ctx *ctx);
 

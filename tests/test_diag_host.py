@@ -36,3 +36,18 @@ def test_oracle_diag_known_answers(oracle_built):
     h, u, v = o.ts2(u0=u0, h_mean=1000.0, axis=axis, linear_mode=True)
     _, _, _, cx, cy = o.diag(h, u, v, dt)
     assert 0.5 * u0 * dt / dx < max(cx, cy) < 2.0 * u0 * dt / dx
+
+
+def test_write_latlon_records(tmp_path):
+    """write_latlon: record rec holds the real*4 field, longitude fastest, and earlier
+    records are kept."""
+    from ch_swe_b200.diag import write_latlon
+    path = str(tmp_path / "h.dat")
+    a = np.arange(5 * 8, dtype=np.float64).reshape(5, 8) * 0.5
+    b = -a
+    write_latlon(path, a, rec=1)
+    write_latlon(path, b, rec=3)
+    raw = np.fromfile(path, dtype="<f4").reshape(-1, 5, 8)
+    assert raw.shape[0] == 3
+    np.testing.assert_array_equal(raw[0], a.astype("<f4"))
+    np.testing.assert_array_equal(raw[2], b.astype("<f4"))

@@ -114,3 +114,58 @@ def test_curl_solid_body_rotation_large_cube():
     exact = 2 * u0 / dom.planet_radius * (r @ axis)
     assert np.abs(curl - exact).max() < 1e-4 * np.abs(exact).max()
     dom.destroy()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("grid", [None, (37, 50)])
+def test_latlon_regrid_matches_oracle(precision, tol, grid):
+    """swe_regrid_latlon of h against the oracle's latlon_regrid_t (ECS_xy halo of width 2,
+    cubic stencil), for a state whose duplicated panel-edge copies disagree (the halo
+    averages them), on the outputer's default 2N+1 x 4N grid and on another one."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import LatlonOutputer
+    from oracle.oracle import Oracle
+    N = 24
+    o = Oracle(N)
+    rng = np.random.default_rng(11)
+    h = o.gaussian(lam0=1.0, phi0=0.4, d0=0.5, amp=100.0)[0] + rng.standard_normal((6, N + 1, N + 1))
+    _, u, v = o.zeros()
+    nlat, nlon = grid if grid else (None, None)
+    ref = o.latlon(h, nlat, nlon)
+    dom = create_domain(N, precision=precision, n_members=2)
+    st = create_stvec_swm(dom)
+    st.upload(h, u, v, member=1)
+    st.upload(h * 0, u, v, member=0)
+    out = LatlonOutputer(dom, nlat, nlon)
+    got = out.regrid(st, member=1)
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
+    assert np.abs(out.regrid(st, member=0)).max() == 0.0
+    dom.destroy()
+
+
+def test_latlon_regrid_large_cube_converges(tmp_path):
+    """At C192: the regridded Gaussian hill matches the analytic field to the cubic
+    interpolation error, and the record written is its real*4 image."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import LatlonOutputer
+    from ch_swe_b200.testcases import gaussian_hill
+    N = 192
+    dom = create_domain(N, precision="fp64")
+    st = create_stvec_swm(dom)
+    st.upload(*gaussian_hill(N, lam0=1.0, phi0=0.4, d0=0.5, amp=1.0))
+    out = LatlonOutputer(dom)
+    path = str(tmp_path / "h.dat")
+    f = out.write(st, path, rec=2)
+    nlat, nlon = f.shape
+    phi = -np.pi / 2 + np.arange(nlat) * np.pi / (nlat - 1)
+    lam = np.arange(nlon) * 2 * np.pi / nlon
+    P, L = np.meshgrid(phi, lam, indexing="ij")
+    c0 = (np.cos(0.4) * np.cos(1.0), np.cos(0.4) * np.sin(1.0), np.sin(0.4))
+    d = np.clip(np.cos(P) * np.cos(L) * c0[0] + np.cos(P) * np.sin(L) * c0[1] + np.sin(P) * c0[2], -1, 1)
+    exact = np.exp(-(np.arccos(d) / 0.5) ** 2)
+    assert np.abs(f - exact).max() < 1e-7
+    raw = np.fromfile(path, dtype="<f4")
+    assert raw.size == 2 * nlat * nlon
+    np.testing.assert_array_equal(raw[nlat * nlon:].reshape(nlat, nlon), f.astype("<f4"))
+    dom.destroy()

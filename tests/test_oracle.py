@@ -262,3 +262,23 @@ def test_energies_consistent_across_orders():
         assert abs(vals[order][0] - vals[order][1] - vals[order][2]) < 1e-13 * vals[order][0]
     assert np.all(np.abs(vals[42] - vals[63]) < 1e-5 * np.abs(vals[63]))
     assert np.all(np.abs(vals[21] - vals[63]) < 1e-3 * np.abs(vals[63]))
+
+
+def test_latlon_regrid_converges():
+    """The oracle's cubic lat-lon regrid of a smooth xy field (through the ECS_xy halo of
+    width 2) converges at fourth order and reads no unfilled halo value."""
+    errs = []
+    for N in (16, 32, 64):
+        o = Oracle(N)
+        h = o.gaussian(lam0=1.0, phi0=0.4, d0=0.5, amp=1.0)[0]
+        ll = o.latlon(h)
+        nlat, nlon = ll.shape
+        assert (nlat, nlon) == (2 * N + 1, 4 * N) and not np.isnan(ll).any()
+        phi = -np.pi / 2 + np.arange(nlat) * np.pi / (nlat - 1)
+        lam = np.arange(nlon) * 2 * np.pi / nlon
+        P, L = np.meshgrid(phi, lam, indexing="ij")
+        c0 = (np.cos(0.4) * np.cos(1.0), np.cos(0.4) * np.sin(1.0), np.sin(0.4))
+        d = np.clip(np.cos(P) * np.cos(L) * c0[0] + np.cos(P) * np.sin(L) * c0[1] + np.sin(P) * c0[2], -1, 1)
+        errs.append(np.abs(ll - np.exp(-(np.arccos(d) / 0.5) ** 2)).max())
+    rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert rates.min() > 3.5, (errs, rates)
