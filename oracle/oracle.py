@@ -67,6 +67,9 @@ def lib():
         L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_curl.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
         L.orc_energies.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+        L.orc_ah_apply.argtypes = [ctypes.c_void_p] + [_dp] * 6
+        L.orc_ah_rk4.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int]
+        L.orc_ah_integrals.argtypes = [ctypes.c_void_p] + [_dp] * 5
         L.orc_latlon_xy.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
         _lib = L
     return _lib
@@ -129,6 +132,25 @@ class Oracle:
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v)]
         lib().orc_curl(self._c, _p(a[0]), _p(a[1]), _p(out))
         return out
+
+    # Ah staggering (linear operator, SBP 4-2): h, u, v all (6, N+1, N+1) on the xy mesh
+    def ah_apply(self, h, u, v):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        out = [np.zeros_like(a[0]) for _ in range(3)]
+        lib().orc_ah_apply(self._c, *(_p(x) for x in a), *(_p(x) for x in out))
+        return tuple(out)
+
+    def ah_rk4(self, h, u, v, dt: float, nsteps: int):
+        a = [np.array(x, dtype=np.float64, order="C") for x in (h, u, v)]
+        lib().orc_ah_rk4(self._c, *(_p(x) for x in a), float(dt), int(nsteps))
+        return tuple(a)
+
+    def ah_integrals(self, h, u, v):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        m = ctypes.c_double()
+        e = ctypes.c_double()
+        lib().orc_ah_integrals(self._c, *(_p(x) for x in a), ctypes.byref(m), ctypes.byref(e))
+        return m.value, e.value
 
     def latlon(self, f, nlat=None, nlon=None):
         """Cubic lat-lon regrid of an xy field (latlon_outputer_t, default grid 2N+1 x 4N):

@@ -848,6 +848,10 @@ typedef struct orc_ctx {
     mesh_t mo;
     double *fo;                  /* Coriolis parameter on o, [t][j][i] */
     fld_t oDx, oDy, curl, hqu, hqv, ehu, ehv;
+    /* Ah staggering (h, u, v all on xy): state, work fields and RK4 stages */
+    int ah;
+    double *fxy;                 /* Coriolis parameter on xy, [t][j][i] */
+    fld_t ah_u, ah_v, ah_du, ah_dv, ah_gx, ah_gy, ah_ut, ah_vt, ah_Ju, ah_Jv, ah_y[3], ah_k[4][3];
 } orc_ctx;
 
 /* calc_coriolis_parameter (coriolis_factory_mod.f90:239-280) at point k of mesh m */
@@ -873,6 +877,8 @@ static void coriolis_parameter(orc_ctx *c)
     const size_t no = (size_t)NPAN * o->nx * o->ny;
     c->fo = malloc(sizeof(double) * no);
     for (size_t k = 0; k < no; k++) c->fo[k] = coriolis_f(c, o, k);
+    c->fxy = malloc(sizeof(double) * n);
+    for (size_t k = 0; k < n; k++) c->fxy[k] = coriolis_f(c, m, k);
 }
 
 static void sync_weights(orc_ctx *c)
@@ -947,6 +953,11 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     for (unsigned q = 0; q < sizeof(oo) / sizeof(oo[0]); q++) fld_init(oo[q], N, N, hw);
     fld_init(&c->ehu, N, N + 1, hw);
     fld_init(&c->ehv, N + 1, N, hw);
+    fld_t *ah[] = {&c->ah_u, &c->ah_v, &c->ah_du, &c->ah_dv, &c->ah_gx, &c->ah_gy, &c->ah_ut, &c->ah_vt,
+                   &c->ah_Ju, &c->ah_Jv, &c->ah_y[0], &c->ah_y[1], &c->ah_y[2]};
+    for (unsigned q = 0; q < sizeof(ah) / sizeof(ah[0]); q++) fld_init(ah[q], N + 1, N + 1, hw);
+    for (int s = 0; s < 4; s++)
+        for (int f = 0; f < 3; f++) fld_init(&c->ah_k[s][f], N + 1, N + 1, hw);
     return c;
 }
 
@@ -954,14 +965,16 @@ void orc_destroy(orc_ctx *c)
 {
     if (!c) return;
     mesh_free(&c->mxy); mesh_free(&c->mx); mesh_free(&c->my); mesh_free(&c->mo);
-    free(c->fJ2); free(c->fo); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
+    free(c->fJ2); free(c->fo); free(c->fxy); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
                     &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
                     &c->vh, &c->vau, &c->uav, &c->uhal, &c->vhal, &c->oDx, &c->oDy, &c->curl,
-                    &c->hqu, &c->hqv, &c->ehu, &c->ehv};
+                    &c->hqu, &c->hqv, &c->ehu, &c->ehv, &c->ah_u, &c->ah_v, &c->ah_du, &c->ah_dv,
+                    &c->ah_gx, &c->ah_gy, &c->ah_ut, &c->ah_vt, &c->ah_Ju, &c->ah_Jv,
+                    &c->ah_y[0], &c->ah_y[1], &c->ah_y[2]};
     for (unsigned q = 0; q < sizeof(all) / sizeof(all[0]); q++) fld_free(all[q]);
-    for (int s = 0; s < 4; s++) for (int f = 0; f < 3; f++) fld_free(&c->k[s][f]);
+    for (int s = 0; s < 4; s++) for (int f = 0; f < 3; f++) { fld_free(&c->k[s][f]); fld_free(&c->ah_k[s][f]); }
     free(c);
 }
 
@@ -1541,6 +1554,114 @@ static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_
     else op_apply_lin(c, dh, du, dv, h, u, v);
 }
 
+/* ---- Ah staggering: the linear operator of gen_config_linear.sh:9-36 (div_ah_sbp_proj_*,
+   grad_ah_sbp_proj_*, coriolis_colocated, co2contra_colocated), h, u, v on the xy mesh ---- */
+
+/* node-to-node SBP first derivative along dir of a line of n nodes (no halo, one-sided
+   closures): sbp_diff_21_mod.f90, sbp_diff_42_mod.f90:30-156 (the reference's decimal
+   coefficients), sbp_diff_63_mod.f90 */
+static const double N42_Q[4][6] = {{-1.4117647058823528, 1.7352941176470589, -0.2352941176470588, -0.08823529411764705, 0, 0},
+                                   {-0.5, 0, 0.5, 0, 0, 0},
+                                   {0.09302325581395347, -0.686046511627907, 0, 0.686046511627907, -0.09302325581395347, 0},
+                                   {0.030612244897959186, 0, -0.6020408163265307, 0, 0.653061224489796, -0.0816326530612245}};
+static void diff_n2n(fld_t *out, const fld_t *in, int t, int dir, int n, int ls, int le, int ord)
+{
+#define O(k) (*((dir) == 0 ? &FA(out, t, k, l) : &FA(out, t, l, k)))
+#define I(k) L(in, t, dir, k, l)
+    (void)ord;
+    for (int l = ls; l <= le; l++) {
+        for (int r = 1; r <= 4; r++) {
+            double a = 0.0, b = 0.0;
+            for (int q = 0; q < 6; q++) {
+                if (N42_Q[r - 1][q] == 0.0) continue;
+                a = a + N42_Q[r - 1][q] * I(q + 1);
+                b = b - N42_Q[r - 1][q] * I(n + 1 - (q + 1));
+            }
+            O(r) = a;
+            O(n + 1 - r) = b;
+        }
+        for (int k = 5; k <= n - 4; k++) O(k) = (I(k - 2) + -8 * I(k - 1) + 8 * I(k + 1) + -I(k + 2)) / 12.0;
+    }
+#undef O
+#undef I
+}
+
+/* grad_sbp_proj_t%calc_grad (grad_sbp_proj_mod.f90:26-72) with the covariant
+   ecs_Ah_vec_sync (ecs_Ah_vec_sync_mod.f90:34-60: syncronize_grad_on_edges(gy, gx)) */
+static void op_grad_ah(orc_ctx *c, fld_t *gx, fld_t *gy, fld_t *h)
+{
+    int N = c->N, n = N + 1;
+    const mesh_t *m = &c->mxy;
+    for (int t = 0; t < NPAN; t++) {
+        diff_n2n(gx, h, t, 0, n, 1, n, c->ord);
+        diff_n2n(gy, h, t, 1, n, 1, n, c->ord);
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                FA(gx, t, i, j) = FA(gx, t, i, j) / (m->hx * c->a);
+                FA(gy, t, i, j) = FA(gy, t, i, j) / (m->hy * c->a);
+            }
+    }
+    exch_do(&c->ex_xy1_cross_v, gx, gy);
+    for (int t = 0; t < NPAN; t++) sync_grad_on_edges(c, gy, gx, t);
+}
+
+/* div_sbp_proj_t%calc_div (div_sbp_proj_mod.f90:25-76) with the Ah scalar sync */
+static void op_div_ah(orc_ctx *c, fld_t *div, fld_t *ut, fld_t *vt)
+{
+    int N = c->N, n = N + 1;
+    const mesh_t *m = &c->mxy;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const double J = m->J[MI(m, t, i, j)];
+                FA(&c->ah_Ju, t, i, j) = FA(ut, t, i, j) * J;
+                FA(&c->ah_Jv, t, i, j) = FA(vt, t, i, j) * J;
+            }
+    for (int t = 0; t < NPAN; t++) {
+        diff_n2n(&c->Dx, &c->ah_Ju, t, 0, n, 1, n, c->ord);
+        diff_n2n(&c->Dy, &c->ah_Jv, t, 1, n, 1, n, c->ord);
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++)
+                FA(div, t, i, j) = (FA(&c->Dx, t, i, j) / m->hx + FA(&c->Dy, t, i, j) / m->hy) /
+                                   (m->J[MI(m, t, i, j)] * c->a);
+    }
+    exch_do(&c->ex_xy1_full_s, div, NULL);
+    for (int t = 0; t < NPAN; t++) sync_ah_scalar(c, div, t);
+}
+
+/* operator_swm_lin_t%apply (operator_swm_lin_mod.f90:66-108) with the Ah operators:
+   co2contra_colocated (co2contra_colocated_mod.f90:17-47: ut = Qi11 u + Qi12 v,
+   vt = Qi12 u + Qi22 v) and coriolis_colocated (coriolis_colocated_mod.f90:17-45:
+   cor_u = f vt J, cor_v = -f ut J) */
+static void op_apply_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
+{
+    int n = c->N + 1;
+    const mesh_t *m = &c->mxy;
+    op_grad_ah(c, &c->ah_gx, &c->ah_gy, h);
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                FA(du, t, i, j) = -c->g * FA(&c->ah_gx, t, i, j);
+                FA(dv, t, i, j) = -c->g * FA(&c->ah_gy, t, i, j);
+                FA(&c->ah_ut, t, i, j) = m->Q1[k] * FA(u, t, i, j) + m->Q2[k] * FA(v, t, i, j);
+                FA(&c->ah_vt, t, i, j) = m->Q2[k] * FA(u, t, i, j) + m->Q3[k] * FA(v, t, i, j);
+            }
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                const double cu = c->fxy[k] * FA(&c->ah_vt, t, i, j) * m->J[k];
+                const double cv = -c->fxy[k] * FA(&c->ah_ut, t, i, j) * m->J[k];
+                FA(du, t, i, j) = FA(du, t, i, j) + 1.0 * cu;
+                FA(dv, t, i, j) = FA(dv, t, i, j) + 1.0 * cv;
+            }
+    op_div_ah(c, &c->div, &c->ah_ut, &c->ah_vt);
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) FA(dh, t, i, j) = -c->H * FA(&c->div, t, i, j);
+}
+
 /* stvec assign/update over interior points (grid_field_mod.f90:442-534) */
 static void st_assign2(fld_t *y[3], double s1, fld_t *a[3], double s2, fld_t *b[3])
 {
@@ -1557,6 +1678,25 @@ static void st_update2(fld_t *y[3], double s1, fld_t *a[3], double s2, fld_t *b[
             for (int j = 1; j <= y[f]->ny; j++)
                 for (int i = 1; i <= y[f]->nx; i++)
                     FA(y[f], t, i, j) = FA(y[f], t, i, j) + s1 * FA(a[f], t, i, j) + s2 * FA(b[f], t, i, j);
+}
+
+/* rk4_t%step (rk4_mod.f90:20-42) for the Ah state */
+static void rk4_step_ah(orc_ctx *c, double dt)
+{
+    fld_t *v0[3] = {&c->h, &c->ah_u, &c->ah_v};
+    fld_t *y[3] = {&c->ah_y[0], &c->ah_y[1], &c->ah_y[2]};
+    fld_t *k[4][3];
+    for (int s = 0; s < 4; s++)
+        for (int f = 0; f < 3; f++) k[s][f] = &c->ah_k[s][f];
+    op_apply_ah(c, k[0][0], k[0][1], k[0][2], v0[0], v0[1], v0[2]);
+    st_assign2(y, 1.0, v0, 0.5 * dt, k[0]);
+    op_apply_ah(c, k[1][0], k[1][1], k[1][2], y[0], y[1], y[2]);
+    st_assign2(y, 1.0, v0, 0.5 * dt, k[1]);
+    op_apply_ah(c, k[2][0], k[2][1], k[2][2], y[0], y[1], y[2]);
+    st_assign2(y, 1.0, v0, dt, k[2]);
+    op_apply_ah(c, k[3][0], k[3][1], k[3][2], y[0], y[1], y[2]);
+    st_update2(v0, dt / 6.0, k[0], dt / 3.0, k[1]);
+    st_update2(v0, dt / 3.0, k[2], dt / 6.0, k[3]);
 }
 
 /* rk4_t%step (rk4_mod.f90:20-42) */
@@ -1831,6 +1971,47 @@ void orc_latlon_xy(orc_ctx *c, const double *f, int nlat, int nlon, double *out)
             out[(size_t)(j - 1) * nlon + (i - 1)] = acc;
         }
     }
+}
+
+/* Ah staggering: the linear operator's tendency and RK4 steps of a state with h, u, v
+   all on the xy mesh (each packed [t][j][i], (N+1) x (N+1) per panel) */
+void orc_ah_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv)
+{
+    fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
+    op_apply_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v);
+    fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
+}
+void orc_ah_rk4(orc_ctx *c, double *h, double *u, double *v, double dt, int nsteps)
+{
+    fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
+    for (int s = 0; s < nsteps; s++) rk4_step_ah(c, dt);
+    fld_to_packed(&c->h, h); fld_to_packed(&c->ah_u, u); fld_to_packed(&c->ah_v, v);
+}
+/* mass <h,1> and linear energy H/2 (<u,ut> + <v,vt>) + g/2 <h,h> in the SBP_Ah quadrature
+   (quadrature_factory_mod.f90:31-66: the node norm in both directions) */
+void orc_ah_integrals(orc_ctx *c, const double *h, const double *u, const double *v, double *mass, double *energy)
+{
+    fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
+    const int n = c->N + 1;
+    const mesh_t *m = &c->mxy;
+    const double A42[4] = {17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0};
+    double *A = malloc(sizeof(double) * n);
+    mass_coeffs(A, n, A42, 4);
+    double sm = 0.0, se = 0.0, sh = 0.0;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                const double w = m->J[k] * m->hx * m->hy * A[i - 1] * A[j - 1];
+                const double uu = FA(&c->ah_u, t, i, j), vv = FA(&c->ah_v, t, i, j), hh = FA(&c->h, t, i, j);
+                const double ut = m->Q1[k] * uu + m->Q2[k] * vv, vt = m->Q2[k] * uu + m->Q3[k] * vv;
+                sm += hh * w;
+                sh += hh * hh * w;
+                se += (uu * ut + vv * vt) * w;
+            }
+    free(A);
+    if (mass) *mass = sm;
+    if (energy) *energy = 0.5 * c->H * se + 0.5 * c->g * sh;
 }
 
 /* curl of the covariant (u, v) on mesh o (N x N per panel, packed [t][j][i]) */
