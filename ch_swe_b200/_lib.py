@@ -16,6 +16,8 @@ SWE_FP64 = 0
 SWE_FP32 = 1
 SWE_OP_LINEAR = 0
 SWE_OP_ADVECTIVE = 1
+SWE_STAG_CH = 0
+SWE_STAG_AH = 1
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "no CUDA device",
           -5: "cube size above SWE_NOALLOC_MAX_N"}
@@ -47,6 +49,7 @@ class SweCfg(ctypes.Structure):
         ("coriolis_constant", ctypes.c_int),
         ("h_mean", ctypes.c_double),
         ("sbp_order", ctypes.c_int),
+        ("staggering", ctypes.c_int),
     ]
 
 

@@ -17,8 +17,10 @@ OBJDIR = os.path.join(HERE, "_build")
 # device modules, compiled in parallel
 STAGE_SOURCES = [f"stage_{p}{tm}.cu" for p in ("f", "d") for tm in (17, 25, 33)]
 SOURCES = ["swe_api.cu", *STAGE_SOURCES]
-HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_tiled.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh",
-           "swe_launch.cuh", "swe_stage_tu.cuh"]
+COMMON_HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh", "swe_launch.cuh"]
+UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh"]}
+STAGE_HEADERS = COMMON_HEADERS + ["swe_tiled.cuh", "swe_stage_tu.cuh"]
+HEADERS = sorted(set(COMMON_HEADERS + UNIT_HEADERS["swe_api.cu"] + STAGE_HEADERS))
 DEPS = SOURCES + HEADERS
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -40,7 +42,7 @@ def up_to_date() -> bool:
 
 def _compile(src: str, verbose: bool, force: bool = False) -> str:
     obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
-    deps = [os.path.join(CSRC, d) for d in [src, *HEADERS]]
+    deps = [os.path.join(CSRC, d) for d in [src, *UNIT_HEADERS.get(src, STAGE_HEADERS)]]
     if src == "swe_api.cu":   # the only unit that includes the C header
         deps.append(os.path.join(ROOT, "include", "chswe.h"))
     if not force and os.path.exists(obj) and all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in deps):

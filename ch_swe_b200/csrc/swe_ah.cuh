@@ -1,0 +1,213 @@
+// swe_ah.cuh -- the linear shallow-water operator on the Ah staggering: h, u and v
+// all on the cell vertices (the xy mesh), the operator set of the reference's Ah
+// configuration (gen_config_linear.sh:9-36):
+//   grad_ah_sbp_proj_42     node-to-node SBP 4-2 differences (sbp_diff_42_mod.f90:30-156)
+//                           and the covariant ECS Ah vector sync of the panel-edge
+//                           vertices (grad_sbp_proj_mod.f90:26-72, ecs_Ah_vec_sync_mod.f90:34-125)
+//   co2contra_colocated     ut = Qi11 u + Qi12 v, vt = Qi12 u + Qi22 v at each vertex
+//                           (co2contra_colocated_mod.f90:17-47)
+//   coriolis_colocated      cor_u = f vt J, cor_v = -f ut J (coriolis_colocated_mod.f90:17-45)
+//   div_ah_sbp_proj_42      the same differences of J ut, J vt over J a and the Ah scalar
+//                           sync (div_sbp_proj_mod.f90:25-76, halo_Ah_scalar_sync_mod.f90:43-98)
+// then du = -g grad_x h + cor_u, dv = -g grad_y h + cor_v, dh = -H div
+// (operator_swm_lin_mod.f90:66-108) and the RK4 stage update.
+// Per RK stage two launches: k_ah_edge (the raw gradient and divergence of every
+// panel-boundary vertex, for its neighbours' syncs) and k_ah_stage (every vertex:
+// raw values, the syncs on the panel edges, the tendency and the RK update).
+#pragma once
+
+#include "swe_kernels.cuh"
+
+namespace chswe {
+
+// Metric of the Ah operator at the vertices (host FP64, stored in T).
+template <class T>
+struct AhView {
+    const T *J;            // J (one panel-independent box)
+    const T *Q1, *Q2, *Q3; // the inverse metric Qi11, Qi12, Qi22 (boxes)
+    const T *fJ;           // f J, one box per panel
+};
+
+namespace sbp {
+// sbp_diff_42_mod.f90:10-23: the reference's decimal coefficients of the node-to-node
+// SBP 4-2 first derivative's closure rows
+constexpr double N11 = -1.4117647058823528, N12 = 1.7352941176470589, N13 = -0.2352941176470588,
+                 N14 = -0.08823529411764705, N21 = -0.5, N23 = 0.5, N31 = 0.09302325581395347,
+                 N32 = -0.686046511627907, N34 = 0.686046511627907, N35 = -0.09302325581395347,
+                 N41 = 0.030612244897959186, N43 = -0.6020408163265307, N45 = 0.653061224489796,
+                 N46 = -0.0816326530612245;
+}  // namespace sbp
+
+// SBP 4-2 first derivative at node k of n nodes (inputs f(1..n), no halo).
+template <class T, class F>
+__device__ __forceinline__ T dn2n42(int k, int n, const F &f)
+{
+    using namespace sbp;
+    if (k >= 5 && k <= n - 4) return (f(k - 2) + T(-8) * f(k - 1) + T(8) * f(k + 1) + -f(k + 2)) / T(12);
+    if (k == 1) return T(N11) * f(1) + T(N12) * f(2) + T(N13) * f(3) + T(N14) * f(4);
+    if (k == 2) return T(N21) * f(1) + T(N23) * f(3);
+    if (k == 3) return T(N31) * f(1) + T(N32) * f(2) + T(N34) * f(4) + T(N35) * f(5);
+    if (k == 4) return T(N41) * f(1) + T(N43) * f(3) + T(N45) * f(5) + T(N46) * f(6);
+    if (k == n - 3) return -T(N41) * f(n) - T(N43) * f(n - 2) - T(N45) * f(n - 4) - T(N46) * f(n - 5);
+    if (k == n - 2) return -T(N31) * f(n) - T(N32) * f(n - 1) - T(N34) * f(n - 3) - T(N35) * f(n - 4);
+    if (k == n - 1) return -T(N21) * f(n) - T(N23) * f(n - 2);
+    return -T(N11) * f(n) - T(N12) * f(n - 1) - T(N13) * f(n - 2) - T(N14) * f(n - 3);
+}
+
+// Raw (before the panel-edge syncs) gradient (gx, gy) and divergence of the
+// contravariant wind at vertex (i, j) of panel t; y is the member's state.
+template <class T>
+__device__ __forceinline__ void ah_raw(const T *y, const Dims &d, const AhView<T> &a, const MetricView<T> &m, int t,
+                                       int i, int j, T &gx, T &gy, T &dv)
+{
+    const int n = d.N + 1;
+    const GV<T> H = gview(y, d, 0, t), U = gview(y, d, 1, t), V = gview(y, d, 2, t);
+    const GV<T> J = mview(a.J, d), Q1 = mview(a.Q1, d), Q2 = mview(a.Q2, d), Q3 = mview(a.Q3, d);
+    gx = dn2n42<T>(i, n, [&](int k) { return H(k, j); }) * m.inv_hxa;
+    gy = dn2n42<T>(j, n, [&](int k) { return H(i, k); }) * m.inv_hxa;
+    const T dx = dn2n42<T>(i, n, [&](int k) { return J(k, j) * (Q1(k, j) * U(k, j) + Q2(k, j) * V(k, j)); });
+    const T dy = dn2n42<T>(j, n, [&](int k) { return J(i, k) * (Q2(i, k) * U(i, k) + Q3(i, k) * V(i, k)); });
+    dv = (dx * m.inv_hx + dy * m.inv_hx) * mview(m.iJa, d)(i, j);
+}
+
+// k_ah_edge: the raw (gx, gy, div) of every panel-boundary vertex into the edge
+// buffer (edge_index: member, panel, side, along index).  Grid (along chunks,
+// panel * 4 + side, member).
+template <class T>
+__global__ void __launch_bounds__(128) k_ah_edge(const T *__restrict__ Y, T *__restrict__ E, Dims d, AhView<T> a,
+                                                 MetricView<T> m, const double *__restrict__ dtm)
+{
+    const int N = d.N, n = N + 1;
+    const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
+    if (member_frozen(dtm, mem)) return;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    pdl_trigger();
+    pdl_wait();
+    if (b > n) return;
+    int i, j;
+    side_vertex(N, s, b, 0, i, j);
+    T gx, gy, dv;
+    ah_raw(Y + mem * d.ms, d, a, m, t, i, j, gx, gy, dv);
+    T *e = E + edge_index(N, mem, t, s, b);
+    e[0] = gx;
+    e[1] = gy;
+    e[2] = dv;
+}
+
+// k_ah_stage: every vertex of every panel and member.  The raw values, on the panel
+// edges the syncs with the neighbours' raw values from k_ah_edge (the neighbour's
+// vector is handed over as the 'cross' exchange does, halo_vec), the tendency and
+// the RK update of k_stage (modes 0..4; FP32 mode 4 Kahan-compensated).
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, const T *__restrict__ E, T *V0, T *Y1,
+                                                  T *ACC, T *CMP, Dims d, AhView<T> a, MetricView<T> m, StageArgs sa,
+                                                  T grav)
+{
+    const int N = d.N, n = N + 1;
+    const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
+    if (member_frozen(sa.dtm, mem)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    pdl_trigger();
+    pdl_wait();
+    if (i > n || j > n) return;
+    const T *y = Yin + mem * d.ms;
+    T gx, gy, dv;
+    ah_raw(y, d, a, m, t, i, j, gx, gy, dv);
+    const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
+    const bool cx = il || ir, cy = jb || jt;
+    if (cx || cy) {
+        T uhx = 0, vhx = 0, dvx = 0, uhy = 0, vhy = 0, dvy = 0, qx = 0, qy = 0;
+        if (cx) {
+            const int s = il ? SIDE_L : SIDE_R;
+            const Link L = c_link[t][s];
+            const T *e = E + edge_index(N, mem, L.nb, L.nside, nb_along(L, n, j));
+            halo_vec(t, s, e[0], e[1], uhx, vhx);
+            dvx = e[2];
+            qx = (il ? m.ql : m.qr)[j - 1];
+        }
+        if (cy) {
+            const int s = jb ? SIDE_B : SIDE_T;
+            const Link L = c_link[t][s];
+            const T *e = E + edge_index(N, mem, L.nb, L.nside, nb_along(L, n, i));
+            halo_vec(t, s, e[0], e[1], uhy, vhy);
+            dvy = e[2];
+            qy = (jb ? m.qb : m.qt)[i - 1];
+        }
+        // syncronize_grad_on_edges(gy, gx) and sync_Ah_scalar_tile
+        if (cx && cy) {
+            const T sx = (gx + uhx + uhy + qx * vhx) / T(3);
+            gy = (gy + vhx + vhy + qy * uhy) / T(3);
+            gx = sx;
+            dv = (dv + dvx + dvy) / T(3);
+        } else if (cx) {
+            gx = T(0.5) * (gx + uhx + qx * vhx);
+            gy = T(0.5) * (gy + vhx);
+            dv = T(0.5) * (dv + dvx);
+        } else {
+            gx = T(0.5) * (gx + uhy);
+            gy = T(0.5) * (gy + vhy + qy * uhy);
+            dv = T(0.5) * (dv + dvy);
+        }
+    }
+    const int64_t o = box_off(d.P, i, j);
+    const T u = y[t * d.ps + d.fs + o], v = y[t * d.ps + 2 * d.fs + o];
+    const T ut = a.Q1[o] * u + a.Q2[o] * v, vt = a.Q2[o] * u + a.Q3[o] * v;
+    const T fJ = a.fJ[t * d.ps + o];
+    const T k3[3] = {-T(sa.Hm[mem]) * dv, -grav * gx + fJ * vt, -grav * gy - fJ * ut};
+    const int64_t po = mem * d.ms + t * d.ps + o;
+    const T dt = T(sa.dtm ? sa.dtm[mem] : sa.dt);
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        const int64_t of = po + f * d.fs;
+        if constexpr (MODE == 0) {
+            Y1[of] = k3[f];
+        } else if constexpr (MODE <= 3) {
+            const T ca = (MODE == 3) ? dt : T(0.5) * dt;
+            const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
+            Y1[of] = V0[of] + ca * k3[f];
+            ACC[of] = (MODE == 1) ? cb * k3[f] : ACC[of] + cb * k3[f];
+        } else if constexpr (sizeof(T) == 4) {
+            float sv = V0[of], cv = CMP[of];
+            kahan_add(sv, cv, ACC[of] + (dt / T(6)) * k3[f]);
+            V0[of] = sv;
+            CMP[of] = cv;
+        } else {
+            V0[of] = V0[of] + (ACC[of] + (dt / T(6)) * k3[f]);
+        }
+    }
+}
+
+// FP64 sums of the Ah integrals per block: term 0 <h, 1>, 1 <h, h>, 2 <u, ut> + <v, vt>
+// with the SBP_Ah quadrature weights qa (J hx hy Ax Ay at the vertices).
+template <class T>
+__global__ void k_quad_ah(const T *__restrict__ y, const double *__restrict__ qa, AhView<T> a, Dims d,
+                          double *partial)
+{
+    const int term = blockIdx.y;
+    const int n = d.N + 1;
+    const int64_t npts = (int64_t)NPAN * n * n;
+    double acc = 0.0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npts; k += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(k / ((int64_t)n * n)), r = (int)(k % ((int64_t)n * n));
+        const int j = r / n + 1, i = r % n + 1;
+        const int64_t o = box_off(d.P, i, j);
+        const double h = (double)y[t * d.ps + o];
+        if (term == 0) acc += h * qa[o];
+        else if (term == 1) acc += h * h * qa[o];
+        else {
+            const double u = (double)y[d.fs + t * d.ps + o], v = (double)y[2 * d.fs + t * d.ps + o];
+            const double ut = (double)a.Q1[o] * u + (double)a.Q2[o] * v, vt = (double)a.Q2[o] * u + (double)a.Q3[o] * v;
+            acc += (u * ut + v * vt) * qa[o];
+        }
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+}  // namespace chswe

@@ -14,6 +14,7 @@
 #include "chswe.h"
 #include "swe_common.cuh"
 #include "swe_advective.cuh"
+#include "swe_ah.cuh"
 #include "swe_kernels.cuh"
 #include "swe_launch.cuh"
 
@@ -192,6 +193,13 @@ struct DevMetric {
     MetricView<T> v{};
 };
 
+// Metric of the Ah operator on the device.
+template <class T>
+struct DevAh {
+    T *base = nullptr;
+    AhView<T> v{};
+};
+
 // Static tables of the advective operator on the device.
 template <class T>
 struct DevAdv {
@@ -252,6 +260,11 @@ struct swe_ctx {
     void *vh = nullptr;              // covariant wind at the virtual points beyond the panel edges
     void *hb = nullptr;              // panel-boundary h before the in-place averaging
     double *ones = nullptr;          // per-member depth factor 1 (dh = -div F)
+    // Ah staggering (cfg.staggering == SWE_STAG_AH): h, u, v on the vertices
+    bool ah = false;
+    DevAh<double> ah64;
+    DevAh<float> ah32;
+    double *qa = nullptr;            // SBP_Ah quadrature weights J hx hy Ax Ay at the vertices (one box)
 };
 
 struct swe_stvec {
@@ -413,6 +426,52 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
     k_edge_tables<T><<<(N + 1 + 127) / 128, 128, 0, c->stream>>>(v, c->dims, ej, ef, ea, ord_strip_lines(c->ord));
     CU(c, cudaGetLastError());
     CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+// The Ah operator's metric at the vertices (FP64 on the host, stored in T): J, the
+// inverse metric Qi11, Qi12, Qi22, f J per panel (coriolis_colocated's f from
+// calc_coriolis_parameter, coriolis_factory_mod.f90:239-280), and the SBP_Ah
+// quadrature weights J hx hy Ax Ay with the node norm in both directions
+// (quadrature_factory_mod.f90:31-66; Q42_A, sbp_operators_collection_mod.f90:35).
+template <class T>
+static int build_ah_metric(swe_ctx *c, DevAh<T> &da)
+{
+    const int N = c->cfg.N, P = c->dims.P, n = N + 1;
+    const size_t box = (size_t)c->dims.ps;
+    std::vector<T> h(10 * box, T(0));
+    std::vector<double> q(box, 0.0);
+    const HostMetric mxy = host_metric(N, 0.0, 0.0);
+    const double Q42A[4] = {17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0};
+    auto A = [&](int i) { return i <= 4 ? Q42A[i - 1] : (i >= n - 3 ? Q42A[n - i] : 1.0); };
+    const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
+    for (int j = 1; j <= n; j++)
+        for (int i = 1; i <= n; i++) {
+            const size_t k = (size_t)(j - 1) * n + (i - 1), o = (size_t)box_off(P, i, j);
+            h[o] = T(mxy.J[k]);
+            h[box + o] = T(mxy.Q1[k]);
+            h[2 * box + o] = T(mxy.Q2[k]);
+            h[3 * box + o] = T(mxy.Q3[k]);
+            q[o] = mxy.J[k] * hx * hx * A(i) * A(j);
+            for (int p = 0; p < NPAN; p++) {
+                double f = c->cfg.omega;
+                if (!c->cfg.coriolis_constant) {
+                    double r[3];
+                    vertex_r(N, p, i, j, r);
+                    const double *ax = c->cfg.rotation_axis;
+                    f = 2 * c->cfg.omega * (ax[0] * r[0] + ax[1] * r[1] + ax[2] * r[2]) /
+                        std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                }
+                h[(4 + p) * box + o] = T(f * mxy.J[k]);
+            }
+        }
+    T *d = nullptr;
+    if (cudaMalloc(&d, h.size() * sizeof(T)) != cudaSuccess) return fail(c, SWE_ENOMEM, "Ah metric allocation failed");
+    da.base = d;
+    CU(c, cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    da.v.J = d; da.v.Q1 = d + box; da.v.Q2 = d + 2 * box; da.v.Q3 = d + 3 * box; da.v.fJ = d + 4 * box;
+    if (cudaMalloc(&c->qa, box * sizeof(double)) != cudaSuccess) return fail(c, SWE_ENOMEM, "Ah quadrature allocation failed");
+    CU(c, cudaMemcpy(c->qa, q.data(), box * sizeof(double), cudaMemcpyHostToDevice));
     return SWE_OK;
 }
 
@@ -696,6 +755,7 @@ extern "C" int swe_cfg_default(swe_cfg *cfg)
     cfg->coriolis_constant = 0;
     cfg->h_mean = 1000.0;
     cfg->sbp_order = 42;
+    cfg->staggering = SWE_STAG_CH;
     return SWE_OK;
 }
 
@@ -708,6 +768,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
+    cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -734,6 +795,10 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     const int ord = cfg->sbp_order == 0 ? 42 : cfg->sbp_order;
     if ((ord != 42 && ord != 21 && ord != 63) || (ord != 42 && cfg->operator_kind != SWE_OP_LINEAR) ||
         (ord == 63 && cfg->N < 16))
+        return SWE_EINVAL;
+    // Ah staggering: the linear operator with the SBP 4-2 node operators
+    if ((cfg->staggering != SWE_STAG_CH && cfg->staggering != SWE_STAG_AH) ||
+        (cfg->staggering == SWE_STAG_AH && (cfg->operator_kind != SWE_OP_LINEAR || ord != 42)))
         return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
@@ -764,6 +829,11 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     else rc = build_metric<float>(c, c->m32);
     if (rc != SWE_OK) return bail(rc);
     if ((rc = build_quadrature(c)) != SWE_OK) return bail(rc);
+    if (cfg->staggering == SWE_STAG_AH) {
+        c->ah = true;
+        rc = cfg->precision == SWE_FP64 ? build_ah_metric<double>(c, c->ah64) : build_ah_metric<float>(c, c->ah32);
+        if (rc != SWE_OK) return bail(rc);
+    }
     c->Hhost.assign(cfg->n_members, cfg->h_mean);
     if (cudaMalloc(&c->Hm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
     if (cudaMalloc(&c->dtm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
@@ -873,18 +943,28 @@ extern "C" int swe_stvec_destroy(swe_stvec *v)
 }
 
 // Packed host member (Fortran per-panel layout) <-> padded device box.
+// Points per panel of u (nx by ny) and v (ny by nx): the y and x meshes on Ch, the
+// vertices on Ah.
+static void uv_extent(const swe_ctx *c, int &nx, int &ny)
+{
+    nx = c->ah ? c->cfg.N + 1 : c->cfg.N;
+    ny = c->cfg.N + 1;
+}
+
 template <class T>
 static void pack_member(const swe_ctx *c, const double *h, const double *u, const double *v, T *box)
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t ps = c->dims.ps, fs = c->dims.fs;
+    int nx, ny;
+    uv_extent(c, nx, ny);
     for (int t = 0; t < NPAN; t++) {
         for (int j = 0; j <= N; j++)
             for (int i = 0; i <= N; i++) box[0 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*h++);
-        for (int j = 0; j <= N; j++)
-            for (int i = 0; i < N; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
-        for (int j = 0; j < N; j++)
-            for (int i = 0; i <= N; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
+        for (int j = 0; j < nx; j++)
+            for (int i = 0; i < ny; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
     }
 }
 template <class T>
@@ -892,13 +972,15 @@ static void unpack_member(const swe_ctx *c, const T *box, double *h, double *u, 
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t ps = c->dims.ps, fs = c->dims.fs;
+    int nx, ny;
+    uv_extent(c, nx, ny);
     for (int t = 0; t < NPAN; t++) {
         for (int j = 0; j <= N; j++)
             for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-        for (int j = 0; j <= N; j++)
-            for (int i = 0; i < N; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-        for (int j = 0; j < N; j++)
-            for (int i = 0; i <= N; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
+        for (int j = 0; j < nx; j++)
+            for (int i = 0; i < ny; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
     }
 }
 
@@ -906,7 +988,7 @@ static size_t member_sizes(const swe_ctx *c, size_t *nh, size_t *nu)
 {
     const size_t N = c->cfg.N;
     *nh = NPAN * (N + 1) * (N + 1);
-    *nu = NPAN * N * (N + 1);
+    *nu = NPAN * (c->ah ? N + 1 : N) * (N + 1);
     return *nh + 2 * *nu;
 }
 
@@ -1055,6 +1137,9 @@ static dim3 edge_grid(int N, int members) { return dim3((N + 1 + EDGE_CHUNK - 1)
 static dim3 edge_grid(const swe_ctx *c) { return edge_grid(c->cfg.N, c->cfg.n_members); }
 
 template <class T> static const AdvView<T> &adv_view(const swe_ctx *c);
+template <class T> static const AhView<T> &ah_view(const swe_ctx *c);
+template <> const AhView<double> &ah_view<double>(const swe_ctx *c) { return c->ah64.v; }
+template <> const AhView<float> &ah_view<float>(const swe_ctx *c) { return c->ah32.v; }
 template <> const AdvView<double> &adv_view<double>(const swe_ctx *c) { return c->a64.v; }
 template <> const AdvView<float> &adv_view<float>(const swe_ctx *c) { return c->a32.v; }
 
@@ -1064,6 +1149,25 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                           const MetricView<T> &mv)
 {
     const int M = c->cfg.n_members;
+    if (c->ah) {
+        // Ah staggering: the raw panel-boundary values, then every vertex
+        const int n = c->cfg.N + 1;
+        const AhView<T> &av = ah_view<T>(c);
+        StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
+        launch_k(k_ah_edge<T>, dim3((n + 127) / 128, NPAN * 4, M), dim3(128), 0, c->stream, (const T *)yin,
+                 (T *)c->edge, c->dims, av, mv, dtm);
+        const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
+        const T g = T(c->cfg.grav);
+        switch (mode) {
+        case 0: launch_k(k_ah_stage<T, 0>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
+        case 1: launch_k(k_ah_stage<T, 1>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
+        case 2: launch_k(k_ah_stage<T, 2>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
+        case 3: launch_k(k_ah_stage<T, 3>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
+        default: launch_k(k_ah_stage<T, 4>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
+        }
+        c->launches += 2;
+        return;
+    }
     launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
         launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
@@ -1114,6 +1218,7 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    if (c->ah) return fail(c, SWE_EINVAL, "swe_operator_contravariant: built for the Ch staggering");
     const int M = c->cfg.n_members;
     if (c->elem == 8)
         launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
@@ -1275,6 +1380,24 @@ __global__ void k_quad(const T *__restrict__ y, const T *__restrict__ w, const d
 extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, double *mass, double *energy)
 {
     if (!c || !vec || vec->ctx != c || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    if (c->ah) {
+        const int nb = 256;
+        const size_t mo = (size_t)member * c->dims.ms;
+        const dim3 g(nb, 3), b(256);
+        if (c->elem == 8) k_quad_ah<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, c->qa, c->ah64.v, c->dims, c->red);
+        else k_quad_ah<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, c->qa, c->ah32.v, c->dims, c->red);
+        c->launches += 1;
+        CU(c, cudaGetLastError());
+        std::vector<double> part(nb * 3);
+        CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CU(c, cudaStreamSynchronize(c->stream));
+        double sum[3] = {0, 0, 0};
+        for (int q = 0; q < 3; q++)
+            for (int k = 0; k < nb; k++) sum[q] += part[q * nb + k];
+        if (mass) *mass = sum[0];
+        if (energy) *energy = 0.5 * c->Hhost[member] * sum[2] + 0.5 * c->cfg.grav * sum[1];
+        return SWE_OK;
+    }
     const int nb = 256;
     dim3 g(nb, 4), b(256);
     // contravariant components of this member into the scratch, then the four sums
@@ -1342,6 +1465,7 @@ __global__ void k_extrema(const T *__restrict__ y, const T *__restrict__ w, Dims
 extern "C" int swe_diag(swe_ctx *c, const swe_stvec *vec, int member, double dt, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_diag");
     const int nb = 256;
     dim3 g(nb, 4), b(256);
     Dims d1 = c->dims;
@@ -1544,6 +1668,7 @@ static void launch_energies(swe_ctx *c, const T *y, const Dims &d, double hx, in
 extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_curl");
     int rc = ensure_otab(c);
     if (rc != SWE_OK) return rc;
     const size_t mo = (size_t)member * c->dims.ms, box = (size_t)c->dims.ps;
@@ -1562,6 +1687,7 @@ extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *ou
 extern "C" int swe_energies(swe_ctx *c, const swe_stvec *vec, int member, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_energies");
     int rc = ensure_otab(c);
     if (rc != SWE_OK) return rc;
     const int nb = 256;
@@ -1823,7 +1949,7 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
                                 double *ms_stage)
 {
     if (!c || !v0 || v0->ctx != c || nreps < 1) return SWE_EINVAL;
-    if (c->adv) return fail(c, SWE_EINVAL, "swe_kernel_times times the linear operator's three kernels");
+    if (c->adv || c->ah) return fail(c, SWE_EINVAL, "swe_kernel_times times the Ch linear operator's three kernels");
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     const int nst = 4 * nreps;
@@ -2011,7 +2137,8 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         return SWE_ETOOBIG;
     }
     if (cfg->N < 8 || cfg->precision != SWE_FP64 || cfg->n_members != 1 ||
-        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0) || (cfg->sbp_order != 0 && cfg->sbp_order != 42))
+        cfg->operator_kind != SWE_OP_LINEAR || !(cfg->radius > 0.0) || (cfg->sbp_order != 0 && cfg->sbp_order != 42) ||
+        cfg->staggering != SWE_STAG_CH)
         return SWE_EINVAL;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SWE_ENODEV;
@@ -2143,6 +2270,11 @@ std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
 extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_per_step)
 {
     if (!c || nreps < 1) return SWE_EINVAL;
+    if (c->ah) {   // the Ah kernels have no tile configuration
+        if (best_tile) *best_tile = c->tile;
+        if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = 0.0;
+        return SWE_OK;
+    }
     const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind, c->ord};
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {

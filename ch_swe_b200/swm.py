@@ -55,15 +55,28 @@ LINEAR_CH63_NAMES = {
     "quadrature_name": "SBP_C63_quadrature",
 }
 LINEAR_NAMES_BY_ORDER = {42: LINEAR_CH42_NAMES, 21: LINEAR_CH21_NAMES, 63: LINEAR_CH63_NAMES}
+# the linear operator on the Ah staggering (gen_config_linear.sh:9-36, SBP_ORDER 42)
+LINEAR_AH42_NAMES = {
+    "div_op_name": "div_ah_sbp_proj_42",
+    "grad_op_name": "grad_ah_sbp_proj_42",
+    "coriolis_op_name": "coriolis_colocated",
+    "co2contra_op_name": "co2contra_colocated",
+    "quadrature_name": "SBP_Ah42_quadrature",
+}
+STAGGERINGS = {"Ch": _lib.SWE_STAG_CH, "Ah": _lib.SWE_STAG_AH}
 # advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4)
 ADVECTIVE_CH42_NAMES = dict(LINEAR_CH42_NAMES, vector_advection_op_name="vector_advection_Ch_up4_cov",
                             massflux_op_name="massflux_ch_up4")
 OPERATORS = {"linear": _lib.SWE_OP_LINEAR, "advective": _lib.SWE_OP_ADVECTIVE}
 
 
-def state_shapes(N: int, members: int | None = None):
-    """Packed host shapes of (h, u, v) for one member (or a batch of members)."""
-    sh = [(6, N + 1, N + 1), (6, N + 1, N), (6, N, N + 1)]
+def state_shapes(N: int, members: int | None = None, staggering: str = "Ch"):
+    """Packed host shapes of (h, u, v) for one member (or a batch of members): on Ch,
+    h on the vertices, u on the y points, v on the x points; on Ah all on the vertices."""
+    if staggering == "Ah":
+        sh = [(6, N + 1, N + 1)] * 3
+    else:
+        sh = [(6, N + 1, N + 1), (6, N + 1, N), (6, N, N + 1)]
     if members is None:
         return tuple(sh)
     return tuple((members,) + s for s in sh)
@@ -71,7 +84,7 @@ def state_shapes(N: int, members: int | None = None):
 
 @dataclass
 class Domain:
-    """Cubed-sphere domain with Ch staggering; owns the device context."""
+    """Cubed-sphere domain with Ch (default) or Ah staggering; owns the device context."""
     N: int
     precision: str = "fp64"
     n_members: int = 1
@@ -87,8 +100,10 @@ class Domain:
     _ctx: int = field(default=None, repr=False)
 
     def __post_init__(self):
-        if self.horizontal_staggering != "Ch":
+        if self.horizontal_staggering not in STAGGERINGS:
             raise ValueError("domain_factory_mod, unsupported horizontal staggering: " + self.horizontal_staggering)
+        if self.horizontal_staggering == "Ah" and (self.operator != "linear" or self.sbp_order != 42):
+            raise ValueError("the Ah staggering is built for the linear operator with SBP 4-2")
         if self.precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if self.operator not in OPERATORS:
@@ -112,6 +127,7 @@ class Domain:
         cfg.h_mean = float(self.h_mean)
         cfg.operator_kind = OPERATORS[self.operator]
         cfg.sbp_order = int(self.sbp_order)
+        cfg.staggering = STAGGERINGS[self.horizontal_staggering]
         ctx = ctypes.c_void_p()
         check(L.swe_ctx_create(ctypes.byref(cfg), ctypes.byref(ctx)), None, "swe_ctx_create")
         self._ctx = ctx.value
@@ -208,16 +224,16 @@ class StvecSwm:
 
     # -- transfers ------------------------------------------------------
     def upload(self, h, u, v, member: int | None = 0):
-        N = self.domain.N
+        N, stag = self.domain.N, self.domain.horizontal_staggering
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
         L = _lib.load()
         if member is None:
-            for a, s in zip(arrs, state_shapes(N, self.domain.n_members)):
+            for a, s in zip(arrs, state_shapes(N, self.domain.n_members, stag)):
                 if a.shape != s:
                     raise ValueError(f"expected shape {s}, got {a.shape}")
             rc = L.swe_stvec_upload_all(self._p, *(dptr(a) for a in arrs))
         else:
-            for a, s in zip(arrs, state_shapes(N)):
+            for a, s in zip(arrs, state_shapes(N, None, stag)):
                 if a.shape != s:
                     raise ValueError(f"expected shape {s}, got {a.shape}")
             rc = L.swe_stvec_upload(self._p, int(member), *(dptr(a) for a in arrs))
@@ -225,13 +241,13 @@ class StvecSwm:
         return self
 
     def download(self, member: int | None = 0):
-        N = self.domain.N
+        N, stag = self.domain.N, self.domain.horizontal_staggering
         L = _lib.load()
         if member is None:
-            out = [np.empty(s) for s in state_shapes(N, self.domain.n_members)]
+            out = [np.empty(s) for s in state_shapes(N, self.domain.n_members, stag)]
             rc = L.swe_stvec_download_all(self._p, *(dptr(a) for a in out))
         else:
-            out = [np.empty(s) for s in state_shapes(N)]
+            out = [np.empty(s) for s in state_shapes(N, None, stag)]
             rc = L.swe_stvec_download(self._p, int(member), *(dptr(a) for a in out))
         check(rc, self.domain.ctx, "swe_stvec_download")
         return tuple(out)
@@ -321,6 +337,8 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
         if "h_mean" not in config:
             raise ValueError("linear_swm_operator requires h_mean")
         names, want_op = LINEAR_NAMES_BY_ORDER[domain.sbp_order], "linear"
+        if domain.horizontal_staggering == "Ah":
+            names = LINEAR_AH42_NAMES
     elif kind == "advective_swm_operator":
         if config.get("v_components_type", "covariant") != "covariant":
             raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
@@ -332,6 +350,8 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     for key, want in names.items():
         got = config.get(key, want)
         if got != want:
+            if want_op == "linear" and got == LINEAR_AH42_NAMES.get(key) and domain.horizontal_staggering != "Ah":
+                raise ValueError(f"{key} = {got} needs a domain created with horizontal_staggering='Ah'")
             for order, other in LINEAR_NAMES_BY_ORDER.items():
                 if want_op == "linear" and got == other.get(key):
                     raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")

@@ -54,11 +54,14 @@ def mesh_geometry(N: int, mesh: str):
     return r, a1, a2
 
 
-def gaussian_hill(N: int, lam0: float = np.pi, phi0: float = 0.0, d0: float = 0.25, amp: float = 1.0):
+def gaussian_hill(N: int, lam0: float = np.pi, phi0: float = 0.0, d0: float = 0.25, amp: float = 1.0,
+                  staggering: str = "Ch"):
     r, _, _ = mesh_geometry(N, "xy")
     x0, y0, z0 = np.cos(phi0) * np.cos(lam0), np.cos(phi0) * np.sin(lam0), np.sin(phi0)
     d = np.clip(r[..., 0] * x0 + r[..., 1] * y0 + r[..., 2] * z0, -1.0, 1.0)
     h = amp * np.exp(-(np.arccos(d) / d0) ** 2)
+    if staggering == "Ah":
+        return np.ascontiguousarray(h), np.zeros((6, N + 1, N + 1)), np.zeros((6, N + 1, N + 1))
     return np.ascontiguousarray(h), np.zeros((6, N + 1, N)), np.zeros((6, N, N + 1))
 
 
@@ -72,7 +75,8 @@ def gaussian_sum(N: int, centres, widths, amps):
 
 def williamson2(N: int, u0: float = np.pi * EARTH_RADIUS / 6.0 / (23 * 60 * 60 + 56 * 60 + 4),
                 h_mean: float = 29400.0 / EARTH_GRAV, axis=(0.0, 0.0, 1.0), linear_mode: bool = False,
-                radius: float = EARTH_RADIUS, omega: float = EARTH_OMEGA, grav: float = EARTH_GRAV):
+                radius: float = EARTH_RADIUS, omega: float = EARTH_OMEGA, grav: float = EARTH_GRAV,
+                staggering: str = "Ch"):
     ax = np.asarray(axis, dtype=np.float64)
     ax = ax / np.sqrt(np.sum(ax ** 2))
     r, _, _ = mesh_geometry(N, "xy")
@@ -81,7 +85,8 @@ def williamson2(N: int, u0: float = np.pi * EARTH_RADIUS / 6.0 / (23 * 60 * 60 +
     mt = 0.0 if linear_mode else 1.0
     h = h_mean - (radius * omega * u0 + mt * 0.5 * u0 ** 2) / grav * np.sin(phi) ** 2
     out = [np.ascontiguousarray(h)]
-    for mesh, comp in (("y", 1), ("x", 2)):
+    meshes = (("xy", 1), ("xy", 2)) if staggering == "Ah" else (("y", 1), ("x", 2))
+    for mesh, comp in meshes:
         rm, a1, a2 = mesh_geometry(N, mesh)
         rn = rm / np.linalg.norm(rm, axis=-1, keepdims=True)
         vel = u0 * np.cross(ax, rn)

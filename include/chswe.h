@@ -59,6 +59,9 @@ extern "C" {
                               vector_advection_Ch_up4_cov; operator_adv_swm_mod.f90:62-96);
                               h is the full depth, h_mean is not used, no orography */
 
+#define SWE_STAG_CH 0      /* horizontal_staggering 'Ch': h on vertices, u on y, v on x points */
+#define SWE_STAG_AH 1      /* horizontal_staggering 'Ah': h, u, v on the vertices (linear operator) */
+
 typedef struct swe_ctx swe_ctx;
 typedef struct swe_stvec swe_stvec;
 
@@ -78,6 +81,11 @@ typedef struct swe_cfg {
                                  _sbp_sat_42 / _21 / _63 names of grad_factory_mod.f90,
                                  div_factory_mod.f90, co2contra_factory_mod.f90,
                                  coriolis_factory_mod.f90 and the SBP_C42/C21/C63 quadratures */
+    int staggering;           /* SWE_STAG_CH (default) or SWE_STAG_AH: h, u, v all on the cell
+                                 vertices, the linear operator with div_ah_sbp_proj_42,
+                                 grad_ah_sbp_proj_42, coriolis_colocated, co2contra_colocated and
+                                 SBP_Ah42_quadrature (gen_config_linear.sh:9-36); SBP 4-2 only.
+                                 Packed u and v are then (N+1) x (N+1) per panel like h. */
 } swe_cfg;
 
 /* Fill *cfg with the defaults listed above. */
