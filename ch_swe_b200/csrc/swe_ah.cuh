@@ -1,7 +1,8 @@
 // swe_ah.cuh -- the linear shallow-water operator on the Ah staggering: h, u and v
 // all on the cell vertices (the xy mesh), the operator set of the reference's Ah
 // configuration (gen_config_linear.sh:9-36):
-//   grad_ah_sbp_proj_42     node-to-node SBP 4-2 differences (sbp_diff_42_mod.f90:30-156)
+//   grad_ah_sbp_proj_42     node-to-node SBP 4-2 differences (sbp_diff_42_mod.f90:30-156;
+//                           2-1 and 6-3 for the _21 / _63 names)
 //                           and the covariant ECS Ah vector sync of the panel-edge
 //                           vertices (grad_sbp_proj_mod.f90:26-72, ecs_Ah_vec_sync_mod.f90:34-125)
 //   co2contra_colocated     ut = Qi11 u + Qi12 v, vt = Qi12 u + Qi22 v at each vertex
@@ -38,7 +39,32 @@ constexpr double N11 = -1.4117647058823528, N12 = 1.7352941176470589, N13 = -0.2
                  N46 = -0.0816326530612245;
 }  // namespace sbp
 
-// SBP 4-2 first derivative at node k of n nodes (inputs f(1..n), no halo).
+// SBP first derivative at node k of n nodes (inputs f(1..n), no halo) of order ORD:
+// 2-1 (sbp_diff_21_mod.f90:8-40), 4-2 (sbp_diff_42_mod.f90:30-156), 6-3 (the table
+// D_SBP63_NN_Q of sbp_diff_63_mod.f90:9-140).
+template <class T, class F>
+__device__ __forceinline__ T dn2n21(int k, int n, const F &f)
+{
+    if (k >= 2 && k <= n - 1) return (-f(k - 1) + f(k + 1)) / T(2);
+    if (k == 1) return T(-1) * f(1) + T(1) * f(2);
+    return -T(-1) * f(n) - T(1) * f(n - 1);
+}
+template <class T, class F>
+__device__ __forceinline__ T dn2n63(int k, int n, const F &f)
+{
+    if (k >= 7 && k <= n - 6)
+        return (-f(k - 3) + T(9) * f(k - 2) + T(-45) * f(k - 1) + T(45) * f(k + 1) + T(-9) * f(k + 2) + f(k + 3)) / T(60);
+    const bool lo = k <= 6;
+    const int r = lo ? k : n + 1 - k;
+    T a = T(0);
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const double c = D_SBP63_NN_Q[r - 1][q];
+        if (c == 0.0) continue;
+        a = lo ? a + T(c) * f(q + 1) : a - T(c) * f(n - q);
+    }
+    return a;
+}
 template <class T, class F>
 __device__ __forceinline__ T dn2n42(int k, int n, const F &f)
 {
@@ -54,26 +80,34 @@ __device__ __forceinline__ T dn2n42(int k, int n, const F &f)
     return -T(N11) * f(n) - T(N12) * f(n - 1) - T(N13) * f(n - 2) - T(N14) * f(n - 3);
 }
 
+template <class T, int ORD, class F>
+__device__ __forceinline__ T dn2n(int k, int n, const F &f)
+{
+    if constexpr (ORD == 21) return dn2n21<T>(k, n, f);
+    else if constexpr (ORD == 63) return dn2n63<T>(k, n, f);
+    else return dn2n42<T>(k, n, f);
+}
+
 // Raw (before the panel-edge syncs) gradient (gx, gy) and divergence of the
 // contravariant wind at vertex (i, j) of panel t; y is the member's state.
-template <class T>
+template <class T, int ORD>
 __device__ __forceinline__ void ah_raw(const T *y, const Dims &d, const AhView<T> &a, const MetricView<T> &m, int t,
                                        int i, int j, T &gx, T &gy, T &dv)
 {
     const int n = d.N + 1;
     const GV<T> H = gview(y, d, 0, t), U = gview(y, d, 1, t), V = gview(y, d, 2, t);
     const GV<T> J = mview(a.J, d), Q1 = mview(a.Q1, d), Q2 = mview(a.Q2, d), Q3 = mview(a.Q3, d);
-    gx = dn2n42<T>(i, n, [&](int k) { return H(k, j); }) * m.inv_hxa;
-    gy = dn2n42<T>(j, n, [&](int k) { return H(i, k); }) * m.inv_hxa;
-    const T dx = dn2n42<T>(i, n, [&](int k) { return J(k, j) * (Q1(k, j) * U(k, j) + Q2(k, j) * V(k, j)); });
-    const T dy = dn2n42<T>(j, n, [&](int k) { return J(i, k) * (Q2(i, k) * U(i, k) + Q3(i, k) * V(i, k)); });
+    gx = dn2n<T, ORD>(i, n, [&](int k) { return H(k, j); }) * m.inv_hxa;
+    gy = dn2n<T, ORD>(j, n, [&](int k) { return H(i, k); }) * m.inv_hxa;
+    const T dx = dn2n<T, ORD>(i, n, [&](int k) { return J(k, j) * (Q1(k, j) * U(k, j) + Q2(k, j) * V(k, j)); });
+    const T dy = dn2n<T, ORD>(j, n, [&](int k) { return J(i, k) * (Q2(i, k) * U(i, k) + Q3(i, k) * V(i, k)); });
     dv = (dx * m.inv_hx + dy * m.inv_hx) * mview(m.iJa, d)(i, j);
 }
 
 // k_ah_edge: the raw (gx, gy, div) of every panel-boundary vertex into the edge
 // buffer (edge_index: member, panel, side, along index).  Grid (along chunks,
 // panel * 4 + side, member).
-template <class T>
+template <class T, int ORD>
 __global__ void __launch_bounds__(128) k_ah_edge(const T *__restrict__ Y, T *__restrict__ E, Dims d, AhView<T> a,
                                                  MetricView<T> m, const double *__restrict__ dtm)
 {
@@ -87,7 +121,7 @@ __global__ void __launch_bounds__(128) k_ah_edge(const T *__restrict__ Y, T *__r
     int i, j;
     side_vertex(N, s, b, 0, i, j);
     T gx, gy, dv;
-    ah_raw(Y + mem * d.ms, d, a, m, t, i, j, gx, gy, dv);
+    ah_raw<T, ORD>(Y + mem * d.ms, d, a, m, t, i, j, gx, gy, dv);
     T *e = E + edge_index(N, mem, t, s, b);
     e[0] = gx;
     e[1] = gy;
@@ -98,7 +132,7 @@ __global__ void __launch_bounds__(128) k_ah_edge(const T *__restrict__ Y, T *__r
 // edges the syncs with the neighbours' raw values from k_ah_edge (the neighbour's
 // vector is handed over as the 'cross' exchange does, halo_vec), the tendency and
 // the RK update of k_stage (modes 0..4; FP32 mode 4 Kahan-compensated).
-template <class T, int MODE>
+template <class T, int MODE, int ORD>
 __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, const T *__restrict__ E, T *V0, T *Y1,
                                                   T *ACC, T *CMP, Dims d, AhView<T> a, MetricView<T> m, StageArgs sa,
                                                   T grav)
@@ -112,7 +146,7 @@ __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, con
     if (i > n || j > n) return;
     const T *y = Yin + mem * d.ms;
     T gx, gy, dv;
-    ah_raw(y, d, a, m, t, i, j, gx, gy, dv);
+    ah_raw<T, ORD>(y, d, a, m, t, i, j, gx, gy, dv);
     const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
     const bool cx = il || ir, cy = jb || jt;
     if (cx || cy) {

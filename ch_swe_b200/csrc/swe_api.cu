@@ -442,8 +442,11 @@ static int build_ah_metric(swe_ctx *c, DevAh<T> &da)
     std::vector<T> h(10 * box, T(0));
     std::vector<double> q(box, 0.0);
     const HostMetric mxy = host_metric(N, 0.0, 0.0);
-    const double Q42A[4] = {17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0};
-    auto A = [&](int i) { return i <= 4 ? Q42A[i - 1] : (i >= n - 3 ? Q42A[n - i] : 1.0); };
+    // Q21_A, Q42_A, Q63_A (sbp_operators_collection_mod.f90:22,35,38-40)
+    const double Q21A[2] = {0.5, 1.0}, Q42A[4] = {17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0};
+    const double *QA = c->ord == 21 ? Q21A : (c->ord == 63 ? SBP63_NN_A : Q42A);
+    const int ne = c->ord == 21 ? 2 : (c->ord == 63 ? 6 : 4);
+    auto A = [&](int i) { return i <= ne ? QA[i - 1] : (i >= n - ne + 1 ? QA[n - i] : 1.0); };
     const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
     for (int j = 1; j <= n; j++)
         for (int i = 1; i <= n; i++) {
@@ -796,9 +799,9 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if ((ord != 42 && ord != 21 && ord != 63) || (ord != 42 && cfg->operator_kind != SWE_OP_LINEAR) ||
         (ord == 63 && cfg->N < 16))
         return SWE_EINVAL;
-    // Ah staggering: the linear operator with the SBP 4-2 node operators
+    // Ah staggering: the linear operator with the SBP node operators
     if ((cfg->staggering != SWE_STAG_CH && cfg->staggering != SWE_STAG_AH) ||
-        (cfg->staggering == SWE_STAG_AH && (cfg->operator_kind != SWE_OP_LINEAR || ord != 42)))
+        (cfg->staggering == SWE_STAG_AH && cfg->operator_kind != SWE_OP_LINEAR))
         return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
@@ -1143,6 +1146,27 @@ template <> const AhView<float> &ah_view<float>(const swe_ctx *c) { return c->ah
 template <> const AdvView<double> &adv_view<double>(const swe_ctx *c) { return c->a64.v; }
 template <> const AdvView<float> &adv_view<float>(const swe_ctx *c) { return c->a32.v; }
 
+// The two launches of an Ah stage: the raw panel-boundary values, then every vertex.
+template <class T, int ORD>
+static void launch_ah(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode,
+                      const StageArgs &a, const AhView<T> &av, const MetricView<T> &mv, const double *dtm)
+{
+    const int n = c->cfg.N + 1, M = c->cfg.n_members;
+    launch_k(k_ah_edge<T, ORD>, dim3((n + 127) / 128, NPAN * 4, M), dim3(128), 0, c->stream, (const T *)yin,
+             (T *)c->edge, c->dims, av, mv, dtm);
+    const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
+    const T g = T(c->cfg.grav);
+    const T *Y = (const T *)yin, *E = (const T *)c->edge;
+    T *V = (T *)v0, *Y1 = (T *)y1, *A = (T *)acc, *C = (T *)cmp;
+    switch (mode) {
+    case 0: launch_k(k_ah_stage<T, 0, ORD>, pg, pb, 0, c->stream, Y, E, V, Y1, A, C, c->dims, av, mv, a, g); break;
+    case 1: launch_k(k_ah_stage<T, 1, ORD>, pg, pb, 0, c->stream, Y, E, V, Y1, A, C, c->dims, av, mv, a, g); break;
+    case 2: launch_k(k_ah_stage<T, 2, ORD>, pg, pb, 0, c->stream, Y, E, V, Y1, A, C, c->dims, av, mv, a, g); break;
+    case 3: launch_k(k_ah_stage<T, 3, ORD>, pg, pb, 0, c->stream, Y, E, V, Y1, A, C, c->dims, av, mv, a, g); break;
+    default: launch_k(k_ah_stage<T, 4, ORD>, pg, pb, 0, c->stream, Y, E, V, Y1, A, C, c->dims, av, mv, a, g); break;
+    }
+}
+
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const double *dtm,
@@ -1151,20 +1175,11 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     const int M = c->cfg.n_members;
     if (c->ah) {
         // Ah staggering: the raw panel-boundary values, then every vertex
-        const int n = c->cfg.N + 1;
         const AhView<T> &av = ah_view<T>(c);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
-        launch_k(k_ah_edge<T>, dim3((n + 127) / 128, NPAN * 4, M), dim3(128), 0, c->stream, (const T *)yin,
-                 (T *)c->edge, c->dims, av, mv, dtm);
-        const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
-        const T g = T(c->cfg.grav);
-        switch (mode) {
-        case 0: launch_k(k_ah_stage<T, 0>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
-        case 1: launch_k(k_ah_stage<T, 1>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
-        case 2: launch_k(k_ah_stage<T, 2>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
-        case 3: launch_k(k_ah_stage<T, 3>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
-        default: launch_k(k_ah_stage<T, 4>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc, (T *)cmp, c->dims, av, mv, a, g); break;
-        }
+        if (c->ord == 21) launch_ah<T, 21>(c, yin, v0, y1, acc, cmp, mode, a, av, mv, dtm);
+        else if (c->ord == 63) launch_ah<T, 63>(c, yin, v0, y1, acc, cmp, mode, a, av, mv, dtm);
+        else launch_ah<T, 42>(c, yin, v0, y1, acc, cmp, mode, a, av, mv, dtm);
         c->launches += 2;
         return;
     }

@@ -55,14 +55,18 @@ LINEAR_CH63_NAMES = {
     "quadrature_name": "SBP_C63_quadrature",
 }
 LINEAR_NAMES_BY_ORDER = {42: LINEAR_CH42_NAMES, 21: LINEAR_CH21_NAMES, 63: LINEAR_CH63_NAMES}
-# the linear operator on the Ah staggering (gen_config_linear.sh:9-36, SBP_ORDER 42)
-LINEAR_AH42_NAMES = {
-    "div_op_name": "div_ah_sbp_proj_42",
-    "grad_op_name": "grad_ah_sbp_proj_42",
-    "coriolis_op_name": "coriolis_colocated",
-    "co2contra_op_name": "co2contra_colocated",
-    "quadrature_name": "SBP_Ah42_quadrature",
+# the linear operator on the Ah staggering (gen_config_linear.sh:9-36), per SBP order
+LINEAR_AH_NAMES_BY_ORDER = {
+    order: {
+        "div_op_name": f"div_ah_sbp_proj_{order}",
+        "grad_op_name": f"grad_ah_sbp_proj_{order}",
+        "coriolis_op_name": "coriolis_colocated",
+        "co2contra_op_name": "co2contra_colocated",
+        "quadrature_name": f"SBP_Ah{order}_quadrature",
+    }
+    for order in (42, 21, 63)
 }
+LINEAR_AH42_NAMES = LINEAR_AH_NAMES_BY_ORDER[42]
 STAGGERINGS = {"Ch": _lib.SWE_STAG_CH, "Ah": _lib.SWE_STAG_AH}
 # advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4)
 ADVECTIVE_CH42_NAMES = dict(LINEAR_CH42_NAMES, vector_advection_op_name="vector_advection_Ch_up4_cov",
@@ -102,8 +106,8 @@ class Domain:
     def __post_init__(self):
         if self.horizontal_staggering not in STAGGERINGS:
             raise ValueError("domain_factory_mod, unsupported horizontal staggering: " + self.horizontal_staggering)
-        if self.horizontal_staggering == "Ah" and (self.operator != "linear" or self.sbp_order != 42):
-            raise ValueError("the Ah staggering is built for the linear operator with SBP 4-2")
+        if self.horizontal_staggering == "Ah" and self.operator != "linear":
+            raise ValueError("the Ah staggering is built for the linear operator")
         if self.precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if self.operator not in OPERATORS:
@@ -338,7 +342,7 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
             raise ValueError("linear_swm_operator requires h_mean")
         names, want_op = LINEAR_NAMES_BY_ORDER[domain.sbp_order], "linear"
         if domain.horizontal_staggering == "Ah":
-            names = LINEAR_AH42_NAMES
+            names = LINEAR_AH_NAMES_BY_ORDER[domain.sbp_order]
     elif kind == "advective_swm_operator":
         if config.get("v_components_type", "covariant") != "covariant":
             raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
@@ -350,8 +354,11 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     for key, want in names.items():
         got = config.get(key, want)
         if got != want:
-            if want_op == "linear" and got == LINEAR_AH42_NAMES.get(key) and domain.horizontal_staggering != "Ah":
-                raise ValueError(f"{key} = {got} needs a domain created with horizontal_staggering='Ah'")
+            for order, ah in LINEAR_AH_NAMES_BY_ORDER.items():
+                if want_op == "linear" and got == ah.get(key) and domain.horizontal_staggering != "Ah":
+                    raise ValueError(f"{key} = {got} needs a domain created with horizontal_staggering='Ah'")
+                if want_op == "linear" and got == ah.get(key) and domain.sbp_order != order:
+                    raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")
             for order, other in LINEAR_NAMES_BY_ORDER.items():
                 if want_op == "linear" and got == other.get(key):
                     raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")

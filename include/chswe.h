@@ -82,10 +82,11 @@ typedef struct swe_cfg {
                                  div_factory_mod.f90, co2contra_factory_mod.f90,
                                  coriolis_factory_mod.f90 and the SBP_C42/C21/C63 quadratures */
     int staggering;           /* SWE_STAG_CH (default) or SWE_STAG_AH: h, u, v all on the cell
-                                 vertices, the linear operator with div_ah_sbp_proj_42,
-                                 grad_ah_sbp_proj_42, coriolis_colocated, co2contra_colocated and
-                                 SBP_Ah42_quadrature (gen_config_linear.sh:9-36); SBP 4-2 only.
-                                 Packed u and v are then (N+1) x (N+1) per panel like h. */
+                                 vertices, the linear operator with div_ah_sbp_proj_<order>,
+                                 grad_ah_sbp_proj_<order>, coriolis_colocated, co2contra_colocated
+                                 and SBP_Ah<order>_quadrature (gen_config_linear.sh:9-36), the
+                                 order from sbp_order (42, 21 or 63).  Packed u and v are then
+                                 (N+1) x (N+1) per panel like h. */
 } swe_cfg;
 
 /* Fill *cfg with the defaults listed above. */

@@ -1558,8 +1558,8 @@ static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_
    grad_ah_sbp_proj_*, coriolis_colocated, co2contra_colocated), h, u, v on the xy mesh ---- */
 
 /* node-to-node SBP first derivative along dir of a line of n nodes (no halo, one-sided
-   closures): sbp_diff_21_mod.f90, sbp_diff_42_mod.f90:30-156 (the reference's decimal
-   coefficients), sbp_diff_63_mod.f90 */
+   closures): sbp_diff_21_mod.f90:8-40, sbp_diff_42_mod.f90:30-156 (the reference's decimal
+   coefficients), sbp_diff_63_mod.f90:9-140 (SBP63_NN_Q) */
 static const double N42_Q[4][6] = {{-1.4117647058823528, 1.7352941176470589, -0.2352941176470588, -0.08823529411764705, 0, 0},
                                    {-0.5, 0, 0.5, 0, 0, 0},
                                    {0.09302325581395347, -0.686046511627907, 0, 0.686046511627907, -0.09302325581395347, 0},
@@ -1568,7 +1568,32 @@ static void diff_n2n(fld_t *out, const fld_t *in, int t, int dir, int n, int ls,
 {
 #define O(k) (*((dir) == 0 ? &FA(out, t, k, l) : &FA(out, t, l, k)))
 #define I(k) L(in, t, dir, k, l)
-    (void)ord;
+    if (ord == 21) {
+        /* sbp_diff_21_mod.f90: q11 = -1, q12 = 1; interior (-f(i-1) + f(i+1)) / 2 */
+        for (int l = ls; l <= le; l++) {
+            O(1) = -1.0 * I(1) + 1.0 * I(2);
+            for (int k = 2; k <= n - 1; k++) O(k) = (-I(k - 1) + I(k + 1)) / 2.0;
+            O(n) = -(-1.0) * I(n) - 1.0 * I(n - 1);
+        }
+        return;
+    }
+    if (ord == 63) {
+        for (int l = ls; l <= le; l++) {
+            for (int r = 1; r <= 6; r++) {
+                double a = 0.0, b = 0.0;
+                for (int q = 0; q < 9; q++) {
+                    if (SBP63_NN_Q[r - 1][q] == 0.0) continue;
+                    a = a + SBP63_NN_Q[r - 1][q] * I(q + 1);
+                    b = b - SBP63_NN_Q[r - 1][q] * I(n + 1 - (q + 1));
+                }
+                O(r) = a;
+                O(n + 1 - r) = b;
+            }
+            for (int k = 7; k <= n - 6; k++)
+                O(k) = (-I(k - 3) + 9 * I(k - 2) + -45 * I(k - 1) + 45 * I(k + 1) + -9 * I(k + 2) + I(k + 3)) / 60.0;
+        }
+        return;
+    }
     for (int l = ls; l <= le; l++) {
         for (int r = 1; r <= 4; r++) {
             double a = 0.0, b = 0.0;
@@ -1995,8 +2020,11 @@ void orc_ah_integrals(orc_ctx *c, const double *h, const double *u, const double
     const int n = c->N + 1;
     const mesh_t *m = &c->mxy;
     const double A42[4] = {17.0 / 48.0, 59.0 / 48.0, 43.0 / 48.0, 49.0 / 48.0};
+    const double A21[2] = {0.5, 1.0};   /* Q21_A (sbp_operators_collection_mod.f90:22) */
     double *A = malloc(sizeof(double) * n);
-    mass_coeffs(A, n, A42, 4);
+    if (c->ord == 21) mass_coeffs(A, n, A21, 2);
+    else if (c->ord == 63) mass_coeffs(A, n, SBP63_NN_A, 6);
+    else mass_coeffs(A, n, A42, 4);
     double sm = 0.0, se = 0.0, sh = 0.0;
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= n; j++)

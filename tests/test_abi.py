@@ -83,15 +83,13 @@ def test_no_device_fails_loudly(lib_built):
 
 
 def test_ah_domain_validation():
-    """The Ah staggering is built for the linear operator with SBP 4-2 (checked before
-    any device call)."""
+    """The Ah staggering is built for the linear operator (checked before any device
+    call)."""
     import pytest
     from ch_swe_b200 import create_domain
     from ch_swe_b200.swm import state_shapes
     with pytest.raises(ValueError):
         create_domain(16, horizontal_staggering="Ah", operator="advective")
-    with pytest.raises(ValueError):
-        create_domain(16, horizontal_staggering="Ah", sbp_order=63)
     with pytest.raises(ValueError):
         create_domain(16, horizontal_staggering="C")
     assert state_shapes(16, None, "Ah") == ((6, 17, 17),) * 3

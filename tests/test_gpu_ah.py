@@ -30,34 +30,37 @@ def random_state(N, seed):
     return tuple(rng.standard_normal((6, N + 1, N + 1)) * s for s in (1.0, 10.0, 10.0))
 
 
-def ah_domain(N, precision="fp64", members=1, axis=(0.0, 0.0, 1.0)):
+def ah_domain(N, precision="fp64", members=1, axis=(0.0, 0.0, 1.0), order=42):
     from ch_swe_b200 import create_domain, create_swm_operator
     dom = create_domain(N, precision=precision, horizontal_staggering="Ah", n_members=members, h_mean=H,
-                        rotation_axis=axis)
+                        rotation_axis=axis, sbp_order=order)
     op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H,
-                                        "div_op_name": "div_ah_sbp_proj_42", "grad_op_name": "grad_ah_sbp_proj_42",
+                                        "div_op_name": f"div_ah_sbp_proj_{order}",
+                                        "grad_op_name": f"grad_ah_sbp_proj_{order}",
                                         "coriolis_op_name": "coriolis_colocated",
                                         "co2contra_op_name": "co2contra_colocated",
-                                        "quadrature_name": "SBP_Ah42_quadrature"}, dom)
+                                        "quadrature_name": f"SBP_Ah{order}_quadrature"}, dom)
     return dom, op
 
 
-@pytest.mark.parametrize("N", [8, 12, 17, 24, 33])
-def test_apply_parity_fp64_random(N):
+@pytest.mark.parametrize("order,N", [(42, 8), (42, 12), (42, 17), (42, 24), (42, 33), (21, 8), (21, 17),
+                                     (63, 16), (63, 25)])
+def test_apply_parity_fp64_random(order, N):
     from ch_swe_b200 import create_stvec_swm
     from oracle.oracle import Oracle
     st = random_state(N, 300 + N)
-    ref = Oracle(N, h_mean=H).ah_apply(*st)
-    dom, op = ah_domain(N)
+    ref = Oracle(N, h_mean=H, sbp_order=order).ah_apply(*st)
+    dom, op = ah_domain(N, order=order)
     x = create_stvec_swm(dom).upload(*st)
     y = create_stvec_swm(dom)
     op.apply(y, x, dom)
     for g, r, name in zip(y.download(), ref, "huv"):
-        assert rel(g, r) < FP64_RTOL, (N, name, rel(g, r))
+        assert rel(g, r) < FP64_RTOL, (order, N, name, rel(g, r))
     dom.destroy()
 
 
-def test_rk4_parity_fp64_and_fp32():
+@pytest.mark.parametrize("order", [42, 21, 63])
+def test_rk4_parity_fp64_and_fp32(order):
     """24 RK4 steps of a Gaussian hill under a tilted rotation axis: FP64 within 1e-12
     of the oracle, FP32 within 1e-5 (relative L2) of FP64; mass conserved."""
     from ch_swe_b200 import create_stvec_swm, create_timescheme
@@ -66,11 +69,11 @@ def test_rk4_parity_fp64_and_fp32():
     N, dt, nst = 20, 900.0, 24
     axis = (np.sin(0.7), 0.0, np.cos(0.7))
     st = gaussian_hill(N, lam0=0.5, phi0=0.6, d0=0.3, amp=5.0, staggering="Ah")
-    o = Oracle(N, h_mean=H, axis=axis)
+    o = Oracle(N, h_mean=H, axis=axis, sbp_order=order)
     ref = o.ah_rk4(*st, dt, nst)
     out = {}
     for prec in ("fp64", "fp32"):
-        dom, op = ah_domain(N, prec, axis=axis)
+        dom, op = ah_domain(N, prec, axis=axis, order=order)
         x = create_stvec_swm(dom).upload(*st)
         create_timescheme(x, "rk4").steps(x, op, dom, dt, nst)
         out[prec] = x.download()
@@ -85,14 +88,15 @@ def test_rk4_parity_fp64_and_fp32():
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5, name
 
 
-def test_integrals_match_oracle():
+@pytest.mark.parametrize("order", [42, 21, 63])
+def test_integrals_match_oracle(order):
     from ch_swe_b200 import create_stvec_swm
     from oracle.oracle import Oracle
     N = 16
     st = random_state(N, 5)
-    o = Oracle(N, h_mean=H)
+    o = Oracle(N, h_mean=H, sbp_order=order)
     m_ref, e_ref = o.ah_integrals(*st)
-    dom, op = ah_domain(N)
+    dom, op = ah_domain(N, order=order)
     m, e = op.integrals(create_stvec_swm(dom).upload(*st))
     assert abs(m - m_ref) < 1e-12 * max(abs(m_ref), 1.0) and abs(e - e_ref) < 1e-12 * abs(e_ref)
     dom.destroy()
