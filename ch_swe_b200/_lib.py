@@ -32,7 +32,7 @@ EXPORTED = [
     "swe_rk4_step", "swe_rk4_steps", "swe_integrals", "swe_launch_count", "swe_edge_links",
     "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
     "swe_set_tile", "swe_get_tile", "swe_autotune", "swe_rk4_steps_members",
-    "swe_set_kernel_config", "swe_get_kernel_config", "swe_diag", "swe_energies", "swe_curl", "swe_regrid_latlon",
+    "swe_set_kernel_config", "swe_get_kernel_config", "swe_diag", "swe_energies", "swe_curl", "swe_regrid_latlon", "swe_regrid_latlon_wind",
 ]
 
 
@@ -106,6 +106,7 @@ def load(path: str = LIB_PATH):
     L.swe_energies.argtypes = [_vp, _vp, ctypes.c_int, _dp]
     L.swe_curl.argtypes = [_vp, _vp, ctypes.c_int, _dp]
     L.swe_regrid_latlon.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+    L.swe_regrid_latlon_wind.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
     L.swe_set_kernel_config.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.swe_get_kernel_config.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]

@@ -213,6 +213,11 @@ struct swe_ctx {
     Dims dims{};
     int device = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
+    // advective operator: a second stream and events for the stage's independent
+    // kernels (h averaging, wind halo, wind at the vertices), forked off the stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_havg = nullptr, ev_co2 = nullptr, ev_side = nullptr;
+    bool branches = true;            // fork the advective stage (when the side stream exists); autotuned
     std::string err;
     long long launches = 0;
     size_t elem = 8;                 // bytes per element
@@ -762,6 +767,17 @@ extern "C" int swe_cfg_default(swe_cfg *cfg)
     return SWE_OK;
 }
 
+// The advective stage forks its independent kernels onto a second stream;
+// CHSWE_ADV_BRANCHES=0 in the environment keeps the whole stage on one stream.
+static bool adv_branches_enabled()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("CHSWE_ADV_BRANCHES");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 static void free_ctx(swe_ctx *c)
 {
     if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -774,6 +790,9 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    for (cudaEvent_t e : {c->ev_fork, c->ev_havg, c->ev_co2, c->ev_side})
+        if (e) cudaEventDestroy(e);
 }
 
 static int alloc_box(swe_ctx *c, void **p)
@@ -869,6 +888,11 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
                 return bail(SWE_ECUDA);
             rc = cfg->precision == SWE_FP64 ? build_adv_tables<double>(c, c->a64) : build_adv_tables<float>(c, c->a32);
             if (rc != SWE_OK) return bail(rc);
+            if (adv_branches_enabled()) {
+                if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) return bail(SWE_ECUDA);
+                for (cudaEvent_t *e : {&c->ev_fork, &c->ev_havg, &c->ev_co2, &c->ev_side})
+                    if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return bail(SWE_ECUDA);
+            }
         }
     }
     if (cudaHostAlloc((void **)&c->pinned, c->box_elems * c->elem, cudaHostAllocDefault) != cudaSuccess)
@@ -1183,8 +1207,9 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
         c->launches += 2;
         return;
     }
-    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream, dtm);
     if (!c->adv) {
+        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm);
         launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
@@ -1198,15 +1223,40 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     const AdvView<T> &av = adv_view<T>(c);
     const int N = c->cfg.N, n = N + 1;
     const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
-    launch_k(k_havg<T>, dim3(1 + (12 * (N - 1) + HAVG_THREADS - 1) / HAVG_THREADS, M), dim3(HAVG_THREADS), 0, c->stream,
-             (T *)yin, (T *)c->hb, c->dims, dtm);
+    const dim3 hg(1 + (12 * (N - 1) + HAVG_THREADS - 1) / HAVG_THREADS, M);
+    const long long nvh = (long long)NPAN * av.hp * M;
+    const dim3 vg((unsigned)((nvh + 255) / 256));
+    const bool fork = c->side && c->branches;
+    if (fork) {
+        // The averaging of h and the wind halo depend on the stage input only, the
+        // wind at the vertices on k_co2contra: they run on the side stream beside
+        // k_co2contra, k_flux and k_edge, and join before k_adv.
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->side, (T *)yin, (T *)c->hb, c->dims, dtm);
+        cudaEventRecord(c->ev_havg, c->side);
+        launch_k(k_vhalo<T>, vg, dim3(256), 0, c->side, (const T *)yin, (T *)c->vh, c->dims, av, M, dtm);
+        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm);
+        cudaEventRecord(c->ev_co2, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_co2, 0);
+        launch_k(k_uhvh<T>, pg, pb, 0, c->side, (const T *)c->w, (T *)c->ph, c->dims, dtm);
+        cudaEventRecord(c->ev_side, c->side);
+        cudaStreamWaitEvent(c->stream, c->ev_havg, 0);
+    } else {
+        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm);
+        launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->stream, (T *)yin, (T *)c->hb, c->dims, dtm);
+    }
     launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
     launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
              (T *)c->edge, c->dims, mv, dtm);
-    launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
-    const long long nvh = (long long)NPAN * av.hp * M;
-    launch_k(k_vhalo<T>, dim3((unsigned)((nvh + 255) / 256)), dim3(256), 0, c->stream, (const T *)yin, (T *)c->vh,
-             c->dims, av, M, dtm);
+    if (fork) {
+        cudaStreamWaitEvent(c->stream, c->ev_side, 0);
+    } else {
+        launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
+        launch_k(k_vhalo<T>, vg, dim3(256), 0, c->stream, (const T *)yin, (T *)c->vh, c->dims, av, M, dtm);
+    }
     launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
              (T *)c->adt, c->dims, av, mv, dtm);
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
@@ -1756,11 +1806,56 @@ __device__ __forceinline__ double xy_nb(const T *Y, const Dims &d, int t, int s,
     return (double)gview(Y, d, 0, L.nb)(k, l);
 }
 
-// get_ecs_halo + ext_ecs_tile_halo on one panel (ecs_halo_xy_mod.f90:66-235), evaluated
-// point by point: the extended panel (indices 1-LL_HW .. N+1+LL_HW) with the averaged
-// duplicated vertices, the corner diagonals and the rows / columns of virtual points
-// interpolated along the neighbours' grid lines (cubic Lagrange, weights wt / lines kt
-// per depth and along index).  FP64 into ext[panel][j][i].
+// ext_ecs_tile_halo (ecs_halo_xy_mod.f90:109-235) at one point (i, j) of the extended
+// panel (indices 1-LL_HW .. N+1+LL_HW): the averaged duplicated vertices, the corner
+// diagonals and the rows / columns of virtual points interpolated along the
+// neighbours' grid lines (cubic Lagrange, weights wt / lines kt per depth and along
+// index).  raw: the panel's own value at (i, j) when inside; X(s, depth, a): the
+// exchange's halo value across side s at that depth and along index a.
+template <class RAW, class XF>
+__device__ __forceinline__ double ecs_ext_point(int i, int j, int n, const int *kt, const double *wt, const RAW &raw,
+                                                const XF &X)
+{
+    // corner diagonals at offset m (1..LL_HW) from the four corner vertices
+    auto DBL = [&](int m) { return 0.5 * (X(SIDE_L, m, 1) + X(SIDE_B, m, 1)); };
+    auto DBR = [&](int m) { return 0.5 * (X(SIDE_R, m, 1) + X(SIDE_B, m, n)); };
+    auto DTR = [&](int m) { return 0.5 * (X(SIDE_R, m, n) + X(SIDE_T, m, n)); };
+    auto DTL = [&](int m) { return 0.5 * (X(SIDE_T, m, 1) + X(SIDE_L, m, n)); };
+    // the neighbour's grid line at depth m along side s, its ends replaced by the diagonals
+    auto line = [&](int s, int m, int b) {
+        if (b == 1) return s == SIDE_R ? DBR(m) : (s == SIDE_T ? DTL(m) : DBL(m));
+        if (b == n) return s == SIDE_L ? DTL(m) : (s == SIDE_B ? DBR(m) : DTR(m));
+        return X(s, m, b);
+    };
+    auto virt = [&](int s, int m, int a) {
+        const int row = (m - 1) * (n + 2) + a;   // a in 2-m .. n+m-1, i.e. 0 .. n+1
+        const int k = kt[row];
+        const double *w = wt + 4 * row;
+        return w[0] * line(s, m, k - 1) + w[1] * line(s, m, k) + w[2] * line(s, m, k + 1) + w[3] * line(s, m, k + 2);
+    };
+    if (i >= 1 && i <= n && j >= 1 && j <= n) {
+        const double r = raw();
+        const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
+        if (il && jb) return (r + X(SIDE_B, 0, 1) + X(SIDE_L, 0, 1)) / 3.0;
+        if (ir && jb) return (r + X(SIDE_B, 0, n) + X(SIDE_R, 0, 1)) / 3.0;
+        if (ir && jt) return (r + X(SIDE_T, 0, n) + X(SIDE_R, 0, n)) / 3.0;
+        if (il && jt) return (r + X(SIDE_L, 0, n) + X(SIDE_T, 0, 1)) / 3.0;
+        if (jb) return 0.5 * (r + X(SIDE_B, 0, i));
+        if (jt) return 0.5 * (r + X(SIDE_T, 0, i));
+        if (il) return 0.5 * (r + X(SIDE_L, 0, j));
+        if (ir) return 0.5 * (r + X(SIDE_R, 0, j));
+        return r;
+    }
+    if (j < 1 && i >= 2 - (1 - j) && i <= n + (1 - j) - 1) return virt(SIDE_B, 1 - j, i);
+    if (j > n && i >= 2 - (j - n) && i <= n + (j - n) - 1) return virt(SIDE_T, j - n, i);
+    if (i < 1 && j >= 2 - (1 - i) && j <= n + (1 - i) - 1) return virt(SIDE_L, 1 - i, j);
+    if (i > n && j >= 2 - (i - n) && j <= n + (i - n) - 1) return virt(SIDE_R, i - n, j);
+    if (i < 1) return j < 1 ? DBL(1 - i) : DTL(1 - i);
+    return j < 1 ? DBR(i - n) : DTR(i - n);
+}
+
+// get_ecs_halo (ecs_halo_xy_mod.f90:66-107) of h on every panel: the xy exchange's
+// values (xy_nb) and ext_ecs_tile_halo at every point.  FP64 into ext[panel][j][i].
 template <class T>
 __global__ void k_ecs_xy_ext(const T *__restrict__ y, Dims d, const int *__restrict__ kt,
                              const double *__restrict__ wt, double *__restrict__ ext)
@@ -1770,51 +1865,55 @@ __global__ void k_ecs_xy_ext(const T *__restrict__ y, Dims d, const int *__restr
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
         const int t = (int)(q / ((int64_t)E * E)), r = (int)(q % ((int64_t)E * E));
         const int j = r / E + 1 - LL_HW, i = r % E + 1 - LL_HW;
-        auto X = [&](int s, int depth, int a) { return xy_nb(y, d, t, s, depth, a); };
-        // corner diagonals at offset m (1..LL_HW) from the four corner vertices
-        auto DBL = [&](int m) { return 0.5 * (X(SIDE_L, m, 1) + X(SIDE_B, m, 1)); };
-        auto DBR = [&](int m) { return 0.5 * (X(SIDE_R, m, 1) + X(SIDE_B, m, n)); };
-        auto DTR = [&](int m) { return 0.5 * (X(SIDE_R, m, n) + X(SIDE_T, m, n)); };
-        auto DTL = [&](int m) { return 0.5 * (X(SIDE_T, m, 1) + X(SIDE_L, m, n)); };
-        // the neighbour's grid line at depth m along side s, its ends replaced by the diagonals
-        auto line = [&](int s, int m, int b) {
-            if (b == 1) return s == SIDE_R ? DBR(m) : (s == SIDE_T ? DTL(m) : DBL(m));
-            if (b == n) return s == SIDE_L ? DTL(m) : (s == SIDE_B ? DBR(m) : DTR(m));
-            return X(s, m, b);
-        };
-        auto virt = [&](int s, int m, int a) {
-            const int row = (m - 1) * (n + 2) + a;   // a in 2-m .. n+m-1, i.e. 0 .. n+1
-            const int k = kt[row];
-            const double *w = wt + 4 * row;
-            return w[0] * line(s, m, k - 1) + w[1] * line(s, m, k) + w[2] * line(s, m, k + 1) + w[3] * line(s, m, k + 2);
-        };
-        double v;
-        if (i >= 1 && i <= n && j >= 1 && j <= n) {
-            const double raw = (double)gview(y, d, 0, t)(i, j);
-            const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
-            if (il && jb) v = (raw + X(SIDE_B, 0, 1) + X(SIDE_L, 0, 1)) / 3.0;
-            else if (ir && jb) v = (raw + X(SIDE_B, 0, n) + X(SIDE_R, 0, 1)) / 3.0;
-            else if (ir && jt) v = (raw + X(SIDE_T, 0, n) + X(SIDE_R, 0, n)) / 3.0;
-            else if (il && jt) v = (raw + X(SIDE_L, 0, n) + X(SIDE_T, 0, 1)) / 3.0;
-            else if (jb) v = 0.5 * (raw + X(SIDE_B, 0, i));
-            else if (jt) v = 0.5 * (raw + X(SIDE_T, 0, i));
-            else if (il) v = 0.5 * (raw + X(SIDE_L, 0, j));
-            else if (ir) v = 0.5 * (raw + X(SIDE_R, 0, j));
-            else v = raw;
-        } else if (j < 1 && i >= 2 - (1 - j) && i <= n + (1 - j) - 1) {
-            v = virt(SIDE_B, 1 - j, i);
-        } else if (j > n && i >= 2 - (j - n) && i <= n + (j - n) - 1) {
-            v = virt(SIDE_T, j - n, i);
-        } else if (i < 1 && j >= 2 - (1 - i) && j <= n + (1 - i) - 1) {
-            v = virt(SIDE_L, 1 - i, j);
-        } else if (i > n && j >= 2 - (i - n) && j <= n + (i - n) - 1) {
-            v = virt(SIDE_R, i - n, j);
-        } else if (i < 1) {
-            v = j < 1 ? DBL(1 - i) : DTL(1 - i);
-        } else {
-            v = j < 1 ? DBR(i - n) : DTR(i - n);
+        ext[q] = ecs_ext_point(
+            i, j, n, kt, wt, [&]() { return (double)gview(y, d, 0, t)(i, j); },
+            [&](int s, int depth, int a) { return xy_nb(y, d, t, s, depth, a); });
+    }
+}
+
+// The covariant wind at vertex (k, l) of panel p, interpolated from the Ch points
+// (interp2d_uv2pvec_Ch_sbp42: the c2i interpolation of u along x, of v along y).
+template <class T>
+__device__ __forceinline__ void uv_at_vertex(const T *y, const Dims &d, int p, int k, int l, double &u, double &v)
+{
+    const int n = d.N + 1;
+    const GV<T> U = gview(y, d, 1, p), V = gview(y, d, 2, p);
+    u = ic2i<double>(k, n, [&](int c) { return (double)U(c, l); });
+    v = ic2i<double>(l, n, [&](int c) { return (double)V(k, c); });
+}
+
+// The covariant ecs_xy_vec halo of the wind (ecs_halo_vec_xy_mod.f90:30-98) on every
+// panel: at each halo point the neighbour's vertex wind as the vector exchange hands
+// it over (halo_vec), turned into this panel's components by the transform matrix
+// of the edge, depth and along index (tm: [edge B, T, L, R][depth 0..LL_HW][a 1..n][4]);
+// then ext_ecs_tile_halo of each component.  FP64 into extu, extv.
+template <class T>
+__global__ void k_ecs_vec_ext(const T *__restrict__ y, Dims d, const int *__restrict__ kt,
+                              const double *__restrict__ wt, const double *__restrict__ tm, double *__restrict__ extu,
+                              double *__restrict__ extv)
+{
+    const int N = d.N, n = N + 1, E = ll_pitch(N);
+    const int64_t npts = (int64_t)NPAN * E * E;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(q / ((int64_t)E * E)), r = (int)(q % ((int64_t)E * E));
+        const int j = r / E + 1 - LL_HW, i = r % E + 1 - LL_HW;
+        double uo = 0.0, vo = 0.0;
+        if (i >= 1 && i <= n && j >= 1 && j <= n) uv_at_vertex(y, d, t, i, j, uo, vo);
+        for (int comp = 0; comp < 2; comp++) {
+            auto X = [&](int s, int depth, int a) {
+                const Link L = c_link[t][s];
+                int k, l;
+                side_vertex(N, L.nside, L.rev ? n + 1 - a : a, depth, k, l);
+                double un, vn, uh, vh;
+                uv_at_vertex(y, d, L.nb, k, l, un, vn);
+                halo_vec<double>(t, s, un, vn, uh, vh);
+                const int e = s == SIDE_B ? 0 : (s == SIDE_T ? 1 : (s == SIDE_L ? 2 : 3));
+                const double *M = tm + ((e * (LL_HW + 1) + depth) * n + (a - 1)) * 4;
+                return comp == 0 ? M[0] * uh + M[1] * vh : M[2] * uh + M[3] * vh;
+            };
+            const double v = ecs_ext_point(i, j, n, kt, wt, [&]() { return comp == 0 ? uo : vo; }, X);
+            (comp == 0 ? extu : extv)[q] = v;
         }
-        ext[q] = v;
     }
 }
 
@@ -1835,19 +1934,115 @@ __global__ void k_latlon(const double *__restrict__ ext, const int *__restrict__
     }
 }
 
+// do_latlon_vector_regrid (latlon_regrid_mod.f90:132-212): the stencils of both
+// components and their rotation to the eastward / northward components
+// (q: [iv.b1, iv.b2, jv.b1, jv.b2] per point).
+__global__ void k_latlon_vec(const double *__restrict__ extu, const double *__restrict__ extv,
+                             const int *__restrict__ idx, const double *__restrict__ w, const double *__restrict__ qr,
+                             int N, int64_t npts, double *__restrict__ uo, double *__restrict__ vo)
+{
+    const int E = ll_pitch(N);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
+        const int t = idx[3 * q], xi = idx[3 * q + 1], yi = idx[3 * q + 2];
+        const double *wx = w + 8 * q, *wy = wx + 4;
+        const int64_t base = ((int64_t)t * E + (yi + LL_HW - 1)) * E + (xi + LL_HW - 1);
+        double au = 0.0, av = 0.0;
+        for (int b = -1; b <= 2; b++)
+            for (int a = -1; a <= 2; a++) {
+                au = au + wx[a + 1] * wy[b + 1] * extu[base + b * E + a];
+                av = av + wx[a + 1] * wy[b + 1] * extv[base + b * E + a];
+            }
+        const double *Q = qr + 4 * q;
+        uo[q] = Q[0] * au + Q[1] * av;
+        vo[q] = Q[2] * au + Q[3] * av;
+    }
+}
+
 // Point location and cubic weights (distribute_latlon_points_to_cubsphere,
 // regrid_factory_mod.f90:165-262; init_interpolation, latlon_regrid_mod.f90:286-336;
 // latlon_grid_generator_t%init / get_cartesian_coords) and the ECS_xy halo weights
 // (init_halo_xy_interp, ecs_halo_factory_mod.f90:236-270), built on the host in FP64.
+// Layout of the lat-lon regrid's device tables (ll_i ints, ll_d doubles).
+struct LatlonLayout {
+    size_t np, nrow, ntm, next;
+    // ints: idx (3 per point), kt (nrow)
+    size_t i_kt() const { return 3 * np; }
+    size_t ints() const { return 3 * np + nrow; }
+    // doubles: w (8 per point), qrot (4 per point), wt (4 per row), tm, ext u/h, ext v, out u/h, out v
+    size_t d_q() const { return 8 * np; }
+    size_t d_wt() const { return 12 * np; }
+    size_t d_tm() const { return d_wt() + 4 * nrow; }
+    size_t d_ext() const { return d_tm() + ntm; }
+    size_t d_out() const { return d_ext() + 2 * next; }
+    size_t doubles() const { return d_out() + 2 * np; }
+};
+static LatlonLayout latlon_layout(int N, int nlat, int nlon)
+{
+    const int n = N + 1, E = ll_pitch(N);
+    LatlonLayout L;
+    L.np = (size_t)nlat * nlon;
+    L.nrow = (size_t)LL_HW * (n + 2);
+    L.ntm = (size_t)4 * (LL_HW + 1) * n * 4;
+    L.next = (size_t)NPAN * E * E;
+    return L;
+}
+
+// init_transform_matrix for covariant components (ecs_halo_vec_xy_factory_mod.f90:103-186):
+// at halo row j (1: the neighbour's copy of the edge row) and along index i of edge e
+// (1 bottom, 2 top, 3 left, 4 right), the matrix taking the neighbour's covariant
+// components, as the vector exchange hands them over, to this panel's.
+static void xy_vec_tm(int e, int i, int j, double hx, double TM[4])
+{
+    static const int rot[4][3][3] = {{{1, 0, 0}, {0, 0, -1}, {0, 1, 0}},
+                                     {{1, 0, 0}, {0, 0, 1}, {0, -1, 0}},
+                                     {{0, 0, -1}, {0, 1, 0}, {1, 0, 0}},
+                                     {{0, 0, 1}, {0, 1, 0}, {-1, 0, 0}}};
+    static const int ab_shift[4] = {0, 0, 1, 1}, b_sign[4] = {1, -1, 1, -1};
+    const double pi = 3.141592653589793238462643383279502884;
+    const int q = e - 1;
+    const double alpha = -0.25 * pi + (i - 1.0) * hx;
+    const double beta = b_sign[q] * (0.25 * pi - (j - 1.0) * hx);
+    const double as = (1 - ab_shift[q]) * alpha + ab_shift[q] * beta;
+    const double bs = ab_shift[q] * alpha + (1 - ab_shift[q]) * beta;
+    auto rotate = [&](const double v[3], double out[3]) {
+        for (int d = 0; d < 3; d++) out[d] = rot[q][d][0] * v[0] + rot[q][d][1] * v[1] + rot[q][d][2] * v[2];
+    };
+    double v[3], a1s[3], a2s[3], r[3], b1t[3], b2t[3];
+    b1p(as, bs, v);
+    rotate(v, a1s);
+    b2p(as, bs, v);
+    rotate(v, a2s);
+    const double ta = std::tan(as), tb = std::tan(bs);
+    v[0] = ta / std::sqrt(1.0 + std::pow(ta, 2.0) + std::pow(tb, 2.0));
+    v[1] = tb / std::sqrt(1.0 + std::pow(ta, 2.0) + std::pow(tb, 2.0));
+    v[2] = 1.0 / std::sqrt(1.0 + std::pow(ta, 2.0) + std::pow(tb, 2.0));
+    rotate(v, r);
+    const double at = std::atan(r[0] / r[2]), bt = std::atan(r[1] / r[2]);
+    a1p(at, bt, b1t);
+    a2p(at, bt, b2t);
+    TM[0] = a1s[0] * b1t[0] + a1s[1] * b1t[1] + a1s[2] * b1t[2];
+    TM[1] = a2s[0] * b1t[0] + a2s[1] * b1t[1] + a2s[2] * b1t[2];
+    TM[2] = a1s[0] * b2t[0] + a1s[1] * b2t[1] + a1s[2] * b2t[2];
+    TM[3] = a2s[0] * b2t[0] + a2s[1] * b2t[1] + a2s[2] * b2t[2];
+}
+
+// Point location and cubic weights (distribute_latlon_points_to_cubsphere,
+// regrid_factory_mod.f90:165-262; init_interpolation, latlon_regrid_mod.f90:286-336;
+// latlon_grid_generator_t%init / get_cartesian_coords / get_basis_vectors), the
+// rotation to lat-lon components (init_transform_to_latlon_vec_tile,
+// regrid_factory_mod.f90:324-370), the ECS_xy halo weights (init_halo_xy_interp,
+// ecs_halo_factory_mod.f90:236-270) and the vector halo's transform matrices, built
+// on the host in FP64.
 static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
 {
     if (c->ll_i && c->ll_nlat == nlat && c->ll_nlon == nlon) return SWE_OK;
     cudaFree(c->ll_i); cudaFree(c->ll_d);
     c->ll_i = nullptr; c->ll_d = nullptr; c->ll_nlat = c->ll_nlon = 0;
-    const int N = c->cfg.N, n = N + 1, E = ll_pitch(N);
-    const size_t np = (size_t)nlat * nlon, nrow = (size_t)LL_HW * (n + 2);
-    std::vector<int> hi(3 * np + nrow, 0);
-    std::vector<double> hd(8 * np + 4 * nrow, 0.0);
+    const int N = c->cfg.N, n = N + 1;
+    const LatlonLayout Lo = latlon_layout(N, nlat, nlon);
+    const size_t np = Lo.np;
+    std::vector<int> hi(Lo.ints(), 0);
+    std::vector<double> hd(Lo.d_ext(), 0.0);
     const double pi = 3.141592653589793238462643383279502884;
     const double hx = 0.5 * pi / N, a0 = -0.25 * pi;
     for (int j = 1; j <= nlat; j++) {
@@ -1876,16 +2071,32 @@ static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
             // the stencil (indices xi-1 .. xi+2) stays inside the extended panel
             if (t < 0 || t >= NPAN || xi < 0 || xi > n || yi < 0 || yi > n)
                 return fail(c, SWE_EINVAL, "lat-lon point (%d, %d) outside the cube panels", i, j);
+            // q = [iv.b1, iv.b2; jv.b1, jv.b2] with the panel's contravariant basis b1, b2
+            const double iv[3] = {-std::sin(lam), std::cos(lam), 0.0};
+            const double jv[3] = {-std::sin(phi) * std::cos(lam), -std::sin(phi) * std::sin(lam), std::cos(phi)};
+            double p1[3], p2[3], b1[3], b2[3];
+            b1p(alpha, beta, p1);
+            b2p(alpha, beta, p2);
+            p2r(t, p1, b1);
+            p2r(t, p2, b2);
+            double *Q = &hd[Lo.d_q() + 4 * q];
+            Q[0] = iv[0] * b1[0] + iv[1] * b1[1] + iv[2] * b1[2];
+            Q[1] = iv[0] * b2[0] + iv[1] * b2[1] + iv[2] * b2[2];
+            Q[2] = jv[0] * b1[0] + jv[1] * b1[1] + jv[2] * b1[2];
+            Q[3] = jv[0] * b2[0] + jv[1] * b2[1] + jv[2] * b2[2];
         }
     }
     for (int m = 1; m <= LL_HW; m++)
         for (int a = 2 - m; a <= n + m - 1; a++) {
             const size_t row = (size_t)(m - 1) * (n + 2) + a;
-            halo_xy_weights(n, hx, a, m, &hd[8 * np + 4 * row], hi[3 * np + row]);
+            halo_xy_weights(n, hx, a, m, &hd[Lo.d_wt() + 4 * row], hi[Lo.i_kt() + row]);
         }
-    const size_t nd = hd.size() + (size_t)NPAN * E * E + np;
+    for (int e = 0; e < 4; e++)
+        for (int dep = 0; dep <= LL_HW; dep++)
+            for (int a = 1; a <= n; a++)
+                xy_vec_tm(e + 1, a, dep + 1, hx, &hd[Lo.d_tm() + ((size_t)(e * (LL_HW + 1) + dep) * n + (a - 1)) * 4]);
     if (cudaMalloc(&c->ll_i, hi.size() * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&c->ll_d, nd * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&c->ll_d, Lo.doubles() * sizeof(double)) != cudaSuccess) {
         cudaFree(c->ll_i); c->ll_i = nullptr; c->ll_d = nullptr;
         return fail(c, SWE_ENOMEM, "lat-lon regrid allocation failed");
     }
@@ -1905,15 +2116,14 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
         return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
     int rc = ensure_latlon(c, nlat, nlon);
     if (rc != SWE_OK) return rc;
-    const int N = c->cfg.N, n = N + 1, E = ll_pitch(N);
-    const int64_t np = (int64_t)nlat * nlon;
-    const size_t nrow = (size_t)LL_HW * (n + 2);
-    const int *kt = c->ll_i + 3 * np;
-    const double *wt = c->ll_d + 8 * np;
-    double *ext = c->ll_d + 8 * np + 4 * nrow, *dout = ext + (size_t)NPAN * E * E;
+    const int N = c->cfg.N;
+    const LatlonLayout Lo = latlon_layout(N, nlat, nlon);
+    const int64_t np = (int64_t)Lo.np;
+    const int *kt = c->ll_i + Lo.i_kt();
+    const double *wt = c->ll_d + Lo.d_wt();
+    double *ext = c->ll_d + Lo.d_ext(), *dout = c->ll_d + Lo.d_out();
     const size_t mo = (size_t)member * c->dims.ms;
-    const int64_t next = (int64_t)NPAN * E * E;
-    const dim3 b(256), g1((unsigned)std::min<int64_t>((next + 255) / 256, 8192)),
+    const dim3 b(256), g1((unsigned)std::min<int64_t>(((int64_t)Lo.next + 255) / 256, 8192)),
         g2((unsigned)std::min<int64_t>((np + 255) / 256, 8192));
     if (c->elem == 8) k_ecs_xy_ext<double><<<g1, b, 0, c->stream>>>((const double *)vec->d + mo, c->dims, kt, wt, ext);
     else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)vec->d + mo, c->dims, kt, wt, ext);
@@ -1921,6 +2131,38 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
     c->launches += 2;
     CU(c, cudaGetLastError());
     CU(c, cudaMemcpyAsync(out, dout, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+extern "C" int swe_regrid_latlon_wind(swe_ctx *c, const swe_stvec *vec, int member, int nlat, int nlon, double *u_out,
+                                      double *v_out)
+{
+    if (!c || !vec || vec->ctx != c || !u_out || !v_out || member < 0 || member >= c->cfg.n_members)
+        return SWE_EINVAL;
+    if (c->ah) return fail(c, SWE_EINVAL, "swe_regrid_latlon_wind: built for the Ch staggering");
+    if (nlat < 2 || nlon < 1 || (int64_t)nlat * nlon > (1 << 28))
+        return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
+    int rc = ensure_latlon(c, nlat, nlon);
+    if (rc != SWE_OK) return rc;
+    const int N = c->cfg.N;
+    const LatlonLayout Lo = latlon_layout(N, nlat, nlon);
+    const int64_t np = (int64_t)Lo.np;
+    const int *kt = c->ll_i + Lo.i_kt();
+    const double *wt = c->ll_d + Lo.d_wt(), *tm = c->ll_d + Lo.d_tm(), *qr = c->ll_d + Lo.d_q();
+    double *extu = c->ll_d + Lo.d_ext(), *extv = extu + Lo.next;
+    double *uo = c->ll_d + Lo.d_out(), *vo = uo + np;
+    const size_t mo = (size_t)member * c->dims.ms;
+    const dim3 b(256), g1((unsigned)std::min<int64_t>(((int64_t)Lo.next + 255) / 256, 8192)),
+        g2((unsigned)std::min<int64_t>((np + 255) / 256, 8192));
+    if (c->elem == 8)
+        k_ecs_vec_ext<double><<<g1, b, 0, c->stream>>>((const double *)vec->d + mo, c->dims, kt, wt, tm, extu, extv);
+    else k_ecs_vec_ext<float><<<g1, b, 0, c->stream>>>((const float *)vec->d + mo, c->dims, kt, wt, tm, extu, extv);
+    k_latlon_vec<<<g2, b, 0, c->stream>>>(extu, extv, c->ll_i, c->ll_d, qr, N, np, uo, vo);
+    c->launches += 2;
+    CU(c, cudaGetLastError());
+    CU(c, cudaMemcpyAsync(u_out, uo, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(c, cudaMemcpyAsync(v_out, vo, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
 }
@@ -2272,6 +2514,7 @@ struct TuneEntry {
     TuneKey key;
     int tile, occ, runs;
     double ms[3];
+    bool branches;
 };
 std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
 }  // namespace
@@ -2294,6 +2537,8 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {
             set_cfg(c, e.tile, e.occ, e.runs);
+            if (c->branches != e.branches) drop_graph(c);
+            c->branches = e.branches;
             if (best_tile) *best_tile = e.tile;
             if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = e.ms[k];
             return SWE_OK;
@@ -2315,7 +2560,8 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
         const KernelCfg kc = cfgs[k];
         if (c->adv && kc.occ != default_occ(kc.tile)) continue;
         set_cfg(c, kc.tile, kc.occ, kc.runs);
-        if ((rc = swe_rk4_steps(c, v, dt, 2)) != SWE_OK) break;
+        // untimed: the same step counts capture and instantiate the graphs
+        if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
         if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
         if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
         float t = 0.f;
@@ -2329,13 +2575,35 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
         ms[ti] = std::min(ms[ti], m);
         if (m < best_ms) { best_ms = m; best_t = kc.tile; best_o = kc.occ; best_r = kc.runs; }
     }
+    // advective operator: the best configuration with the stage forked onto the side
+    // stream and on one stream (forking pays for small cubes, not always for C384)
+    bool best_b = c->branches;
+    if (rc == SWE_OK && c->side) {
+        set_cfg(c, best_t, best_o, best_r);
+        double tb[2] = {1e300, 1e300};
+        for (int b = 0; b < 2 && rc == SWE_OK; b++) {
+            drop_graph(c);
+            c->branches = b == 1;
+            if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
+            float t = 0.f;
+            if (cudaEventRecord(e0, c->stream) != cudaSuccess || swe_rk4_steps(c, v, dt, nreps) != SWE_OK ||
+                cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+                rc = fail(c, SWE_ECUDA, "autotune timing");
+                break;
+            }
+            tb[b] = t / nreps;
+        }
+        best_b = tb[1] <= tb[0];
+        c->branches = best_b;
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     swe_stvec_destroy(v);
     drop_graph(c);
     if (rc != SWE_OK) { set_cfg(c, keep_tile, keep_occ, keep_runs); return rc; }
     set_cfg(c, best_t, best_o, best_r);
-    TuneEntry te{key, best_t, best_o, best_r, {ms[0], ms[1], ms[2]}};
+    TuneEntry te{key, best_t, best_o, best_r, {ms[0], ms[1], ms[2]}, best_b};
     g_tuned.push_back(te);
     if (best_tile) *best_tile = best_t;
     if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = ms[k];

@@ -98,6 +98,33 @@ class LatlonOutputer:
         return f
 
 
+class LatlonVecOutputer:
+    """latlon_vec_outputer_t for the covariant Ch wind (latlon_outputer_mod.f90:55-85): the
+    regrid on the device (swe_regrid_latlon_wind) to eastward / northward components on
+    nlat x nlon points (default 2N+1 x 4N) and one real*4 record per file per write."""
+
+    def __init__(self, domain, nlat: int | None = None, nlon: int | None = None):
+        self.domain = domain
+        self.nlat = 2 * domain.N + 1 if nlat is None else int(nlat)
+        self.nlon = 4 * domain.N if nlon is None else int(nlon)
+
+    def regrid(self, state, member: int = 0):
+        """(u, v) on the lat-lon grid, each (nlat, nlon) in FP64, longitude fastest."""
+        u = np.empty((self.nlat, self.nlon))
+        v = np.empty((self.nlat, self.nlon))
+        dp = ctypes.POINTER(ctypes.c_double)
+        check(_lib.load().swe_regrid_latlon_wind(self.domain.ctx, state.handle, int(member), self.nlat, self.nlon,
+                                                 u.ctypes.data_as(dp), v.ctypes.data_as(dp)),
+              self.domain.ctx, "swe_regrid_latlon_wind")
+        return u, v
+
+    def write(self, state, path_u: str, path_v: str, rec: int = 1, member: int = 0):
+        u, v = self.regrid(state, member)
+        write_latlon(path_u, u, rec)
+        write_latlon(path_v, v, rec)
+        return u, v
+
+
 def write_latlon(path: str, field: np.ndarray, rec: int = 1) -> None:
     """One record of latlon_outputer_t%write: real(f_latlon, 4) with f_latlon(Nlon, Nlat),
     longitude fastest, record length nlat * nlon values.  field: (nlat, nlon)."""

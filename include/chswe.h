@@ -168,6 +168,17 @@ int swe_curl(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
 int swe_regrid_latlon(swe_ctx *ctx, const swe_stvec *vec, int member, int field, int nlat, int nlon,
                       double *out);
 
+/* Cubic lat-lon regrid of the covariant wind of one member (Ch), the values that
+   latlon_vec_outputer_t%write puts in the u.dat / v.dat records
+   (latlon_outputer_mod.f90:55-85, regrid_factory_mod.f90:72-163,
+   latlon_regrid_mod.f90:132-212): u, v interpolated to the vertices
+   (interp2d_uv2pvec_Ch_sbp42), the covariant ecs_xy_vec halo of width 2
+   (ecs_halo_vec_xy_mod.f90:30-98), the cubic stencils and the rotation to the
+   eastward / northward components.  u_out, v_out [nlat][nlon] in FP64, longitude
+   fastest.  Synchronous. */
+int swe_regrid_latlon_wind(swe_ctx *ctx, const swe_stvec *vec, int member, int nlat, int nlon, double *u_out,
+                           double *v_out);
+
 /* Number of kernel launches issued on the context's stream since creation. */
 long long swe_launch_count(const swe_ctx *ctx);
 

@@ -70,6 +70,7 @@ def lib():
         L.orc_ah_apply.argtypes = [ctypes.c_void_p] + [_dp] * 6
         L.orc_ah_rk4.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int]
         L.orc_ah_integrals.argtypes = [ctypes.c_void_p] + [_dp] * 5
+        L.orc_latlon_vec.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_latlon_xy.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
         _lib = L
     return _lib
@@ -160,6 +161,17 @@ class Oracle:
         out = np.zeros((nlat, nlon))
         lib().orc_latlon_xy(self._c, _p(np.ascontiguousarray(f, dtype=np.float64)), nlat, nlon, _p(out))
         return out
+
+    def latlon_vec(self, u, v, nlat=None, nlon=None):
+        """Cubic lat-lon regrid of the covariant Ch wind (latlon_vec_outputer_t): the
+        eastward and northward components, each (nlat, nlon)."""
+        nlat = 2 * self.N + 1 if nlat is None else int(nlat)
+        nlon = 4 * self.N if nlon is None else int(nlon)
+        uo = np.zeros((nlat, nlon))
+        vo = np.zeros((nlat, nlon))
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v)]
+        lib().orc_latlon_vec(self._c, _p(a[0]), _p(a[1]), nlat, nlon, _p(uo), _p(vo))
+        return uo, vo
 
     def energies(self, h, u, v):
         """(TE, KE, PE, enstrophy) of swm_output_diag_t%calc_energies (covariant u, v)."""

@@ -1240,11 +1240,18 @@ static double halo_xy_line(int n, double dxa, int i, int j, const double *zf)
    (one tile per panel): the exchange, then corner diagonals and the averaging of
    the duplicated vertices, then rows / columns of interpolated virtual points.
    Modifies the interior edge and corner values of f, as the reference does. */
+static void ecs_xy_interp(orc_ctx *c, fld_t *f, int hw);
 static void ecs_xy_halo(orc_ctx *c, fld_t *f, int hw)
+{
+    exch_do(&c->ex_xy5_full_s, f, NULL);
+    ecs_xy_interp(c, f, hw);
+}
+
+/* ecs_tile_halo_xy_t%interp (ecs_halo_xy_mod.f90:109-235): the part after the exchange */
+static void ecs_xy_interp(orc_ctx *c, fld_t *f, int hw)
 {
     int n = c->N + 1;
     double dxa = c->mxy.hx;
-    exch_do(&c->ex_xy5_full_s, f, NULL);
     double *zb = malloc(sizeof(double) * (n + 2 * hw + 8));
     double *zl = zb + hw + 2;   /* zl[b], b = 1 - hw - 2 .. n + hw + 4 */
     for (int t = 0; t < NPAN; t++) {
@@ -2040,6 +2047,140 @@ void orc_ah_integrals(orc_ctx *c, const double *h, const double *u, const double
     free(A);
     if (mass) *mass = sm;
     if (energy) *energy = 0.5 * c->H * se + 0.5 * c->g * sh;
+}
+
+/* init_transform_matrix (ecs_halo_vec_xy_factory_mod.f90:103-186), covariant
+   components: for halo row j (1 = the neighbour's copy of the edge row) at along
+   index i of edge e (1 bottom, 2 top, 3 left, 4 right), the 2 x 2 matrix taking the
+   neighbour's covariant components (as the exchange delivers them) to this panel's. */
+static void xy_vec_tm(int e, int i, int j, double hx, double TM[4])
+{
+    static const int rot[4][3][3] = {{{1, 0, 0}, {0, 0, -1}, {0, 1, 0}},
+                                     {{1, 0, 0}, {0, 0, 1}, {0, -1, 0}},
+                                     {{0, 0, -1}, {0, 1, 0}, {1, 0, 0}},
+                                     {{0, 0, 1}, {0, 1, 0}, {-1, 0, 0}}};
+    static const int ab_shift[4] = {0, 0, 1, 1}, b_sign[4] = {1, -1, 1, -1};
+    const int q = e - 1;
+    const double alpha = -0.25 * PI_ + (i - 1.0) * hx;
+    const double beta = b_sign[q] * (0.25 * PI_ - (j - 1.0) * hx);
+    const double as = (1 - ab_shift[q]) * alpha + ab_shift[q] * beta;
+    const double bs = ab_shift[q] * alpha + (1 - ab_shift[q]) * beta;
+    double v[3], a1s[3], a2s[3], r[3], b1t[3], b2t[3];
+    /* rot_matrix(m, d, e) in Fortran order: element (m, d) = rot[q][d][m] */
+#define ROT(out, vin)                                                                                   \
+    for (int d = 0; d < 3; d++)                                                                         \
+        out[d] = rot[q][d][0] * vin[0] + rot[q][d][1] * vin[1] + rot[q][d][2] * vin[2];
+    b1_proto(as, bs, v);
+    ROT(a1s, v);
+    b2_proto(as, bs, v);
+    ROT(a2s, v);
+    {
+        const double ta = tan(as), tb = tan(bs);
+        v[0] = ta / sqrt(1.0 + pow(ta, 2.0) + pow(tb, 2.0));
+        v[1] = tb / sqrt(1.0 + pow(ta, 2.0) + pow(tb, 2.0));
+        v[2] = 1.0 / sqrt(1.0 + pow(ta, 2.0) + pow(tb, 2.0));
+    }
+    ROT(r, v);
+#undef ROT
+    const double at = atan(r[0] / r[2]), bt = atan(r[1] / r[2]);
+    a1_proto(at, bt, b1t);
+    a2_proto(at, bt, b2t);
+    TM[0] = a1s[0] * b1t[0] + a1s[1] * b1t[1] + a1s[2] * b1t[2];
+    TM[1] = a2s[0] * b1t[0] + a2s[1] * b1t[1] + a2s[2] * b1t[2];
+    TM[2] = a1s[0] * b2t[0] + a1s[1] * b2t[1] + a1s[2] * b2t[2];
+    TM[3] = a2s[0] * b2t[0] + a2s[1] * b2t[1] + a2s[2] * b2t[2];
+}
+
+/* latlon_vec_outputer_t%write for covariant (u, v) on Ch (latlon_outputer_mod.f90:55-85,
+   regrid_factory_mod.f90:72-163 create_latlon_vector_regrid, latlon_regrid_mod.f90:132-212
+   do_latlon_vector_regrid): interp2d_uv2pvec_Ch_sbp* to the vertices, the covariant
+   ecs_xy_vec halo of width 2 (exchange, transform matrices, ECS_xy interpolation of
+   each component; ecs_halo_vec_xy_mod.f90:30-98), the cubic stencils, and the rotation
+   to the lat-lon components (init_transform_to_latlon_vec_tile, regrid_factory_mod.f90:
+   324-370: q = [iv.b1, iv.b2; jv.b1, jv.b2]).  uo, vo: [nlat][nlon]. */
+void orc_latlon_vec(orc_ctx *c, const double *u, const double *v, int nlat, int nlon, double *uo, double *vo)
+{
+    const int N = c->N, n = N + 1, hw = 2;
+    fld_from_packed(&c->u, u);
+    fld_from_packed(&c->v, v);
+    exch_do(&c->ex_ch3_u, &c->u, &c->v);
+    exch_do(&c->ex_ch3_v, &c->u, &c->v);
+    fld_t *bu = &c->uq, *bv = &c->vq;
+    for (int t = 0; t < NPAN; t++) {
+        /* the outputer's interpolator is interp2d_uv2pvec_Ch_sbp42 whatever the model's order */
+        interp_c2i(bu, &c->u, t, 0, N + 1, 1, N + 1, 42);
+        interp_c2i(bv, &c->v, t, 1, N + 1, 1, N + 1, 42);
+    }
+    exch_do(&c->ex_xy3_full_v, bu, bv);
+    const double hx = c->mxy.hx;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= hw + 1; j++)
+            for (int i = 1; i <= n; i++) {
+                double TM[4], zu, zv;
+                xy_vec_tm(1, i, j, hx, TM);
+                zu = FA(bu, t, i, 1 - j); zv = FA(bv, t, i, 1 - j);
+                FA(bu, t, i, 1 - j) = TM[0] * zu + TM[1] * zv;
+                FA(bv, t, i, 1 - j) = TM[2] * zu + TM[3] * zv;
+                xy_vec_tm(2, i, j, hx, TM);
+                zu = FA(bu, t, i, n + j); zv = FA(bv, t, i, n + j);
+                FA(bu, t, i, n + j) = TM[0] * zu + TM[1] * zv;
+                FA(bv, t, i, n + j) = TM[2] * zu + TM[3] * zv;
+                xy_vec_tm(3, i, j, hx, TM);
+                zu = FA(bu, t, 1 - j, i); zv = FA(bv, t, 1 - j, i);
+                FA(bu, t, 1 - j, i) = TM[0] * zu + TM[1] * zv;
+                FA(bv, t, 1 - j, i) = TM[2] * zu + TM[3] * zv;
+                xy_vec_tm(4, i, j, hx, TM);
+                zu = FA(bu, t, n + j, i); zv = FA(bv, t, n + j, i);
+                FA(bu, t, n + j, i) = TM[0] * zu + TM[1] * zv;
+                FA(bv, t, n + j, i) = TM[2] * zu + TM[3] * zv;
+            }
+    ecs_xy_interp(c, bu, hw);
+    ecs_xy_interp(c, bv, hw);
+    const mesh_t *m = &c->mxy;
+    for (int j = 1; j <= nlat; j++) {
+        const double phi = -0.5 * PI_ + (j - 1) * PI_ / (nlat - 1.0);
+        for (int i = 1; i <= nlon; i++) {
+            const double lam = (i - 1) * 2.0 * PI_ / nlon;
+            const double r[3] = {cos(phi) * cos(lam), cos(phi) * sin(lam), sin(phi)};
+            int t;
+            double alpha, beta;
+            cart_to_native(r, &t, &alpha, &beta);
+            double zdx = (alpha + 0.25 * PI_) / m->hx + 1, zdy = (beta + 0.25 * PI_) / m->hy + 1;
+            const int xi = (int)zdx, yi = (int)zdy;
+            zdx = zdx - xi;
+            zdy = zdy - yi;
+            double wx[4], wy[4];
+            wx[0] = -zdx * (zdx - 1.0) * (zdx - 2.0) / 6.0;
+            wx[1] = (zdx + 1.0) * (zdx - 1.0) * (zdx - 2.0) / 2.0;
+            wx[2] = -(zdx + 1.0) * zdx * (zdx - 2.0) / 2.0;
+            wx[3] = (zdx + 1.0) * zdx * (zdx - 1.0) / 6.0;
+            wy[0] = -zdy * (zdy - 1.0) * (zdy - 2.0) / 6.0;
+            wy[1] = (zdy + 1.0) * (zdy - 1.0) * (zdy - 2.0) / 2.0;
+            wy[2] = -(zdy + 1.0) * zdy * (zdy - 2.0) / 2.0;
+            wy[3] = (zdy + 1.0) * zdy * (zdy - 1.0) / 6.0;
+            double au = 0.0, av = 0.0;
+            for (int qq = -1; qq <= 2; qq++)
+                for (int p = -1; p <= 2; p++) {
+                    au = au + wx[p + 1] * wy[qq + 1] * FA(bu, t, xi + p, yi + qq);
+                    av = av + wx[p + 1] * wy[qq + 1] * FA(bv, t, xi + p, yi + qq);
+                }
+            /* latlon basis iv, jv and the contravariant basis b1, b2 of panel t at (alpha, beta) */
+            const double iv[3] = {-sin(lam), cos(lam), 0.0};
+            const double jv[3] = {-sin(phi) * cos(lam), -sin(phi) * sin(lam), cos(phi)};
+            double p1[3], p2[3], b1[3], b2[3];
+            b1_proto(alpha, beta, p1);
+            b2_proto(alpha, beta, p2);
+            proto2real(t, p1, b1);
+            proto2real(t, p2, b2);
+            const double q11 = iv[0] * b1[0] + iv[1] * b1[1] + iv[2] * b1[2];
+            const double q12 = iv[0] * b2[0] + iv[1] * b2[1] + iv[2] * b2[2];
+            const double q21 = jv[0] * b1[0] + jv[1] * b1[1] + jv[2] * b1[2];
+            const double q22 = jv[0] * b2[0] + jv[1] * b2[1] + jv[2] * b2[2];
+            const size_t k = (size_t)(j - 1) * nlon + (i - 1);
+            uo[k] = q11 * au + q12 * av;
+            vo[k] = q21 * au + q22 * av;
+        }
+    }
 }
 
 /* curl of the covariant (u, v) on mesh o (N x N per panel, packed [t][j][i]) */

@@ -326,3 +326,31 @@ def test_ah_williamson2_converges(order, expect):
         errs.append(max(np.abs(dh).max() / np.abs(h).max(), np.abs(du).max() / np.abs(u).max()))
     rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
     assert rates.min() > expect, (errs, rates)
+
+
+def test_latlon_wind_regrid_converges():
+    """The oracle's wind regrid (Ch to vertex interpolation, covariant ecs_xy_vec halo
+    with its transform matrices, rotation to lat-lon components) converges to the
+    exact wind of a solid-body rotation about a tilted axis, away from the poles; a
+    wrong transform matrix or rotation leaves an O(1) error."""
+    ax = np.array([np.sin(0.7), 0.0, np.cos(0.7)])
+    u0 = 20.0
+    errs = []
+    for N in (16, 32, 64):
+        o = Oracle(N)
+        _, u, v = o.ts2(u0=u0, h_mean=1000.0, axis=ax)
+        uo, vo = o.latlon_vec(u, v)
+        nlat, nlon = uo.shape
+        assert not np.isnan(uo).any() and not np.isnan(vo).any()
+        phi = -np.pi / 2 + np.arange(nlat) * np.pi / (nlat - 1)
+        lam = np.arange(nlon) * 2 * np.pi / nlon
+        P, L = np.meshgrid(phi, lam, indexing="ij")
+        r = np.stack([np.cos(P) * np.cos(L), np.cos(P) * np.sin(L), np.sin(P)], -1)
+        vel = u0 * np.cross(ax, r)
+        iv = np.stack([-np.sin(L), np.cos(L), 0 * L], -1)
+        jv = np.stack([-np.sin(P) * np.cos(L), -np.sin(P) * np.sin(L), np.cos(P)], -1)
+        inner = slice(1, nlat - 1)
+        errs.append(max(np.abs(uo - (vel * iv).sum(-1))[inner].max(), np.abs(vo - (vel * jv).sum(-1))[inner].max()))
+    assert errs[0] < 5e-3 * u0
+    rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert rates.min() > 1.7, (errs, rates)
