@@ -350,6 +350,44 @@ def run_nonlinear(args, torch, dist, world):
     return out
 
 
+def run_ah(args, torch, dist, world):
+    """The Ah staggering of the linear operator (h, u, v on the vertices, node SBP 4-2
+    operators with projections) on the day workload: C192, dt 150 s, 576 RK4 steps,
+    FP32, the same cube-corner Gaussian with the wind at rest; mass and energy drift
+    over the day from the FP64 SBP_Ah42 quadrature."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    ic = workload_ic()[0]
+    h = ic[0]
+    z = np.zeros_like(h)
+    stream = torch.cuda.current_stream()
+    dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN, horizontal_staggering="Ah")
+    dom.set_stream(stream.cuda_stream)
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
+    x = create_stvec_swm(dom).upload(h, z, z)
+    rk = create_timescheme(x, "rk4")
+    rk.steps(x, op, dom, DT, 8)
+    x.upload(h, z, z)
+    m0, e0 = op.integrals(x)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    rk.steps(x, op, dom, DT, NSTEPS)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if world > 1:
+        from ch_swe_b200 import replicas
+        ms = replicas.max_over_ranks(ms, dist, device="cuda")
+    m1, e1 = op.integrals(x)
+    dom.destroy()
+    return {"workload": f"C{N_CELLS} linear SWE on the Ah staggering (div_ah_sbp_proj_42, grad_ah_sbp_proj_42, "
+                        f"coriolis_colocated, co2contra_colocated), FP32, dt {DT:g} s, {NSTEPS} RK4 steps, "
+                        "the day workload's Gaussian with the wind at rest",
+            "value": world * 6 * N_CELLS ** 2 * NSTEPS / (ms / 1e3), "unit": "cell-updates/s",
+            "ms_total": ms, "mass_rel_drift": (m1 - m0) / abs(m0), "energy_rel_drift": (e1 - e0) / abs(e0)}
+
+
 def run_serving(args, torch):
     """Config 5: continuous batching of a Poisson request stream."""
     from ch_swe_b200 import serve
@@ -479,6 +517,7 @@ def run_ours(args):
         ens = None if args.no_ensemble else run_ensemble(args, torch, dist, world)
         srv = None if (args.no_serving or world > 1) else run_serving(args, torch)
         nl = None if args.no_nonlinear else run_nonlinear(args, torch, dist, world)
+        ah = None if args.no_ah else run_ah(args, torch, dist, world)
     clocks = clk.summary()
 
     K = args.steps
@@ -531,6 +570,8 @@ def run_ours(args):
         line["serving"] = srv
     if nl is not None:
         line["nonlinear"] = nl
+    if ah is not None:
+        line["ah"] = ah
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -557,6 +598,12 @@ def run_profile_leg(args):
         op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
         st = create_stvec_swm(dom).upload(*testcases.williamson2(NL_N, axis=axis))
         dt = NL_DT
+    elif args.profile_leg == "ah":
+        dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN, horizontal_staggering="Ah")
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
+        h = workload_ic()[0][0]
+        st = create_stvec_swm(dom).upload(h, np.zeros_like(h), np.zeros_like(h))
+        dt = DT
     else:
         dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN)
         op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
@@ -593,7 +640,8 @@ def main():
                     help="stage-kernel configuration 'tile,blocks_per_sm,runs' (overrides --tile and autotuning)")
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
-    ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear"], default=None,
+    ap.add_argument("--no-ah", action="store_true", help="skip the Ah-staggering leg")
+    ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear", "ah"], default=None,
                     help="run --rk4-steps steps of one workload only (for ncu captures; prints no bench line)")
     args = ap.parse_args()
     if args.profile_leg:

@@ -2554,14 +2554,16 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     rc = SWE_OK;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(c, SWE_ECUDA, "autotune events");
     const double dt = 1.0;
+    // steps that capture both graphs nreps steps replay (GRAPH_STEPS-step and 1-step)
+    const int warm = (nreps >= GRAPH_STEPS ? GRAPH_STEPS : 0) + (nreps % GRAPH_STEPS ? 1 : 0);
     int ncfg = 0;
     const KernelCfg *cfgs = cfgs_of(c->ord, &ncfg);
     for (int k = 0; k < ncfg && rc == SWE_OK; k++) {
         const KernelCfg kc = cfgs[k];
         if (c->adv && kc.occ != default_occ(kc.tile)) continue;
         set_cfg(c, kc.tile, kc.occ, kc.runs);
-        // untimed: the same step counts capture and instantiate the graphs
-        if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
+        // untimed: capture and instantiate the graphs the timed steps replay
+        if ((rc = swe_rk4_steps(c, v, dt, warm)) != SWE_OK) break;
         if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
         if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
         float t = 0.f;
@@ -2584,7 +2586,7 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
         for (int b = 0; b < 2 && rc == SWE_OK; b++) {
             drop_graph(c);
             c->branches = b == 1;
-            if ((rc = swe_rk4_steps(c, v, dt, nreps)) != SWE_OK) break;
+            if ((rc = swe_rk4_steps(c, v, dt, warm)) != SWE_OK) break;
             float t = 0.f;
             if (cudaEventRecord(e0, c->stream) != cudaSuccess || swe_rk4_steps(c, v, dt, nreps) != SWE_OK ||
                 cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
