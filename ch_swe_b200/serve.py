@@ -243,6 +243,28 @@ class Server:
     def used_bytes(self) -> int:
         return sum(p.bytes for p in self.pools.values())
 
+    def pool_capacity(self, key) -> int:
+        """Slots a pool of key (N, precision, operator) gets when the budget is free."""
+        N, precision, operator = key
+        return int(min(self.max_slots.get(N, 4), self.budget // member_bytes(N, precision, operator)))
+
+    def pretune(self, keys, nreps: int = 16):
+        """Autotune the stage kernels of the pools of `keys` one after another on an idle
+        device, before requests arrive.  The choices go to the library's process-wide
+        tuning cache, so pools created while serving take them instead of timing
+        under the load of the other pools."""
+        from .swm import create_domain
+        for key in sorted(set(keys)):
+            if key in self.tiles:
+                continue
+            N, precision, operator = key
+            cap = self.pool_capacity(key)
+            if cap < 1:
+                continue
+            dom = create_domain(N, precision=precision, n_members=cap, operator=operator)
+            dom.autotune(nreps=nreps)
+            dom.destroy()
+
     def _pool_for(self, req: Request):
         if req.operator not in ("linear", "advective"):
             raise ValueError(f"request {req.rid}: operator {req.operator!r} is not served")

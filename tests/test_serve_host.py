@@ -29,3 +29,15 @@ def test_member_bytes_and_dt():
     pitch = (rows + 7) // 8 * 8
     assert member_bytes(N, "fp64") >= 5 * 18 * rows * pitch * 8
     assert stable_dt(192) == 150.0 and stable_dt(384) == 75.0
+
+
+def test_pool_capacity_follows_budget():
+    """A pool gets its size's slot count while the budget allows, fewer when it does
+    not, and none when one member does not fit (the capacity pretune tunes for)."""
+    from ch_swe_b200.serve import MAX_SLOTS, Server, member_bytes
+    per = member_bytes(192, "fp64", "advective")
+    big = Server(hbm_budget_bytes=64 << 30)
+    assert big.pool_capacity((192, "fp64", "advective")) == MAX_SLOTS.get(192, 4)
+    small = Server(hbm_budget_bytes=2 * per + 1)
+    assert small.pool_capacity((192, "fp64", "advective")) == min(MAX_SLOTS.get(192, 4), 2)
+    assert Server(hbm_budget_bytes=per - 1).pool_capacity((192, "fp64", "advective")) == 0
