@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "chswe.h"
@@ -978,37 +979,61 @@ static void uv_extent(const swe_ctx *c, int &nx, int &ny)
     ny = c->cfg.N + 1;
 }
 
-template <class T>
-static void pack_member(const swe_ctx *c, const double *h, const double *u, const double *v, T *box)
+// Host copies between the packed arrays and the pinned staging box, one task per
+// (member, panel): on several threads when the copy is large (the e2e path's host
+// share), serially for small cubes.
+template <class F>
+static void panel_tasks(int count, int N, const F &task)
 {
-    const int N = c->cfg.N, P = c->dims.P;
-    const size_t ps = c->dims.ps, fs = c->dims.fs;
-    int nx, ny;
-    uv_extent(c, nx, ny);
-    for (int t = 0; t < NPAN; t++) {
-        for (int j = 0; j <= N; j++)
-            for (int i = 0; i <= N; i++) box[0 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*h++);
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
-        for (int j = 0; j < nx; j++)
-            for (int i = 0; i < ny; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
+    const int ntask = count * NPAN;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthreads = (int)std::min<long long>(std::min<long long>(hw ? hw : 1, 16), ntask);
+    if ((long long)ntask * (N + 1) * (N + 1) < (1LL << 15) || nthreads <= 1) {
+        for (int k = 0; k < ntask; k++) task(k / NPAN, k % NPAN);
+        return;
     }
+    std::vector<std::thread> pool;
+    for (int w = 0; w < nthreads; w++)
+        pool.emplace_back([&, w] {
+            for (int k = w; k < ntask; k += nthreads) task(k / NPAN, k % NPAN);
+        });
+    for (auto &th : pool) th.join();
 }
+
 template <class T>
-static void unpack_member(const swe_ctx *c, const T *box, double *h, double *u, double *v)
+static void pack_panel(const swe_ctx *c, const double *h, const double *u, const double *v, T *box, int t)
 {
     const int N = c->cfg.N, P = c->dims.P;
     const size_t ps = c->dims.ps, fs = c->dims.fs;
     int nx, ny;
     uv_extent(c, nx, ny);
-    for (int t = 0; t < NPAN; t++) {
-        for (int j = 0; j <= N; j++)
-            for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-        for (int j = 0; j < ny; j++)
-            for (int i = 0; i < nx; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-        for (int j = 0; j < nx; j++)
-            for (int i = 0; i < ny; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-    }
+    h += (size_t)t * (N + 1) * (N + 1);
+    u += (size_t)t * nx * ny;
+    v += (size_t)t * nx * ny;
+    for (int j = 0; j <= N; j++)
+        for (int i = 0; i <= N; i++) box[0 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*h++);
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
+    for (int j = 0; j < nx; j++)
+        for (int i = 0; i < ny; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
+}
+
+template <class T>
+static void unpack_panel(const swe_ctx *c, const T *box, double *h, double *u, double *v, int t)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t ps = c->dims.ps, fs = c->dims.fs;
+    int nx, ny;
+    uv_extent(c, nx, ny);
+    h += (size_t)t * (N + 1) * (N + 1);
+    u += (size_t)t * nx * ny;
+    v += (size_t)t * nx * ny;
+    for (int j = 0; j <= N; j++)
+        for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + box_off(P, i + 1, j + 1)]);
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
+    for (int j = 0; j < nx; j++)
+        for (int i = 0; i < ny; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
 }
 
 static size_t member_sizes(const swe_ctx *c, size_t *nh, size_t *nu)
@@ -1027,12 +1052,12 @@ static int upload_range(swe_stvec *vec, int m0, int count, const double *h, cons
     const size_t mbytes = (size_t)c->dims.ms * c->elem;
     CU(c, cudaStreamSynchronize(c->stream));   // the staging buffer may still feed an earlier copy
     unsigned char *buf = c->pinned;
-    for (int k = 0; k < count; k++) {
+    panel_tasks(count, c->cfg.N, [&](int k, int t) {
         if (c->elem == 8)
-            pack_member<double>(c, h + k * nh, u + k * nu, v + k * nu, (double *)(buf + k * mbytes));
+            pack_panel<double>(c, h + k * nh, u + k * nu, v + k * nu, (double *)(buf + k * mbytes), t);
         else
-            pack_member<float>(c, h + k * nh, u + k * nu, v + k * nu, (float *)(buf + k * mbytes));
-    }
+            pack_panel<float>(c, h + k * nh, u + k * nu, v + k * nu, (float *)(buf + k * mbytes), t);
+    });
     CU(c, cudaMemcpyAsync((char *)vec->d + m0 * mbytes, buf, mbytes * count, cudaMemcpyHostToDevice, c->stream));
     if (vec->cmp) CU(c, cudaMemsetAsync((char *)vec->cmp + m0 * (size_t)c->dims.ms * 4, 0, (size_t)c->dims.ms * 4 * count, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
@@ -1048,12 +1073,12 @@ static int download_range(const swe_stvec *vec, int m0, int count, double *h, do
     unsigned char *buf = c->pinned;
     CU(c, cudaMemcpyAsync(buf, (char *)vec->d + m0 * mbytes, mbytes * count, cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
-    for (int k = 0; k < count; k++) {
+    panel_tasks(count, c->cfg.N, [&](int k, int t) {
         if (c->elem == 8)
-            unpack_member<double>(c, (const double *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
+            unpack_panel<double>(c, (const double *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu, t);
         else
-            unpack_member<float>(c, (const float *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu);
-    }
+            unpack_panel<float>(c, (const float *)(buf + k * mbytes), h + k * nh, u + k * nu, v + k * nu, t);
+    });
     return SWE_OK;
 }
 
@@ -2040,7 +2065,6 @@ static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
     c->ll_i = nullptr; c->ll_d = nullptr; c->ll_nlat = c->ll_nlon = 0;
     const int N = c->cfg.N, n = N + 1;
     const LatlonLayout Lo = latlon_layout(N, nlat, nlon);
-    const size_t np = Lo.np;
     std::vector<int> hi(Lo.ints(), 0);
     std::vector<double> hd(Lo.d_ext(), 0.0);
     const double pi = 3.141592653589793238462643383279502884;

@@ -222,9 +222,12 @@ class StvecSwm:
 
     def __del__(self):
         p = getattr(self, "_p", None)
-        if p and self.domain._ctx:
-            _lib.load().swe_stvec_destroy(p)
-            self._p = None
+        try:
+            if p and self.domain._ctx:
+                _lib.load().swe_stvec_destroy(p)
+                self._p = None
+        except Exception:   # interpreter shutdown: the module globals may be gone already
+            pass
 
     # -- transfers ------------------------------------------------------
     def upload(self, h, u, v, member: int | None = 0):
