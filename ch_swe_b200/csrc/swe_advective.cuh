@@ -172,10 +172,12 @@ __device__ __forceinline__ T up4_flux(T c, T fm2, T fm1, T f0, T fp1, T fp2, T f
 }
 
 // Writes F (field 1: flux on the y mesh, field 2: on the x mesh) and the flux edge
-// strips (the same layout k_co2contra writes for ut, vt).
+// strips (the same layout k_co2contra writes for ut, vt: nl lines per side, the
+// normal flux at depths 1..nl-1 and the tangential one on the edge line).
 template <class T>
 __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *__restrict__ W, T *__restrict__ F,
-                                              T *__restrict__ FS, Dims d, AdvView<T> av, const double *__restrict__ dtm)
+                                              T *__restrict__ FS, Dims d, AdvView<T> av, const double *__restrict__ dtm,
+                                              int nl)
 {
     const int N = d.N, n = N + 1;
     const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
     const T *h = Y + mem * d.ms;
     const int64_t o = box_off(d.P, i, j);
     const int64_t po = mem * d.ms + t * d.ps;
-    T *fs = FS + strip_member(N, mem) + (int64_t)t * 4 * STRIP_LINES * n - 1;
+    T *fs = FS + strip_member(N, mem, nl) + (int64_t)t * 4 * nl * n - 1;
     const T *hr = h + t * d.ps + (j - 1 + MG) * d.P + (i - 1 + MG);   // h(i, j); the box has 4-point margins
     if (i <= N) {
         const T c = __ldg(W + po + d.fs + o);
@@ -197,10 +199,10 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
                          : up4_flux(c, h_ext(h, d, av, t, i - 2, j), h_ext(h, d, av, t, i - 1, j), h_ext(h, d, av, t, i, j),
                                     h_ext(h, d, av, t, i + 1, j), h_ext(h, d, av, t, i + 2, j), h_ext(h, d, av, t, i + 3, j));
         F[po + d.fs + o] = fx;
-        if (i <= 3) fs[(SIDE_L * 4 + i - 1) * n + j] = fx;
-        if (i >= N - 2) fs[(SIDE_R * 4 + N - i) * n + j] = fx;
-        if (j == 1) fs[(SIDE_B * 4 + 3) * n + i] = fx;
-        if (j == n) fs[(SIDE_T * 4 + 3) * n + i] = fx;
+        if (i <= nl - 1) fs[(SIDE_L * nl + i - 1) * n + j] = fx;
+        if (i >= N + 2 - nl) fs[(SIDE_R * nl + N - i) * n + j] = fx;
+        if (j == 1) fs[(SIDE_B * nl + nl - 1) * n + i] = fx;
+        if (j == n) fs[(SIDE_T * nl + nl - 1) * n + i] = fx;
     }
     if (j <= N) {
         const T c = __ldg(W + po + 2 * d.fs + o);
@@ -211,10 +213,10 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
                          : up4_flux(c, h_ext(h, d, av, t, i, j - 2), h_ext(h, d, av, t, i, j - 1), h_ext(h, d, av, t, i, j),
                                     h_ext(h, d, av, t, i, j + 1), h_ext(h, d, av, t, i, j + 2), h_ext(h, d, av, t, i, j + 3));
         F[po + 2 * d.fs + o] = fy;
-        if (j <= 3) fs[(SIDE_B * 4 + j - 1) * n + i] = fy;
-        if (j >= N - 2) fs[(SIDE_T * 4 + N - j) * n + i] = fy;
-        if (i == 1) fs[(SIDE_L * 4 + 3) * n + j] = fy;
-        if (i == n) fs[(SIDE_R * 4 + 3) * n + j] = fy;
+        if (j <= nl - 1) fs[(SIDE_B * nl + j - 1) * n + i] = fy;
+        if (j >= N + 2 - nl) fs[(SIDE_T * nl + N - j) * n + i] = fy;
+        if (i == 1) fs[(SIDE_L * nl + nl - 1) * n + j] = fy;
+        if (i == n) fs[(SIDE_R * nl + nl - 1) * n + j] = fy;
     }
 }
 

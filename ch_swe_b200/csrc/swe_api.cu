@@ -814,11 +814,9 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (cfg->N < 8 || cfg->n_members < 1 || (cfg->precision != SWE_FP64 && cfg->precision != SWE_FP32) ||
         (cfg->operator_kind != SWE_OP_LINEAR && cfg->operator_kind != SWE_OP_ADVECTIVE) || !(cfg->radius > 0.0))
         return SWE_EINVAL;
-    // SBP order: 4-2 (0 selects it too), 2-1 or 6-3 (N >= 16), the last two for the linear operator
+    // SBP order: 4-2 (0 selects it too), 2-1 or 6-3 (N >= 16)
     const int ord = cfg->sbp_order == 0 ? 42 : cfg->sbp_order;
-    if ((ord != 42 && ord != 21 && ord != 63) || (ord != 42 && cfg->operator_kind != SWE_OP_LINEAR) ||
-        (ord == 63 && cfg->N < 16))
-        return SWE_EINVAL;
+    if ((ord != 42 && ord != 21 && ord != 63) || (ord == 63 && cfg->N < 16)) return SWE_EINVAL;
     // Ah staggering: the linear operator with the SBP node operators
     if ((cfg->staggering != SWE_STAG_CH && cfg->staggering != SWE_STAG_AH) ||
         (cfg->staggering == SWE_STAG_AH && cfg->operator_kind != SWE_OP_LINEAR))
@@ -1273,7 +1271,8 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                             c->stream, dtm);
         launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->stream, (T *)yin, (T *)c->hb, c->dims, dtm);
     }
-    launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm);
+    launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm,
+             ord_strip_lines(c->ord));
     launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->fs,
              (T *)c->edge, c->dims, mv, dtm);
     if (fork) {

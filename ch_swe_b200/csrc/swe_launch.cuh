@@ -28,6 +28,9 @@ namespace chswe {
 #define CHSWE_LINEAR21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 // SBP 6-3 stage kernels: the same configurations
 #define CHSWE_LINEAR63_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
+// the advective operator in SBP 2-1 and 6-3: the same configurations
+#define CHSWE_ADV21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
+#define CHSWE_ADV63_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 
 static inline dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
 

@@ -52,15 +52,21 @@ cudaError_t StageTU<T, TMX>::optin()
 #define CHSWE_OPTIN_21(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, false, 21)
 #define CHSWE_OPTIN_63(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, false, 63)
 #define CHSWE_OPTIN_ADV(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, true, 42)
+#define CHSWE_OPTIN_ADV21(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, true, 21)
+#define CHSWE_OPTIN_ADV63(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, true, 63)
     CHSWE_LINEAR_CFGS(CHSWE_OPTIN_42)
     CHSWE_LINEAR21_CFGS(CHSWE_OPTIN_21)
     CHSWE_LINEAR63_CFGS(CHSWE_OPTIN_63)
     CHSWE_ADV_CFGS(CHSWE_OPTIN_ADV)
+    CHSWE_ADV21_CFGS(CHSWE_OPTIN_ADV21)
+    CHSWE_ADV63_CFGS(CHSWE_OPTIN_ADV63)
 #undef CHSWE_OPTIN
 #undef CHSWE_OPTIN_42
 #undef CHSWE_OPTIN_21
 #undef CHSWE_OPTIN_63
 #undef CHSWE_OPTIN_ADV
+#undef CHSWE_OPTIN_ADV21
+#undef CHSWE_OPTIN_ADV63
     return e;
 }
 
@@ -109,15 +115,21 @@ void StageTU<T, TMX>::stage(int occ, int runs, int ord, int members, const T *y,
 #define CHSWE_STG_21(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, false, 21)
 #define CHSWE_STG_63(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, false, 63)
 #define CHSWE_STG_ADV(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, true, 42)
+#define CHSWE_STG_ADV21(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, true, 21)
+#define CHSWE_STG_ADV63(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, true, 63)
     CHSWE_LINEAR_CFGS(CHSWE_STG_42)
     CHSWE_LINEAR21_CFGS(CHSWE_STG_21)
     CHSWE_LINEAR63_CFGS(CHSWE_STG_63)
     CHSWE_ADV_CFGS(CHSWE_STG_ADV)
+    CHSWE_ADV21_CFGS(CHSWE_STG_ADV21)
+    CHSWE_ADV63_CFGS(CHSWE_STG_ADV63)
 #undef CHSWE_STG
 #undef CHSWE_STG_42
 #undef CHSWE_STG_21
 #undef CHSWE_STG_63
 #undef CHSWE_STG_ADV
+#undef CHSWE_STG_ADV21
+#undef CHSWE_STG_ADV63
 }
 
 template <class T, int TMX>

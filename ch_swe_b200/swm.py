@@ -68,9 +68,13 @@ LINEAR_AH_NAMES_BY_ORDER = {
 }
 LINEAR_AH42_NAMES = LINEAR_AH_NAMES_BY_ORDER[42]
 STAGGERINGS = {"Ch": _lib.SWE_STAG_CH, "Ah": _lib.SWE_STAG_AH}
-# advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4)
-ADVECTIVE_CH42_NAMES = dict(LINEAR_CH42_NAMES, vector_advection_op_name="vector_advection_Ch_up4_cov",
-                            massflux_op_name="massflux_ch_up4")
+# advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4),
+# per SBP order of its Ch operators
+ADVECTIVE_NAMES_BY_ORDER = {
+    order: dict(names, vector_advection_op_name="vector_advection_Ch_up4_cov", massflux_op_name="massflux_ch_up4")
+    for order, names in LINEAR_NAMES_BY_ORDER.items()
+}
+ADVECTIVE_CH42_NAMES = ADVECTIVE_NAMES_BY_ORDER[42]
 OPERATORS = {"linear": _lib.SWE_OP_LINEAR, "advective": _lib.SWE_OP_ADVECTIVE}
 
 
@@ -112,8 +116,8 @@ class Domain:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if self.operator not in OPERATORS:
             raise ValueError(f"operator must be one of {sorted(OPERATORS)}")
-        if self.sbp_order not in (42, 21, 63) or (self.sbp_order != 42 and self.operator != "linear"):
-            raise ValueError("sbp_order must be 42, or 21 / 63 with the linear operator")
+        if self.sbp_order not in (42, 21, 63):
+            raise ValueError("sbp_order must be 42, 21 or 63")
         if self.sbp_order == 63 and self.N < 16:
             raise ValueError("SBP 6-3 needs N >= 16")
         L = _lib.load()
@@ -351,7 +355,7 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
             raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
         if orography_generator is not None:
             raise ValueError("advective_swm_operator: orography is not supported")
-        names, want_op = ADVECTIVE_CH42_NAMES, "advective"
+        names, want_op = ADVECTIVE_NAMES_BY_ORDER[domain.sbp_order], "advective"
     else:
         raise ValueError(f"unknown swm_op_type: {kind}")
     for key, want in names.items():
@@ -363,7 +367,7 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
                 if want_op == "linear" and got == ah.get(key) and domain.sbp_order != order:
                     raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")
             for order, other in LINEAR_NAMES_BY_ORDER.items():
-                if want_op == "linear" and got == other.get(key):
+                if got == other.get(key):
                     raise ValueError(f"{key} = {got} needs a domain created with sbp_order={order}")
             raise ValueError(f"unsupported {key}: {got} (this build implements {want})")
     if domain.operator != want_op:

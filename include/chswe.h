@@ -77,7 +77,7 @@ typedef struct swe_cfg {
     int coriolis_constant;    /* metric%coriolis_const: f = omega instead of 2 omega sin(lat) */
     double h_mean;            /* operator h_mean (H) for every member (default 1000 m) */
     int sbp_order;            /* SBP order of the Ch operators: 42 (default; 0 also selects it),
-                                 21 or 63 (linear operator only; 63 needs N >= 16): the
+                                 21 or 63 (63 needs N >= 16), for both operators: the
                                  _sbp_sat_42 / _21 / _63 names of grad_factory_mod.f90,
                                  div_factory_mod.f90, co2contra_factory_mod.f90,
                                  coriolis_factory_mod.f90 and the SBP_C42/C21/C63 quadratures */

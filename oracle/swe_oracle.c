@@ -1496,14 +1496,16 @@ static void op_vec_adv(orc_ctx *c, fld_t *utd, fld_t *vtd, fld_t *u, fld_t *v, f
     exch_do(&c->ex_ch3_u, ut, vt);
     exch_do(&c->ex_ch3_v, ut, vt);
     for (int t = 0; t < NPAN; t++) {
-        interp_c2i(&c->uh, ut, t, 0, N + 1, 1, N + 1, c->ord);
-        interp_c2i(&c->vh, vt, t, 1, N + 1, 1, N + 1, c->ord);
+        /* the vector advection's interpolators are the _sbp42 ones whatever the operator's
+           order (vector_advection_factory_mod.f90:65) */
+        interp_c2i(&c->uh, ut, t, 0, N + 1, 1, N + 1, 42);
+        interp_c2i(&c->vh, vt, t, 1, N + 1, 1, N + 1, 42);
     }
     /* interp2d_pvec2uv_Ch_sbp42 on (vh, uh): v_at_u = I_i2c,x(vh), u_at_v = I_i2c,y(uh)
        (its xy exchange fills halos that the SBP interpolation does not read) */
     for (int t = 0; t < NPAN; t++) {
-        interp_i2c(&c->vau, &c->vh, t, 0, N, 1, N + 1, c->ord);
-        interp_i2c(&c->uav, &c->uh, t, 1, N, 1, N + 1, c->ord);
+        interp_i2c(&c->vau, &c->vh, t, 0, N, 1, N + 1, 42);
+        interp_i2c(&c->uav, &c->uh, t, 1, N, 1, N + 1, 42);
     }
     /* u_halo = u, v_halo = v, then the ECS Ch vector halo of width 3 */
     for (int t = 0; t < NPAN; t++) {

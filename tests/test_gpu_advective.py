@@ -137,3 +137,51 @@ def test_fp32_williamson2_against_fp64():
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5, name
     # steady state: the FP64 run stays near the analytic state (discretisation error)
     assert rel(out["fp64"][0], st[0]) < 1e-4
+
+
+@pytest.mark.parametrize("order,N", [(21, 12), (21, 24), (63, 16), (63, 26)])
+def test_apply_parity_fp64_sbp_orders(order, N):
+    """The advective operator with the SBP 2-1 / 6-3 Ch operators (the _21 / _63 names
+    of its div, grad, Coriolis, co2contra and quadrature; the vector advection keeps
+    its _sbp42 interpolators, as in the reference) against the oracle."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
+    from oracle.oracle import Oracle
+    st = random_state(N, 40 + N + order)
+    ref = Oracle(N, h_mean=H0, operator="advective", sbp_order=order).apply(*st)
+    dom = create_domain(N, operator="advective", sbp_order=order)
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator",
+                                        "div_op_name": f"div_ch_sbp_sat_{order}_proj"}, dom)
+    x = create_stvec_swm(dom).upload(*st)
+    y = create_stvec_swm(dom)
+    op.apply(y, x, dom)
+    for g, r, name in zip(y.download(), ref, "huv"):
+        assert rel(g, r) < FP64_RTOL, (order, N, name, rel(g, r))
+    dom.destroy()
+
+
+@pytest.mark.parametrize("order", [21, 63])
+def test_rk4_williamson2_tilted_sbp_orders(order):
+    """Eight RK4 steps of tilted-axis Williamson-2 with the 2-1 / 6-3 operators: FP64
+    within 1e-12 of the oracle for every tile, FP32 within 1e-5 of FP64."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    from oracle.oracle import EARTH_RADIUS, Oracle
+    N, dt, nst = 20, 1200.0, 8
+    axis = (np.sin(0.8), 0.0, np.cos(0.8))
+    u0 = 2 * np.pi * EARTH_RADIUS / (12 * 86400)
+    o = Oracle(N, h_mean=H0, axis=axis, operator="advective", sbp_order=order)
+    st = o.ts2(u0=u0, h_mean=H0, axis=axis)
+    ref = o.rk4(*st, dt, nst)
+    out = {}
+    for prec, tile in (("fp64", 17), ("fp64", 25), ("fp64", 33), ("fp32", 25)):
+        dom = create_domain(N, precision=prec, operator="advective", rotation_axis=axis, sbp_order=order)
+        dom.kernel_config = (tile, 3 if tile == 17 else 2, 0)
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
+        x = create_stvec_swm(dom).upload(*st)
+        create_timescheme(x, "rk4").steps(x, op, dom, dt, nst)
+        out[(prec, tile)] = x.download()
+        dom.destroy()
+    for tile in (17, 25, 33):
+        for g, r, name in zip(out[("fp64", tile)], ref, "huv"):
+            assert rel(g, r) < FP64_RTOL, (order, tile, name, rel(g, r))
+    for a, b, name in zip(out[("fp32", 25)], out[("fp64", 25)], "huv"):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5, name

@@ -126,5 +126,3 @@ def test_orders_differ_and_configs_are_checked(order):
     with pytest.raises(ValueError):
         create_swm_operator(dom.grav, dict(LIN, div_op_name="div_ch_sbp_sat_42_proj"), dom)
     dom.destroy()
-    with pytest.raises(ValueError):
-        create_domain(N, operator="advective", sbp_order=order)

@@ -91,3 +91,23 @@ def test_williamson2_steady_state_converges():
         errs.append(np.abs(h1 - h).max() / np.abs(h).max())
     assert errs[1] < 2e-4
     assert np.log2(errs[0] / errs[1]) > 2.3, errs
+
+
+@pytest.mark.parametrize("order", [21, 63])
+def test_advective_sbp_orders_conserve_mass_and_match_at_rest(order):
+    """The advective operator with the 2-1 / 6-3 Ch operators: at rest its tendency is
+    the linear operator's gradient wind of the same order (the advection and the
+    Christoffel terms vanish), and RK4 conserves mass to round-off."""
+    from oracle.oracle import Oracle
+    N = 16
+    o = Oracle(N, h_mean=1000.0, operator="advective", sbp_order=order)
+    h = 1000.0 + o.gaussian(lam0=1.0, phi0=0.3, d0=0.4, amp=20.0)[0]
+    _, u, v = o.zeros()
+    dh, du, dv = o.apply(h, u, v)
+    lin = Oracle(N, h_mean=1000.0, sbp_order=order)
+    _, lu, lv = lin.apply(h - 1000.0, u, v)
+    assert np.abs(du - lu).max() < 1e-12 * np.abs(lu).max() and np.abs(dv - lv).max() < 1e-12 * np.abs(lv).max()
+    assert np.abs(dh).max() == 0.0
+    m0 = o.integrals(h, u, v)[0]
+    hs, us, vs = o.rk4(h, u, v, 600.0, 6)
+    assert abs(o.integrals(hs, us, vs)[0] - m0) < 1e-13 * abs(m0)
