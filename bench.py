@@ -77,7 +77,10 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        # the raw samples go to CHSWE_CLOCKS_DIR (default: the system's temporary directory)
+        import tempfile
+        out_dir = os.environ.get("CHSWE_CLOCKS_DIR", tempfile.gettempdir())
+        self.path = os.path.join(out_dir, f"clocks_gpu{gpu_index}.csv")
 
     def __enter__(self):
         try:
