@@ -266,6 +266,7 @@ struct swe_ctx {
     void *vh = nullptr;              // covariant wind at the virtual points beyond the panel edges
     void *hb = nullptr;              // panel-boundary h before the in-place averaging
     double *ones = nullptr;          // per-member depth factor 1 (dh = -div F)
+    double *negones = nullptr;       // per-member factor -1: the linear stage's dh is then div (outputs)
     // Ah staggering (cfg.staggering == SWE_STAG_AH): h, u, v on the vertices
     bool ah = false;
     DevAh<double> ah64;
@@ -788,7 +789,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
-    cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa);
+    cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     if (c->side) cudaStreamDestroy(c->side);
@@ -2130,11 +2131,42 @@ static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
     return SWE_OK;
 }
 
+// The divergence of the wind of every member (div_ch_sbp_sat_<order>_proj of the
+// contravariant components, the operator the diagnostics' div_operator_name names)
+// into field 0 of the scratch box ya: the linear operator's stage kernel in mode 0
+// with the depth factor -1, so that its dh = -(-1) div.
+template <class T>
+static int enqueue_div(swe_ctx *c, const void *yin, const MetricView<T> &mv)
+{
+    const int M = c->cfg.n_members;
+    if (!c->negones) {
+        std::vector<double> neg(M, -1.0);
+        if (cudaMalloc(&c->negones, sizeof(double) * M) != cudaSuccess) {
+            c->negones = nullptr;
+            return fail(c, SWE_ENOMEM, "divergence factor allocation failed");
+        }
+        CU(c, cudaMemcpy(c->negones, neg.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    }
+    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                        c->stream, nullptr);
+    launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c),
+             dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es, (T *)c->edge, c->dims, mv,
+             (const double *)nullptr);
+    StageArgs a{0, 0.0, c->negones, nullptr, nullptr, nullptr, nullptr};
+    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, nullptr,
+                    (T *)c->ya, nullptr, nullptr, c->dims, mv, a, c->stream);
+    c->launches += 3;
+    CU(c, cudaGetLastError());
+    return SWE_OK;
+}
+
 extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, int field, int nlat, int nlon,
                                  double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
-    if (field != 0) return fail(c, SWE_EINVAL, "lat-lon regrid: only field 0 (h, xy points) is supported");
+    if (field != 0 && field != 1)
+        return fail(c, SWE_EINVAL, "lat-lon regrid: field 0 (h) or 1 (the divergence of the wind)");
+    if (field == 1 && c->ah) return fail(c, SWE_EINVAL, "lat-lon regrid of the divergence: built for Ch");
     if (nlat < 2 || nlon < 1 || (int64_t)nlat * nlon > (1 << 28))
         return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
     int rc = ensure_latlon(c, nlat, nlon);
@@ -2148,8 +2180,14 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
     const size_t mo = (size_t)member * c->dims.ms;
     const dim3 b(256), g1((unsigned)std::min<int64_t>(((int64_t)Lo.next + 255) / 256, 8192)),
         g2((unsigned)std::min<int64_t>((np + 255) / 256, 8192));
-    if (c->elem == 8) k_ecs_xy_ext<double><<<g1, b, 0, c->stream>>>((const double *)vec->d + mo, c->dims, kt, wt, ext);
-    else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)vec->d + mo, c->dims, kt, wt, ext);
+    const void *src = vec->d;
+    if (field == 1) {
+        rc = c->elem == 8 ? enqueue_div<double>(c, vec->d, c->m64.v) : enqueue_div<float>(c, vec->d, c->m32.v);
+        if (rc != SWE_OK) return rc;
+        src = c->ya;
+    }
+    if (c->elem == 8) k_ecs_xy_ext<double><<<g1, b, 0, c->stream>>>((const double *)src + mo, c->dims, kt, wt, ext);
+    else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)src + mo, c->dims, kt, wt, ext);
     k_latlon<<<g2, b, 0, c->stream>>>(ext, c->ll_i, c->ll_d, N, np, dout);
     c->launches += 2;
     CU(c, cudaGetLastError());

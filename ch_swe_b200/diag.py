@@ -97,6 +97,15 @@ class LatlonOutputer:
         write_latlon(path, f, rec)
         return f
 
+    def regrid_div(self, state, member: int = 0) -> np.ndarray:
+        """The divergence of the wind (the div.dat field of output_div: the model's
+        div_ch_sbp_sat_<order>_proj of the contravariant wind) on the lat-lon grid."""
+        out = np.empty((self.nlat, self.nlon))
+        check(_lib.load().swe_regrid_latlon(self.domain.ctx, state.handle, int(member), 1, self.nlat, self.nlon,
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self.domain.ctx, "swe_regrid_latlon (div)")
+        return out
+
 
 class LatlonVecOutputer:
     """latlon_vec_outputer_t for the covariant Ch wind (latlon_outputer_mod.f90:55-85): the

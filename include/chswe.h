@@ -164,7 +164,9 @@ int swe_curl(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
    ECS_xy halo of width 2, the points phi_j = -pi/2 + (j-1) pi / (nlat-1),
    lam_i = (i-1) 2 pi / nlon are located on their panels and the 4 x 4 cubic Lagrange
    stencil is summed.  out[nlat][nlon] in FP64, longitude fastest (the reference's
-   outputer uses nlat = 2N+1, nlon = 4N).  Other fields give SWE_EINVAL.  Synchronous. */
+   outputer uses nlat = 2N+1, nlon = 4N).  field 1: the divergence of the wind instead
+   (output_div's div.dat: div_ch_sbp_sat_<order>_proj of the contravariant wind,
+   swm_output_diag_mod.f90:92-106; Ch only).  Other fields give SWE_EINVAL.  Synchronous. */
 int swe_regrid_latlon(swe_ctx *ctx, const swe_stvec *vec, int member, int field, int nlat, int nlon,
                       double *out);
 

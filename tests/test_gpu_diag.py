@@ -220,3 +220,29 @@ def test_latlon_wind_solid_body_rotation_large_cube(tmp_path):
     raw = np.fromfile(str(tmp_path / "v.dat"), dtype="<f4").reshape(nlat, nlon)
     np.testing.assert_array_equal(raw, vo.astype("<f4"))
     dom.destroy()
+
+
+@pytest.mark.parametrize("operator,order", [("linear", 42), ("advective", 42), ("linear", 63)])
+def test_latlon_div_regrid_matches_oracle(operator, order):
+    """The div.dat field of output_div: the model's divergence of the contravariant wind
+    (div_ch_sbp_sat_<order>_proj) regridded like h, against the oracle's co2contra, div
+    and lat-lon regrid; for the advective context too, whose tendency is not -H div."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import LatlonOutputer
+    from oracle.oracle import Oracle
+    N = 24
+    o = Oracle(N, sbp_order=order)
+    rng = np.random.default_rng(3)
+    h, u, v = o.ts2(u0=20.0, h_mean=1000.0, axis=(0.3, 0.0, 0.95))
+    u = u + rng.standard_normal(u.shape)
+    v = v + rng.standard_normal(v.shape)
+    ref = o.latlon(o.div(*o.co2contra(u, v)))
+    dom = create_domain(N, precision="fp64", operator=operator, sbp_order=order, n_members=2)
+    st = create_stvec_swm(dom)
+    st.upload(h + 1000.0, u, v, member=1)
+    st.upload(h + 1000.0, 0 * u, 0 * v, member=0)
+    out = LatlonOutputer(dom)
+    got = out.regrid_div(st, member=1)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.abs(out.regrid_div(st, member=0)).max() == 0.0
+    dom.destroy()
