@@ -33,6 +33,7 @@ EXPORTED = [
     "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
     "swe_set_tile", "swe_get_tile", "swe_autotune", "swe_rk4_steps_members",
     "swe_set_kernel_config", "swe_get_kernel_config", "swe_diag", "swe_energies", "swe_curl", "swe_regrid_latlon", "swe_regrid_latlon_wind",
+    "swe_set_orography",
 ]
 
 
@@ -78,6 +79,7 @@ def load(path: str = LIB_PATH):
     L.swe_set_stream.argtypes = [_vp, _vp]
     L.swe_synchronize.argtypes = [_vp]
     L.swe_set_member_h_mean.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
+    L.swe_set_orography.argtypes = [_vp, _vp]
     L.swe_stvec_create.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.swe_stvec_destroy.argtypes = [_vp]
     L.swe_stvec_upload.argtypes = [_vp, ctypes.c_int, _dp, _dp, _dp]

@@ -16,11 +16,16 @@ OBJDIR = os.path.join(HERE, "_build")
 # unit per precision and maximal tile for the stage and contravariant kernels: small
 # device modules, compiled in parallel
 STAGE_SOURCES = [f"stage_{p}{tm}.cu" for p in ("f", "d") for tm in (17, 25, 33)]
-SOURCES = ["swe_api.cu", *STAGE_SOURCES]
-COMMON_HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh", "swe_launch.cuh"]
-UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh"]}
+# the fused stage (TMA tiles, contravariant components in the stage) and its edge-strip
+# kernel, one unit per precision
+FUSED_SOURCES = ["fused_f.cu", "fused_d.cu"]
+SOURCES = ["swe_api.cu", *STAGE_SOURCES, *FUSED_SOURCES]
+COMMON_HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh", "swe_launch.cuh",
+                  "swe_fused.cuh", "swe_tma.cuh"]
+UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh"],
+                **{src: COMMON_HEADERS + ["fused_tu.cuh"] for src in FUSED_SOURCES}}
 STAGE_HEADERS = COMMON_HEADERS + ["swe_tiled.cuh", "swe_stage_tu.cuh"]
-HEADERS = sorted(set(COMMON_HEADERS + UNIT_HEADERS["swe_api.cu"] + STAGE_HEADERS))
+HEADERS = sorted(set(COMMON_HEADERS + UNIT_HEADERS["swe_api.cu"] + STAGE_HEADERS + ["fused_tu.cuh"]))
 DEPS = SOURCES + HEADERS
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -2,6 +2,7 @@
 // and state-vector management, host-side FP64 geometry, kernel launches and
 // CUDA-graph capture of the RK4 loop.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdarg>
@@ -255,6 +256,15 @@ struct swe_ctx {
     int occ = 2;                     // resident blocks per SM of the stage kernels' register cap
     int runs = 0;                    // 1: stencil runs of several outputs per thread
     int ord = 42;                    // SBP order of the Ch operators (42 or 21)
+    // fused stage (swe_fused.cuh) of the linear Ch 4-2 operator: selected instead of the
+    // three split kernels when `fused`; (fth, focc) is its configuration.  The split
+    // configuration above stays valid for the diagnostics that launch k_co2contra.
+    bool fused = false;
+    int fth = 25, focc = 3;
+    void *fmet = nullptr;            // FM_BOXES metric boxes of the fused stage (built on first use)
+    CUtensorMap tm_metric;           // TMA map of fmet
+    int *derr = nullptr;             // device error word: a bounded wait in a kernel gave up
+    bool launch_miss = false;        // a stage or contravariant launch found no built configuration
     bool graph_members = false;      // the cached graph uses the per-member time steps
     double *dtm = nullptr;           // per-member time steps (device), swe_rk4_steps_members
     // advective operator (cfg.operator_kind == SWE_OP_ADVECTIVE)
@@ -265,6 +275,7 @@ struct swe_ctx {
     void *fs = nullptr;              // mass-flux edge strips
     void *vh = nullptr;              // covariant wind at the virtual points beyond the panel edges
     void *hb = nullptr;              // panel-boundary h before the in-place averaging
+    void *hs = nullptr;              // orography h_surf (one field box of panels), swe_set_orography
     double *ones = nullptr;          // per-member depth factor 1 (dh = -div F)
     double *negones = nullptr;       // per-member factor -1: the linear stage's dh is then div (outputs)
     // Ah staggering (cfg.staggering == SWE_STAG_AH): h, u, v on the vertices
@@ -279,6 +290,8 @@ struct swe_stvec {
     void *d = nullptr;       // state
     float *cmp = nullptr;    // Kahan compensation of the FP32 RK4 state update
 };
+
+static void drop_graph(swe_ctx *c);
 
 static int fail(swe_ctx *c, int code, const char *fmt, ...)
 {
@@ -297,6 +310,19 @@ static int fail(swe_ctx *c, int code, const char *fmt, ...)
     do {                                                                                                \
         cudaError_t e_ = (call);                                                                        \
         if (e_ != cudaSuccess) return fail((ctx), SWE_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// A stage or contravariant launch that found no built configuration (nothing was
+// launched), or a CUDA launch error.
+#define CU_LAUNCHED(ctx)                                                                                        \
+    do {                                                                                                        \
+        if ((ctx)->launch_miss) {                                                                               \
+            (ctx)->launch_miss = false;                                                                         \
+            return fail((ctx), SWE_EINVAL,                                                                      \
+                        "no built stage-kernel configuration matches the context's (tile, blocks per SM, runs, " \
+                        "SBP order, operator); nothing was launched");                                          \
+        }                                                                                                       \
+        CU(ctx, cudaGetLastError());                                                                            \
     } while (0)
 
 static bool g_tables_ready[64] = {false};
@@ -355,6 +381,8 @@ static cudaError_t upload_link_tables()
     if (e == cudaSuccess) e = StageTU<double, 17>::upload_tables(l, q);
     if (e == cudaSuccess) e = StageTU<double, 25>::upload_tables(l, q);
     if (e == cudaSuccess) e = StageTU<double, 33>::upload_tables(l, q);
+    if (e == cudaSuccess) e = FusedTU<float>::upload_tables(l);
+    if (e == cudaSuccess) e = FusedTU<double>::upload_tables(l);
     return e;
 }
 
@@ -433,6 +461,120 @@ static int build_metric(swe_ctx *c, DevMetric<T> &dm)
     k_edge_tables<T><<<(N + 1 + 127) / 128, 128, 0, c->stream>>>(v, c->dims, ej, ef, ea, ord_strip_lines(c->ord));
     CU(c, cudaGetLastError());
     CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fused stage: metric boxes and TMA tensor maps
+// ---------------------------------------------------------------------------
+// cuTensorMapEncodeTiled from the driver, through the runtime (no -lcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }();
+    return fn;
+}
+
+// A 2-D map over `nrows` rows of P elements at base, with tiles of bw x bh elements.
+static bool encode_rows(CUtensorMap *m, const void *base, size_t elem, int P, int64_t nrows, int bw, int bh)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)P, (cuuint64_t)nrows};
+    const cuuint64_t strides[1] = {(cuuint64_t)P * elem};
+    const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+    const cuuint32_t es[2] = {1, 1};
+    return enc(m, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base),
+               dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA tile of the fused stage for maximal tile height th: box width by precision, th + 8 rows.
+static int fused_box_w(const swe_ctx *c) { return c->elem == 8 ? FusedLayout<double, 17>::SW : FusedLayout<float, 17>::SW; }
+
+// The fused stage's metric, FP64 on the host and stored in the context's precision:
+// JQ12 = J Qi12 (xy), JQ11 = J Qi11 and 1/J (y mesh), JQ22 = J Qi22 and 1/J (x mesh),
+// 1/(J a) (xy) and f J^2 of every panel, one panel box each (FM_* order).
+template <class T>
+static int build_fused_metric(swe_ctx *c, const MetricView<T> &mv)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t box = (size_t)c->dims.ps;
+    std::vector<T> h((size_t)FM_BOXES * box, T(0));
+    HostMetric my = host_metric(N, 0.5, 0.0), mx = host_metric(N, 0.0, 0.5), mxy = host_metric(N, 0.0, 0.0);
+    const double a = c->cfg.radius;
+    T *JQ12 = h.data() + FM_JQ12 * box, *JQ11 = h.data() + FM_JQ11Y * box, *iJy = h.data() + FM_IJY * box,
+      *JQ22 = h.data() + FM_JQ22X * box, *iJx = h.data() + FM_IJX * box, *iJa = h.data() + FM_IJA * box;
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N; i++) {
+            size_t k = (size_t)(j - 1) * my.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            JQ11[o] = T(my.J[k] * my.Q1[k]);
+            iJy[o] = T(1.0 / my.J[k]);
+        }
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            size_t k = (size_t)(j - 1) * mx.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            JQ22[o] = T(mx.J[k] * mx.Q3[k]);
+            iJx[o] = T(1.0 / mx.J[k]);
+        }
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            size_t k = (size_t)(j - 1) * mxy.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            JQ12[o] = T(mxy.J[k] * mxy.Q2[k]);
+            iJa[o] = T(1.0 / (mxy.J[k] * a));
+        }
+    T *d = nullptr;
+    if (cudaMalloc(&d, h.size() * sizeof(T)) != cudaSuccess) return fail(c, SWE_ENOMEM, "fused metric allocation failed");
+    c->fmet = d;
+    CU(c, cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    // f J^2 per panel: the same values the split kernels use
+    CU(c, cudaMemcpy(d + FM_FJ2 * box, mv.fJ2, NPAN * box * sizeof(T), cudaMemcpyDeviceToDevice));
+    if (!encode_rows(&c->tm_metric, d, sizeof(T), P, (int64_t)FM_BOXES * (N + 1 + 2 * MG), fused_box_w(c), c->fth + 8))
+        return fail(c, SWE_ECUDA, "TMA tensor map of the fused metric");
+    return SWE_OK;
+}
+
+// The fused stage serves the linear operator on the Ch grid in SBP 4-2.
+static bool fused_supported(const swe_ctx *c) { return !c->adv && !c->ah && c->ord == 42; }
+
+static bool fused_cfg_built(const swe_ctx *c, int th, int occ)
+{
+#define CHSWE_FCHK(TH, OCC) if (th == TH && occ == OCC) return true;
+    if (c->elem == 4) {
+        CHSWE_FUSED_CFGS_F(CHSWE_FCHK)
+    } else {
+        CHSWE_FUSED_CFGS_D(CHSWE_FCHK)
+    }
+#undef CHSWE_FCHK
+    return false;
+}
+
+// Select the fused stage with configuration (th, occ): builds its metric on first use
+// and re-encodes the metric map for the tile height.
+static int select_fused(swe_ctx *c, int th, int occ)
+{
+    dim3 g;
+    if (!fused_supported(c) || !fused_cfg_built(c, th, occ) || !fused_grid(c->cfg.N, c->cfg.n_members, th, g))
+        return fail(c, SWE_EINVAL, "fused stage configuration (%d, %d) is not available for this context", th, occ);
+    const bool retile = c->fth != th;
+    c->fth = th;
+    c->focc = occ;
+    c->fused = true;
+    if (!c->fmet) {
+        int rc = c->elem == 8 ? build_fused_metric<double>(c, c->m64.v) : build_fused_metric<float>(c, c->m32.v);
+        if (rc) { c->fused = false; return rc; }
+    } else if (retile &&
+               !encode_rows(&c->tm_metric, c->fmet, c->elem, c->dims.P,
+                            (int64_t)FM_BOXES * (c->cfg.N + 1 + 2 * MG), fused_box_w(c), th + 8)) {
+        c->fused = false;
+        return fail(c, SWE_ECUDA, "TMA tensor map of the fused metric");
+    }
     return SWE_OK;
 }
 
@@ -790,6 +932,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
+    cudaFree(c->fmet); cudaFree(c->derr); cudaFree(c->hs);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     if (c->side) cudaStreamDestroy(c->side);
@@ -859,6 +1002,8 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     c->Hhost.assign(cfg->n_members, cfg->h_mean);
     if (cudaMalloc(&c->Hm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
     if (cudaMalloc(&c->dtm, sizeof(double) * cfg->n_members) != cudaSuccess) return bail(SWE_ENOMEM);
+    if (cudaMalloc(&c->derr, sizeof(int)) != cudaSuccess) return bail(SWE_ENOMEM);
+    if (cudaMemset(c->derr, 0, sizeof(int)) != cudaSuccess) return bail(SWE_ECUDA);
     if (cudaMemcpy(c->Hm, c->Hhost.data(), sizeof(double) * cfg->n_members, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(SWE_ECUDA);
     if ((rc = alloc_box(c, &c->ya)) || (rc = alloc_box(c, &c->yb)) || (rc = alloc_box(c, &c->acc)) ||
@@ -926,6 +1071,13 @@ extern "C" int swe_synchronize(swe_ctx *c)
 {
     if (!c) return SWE_EINVAL;
     CU(c, cudaStreamSynchronize(c->stream));
+    // a kernel whose bounded wait for its tile loads ran out leaves a flag behind
+    int flag = 0;
+    CU(c, cudaMemcpy(&flag, c->derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        CU(c, cudaMemset(c->derr, 0, sizeof(int)));
+        return fail(c, SWE_ECUDA, "a stage kernel gave up waiting for its tile loads; its outputs are incomplete");
+    }
     return SWE_OK;
 }
 
@@ -937,6 +1089,42 @@ extern "C" int swe_set_member_h_mean(swe_ctx *c, int member, double H)
     c->Hhost[member] = H;
     CU(c, cudaMemcpyAsync(c->Hm + member, &c->Hhost[member], sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
+    return SWE_OK;
+}
+
+// Orography of the advective operator: h_surf packed like h ((N+1) x (N+1) per panel),
+// shared by every member; NULL removes it.  The gradient's input becomes h + h_surf
+// (operator_adv_swm_mod.f90:37-38,78).
+extern "C" int swe_set_orography(swe_ctx *c, const double *h_surf)
+{
+    if (!c) return SWE_EINVAL;
+    if (!c->adv) return fail(c, SWE_EINVAL, "swe_set_orography: orography belongs to the advective operator");
+    if (!h_surf) {
+        if (c->hs) CU(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->hs);
+        c->hs = nullptr;
+        drop_graph(c);
+        return SWE_OK;
+    }
+    const int N = c->cfg.N, n = N + 1, P = c->dims.P;
+    const size_t box = (size_t)c->dims.ps, fbox = NPAN * box;
+    std::vector<unsigned char> host(fbox * c->elem, 0);
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const double v = h_surf[((size_t)t * n + j - 1) * n + i - 1];
+                const size_t o = t * box + (size_t)box_off(P, i, j);
+                if (c->elem == 8) ((double *)host.data())[o] = v;
+                else ((float *)host.data())[o] = (float)v;
+            }
+    const bool fresh = !c->hs;
+    if (fresh && cudaMalloc(&c->hs, host.size()) != cudaSuccess) {
+        c->hs = nullptr;
+        return fail(c, SWE_ENOMEM, "orography allocation failed");
+    }
+    CU(c, cudaMemcpyAsync(c->hs, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+    CU(c, cudaStreamSynchronize(c->stream));
+    if (fresh) drop_graph(c);   // captured steps hold the orography pointer
     return SWE_OK;
 }
 
@@ -1153,33 +1341,35 @@ static cudaError_t stage_smem_optin()
     e = StageTU<T, 17>::optin();
     if (e == cudaSuccess) e = StageTU<T, 25>::optin();
     if (e == cudaSuccess) e = StageTU<T, 33>::optin();
+    if (e == cudaSuccess) e = FusedTU<T>::optin();
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
 
 // ord: SBP order (42, 21 or 63).  Configurations are validated when set.
+// false: no built configuration matched and nothing was launched.
 template <class T>
-static void launch_co2contra(int tm, int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
+static bool launch_co2contra(int tm, int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                              const MetricView<T> &m, cudaStream_t st, const double *dtm = nullptr)
 {
     switch (tm) {
-    case 17: StageTU<T, 17>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
-    case 25: StageTU<T, 25>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
-    default: StageTU<T, 33>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm); break;
+    case 17: return StageTU<T, 17>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm);
+    case 25: return StageTU<T, 25>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm);
+    default: return StageTU<T, 33>::co2contra(occ, runs, ord, members, y, w, es, d, m, st, dtm);
     }
 }
 
 // The advective variant exists for the first blocks-per-SM value of each tile only.
 template <class T>
-static void launch_stage(int tm, int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0,
+static bool launch_stage(int tm, int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0,
                          T *y1, T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a,
                          cudaStream_t st)
 {
     if (a.A) occ = default_occ(tm);
     switch (tm) {
-    case 17: StageTU<T, 17>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    case 25: StageTU<T, 25>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
-    default: StageTU<T, 33>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st); break;
+    case 17: return StageTU<T, 17>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
+    case 25: return StageTU<T, 25>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
+    default: return StageTU<T, 33>::stage(occ, runs, ord, members, y, w, e, v0, y1, acc, cmp, d, m, a, st);
     }
 }
 
@@ -1215,6 +1405,28 @@ static void launch_ah(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc
     }
 }
 
+// One fused RK stage: edge strips, edge sync, tiles.
+template <class T>
+static bool enqueue_fused(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
+                          const double *dtm, const MetricView<T> &mv)
+{
+    const int M = c->cfg.n_members, N = c->cfg.N;
+    const FusedMetric<T> fm{(const T *)c->fmet, mv.inv_hxa, mv.inv_hx, mv.grav};
+    CUtensorMap tmY;
+    if (!encode_rows(&tmY, yin, sizeof(T), c->dims.P, (int64_t)M * 3 * NPAN * (N + 1 + 2 * MG), fused_box_w(c),
+                     c->fth + 8))
+        return false;
+    FusedTU<T>::strip(M, (const T *)yin, (T *)c->es, c->dims, fm, dtm, c->stream);
+    launch_k(k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
+             (T *)c->edge, c->dims, mv, dtm);
+    StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
+    if (!FusedTU<T>::stage(c->fth, c->focc, M, tmY, c->tm_metric, (const T *)yin, (const T *)c->edge, (T *)v0,
+                           (T *)y1, (T *)acc, (T *)cmp, c->dims, fm, a, c->derr, c->stream))
+        return false;
+    c->launches += 3;
+    return true;
+}
+
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const double *dtm,
@@ -1232,13 +1444,19 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
         return;
     }
     if (!c->adv) {
-        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
-                            c->stream, dtm);
+        if (c->fused) {
+            if (enqueue_fused<T>(c, yin, v0, y1, acc, cmp, mode, dt, dtm, mv)) return;
+            // a tensor map that cannot be encoded: the split kernels take over
+            c->fused = false;
+            c->err = "fused stage unavailable (TMA tensor map); using the split stage kernels";
+        }
+        if (!launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm)) c->launch_miss = true;
         launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
                  (T *)c->edge, c->dims, mv, dtm);
         StageArgs a{mode, dt, c->Hm, dtm, nullptr, nullptr, nullptr};
-        launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
-                        (T *)cmp, c->dims, mv, a, c->stream);
+        if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+                        (T *)cmp, c->dims, mv, a, c->stream)) c->launch_miss = true;
         c->launches += 3;
         return;
     }
@@ -1260,16 +1478,16 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
         launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->side, (T *)yin, (T *)c->hb, c->dims, dtm);
         cudaEventRecord(c->ev_havg, c->side);
         launch_k(k_vhalo<T>, vg, dim3(256), 0, c->side, (const T *)yin, (T *)c->vh, c->dims, av, M, dtm);
-        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
-                            c->stream, dtm);
+        if (!launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm)) c->launch_miss = true;
         cudaEventRecord(c->ev_co2, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_co2, 0);
         launch_k(k_uhvh<T>, pg, pb, 0, c->side, (const T *)c->w, (T *)c->ph, c->dims, dtm);
         cudaEventRecord(c->ev_side, c->side);
         cudaStreamWaitEvent(c->stream, c->ev_havg, 0);
     } else {
-        launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
-                            c->stream, dtm);
+        if (!launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                            c->stream, dtm)) c->launch_miss = true;
         launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->stream, (T *)yin, (T *)c->hb, c->dims, dtm);
     }
     launch_k(k_flux<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (T *)c->fl, (T *)c->fs, c->dims, av, dtm,
@@ -1284,9 +1502,9 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     }
     launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
              (T *)c->adt, c->dims, av, mv, dtm);
-    StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb};
-    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
-                    (T *)cmp, c->dims, mv, a, c->stream);
+    StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb, c->hs};
+    if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
+                    (T *)cmp, c->dims, mv, a, c->stream)) c->launch_miss = true;
     c->launches += 8;
 }
 
@@ -1300,7 +1518,7 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     enqueue_apply(c, vout->d, vin->d);
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     return SWE_OK;
 }
 
@@ -1311,13 +1529,13 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     if (c->ah) return fail(c, SWE_EINVAL, "swe_operator_contravariant: built for the Ch staggering");
     const int M = c->cfg.n_members;
     if (c->elem == 8)
-        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
-                                 c->m64.v, c->stream);
+        if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
+                                 c->m64.v, c->stream)) c->launch_miss = true;
     else
-        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
-                                c->m32.v, c->stream);
+        if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
+                                c->m32.v, c->stream)) c->launch_miss = true;
     c->launches++;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     return SWE_OK;
 }
 
@@ -1357,7 +1575,7 @@ extern "C" int swe_rk4_step(swe_ctx *c, swe_stvec *v0, double dt)
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     enqueue_rk4(c, v0, dt);
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     return SWE_OK;
 }
 
@@ -1376,6 +1594,11 @@ static int capture_steps(swe_ctx *c, swe_stvec *v0, double dt, bool members, int
     if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph capture: %s", cudaGetErrorString(e));
     *kernels = (int)(c->launches - before);
     c->launches = before;
+    if (c->launch_miss) {
+        cudaGraphDestroy(g);
+        c->launch_miss = false;
+        return fail(c, SWE_EINVAL, "no built stage-kernel configuration matches the context's; nothing was captured");
+    }
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(c, SWE_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
@@ -1477,7 +1700,7 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
         if (c->elem == 8) k_quad_ah<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, c->qa, c->ah64.v, c->dims, c->red);
         else k_quad_ah<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, c->qa, c->ah32.v, c->dims, c->red);
         c->launches += 1;
-        CU(c, cudaGetLastError());
+        CU_LAUNCHED(c);
         std::vector<double> part(nb * 3);
         CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CU(c, cudaStreamSynchronize(c->stream));
@@ -1494,16 +1717,16 @@ extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, doubl
     Dims d1 = c->dims;
     const size_t mo = (size_t)member * c->dims.ms;
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
-                                 c->stream);
+        if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w, (double *)c->es, d1, c->m64.v,
+                                 c->stream)) c->launch_miss = true;
         k_quad<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, c->qw, d1, c->red);
     } else {
-        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
-                                c->stream);
+        if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w, (float *)c->es, d1, c->m32.v,
+                                c->stream)) c->launch_miss = true;
         k_quad<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, c->qw, d1, c->red);
     }
     c->launches += 2;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     std::vector<double> part(nb * 4);
     CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
@@ -1564,16 +1787,16 @@ extern "C" int swe_diag(swe_ctx *c, const swe_stvec *vec, int member, double dt,
     const double dx = c->cfg.radius * (0.5 * pi / c->cfg.N);   // dx = dy on the xy mesh
     const double cxy = 1.0 / (dx * dx);
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
-                                 (double *)c->es, d1, c->m64.v, c->stream);
+        if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
+                                 (double *)c->es, d1, c->m64.v, c->stream)) c->launch_miss = true;
         k_extrema<double><<<g, b, 0, c->stream>>>((const double *)vec->d + mo, (const double *)c->w, d1, cxy, cxy, c->red);
     } else {
-        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
-                                (float *)c->es, d1, c->m32.v, c->stream);
+        if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
+                                (float *)c->es, d1, c->m32.v, c->stream)) c->launch_miss = true;
         k_extrema<float><<<g, b, 0, c->stream>>>((const float *)vec->d + mo, (const float *)c->w, d1, cxy, cxy, c->red);
     }
     c->launches += 2;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     std::vector<double> part(nb * 4);
     CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
@@ -1768,7 +1991,7 @@ extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *ou
     if (c->elem == 8) launch_curl<double>(c, (const double *)vec->d + mo, c->dims, hx, dcurl);
     else launch_curl<float>(c, (const float *)vec->d + mo, c->dims, hx, dcurl);
     c->launches += 1;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     CU(c, cudaMemcpyAsync(out, dcurl, ncurl * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
@@ -1785,16 +2008,16 @@ extern "C" int swe_energies(swe_ctx *c, const swe_stvec *vec, int member, double
     const double hx = 0.5 * 3.141592653589793238462643383279502884 / c->cfg.N;
     Dims d1 = c->dims;
     if (c->elem == 8) {
-        launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
-                                 (double *)c->es, d1, c->m64.v, c->stream);
+        if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, 1, (const double *)vec->d + mo, (double *)c->w,
+                                 (double *)c->es, d1, c->m64.v, c->stream)) c->launch_miss = true;
         launch_energies<double>(c, (const double *)vec->d + mo, d1, hx, nb);
     } else {
-        launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
-                                (float *)c->es, d1, c->m32.v, c->stream);
+        if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, 1, (const float *)vec->d + mo, (float *)c->w,
+                                (float *)c->es, d1, c->m32.v, c->stream)) c->launch_miss = true;
         launch_energies<float>(c, (const float *)vec->d + mo, d1, hx, nb);
     }
     c->launches += 2;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     std::vector<double> part(nb * 4);
     CU(c, cudaMemcpyAsync(part.data(), c->red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
@@ -2147,16 +2370,16 @@ static int enqueue_div(swe_ctx *c, const void *yin, const MetricView<T> &mv)
         }
         CU(c, cudaMemcpy(c->negones, neg.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     }
-    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
-                        c->stream, nullptr);
+    if (!launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv,
+                        c->stream, nullptr)) c->launch_miss = true;
     launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c),
              dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es, (T *)c->edge, c->dims, mv,
              (const double *)nullptr);
     StageArgs a{0, 0.0, c->negones, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, nullptr,
-                    (T *)c->ya, nullptr, nullptr, c->dims, mv, a, c->stream);
+    if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, nullptr,
+                    (T *)c->ya, nullptr, nullptr, c->dims, mv, a, c->stream)) c->launch_miss = true;
     c->launches += 3;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     return SWE_OK;
 }
 
@@ -2190,7 +2413,7 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
     else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)src + mo, c->dims, kt, wt, ext);
     k_latlon<<<g2, b, 0, c->stream>>>(ext, c->ll_i, c->ll_d, N, np, dout);
     c->launches += 2;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     CU(c, cudaMemcpyAsync(out, dout, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
     return SWE_OK;
@@ -2221,7 +2444,7 @@ extern "C" int swe_regrid_latlon_wind(swe_ctx *c, const swe_stvec *vec, int memb
     else k_ecs_vec_ext<float><<<g1, b, 0, c->stream>>>((const float *)vec->d + mo, c->dims, kt, wt, tm, extu, extv);
     k_latlon_vec<<<g2, b, 0, c->stream>>>(extu, extv, c->ll_i, c->ll_d, qr, N, np, uo, vo);
     c->launches += 2;
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     CU(c, cudaMemcpyAsync(u_out, uo, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaMemcpyAsync(v_out, vo, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(c, cudaStreamSynchronize(c->stream));
@@ -2249,16 +2472,36 @@ static void timed_stage(swe_ctx *c, const MetricView<T> &mv, const void *yin, vo
                         double dt, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, cudaEvent_t e3)
 {
     const int M = c->cfg.n_members;
+    if (c->fused) {
+        // fused stage: the edge-strip kernel, the edge sync, the tiles
+        const FusedMetric<T> fm{(const T *)c->fmet, mv.inv_hxa, mv.inv_hx, mv.grav};
+        CUtensorMap tmY;
+        if (encode_rows(&tmY, yin, sizeof(T), c->dims.P, (int64_t)M * 3 * NPAN * (c->cfg.N + 1 + 2 * MG),
+                        fused_box_w(c), c->fth + 8)) {
+            cudaEventRecord(e0, c->stream);
+            FusedTU<T>::strip(M, (const T *)yin, (T *)c->es, c->dims, fm, nullptr, c->stream);
+            cudaEventRecord(e1, c->stream);
+            launch_k(k_edge<T, 42>, edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es,
+                     (const T *)c->es, (T *)c->edge, c->dims, mv, (const double *)nullptr);
+            cudaEventRecord(e2, c->stream);
+            StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
+            FusedTU<T>::stage(c->fth, c->focc, M, tmY, c->tm_metric, (const T *)yin, (const T *)c->edge, (T *)v0,
+                              (T *)y1, (T *)c->acc, (T *)cmp, c->dims, fm, a, c->derr, c->stream);
+            cudaEventRecord(e3, c->stream);
+            c->launches += 3;
+            return;
+        }
+    }
     cudaEventRecord(e0, c->stream);
-    launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream);
+    if (!launch_co2contra<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (T *)c->w, (T *)c->es, c->dims, mv, c->stream)) c->launch_miss = true;
     cudaEventRecord(e1, c->stream);
     launch_k(c->ord == 21 ? k_edge<T, 21> : (c->ord == 63 ? k_edge<T, 63> : k_edge<T, 42>), edge_grid(c), dim3(EDGE_THREADS), 0, c->stream, (const T *)c->es, (const T *)c->es,
              (T *)c->edge, c->dims, mv, (const double *)nullptr);
     cudaEventRecord(e2, c->stream);
     StageArgs a{mode, dt, c->Hm, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
+    if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)c->acc,
                     (T *)cmp,
-                    c->dims, mv, a, c->stream);
+                    c->dims, mv, a, c->stream)) c->launch_miss = true;
     cudaEventRecord(e3, c->stream);
     c->launches += 3;
 }
@@ -2283,7 +2526,7 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
             else
                 timed_stage<float>(c, c->m32.v, bufs_in[s], v0->d, bufs_out[s], v0->cmp, s + 1, dt, e[0], e[1], e[2], e[3]);
         }
-    CU(c, cudaGetLastError());
+    CU_LAUNCHED(c);
     CU(c, cudaStreamSynchronize(c->stream));
     double t_co = 0.0, t_ed = 0.0, t_st = 0.0;
     for (int q = 0; q < nst; q++) {
@@ -2311,6 +2554,7 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int NA_MAXN = SWE_NOALLOC_MAX_N;
+constexpr int NA_TILE = 33, NA_OCC = 2;   // stage-kernel configuration of the allocation-free apply
 constexpr int NA_ROWS = NA_MAXN + 1 + 2 * MG;
 constexpr int NA_P = (NA_ROWS + 7) / 8 * 8;
 constexpr size_t NA_BOX = (size_t)NA_ROWS * NA_P;
@@ -2503,14 +2747,18 @@ extern "C" int swe_operator_apply_noalloc(const swe_cfg *cfg, const double *vin,
         nd.cached = *cfg;
         nd.metric_ok = true;
     }
-    // the contravariant scratch is read with its zero margins: clear what this size uses
+    // the contravariant scratch is read with its zero margins, and the edge strips of an
+    // earlier call of another size hold that size's layout: clear what this size uses
     if (cudaMemsetAsync(W, 0, (size_t)dm.ms * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
+    if (cudaMemsetAsync(ES, 0, (size_t)strip_member(N, 1) * sizeof(double), st) != cudaSuccess) return SWE_ECUDA;
     k_noalloc_set<<<1, 1, 0, st>>>(Hp, cfg->h_mean);
-    launch_co2contra<double>(33, 2, 0, 42, 1, vin, W, ES, dm, mv, st);
+    static_assert(linear42_built(NA_TILE, NA_OCC, 0), "the allocation-free apply uses a built configuration");
+    if (!launch_co2contra<double>(NA_TILE, NA_OCC, 0, 42, 1, vin, W, ES, dm, mv, st)) return SWE_ECUDA;
     launch_k(k_edge<double, 42>, edge_grid(N, 1), dim3(EDGE_THREADS), 0, st, (const double *)ES, (const double *)ES, E, dm,
              mv, (const double *)nullptr);
     StageArgs a{0, 0.0, Hp, nullptr, nullptr, nullptr, nullptr};
-    launch_stage<double>(33, 2, 0, 42, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st);
+    if (!launch_stage<double>(NA_TILE, NA_OCC, 0, 42, 1, vin, W, E, nullptr, vout, nullptr, nullptr, dm, mv, a, st))
+        return SWE_ECUDA;
     if (cudaGetLastError() != cudaSuccess) return SWE_ECUDA;
     return SWE_OK;
 }
@@ -2532,30 +2780,53 @@ static void set_cfg(swe_ctx *c, int tile, int occ, int runs)
     c->runs = runs;
 }
 
+// runs 0 / 1: the split stage kernels (tile, blocks per SM, stencil runs); runs 2: the
+// fused stage with tiles of at most `tile` rows (17, 25 or 33) and FUSED_TW columns.
+static int apply_cfg(swe_ctx *c, int tile, int occ, int runs)
+{
+    if (runs == 2) {
+        const bool changed = !c->fused || c->fth != tile || c->focc != occ;
+        int rc = select_fused(c, tile, occ);
+        if (rc) return rc;
+        if (changed) drop_graph(c);
+        return SWE_OK;
+    }
+    if (c->fused) drop_graph(c);
+    c->fused = false;
+    set_cfg(c, tile, occ, runs);
+    return SWE_OK;
+}
+
 extern "C" int swe_set_tile(swe_ctx *c, int tile)
 {
     if (!c || !valid_tile(tile)) return SWE_EINVAL;
-    set_cfg(c, tile, default_occ(tile), 0);
-    return SWE_OK;
+    return apply_cfg(c, tile, default_occ(tile), 0);
 }
 
 extern "C" int swe_get_tile(const swe_ctx *c, int *tile)
 {
     if (!c || !tile) return SWE_EINVAL;
-    *tile = c->tile;
+    *tile = c->fused ? c->fth : c->tile;
     return SWE_OK;
 }
 
 extern "C" int swe_set_kernel_config(swe_ctx *c, int tile, int blocks_per_sm, int runs)
 {
-    if (!c || !valid_cfg(c->ord, tile, blocks_per_sm, runs)) return SWE_EINVAL;
-    set_cfg(c, tile, blocks_per_sm, runs);
-    return SWE_OK;
+    if (!c) return SWE_EINVAL;
+    if (runs == 2) return apply_cfg(c, tile, blocks_per_sm, runs);
+    if (!valid_cfg(c->ord, tile, blocks_per_sm, runs)) return SWE_EINVAL;
+    return apply_cfg(c, tile, blocks_per_sm, runs);
 }
 
 extern "C" int swe_get_kernel_config(const swe_ctx *c, int *tile, int *blocks_per_sm, int *runs)
 {
     if (!c || !tile || !blocks_per_sm || !runs) return SWE_EINVAL;
+    if (c->fused) {
+        *tile = c->fth;
+        *blocks_per_sm = c->focc;
+        *runs = 2;
+        return SWE_OK;
+    }
     *tile = c->tile;
     *blocks_per_sm = c->occ;
     *runs = c->runs;
@@ -2597,7 +2868,7 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     const TuneKey key{c->device, c->cfg.N, c->cfg.precision, c->cfg.n_members, c->cfg.operator_kind, c->ord};
     for (const TuneEntry &e : g_tuned)
         if (e.key == key) {
-            set_cfg(c, e.tile, e.occ, e.runs);
+            if (int rc = apply_cfg(c, e.tile, e.occ, e.runs)) return rc;
             if (c->branches != e.branches) drop_graph(c);
             c->branches = e.branches;
             if (best_tile) *best_tile = e.tile;
@@ -2607,7 +2878,8 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     swe_stvec *v = nullptr;
     int rc = swe_stvec_create(c, &v);
     if (rc) return rc;
-    const int keep_tile = c->tile, keep_occ = c->occ, keep_runs = c->runs;
+    const int keep_tile = c->fused ? c->fth : c->tile, keep_occ = c->fused ? c->focc : c->occ,
+              keep_runs = c->fused ? 2 : c->runs;
     double ms[3] = {1e300, 1e300, 1e300};
     int best_t = keep_tile, best_o = keep_occ, best_r = keep_runs;
     double best_ms = 1e300;
@@ -2619,10 +2891,21 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     const int warm = (nreps >= GRAPH_STEPS ? GRAPH_STEPS : 0) + (nreps % GRAPH_STEPS ? 1 : 0);
     int ncfg = 0;
     const KernelCfg *cfgs = cfgs_of(c->ord, &ncfg);
-    for (int k = 0; k < ncfg && rc == SWE_OK; k++) {
-        const KernelCfg kc = cfgs[k];
+    std::vector<KernelCfg> all(cfgs, cfgs + ncfg);
+    if (fused_supported(c)) {
+        // the fused stage's configurations of this precision
+#define CHSWE_FADD(TH, OCC) all.push_back(KernelCfg{TH, OCC, 2});
+        if (c->elem == 4) {
+            CHSWE_FUSED_CFGS_F(CHSWE_FADD)
+        } else {
+            CHSWE_FUSED_CFGS_D(CHSWE_FADD)
+        }
+#undef CHSWE_FADD
+    }
+    for (size_t k = 0; k < all.size() && rc == SWE_OK; k++) {
+        const KernelCfg kc = all[k];
         if (c->adv && kc.occ != default_occ(kc.tile)) continue;
-        set_cfg(c, kc.tile, kc.occ, kc.runs);
+        if (apply_cfg(c, kc.tile, kc.occ, kc.runs) != SWE_OK) continue;   // a fused tile the cube cannot take
         // untimed: capture and instantiate the graphs the timed steps replay
         if ((rc = swe_rk4_steps(c, v, dt, warm)) != SWE_OK) break;
         if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(c, SWE_ECUDA, "autotune record"); break; }
@@ -2642,7 +2925,7 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     // stream and on one stream (forking pays for small cubes, not always for C384)
     bool best_b = c->branches;
     if (rc == SWE_OK && c->side) {
-        set_cfg(c, best_t, best_o, best_r);
+        apply_cfg(c, best_t, best_o, best_r);
         double tb[2] = {1e300, 1e300};
         for (int b = 0; b < 2 && rc == SWE_OK; b++) {
             drop_graph(c);
@@ -2664,8 +2947,8 @@ extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_pe
     if (e1) cudaEventDestroy(e1);
     swe_stvec_destroy(v);
     drop_graph(c);
-    if (rc != SWE_OK) { set_cfg(c, keep_tile, keep_occ, keep_runs); return rc; }
-    set_cfg(c, best_t, best_o, best_r);
+    if (rc != SWE_OK) { apply_cfg(c, keep_tile, keep_occ, keep_runs); return rc; }
+    if ((rc = apply_cfg(c, best_t, best_o, best_r)) != SWE_OK) return rc;
     TuneEntry te{key, best_t, best_o, best_r, {ms[0], ms[1], ms[2]}, best_b};
     g_tuned.push_back(te);
     if (best_tile) *best_tile = best_t;

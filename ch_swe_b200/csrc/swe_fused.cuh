@@ -1,0 +1,594 @@
+// swe_fused.cuh -- the fused stage of the linear operator on the Ch grid (SBP 4-2):
+// one kernel per RK stage that computes the contravariant components itself
+// (co2contra_Ch_mod.f90:27-94), the gradient with its SAT, the Coriolis term with
+// the ECS vector edge sync, the divergence with its SAT and scalar edge sync
+// (operator_swm_lin_mod.f90:66-108) and the RK4 update (rk4_mod.f90:28-40).
+//
+// Per RK stage three launches, chained by programmatic dependent launch:
+//   k_strip   : the contravariant components on the edge strips (normal component
+//               at depths 1..3 and tangential component on the edge line of every
+//               panel side), straight from the stage input;
+//   k_edge    : the synchronised Coriolis vector and divergence of every
+//               panel-boundary vertex from the strips (swe_kernels.cuh);
+//   k_fstage  : every point of a tile.
+// k_strip waits for the previous stage and then lets the other two launch, so
+// k_fstage's tiles load and compute while the edge sync runs; only tiles that
+// touch a panel edge wait for it, just before they need its values.
+//
+// Tiles are at most FUSED_TW = 26 columns by TH rows.  The block loads its
+// windows (h, u, v of the stage input and seven metric arrays, each the tile plus
+// four points on every side) with TMA 2-D tile loads into shared memory.  Every
+// pass maps one lane to one column and the eight warps to rows, so a warp reads
+// and writes consecutive shared-memory words for both x and y stencils (no bank
+// conflicts at any pitch), y-stencil closures are warp-uniform, and the widest
+// pass (tile + 6 columns) fits 32 lanes.
+//
+// Window slot layout: element (r, q) of every slot holds point
+// (i0 - 4 - sx + q, j0 - 4 + r), where sx aligns the TMA tile's first column to
+// 16 bytes.  Ranges of the passes (x; y is symmetric), for tile [i0, i1):
+//   vq  = JQ12 I_c2i,y(v)          nodes   [i0-3, i1+3)
+//   uq  = JQ12 I_c2i,x(u)          nodes   [i0-1, i1+2)
+//   Jut = JQ11 u + I_i2c,x(vq)     centres [i0-2, i1+1)     (JQ11 = J Qi11)
+//   Jvt = JQ22 v + I_i2c,y(uq)     nodes   [i0-1, i1+2)     (JQ22 = J Qi22)
+//   up  = fJ2 I_c2i,y(vt)          nodes   [i0-1, i1+2)     (vt = Jvt / J)
+//   vp  = -fJ2 I_c2i,x(ut)         nodes   [i0, i1)         (ut = Jut / J)
+//   div = (D_c2i,x Jut + D_c2i,y Jvt) / (hx J a)  on the tile
+// all clipped to the panel.  These are the interior stencil reaches; the SBP
+// closure rows read within [1, 5] (or the mirror) of a panel edge, which the
+// clipped ranges of a tile on that edge contain, and tiles away from the edges are
+// at least 9 points from them (tiles are at least 13 x 9 points when a panel has
+// more than one).
+#pragma once
+
+#include "swe_kernels.cuh"
+#include "swe_tma.cuh"
+
+namespace chswe {
+
+constexpr int FUSED_THREADS = 256;
+constexpr int FUSED_TW = 26;
+
+// Boxes of the fused metric allocation, in order (one panel box each; fJ2 has six).
+enum { FM_JQ12 = 0, FM_JQ11Y = 1, FM_IJY = 2, FM_JQ22X = 3, FM_IJX = 4, FM_IJA = 5, FM_FJ2 = 6, FM_BOXES = 12 };
+
+template <class T>
+struct FusedMetric {
+    const T *base;   // FM_BOXES panel boxes of the metric (the strip kernel's plain loads)
+    T inv_hxa;       // 1 / (hx a)
+    T inv_hx;        // 1 / hx
+    T grav;
+};
+
+template <class T, int TH>
+struct FusedLayout {
+    static constexpr int ALIGN = 16 / (int)sizeof(T);      // TMA x alignment, elements
+    static constexpr int SW = sizeof(T) == 4 ? 40 : 36;     // TMA box width = slot pitch
+    static constexpr int SR = TH + 8;                       // TMA box height = slot rows
+    static constexpr int BOX_BYTES = SW * SR * (int)sizeof(T);
+    static constexpr int SLOT_BYTES = (BOX_BYTES + 127) / 128 * 128;
+    static constexpr int SLOT = SLOT_BYTES / (int)sizeof(T);
+    static constexpr int NSLOT = 13;
+    static constexpr int NLOAD = 10;                        // tiles loaded per block
+    static constexpr int HALO = NSLOT * SLOT;               // the gradient SAT halos: 4 x 64
+    static constexpr int BAR_OFF = NSLOT * SLOT_BYTES + 4 * 64 * (int)sizeof(T);
+    static constexpr size_t bytes() { return (size_t)BAR_OFF + 16; }
+    static constexpr int MR = (TH + 7) / 8;                 // tile rows per warp
+    static constexpr int MW = (TH + 13) / 8;                // window rows per warp (up to TH + 6)
+    static_assert(TH + 3 <= 40, "the boundary fill covers ranges of at most 40 points");
+    static_assert(SW * (int)sizeof(T) % 16 == 0, "TMA box rows are whole 16-byte units");
+    static_assert(SW - (ALIGN - 1) >= FUSED_TW + 8, "the box covers the widest window after alignment");
+};
+
+// Product of two shared-memory lines: f(c) = p[c s] q[c s].
+template <class T>
+struct Line2 {
+    const T *p, *q;
+    int s;
+    __device__ __forceinline__ T operator()(int c) const { return p[c * s] * q[c * s]; }
+};
+
+// Closure rows out of line: one copy of each in the kernel's code, shared by every
+// pass (the passes run once per block on a cold instruction cache, so code size
+// costs more than the calls).
+template <class T> __device__ __noinline__ T ic2i_cl2(int k, int nx, Line2<T> f) { return ic2i<T>(k, nx, f); }
+
+// The SBP 4-2 operators at one output: interior rows inline, closure rows out of line.
+template <class T>
+__device__ __forceinline__ T f_ic2i(int k, int nx, const Line<T> &f)
+{
+    if (k >= 5 && k <= nx - 4) return (T(9) * (f(k) + f(k - 1)) - (f(k + 1) + f(k - 2))) * T(0.0625);
+    return ic2i_cl<T>(k, nx, f);
+}
+template <class T>
+__device__ __forceinline__ T f_ic2i(int k, int nx, const Line2<T> &f)
+{
+    if (k >= 5 && k <= nx - 4) return (T(9) * (f(k) + f(k - 1)) - (f(k + 1) + f(k - 2))) * T(0.0625);
+    return ic2i_cl2<T>(k, nx, f);
+}
+template <class T>
+__device__ __forceinline__ T f_ii2c(int k, int n, const Line<T> &f)
+{
+    if (k >= 4 && k <= n - 3) return (T(9) * (f(k + 1) + f(k)) - (f(k + 2) + f(k - 1))) * T(0.0625);
+    return ii2c_cl<T>(k, n, f);
+}
+template <class T>
+__device__ __forceinline__ T f_dc2i(int k, int nx, const Line<T> &f)
+{
+    if (k >= 5 && k <= nx - 4) return (T(27) * (f(k) - f(k - 1)) - (f(k + 1) - f(k - 2))) * T(1.0 / 24.0);
+    return dc2i_cl<T>(k, nx, f);
+}
+template <class T>
+__device__ __forceinline__ T f_di2c(int k, int n, const Line<T> &f)
+{
+    if (k >= 4 && k <= n - 3) return (T(27) * (f(k + 1) - f(k)) - (f(k + 2) - f(k - 1))) * T(1.0 / 24.0);
+    return di2c_cl<T>(k, n, f);
+}
+
+// h at the neighbour's copy of the shared vertex, read through L2 (the previous
+// stage wrote it).
+template <class T>
+__device__ __forceinline__ T h_halo_cg(const T *Y, const Dims &d, int t, int s, int a)
+{
+    const Link L = c_link[t][s];
+    const int ap = L.rev ? d.N + 2 - a : a;
+    int k, l;
+    side_vertex(d.N, L.nside, ap, 0, k, l);
+    return ld_cg(Y + d.fs * 0 + L.nb * d.ps + box_off32(d.P, k, l));
+}
+
+__device__ __forceinline__ void ftile_range(int n, int &i0, int &i1, int &j0, int &j1)
+{
+    i0 = 1 + (blockIdx.x * n) / gridDim.x;
+    i1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
+    j0 = 1 + (blockIdx.y * n) / gridDim.y;
+    j1 = 1 + ((blockIdx.y + 1) * n) / gridDim.y;
+}
+
+// Time a block waits for its tile loads before it gives up and flags an error.
+constexpr unsigned long long FUSED_WAIT_NS = 1000000000ull;
+
+//   MODE 0: out = A(y);   1: Y1 = V0 + dt/2 k, ACC = dt/6 k;   2: Y1 = V0 + dt/2 k, ACC += dt/3 k;
+//   3: Y1 = V0 + dt k, ACC += dt/3 k;   4: V0 += ACC + dt/6 k (FP32: Kahan with compensation CMP)
+// tmY: the stage input as rows of P elements ([member][field][panel][row]); tmM: the
+// fused metric ([box][row]); both with TMA boxes of SW x (TH + 8).
+template <class T, int TH, int OCC, int MODE>
+__global__ void __launch_bounds__(FUSED_THREADS, OCC)
+    k_fstage(const __grid_constant__ CUtensorMap tmY, const __grid_constant__ CUtensorMap tmM, const T *__restrict__ Yin,
+             const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP, Dims d, FusedMetric<T> fm, StageArgs a, int *err)
+{
+    constexpr int ORD = 42;
+    using SB = SbpOrder<ORD>;
+    using L = FusedLayout<T, TH>;
+    constexpr int SW = L::SW;
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    T *slot = reinterpret_cast<T *>(fsm_raw);
+    T *const sH = slot, *const sU = slot + L::SLOT, *const sV = slot + 2 * L::SLOT, *const sJQ12 = slot + 3 * L::SLOT,
+             *const sJQ11 = slot + 4 * L::SLOT, *const siJy = slot + 5 * L::SLOT, *const sJQ22 = slot + 6 * L::SLOT,
+             *const siJx = slot + 7 * L::SLOT, *const sF = slot + 8 * L::SLOT, *const siJa = slot + 9 * L::SLOT,
+             *const sVQ = slot + 10 * L::SLOT, *const sUQ = slot + 11 * L::SLOT, *const sJVT = slot + 12 * L::SLOT;
+    // slots reused once their first contents are dead
+    T *const sJUT = sJQ12, *const sUP = sVQ, *const sVP = sUQ, *const sDIV = sU;
+    T *const hl = slot + L::HALO, *const hr = hl + 64, *const hb = hr + 64, *const ht = hb + 64;
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(fsm_raw + L::BAR_OFF);
+
+    const int N = d.N, n = N + 1, P = d.P;
+    int i0, i1, j0, j1;
+    ftile_range(n, i0, i1, j0, j1);
+    const int tw = i1 - i0, th = j1 - j0;
+    const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
+    if (member_frozen(a.dtm, mem)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rows = N + 1 + 2 * MG;
+    const int cc0 = i0 - 1;                          // box column of point i0 - 4
+    const int sx = cc0 & (L::ALIGN - 1), ax = cc0 - sx;
+    // slot offset of point (i, j)
+    auto SI = [&](int i, int j) { return (j - j0 + 4) * SW + (i - i0 + 4 + sx); };
+
+    pdl_trigger();
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+        mbar_arrive_expect_tx(bar, (uint32_t)(L::NLOAD * L::BOX_BYTES));
+        const int yr = (mem * 3 * NPAN + t) * rows + (j0 - 1), fr = NPAN * rows, mr = j0 - 1;
+        tma_load_2d(sH, &tmY, bar, ax, yr);
+        tma_load_2d(sU, &tmY, bar, ax, yr + fr);
+        tma_load_2d(sV, &tmY, bar, ax, yr + 2 * fr);
+        tma_load_2d(sJQ12, &tmM, bar, ax, FM_JQ12 * rows + mr);
+        tma_load_2d(sJQ11, &tmM, bar, ax, FM_JQ11Y * rows + mr);
+        tma_load_2d(siJy, &tmM, bar, ax, FM_IJY * rows + mr);
+        tma_load_2d(sJQ22, &tmM, bar, ax, FM_JQ22X * rows + mr);
+        tma_load_2d(siJx, &tmM, bar, ax, FM_IJX * rows + mr);
+        tma_load_2d(sF, &tmM, bar, ax, (FM_FJ2 + t) * rows + mr);
+        tma_load_2d(siJa, &tmM, bar, ax, FM_IJA * rows + mr);
+    }
+    // the neighbours' copies of the panel-edge vertices for the gradient SAT
+    const bool sat_l = i0 <= SB::NSAT, sat_r = i1 - 1 >= N + 1 - SB::NSAT, sat_b = j0 <= SB::NSAT,
+               sat_t = j1 - 1 >= N + 1 - SB::NSAT;
+    {
+        const T *ym = Yin + (int64_t)mem * d.ms;
+        if (warp == 1)
+            for (int q = lane; q < th; q += 32) {
+                hl[q] = sat_l ? h_halo_cg(ym, d, t, SIDE_L, j0 + q) : T(0);
+                hr[q] = sat_r ? h_halo_cg(ym, d, t, SIDE_R, j0 + q) : T(0);
+            }
+        if (warp == 2)
+            for (int q = lane; q < tw; q += 32) {
+                hb[q] = sat_b ? h_halo_cg(ym, d, t, SIDE_B, i0 + q) : T(0);
+                ht[q] = sat_t ? h_halo_cg(ym, d, t, SIDE_T, i0 + q) : T(0);
+            }
+    }
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(bar, 0, FUSED_WAIT_NS))) {
+        // the tile loads did not arrive: record it and leave (after one more bounded
+        // wait, so that no copy is still writing this block's shared memory)
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            mbar_wait(bar, 0, FUSED_WAIT_NS);
+        }
+        return;
+    }
+
+    // ---- P1: vq = JQ12 I_c2i,y(v) on nodes [i0-3, i1+3) x [j0-1, j1+2);
+    //          uq = JQ12 I_c2i,x(u) on nodes [i0-1, i1+2) x [j0-3, j1+3)
+    {
+        const int ka = max(i0 - 3, 1), kb = min(i1 + 3, n + 1), la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        const int k = ka + lane;
+        if (k < kb) {
+            const Line<T> col{sV + SI(k, 0), SW};
+#pragma unroll 1
+            for (int m = 0; m < L::MW; m++) {
+                const int l = la + warp + 8 * m;
+                if (l >= lb) break;
+                const int o = SI(k, l);
+                sVQ[o] = sJQ12[o] * f_ic2i<T>(l, n, col);
+            }
+        }
+    }
+    {
+        const int ka = max(i0 - 1, 1), kb = min(i1 + 2, n + 1), la = max(j0 - 3, 1), lb = min(j1 + 3, n + 1);
+        const int k = ka + lane;
+        if (k < kb) {
+#pragma unroll 1
+            for (int m = 0; m < L::MW; m++) {
+                const int l = la + warp + 8 * m;
+                if (l >= lb) break;
+                const Line<T> row{sU + SI(0, l), 1};
+                const int o = SI(k, l);
+                sUQ[o] = sJQ12[o] * f_ic2i<T>(k, n, row);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- P2: J ut = JQ11 u + I_i2c,x(vq) on u points [i0-2, i1+1) x [j0-1, j1+2);
+    //          J vt = JQ22 v + I_i2c,y(uq) on v points [i0-1, i1+2) x [j0-2, j1+1)
+    {
+        const int ia = max(i0 - 2, 1), ib = min(i1 + 1, N + 1), la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        const int i = ia + lane;
+        if (i < ib) {
+#pragma unroll 1
+            for (int m = 0; m < L::MW; m++) {
+                const int j = la + warp + 8 * m;
+                if (j >= lb) break;
+                const Line<T> row{sVQ + SI(0, j), 1};
+                const int o = SI(i, j);
+                sJUT[o] = sJQ11[o] * sU[o] + f_ii2c<T>(i, N, row);
+            }
+        }
+    }
+    {
+        const int ia = max(i0 - 1, 1), ib = min(i1 + 2, n + 1), la = max(j0 - 2, 1), lb = min(j1 + 1, N + 1);
+        const int i = ia + lane;
+        if (i < ib) {
+            const Line<T> col{sUQ + SI(i, 0), SW};
+#pragma unroll 1
+            for (int m = 0; m < L::MW; m++) {
+                const int j = la + warp + 8 * m;
+                if (j >= lb) break;
+                const int o = SI(i, j);
+                sJVT[o] = sJQ22[o] * sV[o] + f_ii2c<T>(j, N, col);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- RK4 operands of this thread's points, in flight during P3 (tile column
+    // i0 + lane, rows j0 + warp + 8 m)
+    constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
+    const int64_t po = (int64_t)mem * d.ms + (int64_t)t * d.ps;
+    const int64_t fs = d.fs;
+    const int ip = i0 + lane;
+    T pv[3][L::MR], pa[3][L::MR], pc[3][L::MR];
+#pragma unroll
+    for (int m = 0; m < L::MR; m++) {
+        const int j = j0 + warp + 8 * m;
+        const bool ok = lane < tw && j < j1;
+        const bool has[3] = {ok, ok && ip <= N, ok && j <= N};
+        const int o = box_off32(P, ip, j);
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            pv[f][m] = LV && has[f] ? V0[po + o + f * fs] : T(0);
+            pa[f][m] = LA && has[f] ? ACC[po + o + f * fs] : T(0);
+            pc[f][m] = LC && has[f] ? CMP[po + o + f * fs] : T(0);
+        }
+    }
+
+    // ---- P3: the Coriolis vertex vectors and the divergence away from the panel
+    // boundary (its vertices take the synchronised values below)
+    {
+        // up = fJ2 I_c2i,y(vt) on [i0-1, i1+2) x [j0, j1)
+        const int ka = max(i0 - 1, 1), kb = min(i1 + 2, n + 1);
+        const int k = ka + lane;
+        if (k < kb && k != 1 && k != n) {
+            const Line2<T> col{sJVT + SI(k, 0), siJx + SI(k, 0), SW};
+#pragma unroll 1
+            for (int m = 0; m < L::MR; m++) {
+                const int l = j0 + warp + 8 * m;
+                if (l >= j1) break;
+                if (l == 1 || l == n) continue;
+                const int o = SI(k, l);
+                sUP[o] = sF[o] * f_ic2i<T>(l, n, col);
+            }
+        }
+    }
+    {
+        // vp = -fJ2 I_c2i,x(ut) on [i0, i1) x [j0-1, j1+2)
+        const int la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        const int k = i0 + lane;
+        if (lane < tw && k != 1 && k != n) {
+#pragma unroll 1
+            for (int m = 0; m < L::MW; m++) {
+                const int l = la + warp + 8 * m;
+                if (l >= lb) break;
+                if (l == 1 || l == n) continue;
+                const Line2<T> row{sJUT + SI(0, l), siJy + SI(0, l), 1};
+                const int o = SI(k, l);
+                sVP[o] = -sF[o] * f_ic2i<T>(k, n, row);
+            }
+        }
+    }
+    {
+        // div = (D_c2i,x(J ut) / hx + D_c2i,y(J vt) / hx) / (J a) on the tile
+        const int k = i0 + lane;
+        if (lane < tw && k != 1 && k != n) {
+            const Line<T> col{sJVT + SI(k, 0), SW};
+#pragma unroll 1
+            for (int m = 0; m < L::MR; m++) {
+                const int l = j0 + warp + 8 * m;
+                if (l >= j1) break;
+                if (l == 1 || l == n) continue;
+                const Line<T> row{sJUT + SI(0, l), 1};
+                const int o = SI(k, l);
+                sDIV[o] = (f_dc2i<T>(k, n, row) * fm.inv_hx + f_dc2i<T>(l, n, col) * fm.inv_hx) * siJa[o];
+            }
+        }
+    }
+    // ---- P4: tiles on a panel edge wait for the edge sync and take the synchronised
+    // (up, vp, div) of the panel-boundary vertices
+    if (i0 == 1 || i1 == n + 1 || j0 == 1 || j1 == n + 1) {
+        pdl_wait();
+        // up: columns [i0-1, i1+2) x rows [j0, j1); vp: [i0, i1) x [j0-1, j1+2); div: the tile.
+        // Task q: array q / 160, boundary line (q / 40) % 4 (columns 1, n, rows 1, n), offset q % 40
+        // along it (every range is at most TH + 3 <= 36 long).
+        const int ua = max(i0 - 1, 1), ub = min(i1 + 2, n + 1), va = max(j0 - 1, 1), vb = min(j1 + 2, n + 1);
+        for (int q = threadIdx.x; q < 3 * 4 * 40; q += FUSED_THREADS) {
+            const int which = q / 160, c = (q / 40) % 4, e = q % 40;
+            const int ka = which == 0 ? ua : i0, kb = which == 0 ? ub : i1;
+            const int la = which == 1 ? va : j0, lb = which == 1 ? vb : j1;
+            int k, l;
+            if (c < 2) {
+                k = c == 0 ? 1 : n;
+                l = la + e;
+                if (k < ka || k >= kb || l >= lb) continue;
+            } else {
+                l = c == 2 ? 1 : n;
+                k = ka + e;
+                if (l < la || l >= lb || k >= kb) continue;
+            }
+            T *dst = which == 0 ? sUP : (which == 1 ? sVP : sDIV);
+            dst[SI(k, l)] = ld_cg(edge_entry(E, N, mem, t, k, l) + which);
+        }
+    }
+    __syncthreads();
+
+    // ---- P5: the tendencies of the tile's points and the RK4 update
+    const T H = T(a.Hm[mem]);
+    const T dt = T(a.dtm ? a.dtm[mem] : a.dt);
+    T *v0 = V0 + po, *y1 = Y1 + po, *acc = ACC + po;
+    T *cmp = CMP ? CMP + po : nullptr;
+    if (lane < tw) {
+        const int i = ip;
+        const Line<T> hcol{sH + SI(i, 0), SW}, pcol{sVP + SI(i, 0), SW};
+#pragma unroll
+        for (int m = 0; m < L::MR; m++) {
+            const int j = j0 + warp + 8 * m;
+            if (j >= j1) break;
+            const int so = SI(i, j);
+            T k3[3];
+            k3[0] = -H * sDIV[so];
+            k3[1] = T(0);
+            k3[2] = T(0);
+            if (i <= N) {
+                const Line<T> hrow{sH + SI(0, j), 1}, prow{sUP + SI(0, j), 1};
+                T gx = f_di2c<T>(i, N, hrow);
+                if (i <= SB::NSAT) gx += T(SB::satw(i)) * (hrow(1) - hl[j - j0]);
+                if (i >= N + 1 - SB::NSAT) gx += T(SB::satw(N + 1 - i)) * (hr[j - j0] - hrow(n));
+                k3[1] = -fm.grav * (gx * fm.inv_hxa) + f_ii2c<T>(i, N, prow) * siJy[so];
+            }
+            if (j <= N) {
+                T gy = f_di2c<T>(j, N, hcol);
+                if (j <= SB::NSAT) gy += T(SB::satw(j)) * (hcol(1) - hb[lane]);
+                if (j >= N + 1 - SB::NSAT) gy += T(SB::satw(N + 1 - j)) * (ht[lane] - hcol(n));
+                gy = gy * fm.inv_hxa;
+                k3[2] = -fm.grav * gy + f_ii2c<T>(j, N, pcol) * siJx[so];
+            }
+            const int o = box_off32(P, i, j);
+            const bool has[3] = {true, i <= N, j <= N};
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (!has[f]) continue;
+                const int64_t of = o + f * fs;
+                if constexpr (MODE == 0) {
+                    y1[of] = k3[f];
+                } else if constexpr (MODE <= 3) {
+                    const T ca = (MODE == 3) ? dt : T(0.5) * dt;
+                    const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
+                    y1[of] = pv[f][m] + ca * k3[f];
+                    acc[of] = (MODE == 1) ? cb * k3[f] : pa[f][m] + cb * k3[f];
+                } else if constexpr (sizeof(T) == 4) {
+                    float sv = pv[f][m], cv = pc[f][m];
+                    kahan_add(sv, cv, pa[f][m] + (dt / T(6)) * k3[f]);
+                    v0[of] = sv;
+                    cmp[of] = cv;
+                } else {
+                    v0[of] = pv[f][m] + (pa[f][m] + (dt / T(6)) * k3[f]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The edge strips straight from the stage input.
+// ---------------------------------------------------------------------------
+// Side coordinates of side s: across index x (1 at the edge), along index y.
+//   node (x, y)  -> (i, j): L (x, y), R (n+1-x, y), B (y, x), T (y, n+1-x)
+//   NF, the covariant component normal to the side (u on L/R, v on B/T), at
+//       across centre x, along node y:  L u(x, y), R u(n-x, y), B v(y, x), T v(y, n-x)
+//   TF, the tangential component (v on L/R, u on B/T), at across node x, along centre c
+// With tq(x, y) = JQ12 I_c2i,along(TF(x, .))(y) and nq(y) = JQ12 I_c2i,across(NF(., y))(1)
+// (the first closure row), the strip lines are
+//   normal(dd, y)  = (JQn NF + I_i2c,across(tq(., y))(dd)) / Jn,   dd = 1..3
+//   tangential(c)  = (JQt TF(1, c) + I_i2c,along(nq)(c)) / Jt
+// the values k_fstage computes for the same points.  The across stencils at the far
+// sides R and T are the mirrored closure rows (the interpolations are symmetric
+// under the reversal of their inputs).
+constexpr int STRIP_CHUNK = 64;     // along-edge nodes per block
+constexpr int STRIP_THREADS = 128;
+constexpr int STRIP_BL = STRIP_CHUNK + 8;   // band length along the side
+
+template <class T>
+__global__ void __launch_bounds__(STRIP_THREADS) k_strip(const T *__restrict__ Y, T *__restrict__ ES, Dims d,
+                                                         FusedMetric<T> fm, const double *__restrict__ dtm)
+{
+    using SB = SbpOrder<42>;
+    constexpr int XN = 5, ND = SB::NDEP, NL = ND + 1;
+    constexpr int NT = NL * STRIP_CHUNK / STRIP_THREADS;                      // output tasks per thread
+    constexpr int NB1 = (XN * STRIP_BL + STRIP_THREADS - 1) / STRIP_THREADS;  // band loads per thread
+    constexpr int NB2 = (ND * STRIP_BL + STRIP_THREADS - 1) / STRIP_THREADS;
+    __shared__ T tf[XN][STRIP_BL];    // TF at across nodes 1..XN, along centres y0 ..
+    __shared__ T nf[ND][STRIP_BL];    // NF at across centres 1..ND, along nodes y0 ..
+    __shared__ T jq[XN][STRIP_BL];    // JQ12 at across nodes 1..XN, along nodes y0 ..
+    __shared__ T tq[XN][STRIP_CHUNK]; // tq at across nodes 1..XN, along nodes b0 ..
+    __shared__ T nq[STRIP_BL];        // nq along nodes y0 ..
+    const int N = d.N, n = N + 1, P = d.P;
+    const int s = blockIdx.y & 3, t = blockIdx.y >> 2, mem = blockIdx.z;
+    const int b0 = 1 + blockIdx.x * STRIP_CHUNK, b1 = min(b0 + STRIP_CHUNK, n + 1);
+    const int y0 = b0 - 4;   // band origin along the side
+    const bool lr = s <= SIDE_R, far = (s == SIDE_R || s == SIDE_T);
+    const int64_t box = d.ps;
+    const T *mJQ12 = fm.base + FM_JQ12 * box, *mJQn = fm.base + (lr ? FM_JQ11Y : FM_JQ22X) * box,
+            *miJn = fm.base + (lr ? FM_IJY : FM_IJX) * box, *mJQt = fm.base + (lr ? FM_JQ22X : FM_JQ11Y) * box,
+            *miJt = fm.base + (lr ? FM_IJX : FM_IJY) * box;
+    // panel offsets of side coordinates: node (x, y) (also the TF point at across node
+    // x, along centre y) and across-centre (x, y)
+    auto node_off = [&](int x, int y) {
+        const int xx = far ? n + 1 - x : x;
+        return lr ? box_off32(P, xx, y) : box_off32(P, y, xx);
+    };
+    auto cen_off = [&](int x, int y) {
+        const int xx = far ? n - x : x;
+        return lr ? box_off32(P, xx, y) : box_off32(P, y, xx);
+    };
+    // ---- static data first (before the previous stage completes): the JQ12 band and
+    // the metric of this thread's outputs (task q: line q / CHUNK, along b0 + q % CHUNK)
+    T rj[NB1], mq[NT], mi[NT];
+#pragma unroll
+    for (int r = 0; r < NB1; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS, x = 1 + q / STRIP_BL, y = y0 + q % STRIP_BL;
+        rj[r] = (q < XN * STRIP_BL && y >= 1 && y <= n) ? __ldg(mJQ12 + node_off(x, y)) : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < NT; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS, line = q / STRIP_CHUNK, y = b0 + q % STRIP_CHUNK;
+        mq[r] = mi[r] = T(0);
+        if (y < b1 && line < ND) {
+            const int o = cen_off(line + 1, y);
+            mq[r] = __ldg(mJQn + o);
+            mi[r] = __ldg(miJn + o);
+        } else if (y < b1 && y <= N) {
+            const int o = node_off(1, y);
+            mq[r] = __ldg(mJQt + o);
+            mi[r] = __ldg(miJt + o);
+        }
+    }
+    pdl_wait();
+    pdl_trigger();
+    if (member_frozen(dtm, mem)) return;
+    const T *yp = Y + (int64_t)mem * d.ms + (int64_t)t * d.ps;
+    const T *gNF = yp + (lr ? 1 : 2) * d.fs, *gTF = yp + (lr ? 2 : 1) * d.fs;
+    // ---- the band of the stage input, every load issued before the first store
+    T rt[NB1], rn[NB2];
+#pragma unroll
+    for (int r = 0; r < NB1; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS, x = 1 + q / STRIP_BL, y = y0 + q % STRIP_BL;
+        rt[r] = (q < XN * STRIP_BL && y >= 1 && y <= N) ? ld_cg(gTF + node_off(x, y)) : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < NB2; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS, x = 1 + q / STRIP_BL, y = y0 + q % STRIP_BL;
+        rn[r] = (q < ND * STRIP_BL && y >= 1 && y <= n) ? ld_cg(gNF + cen_off(x, y)) : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < NB1; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS;
+        if (q < XN * STRIP_BL) {
+            (&tf[0][0])[q] = rt[r];
+            (&jq[0][0])[q] = rj[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NB2; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS;
+        if (q < ND * STRIP_BL) (&nf[0][0])[q] = rn[r];
+    }
+    __syncthreads();
+    // ---- tq on the chunk, nq on the band
+    for (int q = threadIdx.x; q < XN * STRIP_CHUNK; q += STRIP_THREADS) {
+        const int x = 1 + q / STRIP_CHUNK, y = b0 + q % STRIP_CHUNK;
+        if (y >= b1) continue;
+        const Line<T> line{&tf[x - 1][0] - y0, 1};
+        tq[x - 1][y - b0] = jq[x - 1][y - y0] * f_ic2i<T>(y, n, line);
+    }
+    for (int q = threadIdx.x; q < STRIP_BL; q += STRIP_THREADS) {
+        const int y = y0 + q;
+        T v = T(0);
+        if (y >= 1 && y <= n) {
+            v = T(SB::ic1(1)) * nf[0][q];
+#pragma unroll
+            for (int dd = 2; dd <= ND; dd++) v += T(SB::ic1(dd)) * nf[dd - 1][q];
+            v = jq[0][q] * v;
+        }
+        nq[q] = v;
+    }
+    __syncthreads();
+    // ---- the strip lines: es[(s NL + line) n + b], b 1-based
+    T *es = ES + strip_member(N, mem, NL) + (int64_t)t * 4 * NL * n - 1;
+#pragma unroll
+    for (int r = 0; r < NT; r++) {
+        const int q = threadIdx.x + r * STRIP_THREADS, line = q / STRIP_CHUNK, y = b0 + q % STRIP_CHUNK;
+        if (y >= b1) continue;
+        T val;
+        if (line < ND) {
+            const Line<T> across{&tq[0][y - b0] - STRIP_CHUNK, STRIP_CHUNK};   // across(x) = tq[x-1][y-b0]
+            val = (mq[r] * nf[line][y - y0] + f_ii2c<T>(line + 1, N, across)) * mi[r];
+        } else {
+            if (y > N) continue;
+            const Line<T> along{&nq[0] - y0, 1};
+            val = (mq[r] * tf[0][y - y0] + f_ii2c<T>(y, N, along)) * mi[r];
+        }
+        es[(s * NL + line) * n + y] = val;
+    }
+}
+
+}  // namespace chswe

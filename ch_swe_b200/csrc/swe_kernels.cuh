@@ -370,6 +370,8 @@ struct StageArgs {
     const void *F;
     const void *A;
     const void *HB;    // panel-boundary h before the in-place averaging (the gradient's input)
+    const void *HS;    // advective operator: orography h_surf (one field box of panels), or null;
+                       // the gradient's input is h + h_surf (operator_adv_swm_mod.f90:78)
 };
 
 // Kahan-compensated state update for FP32 (s += inc with compensation c).

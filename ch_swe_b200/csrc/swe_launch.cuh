@@ -11,6 +11,7 @@
 #include <cstdlib>
 
 #include "swe_common.cuh"
+#include "swe_fused.cuh"
 #include "swe_kernels.cuh"
 
 namespace chswe {
@@ -31,6 +32,16 @@ namespace chswe {
 // the advective operator in SBP 2-1 and 6-3: the same configurations
 #define CHSWE_ADV21_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
 #define CHSWE_ADV63_CFGS(X) X(17, 3, 0) X(25, 2, 0) X(33, 2, 0)
+
+// Whether (tile, blocks per SM, runs) is one of the SBP 4-2 linear configurations.
+constexpr bool linear42_built(int tm, int occ, int runs)
+{
+    bool found = false;
+#define CHSWE_IS_CFG(TM, OCC, RUNS) found = found || (tm == TM && occ == OCC && runs == RUNS);
+    CHSWE_LINEAR_CFGS(CHSWE_IS_CFG)
+#undef CHSWE_IS_CFG
+    return found;
+}
 
 static inline dim3 stage_block() { return dim3(STAGE_THREADS, 1, 1); }
 
@@ -76,12 +87,42 @@ template <class T, int TM>
 struct StageTU {
     // opt in to the dynamic shared memory of every variant (current device)
     static cudaError_t optin();
-    static void co2contra(int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
+    // false: (occ, runs, ord, operator) is not a built configuration; nothing was launched
+    static bool co2contra(int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                           const MetricView<T> &m, cudaStream_t st, const double *dtm);
-    static void stage(int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0, T *y1,
+    static bool stage(int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0, T *y1,
                       T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a, cudaStream_t st);
     // this translation unit's copies of the panel links and cube edges (constant memory)
     static cudaError_t upload_tables(const Link *links, const int *cube_edges);
 };
+
+// The fused stage (swe_fused.cuh) of precision T: configurations (maximal tile
+// height, resident blocks per SM the register allocation is capped for).  Every
+// configuration takes tiles of at most FUSED_TW columns.
+#define CHSWE_FUSED_CFGS_F(X) X(17, 4) X(25, 3) X(33, 2)
+#define CHSWE_FUSED_CFGS_D(X) X(17, 2) X(25, 1)
+
+template <class T>
+struct FusedTU {
+    static cudaError_t optin();
+    // false: (th, occ) is not a built configuration, or the cube's tiles are too small
+    static bool stage(int th, int occ, int members, const CUtensorMap &tmY, const CUtensorMap &tmM, const T *y,
+                      const T *e, T *v0, T *y1, T *acc, T *cmp, const Dims &d, const FusedMetric<T> &fm,
+                      const StageArgs &a, int *err, cudaStream_t st);
+    static void strip(int members, const T *y, T *es, const Dims &d, const FusedMetric<T> &fm, const double *dtm,
+                      cudaStream_t st);
+    static cudaError_t upload_tables(const Link *links);
+};
+
+// Tiles of the fused stage: ceil((N+1) / FUSED_TW) columns and ceil((N+1) / th) rows
+// of balanced tiles; the passes' ranges assume tiles of at least 13 x 9 points
+// whenever a panel holds more than one.
+static inline bool fused_grid(int N, int members, int th, dim3 &g)
+{
+    const int n = N + 1, gx = (n + FUSED_TW - 1) / FUSED_TW, gy = (n + th - 1) / th;
+    if ((gx > 1 && n / gx < 13) || (gy > 1 && n / gy < 9)) return false;
+    g = dim3(gx, gy, NPAN * members);
+    return true;
+}
 
 }  // namespace chswe

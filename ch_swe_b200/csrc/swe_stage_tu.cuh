@@ -72,7 +72,7 @@ cudaError_t StageTU<T, TMX>::optin()
 
 // ord: SBP order (42, 21 or 63).  Configurations are validated when set.
 template <class T, int TMX>
-void StageTU<T, TMX>::co2contra(int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
+bool StageTU<T, TMX>::co2contra(int occ, int runs, int ord, int members, const T *y, T *w, T *es, const Dims &d,
                                 const MetricView<T> &m, cudaStream_t st, const double *dtm)
 {
     const dim3 g = stage_grid(d.N, members, TMX);
@@ -81,7 +81,7 @@ void StageTU<T, TMX>::co2contra(int occ, int runs, int ord, int members, const T
         if (occ == OCC && runs == RUNS && ord == ORD) {                                                           \
             launch_k(k_co2contra<T, TM, OCC, RUNS, ORD>, g, stage_block(), Co2Layout<T, TM>::bytes(), st, y, w,  \
                      es, d, m, dtm);                                                                              \
-            return;                                                                                               \
+            return true;                                                                                          \
         }                                                                                                         \
     }
 #define CHSWE_CO2_42(TM, OCC, RUNS) CHSWE_CO2(TM, OCC, RUNS, 42)
@@ -94,12 +94,13 @@ void StageTU<T, TMX>::co2contra(int occ, int runs, int ord, int members, const T
 #undef CHSWE_CO2_42
 #undef CHSWE_CO2_21
 #undef CHSWE_CO2_63
+    return false;
 }
 
 // The advective variant exists for the first blocks-per-SM value of each tile only
 // (the caller passes that value).
 template <class T, int TMX>
-void StageTU<T, TMX>::stage(int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0,
+bool StageTU<T, TMX>::stage(int occ, int runs, int ord, int members, const T *y, const T *w, const T *e, T *v0,
                             T *y1, T *acc, T *cmp, const Dims &d, const MetricView<T> &m, const StageArgs &a,
                             cudaStream_t st)
 {
@@ -108,7 +109,7 @@ void StageTU<T, TMX>::stage(int occ, int runs, int ord, int members, const T *y,
     if constexpr (TM == TMX) {                                                                                  \
         if (occ == OCC && runs == RUNS && adv == ADV && ord == ORD) {                                           \
             launch_stage_modes<T, TM, OCC, ADV, RUNS, ORD>(members, y, w, e, v0, y1, acc, cmp, d, m, a, st);    \
-            return;                                                                                             \
+            return true;                                                                                        \
         }                                                                                                       \
     }
 #define CHSWE_STG_42(TM, OCC, RUNS) CHSWE_STG(TM, OCC, RUNS, false, 42)
@@ -130,6 +131,7 @@ void StageTU<T, TMX>::stage(int occ, int runs, int ord, int members, const T *y,
 #undef CHSWE_STG_ADV
 #undef CHSWE_STG_ADV21
 #undef CHSWE_STG_ADV63
+    return false;
 }
 
 template <class T, int TMX>

@@ -469,6 +469,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
                         rh[it] = __ldg(hpre + (hi == 1 || hi == n ? hb_index(N, mem, t, hi == 1 ? SIDE_L : SIDE_R, hj)
                                                                : hb_index(N, mem, t, hj == 1 ? SIDE_B : SIDE_T, hi)));
                 }
+                // orography: the gradient's input is h + h_surf (zero margins)
+                if (ADV && a.HS && ok) rh[it] += __ldg((const T *)a.HS + t * d.ps + oh + go);
                 ru[it] = ok ? __ldg(gu + go) : T(0);
                 rjy[it] = jr ? __ldg(gjy + go) : T(0);
                 rfu[it] = ADV && jr ? __ldg(gf + go) : ru[it];
@@ -514,7 +516,15 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
         auto halo = [&](int s, int along) {
             if (!ADV) return h_halo(y, d, t, s, along);
             const Link L = c_link[t][s];
-            return __ldg(hpre + hb_index(N, mem, L.nb, L.nside, nb_along(L, n, along)));
+            const int ap = nb_along(L, n, along);
+            T hv = __ldg(hpre + hb_index(N, mem, L.nb, L.nside, ap));
+            if (a.HS) {
+                // the neighbour's h_surf at its copy of the vertex
+                int k, l;
+                side_vertex(N, L.nside, ap, 0, k, l);
+                hv += __ldg((const T *)a.HS + L.nb * d.ps + box_off(P, k, l));
+            }
+            return hv;
         };
         if (q < th) {
             if (sat_l) hx0 = halo(SIDE_L, j0 + q);

@@ -171,11 +171,15 @@ class Domain:
     # built stage-kernel configurations: (tile edge, resident blocks per SM, runs)
     KERNEL_CONFIGS = tuple((t, o, r) for r in (0, 1)
                            for t, o in ((17, 3), (17, 4), (25, 2), (25, 3), (25, 4), (33, 2), (33, 3)))
+    # the fused stage (linear operator, Ch, SBP 4-2): (maximal tile rows, blocks per SM, 2)
+    FUSED_CONFIGS = {"fp32": ((17, 4, 2), (25, 3, 2), (33, 2, 2)), "fp64": ((17, 2, 2), (25, 1, 2))}
 
     @property
     def kernel_config(self) -> tuple:
         """(tile edge, resident blocks per SM, runs) of the stage kernels; runs 1: each
-        thread evaluates runs of consecutive outputs along a stencil."""
+        thread evaluates runs of consecutive outputs along a stencil; runs 2: the fused
+        stage (contravariant components computed in the stage kernel, TMA-loaded tiles of
+        at most 26 columns and `tile` rows)."""
         t, o, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(_lib.load().swe_get_kernel_config(self.ctx, ctypes.byref(t), ctypes.byref(o), ctypes.byref(r)),
               self.ctx, "swe_get_kernel_config")
@@ -353,8 +357,6 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     elif kind == "advective_swm_operator":
         if config.get("v_components_type", "covariant") != "covariant":
             raise ValueError("advective_swm_operator: only v_components_type = 'covariant' is built for Ch")
-        if orography_generator is not None:
-            raise ValueError("advective_swm_operator: orography is not supported")
         names, want_op = ADVECTIVE_NAMES_BY_ORDER[domain.sbp_order], "advective"
     else:
         raise ValueError(f"unknown swm_op_type: {kind}")
@@ -375,7 +377,12 @@ def create_swm_operator(grav: float, config: dict, domain: Domain, orography_gen
     if abs(float(grav) - domain.grav) > 0.0:
         raise ValueError(f"grav {grav} differs from the domain's {domain.grav}")
     if want_op == "advective":
-        return OperatorSwmAdv(domain, grav)
+        op = OperatorSwmAdv(domain, grav)
+        if orography_generator is not None:
+            op.set_orography(orography_generator)
+        return op
+    if orography_generator is not None:
+        raise ValueError("linear_swm_operator has no orography")
     return OperatorSwmLin(domain, config["h_mean"], grav)
 
 
@@ -389,6 +396,25 @@ class OperatorSwmAdv(OperatorSwmLin):
 
     def set_member_h_mean(self, member: int, h_mean: float):
         raise ValueError("the advective operator has no mean depth")
+
+    def set_orography(self, orography):
+        """h_surf of the operator (set_scalar_test_field(h_surf, orography_generator, mesh_p),
+        operator_swm_factory_mod.f90:365-366): a generator with get_scalar_field(x, y, z)
+        on the unit sphere (testcases.Ts5Orography), or an array packed like h; None
+        removes it."""
+        if orography is None:
+            check(_lib.load().swe_set_orography(self.domain.ctx, None), self.domain.ctx, "orography")
+            return
+        if hasattr(orography, "get_scalar_field"):
+            from .testcases import mesh_geometry
+            r, _, _ = mesh_geometry(self.domain.N, "xy")
+            hs = orography.get_scalar_field(r[..., 0], r[..., 1], r[..., 2])
+        else:
+            hs = orography
+        hs = np.ascontiguousarray(hs, dtype=np.float64)
+        if hs.shape != state_shapes(self.domain.N)[0]:
+            raise ValueError(f"orography shape {hs.shape}, need {state_shapes(self.domain.N)[0]}")
+        check(_lib.load().swe_set_orography(self.domain.ctx, dptr(hs)), self.domain.ctx, "orography")
 
 
 class Rk4:

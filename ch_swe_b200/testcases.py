@@ -9,6 +9,10 @@ packed host layout of include/chswe.h (numpy, FP64).
   solid rotation about ``axis`` with speed u0 (test_fields_mod.f90:586-615) in covariant
   components and the balanced height (test_fields_mod.f90:857-894); ``linear_mode``
   drops the u0^2/2 term.
+* ``williamson5``    ~ setup_Williamson_test5 (.../testcases/Williamson_test5_mod.f90:30-107):
+  the test-2 height and solid rotation with h_mean 5960 m and u0 20 m/s, minus the
+  orography of ``Ts5Orography`` (ts5_orography_generator_t, test_fields_mod.f90:211-219,
+  1118-1136: a cone of 2000 m and radius pi/9 centred at (0, sqrt(3)/2, 1/2)).
 
 Geometry: equiangular gnomonic panels (src/metric/metric_2d_ecs_mod.f90:126-411) in
 the reference's panel frames (src/topology/cubed_sphere_topology_mod.f90:29-55).
@@ -93,3 +97,28 @@ def williamson2(N: int, u0: float = np.pi * EARTH_RADIUS / 6.0 / (23 * 60 * 60 +
         b = a1 if comp == 1 else a2
         out.append(np.ascontiguousarray(np.sum(vel * b, axis=-1)))
     return tuple(out)
+
+
+class Ts5Orography:
+    """ts5_orography_generator_t (test_fields_mod.f90:211-219, 1118-1136): h_surf =
+    h_mount * max(0, 1 - dist / r_mount), dist the great-circle distance (radians) to the
+    point (x_mount, y_mount, z_mount) of the unit sphere."""
+
+    def __init__(self, r_mount: float = np.pi / 9.0, h_mount: float = 2000.0, x_mount: float = 0.0,
+                 y_mount: float = 0.5 * np.sqrt(3.0), z_mount: float = 0.5):
+        self.r_mount, self.h_mount = float(r_mount), float(h_mount)
+        self.c = (float(x_mount), float(y_mount), float(z_mount))
+
+    def get_scalar_field(self, x, y, z):
+        dot = np.clip(x * self.c[0] + y * self.c[1] + z * self.c[2], -1.0, 1.0)
+        return self.h_mount * np.maximum(0.0, 1.0 - np.arccos(dot) / self.r_mount)
+
+
+def williamson5(N: int, u0: float = 20.0, h_mean: float = 5960.0, r_mount: float = np.pi / 9.0,
+                h_mount: float = 2000.0, axis=(0.0, 0.0, 1.0)):
+    """setup_Williamson_test5: returns (h, u, v, h_surf), h the fluid depth (the balanced
+    test-2 height minus the orography) and h_surf the orography on the xy mesh."""
+    h, u, v = williamson2(N, u0=u0, h_mean=h_mean, axis=axis)
+    r, _, _ = mesh_geometry(N, "xy")
+    hs = Ts5Orography(r_mount=r_mount, h_mount=h_mount).get_scalar_field(r[..., 0], r[..., 1], r[..., 2])
+    return np.ascontiguousarray(h - hs), u, v, np.ascontiguousarray(hs)

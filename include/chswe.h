@@ -100,6 +100,12 @@ int swe_set_stream(swe_ctx *ctx, void *cuda_stream);
 int swe_synchronize(swe_ctx *ctx);
 /* Per-member mean depth H (ensembles with different h_mean). */
 int swe_set_member_h_mean(swe_ctx *ctx, int member, double h_mean);
+/* Orography of the advective operator (operator_adv_swm_t%h_surf, operator_adv_swm_mod.f90:37-38;
+   filled by the test case's orography generator, operator_swm_factory_mod.f90:365-366):
+   h_surf packed like h, (N+1) x (N+1) per panel, shared by all members; NULL removes it.
+   The gradient then acts on h + h_surf (operator_adv_swm_mod.f90:78).  SWE_EINVAL on a
+   linear-operator context (the linear operator has no orography in the reference). */
+int swe_set_orography(swe_ctx *ctx, const double *h_surf);
 
 int swe_stvec_create(swe_ctx *ctx, swe_stvec **vec);
 int swe_stvec_destroy(swe_stvec *vec);
@@ -229,8 +235,10 @@ int swe_autotune(swe_ctx *ctx, int nreps, int *best_tile, double *ms_per_step);
      cfg->precision SWE_FP64, cfg->n_members 1, SWE_OP_LINEAR, SBP order 4-2.
    - The first call on a device, with that device current, looks up the array's
      device address and uploads the edge tables; make that first call before any
-     stream capture.  A call with a new geometry (N, radius, rotation) recomputes the
-     metric into the array.
+     stream capture.  A call with a new geometry (N, radius, gravity, rotation rate,
+     rotation axis, Coriolis mode) rewrites the shared metric in the array, under any call still running on
+     another stream: when the geometry changes, issue all calls on one stream or
+     synchronise before the call with the new geometry.
    - Work runs asynchronously on cuda_stream (NULL: the legacy default stream).
    - All calls share the one array, which keeps the last call's contents; calls that
      overlap on the GPU (other streams, other host threads) race on it.  Not thread-safe. */

@@ -62,6 +62,7 @@ def lib():
         L.orc_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_set_operator.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_orography.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_sbp_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_diag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, _dp]
         L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
@@ -184,6 +185,14 @@ class Oracle:
         h, u, v = self.zeros()
         lib().orc_init_gaussian(self._c, lam0, phi0, d0, amp, _p(h), _p(u), _p(v))
         return h, u, v
+
+    def set_orography(self, h_surf):
+        """Orography of the advective operator (packed like h), or None."""
+        if h_surf is None:
+            lib().orc_set_orography(self._c, None)
+        else:
+            self._hs = np.ascontiguousarray(h_surf, dtype=np.float64)
+            lib().orc_set_orography(self._c, _p(self._hs))
 
     def ts2(self, u0, h_mean, axis=(0.0, 0.0, 1.0), linear_mode=False):
         h, u, v = self.zeros()

@@ -844,6 +844,7 @@ typedef struct orc_ctx {
     int nonlinear;
     exch_t ex_xy5_full_s, ex_ch1c_u, ex_ch1c_v;
     fld_t htot, hu, hv, cu, cv, uh, vh, vau, uav, uhal, vhal;
+    double *hsurf;               /* orography h_surf on xy, [t][j][i]; NULL: none */
     /* energies and enstrophy of swm_output_diag_t: mesh o (cell centres, the Ch q mesh) */
     mesh_t mo;
     double *fo;                  /* Coriolis parameter on o, [t][j][i] */
@@ -966,6 +967,7 @@ void orc_destroy(orc_ctx *c)
     if (!c) return;
     mesh_free(&c->mxy); mesh_free(&c->mx); mesh_free(&c->my); mesh_free(&c->mo);
     free(c->fJ2); free(c->fo); free(c->fxy); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
+    free(c->hsurf);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
                     &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
@@ -1538,7 +1540,9 @@ static void op_apply_nl(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, f
     int N = c->N;
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= N + 1; j++)
-            for (int i = 1; i <= N + 1; i++) FA(&c->htot, t, i, j) = 1.0 * FA(h, t, i, j) + 1.0 * 0.0;
+            for (int i = 1; i <= N + 1; i++)
+                FA(&c->htot, t, i, j) = 1.0 * FA(h, t, i, j) +
+                                        1.0 * (c->hsurf ? c->hsurf[((size_t)t * (N + 1) + j - 1) * (N + 1) + i - 1] : 0.0);
     op_co2contra(c, &c->ut, &c->vt, u, v);
     op_massflux_up4(c, &c->hu, &c->hv, h, &c->ut, &c->vt);
     op_div(c, &c->div, &c->hu, &c->hv);
@@ -1853,6 +1857,16 @@ int orc_N(const orc_ctx *c) { return c->N; }
 
 /* operator kind: 0 linear_swm_operator, 1 advective_swm_operator (covariant Ch) */
 void orc_set_operator(orc_ctx *c, int kind) { c->nonlinear = kind == 1; }
+
+/* Orography h_surf of the advective operator (operator_adv_swm_mod.f90:37-38,78:
+   h_total = h + h_surf is the gradient's input), packed [t][j][i] on xy; NULL clears it. */
+void orc_set_orography(orc_ctx *c, const double *hs)
+{
+    const size_t n = (size_t)NPAN * (c->N + 1) * (c->N + 1);
+    if (!hs) { free(c->hsurf); c->hsurf = NULL; return; }
+    if (!c->hsurf) c->hsurf = malloc(sizeof(double) * n);
+    memcpy(c->hsurf, hs, sizeof(double) * n);
+}
 
 /* SBP order of the Ch operators (the _21 / _42 / _63 operator names of the reference's
    factories: grad_ch_sbp_sat_*, div_ch_sbp_sat_*_proj, co2contra_ch_sbp*,

@@ -185,3 +185,50 @@ def test_rk4_williamson2_tilted_sbp_orders(order):
             assert rel(g, r) < FP64_RTOL, (order, tile, name, rel(g, r))
     for a, b, name in zip(out[("fp32", 25)], out[("fp64", 25)], "huv"):
         assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5, name
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_williamson5_orography_matches_oracle(precision):
+    """The advective operator with orography (Williamson test 5: h_total = h + h_surf in
+    the gradient, operator_adv_swm_mod.f90:78): applies and RK4 steps against the oracle
+    with the same h_surf; without the orography the tendency differs at O(1)."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator, create_timescheme
+    from ch_swe_b200.testcases import Ts5Orography, williamson5
+    from oracle.oracle import Oracle
+    N = 24
+    h0, u0, v0, hs = williamson5(N)
+    # applies on an unbalanced state (the balanced one leaves a tendency of the size of the
+    # truncation error, a residual of terms 1e4 times larger)
+    rng = np.random.default_rng(55)
+    h, u, v = (x + s * rng.standard_normal(x.shape) for x, s in ((h0, 20.0), (u0, 2.0), (v0, 2.0)))
+    o = Oracle(N, h_mean=5960.0, operator="advective")
+    o.set_orography(hs)
+    ref = o.apply(h, u, v)
+    dom = create_domain(N, precision=precision, operator="advective")
+    op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom,
+                             orography_generator=Ts5Orography())
+    x = create_stvec_swm(dom).upload(h, u, v)
+    y = create_stvec_swm(dom)
+    op.apply(y, x, dom)
+    tol = FP64_RTOL if precision == "fp64" else 1e-5
+    for g, r, name in zip(y.download(), ref, "huv"):
+        assert rel(g, r) < tol, (name, rel(g, r))
+    # the orography matters: without it the wind tendency is another field
+    o.set_orography(None)
+    flat = o.apply(h, u, v)
+    assert rel(flat[1], ref[1]) > 1e-3
+    if precision == "fp64":
+        ref4 = Oracle(N, h_mean=5960.0, operator="advective")
+        ref4.set_orography(hs)
+        r4 = ref4.rk4(h0, u0, v0, 900.0, 4)
+        x.upload(h0, u0, v0)
+        create_timescheme(x, "rk4").steps(x, op, dom, 900.0, 4)
+        for g, r, name in zip(x.download(), r4, "huv"):
+            assert rel(g, r) < FP64_RTOL, ("rk4", name, rel(g, r))
+        # removing it again gives the operator without orography
+        op.set_orography(None)
+        x.upload(h, u, v)
+        op.apply(y, x, dom)
+        for g, r, name in zip(y.download(), flat, "huv"):
+            assert rel(g, r) < FP64_RTOL, ("none", name, rel(g, r))
+    dom.destroy()

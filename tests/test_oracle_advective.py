@@ -111,3 +111,22 @@ def test_advective_sbp_orders_conserve_mass_and_match_at_rest(order):
     m0 = o.integrals(h, u, v)[0]
     hs, us, vs = o.rk4(h, u, v, 600.0, 6)
     assert abs(o.integrals(hs, us, vs)[0] - m0) < 1e-13 * abs(m0)
+
+
+def test_orography_enters_the_gradient_only():
+    """operator_adv_swm_mod.f90:78: the gradient acts on h + h_surf, the mass flux on h.
+    So with orography the wind tendency equals the one of the flat operator applied to
+    h + h_surf, and the height tendency equals the flat operator's at h."""
+    from ch_swe_b200.testcases import williamson5
+    from oracle.oracle import Oracle
+    N = 16
+    h, u, v, hs = williamson5(N)
+    o = Oracle(N, h_mean=5960.0, operator="advective")
+    o.set_orography(hs)
+    dh, du, dv = o.apply(h, u, v)
+    o.set_orography(None)
+    _, du_t, dv_t = o.apply(h + hs, u, v)
+    dh_f, _, _ = o.apply(h, u, v)
+    assert np.array_equal(dh, dh_f)
+    for a, b in ((du, du_t), (dv, dv_t)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()

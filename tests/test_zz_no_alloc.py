@@ -10,6 +10,9 @@ collected last so that a run stopping at the first failure has already run
 every other test; it also passes when run alone in a fresh process.
 """
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -72,6 +75,84 @@ def test_noalloc_apply_matches_context_apply_twice(N, axis):
         got = out.download()
         for g, r, name in zip(got, ref, "huv"):
             assert _rel(g, r) < FP64_RTOL, (call, name, _rel(g, r))
+
+
+def test_noalloc_larger_then_smaller_cube():
+    """N = 64 and then N = 16: the second call reuses parts of the array that the first
+    wrote in another layout."""
+    import torch
+    from ch_swe_b200 import _lib, create_domain, create_stvec_swm, create_swm_operator, state_shapes
+    L = _lib.load()
+    for N in (64, 16):
+        dom = create_domain(N, h_mean=900.0)
+        op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 900.0}, dom)
+        cfg = _cfg(dom)
+        rng = np.random.default_rng(1000 + N)
+        h, u, v = (rng.standard_normal(s) for s in state_shapes(N))
+        x = create_stvec_swm(dom).upload(h, u, v)
+        ref_out = create_stvec_swm(dom)
+        op.apply(ref_out, x, dom)
+        ref = ref_out.download()
+        out = create_stvec_swm(dom)
+        dom.synchronize()
+        rc = L.swe_operator_apply_noalloc(ctypes.byref(cfg), x.device_view()[0], out.device_view()[0], None)
+        assert rc == 0, _lib.ERRORS.get(rc, rc)
+        torch.cuda.synchronize()
+        for g, r, name in zip(out.download(), ref, "huv"):
+            assert _rel(g, r) < FP64_RTOL, (N, name, _rel(g, r))
+        dom.destroy()
+
+
+_FRESH = r"""
+import ctypes, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from ch_swe_b200 import _lib, state_shapes
+N = 24
+L = _lib.load()
+cfg = _lib.SweCfg()
+_lib.check(L.swe_cfg_default(ctypes.byref(cfg)))
+cfg.N = N
+cfg.h_mean = 800.0
+rng = np.random.default_rng(5)
+h, u, v = (rng.standard_normal(s) for s in state_shapes(N))
+# the caller's own device buffers in the documented layout: [field][panel][N+9 rows][pitch],
+# point (i, j) at row j+3, column i+3, zero margins
+P = (N + 1 + 8 + 7) // 8 * 8
+box = np.zeros((3, 6, N + 9, P))
+box[0, :, 4:N + 5, 4:N + 5] = h
+box[1, :, 4:N + 5, 4:N + 4] = u
+box[2, :, 4:N + 4, 4:N + 5] = v
+xin = torch.tensor(box, device="cuda")
+yout = torch.zeros_like(xin)
+rc = L.swe_operator_apply_noalloc(ctypes.byref(cfg), ctypes.c_void_p(xin.data_ptr()), ctypes.c_void_p(yout.data_ptr()), None)
+assert rc == 0, rc
+torch.cuda.synchronize()
+got = yout.cpu().numpy()
+# the reference afterwards: the context-based apply
+from ch_swe_b200 import create_domain, create_stvec_swm, create_swm_operator
+dom = create_domain(N, h_mean=800.0)
+op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 800.0}, dom)
+x = create_stvec_swm(dom).upload(h, u, v)
+y = create_stvec_swm(dom)
+op.apply(y, x, dom)
+rh, ru, rv = y.download()
+for g, r in ((got[0, :, 4:N + 5, 4:N + 5], rh), (got[1, :, 4:N + 5, 4:N + 4], ru), (got[2, :, 4:N + 4, 4:N + 5], rv)):
+    err = np.abs(g - r).max() / np.abs(r).max()
+    assert err < 1e-12, err
+print("fresh-process noalloc ok")
+"""
+
+
+def test_noalloc_first_call_in_fresh_process():
+    """The first call on a device in a process that never created a context (the case
+    the entry point exists for): it looks up the array, uploads the edge tables and
+    opts the kernels in to their shared memory itself."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH, root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh-process noalloc ok" in r.stdout
 
 
 def test_noalloc_rejects_cube_above_limit():
