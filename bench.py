@@ -299,6 +299,9 @@ def run_precision(precision, ic, args, torch, dist, world):
 
 ENS_N, ENS_M, ENS_DT, ENS_STEPS, ENS_SEED = 48, 256, 600.0, 144, 20261203 + 4
 SRV_REQUESTS, SRV_RATE, SRV_SEED, SRV_BUDGET = 120, 200.0, 20261203 + 5, 24 << 30
+# a second stream of the same generator below the device's capacity (about 15 requests/s
+# of this mix): there the latency is service time, not queueing
+SRV_LOW_REQUESTS, SRV_LOW_RATE, SRV_LOW_SEED = 48, 4.0, 20261203 + 6
 NL_N, NL_DT, NL_STEPS, NL_SEED = 384, 75.0, 1152, 20261203 + 3
 
 
@@ -419,6 +422,16 @@ def run_serving(args, torch):
         if lat:
             by_size[f"C{N}"] = {"n": len(lat), "p50_ms": float(np.percentile(lat, 50)),
                                 "p99_ms": float(np.percentile(lat, 99))}
+    seq_s = sequential_seconds(reqs)
+    # the stream below capacity
+    low = serve.poisson_stream(SRV_LOW_REQUESTS, rate=SRV_LOW_RATE, seed=SRV_LOW_SEED)
+    for r in low:
+        r.ic
+    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16)
+    srv.pretune({(r.N, r.precision, r.operator) for r in low})
+    ls = srv.run(low, realtime=True)
+    srv.close()
+    offered = sum(r.cell_updates for r in low) / max(low[-1].arrival, 1e-9)
     return {
         "workload": f"{SRV_REQUESTS} requests, Poisson {SRV_RATE:g}/s (seed {SRV_SEED}), N in {list(serve.SIZES)}, "
                     "24-576 RK4 steps, FP32/FP64 50/50, linear/advective operator 50/50, 1-4 seeded Gaussians",
@@ -426,8 +439,49 @@ def run_serving(args, torch):
         "mean_ms": stats.mean_ms, "requests_per_s": stats.requests_per_s,
         "cell_updates_per_s": stats.cell_updates_per_s, "hbm_budget_bytes": SRV_BUDGET,
         "peak_pool_bytes": stats.peak_bytes, "pools": stats.pools, "latency_by_size": by_size,
+        "service_p50_ms": stats.service_p50_ms, "service_p99_ms": stats.service_p99_ms,
+        "wait_p50_ms": stats.wait_p50_ms, "wait_p99_ms": stats.wait_p99_ms,
+        "offered_cell_updates_per_s": sum(r.cell_updates for r in reqs) / max(reqs[-1].arrival, 1e-9),
+        "sequential": {"what": "the same requests one after another, each in a single-member context "
+                               "(created before the clock) with its upload and download",
+                       "seconds": seq_s, "cell_updates_per_s": sum(r.cell_updates for r in reqs) / seq_s,
+                       "served_over_sequential": (sum(r.cell_updates for r in reqs) / stats.makespan_s) /
+                                                 (sum(r.cell_updates for r in reqs) / seq_s)},
+        "below_capacity": {
+            "workload": f"{SRV_LOW_REQUESTS} requests, Poisson {SRV_LOW_RATE:g}/s (seed {SRV_LOW_SEED}), same mix",
+            "offered_cell_updates_per_s": offered, "makespan_s": ls.makespan_s,
+            "cell_updates_per_s": ls.cell_updates_per_s, "p50_ms": ls.p50_ms, "p99_ms": ls.p99_ms,
+            "service_p50_ms": ls.service_p50_ms, "service_p99_ms": ls.service_p99_ms,
+            "wait_p50_ms": ls.wait_p50_ms, "wait_p99_ms": ls.wait_p99_ms},
         "fp32_vs_fp64_sample": errs,
     }
+
+
+def sequential_seconds(reqs):
+    """Wall time of the requests run one after another without batching: one
+    single-member context per (N, precision, operator), created and autotuned before
+    the clock; each request uploads its state, integrates and downloads."""
+    from ch_swe_b200 import create_domain, create_stvec_swm, create_timescheme, serve
+    doms = {}
+    for key in sorted({(r.N, r.precision, r.operator) for r in reqs}):
+        dom = create_domain(key[0], precision=key[1], operator=key[2])
+        dom.autotune(nreps=8)
+        op = serve._operator(dom, key[2])
+        st = create_stvec_swm(dom)
+        doms[key] = (dom, op, st, create_timescheme(st, "rk4"))
+    total = 0.0
+    for r in reqs:
+        dom, op, st, ts = doms[(r.N, r.precision, r.operator)]
+        if r.operator == "linear":
+            op.set_member_h_mean(0, r.h_mean)
+        t0 = time.perf_counter()
+        st.upload(*r.initial_state())
+        ts.steps_members(st, op, [r.dt], r.nsteps)
+        st.download()
+        total += time.perf_counter() - t0
+    for dom, _, _, _ in doms.values():
+        dom.destroy()
+    return total
 
 
 def run_ensemble(args, torch, dist, world):

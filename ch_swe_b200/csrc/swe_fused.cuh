@@ -228,33 +228,56 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
         return;
     }
 
+    // Every pass below hands each lane one column and each warp a contiguous block of
+    // rows.  y stencils slide a four-value window down the column (one shared-memory
+    // load per output); x stencils read four neighbours of the row.  Interior rows use
+    // the inline interior formula, closure rows the out-of-line closure functions (the
+    // row test is warp-uniform; the column test is per lane and fixed for the pass).
+    auto rows_of = [&](int la, int lb, int &r0, int &r1) {
+        const int R = (lb - la + 7) >> 3;
+        r0 = la + warp * R;
+        r1 = min(r0 + R, lb);
+    };
+    // interior rows of the 4-2 interpolations / differences on four taps v0..v3
+    auto interp4 = [](T v0, T v1, T v2, T v3) { return (T(9) * (v2 + v1) - (v3 + v0)) * T(0.0625); };
+    auto diff4 = [](T v0, T v1, T v2, T v3) { return (T(27) * (v2 - v1) - (v3 - v0)) * T(1.0 / 24.0); };
+
     // ---- P1: vq = JQ12 I_c2i,y(v) on nodes [i0-3, i1+3) x [j0-1, j1+2);
     //          uq = JQ12 I_c2i,x(u) on nodes [i0-1, i1+2) x [j0-3, j1+3)
     {
-        const int ka = max(i0 - 3, 1), kb = min(i1 + 3, n + 1), la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        const int ka = max(i0 - 3, 1), kb = min(i1 + 3, n + 1);
+        int r0, r1;
+        rows_of(max(j0 - 1, 1), min(j1 + 2, n + 1), r0, r1);
         const int k = ka + lane;
-        if (k < kb) {
-            const Line<T> col{sV + SI(k, 0), SW};
+        if (k < kb && r0 < r1) {
+            const T *col = sV + SI(k, 0), *jq = sJQ12 + SI(k, 0);
+            T *out = sVQ + SI(k, 0);
+            T f0 = col[(r0 - 2) * SW], f1 = col[(r0 - 1) * SW], f2 = col[r0 * SW];
 #pragma unroll 1
-            for (int m = 0; m < L::MW; m++) {
-                const int l = la + warp + 8 * m;
-                if (l >= lb) break;
-                const int o = SI(k, l);
-                sVQ[o] = sJQ12[o] * f_ic2i<T>(l, n, col);
+            for (int l = r0; l < r1; l++) {
+                const T f3 = col[(l + 1) * SW];
+                const T v = (l >= 5 && l <= n - 4) ? interp4(f0, f1, f2, f3) : ic2i_cl<T>(l, n, Line<T>{col, SW});
+                out[l * SW] = jq[l * SW] * v;
+                f0 = f1; f1 = f2; f2 = f3;
             }
         }
     }
     {
-        const int ka = max(i0 - 1, 1), kb = min(i1 + 2, n + 1), la = max(j0 - 3, 1), lb = min(j1 + 3, n + 1);
+        const int ka = max(i0 - 1, 1), kb = min(i1 + 2, n + 1);
+        int r0, r1;
+        rows_of(max(j0 - 3, 1), min(j1 + 3, n + 1), r0, r1);
         const int k = ka + lane;
         if (k < kb) {
+            const T *row = sU + SI(k, r0), *jq = sJQ12 + SI(k, r0);
+            T *out = sUQ + SI(k, r0);
+            if (k >= 5 && k <= n - 4) {
 #pragma unroll 1
-            for (int m = 0; m < L::MW; m++) {
-                const int l = la + warp + 8 * m;
-                if (l >= lb) break;
-                const Line<T> row{sU + SI(0, l), 1};
-                const int o = SI(k, l);
-                sUQ[o] = sJQ12[o] * f_ic2i<T>(k, n, row);
+                for (int l = r0; l < r1; l++, row += SW, jq += SW, out += SW)
+                    *out = *jq * interp4(row[-2], row[-1], row[0], row[1]);
+            } else {
+#pragma unroll 1
+                for (int l = r0; l < r1; l++, row += SW, jq += SW, out += SW)
+                    *out = *jq * ic2i_cl<T>(k, n, Line<T>{row - k, 1});
             }
         }
     }
@@ -263,46 +286,58 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
     // ---- P2: J ut = JQ11 u + I_i2c,x(vq) on u points [i0-2, i1+1) x [j0-1, j1+2);
     //          J vt = JQ22 v + I_i2c,y(uq) on v points [i0-1, i1+2) x [j0-2, j1+1)
     {
-        const int ia = max(i0 - 2, 1), ib = min(i1 + 1, N + 1), la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        const int ia = max(i0 - 2, 1), ib = min(i1 + 1, N + 1);
+        int r0, r1;
+        rows_of(max(j0 - 1, 1), min(j1 + 2, n + 1), r0, r1);
         const int i = ia + lane;
         if (i < ib) {
+            const int o0 = SI(i, r0);
+            const T *vq = sVQ + o0, *u = sU + o0, *jq = sJQ11 + o0;
+            T *out = sJUT + o0;
+            if (i >= 4 && i <= N - 3) {
 #pragma unroll 1
-            for (int m = 0; m < L::MW; m++) {
-                const int j = la + warp + 8 * m;
-                if (j >= lb) break;
-                const Line<T> row{sVQ + SI(0, j), 1};
-                const int o = SI(i, j);
-                sJUT[o] = sJQ11[o] * sU[o] + f_ii2c<T>(i, N, row);
+                for (int j = r0; j < r1; j++, vq += SW, u += SW, jq += SW, out += SW)
+                    *out = *jq * *u + interp4(vq[-1], vq[0], vq[1], vq[2]);
+            } else {
+#pragma unroll 1
+                for (int j = r0; j < r1; j++, vq += SW, u += SW, jq += SW, out += SW)
+                    *out = *jq * *u + ii2c_cl<T>(i, N, Line<T>{vq - i, 1});
             }
         }
     }
     {
-        const int ia = max(i0 - 1, 1), ib = min(i1 + 2, n + 1), la = max(j0 - 2, 1), lb = min(j1 + 1, N + 1);
+        const int ia = max(i0 - 1, 1), ib = min(i1 + 2, n + 1);
+        int r0, r1;
+        rows_of(max(j0 - 2, 1), min(j1 + 1, N + 1), r0, r1);
         const int i = ia + lane;
-        if (i < ib) {
-            const Line<T> col{sUQ + SI(i, 0), SW};
+        if (i < ib && r0 < r1) {
+            const T *col = sUQ + SI(i, 0), *v = sV + SI(i, 0), *jq = sJQ22 + SI(i, 0);
+            T *out = sJVT + SI(i, 0);
+            T g0 = col[(r0 - 1) * SW], g1 = col[r0 * SW], g2 = col[(r0 + 1) * SW];
 #pragma unroll 1
-            for (int m = 0; m < L::MW; m++) {
-                const int j = la + warp + 8 * m;
-                if (j >= lb) break;
-                const int o = SI(i, j);
-                sJVT[o] = sJQ22[o] * sV[o] + f_ii2c<T>(j, N, col);
+            for (int j = r0; j < r1; j++) {
+                const T g3 = col[(j + 2) * SW];
+                const T I = (j >= 4 && j <= N - 3) ? interp4(g0, g1, g2, g3) : ii2c_cl<T>(j, N, Line<T>{col, SW});
+                out[j * SW] = jq[j * SW] * v[j * SW] + I;
+                g0 = g1; g1 = g2; g2 = g3;
             }
         }
     }
     __syncthreads();
 
-    // ---- RK4 operands of this thread's points, in flight during P3 (tile column
-    // i0 + lane, rows j0 + warp + 8 m)
+    // ---- RK4 operands of this thread's points (tile column i0 + lane, the warp's block
+    // of tile rows), in flight during P3
     constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
     const int64_t po = (int64_t)mem * d.ms + (int64_t)t * d.ps;
     const int64_t fs = d.fs;
     const int ip = i0 + lane;
+    int q0, q1;
+    rows_of(j0, j1, q0, q1);
     T pv[3][L::MR], pa[3][L::MR], pc[3][L::MR];
 #pragma unroll
     for (int m = 0; m < L::MR; m++) {
-        const int j = j0 + warp + 8 * m;
-        const bool ok = lane < tw && j < j1;
+        const int j = q0 + m;
+        const bool ok = lane < tw && j < q1;
         const bool has[3] = {ok, ok && ip <= N, ok && j <= N};
         const int o = box_off32(P, ip, j);
 #pragma unroll
@@ -316,50 +351,67 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
     // ---- P3: the Coriolis vertex vectors and the divergence away from the panel
     // boundary (its vertices take the synchronised values below)
     {
-        // up = fJ2 I_c2i,y(vt) on [i0-1, i1+2) x [j0, j1)
+        // up = fJ2 I_c2i,y(vt) on [i0-1, i1+2) x [j0, j1), vt = J vt / J
         const int ka = max(i0 - 1, 1), kb = min(i1 + 2, n + 1);
+        int r0, r1;
+        rows_of(j0, j1, r0, r1);
         const int k = ka + lane;
-        if (k < kb && k != 1 && k != n) {
-            const Line2<T> col{sJVT + SI(k, 0), siJx + SI(k, 0), SW};
+        if (k < kb && k != 1 && k != n && r0 < r1) {
+            const T *cj = sJVT + SI(k, 0), *ci = siJx + SI(k, 0), *fj = sF + SI(k, 0);
+            T *out = sUP + SI(k, 0);
+            T f0 = cj[(r0 - 2) * SW] * ci[(r0 - 2) * SW], f1 = cj[(r0 - 1) * SW] * ci[(r0 - 1) * SW],
+              f2 = cj[r0 * SW] * ci[r0 * SW];
 #pragma unroll 1
-            for (int m = 0; m < L::MR; m++) {
-                const int l = j0 + warp + 8 * m;
-                if (l >= j1) break;
-                if (l == 1 || l == n) continue;
-                const int o = SI(k, l);
-                sUP[o] = sF[o] * f_ic2i<T>(l, n, col);
+            for (int l = r0; l < r1; l++) {
+                const T f3 = cj[(l + 1) * SW] * ci[(l + 1) * SW];
+                if (l != 1 && l != n) {
+                    const T v = (l >= 5 && l <= n - 4) ? interp4(f0, f1, f2, f3)
+                                                       : ic2i_cl2<T>(l, n, Line2<T>{cj, ci, SW});
+                    out[l * SW] = fj[l * SW] * v;
+                }
+                f0 = f1; f1 = f2; f2 = f3;
             }
         }
     }
     {
-        // vp = -fJ2 I_c2i,x(ut) on [i0, i1) x [j0-1, j1+2)
-        const int la = max(j0 - 1, 1), lb = min(j1 + 2, n + 1);
+        // vp = -fJ2 I_c2i,x(ut) on [i0, i1) x [j0-1, j1+2), ut = J ut / J
+        int r0, r1;
+        rows_of(max(j0 - 1, 1), min(j1 + 2, n + 1), r0, r1);
         const int k = i0 + lane;
         if (lane < tw && k != 1 && k != n) {
+            const int o0 = SI(k, r0);
+            const T *rj = sJUT + o0, *ri = siJy + o0, *fj = sF + o0;
+            T *out = sVP + o0;
+            const bool kin = k >= 5 && k <= n - 4;
 #pragma unroll 1
-            for (int m = 0; m < L::MW; m++) {
-                const int l = la + warp + 8 * m;
-                if (l >= lb) break;
+            for (int l = r0; l < r1; l++, rj += SW, ri += SW, fj += SW, out += SW) {
                 if (l == 1 || l == n) continue;
-                const Line2<T> row{sJUT + SI(0, l), siJy + SI(0, l), 1};
-                const int o = SI(k, l);
-                sVP[o] = -sF[o] * f_ic2i<T>(k, n, row);
+                const T v = kin ? interp4(rj[-2] * ri[-2], rj[-1] * ri[-1], rj[0] * ri[0], rj[1] * ri[1])
+                                : ic2i_cl2<T>(k, n, Line2<T>{rj - k, ri - k, 1});
+                *out = -*fj * v;
             }
         }
     }
     {
         // div = (D_c2i,x(J ut) / hx + D_c2i,y(J vt) / hx) / (J a) on the tile
+        int r0, r1;
+        rows_of(j0, j1, r0, r1);
         const int k = i0 + lane;
-        if (lane < tw && k != 1 && k != n) {
-            const Line<T> col{sJVT + SI(k, 0), SW};
+        if (lane < tw && k != 1 && k != n && r0 < r1) {
+            const T *cj = sJVT + SI(k, 0), *ia = siJa + SI(k, 0);
+            const T *rj = sJUT + SI(k, r0);
+            T *out = sDIV + SI(k, 0);
+            const bool kin = k >= 5 && k <= n - 4;
+            T f0 = cj[(r0 - 2) * SW], f1 = cj[(r0 - 1) * SW], f2 = cj[r0 * SW];
 #pragma unroll 1
-            for (int m = 0; m < L::MR; m++) {
-                const int l = j0 + warp + 8 * m;
-                if (l >= j1) break;
-                if (l == 1 || l == n) continue;
-                const Line<T> row{sJUT + SI(0, l), 1};
-                const int o = SI(k, l);
-                sDIV[o] = (f_dc2i<T>(k, n, row) * fm.inv_hx + f_dc2i<T>(l, n, col) * fm.inv_hx) * siJa[o];
+            for (int l = r0; l < r1; l++, rj += SW) {
+                const T f3 = cj[(l + 1) * SW];
+                if (l != 1 && l != n) {
+                    const T dx = kin ? diff4(rj[-2], rj[-1], rj[0], rj[1]) : dc2i_cl<T>(k, n, Line<T>{rj - k, 1});
+                    const T dy = (l >= 5 && l <= n - 4) ? diff4(f0, f1, f2, f3) : dc2i_cl<T>(l, n, Line<T>{cj, SW});
+                    out[l * SW] = (dx * fm.inv_hx + dy * fm.inv_hx) * ia[l * SW];
+                }
+                f0 = f1; f1 = f2; f2 = f3;
             }
         }
     }
@@ -396,34 +448,51 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
     const T dt = T(a.dtm ? a.dtm[mem] : a.dt);
     T *v0 = V0 + po, *y1 = Y1 + po, *acc = ACC + po;
     T *cmp = CMP ? CMP + po : nullptr;
-    if (lane < tw) {
+    if (lane < tw && q0 < q1) {
         const int i = ip;
-        const Line<T> hcol{sH + SI(i, 0), SW}, pcol{sVP + SI(i, 0), SW};
+        const bool iu = i <= N, iin = i >= 4 && i <= N - 3;
+        const T *hc = sH + SI(i, 0), *pc_ = sVP + SI(i, 0);
+        // y windows of h (rows j-1 .. j+2) and vp
+        T h0 = hc[(q0 - 1) * SW], h1 = hc[q0 * SW], h2 = hc[(q0 + 1) * SW];
+        T p0 = pc_[(q0 - 1) * SW], p1 = pc_[q0 * SW], p2 = pc_[(q0 + 1) * SW];
 #pragma unroll
         for (int m = 0; m < L::MR; m++) {
-            const int j = j0 + warp + 8 * m;
-            if (j >= j1) break;
+            const int j = q0 + m;
+            if (j >= q1) break;
+            const T h3 = hc[(j + 2) * SW], p3 = pc_[(j + 2) * SW];
             const int so = SI(i, j);
             T k3[3];
             k3[0] = -H * sDIV[so];
             k3[1] = T(0);
             k3[2] = T(0);
-            if (i <= N) {
-                const Line<T> hrow{sH + SI(0, j), 1}, prow{sUP + SI(0, j), 1};
-                T gx = f_di2c<T>(i, N, hrow);
-                if (i <= SB::NSAT) gx += T(SB::satw(i)) * (hrow(1) - hl[j - j0]);
-                if (i >= N + 1 - SB::NSAT) gx += T(SB::satw(N + 1 - i)) * (hr[j - j0] - hrow(n));
-                k3[1] = -fm.grav * (gx * fm.inv_hxa) + f_ii2c<T>(i, N, prow) * siJy[so];
+            if (iu) {
+                const T *hr_ = sH + so, *ur = sUP + so;
+                T gx;
+                T cu;
+                if (iin) {
+                    gx = diff4(hr_[-1], hr_[0], hr_[1], hr_[2]);
+                    cu = interp4(ur[-1], ur[0], ur[1], ur[2]);
+                } else {
+                    gx = di2c_cl<T>(i, N, Line<T>{hr_ - i, 1});
+                    cu = ii2c_cl<T>(i, N, Line<T>{ur - i, 1});
+                }
+                if (i <= SB::NSAT) gx += T(SB::satw(i)) * (hr_[1 - i] - hl[j - j0]);
+                if (i >= N + 1 - SB::NSAT) gx += T(SB::satw(N + 1 - i)) * (hr[j - j0] - hr_[n - i]);
+                k3[1] = -fm.grav * (gx * fm.inv_hxa) + cu * siJy[so];
             }
             if (j <= N) {
-                T gy = f_di2c<T>(j, N, hcol);
-                if (j <= SB::NSAT) gy += T(SB::satw(j)) * (hcol(1) - hb[lane]);
-                if (j >= N + 1 - SB::NSAT) gy += T(SB::satw(N + 1 - j)) * (ht[lane] - hcol(n));
+                const bool jin = j >= 4 && j <= N - 3;
+                T gy = jin ? diff4(h0, h1, h2, h3) : di2c_cl<T>(j, N, Line<T>{hc, SW});
+                const T cv = jin ? interp4(p0, p1, p2, p3) : ii2c_cl<T>(j, N, Line<T>{pc_, SW});
+                if (j <= SB::NSAT) gy += T(SB::satw(j)) * (hc[SW] - hb[lane]);
+                if (j >= N + 1 - SB::NSAT) gy += T(SB::satw(N + 1 - j)) * (ht[lane] - hc[n * SW]);
                 gy = gy * fm.inv_hxa;
-                k3[2] = -fm.grav * gy + f_ii2c<T>(j, N, pcol) * siJx[so];
+                k3[2] = -fm.grav * gy + cv * siJx[so];
             }
+            h0 = h1; h1 = h2; h2 = h3;
+            p0 = p1; p1 = p2; p2 = p3;
             const int o = box_off32(P, i, j);
-            const bool has[3] = {true, i <= N, j <= N};
+            const bool has[3] = {true, iu, j <= N};
 #pragma unroll
             for (int f = 0; f < 3; f++) {
                 if (!has[f]) continue;
@@ -436,10 +505,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
                     y1[of] = pv[f][m] + ca * k3[f];
                     acc[of] = (MODE == 1) ? cb * k3[f] : pa[f][m] + cb * k3[f];
                 } else if constexpr (sizeof(T) == 4) {
-                    float sv = pv[f][m], cv = pc[f][m];
-                    kahan_add(sv, cv, pa[f][m] + (dt / T(6)) * k3[f]);
+                    float sv = pv[f][m], cv_ = pc[f][m];
+                    kahan_add(sv, cv_, pa[f][m] + (dt / T(6)) * k3[f]);
                     v0[of] = sv;
-                    cmp[of] = cv;
+                    cmp[of] = cv_;
                 } else {
                     v0[of] = pv[f][m] + (pa[f][m] + (dt / T(6)) * k3[f]);
                 }

@@ -227,6 +227,11 @@ class ServeStats:
     cell_updates_per_s: float
     pools: dict = field(default_factory=dict)
     peak_bytes: int = 0
+    # service time (admission to finish) and queue wait (arrival to admission)
+    service_p50_ms: float = 0.0
+    service_p99_ms: float = 0.0
+    wait_p50_ms: float = 0.0
+    wait_p99_ms: float = 0.0
 
 
 class Server:
@@ -330,13 +335,17 @@ class Server:
                 time.sleep(20e-6)
         makespan = max(r.finished for r in done) - min(r.arrival for r in done) if realtime else time.perf_counter() - t0
         lat = np.array([r.latency for r in done]) * 1e3 if realtime else np.array([0.0])
+        svc = np.array([r.finished - r.admitted for r in done]) * 1e3 if realtime else np.array([0.0])
+        wait = np.array([r.admitted - r.arrival for r in done]) * 1e3 if realtime else np.array([0.0])
         cells = sum(r.cell_updates for r in done)
         return ServeStats(
             n=len(done), makespan_s=makespan, p50_ms=float(np.percentile(lat, 50)),
             p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
             requests_per_s=len(done) / makespan, cell_updates_per_s=cells / makespan,
             pools={f"{k[2]}/C{k[0]}/{k[1]}": {"slots": p.capacity, "tile": p.dom.tile} for k, p in self.pools.items()},
-            peak_bytes=self.peak)
+            peak_bytes=self.peak,
+            service_p50_ms=float(np.percentile(svc, 50)), service_p99_ms=float(np.percentile(svc, 99)),
+            wait_p50_ms=float(np.percentile(wait, 50)), wait_p99_ms=float(np.percentile(wait, 99)))
 
     def close(self):
         for p in self.pools.values():
