@@ -18,6 +18,7 @@ SWE_OP_LINEAR = 0
 SWE_OP_ADVECTIVE = 1
 SWE_STAG_CH = 0
 SWE_STAG_AH = 1
+SWE_STAG_C = 2
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "no CUDA device",
           -5: "cube size above SWE_NOALLOC_MAX_N"}
@@ -33,7 +34,7 @@ EXPORTED = [
     "swe_kernel_times", "swe_operator_contravariant", "swe_operator_apply_noalloc",
     "swe_set_tile", "swe_get_tile", "swe_autotune", "swe_rk4_steps_members",
     "swe_set_kernel_config", "swe_get_kernel_config", "swe_diag", "swe_energies", "swe_curl", "swe_regrid_latlon", "swe_regrid_latlon_wind",
-    "swe_set_orography",
+    "swe_set_orography", "swe_c_grad", "swe_c_div",
 ]
 
 
@@ -80,6 +81,8 @@ def load(path: str = LIB_PATH):
     L.swe_synchronize.argtypes = [_vp]
     L.swe_set_member_h_mean.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
     L.swe_set_orography.argtypes = [_vp, _vp]
+    L.swe_c_grad.argtypes = [_vp, _vp, _vp]
+    L.swe_c_div.argtypes = [_vp, _vp, _vp]
     L.swe_stvec_create.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.swe_stvec_destroy.argtypes = [_vp]
     L.swe_stvec_upload.argtypes = [_vp, ctypes.c_int, _dp, _dp, _dp]

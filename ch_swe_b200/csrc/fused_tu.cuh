@@ -16,6 +16,12 @@ static cudaError_t fused_optin_modes()
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fstage<T, TH, OCC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fstage<T, TH, OCC, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fstage<T, TH, OCC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+        void (*f[5])(CUtensorMap, CUtensorMap, const T *, const T *, T *, T *, T *, T *, Dims, FusedMetric<T>,
+                     StageArgs, int *) = {k_fstage<T, TH, OCC, 0>, k_fstage<T, TH, OCC, 1>, k_fstage<T, TH, OCC, 2>,
+                                           k_fstage<T, TH, OCC, 3>, k_fstage<T, TH, OCC, 4>};
+        e = set_carveout(f[k]);
+    }
     return e;
 }
 
@@ -47,6 +53,7 @@ cudaError_t FusedTU<T>::optin()
         CHSWE_FUSED_CFGS_D(CHSWE_FOPTIN)
     }
 #undef CHSWE_FOPTIN
+    if (e == cudaSuccess) e = set_carveout(k_strip<T>);
     return e;
 }
 

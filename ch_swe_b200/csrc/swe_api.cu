@@ -17,6 +17,7 @@
 #include "swe_common.cuh"
 #include "swe_advective.cuh"
 #include "swe_ah.cuh"
+#include "swe_cgrid.cuh"
 #include "swe_kernels.cuh"
 #include "swe_launch.cuh"
 
@@ -283,6 +284,10 @@ struct swe_ctx {
     DevAh<double> ah64;
     DevAh<float> ah32;
     double *qa = nullptr;            // SBP_Ah quadrature weights J hx hy Ax Ay at the vertices (one box)
+    // C staggering (cfg.staggering == SWE_STAG_C): h on the cell centres, u on the x
+    // points, v on the y points; the C-grid gradient, divergence and co2contra
+    bool cstag = false;
+    void *cmet = nullptr;            // CMetric boxes (swe_cgrid.cuh)
 };
 
 struct swe_stvec {
@@ -576,6 +581,53 @@ static int select_fused(swe_ctx *c, int th, int occ)
         return fail(c, SWE_ECUDA, "TMA tensor map of the fused metric");
     }
     return SWE_OK;
+}
+
+// The C staggering's metric (FP64 on the host, stored in T), one panel box each:
+// 1/(J a) and J Qi12 on the cell centres, Qi11, 1/J, J on the x points, Qi22, 1/J, J on
+// the y points (metric_2d_ecs_mod.f90:338-411 on the o, x and y meshes).
+template <class T>
+static int build_c_metric(swe_ctx *c)
+{
+    const int N = c->cfg.N, P = c->dims.P;
+    const size_t box = (size_t)c->dims.ps;
+    std::vector<T> h(8 * box, T(0));
+    HostMetric mo = host_metric(N, 0.5, 0.5), mx = host_metric(N, 0.0, 0.5), my = host_metric(N, 0.5, 0.0);
+    const double a = c->cfg.radius;
+    T *iJao = h.data(), *JQ12o = iJao + box, *Q11x = JQ12o + box, *iJx = Q11x + box, *Jx = iJx + box,
+      *Q22y = Jx + box, *iJy = Q22y + box, *Jy = iJy + box;
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N; i++) {
+            const size_t k = (size_t)(j - 1) * mo.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            iJao[o] = T(1.0 / (mo.J[k] * a));
+            JQ12o[o] = T(mo.J[k] * mo.Q2[k]);
+        }
+    for (int j = 1; j <= N; j++)
+        for (int i = 1; i <= N + 1; i++) {
+            const size_t k = (size_t)(j - 1) * mx.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            Q11x[o] = T(mx.Q1[k]); iJx[o] = T(1.0 / mx.J[k]); Jx[o] = T(mx.J[k]);
+        }
+    for (int j = 1; j <= N + 1; j++)
+        for (int i = 1; i <= N; i++) {
+            const size_t k = (size_t)(j - 1) * my.nx + (i - 1), o = (size_t)box_off(P, i, j);
+            Q22y[o] = T(my.Q3[k]); iJy[o] = T(1.0 / my.J[k]); Jy[o] = T(my.J[k]);
+        }
+    T *d = nullptr;
+    if (cudaMalloc(&d, h.size() * sizeof(T)) != cudaSuccess) return fail(c, SWE_ENOMEM, "C metric allocation failed");
+    c->cmet = d;
+    CU(c, cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SWE_OK;
+}
+
+template <class T>
+static CMetric<T> c_view(const swe_ctx *c)
+{
+    const size_t box = (size_t)c->dims.ps;
+    const T *d = (const T *)c->cmet;
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = (0.25 * pi - (-0.25 * pi)) / (double)c->cfg.N;
+    return CMetric<T>{d, d + box, d + 2 * box, d + 3 * box, d + 4 * box, d + 5 * box, d + 6 * box, d + 7 * box,
+                      T(1.0 / (hx * c->cfg.radius)), T(1.0 / hx)};
 }
 
 // The Ah operator's metric at the vertices (FP64 on the host, stored in T): J, the
@@ -932,7 +984,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
-    cudaFree(c->fmet); cudaFree(c->derr); cudaFree(c->hs);
+    cudaFree(c->fmet); cudaFree(c->derr); cudaFree(c->hs); cudaFree(c->cmet);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     if (c->side) cudaStreamDestroy(c->side);
@@ -962,8 +1014,9 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     const int ord = cfg->sbp_order == 0 ? 42 : cfg->sbp_order;
     if ((ord != 42 && ord != 21 && ord != 63) || (ord == 63 && cfg->N < 16)) return SWE_EINVAL;
     // Ah staggering: the linear operator with the SBP node operators
-    if ((cfg->staggering != SWE_STAG_CH && cfg->staggering != SWE_STAG_AH) ||
-        (cfg->staggering == SWE_STAG_AH && cfg->operator_kind != SWE_OP_LINEAR))
+    if ((cfg->staggering != SWE_STAG_CH && cfg->staggering != SWE_STAG_AH && cfg->staggering != SWE_STAG_C) ||
+        (cfg->staggering != SWE_STAG_CH && cfg->operator_kind != SWE_OP_LINEAR) ||
+        (cfg->staggering == SWE_STAG_C && ord != 42))
         return SWE_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SWE_ENODEV;
@@ -997,6 +1050,11 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
     if (cfg->staggering == SWE_STAG_AH) {
         c->ah = true;
         rc = cfg->precision == SWE_FP64 ? build_ah_metric<double>(c, c->ah64) : build_ah_metric<float>(c, c->ah32);
+        if (rc != SWE_OK) return bail(rc);
+    }
+    if (cfg->staggering == SWE_STAG_C) {
+        c->cstag = true;
+        rc = cfg->precision == SWE_FP64 ? build_c_metric<double>(c) : build_c_metric<float>(c);
         if (rc != SWE_OK) return bail(rc);
     }
     c->Hhost.assign(cfg->n_members, cfg->h_mean);
@@ -1160,10 +1218,20 @@ extern "C" int swe_stvec_destroy(swe_stvec *v)
 // Packed host member (Fortran per-panel layout) <-> padded device box.
 // Points per panel of u (nx by ny) and v (ny by nx): the y and x meshes on Ch, the
 // vertices on Ah.
-static void uv_extent(const swe_ctx *c, int &nx, int &ny)
+// Packed extents (nx along i, ny along j) of field f (0 h, 1 u, 2 v) per panel: on Ch h on
+// the vertices, u on the y points, v on the x points; on Ah all on the vertices; on C h on
+// the cell centres, u on the x points, v on the y points.
+static void field_extent(const swe_ctx *c, int f, int &nx, int &ny)
 {
-    nx = c->ah ? c->cfg.N + 1 : c->cfg.N;
-    ny = c->cfg.N + 1;
+    const int N = c->cfg.N, n = N + 1;
+    if (c->ah) { nx = ny = n; return; }
+    if (c->cstag) {
+        nx = f == 0 ? N : (f == 1 ? n : N);
+        ny = f == 0 ? N : (f == 1 ? N : n);
+        return;
+    }
+    nx = f == 0 ? n : (f == 1 ? N : n);
+    ny = f == 0 ? n : (f == 1 ? n : N);
 }
 
 // Host copies between the packed arrays and the pinned staging box, one task per
@@ -1190,44 +1258,40 @@ static void panel_tasks(int count, int N, const F &task)
 template <class T>
 static void pack_panel(const swe_ctx *c, const double *h, const double *u, const double *v, T *box, int t)
 {
-    const int N = c->cfg.N, P = c->dims.P;
+    const int P = c->dims.P;
     const size_t ps = c->dims.ps, fs = c->dims.fs;
-    int nx, ny;
-    uv_extent(c, nx, ny);
-    h += (size_t)t * (N + 1) * (N + 1);
-    u += (size_t)t * nx * ny;
-    v += (size_t)t * nx * ny;
-    for (int j = 0; j <= N; j++)
-        for (int i = 0; i <= N; i++) box[0 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*h++);
-    for (int j = 0; j < ny; j++)
-        for (int i = 0; i < nx; i++) box[1 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*u++);
-    for (int j = 0; j < nx; j++)
-        for (int i = 0; i < ny; i++) box[2 * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*v++);
+    const double *src[3] = {h, u, v};
+    for (int f = 0; f < 3; f++) {
+        int nx, ny;
+        field_extent(c, f, nx, ny);
+        const double *p = src[f] + (size_t)t * nx * ny;
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) box[f * fs + t * ps + box_off(P, i + 1, j + 1)] = T(*p++);
+    }
 }
 
 template <class T>
 static void unpack_panel(const swe_ctx *c, const T *box, double *h, double *u, double *v, int t)
 {
-    const int N = c->cfg.N, P = c->dims.P;
+    const int P = c->dims.P;
     const size_t ps = c->dims.ps, fs = c->dims.fs;
-    int nx, ny;
-    uv_extent(c, nx, ny);
-    h += (size_t)t * (N + 1) * (N + 1);
-    u += (size_t)t * nx * ny;
-    v += (size_t)t * nx * ny;
-    for (int j = 0; j <= N; j++)
-        for (int i = 0; i <= N; i++) *h++ = double(box[0 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-    for (int j = 0; j < ny; j++)
-        for (int i = 0; i < nx; i++) *u++ = double(box[1 * fs + t * ps + box_off(P, i + 1, j + 1)]);
-    for (int j = 0; j < nx; j++)
-        for (int i = 0; i < ny; i++) *v++ = double(box[2 * fs + t * ps + box_off(P, i + 1, j + 1)]);
+    double *dst[3] = {h, u, v};
+    for (int f = 0; f < 3; f++) {
+        int nx, ny;
+        field_extent(c, f, nx, ny);
+        double *p = dst[f] + (size_t)t * nx * ny;
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) *p++ = double(box[f * fs + t * ps + box_off(P, i + 1, j + 1)]);
+    }
 }
 
 static size_t member_sizes(const swe_ctx *c, size_t *nh, size_t *nu)
 {
-    const size_t N = c->cfg.N;
-    *nh = NPAN * (N + 1) * (N + 1);
-    *nu = NPAN * (c->ah ? N + 1 : N) * (N + 1);
+    int hx, hy, ux, uy;
+    field_extent(c, 0, hx, hy);
+    field_extent(c, 1, ux, uy);
+    *nh = (size_t)NPAN * hx * hy;
+    *nu = (size_t)NPAN * ux * uy;
     return *nh + 2 * *nu;
 }
 
@@ -1342,6 +1406,9 @@ static cudaError_t stage_smem_optin()
     if (e == cudaSuccess) e = StageTU<T, 25>::optin();
     if (e == cudaSuccess) e = StageTU<T, 33>::optin();
     if (e == cudaSuccess) e = FusedTU<T>::optin();
+    if (e == cudaSuccess) e = set_carveout(k_edge<T, 42>);
+    if (e == cudaSuccess) e = set_carveout(k_edge<T, 21>);
+    if (e == cudaSuccess) e = set_carveout(k_edge<T, 63>);
     if (e == cudaSuccess && dev < 64) done[dev] = true;
     return e;
 }
@@ -1514,9 +1581,25 @@ static void enqueue_apply(swe_ctx *c, void *out, const void *in)
     else enqueue_stage<float>(c, in, nullptr, out, nullptr, nullptr, 0, 0.0, nullptr, c->m32.v);
 }
 
+// C-grid kernels: one thread per point of the (N+1) x (N+1) box, 32 x 8 blocks.
+static dim3 c_grid_dims(const swe_ctx *c) { const int n = c->cfg.N + 1; return dim3((n + 31) / 32, (n + 7) / 8, NPAN * c->cfg.n_members); }
+
+// The linear operator and what builds on it do not exist on the C staggering (the
+// reference's linear operator aborts in its C-grid Coriolis operator).
+#define CHSWE_NOT_ON_C(ctx, what)                                                                              \
+    do {                                                                                                       \
+        if ((ctx)->cstag)                                                                                      \
+            return fail((ctx), SWE_EINVAL,                                                                     \
+                        "%s: the linear operator on the C staggering calls coriolis_Cgrid_t%%calc_coriolis, " \
+                        "which aborts in the reference; C contexts offer swe_c_grad, swe_c_div and "          \
+                        "swe_operator_contravariant",                                                          \
+                        what);                                                                                 \
+    } while (0)
+
 extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_operator_apply");
     enqueue_apply(c, vout->d, vin->d);
     CU_LAUNCHED(c);
     return SWE_OK;
@@ -1526,7 +1609,15 @@ extern "C" int swe_operator_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *
 extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 {
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
-    if (c->ah) return fail(c, SWE_EINVAL, "swe_operator_contravariant: built for the Ch staggering");
+    if (c->ah) return fail(c, SWE_EINVAL, "swe_operator_contravariant: built for the Ch and C staggerings");
+    if (c->cstag) {
+        // co2contra_c_sbp42_new
+        if (c->elem == 8) launch_k(k_c_co2contra<double>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const double *)vin->d, (double *)vout->d, c->dims, c_view<double>(c));
+        else launch_k(k_c_co2contra<float>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const float *)vin->d, (float *)vout->d, c->dims, c_view<float>(c));
+        c->launches++;
+        CU_LAUNCHED(c);
+        return SWE_OK;
+    }
     const int M = c->cfg.n_members;
     if (c->elem == 8)
         if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
@@ -1534,6 +1625,29 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
     else
         if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
                                 c->m32.v, c->stream)) c->launch_miss = true;
+    c->launches++;
+    CU_LAUNCHED(c);
+    return SWE_OK;
+}
+
+
+extern "C" int swe_c_grad(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
+{
+    if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    if (!c->cstag) return fail(c, SWE_EINVAL, "swe_c_grad: the context has no C staggering");
+    if (c->elem == 8) launch_k(k_c_grad<double>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const double *)vin->d, (double *)vout->d, c->dims, c_view<double>(c));
+    else launch_k(k_c_grad<float>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const float *)vin->d, (float *)vout->d, c->dims, c_view<float>(c));
+    c->launches++;
+    CU_LAUNCHED(c);
+    return SWE_OK;
+}
+
+extern "C" int swe_c_div(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
+{
+    if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    if (!c->cstag) return fail(c, SWE_EINVAL, "swe_c_div: the context has no C staggering");
+    if (c->elem == 8) launch_k(k_c_div<double>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const double *)vin->d, (double *)vout->d, c->dims, c_view<double>(c));
+    else launch_k(k_c_div<float>, c_grid_dims(c), dim3(32, 8), 0, c->stream, (const float *)vin->d, (float *)vout->d, c->dims, c_view<float>(c));
     c->launches++;
     CU_LAUNCHED(c);
     return SWE_OK;
@@ -1572,6 +1686,7 @@ static int ensure_cmp(swe_stvec *v)
 extern "C" int swe_rk4_step(swe_ctx *c, swe_stvec *v0, double dt)
 {
     if (!c || !v0 || v0->ctx != c) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_rk4_step");
     int rc = ensure_cmp(v0);
     if (rc) return rc;
     enqueue_rk4(c, v0, dt);
@@ -1638,12 +1753,14 @@ static int run_steps(swe_ctx *c, swe_stvec *v0, double dt, bool members, int nst
 extern "C" int swe_rk4_steps(swe_ctx *c, swe_stvec *v0, double dt, int nsteps)
 {
     if (!c || !v0 || v0->ctx != c || nsteps < 0) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_rk4_steps");
     return run_steps(c, v0, dt, false, nsteps);
 }
 
 extern "C" int swe_rk4_steps_members(swe_ctx *c, swe_stvec *v0, const double *dt, int nsteps)
 {
     if (!c || !v0 || v0->ctx != c || !dt || nsteps < 0) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_rk4_steps_members");
     const int M = c->cfg.n_members;
     for (int k = 0; k < M; k++)
         if (!(dt[k] >= 0.0) || !std::isfinite(dt[k]))
@@ -1693,6 +1810,7 @@ __global__ void k_quad(const T *__restrict__ y, const T *__restrict__ w, const d
 extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, double *mass, double *energy)
 {
     if (!c || !vec || vec->ctx != c || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_integrals");
     if (c->ah) {
         const int nb = 256;
         const size_t mo = (size_t)member * c->dims.ms;
@@ -1778,6 +1896,7 @@ __global__ void k_extrema(const T *__restrict__ y, const T *__restrict__ w, Dims
 extern "C" int swe_diag(swe_ctx *c, const swe_stvec *vec, int member, double dt, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_diag");
     if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_diag");
     const int nb = 256;
     dim3 g(nb, 4), b(256);
@@ -1981,6 +2100,7 @@ static void launch_energies(swe_ctx *c, const T *y, const Dims &d, double hx, in
 extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_curl");
     if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_curl");
     int rc = ensure_otab(c);
     if (rc != SWE_OK) return rc;
@@ -2000,6 +2120,7 @@ extern "C" int swe_curl(swe_ctx *c, const swe_stvec *vec, int member, double *ou
 extern "C" int swe_energies(swe_ctx *c, const swe_stvec *vec, int member, double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_energies");
     if (c->ah) return fail(c, SWE_EINVAL, "%s: built for the Ch staggering", "swe_energies");
     int rc = ensure_otab(c);
     if (rc != SWE_OK) return rc;
@@ -2387,6 +2508,7 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
                                  double *out)
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_regrid_latlon");
     if (field != 0 && field != 1)
         return fail(c, SWE_EINVAL, "lat-lon regrid: field 0 (h) or 1 (the divergence of the wind)");
     if (field == 1 && c->ah) return fail(c, SWE_EINVAL, "lat-lon regrid of the divergence: built for Ch");
@@ -2424,6 +2546,7 @@ extern "C" int swe_regrid_latlon_wind(swe_ctx *c, const swe_stvec *vec, int memb
 {
     if (!c || !vec || vec->ctx != c || !u_out || !v_out || member < 0 || member >= c->cfg.n_members)
         return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_regrid_latlon_wind");
     if (c->ah) return fail(c, SWE_EINVAL, "swe_regrid_latlon_wind: built for the Ch staggering");
     if (nlat < 2 || nlon < 1 || (int64_t)nlat * nlon > (1 << 28))
         return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
@@ -2510,6 +2633,7 @@ extern "C" int swe_kernel_times(swe_ctx *c, swe_stvec *v0, double dt, int nreps,
                                 double *ms_stage)
 {
     if (!c || !v0 || v0->ctx != c || nreps < 1) return SWE_EINVAL;
+    CHSWE_NOT_ON_C(c, "swe_kernel_times");
     if (c->adv || c->ah) return fail(c, SWE_EINVAL, "swe_kernel_times times the Ch linear operator's three kernels");
     int rc = ensure_cmp(v0);
     if (rc) return rc;
@@ -2860,7 +2984,7 @@ std::vector<TuneEntry> g_tuned;   // process-wide results of swe_autotune
 extern "C" int swe_autotune(swe_ctx *c, int nreps, int *best_tile, double *ms_per_step)
 {
     if (!c || nreps < 1) return SWE_EINVAL;
-    if (c->ah) {   // the Ah kernels have no tile configuration
+    if (c->ah || c->cstag) {   // the Ah and C kernels have no tile configuration
         if (best_tile) *best_tile = c->tile;
         if (ms_per_step) for (int k = 0; k < 3; k++) ms_per_step[k] = 0.0;
         return SWE_OK;

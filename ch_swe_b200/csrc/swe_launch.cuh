@@ -58,6 +58,25 @@ static inline bool pdl_enabled()
     return on;
 }
 
+// CHSWE_CARVEOUT=1 asks for the largest shared-memory carveout on every kernel of the
+// stage chain, so that an SM does not switch its L1 / shared-memory split between the
+// small-memory edge kernels and the stage kernels that overlap them.
+static inline bool carveout_max()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("CHSWE_CARVEOUT");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+template <class K>
+static inline cudaError_t set_carveout(K kern)
+{
+    return carveout_max() ? cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                 (int)cudaSharedmemCarveoutMaxShared)
+                          : cudaSuccess;
+}
+
 template <typename... KArgs, typename... Args>
 static inline void launch_k(void (*kern)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t st, Args... args)
 {

@@ -19,6 +19,11 @@ static cudaError_t stage_smem_optin_modes()
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    if (e == cudaSuccess) e = set_carveout(k_stage<T, TM, OCC, 0, ADV, RUNS, ORD>);
+    if (e == cudaSuccess) e = set_carveout(k_stage<T, TM, OCC, 1, ADV, RUNS, ORD>);
+    if (e == cudaSuccess) e = set_carveout(k_stage<T, TM, OCC, 2, ADV, RUNS, ORD>);
+    if (e == cudaSuccess) e = set_carveout(k_stage<T, TM, OCC, 3, ADV, RUNS, ORD>);
+    if (e == cudaSuccess) e = set_carveout(k_stage<T, TM, OCC, 4, ADV, RUNS, ORD>);
     return e;
 }
 
@@ -46,6 +51,7 @@ cudaError_t StageTU<T, TMX>::optin()
         if (e == cudaSuccess && !ADV)                                                                              \
             e = cudaFuncSetAttribute(k_co2contra<T, TM, OCC, RUNS, ORD>,                                           \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Co2Layout<T, TM>::bytes()); \
+        if (e == cudaSuccess && !ADV) e = set_carveout(k_co2contra<T, TM, OCC, RUNS, ORD>);                       \
         if (e == cudaSuccess) e = stage_smem_optin_modes<T, TM, OCC, ADV, RUNS, ORD>();                           \
     }
 #define CHSWE_OPTIN_42(TM, OCC, RUNS) CHSWE_OPTIN(TM, OCC, RUNS, false, 42)

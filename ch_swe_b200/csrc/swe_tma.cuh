@@ -58,14 +58,16 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Wait for phase `parity` of the barrier for at most limit_ns nanoseconds.
+// Wait for phase `parity` of the barrier for at most limit_ns nanoseconds (the clock is
+// read every 256 polls).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
 {
     if (mbar_test(bar, parity)) return true;
     const uint64_t t0 = global_ns();
-    while (!mbar_test(bar, parity))
-        if (global_ns() - t0 > limit_ns) return false;
-    return true;
+    for (uint32_t it = 1;; it++) {
+        if (mbar_test(bar, parity)) return true;
+        if ((it & 255u) == 0 && global_ns() - t0 > limit_ns) return false;
+    }
 }
 
 // One 2-D tile of a tensor map into shared memory at dst (128-byte aligned),

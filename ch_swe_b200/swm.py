@@ -67,7 +67,7 @@ LINEAR_AH_NAMES_BY_ORDER = {
     for order in (42, 21, 63)
 }
 LINEAR_AH42_NAMES = LINEAR_AH_NAMES_BY_ORDER[42]
-STAGGERINGS = {"Ch": _lib.SWE_STAG_CH, "Ah": _lib.SWE_STAG_AH}
+STAGGERINGS = {"Ch": _lib.SWE_STAG_CH, "Ah": _lib.SWE_STAG_AH, "C": _lib.SWE_STAG_C}
 # advective_swm_operator, covariant Ch (gen_config.sh Ch template with UPSTREAM_ORDER up4),
 # per SBP order of its Ch operators
 ADVECTIVE_NAMES_BY_ORDER = {
@@ -80,9 +80,13 @@ OPERATORS = {"linear": _lib.SWE_OP_LINEAR, "advective": _lib.SWE_OP_ADVECTIVE}
 
 def state_shapes(N: int, members: int | None = None, staggering: str = "Ch"):
     """Packed host shapes of (h, u, v) for one member (or a batch of members): on Ch,
-    h on the vertices, u on the y points, v on the x points; on Ah all on the vertices."""
+    h on the vertices, u on the y points, v on the x points; on Ah all on the vertices;
+    on C h on the cell centres, u on the x points, v on the y points."""
     if staggering == "Ah":
         sh = [(6, N + 1, N + 1)] * 3
+    elif staggering == "C":
+        # h on the cell centres, u on the x points, v on the y points
+        sh = [(6, N, N), (6, N, N + 1), (6, N + 1, N)]
     else:
         sh = [(6, N + 1, N + 1), (6, N + 1, N), (6, N, N + 1)]
     if members is None:
@@ -110,8 +114,10 @@ class Domain:
     def __post_init__(self):
         if self.horizontal_staggering not in STAGGERINGS:
             raise ValueError("domain_factory_mod, unsupported horizontal staggering: " + self.horizontal_staggering)
-        if self.horizontal_staggering == "Ah" and self.operator != "linear":
-            raise ValueError("the Ah staggering is built for the linear operator")
+        if self.horizontal_staggering in ("Ah", "C") and self.operator != "linear":
+            raise ValueError(f"the {self.horizontal_staggering} staggering is built for the linear operator")
+        if self.horizontal_staggering == "C" and self.sbp_order != 42:
+            raise ValueError("the C staggering is built for SBP 4-2")
         if self.precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if self.operator not in OPERATORS:
@@ -415,6 +421,73 @@ class OperatorSwmAdv(OperatorSwmLin):
         if hs.shape != state_shapes(self.domain.N)[0]:
             raise ValueError(f"orography shape {hs.shape}, need {state_shapes(self.domain.N)[0]}")
         check(_lib.load().swe_set_orography(self.domain.ctx, dptr(hs)), self.domain.ctx, "orography")
+
+
+# ---------------------------------------------------------------------------
+# C staggering: the C-grid operators the reference runs (its linear operator on C aborts in
+# coriolis_Cgrid_t%calc_coriolis, coriolis_Cgrid_mod.f90:28-37)
+# ---------------------------------------------------------------------------
+C_OPERATOR_NAMES = {"grad": "grad_c_sbp_sat_42", "div": "div_c_sbp_sat_42", "co2contra": "co2contra_c_sbp42_new"}
+
+
+def _need_c(domain: Domain, name: str):
+    if domain.horizontal_staggering != "C":
+        raise ValueError(f"{name} needs a domain created with horizontal_staggering='C'")
+
+
+class GradC:
+    """grad_c_sbp_sat_42 (grad_factory_mod.f90:115-150, grad_sbp_sat_mod.f90:24-76)."""
+
+    def __init__(self, domain: Domain):
+        _need_c(domain, C_OPERATOR_NAMES["grad"])
+        self.domain = domain
+
+    def calc_grad(self, out: StvecSwm, src: StvecSwm):
+        """out.u, out.v (x, y points) = gradient of src.h (cell centres)."""
+        check(_lib.load().swe_c_grad(self.domain.ctx, out.handle, src.handle), self.domain.ctx, "grad_c")
+
+
+class DivC:
+    """div_c_sbp_sat_42 (div_factory_mod.f90:112-156, div_sbp_sat_mod.f90:29-80)."""
+
+    def __init__(self, domain: Domain):
+        _need_c(domain, C_OPERATOR_NAMES["div"])
+        self.domain = domain
+
+    def calc_div(self, out: StvecSwm, src: StvecSwm):
+        """out.h (cell centres) = divergence of the contravariant (src.u, src.v)."""
+        check(_lib.load().swe_c_div(self.domain.ctx, out.handle, src.handle), self.domain.ctx, "div_c")
+
+
+class Co2ContraC:
+    """co2contra_c_sbp42_new (co2contra_Cgrid_mod.f90, transform_co2contra_c_sbp_new)."""
+
+    def __init__(self, domain: Domain):
+        _need_c(domain, C_OPERATOR_NAMES["co2contra"])
+        self.domain = domain
+
+    def transform(self, out: StvecSwm, src: StvecSwm):
+        """out.u, out.v = contravariant components of the covariant (src.u, src.v)."""
+        check(_lib.load().swe_operator_contravariant(self.domain.ctx, out.handle, src.handle), self.domain.ctx,
+              "co2contra_c")
+
+
+def create_grad_operator(domain: Domain, name: str):
+    if name != C_OPERATOR_NAMES["grad"]:
+        raise ValueError(f"unknown C-grid gradient {name!r} (this build implements {C_OPERATOR_NAMES['grad']})")
+    return GradC(domain)
+
+
+def create_div_operator(domain: Domain, name: str):
+    if name != C_OPERATOR_NAMES["div"]:
+        raise ValueError(f"unknown C-grid divergence {name!r} (this build implements {C_OPERATOR_NAMES['div']})")
+    return DivC(domain)
+
+
+def create_co2contra_operator(domain: Domain, name: str):
+    if name != C_OPERATOR_NAMES["co2contra"]:
+        raise ValueError(f"unknown C-grid co2contra {name!r} (this build implements {C_OPERATOR_NAMES['co2contra']})")
+    return Co2ContraC(domain)
 
 
 class Rk4:

@@ -61,6 +61,10 @@ extern "C" {
 
 #define SWE_STAG_CH 0      /* horizontal_staggering 'Ch': h on vertices, u on y, v on x points */
 #define SWE_STAG_AH 1      /* horizontal_staggering 'Ah': h, u, v on the vertices (linear operator) */
+#define SWE_STAG_C 2       /* horizontal_staggering 'C': h on the cell centres, u on the x points, v on
+                              the y points (domain_factory_mod.f90:281-295); the C-grid gradient,
+                              divergence and co2contra only (swe_c_grad, swe_c_div,
+                              swe_operator_contravariant): see swe_c_grad */
 
 typedef struct swe_ctx swe_ctx;
 typedef struct swe_stvec swe_stvec;
@@ -86,7 +90,9 @@ typedef struct swe_cfg {
                                  grad_ah_sbp_proj_<order>, coriolis_colocated, co2contra_colocated
                                  and SBP_Ah<order>_quadrature (gen_config_linear.sh:9-36), the
                                  order from sbp_order (42, 21 or 63).  Packed u and v are then
-                                 (N+1) x (N+1) per panel like h. */
+                                 (N+1) x (N+1) per panel like h.
+                                 SWE_STAG_C: packed h is N x N per panel, u (N+1) x N (x points,
+                                 N+1 values per row, N rows), v N x (N+1) (y points). */
 } swe_cfg;
 
 /* Fill *cfg with the defaults listed above. */
@@ -128,6 +134,24 @@ int swe_operator_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
 /* vout.u, vout.v = contravariant components (ut, vt) of vin's covariant wind; vout.h unchanged.
    Mirrors co2contra_operator_t%transform (co2contra_Ch_mod.f90:27-94). */
 int swe_operator_contravariant(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
+
+/* C staggering (contexts created with SWE_STAG_C, SBP 4-2, FP32 or FP64):
+   swe_c_grad: vout.u, vout.v = grad_c_sbp_sat_42 of vin.h (grad_operator_t%calc_grad,
+     grad_factory_mod.f90:115-150 with sbp_diff_c2i_42; grad_sbp_sat_mod.f90:24-76): the
+     centres->nodes difference with its SAT across the panel edges, divided by h a.
+   swe_c_div: vout.h = div_c_sbp_sat_42 of the contravariant (vin.u, vin.v)
+     (div_operator_t%calc_div, div_factory_mod.f90:112-156 with sbp_diff_i2c_42;
+     div_sbp_sat_mod.f90:29-80, no projection).
+   swe_operator_contravariant on a C context: co2contra_c_sbp42_new
+     (co2contra_Cgrid_mod.f90, transform_co2contra_c_sbp_new).
+   The reference's linear operator cannot run on the C staggering: it calls
+   coriolis_op%calc_coriolis, and both C-grid Coriolis operators abort there
+   (coriolis_Cgrid_mod.f90:28-37, coriolis_Cgrid_noncons_mod.f90:96-106).  So
+   swe_operator_apply, the RK4 steps and the linear energy return SWE_EINVAL on a C
+   context; these three operators are what the reference runs on C (its Helmholtz,
+   Laplace and diffusion operators use them). */
+int swe_c_grad(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
+int swe_c_div(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin);
 /* One classic RK4 step of size dt on v0 (in place). */
 int swe_rk4_step(swe_ctx *ctx, swe_stvec *v0, double dt);
 /* nsteps RK4 steps (captured into a CUDA graph after the first call with the same shape). */

@@ -63,6 +63,12 @@ def lib():
         L.orc_sbp1d.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_set_operator.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_orography.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_c_grad.argtypes = [ctypes.c_void_p] * 4
+        L.orc_c_div.argtypes = [ctypes.c_void_p] * 4
+        L.orc_c_co2contra.argtypes = [ctypes.c_void_p] * 5
+        L.orc_c_weights.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.orc_c_halo_probe.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_sbp_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_diag.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, _dp]
         L.orc_sbp1d_ord.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
@@ -185,6 +191,53 @@ class Oracle:
         h, u, v = self.zeros()
         lib().orc_init_gaussian(self._c, lam0, phi0, d0, amp, _p(h), _p(u), _p(v))
         return h, u, v
+
+    # ---- C staggering (h on the cell centres, u on the x mesh, v on the y mesh)
+    def c_shapes(self):
+        N = self.N
+        return (6, N, N), (6, N, N + 1), (6, N + 1, N)
+
+    def c_grad(self, h):
+        """grad_c_sbp_sat_<order>: (gx on x, gy on y) of h on the cell centres."""
+        _, sx, sy = self.c_shapes()
+        gx, gy = np.zeros(sx), np.zeros(sy)
+        lib().orc_c_grad(self._c, _p(np.ascontiguousarray(h, dtype=np.float64)), _p(gx), _p(gy))
+        return gx, gy
+
+    def c_div(self, ut, vt):
+        """div_c_sbp_sat_<order> of (ut on x, vt on y), on the cell centres."""
+        so, _, _ = self.c_shapes()
+        d = np.zeros(so)
+        lib().orc_c_div(self._c, _p(np.ascontiguousarray(ut, dtype=np.float64)),
+                        _p(np.ascontiguousarray(vt, dtype=np.float64)), _p(d))
+        return d
+
+    def c_co2contra(self, u, v):
+        """co2contra_c_sbp<order>_new: contravariant (ut on x, vt on y) of covariant (u, v)."""
+        _, sx, sy = self.c_shapes()
+        ut, vt = np.zeros(sx), np.zeros(sy)
+        lib().orc_c_co2contra(self._c, _p(np.ascontiguousarray(u, dtype=np.float64)),
+                              _p(np.ascontiguousarray(v, dtype=np.float64)), _p(ut), _p(vt))
+        return ut, vt
+
+    def c_weights(self, mesh: int):
+        """SBP quadrature weights J hx hy Ax Ay on the C meshes: 0 = o, 1 = x, 2 = y."""
+        w = np.zeros(self.c_shapes()[mesh])
+        lib().orc_c_weights(self._c, int(mesh), _p(w))
+        return w
+
+    def c_halo_probe(self, kind: int, f, f2=None, w: int = 3):
+        """The C exchanges' halos: kind 0 o-point scalar (width 3), 1 C vector (width 3)."""
+        N = self.N
+        if kind == 0:
+            out = np.zeros((6, N + 2 * w, N + 2 * w))
+            lib().orc_c_halo_probe(self._c, 0, _p(np.ascontiguousarray(f, dtype=np.float64)), None, w, _p(out), None)
+            return out
+        o1 = np.zeros((6, N + 2 * w, N + 1 + 2 * w))
+        o2 = np.zeros((6, N + 1 + 2 * w, N + 2 * w))
+        lib().orc_c_halo_probe(self._c, 1, _p(np.ascontiguousarray(f, dtype=np.float64)),
+                               _p(np.ascontiguousarray(f2, dtype=np.float64)), w, _p(o1), _p(o2))
+        return o1, o2
 
     def set_orography(self, h_surf):
         """Orography of the advective operator (packed like h), or None."""

@@ -347,6 +347,39 @@ static void build_ch_exchange(exch_t *e, int N, int hw, int cross, int fill_x)
     e->dst_is_u = fill_x ? 0 : 1;
 }
 
+/* create_o_points_halo_exchange -> create_o_z_points_halo_exchange (exchange_factory_mod.f90:13-27,45-150):
+   the scalar exchange of the xy points on the cell-centre (o) tiles, N x N per panel. */
+static void build_o_exchange(exch_t *e, int N, int hw, int cross)
+{
+    static half_t send[NPAN][NPAN], recv[NPAN][NPAN];
+    memset(send, 0, sizeof(send)); memset(recv, 0, sizeof(recv));
+    box_t tile = {1, N, 1, N};
+    for (int loc = 0; loc < NPAN; loc++)
+        for (int rem = 0; rem < NPAN; rem++) {
+            if (rem == loc) continue;
+            box_t temp = transform_box(rem, tile, loc, N, N);
+            box_t b;
+            if (halo_intersection(tile, hw, hw, temp, cross, &b)) { recv[loc][rem].valid = 1; recv[loc][rem].b = b; }
+            half_t *h = &send[loc][rem];
+            basis_orientation(rem, loc, &h->is, &h->js, &h->fdim);
+            if (halo_intersection(temp, hw, hw, tile, cross, &b)) { h->valid = 1; h->b = b; }
+        }
+    exch_pair(e, send, recv);
+    e->pack = PK_SCALAR;
+}
+
+/* create_symmetric_halo_vec_exchange_C (exchange_factory_mod.f90:335-350) with the C
+   exchange's packing (exchange_halo_C_mod.f90: do_u packs pack_to_buf_u_vec into exch_u,
+   do_v packs pack_to_buf_v_vec into exch_v): the tiles are those of the Ch exchange,
+   but on C the x-mesh field is u (the alpha component) and the y-mesh field v.
+   exch_do(e, u on x, v on y); fill_x 1: exch_u (fills u), 0: exch_v (fills v). */
+static void build_c_exchange(exch_t *e, int N, int hw, int fill_x)
+{
+    build_ch_exchange(e, N, hw, 0, fill_x);
+    e->pack = fill_x ? PK_U_VEC : PK_V_VEC;
+    e->dst_is_u = fill_x;
+}
+
 /* pack traversal: returns the source points in the order of
    pack_to_buf* (buffer_mod.f90:44-476) */
 static int pack_order(const msg_t *m, int *ii, int *jj)
@@ -375,7 +408,8 @@ static int pack_order(const msg_t *m, int *ii, int *jj)
 
 /* exchange_2D_halo_t%do / do_vec and exchange_2D_halo_Ch_t%do_u / do_v.
    For PK_SCALAR only f1 is used.  For PK_VEC (f1, f2) = (u, v) on the same mesh.
-   For Ch exchanges f1 is the y-mesh field (Ch "u") and f2 the x-mesh field. */
+   For Ch exchanges f1 is the y-mesh field (Ch "u") and f2 the x-mesh field; for the C
+   exchanges (build_c_exchange) f1 is the x-mesh field (C "u") and f2 the y-mesh field. */
 static void exch_do(const exch_t *e, fld_t *f1, fld_t *f2)
 {
     for (int k = 0; k < e->n; k++) {
@@ -845,6 +879,11 @@ typedef struct orc_ctx {
     exch_t ex_xy5_full_s, ex_ch1c_u, ex_ch1c_v;
     fld_t htot, hu, hv, cu, cv, uh, vh, vau, uav, uhal, vhal;
     double *hsurf;               /* orography h_surf on xy, [t][j][i]; NULL: none */
+    /* C staggering (h on o, u on x, v on y): operators of the C-grid configurations, built
+       on first use */
+    int cgrid;
+    exch_t ex_o3, ex_c3_u, ex_c3_v;
+    fld_t c_h, c_u, c_v, c_gx, c_gy, c_ut, c_vt, c_uh, c_vh, c_Ju, c_Jv, c_Dx, c_Dy, c_div;
     /* energies and enstrophy of swm_output_diag_t: mesh o (cell centres, the Ch q mesh) */
     mesh_t mo;
     double *fo;                  /* Coriolis parameter on o, [t][j][i] */
@@ -962,12 +1001,15 @@ orc_ctx *orc_create(int N, double radius, double grav, double omega, double h_me
     return c;
 }
 
+static void c_free(orc_ctx *c);
+
 void orc_destroy(orc_ctx *c)
 {
     if (!c) return;
     mesh_free(&c->mxy); mesh_free(&c->mx); mesh_free(&c->my); mesh_free(&c->mo);
     free(c->fJ2); free(c->fo); free(c->fxy); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
     free(c->hsurf);
+    c_free(c);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
                     &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
@@ -1561,6 +1603,110 @@ static void op_apply_nl(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, f
     }
 }
 
+/* ================================================================== */
+/* C staggering: h on the cell centres (o), u on the x mesh, v on the y mesh          */
+/* (domain_factory_mod.f90:281-295)                                                   */
+/* ================================================================== */
+static void c_init(orc_ctx *c)
+{
+    if (c->cgrid) return;
+    const int N = c->N, hw = 5;
+    build_o_exchange(&c->ex_o3, N, 3, 0);
+    build_c_exchange(&c->ex_c3_u, N, 3, 1);
+    build_c_exchange(&c->ex_c3_v, N, 3, 0);
+    fld_t *oo[] = {&c->c_h, &c->c_uh, &c->c_vh, &c->c_Dx, &c->c_Dy, &c->c_div};
+    fld_t *xx[] = {&c->c_u, &c->c_gx, &c->c_ut, &c->c_Ju};
+    fld_t *yy[] = {&c->c_v, &c->c_gy, &c->c_vt, &c->c_Jv};
+    for (unsigned q = 0; q < sizeof(oo) / sizeof(oo[0]); q++) fld_init(oo[q], N, N, hw);
+    for (unsigned q = 0; q < sizeof(xx) / sizeof(xx[0]); q++) fld_init(xx[q], N + 1, N, hw);
+    for (unsigned q = 0; q < sizeof(yy) / sizeof(yy[0]); q++) fld_init(yy[q], N, N + 1, hw);
+    c->cgrid = 1;
+}
+
+static void c_free(orc_ctx *c)
+{
+    if (!c->cgrid) return;
+    fld_t *all[] = {&c->c_h, &c->c_u, &c->c_v, &c->c_gx, &c->c_gy, &c->c_ut, &c->c_vt, &c->c_uh, &c->c_vh,
+                    &c->c_Ju, &c->c_Jv, &c->c_Dx, &c->c_Dy, &c->c_div};
+    for (unsigned q = 0; q < sizeof(all) / sizeof(all[0]); q++) fld_free(all[q]);
+    c->cgrid = 0;
+}
+
+/* grad_c_sbp_sat_<order>: grad_sbp_sat_t with the centres->nodes difference and its SAT on
+   the o-point halo of width 3 (grad_factory_mod.f90:115-150, grad_sbp_sat_mod.f90:24-76):
+   gx on the x mesh, gy on the y mesh, each divided by h a. */
+static void op_grad_c(orc_ctx *c, fld_t *gx, fld_t *gy, fld_t *h)
+{
+    const int N = c->N;
+    exch_do(&c->ex_o3, h, NULL);
+    for (int t = 0; t < NPAN; t++) {
+        diff_c2i(gx, h, t, 0, N + 1, 1, N, c->ord);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) FA(gx, t, i, j) = FA(gx, t, i, j) / (c->mx.hx * c->a);
+        diff_c2i(gy, h, t, 1, N + 1, 1, N, c->ord);
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) FA(gy, t, i, j) = FA(gy, t, i, j) / (c->my.hy * c->a);
+    }
+}
+
+/* div_c_sbp_sat_<order>: div_sbp_SAT_t with the nodes->centres difference, its SAT on the
+   C vector halo and no projection (div_factory_mod.f90:112-156, div_sbp_sat_mod.f90:29-80). */
+static void op_div_c(orc_ctx *c, fld_t *div, fld_t *ut, fld_t *vt)
+{
+    const int N = c->N;
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) FA(&c->c_Ju, t, i, j) = FA(ut, t, i, j) * c->mx.J[MI(&c->mx, t, i, j)];
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) FA(&c->c_Jv, t, i, j) = FA(vt, t, i, j) * c->my.J[MI(&c->my, t, i, j)];
+    }
+    exch_do(&c->ex_c3_u, &c->c_Ju, &c->c_Jv);
+    exch_do(&c->ex_c3_v, &c->c_Ju, &c->c_Jv);
+    for (int t = 0; t < NPAN; t++) {
+        diff_i2c(&c->c_Dx, &c->c_Ju, t, 0, N, 1, N, c->ord);
+        diff_i2c(&c->c_Dy, &c->c_Jv, t, 1, N, 1, N, c->ord);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++)
+                FA(div, t, i, j) = (FA(&c->c_Dx, t, i, j) / c->mo.hx + FA(&c->c_Dy, t, i, j) / c->mo.hy) /
+                                   (c->mo.J[MI(&c->mo, t, i, j)] * c->a);
+    }
+}
+
+/* co2contra_c_sbp<order>_new (co2contra_Cgrid_mod.f90, transform_co2contra_c_sbp_new): u, v to
+   the cell centres (interp2d_uv2pvec_C: nodes->centres interpolation along x / y,
+   interpolator_uv2p_mod.f90:22-49), there times J Qi12 and swapped, back to the faces
+   (interp2d_pvec2uv_C: centres->nodes interpolation, interpolator_p2uv_mod.f90:54-99),
+   then ut = Qi11 u + (.)/J, vt = Qi22 v + (.)/J.  The exchanges before the two
+   interpolations fill halos the SBP closure rows never read. */
+static void op_co2contra_c(orc_ctx *c, fld_t *ut, fld_t *vt, fld_t *u, fld_t *v)
+{
+    const int N = c->N;
+    for (int t = 0; t < NPAN; t++) {
+        interp_i2c(&c->c_uh, u, t, 0, N, 1, N, c->ord);
+        interp_i2c(&c->c_vh, v, t, 1, N, 1, N, c->ord);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N; i++) {
+                const size_t k = MI(&c->mo, t, i, j);
+                const double uu = FA(&c->c_uh, t, i, j) * c->mo.J[k] * c->mo.Q2[k];
+                const double vv = FA(&c->c_vh, t, i, j) * c->mo.J[k] * c->mo.Q2[k];
+                FA(&c->c_uh, t, i, j) = vv;
+                FA(&c->c_vh, t, i, j) = uu;
+            }
+        interp_c2i(ut, &c->c_uh, t, 0, N + 1, 1, N, c->ord);
+        interp_c2i(vt, &c->c_vh, t, 1, N + 1, 1, N, c->ord);
+        for (int j = 1; j <= N; j++)
+            for (int i = 1; i <= N + 1; i++) {
+                const size_t k = MI(&c->mx, t, i, j);
+                FA(ut, t, i, j) = c->mx.Q1[k] * FA(u, t, i, j) + FA(ut, t, i, j) / c->mx.J[k];
+            }
+        for (int j = 1; j <= N + 1; j++)
+            for (int i = 1; i <= N; i++) {
+                const size_t k = MI(&c->my, t, i, j);
+                FA(vt, t, i, j) = c->my.Q3[k] * FA(v, t, i, j) + FA(vt, t, i, j) / c->my.J[k];
+            }
+    }
+}
+
 static void op_apply(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v)
 {
     if (c->nonlinear) op_apply_nl(c, dh, du, dv, h, u, v);
@@ -1857,6 +2003,50 @@ int orc_N(const orc_ctx *c) { return c->N; }
 
 /* operator kind: 0 linear_swm_operator, 1 advective_swm_operator (covariant Ch) */
 void orc_set_operator(orc_ctx *c, int kind) { c->nonlinear = kind == 1; }
+
+/* C-grid operators on packed fields: h (6, N, N) on the cell centres, u (6, N, N+1) on the
+   x mesh, v (6, N+1, N) on the y mesh, each [t][j][i] with i fastest. */
+void orc_c_grad(orc_ctx *c, const double *h, double *gx, double *gy)
+{
+    c_init(c);
+    fld_from_packed(&c->c_h, h);
+    op_grad_c(c, &c->c_gx, &c->c_gy, &c->c_h);
+    fld_to_packed(&c->c_gx, gx);
+    fld_to_packed(&c->c_gy, gy);
+}
+void orc_c_div(orc_ctx *c, const double *ut, const double *vt, double *div)
+{
+    c_init(c);
+    fld_from_packed(&c->c_ut, ut);
+    fld_from_packed(&c->c_vt, vt);
+    op_div_c(c, &c->c_div, &c->c_ut, &c->c_vt);
+    fld_to_packed(&c->c_div, div);
+}
+void orc_c_co2contra(orc_ctx *c, const double *u, const double *v, double *ut, double *vt)
+{
+    c_init(c);
+    fld_from_packed(&c->c_u, u);
+    fld_from_packed(&c->c_v, v);
+    op_co2contra_c(c, &c->c_ut, &c->c_vt, &c->c_u, &c->c_v);
+    fld_to_packed(&c->c_ut, ut);
+    fld_to_packed(&c->c_vt, vt);
+}
+/* SBP_C42 quadrature weights on the C meshes: mesh 0 = o, 1 = x, 2 = y (packed like the fields). */
+void orc_c_weights(orc_ctx *c, int mesh, double *w)
+{
+    const mesh_t *m = mesh == 0 ? &c->mo : (mesh == 1 ? &c->mx : &c->my);
+    size_t k = 0;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= m->ny; j++)
+            for (int i = 1; i <= m->nx; i++) {
+                const size_t q = MI(m, t, i, j);
+                w[k++] = m->J[q] * m->hx * m->hy * m->Ax[i - 1] * m->Ay[j - 1];
+            }
+}
+/* The C halos as the exchanges deliver them: kind 0 the o-point scalar exchange of width 3
+   (f on o), kind 1 the C vector exchange of width 3 (f = u on x, f2 = v on y); the ring of
+   width w around every panel is written like orc_halo_probe's. */
+void orc_c_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int w, double *out, double *out2);
 
 /* Orography h_surf of the advective operator (operator_adv_swm_mod.f90:37-38,78:
    h_total = h + h_surf is the gradient's input), packed [t][j][i] on xy; NULL clears it. */
@@ -2332,6 +2522,23 @@ void orc_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int
         fld_from_packed(&a, f); fld_from_packed(&b, f2);
         exch_do(kind == 4 ? &c->ex_ch1c_u : &c->ex_ch3_u, &a, &b);
         exch_do(kind == 4 ? &c->ex_ch1c_v : &c->ex_ch3_v, &a, &b);
+        ring_out(&a, w, out); ring_out(&b, w, out2); fld_free(&a); fld_free(&b);
+    }
+}
+
+void orc_c_halo_probe(orc_ctx *c, int kind, const double *f, const double *f2, int w, double *out, double *out2)
+{
+    c_init(c);
+    if (kind == 0) {
+        fld_t a; fld_init(&a, c->N, c->N, 5);
+        fld_from_packed(&a, f);
+        exch_do(&c->ex_o3, &a, NULL);
+        ring_out(&a, w, out); fld_free(&a);
+    } else {
+        fld_t a, b; fld_init(&a, c->N + 1, c->N, 5); fld_init(&b, c->N, c->N + 1, 5);
+        fld_from_packed(&a, f); fld_from_packed(&b, f2);
+        exch_do(&c->ex_c3_u, &a, &b);
+        exch_do(&c->ex_c3_v, &a, &b);
         ring_out(&a, w, out); ring_out(&b, w, out2); fld_free(&a); fld_free(&b);
     }
 }

@@ -83,14 +83,19 @@ def test_no_device_fails_loudly(lib_built):
 
 
 def test_ah_domain_validation():
-    """The Ah staggering is built for the linear operator (checked before any device
-    call)."""
+    """The Ah and C staggerings are built for the linear operator, C for SBP 4-2
+    (checked before any device call)."""
     import pytest
     from ch_swe_b200 import create_domain
     from ch_swe_b200.swm import state_shapes
     with pytest.raises(ValueError):
         create_domain(16, horizontal_staggering="Ah", operator="advective")
     with pytest.raises(ValueError):
-        create_domain(16, horizontal_staggering="C")
+        create_domain(16, horizontal_staggering="C", operator="advective")
+    with pytest.raises(ValueError):
+        create_domain(16, horizontal_staggering="C", sbp_order=21)
+    with pytest.raises(ValueError):
+        create_domain(16, horizontal_staggering="D")
+    assert state_shapes(16, None, "C") == ((6, 16, 16), (6, 16, 17), (6, 17, 16))
     assert state_shapes(16, None, "Ah") == ((6, 17, 17),) * 3
     assert state_shapes(16, 2, "Ah")[1] == (2, 6, 17, 17)

@@ -102,3 +102,42 @@ def test_ch_tendency_exchange_cross_width1(links):
                 else:
                     got = V[t, c + w - 1, (0 if s == 0 else N + 2) + w - 1]
                 assert got == st * nbv
+
+
+def test_c_grid_o_point_halo_width3(links):
+    """The o-point exchange (create_o_points_halo_exchange): beyond side s at depth d, the
+    neighbour's cell at depth d from its side, along index reversed by the link."""
+    L, o = links
+    rng = np.random.default_rng(5)
+    h = rng.standard_normal((6, N, N))
+    w = 3
+    H = o.c_halo_probe(0, h, w=w)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, _, _ = L[t, s]
+            for a in range(1, N + 1):
+                ap = N + 1 - a if rev else a
+                for d in range(3):
+                    i, j = [(0 - d, a), (N + 1 + d, a), (a, 0 - d), (a, N + 1 + d)][s]
+                    k, l = [(d + 1, ap), (N - d, ap), (ap, d + 1), (ap, N - d)][ns]
+                    assert H[t, j + w - 1, i + w - 1] == h[nb, l - 1, k - 1]
+
+
+def test_c_grid_vector_halo_first_node(links):
+    """The C vector exchange (create_symmetric_halo_vec_exchange_C): the first node beyond
+    side s holds the neighbour's normal component at its own edge node, times the
+    normal-component sign -- the value the C divergence SAT reads."""
+    L, o = links
+    rng = np.random.default_rng(6)
+    u, v = rng.standard_normal((6, N, N + 1)), rng.standard_normal((6, N + 1, N))
+    w = 4
+    U, V = o.c_halo_probe(1, u, v, w=w)
+    for t in range(6):
+        for s in range(4):
+            nb, ns, rev, sn, _ = L[t, s]
+            for a in range(1, N + 1):
+                ap = N + 1 - a if rev else a
+                got = [U[t, a + w - 1, w - 1], U[t, a + w - 1, N + 2 + w - 1],
+                       V[t, w - 1, a + w - 1], V[t, N + 2 + w - 1, a + w - 1]][s]
+                nbv = [u[nb, ap - 1, 0], u[nb, ap - 1, N], v[nb, 0, ap - 1], v[nb, N, ap - 1]][ns]
+                assert got == sn * nbv
