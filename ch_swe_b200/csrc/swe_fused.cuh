@@ -124,6 +124,93 @@ __device__ __forceinline__ T f_di2c(int k, int n, const Line<T> &f)
     return di2c_cl<T>(k, n, f);
 }
 
+// Branch-free x stencils: a lane owns one column k for a whole pass, so it looks up its
+// SBP 4-2 row once -- interior or closure -- as five weights on the inputs base .. base+4,
+// and every row of the pass is the same five-tap multiply-add on every lane (no divergent
+// closure branches in the tiles on a panel's left and right edges).  The weights are
+// those of swe_sbp.cuh (the interior rows and the closure rows with their mirrors).
+template <class T>
+struct XRow {
+    int base;   // first input index
+    T w[5];
+    // p points at input `base` of the row
+    __device__ __forceinline__ T dot(const T *p) const
+    {
+        T a = w[0] * p[0];
+#pragma unroll
+        for (int m = 1; m < 5; m++) a += w[m] * p[m];
+        return a;
+    }
+    // the same on the product of two rows
+    __device__ __forceinline__ T dot2(const T *p, const T *q) const
+    {
+        T a = w[0] * (p[0] * q[0]);
+#pragma unroll
+        for (int m = 1; m < 5; m++) a += w[m] * (p[m] * q[m]);
+        return a;
+    }
+};
+
+// op 0: I_c2i (nodes k = 1..nx from centres 1..nx-1), 1: D_c2i, 2: I_i2c (centres
+// k = 1..n from nodes 1..n+1), 3: D_i2c.
+template <class T>
+__device__ __noinline__ XRow<T> xrow42(int op, int k, int nm)
+{
+    using namespace sbp;
+    XRow<T> r;
+    double w[5] = {0, 0, 0, 0, 0};
+    if (op <= 1) {
+        const int nx = nm;
+        const bool D = op == 1;
+        if (k >= 5 && k <= nx - 4) {
+            r.base = k - 2;
+            if (D) { w[0] = 1.0 / 24.0; w[1] = -27.0 / 24.0; w[2] = 27.0 / 24.0; w[3] = -1.0 / 24.0; }
+            else { w[0] = -0.0625; w[1] = 0.5625; w[2] = 0.5625; w[3] = -0.0625; }
+        } else {
+            const double q[4][5] = {
+                {D ? DC11 : IC11, D ? DC12 : IC12, D ? DC13 : IC13, 0, 0},
+                {D ? DC21 : IC21, D ? DC22 : IC22, D ? 0.0 : IC23, 0, 0},
+                {D ? DC31 : IC31, D ? DC32 : IC32, D ? DC33 : IC33, D ? DC34 : IC34, 0},
+                {D ? DC41 : IC41, D ? DC42 : IC42, D ? DC43 : IC43, D ? DC44 : IC44, D ? DC45 : IC45}};
+            if (k <= 4) {
+                r.base = 1;
+                for (int m = 0; m < 5; m++) w[m] = q[k - 1][m];
+            } else {
+                // mirrored rows: input nx - 1 - m carries q[row][m] (negated for the difference)
+                const int row = nx - k;
+                r.base = nx - 5;
+                for (int m = 0; m < 5; m++) w[4 - m] = D ? -q[row][m] : q[row][m];
+            }
+        }
+    } else {
+        const int n = nm;
+        const bool D = op == 3;
+        if (k >= 4 && k <= n - 3) {
+            r.base = k - 1;
+            if (D) { w[0] = 1.0 / 24.0; w[1] = -27.0 / 24.0; w[2] = 27.0 / 24.0; w[3] = -1.0 / 24.0; }
+            else { w[0] = -0.0625; w[1] = 0.5625; w[2] = 0.5625; w[3] = -0.0625; }
+        } else {
+            const double q[3][5] = {{D ? DI11 : II11, D ? DI12 : II12, D ? DI13 : II13, D ? DI14 : II14, 0},
+                                    {D ? DI21 : II21, D ? DI22 : II22, D ? DI23 : II23, D ? DI24 : II24, 0},
+                                    {D ? DI31 : II31, D ? 0.0 : II32, D ? DI33 : II33, D ? DI34 : II34, D ? 0.0 : II35}};
+            // the 4-2 i2c difference's third row skips its second input and reaches the fifth
+            if (k <= 3) {
+                r.base = 1;
+                for (int m = 0; m < 5; m++) w[m] = q[k - 1][m];
+                if (D && k == 3) w[4] = DI35;
+            } else {
+                // mirrored rows: input n + 1 - m carries q[row][m] (negated for the difference)
+                const int row = n - k;
+                r.base = n - 3;
+                for (int m = 0; m < 5; m++) w[4 - m] = D ? -q[row][m] : q[row][m];
+                if (D && row == 2) w[0] = -DI35;
+            }
+        }
+    }
+    for (int m = 0; m < 5; m++) r.w[m] = T(w[m]);
+    return r;
+}
+
 // h at the neighbour's copy of the shared vertex, read through L2 (the previous
 // stage wrote it).
 template <class T>
@@ -217,6 +304,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
                 ht[q] = sat_t ? h_halo_cg(ym, d, t, SIDE_T, i0 + q) : T(0);
             }
     }
+    // The five-tap x rows read one input past the interior stencils with weight zero:
+    // the slots computed over part of their area start at zero, so that such a tap
+    // reads a finite value (the other slots hold loaded or earlier computed data)
+    for (int q = threadIdx.x; q < L::SLOT; q += FUSED_THREADS) sVQ[q] = sUQ[q] = sJVT[q] = T(0);
     __syncthreads();
     if (!__syncthreads_and(mbar_wait(bar, 0, FUSED_WAIT_NS))) {
         // the tile loads did not arrive: record it and leave (after one more bounded
@@ -268,17 +359,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
         rows_of(max(j0 - 3, 1), min(j1 + 3, n + 1), r0, r1);
         const int k = ka + lane;
         if (k < kb) {
-            const T *row = sU + SI(k, r0), *jq = sJQ12 + SI(k, r0);
+            const XRow<T> xr = xrow42<T>(0, k, n);
+            const T *row = sU + SI(xr.base, r0), *jq = sJQ12 + SI(k, r0);
             T *out = sUQ + SI(k, r0);
-            if (k >= 5 && k <= n - 4) {
 #pragma unroll 1
-                for (int l = r0; l < r1; l++, row += SW, jq += SW, out += SW)
-                    *out = *jq * interp4(row[-2], row[-1], row[0], row[1]);
-            } else {
-#pragma unroll 1
-                for (int l = r0; l < r1; l++, row += SW, jq += SW, out += SW)
-                    *out = *jq * ic2i_cl<T>(k, n, Line<T>{row - k, 1});
-            }
+            for (int l = r0; l < r1; l++, row += SW, jq += SW, out += SW) *out = *jq * xr.dot(row);
         }
     }
     __syncthreads();
@@ -291,18 +376,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
         rows_of(max(j0 - 1, 1), min(j1 + 2, n + 1), r0, r1);
         const int i = ia + lane;
         if (i < ib) {
+            const XRow<T> xr = xrow42<T>(2, i, N);
             const int o0 = SI(i, r0);
-            const T *vq = sVQ + o0, *u = sU + o0, *jq = sJQ11 + o0;
+            const T *vq = sVQ + SI(xr.base, r0), *u = sU + o0, *jq = sJQ11 + o0;
             T *out = sJUT + o0;
-            if (i >= 4 && i <= N - 3) {
 #pragma unroll 1
-                for (int j = r0; j < r1; j++, vq += SW, u += SW, jq += SW, out += SW)
-                    *out = *jq * *u + interp4(vq[-1], vq[0], vq[1], vq[2]);
-            } else {
-#pragma unroll 1
-                for (int j = r0; j < r1; j++, vq += SW, u += SW, jq += SW, out += SW)
-                    *out = *jq * *u + ii2c_cl<T>(i, N, Line<T>{vq - i, 1});
-            }
+            for (int j = r0; j < r1; j++, vq += SW, u += SW, jq += SW, out += SW) *out = *jq * *u + xr.dot(vq);
         }
     }
     {
@@ -379,16 +458,14 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
         rows_of(max(j0 - 1, 1), min(j1 + 2, n + 1), r0, r1);
         const int k = i0 + lane;
         if (lane < tw && k != 1 && k != n) {
-            const int o0 = SI(k, r0);
-            const T *rj = sJUT + o0, *ri = siJy + o0, *fj = sF + o0;
+            const XRow<T> xr = xrow42<T>(0, k, n);
+            const int o0 = SI(k, r0), ob = SI(xr.base, r0);
+            const T *rj = sJUT + ob, *ri = siJy + ob, *fj = sF + o0;
             T *out = sVP + o0;
-            const bool kin = k >= 5 && k <= n - 4;
 #pragma unroll 1
             for (int l = r0; l < r1; l++, rj += SW, ri += SW, fj += SW, out += SW) {
                 if (l == 1 || l == n) continue;
-                const T v = kin ? interp4(rj[-2] * ri[-2], rj[-1] * ri[-1], rj[0] * ri[0], rj[1] * ri[1])
-                                : ic2i_cl2<T>(k, n, Line2<T>{rj - k, ri - k, 1});
-                *out = -*fj * v;
+                *out = -*fj * xr.dot2(rj, ri);
             }
         }
     }
@@ -398,16 +475,16 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
         rows_of(j0, j1, r0, r1);
         const int k = i0 + lane;
         if (lane < tw && k != 1 && k != n && r0 < r1) {
+            const XRow<T> xr = xrow42<T>(1, k, n);
             const T *cj = sJVT + SI(k, 0), *ia = siJa + SI(k, 0);
-            const T *rj = sJUT + SI(k, r0);
+            const T *rj = sJUT + SI(xr.base, r0);
             T *out = sDIV + SI(k, 0);
-            const bool kin = k >= 5 && k <= n - 4;
             T f0 = cj[(r0 - 2) * SW], f1 = cj[(r0 - 1) * SW], f2 = cj[r0 * SW];
 #pragma unroll 1
             for (int l = r0; l < r1; l++, rj += SW) {
                 const T f3 = cj[(l + 1) * SW];
                 if (l != 1 && l != n) {
-                    const T dx = kin ? diff4(rj[-2], rj[-1], rj[0], rj[1]) : dc2i_cl<T>(k, n, Line<T>{rj - k, 1});
+                    const T dx = xr.dot(rj);
                     const T dy = (l >= 5 && l <= n - 4) ? diff4(f0, f1, f2, f3) : dc2i_cl<T>(l, n, Line<T>{cj, SW});
                     out[l * SW] = (dx * fm.inv_hx + dy * fm.inv_hx) * ia[l * SW];
                 }
@@ -450,7 +527,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
     T *cmp = CMP ? CMP + po : nullptr;
     if (lane < tw && q0 < q1) {
         const int i = ip;
-        const bool iu = i <= N, iin = i >= 4 && i <= N - 3;
+        const bool iu = i <= N;
+        // x rows of the u points: the nodes->centres difference of h and interpolation of up
+        const XRow<T> xd = xrow42<T>(3, iu ? i : N, N), xi = xrow42<T>(2, iu ? i : N, N);
         const T *hc = sH + SI(i, 0), *pc_ = sVP + SI(i, 0);
         // y windows of h (rows j-1 .. j+2) and vp
         T h0 = hc[(q0 - 1) * SW], h1 = hc[q0 * SW], h2 = hc[(q0 + 1) * SW];
@@ -466,16 +545,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, OCC)
             k3[1] = T(0);
             k3[2] = T(0);
             if (iu) {
-                const T *hr_ = sH + so, *ur = sUP + so;
-                T gx;
-                T cu;
-                if (iin) {
-                    gx = diff4(hr_[-1], hr_[0], hr_[1], hr_[2]);
-                    cu = interp4(ur[-1], ur[0], ur[1], ur[2]);
-                } else {
-                    gx = di2c_cl<T>(i, N, Line<T>{hr_ - i, 1});
-                    cu = ii2c_cl<T>(i, N, Line<T>{ur - i, 1});
-                }
+                const T *hr_ = sH + so;
+                T gx = xd.dot(sH + SI(xd.base, j));
+                const T cu = xi.dot(sUP + SI(xi.base, j));
                 if (i <= SB::NSAT) gx += T(SB::satw(i)) * (hr_[1 - i] - hl[j - j0]);
                 if (i >= N + 1 - SB::NSAT) gx += T(SB::satw(N + 1 - i)) * (hr[j - j0] - hr_[n - i]);
                 k3[1] = -fm.grav * (gx * fm.inv_hxa) + cu * siJy[so];
