@@ -89,7 +89,16 @@ void FusedTU<T>::strip(int members, const T *y, T *es, const Dims &d, const Fuse
 template <class T>
 cudaError_t FusedTU<T>::upload_tables(const Link *links)
 {
-    return cudaMemcpyToSymbol(c_link, links, sizeof(Link) * NPAN * 4);
+    cudaError_t e = cudaMemcpyToSymbol(c_link, links, sizeof(Link) * NPAN * 4);
+    double w[XROW_LEN];
+    T wt[XROW_LEN];
+    xrow42_table(w);
+    for (int m = 0; m < XROW_LEN; m++) wt[m] = T(w[m]);
+    if (e == cudaSuccess) {
+        if constexpr (sizeof(T) == 4) e = cudaMemcpyToSymbol(g_xrow_f, wt, sizeof(wt));
+        else e = cudaMemcpyToSymbol(g_xrow_d, wt, sizeof(wt));
+    }
+    return e;
 }
 
 }  // namespace chswe

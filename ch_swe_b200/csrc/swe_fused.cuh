@@ -151,63 +151,81 @@ struct XRow {
     }
 };
 
-// op 0: I_c2i (nodes k = 1..nx from centres 1..nx-1), 1: D_c2i, 2: I_i2c (centres
-// k = 1..n from nodes 1..n+1), 3: D_i2c.
-template <class T>
-__device__ __noinline__ XRow<T> xrow42(int op, int k, int nm)
+// The weight rows of the four x operators: [op][row][5], op 0 I_c2i (nodes k = 1..nx from
+// centres 1..nx-1), 1 D_c2i, 2 I_i2c (centres k = 1..n from nodes 1..n+1), 3 D_i2c; rows
+// 0-3 the closures at k = 1..4 (inputs 1..5), rows 4-7 their mirrors at k = nm - row + 4
+// (inputs nm-4..nm for c2i, n-2..n+2 for i2c), row 8 the interior.  Filled on the host
+// (xrow42_table) and copied to the table of each precision when a context is created.
+constexpr int XROW_OPS = 4, XROW_ROWS = 9, XROW_LEN = XROW_OPS * XROW_ROWS * 5;
+static __device__ float g_xrow_f[XROW_LEN];
+static __device__ double g_xrow_d[XROW_LEN];
+
+static inline void xrow42_table(double *out)
 {
     using namespace sbp;
-    XRow<T> r;
-    double w[5] = {0, 0, 0, 0, 0};
-    if (op <= 1) {
-        const int nx = nm;
-        const bool D = op == 1;
-        if (k >= 5 && k <= nx - 4) {
-            r.base = k - 2;
-            if (D) { w[0] = 1.0 / 24.0; w[1] = -27.0 / 24.0; w[2] = 27.0 / 24.0; w[3] = -1.0 / 24.0; }
-            else { w[0] = -0.0625; w[1] = 0.5625; w[2] = 0.5625; w[3] = -0.0625; }
+    for (int m = 0; m < XROW_LEN; m++) out[m] = 0.0;
+    for (int op = 0; op < XROW_OPS; op++) {
+        const bool D = op == 1 || op == 3, c2i = op <= 1;
+        double q[4][5] = {};
+        if (c2i) {
+            const double c[4][5] = {{D ? DC11 : IC11, D ? DC12 : IC12, D ? DC13 : IC13, 0, 0},
+                                    {D ? DC21 : IC21, D ? DC22 : IC22, D ? 0.0 : IC23, 0, 0},
+                                    {D ? DC31 : IC31, D ? DC32 : IC32, D ? DC33 : IC33, D ? DC34 : IC34, 0},
+                                    {D ? DC41 : IC41, D ? DC42 : IC42, D ? DC43 : IC43, D ? DC44 : IC44, D ? DC45 : IC45}};
+            for (int r = 0; r < 4; r++)
+                for (int m = 0; m < 5; m++) q[r][m] = c[r][m];
         } else {
-            const double q[4][5] = {
-                {D ? DC11 : IC11, D ? DC12 : IC12, D ? DC13 : IC13, 0, 0},
-                {D ? DC21 : IC21, D ? DC22 : IC22, D ? 0.0 : IC23, 0, 0},
-                {D ? DC31 : IC31, D ? DC32 : IC32, D ? DC33 : IC33, D ? DC34 : IC34, 0},
-                {D ? DC41 : IC41, D ? DC42 : IC42, D ? DC43 : IC43, D ? DC44 : IC44, D ? DC45 : IC45}};
-            if (k <= 4) {
-                r.base = 1;
-                for (int m = 0; m < 5; m++) w[m] = q[k - 1][m];
-            } else {
-                // mirrored rows: input nx - 1 - m carries q[row][m] (negated for the difference)
-                const int row = nx - k;
-                r.base = nx - 5;
-                for (int m = 0; m < 5; m++) w[4 - m] = D ? -q[row][m] : q[row][m];
-            }
-        }
-    } else {
-        const int n = nm;
-        const bool D = op == 3;
-        if (k >= 4 && k <= n - 3) {
-            r.base = k - 1;
-            if (D) { w[0] = 1.0 / 24.0; w[1] = -27.0 / 24.0; w[2] = 27.0 / 24.0; w[3] = -1.0 / 24.0; }
-            else { w[0] = -0.0625; w[1] = 0.5625; w[2] = 0.5625; w[3] = -0.0625; }
-        } else {
-            const double q[3][5] = {{D ? DI11 : II11, D ? DI12 : II12, D ? DI13 : II13, D ? DI14 : II14, 0},
-                                    {D ? DI21 : II21, D ? DI22 : II22, D ? DI23 : II23, D ? DI24 : II24, 0},
-                                    {D ? DI31 : II31, D ? 0.0 : II32, D ? DI33 : II33, D ? DI34 : II34, D ? 0.0 : II35}};
             // the 4-2 i2c difference's third row skips its second input and reaches the fifth
-            if (k <= 3) {
-                r.base = 1;
-                for (int m = 0; m < 5; m++) w[m] = q[k - 1][m];
-                if (D && k == 3) w[4] = DI35;
-            } else {
-                // mirrored rows: input n + 1 - m carries q[row][m] (negated for the difference)
-                const int row = n - k;
-                r.base = n - 3;
-                for (int m = 0; m < 5; m++) w[4 - m] = D ? -q[row][m] : q[row][m];
-                if (D && row == 2) w[0] = -DI35;
-            }
+            const double c[3][5] = {{D ? DI11 : II11, D ? DI12 : II12, D ? DI13 : II13, D ? DI14 : II14, 0},
+                                    {D ? DI21 : II21, D ? DI22 : II22, D ? DI23 : II23, D ? DI24 : II24, 0},
+                                    {D ? DI31 : II31, D ? 0.0 : II32, D ? DI33 : II33, D ? DI34 : II34, D ? DI35 : II35}};
+            for (int r = 0; r < 3; r++)
+                for (int m = 0; m < 5; m++) q[r][m] = c[r][m];
         }
+        double *o = out + op * XROW_ROWS * 5;
+        const int nrow = c2i ? 4 : 3;
+        for (int r = 0; r < nrow; r++)
+            for (int m = 0; m < 5; m++) {
+                o[r * 5 + m] = q[r][m];
+                // mirrored row: the input at distance m from the far end carries q[r][m]
+                // (negated for the difference)
+                o[(4 + r) * 5 + 4 - m] = D ? -q[r][m] : q[r][m];
+            }
+        const double in[4] = {D ? 1.0 / 24.0 : -0.0625, D ? -27.0 / 24.0 : 0.5625, D ? 27.0 / 24.0 : 0.5625,
+                              D ? -1.0 / 24.0 : -0.0625};
+        for (int m = 0; m < 4; m++) o[8 * 5 + m] = in[m];
     }
-    for (int m = 0; m < 5; m++) r.w[m] = T(w[m]);
+}
+
+template <class T>
+__device__ __forceinline__ const T *xrow_table()
+{
+    if constexpr (sizeof(T) == 4) return g_xrow_f;
+    else return g_xrow_d;
+}
+
+// The weight row of operator op at output k of nm (nx for c2i, n for i2c), k in 1..nm.
+template <class T>
+__device__ __forceinline__ XRow<T> xrow42(int op, int k, int nm)
+{
+    const bool c2i = op <= 1;
+    k = max(1, min(k, nm));
+    int row, base;
+    if (k <= (c2i ? 4 : 3)) {
+        row = k - 1;
+        base = 1;
+    } else if (k > (c2i ? nm - 4 : nm - 3)) {
+        row = 4 + nm - k;
+        base = c2i ? nm - 5 : nm - 3;
+    } else {
+        row = 8;
+        base = c2i ? k - 2 : k - 1;
+    }
+    const T *w = xrow_table<T>() + (op * XROW_ROWS + row) * 5;
+    XRow<T> r;
+    r.base = base;
+#pragma unroll
+    for (int m = 0; m < 5; m++) r.w[m] = __ldg(w + m);
     return r;
 }
 
