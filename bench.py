@@ -205,11 +205,13 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def profile_traffic(precision):
+def profile_traffic(key):
+    """DRAM bytes per launch of the stage kernel at C192 from the ncu captures summarised
+    under profiles/: key "fp32" (the split k_stage) or "fp32_fused" (k_fstage)."""
     p = os.path.join(ROOT, "profiles", "k_stage_c192_traffic.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get(precision)
+            return json.load(open(p)).get(key)
         except Exception:
             return None
     return None
@@ -400,10 +402,19 @@ def run_serving(args, torch):
     reqs = serve.poisson_stream(SRV_REQUESTS, rate=SRV_RATE, seed=SRV_SEED)
     for r in reqs:
         r.ic   # generate the initial states before the clock starts
-    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16)
+    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16, grouped=True)
     # tuning is a one-time cost per pool shape: done before the stream starts
     srv.pretune({(r.N, r.precision, r.operator) for r in reqs})
     stats = srv.run(reqs, realtime=True)
+    srv.close()
+    group_ticks = srv.group_ticks
+    # the same stream with every pool ticking on its own stream (no group launches)
+    reqs_u = serve.poisson_stream(SRV_REQUESTS, rate=SRV_RATE, seed=SRV_SEED)
+    for r in reqs_u:
+        r.ic
+    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16)
+    srv.pretune({(r.N, r.precision, r.operator) for r in reqs_u})
+    su = srv.run(reqs_u, realtime=True)
     srv.close()
     # FP32 requests against the same request in FP64 (the FP64 path is pinned to the
     # oracle at 1e-12): a bounded sample of the smaller cubes
@@ -427,7 +438,7 @@ def run_serving(args, torch):
     low = serve.poisson_stream(SRV_LOW_REQUESTS, rate=SRV_LOW_RATE, seed=SRV_LOW_SEED)
     for r in low:
         r.ic
-    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16)
+    srv = serve.Server(hbm_budget_bytes=SRV_BUDGET, max_tick=16, grouped=True)
     srv.pretune({(r.N, r.precision, r.operator) for r in low})
     ls = srv.run(low, realtime=True)
     srv.close()
@@ -435,6 +446,9 @@ def run_serving(args, torch):
     return {
         "workload": f"{SRV_REQUESTS} requests, Poisson {SRV_RATE:g}/s (seed {SRV_SEED}), N in {list(serve.SIZES)}, "
                     "24-576 RK4 steps, FP32/FP64 50/50, linear/advective operator 50/50, 1-4 seeded Gaussians",
+        "grouped": {"what": "the linear pools of each precision tick together: one grid per kernel over "
+                               "their cube sizes (swe_group_rk4_steps_members), 12 launches per RK4 step",
+                    "group_ticks": group_ticks},
         "requests": stats.n, "makespan_s": stats.makespan_s, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
         "mean_ms": stats.mean_ms, "requests_per_s": stats.requests_per_s,
         "cell_updates_per_s": stats.cell_updates_per_s, "hbm_budget_bytes": SRV_BUDGET,
@@ -447,6 +461,10 @@ def run_serving(args, torch):
                        "seconds": seq_s, "cell_updates_per_s": sum(r.cell_updates for r in reqs) / seq_s,
                        "served_over_sequential": (sum(r.cell_updates for r in reqs) / stats.makespan_s) /
                                                  (sum(r.cell_updates for r in reqs) / seq_s)},
+        "ungrouped": {"what": "the same stream, every pool ticking on its own stream",
+                      "makespan_s": su.makespan_s, "cell_updates_per_s": su.cell_updates_per_s,
+                      "p50_ms": su.p50_ms, "p99_ms": su.p99_ms, "service_p50_ms": su.service_p50_ms,
+                      "service_p99_ms": su.service_p99_ms},
         "below_capacity": {
             "workload": f"{SRV_LOW_REQUESTS} requests, Poisson {SRV_LOW_RATE:g}/s (seed {SRV_LOW_SEED}), same mix",
             "offered_cell_updates_per_s": offered, "makespan_s": ls.makespan_s,
@@ -595,6 +613,11 @@ def run_ours(args):
     # read and write in S4 (2): 19 words of 4 B per step, 19/4 per launch
     alg_bytes_32 = D * 4 * (19 / 4)
     achieved = alg_bytes_32 / (r32["ms_stage"] / 1e3) / 1e9
+    # the stage kernel of the configuration the autotuner chose: the split k_stage (its
+    # contravariant components from k_co2contra) or the fused k_fstage (TMA tiles, the
+    # contravariant components computed in the tile, edge strips from k_strip)
+    fused32 = r32["kernel_config"][2] == 2
+    kn = ("k_strip", "k_edge", "k_fstage") if fused32 else ("k_co2contra", "k_edge", "k_stage")
     peak = float(peaks.get("hbm_gbs", 6650.0))
     line = {
         "metric": "C192 RK4 cell-updates/s", "value": v32, "unit": "cell-updates/s", "n_gpus": world,
@@ -610,14 +633,14 @@ def run_ours(args):
                  "tune_ms_per_rk4_step": r64["tune_ms_per_rk4_step"]},
         "fp32_tile": r32["tile"], "fp32_kernel_config": r32["kernel_config"],
         "fp64_kernel_config": r64["kernel_config"], "fp32_tune_ms_per_rk4_step": r32["tune_ms_per_rk4_step"],
-        "fp32_kernel_ms": {"k_co2contra": r32["ms_co2contra"], "k_edge": r32["ms_edge"], "k_stage": r32["ms_stage"]},
+        "fp32_kernel_ms": {kn[0]: r32["ms_co2contra"], kn[1]: r32["ms_edge"], kn[2]: r32["ms_stage"]},
         "fp32_over_fp64": v32 / v64,
         "fp32_vs_fp64_after_one_day": errs,
         "e2e": {"value": r32["e2e_value"], "unit": "cell-updates/s", "h2d_bytes_per_step": r32["e2e_bytes"],
                 "d2h_bytes_per_step": r32["e2e_bytes"],
                 "path": "ch_swe_b200.swm -> libchswe.so C ABI: upload (pinned staging), 576 RK4 steps, download"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profile_traffic("fp32"), "kernel": "k_stage<float>",
+                     "traffic": profile_traffic("fp32_fused" if fused32 else "fp32"), "kernel": kn[2] + "<float>",
                      "peak_source": src, "ms_per_launch": r32["ms_stage"],
                      "alg_bytes_per_launch": alg_bytes_32},
         "gpu_launches": r32["launches"],

@@ -35,6 +35,8 @@ EXPORTED = [
     "swe_set_tile", "swe_get_tile", "swe_autotune", "swe_rk4_steps_members",
     "swe_set_kernel_config", "swe_get_kernel_config", "swe_diag", "swe_energies", "swe_curl", "swe_regrid_latlon", "swe_regrid_latlon_wind",
     "swe_set_orography", "swe_c_grad", "swe_c_div",
+    "swe_group_create", "swe_group_destroy", "swe_group_rk4_steps_members", "swe_group_synchronize",
+    "swe_group_last_error", "swe_group_launch_count",
 ]
 
 
@@ -115,6 +117,14 @@ def load(path: str = LIB_PATH):
     L.swe_set_kernel_config.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.swe_get_kernel_config.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]
+    L.swe_group_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]
+    L.swe_group_destroy.argtypes = [_vp]
+    L.swe_group_rk4_steps_members.argtypes = [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_dp), ctypes.c_int]
+    L.swe_group_synchronize.argtypes = [_vp]
+    L.swe_group_last_error.argtypes = [_vp]
+    L.swe_group_last_error.restype = ctypes.c_char_p
+    L.swe_group_launch_count.argtypes = [_vp]
+    L.swe_group_launch_count.restype = ctypes.c_longlong
     for name in EXPORTED:
         if not hasattr(L, name):
             raise SweError(f"libchswe.so does not export {name}")

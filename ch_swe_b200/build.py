@@ -19,13 +19,18 @@ STAGE_SOURCES = [f"stage_{p}{tm}.cu" for p in ("f", "d") for tm in (17, 25, 33)]
 # the fused stage (TMA tiles, contravariant components in the stage) and its edge-strip
 # kernel, one unit per precision
 FUSED_SOURCES = ["fused_f.cu", "fused_d.cu"]
-SOURCES = ["swe_api.cu", *STAGE_SOURCES, *FUSED_SOURCES]
+# the group launches (the RK4 stages of several contexts as one grid), one unit per
+# precision
+GROUP_SOURCES = ["group_f.cu", "group_d.cu"]
+SOURCES = ["swe_api.cu", *STAGE_SOURCES, *FUSED_SOURCES, *GROUP_SOURCES]
 COMMON_HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh", "swe_launch.cuh",
                   "swe_fused.cuh", "swe_tma.cuh"]
 UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh"],
                 **{src: COMMON_HEADERS + ["fused_tu.cuh"] for src in FUSED_SOURCES}}
 STAGE_HEADERS = COMMON_HEADERS + ["swe_tiled.cuh", "swe_stage_tu.cuh"]
-HEADERS = sorted(set(COMMON_HEADERS + UNIT_HEADERS["swe_api.cu"] + STAGE_HEADERS + ["fused_tu.cuh"]))
+UNIT_HEADERS.update({src: COMMON_HEADERS + ["swe_tiled.cuh", "swe_group.cuh", "group_tu.cuh"] for src in GROUP_SOURCES})
+HEADERS = sorted(set(COMMON_HEADERS + UNIT_HEADERS["swe_api.cu"] + STAGE_HEADERS + ["fused_tu.cuh", "swe_group.cuh",
+                                                                                    "group_tu.cuh"]))
 DEPS = SOURCES + HEADERS
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

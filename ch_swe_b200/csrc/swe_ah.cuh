@@ -128,25 +128,67 @@ __global__ void __launch_bounds__(128) k_ah_edge(const T *__restrict__ Y, T *__r
     e[2] = dv;
 }
 
-// k_ah_stage: every vertex of every panel and member.  The raw values, on the panel
-// edges the syncs with the neighbours' raw values from k_ah_edge (the neighbour's
-// vector is handed over as the 'cross' exchange does, halo_vec), the tendency and
-// the RK update of k_stage (modes 0..4; FP32 mode 4 Kahan-compensated).
+// Tiles of k_ah_stage: AH_TX x AH_TY vertices per block of 32 x 8 threads (two rows
+// per thread); the windows reach AH_R(ORD) vertices beyond the tile on each side, the
+// farthest input of an SBP row of that order (2-1: 1; 4-2: 3, the closure rows 1
+// and 4; 6-3: 8, the closure row 1 reaches f(9)).
+constexpr int AH_TX = 32, AH_TY = 16;
+template <int ORD>
+__host__ __device__ constexpr int ah_reach() { return ORD == 21 ? 1 : (ORD == 63 ? 8 : 3); }
+
+// k_ah_stage: every vertex of every panel and member, one tile per block.  The block
+// stages h and the fluxes J (Qi11 u + Qi12 v), J (Qi12 u + Qi22 v) of its window in
+// shared memory (each window vertex loaded and multiplied once), then each thread
+// takes the x and y differences of its vertices from there: the raw values; on the
+// panel edges the syncs with the neighbours' raw values from k_ah_edge (the
+// neighbour's vector is handed over as the 'cross' exchange does, halo_vec); the
+// tendency and the RK update of k_stage (modes 0..4; FP32 mode 4 Kahan-compensated).
 template <class T, int MODE, int ORD>
 __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, const T *__restrict__ E, T *V0, T *Y1,
                                                   T *ACC, T *CMP, Dims d, AhView<T> a, MetricView<T> m, StageArgs sa,
                                                   T grav)
 {
+    constexpr int R = ah_reach<ORD>(), W = AH_TX + 2 * R, H = AH_TY + 2 * R;
+    __shared__ T sH[H * W], sF[H * W], sG[H * W];
     const int N = d.N, n = N + 1;
     const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
     if (member_frozen(sa.dtm, mem)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i0 = 1 + blockIdx.x * AH_TX, j0 = 1 + blockIdx.y * AH_TY;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const T *y = Yin + mem * d.ms;
+    const T *yh = y + t * d.ps, *yu = yh + d.fs, *yv = yh + 2 * d.fs;
     pdl_trigger();
     pdl_wait();
-    if (i > n || j > n) return;
-    const T *y = Yin + mem * d.ms;
-    T gx, gy, dv;
-    ah_raw<T, ORD>(y, d, a, m, t, i, j, gx, gy, dv);
+    // the window: the tile's rows over the x reach and its columns over the y reach (the
+    // corners are never read); vertices outside the panel hold zeros (no stencil reads them)
+    for (int q = tid; q < H * W; q += 256) {
+        const int wi = q % W, wj = q / W;
+        const int i = i0 - R + wi, j = j0 - R + wj;
+        const bool band = (wj >= R && wj < R + AH_TY) || (wi >= R && wi < R + AH_TX);
+        T h = T(0), f = T(0), g = T(0);
+        if (band && i >= 1 && i <= n && j >= 1 && j <= n) {
+            const int64_t o = box_off(d.P, i, j);
+            const T u = __ldcg(yu + o), v = __ldcg(yv + o), J = __ldg(a.J + o);
+            h = __ldcg(yh + o);
+            f = J * (__ldg(a.Q1 + o) * u + __ldg(a.Q2 + o) * v);
+            g = J * (__ldg(a.Q2 + o) * u + __ldg(a.Q3 + o) * v);
+        }
+        sH[q] = h;
+        sF[q] = f;
+        sG[q] = g;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int rr = 0; rr < AH_TY / 8; rr++) {
+        const int i = i0 + threadIdx.x, j = j0 + threadIdx.y + 8 * rr;
+        if (i > n || j > n) continue;
+        const int ro = (j - j0 + R) * W - i0 + R, co = i - i0 + R - j0 * W + R * W;
+        // row j of the window at column k, column i at row l
+        T gx = dn2n<T, ORD>(i, n, [&](int k) { return sH[ro + k]; }) * m.inv_hxa;
+        T gy = dn2n<T, ORD>(j, n, [&](int l) { return sH[co + l * W]; }) * m.inv_hxa;
+        const T dx = dn2n<T, ORD>(i, n, [&](int k) { return sF[ro + k]; });
+        const T dy = dn2n<T, ORD>(j, n, [&](int l) { return sG[co + l * W]; });
+        T dv = (dx * m.inv_hx + dy * m.inv_hx) * __ldg(m.iJa + box_off(d.P, i, j));
     const bool il = i == 1, ir = i == n, jb = j == 1, jt = j == n;
     const bool cx = il || ir, cy = jb || jt;
     if (cx || cy) {
@@ -184,7 +226,7 @@ __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, con
         }
     }
     const int64_t o = box_off(d.P, i, j);
-    const T u = y[t * d.ps + d.fs + o], v = y[t * d.ps + 2 * d.fs + o];
+    const T u = __ldcg(yu + o), v = __ldcg(yv + o);
     const T ut = a.Q1[o] * u + a.Q2[o] * v, vt = a.Q2[o] * u + a.Q3[o] * v;
     const T fJ = a.fJ[t * d.ps + o];
     const T k3[3] = {-T(sa.Hm[mem]) * dv, -grav * gx + fJ * vt, -grav * gy - fJ * ut};
@@ -208,6 +250,7 @@ __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, con
         } else {
             V0[of] = V0[of] + (ACC[of] + (dt / T(6)) * k3[f]);
         }
+    }
     }
 }
 

@@ -245,6 +245,10 @@ struct swe_ctx {
     int ll_nlat = 0, ll_nlon = 0;
     int *ll_i = nullptr;
     double *ll_d = nullptr;
+    // lat-lon regrid of the curl (cell centres, ECS_O halo), built on first use for a grid size
+    int llo_nlat = 0, llo_nlon = 0;
+    int *llo_i = nullptr;
+    double *llo_d = nullptr;
     double *red = nullptr;           // reduction partials
     unsigned char *pinned = nullptr; // pinned host staging for uploads/downloads (whole batch)
     // captured RK4 step
@@ -980,7 +984,7 @@ static void free_ctx(swe_ctx *c)
     if (c->graphk) cudaGraphExecDestroy(c->graphk);
     cudaFree(c->m64.base); cudaFree(c->m32.base); cudaFree(c->Hm); cudaFree(c->dtm);
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
-    cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d);
+    cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d); cudaFree(c->llo_i); cudaFree(c->llo_d);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
@@ -1406,6 +1410,7 @@ static cudaError_t stage_smem_optin()
     if (e == cudaSuccess) e = StageTU<T, 25>::optin();
     if (e == cudaSuccess) e = StageTU<T, 33>::optin();
     if (e == cudaSuccess) e = FusedTU<T>::optin();
+    if (e == cudaSuccess) e = GroupTU<T>::optin();
     if (e == cudaSuccess) e = set_carveout(k_edge<T, 42>);
     if (e == cudaSuccess) e = set_carveout(k_edge<T, 21>);
     if (e == cudaSuccess) e = set_carveout(k_edge<T, 63>);
@@ -1459,7 +1464,7 @@ static void launch_ah(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc
     const int n = c->cfg.N + 1, M = c->cfg.n_members;
     launch_k(k_ah_edge<T, ORD>, dim3((n + 127) / 128, NPAN * 4, M), dim3(128), 0, c->stream, (const T *)yin,
              (T *)c->edge, c->dims, av, mv, dtm);
-    const dim3 pb(32, 8), pg((n + 31) / 32, (n + 7) / 8, NPAN * M);
+    const dim3 pb(32, 8), pg((n + AH_TX - 1) / AH_TX, (n + AH_TY - 1) / AH_TY, NPAN * M);
     const T g = T(c->cfg.grav);
     const T *Y = (const T *)yin, *E = (const T *)c->edge;
     T *V = (T *)v0, *Y1 = (T *)y1, *A = (T *)acc, *C = (T *)cmp;
@@ -1768,6 +1773,243 @@ extern "C" int swe_rk4_steps_members(swe_ctx *c, swe_stvec *v0, const double *dt
     if (nsteps == 0) return SWE_OK;
     CU(c, cudaMemcpyAsync(c->dtm, dt, sizeof(double) * M, cudaMemcpyHostToDevice, c->stream));
     return run_steps(c, v0, 0.0, true, nsteps);
+}
+
+// ---------------------------------------------------------------------------
+// Groups: the RK4 steps of several contexts as one grid per kernel
+// ---------------------------------------------------------------------------
+
+struct swe_group {
+    std::vector<swe_ctx *> ctx;
+    size_t elem = 8;
+    int tile = 25, occ = 3, runs = 0;
+    cudaStream_t stream = nullptr;     // the first context's stream
+    cudaEvent_t ev = nullptr;          // joins the contexts' streams and the group's
+    std::vector<const void *> graph_v; // the states the captured graphs advance
+    cudaGraphExec_t graph = nullptr, graphk = nullptr;   // one RK4 step, GRAPH_STEPS steps
+    long long launches = 0;
+    std::string err;
+};
+
+static int gfail(swe_group *g, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g->err = buf;
+    return code;
+}
+
+static bool group_cfg_built(int tm, int occ, int runs)
+{
+    bool found = false;
+#define CHSWE_IS_GCFG(TM, OCC, RUNS) found = found || (tm == TM && occ == OCC && runs == RUNS);
+    CHSWE_GROUP_CFGS(CHSWE_IS_GCFG)
+#undef CHSWE_IS_GCFG
+    return found;
+}
+
+static void group_drop_graphs(swe_group *g)
+{
+    if (g->graph) { cudaGraphExecDestroy(g->graph); g->graph = nullptr; }
+    if (g->graphk) { cudaGraphExecDestroy(g->graphk); g->graphk = nullptr; }
+    g->graph_v.clear();
+}
+
+extern "C" int swe_group_create(swe_ctx *const *ctxs, int n, swe_group **out)
+{
+    if (!out) return SWE_EINVAL;
+    *out = nullptr;
+    if (!ctxs || n < 1 || n > GROUP_MAX || !ctxs[0]) return SWE_EINVAL;
+    swe_ctx *c0 = ctxs[0];
+    for (int k = 0; k < n; k++) {
+        swe_ctx *c = ctxs[k];
+        if (!c) return fail(c0, SWE_EINVAL, "group: context %d is null", k);
+        for (int q = 0; q < k; q++)
+            if (ctxs[q] == c) return fail(c0, SWE_EINVAL, "group: context %d appears twice", k);
+        if (c->device != c0->device || c->elem != c0->elem)
+            return fail(c0, SWE_EINVAL, "group: context %d has another device or precision than context 0", k);
+        if (c->adv || c->ah || c->cstag || c->ord != 42)
+            return fail(c0, SWE_EINVAL, "group: context %d is not the linear operator on Ch in SBP 4-2", k);
+        if (c->fused || c->tile != c0->tile || c->occ != c0->occ || c->runs != c0->runs)
+            return fail(c0, SWE_EINVAL, "group: context %d has another kernel configuration than context 0 "
+                        "(the contexts share one split configuration)", k);
+    }
+    if (c0->fused || !group_cfg_built(c0->tile, c0->occ, c0->runs))
+        return fail(c0, SWE_EINVAL, "group: kernel configuration (%d, %d, %d) has no group launch; built: "
+                    "(17, 4, 0), (25, 3, 0), (33, 2, 0)", c0->tile, c0->occ, c0->runs);
+    swe_group *g = new swe_group;
+    g->ctx.assign(ctxs, ctxs + n);
+    g->elem = c0->elem;
+    g->tile = c0->tile;
+    g->occ = c0->occ;
+    g->runs = c0->runs;
+    g->stream = c0->stream;
+    if (cudaSetDevice(c0->device) != cudaSuccess || cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming) != cudaSuccess) {
+        delete g;
+        return fail(c0, SWE_ECUDA, "group: event creation failed");
+    }
+    *out = g;
+    return SWE_OK;
+}
+
+extern "C" int swe_group_destroy(swe_group *g)
+{
+    if (!g) return SWE_OK;
+    cudaSetDevice(g->ctx[0]->device);
+    cudaStreamSynchronize(g->stream);
+    group_drop_graphs(g);
+    if (g->ev) cudaEventDestroy(g->ev);
+    delete g;
+    return SWE_OK;
+}
+
+extern "C" const char *swe_group_last_error(const swe_group *g) { return g ? g->err.c_str() : "null group"; }
+
+extern "C" long long swe_group_launch_count(const swe_group *g) { return g ? g->launches : -1; }
+
+template <class T>
+static const MetricView<T> &metric_view(const swe_ctx *c);
+template <> const MetricView<double> &metric_view<double>(const swe_ctx *c) { return c->m64.v; }
+template <> const MetricView<float> &metric_view<float>(const swe_ctx *c) { return c->m32.v; }
+
+// The table of one group step: every context's state and scratch, its tiles from
+// flat block tile0 on and its edge chunks from edge0 on.
+template <class T>
+static void group_table(const swe_group *g, swe_stvec *const *st, GroupTable<T> &tab, unsigned &tiles,
+                        unsigned &edges)
+{
+    tab = GroupTable<T>{};
+    tab.n = (int)g->ctx.size();
+    tiles = edges = 0;
+    for (int k = 0; k < tab.n; k++) {
+        const swe_ctx *c = g->ctx[k];
+        GroupEntry<T> &e = tab.e[k];
+        e.d = c->dims;
+        e.m = metric_view<T>(c);
+        e.v = (T *)st[k]->d;
+        e.ya = (T *)c->ya;
+        e.yb = (T *)c->yb;
+        e.acc = (T *)c->acc;
+        e.cmp = sizeof(T) == 4 ? (T *)st[k]->cmp : nullptr;
+        e.w = (T *)c->w;
+        e.es = (T *)c->es;
+        e.e = (T *)c->edge;
+        e.Hm = c->Hm;
+        e.dtm = c->dtm;
+        const dim3 sg = stage_grid(c->cfg.N, c->cfg.n_members, g->tile), eg = edge_grid(c);
+        e.gx = sg.x;
+        e.gy = sg.y;
+        e.nch = eg.x;
+        e.tile0 = tiles;
+        e.edge0 = edges;
+        tiles += sg.x * sg.y * sg.z;
+        edges += eg.x * eg.y * eg.z;
+    }
+}
+
+template <class T>
+static bool group_enqueue_step(swe_group *g, swe_stvec *const *st)
+{
+    GroupTable<T> tab;
+    unsigned tiles, edges;
+    group_table<T>(g, st, tab, tiles, edges);
+    if (!GroupTU<T>::rk4_step(g->tile, g->occ, g->runs, tab, tiles, edges, g->stream)) return false;
+    g->launches += 12;
+    return true;
+}
+
+static int group_capture(swe_group *g, swe_stvec *const *st, int steps, cudaGraphExec_t *out)
+{
+    cudaGraph_t gr;
+    const long long before = g->launches;
+    if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return gfail(g, SWE_ECUDA, "group: graph capture failed to begin");
+    bool ok = true;
+    for (int s = 0; s < steps && ok; s++)
+        ok = g->elem == 8 ? group_enqueue_step<double>(g, st) : group_enqueue_step<float>(g, st);
+    cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
+    g->launches = before;
+    if (e != cudaSuccess) return gfail(g, SWE_ECUDA, "group: graph capture: %s", cudaGetErrorString(e));
+    if (!ok) {
+        cudaGraphDestroy(gr);
+        return gfail(g, SWE_EINVAL, "group: no group launch for the kernel configuration");
+    }
+    e = cudaGraphInstantiate(out, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return gfail(g, SWE_ECUDA, "group: graph instantiate: %s", cudaGetErrorString(e));
+    return SWE_OK;
+}
+
+extern "C" int swe_group_rk4_steps_members(swe_group *g, swe_stvec *const *states, const double *const *dt,
+                                           int nsteps)
+{
+    if (!g || !states || !dt || nsteps < 0) return SWE_EINVAL;
+    const int n = (int)g->ctx.size();
+    for (int k = 0; k < n; k++) {
+        swe_ctx *c = g->ctx[k];
+        if (!states[k] || states[k]->ctx != c) return gfail(g, SWE_EINVAL, "group: state %d is not of context %d", k, k);
+        if (!dt[k]) return gfail(g, SWE_EINVAL, "group: no time steps for context %d", k);
+        for (int m = 0; m < c->cfg.n_members; m++)
+            if (!(dt[k][m] >= 0.0) || !std::isfinite(dt[k][m]))
+                return gfail(g, SWE_EINVAL, "group: context %d member %d: time step %g (need finite, >= 0)", k, m,
+                             dt[k][m]);
+        if (c->fused || c->tile != g->tile || c->occ != g->occ || c->runs != g->runs)
+            return gfail(g, SWE_EINVAL, "group: context %d changed its kernel configuration", k);
+    }
+    if (nsteps == 0) return SWE_OK;
+    if (cudaSetDevice(g->ctx[0]->device) != cudaSuccess) return gfail(g, SWE_ECUDA, "group: cudaSetDevice failed");
+    for (int k = 0; k < n; k++) {
+        int rc = ensure_cmp(states[k]);
+        if (rc) return gfail(g, rc, "group: context %d: %s", k, g->ctx[k]->err.c_str());
+    }
+    // the group's stream waits for the work queued on every context's own stream
+    for (int k = 1; k < n; k++)
+        if (g->ctx[k]->stream != g->stream) {
+            if (cudaEventRecord(g->ev, g->ctx[k]->stream) != cudaSuccess ||
+                cudaStreamWaitEvent(g->stream, g->ev, 0) != cudaSuccess)
+                return gfail(g, SWE_ECUDA, "group: stream join failed");
+        }
+    for (int k = 0; k < n; k++) {
+        swe_ctx *c = g->ctx[k];
+        if (cudaMemcpyAsync(c->dtm, dt[k], sizeof(double) * c->cfg.n_members, cudaMemcpyHostToDevice, g->stream) !=
+            cudaSuccess)
+            return gfail(g, SWE_ECUDA, "group: time step upload failed");
+    }
+    std::vector<const void *> v(n);
+    for (int k = 0; k < n; k++) v[k] = states[k]->d;
+    if (v != g->graph_v) {
+        group_drop_graphs(g);
+        g->graph_v = v;
+    }
+    const int full = nsteps / GRAPH_STEPS, rest = nsteps % GRAPH_STEPS;
+    int rc;
+    if (full > 0 && !g->graphk && (rc = group_capture(g, states, GRAPH_STEPS, &g->graphk))) return rc;
+    if (rest > 0 && !g->graph && (rc = group_capture(g, states, 1, &g->graph))) return rc;
+    for (int s = 0; s < full; s++) {
+        if (cudaGraphLaunch(g->graphk, g->stream) != cudaSuccess) return gfail(g, SWE_ECUDA, "group: graph launch failed");
+        g->launches += 12 * GRAPH_STEPS;
+    }
+    for (int s = 0; s < rest; s++) {
+        if (cudaGraphLaunch(g->graph, g->stream) != cudaSuccess) return gfail(g, SWE_ECUDA, "group: graph launch failed");
+        g->launches += 12;
+    }
+    // every context's own stream waits for the group's steps
+    if (cudaEventRecord(g->ev, g->stream) != cudaSuccess) return gfail(g, SWE_ECUDA, "group: event record failed");
+    for (int k = 1; k < n; k++)
+        if (g->ctx[k]->stream != g->stream && cudaStreamWaitEvent(g->ctx[k]->stream, g->ev, 0) != cudaSuccess)
+            return gfail(g, SWE_ECUDA, "group: stream join failed");
+    return SWE_OK;
+}
+
+extern "C" int swe_group_synchronize(swe_group *g)
+{
+    if (!g) return SWE_EINVAL;
+    if (cudaSetDevice(g->ctx[0]->device) != cudaSuccess || cudaStreamSynchronize(g->stream) != cudaSuccess)
+        return gfail(g, SWE_ECUDA, "group: %s", cudaGetErrorString(cudaGetLastError()));
+    return SWE_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2288,10 +2530,11 @@ __global__ void k_ecs_vec_ext(const T *__restrict__ y, Dims d, const int *__rest
 
 // interp_t%interpolate (latlon_regrid_mod.f90:338-365): the 4 x 4 cubic stencil of
 // every lat-lon point on the extended panel, FP64.
+// ext: the extended panels, pitch E, point (i, j) at [panel][j + 1][i + 1] from i, j = -1 on
+// (the xy panels start at 1 - LL_HW = -1 too).
 __global__ void k_latlon(const double *__restrict__ ext, const int *__restrict__ idx, const double *__restrict__ w,
-                         int N, int64_t npts, double *__restrict__ out)
+                         int E, int64_t npts, double *__restrict__ out)
 {
-    const int E = ll_pitch(N);
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += (int64_t)gridDim.x * blockDim.x) {
         const int t = idx[3 * q], xi = idx[3 * q + 1], yi = idx[3 * q + 2];
         const double *wx = w + 8 * q, *wy = wx + 4;
@@ -2475,6 +2718,226 @@ static int ensure_latlon(swe_ctx *c, int nlat, int nlon)
     return SWE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Lat-lon regrid of the curl (output_curl's curl.dat): the curl on the cell centres,
+// its ECS_O halo of width 2, the cubic stencils on the cell-centre mesh
+// ---------------------------------------------------------------------------
+// Extended cell-centre panels: cells -1 .. N+2 in each direction.
+__host__ __device__ __forceinline__ int llo_pitch(int N) { return N + 4; }
+
+// init_halo_interp (ecs_halo_factory_mod.f90:190-230): for the cell-centre line i of virtual
+// row j beyond a panel edge, the source face's cell left of the projected point and the
+// cubic Lagrange weights on its cells ind-1 .. ind+2 (host, FP64).
+static void halo_o_weights(double dxa, int i, int j, double w[4], int &ind)
+{
+    const double pi = 3.141592653589793238462643383279502884;
+    const double zb = 0.25 * pi + (j - 0.5) * dxa;
+    double za = -0.25 * pi + (i - 0.5) * dxa;
+    double zx = std::tan(za);
+    const double zz = std::tan(zb);
+    zx = zx / zz;
+    za = std::atan(zx);
+    ind = (int)std::floor((za + 0.25 * pi - 0.5 * dxa) / dxa) + 1;
+    const double zxi = (za + 0.25 * pi) / dxa - (ind - 0.5);
+    w[0] = -(zxi * (zxi - 1.0) * (zxi - 2.0) / 6.0);
+    w[1] = (zxi + 1.0) * (zxi - 1.0) * (zxi - 2.0) / 2.0;
+    w[2] = -((zxi + 1.0) * zxi * (zxi - 2.0) / 2.0);
+    w[3] = (zxi + 1.0) * zxi * (zxi - 1.0) / 6.0;
+}
+
+// ext_ecs_tile_halo (ecs_halo_mod.f90:109-175) of a cell-centre field f[panel][j][i] (FP64,
+// N x N per panel) at every point of the extended panels: the cells; the virtual rows of
+// each side interpolated along the neighbour's grid line from its cells at the same
+// depth (ecs_ext_halo_1e, the first row without its end points); and the six special
+// points of each cube corner (ecs_halo_1corner, :230-300), from the cells and the
+// neighbours' cells as the o-point exchange hands them over.  Weights wt / lines kt per
+// row m = 1, 2 and line index i = -1 .. N+2 (the corners use those of i = -1 .. 2,
+// mirrored at the corners with a reversed i direction).
+__global__ void k_ecs_o_ext(const double *__restrict__ f, int N, const int *__restrict__ kt,
+                            const double *__restrict__ wt, double *__restrict__ ext)
+{
+    const int E = llo_pitch(N), ni = N + 4;
+    const int64_t total = (int64_t)NPAN * E * E;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int t = (int)(q / (E * E)), r = (int)(q % (E * E));
+        const int i = r % E - 1, j = r / E - 1;
+        auto cell = [&](int p, int k, int l) { return f[((int64_t)p * N + (l - 1)) * N + (k - 1)]; };
+        // the exchange's value across side s at depth m, along index b (1..N) of this side
+        auto X = [&](int s, int m, int b) {
+            int p, k, l;
+            c_halo_cell(N, t, s, b, m, p, k, l);
+            return cell(p, k, l);
+        };
+        // the exchanged field: a cell of this panel or of a neighbour
+        auto pf = [&](int x, int y) {
+            if (y < 1) return X(SIDE_B, 1 - y, x);
+            if (y > N) return X(SIDE_T, y - N, x);
+            if (x < 1) return X(SIDE_L, 1 - x, y);
+            if (x > N) return X(SIDE_R, x - N, y);
+            return cell(t, x, y);
+        };
+        auto W = [&](int k, int a, int m) { return wt[4 * ((m - 1) * ni + a + 1) + k + 1]; };
+        double v;
+        if (i >= 1 && i <= N && j >= 1 && j <= N) {
+            v = cell(t, i, j);
+        } else {
+            // a virtual row: side, depth m, along index a
+            int s = -1, m = 0, a = 0;
+            if (j < 1) { s = SIDE_B; m = 1 - j; a = i; }
+            else if (j > N) { s = SIDE_T; m = j - N; a = i; }
+            if (s >= 0 && !(a >= (m == 1 ? 2 : 1) && a <= (m == 1 ? N - 1 : N))) s = -1;
+            if (s < 0) {
+                if (i < 1) { s = SIDE_L; m = 1 - i; a = j; }
+                else if (i > N) { s = SIDE_R; m = i - N; a = j; }
+                if (s >= 0 && !(a >= (m == 1 ? 2 : 1) && a <= (m == 1 ? N - 1 : N))) s = -1;
+            }
+            if (s >= 0) {
+                const int K = kt[(m - 1) * ni + a + 1];
+                v = W(-1, a, m) * X(s, m, K - 1) + W(0, a, m) * X(s, m, K) + W(1, a, m) * X(s, m, K + 1) +
+                    W(2, a, m) * X(s, m, K + 2);
+            } else {
+                // a special point of the corner (ist, jst) with directions (idir, jdir)
+                const int idir = i <= 1 ? 1 : -1, jdir = j <= 1 ? 1 : -1;
+                const int ist = idir > 0 ? 0 : N + 1, jst = jdir > 0 ? 0 : N + 1;
+                const int li = (i - ist) * idir, lj = (j - jst) * jdir;
+                auto FC = [&](int x, int y) { return pf(ist + idir * x, jst + jdir * y); };
+                auto PW = [&](int k, int a2, int m2) { return idir > 0 ? W(k, a2, m2) : W(1 - k, N + 1 - a2, m2); };
+                const double z0 = PW(0, 1, 1), z1 = PW(1, 1, 1), z2 = PW(2, 1, 1);
+                const double zw = PW(-1, 1, 1), zw2 = zw * zw, zw3 = zw2 * zw;
+                if (li == 0 && lj == 1) {
+                    const double zx = z0 * FC(0, 1) + z1 * FC(0, 2) + z2 * FC(0, 3);
+                    const double zy = z0 * FC(1, 0) + z1 * FC(1, -1) + z2 * FC(1, -2);
+                    const double zz = z0 * FC(1, 1) + z1 * FC(2, 1) + z2 * FC(3, 1);
+                    v = (zx + zw * zy + zw2 * zz) / (1 - zw3);
+                } else if (li == 1 && lj == 0) {
+                    const double zx = z0 * FC(1, 0) + z1 * FC(2, 0) + z2 * FC(3, 0);
+                    const double zy = z0 * FC(0, 1) + z1 * FC(-1, 1) + z2 * FC(-2, 1);
+                    const double zz = z0 * FC(1, 1) + z1 * FC(1, 2) + z2 * FC(1, 3);
+                    v = (zx + zw * zy + zw2 * zz) / (1 - zw3);
+                } else if (li == 0 && lj == 0) {
+                    double zx = z0 * FC(0, 1) + z1 * FC(0, 2) + z2 * FC(0, 3);
+                    double zy = z0 * FC(1, 0) + z1 * FC(1, -1) + z2 * FC(1, -2);
+                    double zz = z0 * FC(1, 1) + z1 * FC(2, 1) + z2 * FC(3, 1);
+                    const double zfy1 = (zy + zw * zz + zw2 * zx) / (1 - zw3);
+                    zx = z0 * FC(1, 0) + z1 * FC(2, 0) + z2 * FC(3, 0);
+                    zy = z0 * FC(0, 1) + z1 * FC(-1, 1) + z2 * FC(-2, 1);
+                    zz = z0 * FC(1, 1) + z1 * FC(1, 2) + z2 * FC(1, 3);
+                    const double zfy2 = (zy + zw * zz + zw2 * zx) / (1 - zw3);
+                    const double zff1 = PW(-1, 1, 2) * FC(2, 0) + PW(0, 1, 2) * FC(2, -1) + PW(1, 1, 2) * FC(2, -2) +
+                                        PW(2, 1, 2) * FC(2, -3);
+                    const double zff2 = PW(-1, 1, 2) * FC(0, 2) + PW(0, 1, 2) * FC(-1, 2) + PW(1, 1, 2) * FC(-2, 2) +
+                                        PW(2, 1, 2) * FC(-3, 2);
+                    v = 0.5 * (PW(-1, 0, 1) * zff1 + PW(0, 0, 1) * zfy1 + PW(1, 0, 1) * FC(0, 1) + PW(2, 0, 1) * FC(0, 2) +
+                               PW(-1, 0, 1) * zff2 + PW(0, 0, 1) * zfy2 + PW(1, 0, 1) * FC(1, 0) + PW(2, 0, 1) * FC(2, 0));
+                } else {
+                    const double zff1 = PW(-1, 2, 1) * FC(1, 0) + PW(0, 2, 1) * FC(1, -1) + PW(1, 2, 1) * FC(1, -2) +
+                                        PW(2, 2, 1) * FC(1, -3);
+                    const double zff2 = PW(-1, 2, 1) * FC(0, 1) + PW(0, 2, 1) * FC(-1, 1) + PW(1, 2, 1) * FC(-2, 1) +
+                                        PW(2, 2, 1) * FC(-3, 1);
+                    if (li == -1 && lj == 0) {
+                        v = PW(-1, 0, 2) * zff1 + PW(0, 0, 2) * FC(-1, 1) + PW(1, 0, 2) * FC(-1, 2) + PW(2, 0, 2) * FC(-1, 3);
+                    } else if (li == 0 && lj == -1) {
+                        v = PW(-1, 0, 2) * zff2 + PW(0, 0, 2) * FC(1, -1) + PW(1, 0, 2) * FC(2, -1) + PW(2, 0, 2) * FC(3, -1);
+                    } else {
+                        const double zff11 = PW(-1, 2, 2) * FC(2, -1) + PW(0, 2, 2) * FC(2, -2) + PW(1, 2, 2) * FC(2, -3) +
+                                             PW(2, 2, 2) * FC(2, -4);
+                        const double zff22 = PW(-1, 2, 2) * FC(-1, 2) + PW(0, 2, 2) * FC(-2, 2) + PW(1, 2, 2) * FC(-3, 2) +
+                                             PW(2, 2, 2) * FC(-4, 2);
+                        v = 0.5 * (PW(-1, -1, 2) * zff11 + PW(0, -1, 2) * zff1 + PW(1, -1, 2) * FC(-1, 1) +
+                                   PW(2, -1, 2) * FC(-1, 2) + PW(-1, -1, 2) * zff22 + PW(0, -1, 2) * zff2 +
+                                   PW(1, -1, 2) * FC(1, -1) + PW(2, -1, 2) * FC(2, -1));
+                    }
+                }
+            }
+        }
+        ext[q] = v;
+    }
+}
+
+// Layout of the curl regrid's tables: ints idx (3 per point), kt (2 (N+4)); doubles w (8
+// per point), wt (4 per kt entry), the extended panels, the output.
+struct LatlonOLayout {
+    size_t np, nk, next;
+    size_t i_kt() const { return 3 * np; }
+    size_t ints() const { return 3 * np + nk; }
+    size_t d_wt() const { return 8 * np; }
+    size_t d_ext() const { return d_wt() + 4 * nk; }
+    size_t d_out() const { return d_ext() + next; }
+    size_t doubles() const { return d_out() + np; }
+};
+static LatlonOLayout latlon_o_layout(int N, int nlat, int nlon)
+{
+    LatlonOLayout L;
+    L.np = (size_t)nlat * nlon;
+    L.nk = (size_t)2 * llo_pitch(N);
+    L.next = (size_t)NPAN * llo_pitch(N) * llo_pitch(N);
+    return L;
+}
+
+// Point location and cubic weights on the cell-centre mesh (shift 1/2:
+// init_interpolation, latlon_regrid_mod.f90:286-336, on mesh_o) and the ECS_O halo
+// weights, built on the host in FP64.
+static int ensure_latlon_o(swe_ctx *c, int nlat, int nlon)
+{
+    if (c->llo_i && c->llo_nlat == nlat && c->llo_nlon == nlon) return SWE_OK;
+    cudaFree(c->llo_i); cudaFree(c->llo_d);
+    c->llo_i = nullptr; c->llo_d = nullptr; c->llo_nlat = c->llo_nlon = 0;
+    const int N = c->cfg.N;
+    const LatlonOLayout Lo = latlon_o_layout(N, nlat, nlon);
+    std::vector<int> hi(Lo.ints(), 0);
+    std::vector<double> hd(Lo.d_ext(), 0.0);
+    const double pi = 3.141592653589793238462643383279502884;
+    const double hx = 0.5 * pi / N, a0 = -0.25 * pi;
+    for (int j = 1; j <= nlat; j++) {
+        const double phi = -0.5 * pi + (j - 1) * pi / (nlat - 1.0);
+        for (int i = 1; i <= nlon; i++) {
+            const double lam = (i - 1) * 2.0 * pi / nlon;
+            const double r[3] = {std::cos(phi) * std::cos(lam), std::cos(phi) * std::sin(lam), std::sin(phi)};
+            int t;
+            double alpha, beta;
+            cart_to_native(r, t, alpha, beta);
+            double zdx = (alpha - a0) / hx + 1 - 0.5, zdy = (beta - a0) / hx + 1 - 0.5;
+            const int xi = (int)zdx, yi = (int)zdy;
+            zdx = zdx - xi;
+            zdy = zdy - yi;
+            // the stencil (cells xi-1 .. xi+2) stays inside the extended panel
+            if (t < 0 || t >= NPAN || xi < 0 || xi > N || yi < 0 || yi > N)
+                return fail(c, SWE_EINVAL, "lat-lon point (%d, %d) outside the cube panels", i, j);
+            const size_t q = (size_t)(j - 1) * nlon + (i - 1);
+            hi[3 * q] = t; hi[3 * q + 1] = xi; hi[3 * q + 2] = yi;
+            double *wx = &hd[8 * q], *wy = wx + 4;
+            wx[0] = -zdx * (zdx - 1.0) * (zdx - 2.0) / 6.0;
+            wx[1] = (zdx + 1.0) * (zdx - 1.0) * (zdx - 2.0) / 2.0;
+            wx[2] = -(zdx + 1.0) * zdx * (zdx - 2.0) / 2.0;
+            wx[3] = (zdx + 1.0) * zdx * (zdx - 1.0) / 6.0;
+            wy[0] = -zdy * (zdy - 1.0) * (zdy - 2.0) / 6.0;
+            wy[1] = (zdy + 1.0) * (zdy - 1.0) * (zdy - 2.0) / 2.0;
+            wy[2] = -(zdy + 1.0) * zdy * (zdy - 2.0) / 2.0;
+            wy[3] = (zdy + 1.0) * zdy * (zdy - 1.0) / 6.0;
+        }
+    }
+    const int ni = llo_pitch(N);
+    for (int m = 1; m <= 2; m++)
+        for (int a = -1; a <= N + 2; a++) {
+            const size_t row = (size_t)(m - 1) * ni + a + 1;
+            halo_o_weights(hx, a, m, &hd[Lo.d_wt() + 4 * row], hi[Lo.i_kt() + row]);
+            // the rows' stencils read the neighbour's cells 1 .. N
+            const int K = hi[Lo.i_kt() + row];
+            if (a >= (m == 1 ? 2 : 1) && a <= (m == 1 ? N - 1 : N) && (K - 1 < 1 || K + 2 > N))
+                return fail(c, SWE_EINVAL, "ECS_O halo: line %d of row %d reads outside the neighbour", a, m);
+        }
+    if (cudaMalloc(&c->llo_i, hi.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->llo_d, Lo.doubles() * sizeof(double)) != cudaSuccess) {
+        cudaFree(c->llo_i); c->llo_i = nullptr; c->llo_d = nullptr;
+        return fail(c, SWE_ENOMEM, "lat-lon curl regrid allocation failed");
+    }
+    CU(c, cudaMemcpy(c->llo_i, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(c, cudaMemcpy(c->llo_d, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->llo_nlat = nlat;
+    c->llo_nlon = nlon;
+    return SWE_OK;
+}
+
 // The divergence of the wind of every member (div_ch_sbp_sat_<order>_proj of the
 // contravariant components, the operator the diagnostics' div_operator_name names)
 // into field 0 of the scratch box ya: the linear operator's stage kernel in mode 0
@@ -2509,11 +2972,35 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
 {
     if (!c || !vec || vec->ctx != c || !out || member < 0 || member >= c->cfg.n_members) return SWE_EINVAL;
     CHSWE_NOT_ON_C(c, "swe_regrid_latlon");
-    if (field != 0 && field != 1)
-        return fail(c, SWE_EINVAL, "lat-lon regrid: field 0 (h) or 1 (the divergence of the wind)");
-    if (field == 1 && c->ah) return fail(c, SWE_EINVAL, "lat-lon regrid of the divergence: built for Ch");
+    if (field < 0 || field > 2)
+        return fail(c, SWE_EINVAL, "lat-lon regrid: field 0 (h), 1 (the divergence of the wind) or 2 (its curl)");
+    if (field >= 1 && c->ah) return fail(c, SWE_EINVAL, "lat-lon regrid of the divergence or the curl: built for Ch");
     if (nlat < 2 || nlon < 1 || (int64_t)nlat * nlon > (1 << 28))
         return fail(c, SWE_EINVAL, "lat-lon regrid: bad grid %d x %d", nlat, nlon);
+    if (field == 2) {
+        // output_curl: the curl on the cell centres, its ECS_O halo, the cubic stencils
+        int rc = ensure_otab(c);
+        if (rc == SWE_OK) rc = ensure_latlon_o(c, nlat, nlon);
+        if (rc != SWE_OK) return rc;
+        const int N = c->cfg.N;
+        const LatlonOLayout Lo = latlon_o_layout(N, nlat, nlon);
+        const int64_t np = (int64_t)Lo.np;
+        const size_t mo = (size_t)member * c->dims.ms;
+        const double hx = 0.5 * 3.141592653589793238462643383279502884 / N;
+        double *dcurl = c->otab + 7 * (size_t)c->dims.ps;
+        double *ext = c->llo_d + Lo.d_ext(), *dout = c->llo_d + Lo.d_out();
+        if (c->elem == 8) launch_curl<double>(c, (const double *)vec->d + mo, c->dims, hx, dcurl);
+        else launch_curl<float>(c, (const float *)vec->d + mo, c->dims, hx, dcurl);
+        const dim3 b(256), g1((unsigned)std::min<int64_t>(((int64_t)Lo.next + 255) / 256, 8192)),
+            g2((unsigned)std::min<int64_t>((np + 255) / 256, 8192));
+        k_ecs_o_ext<<<g1, b, 0, c->stream>>>(dcurl, N, c->llo_i + Lo.i_kt(), c->llo_d + Lo.d_wt(), ext);
+        k_latlon<<<g2, b, 0, c->stream>>>(ext, c->llo_i, c->llo_d, llo_pitch(N), np, dout);
+        c->launches += 3;
+        CU_LAUNCHED(c);
+        CU(c, cudaMemcpyAsync(out, dout, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CU(c, cudaStreamSynchronize(c->stream));
+        return SWE_OK;
+    }
     int rc = ensure_latlon(c, nlat, nlon);
     if (rc != SWE_OK) return rc;
     const int N = c->cfg.N;
@@ -2533,7 +3020,7 @@ extern "C" int swe_regrid_latlon(swe_ctx *c, const swe_stvec *vec, int member, i
     }
     if (c->elem == 8) k_ecs_xy_ext<double><<<g1, b, 0, c->stream>>>((const double *)src + mo, c->dims, kt, wt, ext);
     else k_ecs_xy_ext<float><<<g1, b, 0, c->stream>>>((const float *)src + mo, c->dims, kt, wt, ext);
-    k_latlon<<<g2, b, 0, c->stream>>>(ext, c->ll_i, c->ll_d, N, np, dout);
+    k_latlon<<<g2, b, 0, c->stream>>>(ext, c->ll_i, c->ll_d, ll_pitch(N), np, dout);
     c->launches += 2;
     CU_LAUNCHED(c);
     CU(c, cudaMemcpyAsync(out, dout, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -243,15 +243,16 @@ constexpr int EDGE_THREADS = 288; // 8 warps of raw stencils + 1 warp for the th
 // warp 8 the copy of the third panel at the two cube corners.  Phase 2 combines
 // the copies from shared memory.  Copies are stored by direction (x-neighbour
 // across L/R, y-neighbour across B/T).
+// Chunk ch of nch along side s of panel t (ts = 4 t + s) of member mem.
 template <class T, int ORD>
-__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, const T *__restrict__ ESd,
-                                                        T *__restrict__ E, Dims d, MetricView<T> m,
-                                                        const double *__restrict__ dtm)
+__device__ __forceinline__ void edge_chunk(unsigned ch, unsigned nch, unsigned ts, unsigned mem, const T *__restrict__ ES,
+                                           const T *__restrict__ ESd, T *__restrict__ E, const Dims &d,
+                                           const MetricView<T> &m, const double *__restrict__ dtm)
 {
     __shared__ T raw[3][4][EDGE_CHUNK];   // [own, x-neighbour, y-neighbour][quantity][vertex]
     const int N = d.N, n = N + 1;
-    const int t = blockIdx.y >> 2, s = blockIdx.y & 3, mem = blockIdx.z;
-    const int a0 = 1 + (blockIdx.x * n) / gridDim.x, a1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
+    const int t = ts >> 2, s = ts & 3;
+    const int a0 = 1 + (ch * n) / nch, a1 = 1 + ((ch + 1) * n) / nch;
     if (member_frozen(dtm, mem)) return;
     // Coriolis parts (q 0, 1) from the ut/vt strips, divergence parts (q 2, 3) from
     // the strips of the field whose divergence is taken (ut/vt, or the mass flux)
@@ -343,6 +344,14 @@ __global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES,
     e[0] = sup;
     e[1] = svp;
     e[2] = sdiv;
+}
+
+template <class T, int ORD>
+__global__ void __launch_bounds__(EDGE_THREADS) k_edge(const T *__restrict__ ES, const T *__restrict__ ESd,
+                                                        T *__restrict__ E, Dims d, MetricView<T> m,
+                                                        const double *__restrict__ dtm)
+{
+    edge_chunk<T, ORD>(blockIdx.x, gridDim.x, blockIdx.y, blockIdx.z, ES, ESd, E, d, m, dtm);
 }
 
 // Synchronised (up, vp, div) of panel-boundary vertex (k, l) from the edge buffer.

@@ -133,6 +133,44 @@ struct FusedTU {
     static cudaError_t upload_tables(const Link *links);
 };
 
+// One context of a group: its dimensions, metric, the state it advances and its
+// scratch (the buffers of its own RK4 steps), and where its blocks sit in the grids.
+template <class T>
+struct GroupEntry {
+    Dims d;
+    MetricView<T> m;
+    T *v;                  // the state (RK4 v0)
+    T *ya, *yb;            // stage inputs / outputs
+    T *acc, *cmp;          // RK4 accumulator; FP32 compensation (null in FP64)
+    T *w, *es, *e;         // contravariant components, edge strips, synchronised edge values
+    const double *Hm;      // per-member mean depth
+    const double *dtm;     // per-member time step (0 freezes a member)
+    unsigned gx, gy;       // stage tiles per panel direction
+    unsigned nch;          // edge chunks per panel side
+    unsigned tile0, edge0; // first flat block of this context in the tile and edge grids
+};
+
+constexpr int GROUP_MAX = 8;
+
+template <class T>
+struct GroupTable {
+    int n;
+    GroupEntry<T> e[GROUP_MAX];
+};
+
+// Group launches (swe_group.cuh) of precision T: the configurations (tile, blocks
+// per SM, runs) they are built for, and one RK4 step of every context in the table
+// as twelve launches (contravariant components, edge sync and stage, per stage).
+#define CHSWE_GROUP_CFGS(X) X(17, 4, 0) X(25, 3, 0) X(33, 2, 0)
+
+template <class T>
+struct GroupTU {
+    static cudaError_t optin();
+    // false: (tm, occ, runs) is not a built group configuration; nothing was launched
+    static bool rk4_step(int tm, int occ, int runs, const GroupTable<T> &g, unsigned tiles, unsigned edges,
+                         cudaStream_t st);
+};
+
 // Tiles of the fused stage: ceil((N+1) / FUSED_TW) columns and ceil((N+1) / th) rows
 // of balanced tiles; the passes' ranges assume tiles of at least 13 x 9 points
 // whenever a panel holds more than one.

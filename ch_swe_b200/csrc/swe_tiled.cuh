@@ -54,12 +54,20 @@ struct Tile {
                   IT_RT = (TM * ((TM + RBT - 1) / RBT) + STAGE_THREADS - 1) / STAGE_THREADS;                \
     (void)RW
 
-__device__ __forceinline__ void tile_range(int n, int &i0, int &i1, int &j0, int &j1)
+// The block a tile kernel works on: tile (x, y) of gx x gy tiles per panel, z = member *
+// 6 + panel.  A plain launch takes it from its grid; a group launch (one grid over the
+// states of several contexts) decodes it from its flat block index.
+struct Blk {
+    unsigned x, y, z, gx, gy;
+};
+__device__ __forceinline__ Blk grid_blk() { return Blk{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y}; }
+
+__device__ __forceinline__ void tile_range(const Blk &b, int n, int &i0, int &i1, int &j0, int &j1)
 {
-    i0 = 1 + (blockIdx.x * n) / gridDim.x;
-    i1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
-    j0 = 1 + (blockIdx.y * n) / gridDim.y;
-    j1 = 1 + ((blockIdx.y + 1) * n) / gridDim.y;
+    i0 = 1 + (b.x * n) / b.gx;
+    i1 = 1 + ((b.x + 1) * n) / b.gx;
+    j0 = 1 + (b.y * n) / b.gy;
+    j1 = 1 + ((b.y + 1) * n) / b.gy;
 }
 
 // q -> (a, b) with q = a * w + b, 0 <= b < w (q < 2^16, w <= 64): exact with a float reciprocal.
@@ -147,9 +155,9 @@ struct Co2Layout {
 // OCC: resident blocks per SM the register allocation is capped for; RUNS: stencil
 // runs of several outputs per thread (both autotuned).
 template <class T, int TM, int OCC, bool RUNS, int ORD>
-__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
-                                                                 T *__restrict__ ES, Dims d, MetricView<T> m,
-                                                                 const double *__restrict__ dtm)
+__device__ __forceinline__ void co2contra_tile(const Blk &bk, const T *__restrict__ Y, T *__restrict__ W,
+                                               T *__restrict__ ES, const Dims &d, const MetricView<T> &m,
+                                               const double *__restrict__ dtm)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     using L = Co2Layout<T, TM>;
@@ -158,10 +166,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
-    tile_range(n, i0, i1, j0, j1);
+    tile_range(bk, n, i0, i1, j0, j1);
     const int tw = i1 - i0, th = j1 - j0, w5 = tw + 5, h5 = th + 5;
     const float iw5 = 1.0f / (float)w5, ih5 = 1.0f / (float)h5, iw = 1.0f / (float)tw, ih = 1.0f / (float)th;
-    const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
+    const int t = bk.z % NPAN, mem = bk.z / NPAN;
     if (member_frozen(dtm, mem)) return;
     const T *y = Y + mem * d.ms + t * d.ps;
     T *w = W + mem * d.ms + t * d.ps;
@@ -360,6 +368,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__res
     }
 }
 
+template <class T, int TM, int OCC, bool RUNS, int ORD>
+__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_co2contra(const T *__restrict__ Y, T *__restrict__ W,
+                                                                 T *__restrict__ ES, Dims d, MetricView<T> m,
+                                                                 const double *__restrict__ dtm)
+{
+    co2contra_tile<T, TM, OCC, RUNS, ORD>(grid_blk(), Y, W, ES, d, m, dtm);
+}
+
 // ---------------------------------------------------------------------------
 // fused stage: tendency of the linear operator + RK4 update
 // ---------------------------------------------------------------------------
@@ -382,9 +398,9 @@ __device__ __forceinline__ bool on_boundary(int k, int l, int n) { return k == 1
 // ADV: the advective operator (divergence of the mass flux a.F, tendencies a.A,
 // gradient of the pre-averaging boundary h a.HB); false: the linear operator.
 template <class T, int TM, int OCC, int MODE, bool ADV, bool RUNS, int ORD>
-__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
-                                                          const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
-                                                          Dims d, MetricView<T> m, StageArgs a)
+__device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ Yin, const T *__restrict__ Wc,
+                                           const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP, const Dims &d,
+                                           const MetricView<T> &m, const StageArgs &a)
 {
     using namespace sbp;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -394,9 +410,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
     T *sm = reinterpret_cast<T *>(smraw);
     const int N = d.N, n = N + 1, P = d.P;
     int i0, i1, j0, j1;
-    tile_range(n, i0, i1, j0, j1);
+    tile_range(bk, n, i0, i1, j0, j1);
     const int tw = i1 - i0, th = j1 - j0;
-    const int t = blockIdx.z % NPAN, mem = blockIdx.z / NPAN;
+    const int t = bk.z % NPAN, mem = bk.z / NPAN;
     if (member_frozen(a.dtm, mem)) return;
     const int64_t mo = mem * d.ms;
     const T *y = Yin + mo;                 // member base (the h halos read the other panels)
@@ -889,6 +905,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restric
             }
         }
     }
+}
+
+template <class T, int TM, int OCC, int MODE, bool ADV, bool RUNS, int ORD>
+__global__ void __launch_bounds__(STAGE_THREADS, OCC) k_stage(const T *__restrict__ Yin, const T *__restrict__ Wc,
+                                                          const T *__restrict__ E, T *V0, T *Y1, T *ACC, T *CMP,
+                                                          Dims d, MetricView<T> m, StageArgs a)
+{
+    stage_tile<T, TM, OCC, MODE, ADV, RUNS, ORD>(grid_blk(), Yin, Wc, E, V0, Y1, ACC, CMP, d, m, a);
 }
 
 }  // namespace chswe

@@ -106,6 +106,16 @@ class LatlonOutputer:
               self.domain.ctx, "swe_regrid_latlon (div)")
         return out
 
+    def regrid_curl(self, state, member: int = 0) -> np.ndarray:
+        """The curl of the covariant wind (the curl.dat field of output_curl:
+        curl_ch_sbp_sat_<order> on the cell centres, regridded from the ECS_O halo) on
+        the lat-lon grid."""
+        out = np.empty((self.nlat, self.nlon))
+        check(_lib.load().swe_regrid_latlon(self.domain.ctx, state.handle, int(member), 2, self.nlat, self.nlon,
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self.domain.ctx, "swe_regrid_latlon (curl)")
+        return out
+
 
 class LatlonVecOutputer:
     """latlon_vec_outputer_t for the covariant Ch wind (latlon_outputer_mod.f90:55-85): the

@@ -15,7 +15,12 @@ Continuous batching:
 - between ticks, finished requests leave (their state is downloaded) and queued
   requests of that pool are uploaded into the free slots;
 - pools run on separate streams, so the work of different cube sizes and
-  precisions overlaps on the device.
+  precisions overlaps on the device;
+- with grouped=True, the linear pools of one precision share one kernel
+  configuration and tick together as a group (swe_group_rk4_steps_members): one
+  grid per kernel covers every cube size of the group, twelve launches per RK4 step
+  for all of them; the tick is as long as the shortest remaining integration of the
+  group.
 
 Admission by HBM budget: a pool is created when a request needs one and its
 slots fit in the budget that other pools leave free (idle empty pools are
@@ -76,6 +81,7 @@ class Request:
     admitted: float | None = None
     finished: float | None = None
     pool_tile: int | None = None
+    pool_cfg: tuple | None = None
     result: tuple | None = None
 
     _ic: tuple | None = None
@@ -132,17 +138,27 @@ def _operator(dom, operator: str):
     return create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": 1000.0}, dom)
 
 
-class Pool:
-    """Member slots of one (operator, N, precision): one context on its own stream."""
+# Kernel configuration of grouped pools (a configuration with a group launch).
+GROUP_CONFIG = {"fp32": (25, 3, 0), "fp64": (25, 3, 0)}
 
-    def __init__(self, N: int, precision: str, capacity: int, torch, tile=None, operator: str = "linear"):
+
+class Pool:
+    """Member slots of one (operator, N, precision): one context on its own stream.
+    kernel_config: a fixed (tile, blocks per SM, runs) instead of the tile or the
+    autotuner's choice."""
+
+    def __init__(self, N: int, precision: str, capacity: int, torch, tile=None, operator: str = "linear",
+                 kernel_config=None):
         from .swm import create_domain, create_stvec_swm, create_timescheme
         self.N, self.precision, self.capacity, self.operator = N, precision, capacity, operator
         self.torch = torch
         self.stream = torch.cuda.Stream()
         self.dom = create_domain(N, precision=precision, n_members=capacity, operator=operator)
         self.dom.set_stream(self.stream.cuda_stream)
-        if tile is None:
+        self.grouped = kernel_config is not None
+        if kernel_config is not None:
+            self.dom.kernel_config = kernel_config
+        elif tile is None:
             with torch.cuda.stream(self.stream):
                 self.dom.autotune(nreps=4)
         else:
@@ -179,15 +195,24 @@ class Pool:
         self.remaining[k] = req.nsteps
         req.admitted = now
         req.pool_tile = self.dom.tile
+        req.pool_cfg = self.dom.kernel_config
+
+    def active(self):
+        return [k for k, r in enumerate(self.slots) if r is not None and self.remaining[k] > 0]
+
+    def tick_dts(self):
+        """Per-slot time steps of the next tick (0: a free or finished slot)."""
+        dts = np.zeros(self.capacity)
+        for k in self.active():
+            dts[k] = self.slots[k].dt
+        return dts
 
     def launch_tick(self, max_tick: int):
-        active = [k for k, r in enumerate(self.slots) if r is not None and self.remaining[k] > 0]
+        active = self.active()
         if not active:
             return False
         L = min(max_tick, min(self.remaining[k] for k in active))
-        dts = np.zeros(self.capacity)
-        for k in active:
-            dts[k] = self.slots[k].dt
+        dts = self.tick_dts()
         with self.torch.cuda.stream(self.stream):
             self.rk.steps_members(self.state, self.op, dts, L)
             self.event = self.torch.cuda.Event()
@@ -235,15 +260,20 @@ class ServeStats:
 
 
 class Server:
-    def __init__(self, hbm_budget_bytes: int = 16 << 30, max_tick: int = 16, max_slots=None, tiles=None):
+    def __init__(self, hbm_budget_bytes: int = 16 << 30, max_tick: int = 16, max_slots=None, tiles=None,
+                 grouped: bool = False):
         import torch
         self.torch = torch
         self.budget = int(hbm_budget_bytes)
         self.max_tick = int(max_tick)
         self.max_slots = dict(MAX_SLOTS if max_slots is None else max_slots)
         self.tiles = dict(tiles or {})
+        self.grouped = bool(grouped)
         self.pools: dict[tuple, Pool] = {}
+        # precision -> (the grouped pools' keys, DomainGroup)
+        self.groups: dict[str, tuple] = {}
         self.peak = 0
+        self.group_ticks = 0
 
     def used_bytes(self) -> int:
         return sum(p.bytes for p in self.pools.values())
@@ -280,19 +310,59 @@ class Server:
         want = self.max_slots.get(req.N, 4)
         free = self.budget - self.used_bytes()
         if free < per:
-            # release idle, empty pools of other keys
+            # release idle, empty pools of other keys (and the groups that hold them)
             for k2, p in list(self.pools.items()):
-                if not p.busy and p.occupied == 0:
+                if not p.busy and p.occupied == 0 and not self._group_busy(k2):
+                    self._drop_group(k2[1])
                     p.destroy()
                     del self.pools[k2]
             free = self.budget - self.used_bytes()
         cap = min(want, free // per)
         if cap < 1:
             return None
-        pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key), operator=req.operator)
+        cfg = GROUP_CONFIG[req.precision] if self.grouped and req.operator == "linear" else None
+        pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key), operator=req.operator,
+                    kernel_config=cfg)
         self.pools[key] = pool
         self.peak = max(self.peak, self.used_bytes())
         return pool
+
+    def _grouped_pools(self, precision: str):
+        return sorted((k for k, p in self.pools.items() if p.grouped and k[1] == precision), key=lambda k: k[0])
+
+    def _group_busy(self, key) -> bool:
+        return any(self.pools[k].busy for k in self._grouped_pools(key[1])) if self.pools[key].grouped else False
+
+    def _drop_group(self, precision: str):
+        g = self.groups.pop(precision, None)
+        if g is not None:
+            g[1].destroy()
+
+    def _group_tick(self, precision: str) -> bool:
+        """One tick of every grouped pool of `precision` as one group launch (all of
+        them idle)."""
+        from .swm import create_group
+        keys = self._grouped_pools(precision)
+        pools = [self.pools[k] for k in keys]
+        if not pools or any(p.busy for p in pools):
+            return False
+        active = [(p, k) for p in pools for k in p.active()]
+        if not active:
+            return False
+        L = min(self.max_tick, min(p.remaining[k] for p, k in active))
+        g = self.groups.get(precision)
+        if g is None or g[0] != keys:
+            self._drop_group(precision)
+            g = (keys, create_group([p.dom for p in pools]))
+            self.groups[precision] = g
+        g[1].steps_members([p.state for p in pools], [p.tick_dts() for p in pools], L)
+        ev = self.torch.cuda.Event()
+        ev.record(pools[0].stream)
+        for p in pools:
+            p.event = ev
+            p.tick_len = L
+        self.group_ticks += 1
+        return True
 
     def run(self, requests, realtime: bool = True) -> ServeStats:
         """Serve `requests` (arrival times in seconds from the start); realtime=False
@@ -329,7 +399,10 @@ class Server:
                     waiting.append(r)
             queue = waiting
             for p in self.pools.values():
-                if not p.busy and p.launch_tick(self.max_tick):
+                if not p.grouped and not p.busy and p.launch_tick(self.max_tick):
+                    progressed = True
+            for prec in ("fp32", "fp64"):
+                if self._group_tick(prec):
                     progressed = True
             if not progressed:
                 time.sleep(20e-6)
@@ -342,22 +415,27 @@ class Server:
             n=len(done), makespan_s=makespan, p50_ms=float(np.percentile(lat, 50)),
             p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
             requests_per_s=len(done) / makespan, cell_updates_per_s=cells / makespan,
-            pools={f"{k[2]}/C{k[0]}/{k[1]}": {"slots": p.capacity, "tile": p.dom.tile} for k, p in self.pools.items()},
+            pools={f"{k[2]}/C{k[0]}/{k[1]}": {"slots": p.capacity, "kernel_config": list(p.dom.kernel_config),
+                                              "grouped": p.grouped} for k, p in self.pools.items()},
             peak_bytes=self.peak,
             service_p50_ms=float(np.percentile(svc, 50)), service_p99_ms=float(np.percentile(svc, 99)),
             wait_p50_ms=float(np.percentile(wait, 50)), wait_p99_ms=float(np.percentile(wait, 99)))
 
     def close(self):
+        for prec in list(self.groups):
+            self._drop_group(prec)
         for p in self.pools.values():
             p.destroy()
         self.pools.clear()
 
 
-def run_alone(req: Request, tile=None):
+def run_alone(req: Request, tile=None, kernel_config=None):
     """The same integration in its own single-member context (the comparison arm)."""
     from .swm import create_domain, create_stvec_swm, create_timescheme
     dom = create_domain(req.N, precision=req.precision, operator=req.operator)
-    if tile is not None:
+    if kernel_config is not None:
+        dom.kernel_config = kernel_config
+    elif tile is not None:
         dom.tile = tile
     op = _operator(dom, req.operator)
     if req.operator == "linear":

@@ -509,6 +509,56 @@ class Rk4:
               operator.domain.ctx, "rk4 steps (members)")
 
 
+class DomainGroup:
+    """The RK4 steps of several domains (cube sizes and member counts of their own, one
+    precision, the linear operator on Ch in SBP 4-2, one split kernel configuration)
+    as one grid per kernel: twelve launches per step for the whole group, on the first
+    domain's stream.  Each domain gets the bits its own Rk4.steps_members gives with
+    the same configuration."""
+
+    def __init__(self, domains):
+        self.domains = list(domains)
+        arr = (ctypes.c_void_p * len(self.domains))(*[d.ctx for d in self.domains])
+        h = ctypes.c_void_p()
+        check(_lib.load().swe_group_create(arr, len(self.domains), ctypes.byref(h)), self.domains[0].ctx,
+              "group create")
+        self.handle = h
+
+    def _check(self, rc: int, what: str):
+        if rc != _lib.SWE_OK:
+            detail = _lib.load().swe_group_last_error(self.handle)
+            raise SweError(f"{what}: {_lib.ERRORS.get(rc, rc)}: {detail.decode() if detail else ''}")
+
+    def steps_members(self, states, dts, nsteps: int):
+        """nsteps RK4 steps of states[k] (of domain k) with the per-member time steps
+        dts[k]; a time step of 0 freezes a member."""
+        if len(states) != len(self.domains) or len(dts) != len(self.domains):
+            raise ValueError(f"need {len(self.domains)} states and time-step arrays")
+        keep = [np.ascontiguousarray(x, dtype=np.float64) for x in dts]
+        for d, x in zip(self.domains, keep):
+            if x.shape != (d.n_members,):
+                raise ValueError(f"need {d.n_members} time steps, got shape {x.shape}")
+        sv = (ctypes.c_void_p * len(states))(*[st.handle for st in states])
+        dv = (_lib._dp * len(keep))(*[dptr(x) for x in keep])
+        self._check(_lib.load().swe_group_rk4_steps_members(self.handle, sv, dv, int(nsteps)), "group steps")
+
+    def synchronize(self):
+        self._check(_lib.load().swe_group_synchronize(self.handle), "group synchronize")
+
+    @property
+    def launches(self) -> int:
+        return int(_lib.load().swe_group_launch_count(self.handle))
+
+    def destroy(self):
+        if self.handle:
+            _lib.load().swe_group_destroy(self.handle)
+            self.handle = None
+
+
+def create_group(domains) -> DomainGroup:
+    return DomainGroup(domains)
+
+
 def create_timescheme(state: StvecSwm, name: str):
     if name != "rk4":
         raise ValueError(f"unknown timescheme_name: {name}")

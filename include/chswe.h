@@ -162,6 +162,27 @@ int swe_rk4_steps(swe_ctx *ctx, swe_stvec *v0, double dt, int nsteps);
    reference counterpart: the reference advances one state per timescheme%step
    (src/time_schemes/rk4_mod.f90:20-42). */
 int swe_rk4_steps_members(swe_ctx *ctx, swe_stvec *v0, const double *dt, int nsteps);
+
+/* Groups: the RK4 steps of up to 8 contexts -- cube sizes and member counts of their
+   own, one device and precision, the linear operator on Ch in SBP 4-2, one split
+   kernel configuration (17, 4, 0), (25, 3, 0) or (33, 2, 0) -- launched as one grid
+   per kernel: twelve launches per RK4 step whatever the number of contexts, on the
+   first context's stream, ordered after the work queued on every context's stream
+   and before the work queued there later.  A context advanced in a group gets the
+   bits it gets from swe_rk4_steps_members with the same configuration.  The group
+   uses each context's scratch and per-member time-step buffer: a context takes no
+   other calls while its group's steps may be in flight on another stream, and
+   outlives its group.  No reference counterpart: the reference advances one state per
+   timescheme%step (src/time_schemes/rk4_mod.f90:20-42). */
+typedef struct swe_group swe_group;
+int swe_group_create(swe_ctx *const *ctxs, int n, swe_group **out);
+int swe_group_destroy(swe_group *g);
+/* nsteps RK4 steps of states[k] (of context k) with the per-member time steps dt[k]
+   (n_members values of context k; 0 freezes a member). */
+int swe_group_rk4_steps_members(swe_group *g, swe_stvec *const *states, const double *const *dt, int nsteps);
+int swe_group_synchronize(swe_group *g);
+const char *swe_group_last_error(const swe_group *g);
+long long swe_group_launch_count(const swe_group *g);
 /* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
 int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
 
@@ -196,7 +217,13 @@ int swe_curl(swe_ctx *ctx, const swe_stvec *vec, int member, double *out);
    stencil is summed.  out[nlat][nlon] in FP64, longitude fastest (the reference's
    outputer uses nlat = 2N+1, nlon = 4N).  field 1: the divergence of the wind instead
    (output_div's div.dat: div_ch_sbp_sat_<order>_proj of the contravariant wind,
-   swm_output_diag_mod.f90:92-106; Ch only).  Other fields give SWE_EINVAL.  Synchronous. */
+   swm_output_diag_mod.f90:92-106; Ch only).  field 2: the curl of the covariant wind
+   (output_curl's curl.dat, swm_output_diag_mod.f90:78-90; Ch only): curl_ch_sbp_sat_<order>
+   on the cell centres, its ECS_O halo of width 2 (the o-point exchange, the rows of
+   virtual cells interpolated along the neighbours' grid lines and the six special
+   points of each cube corner: ecs_halo_mod.f90:74-477, ecs_halo_factory_mod.f90:26-68,
+   190-230) and the cubic stencils on the cell-centre mesh (shift 1/2,
+   regrid_factory_mod.f90:285-287).  Other fields give SWE_EINVAL.  Synchronous. */
 int swe_regrid_latlon(swe_ctx *ctx, const swe_stvec *vec, int member, int field, int nlat, int nlon,
                       double *out);
 

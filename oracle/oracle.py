@@ -79,6 +79,7 @@ def lib():
         L.orc_ah_integrals.argtypes = [ctypes.c_void_p] + [_dp] * 5
         L.orc_latlon_vec.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_latlon_xy.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_latlon_o.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
         _lib = L
     return _lib
 
@@ -168,6 +169,20 @@ class Oracle:
         out = np.zeros((nlat, nlon))
         lib().orc_latlon_xy(self._c, _p(np.ascontiguousarray(f, dtype=np.float64)), nlat, nlon, _p(out))
         return out
+
+    def latlon_o(self, f, nlat=None, nlon=None):
+        """Cubic lat-lon regrid of a cell-centre field (6, N, N) on its ECS_O halo of width
+        2 (the curl output of output_curl): shape (nlat, nlon)."""
+        nlat = 2 * self.N + 1 if nlat is None else int(nlat)
+        nlon = 4 * self.N if nlon is None else int(nlon)
+        out = np.zeros((nlat, nlon))
+        lib().orc_latlon_o(self._c, _p(np.ascontiguousarray(f, dtype=np.float64)), nlat, nlon, _p(out))
+        return out
+
+    def latlon_curl(self, u, v, nlat=None, nlon=None):
+        """curl.dat of output_curl: the curl of the covariant Ch wind on the cell centres,
+        regridded to the lat-lon grid."""
+        return self.latlon_o(self.curl(u, v), nlat, nlon)
 
     def latlon_vec(self, u, v, nlat=None, nlon=None):
         """Cubic lat-lon regrid of the covariant Ch wind (latlon_vec_outputer_t): the

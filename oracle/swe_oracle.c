@@ -887,6 +887,11 @@ typedef struct orc_ctx {
     /* energies and enstrophy of swm_output_diag_t: mesh o (cell centres, the Ch q mesh) */
     mesh_t mo;
     double *fo;                  /* Coriolis parameter on o, [t][j][i] */
+    /* lat-lon regrid of an o field (the curl output): the o-point exchange of width 5 and
+       the field with its ECS_O halo, built on first use */
+    int llo;
+    exch_t ex_o5;
+    fld_t o_ll;
     fld_t oDx, oDy, curl, hqu, hqv, ehu, ehv;
     /* Ah staggering (h, u, v all on xy): state, work fields and RK4 stages */
     int ah;
@@ -1010,6 +1015,7 @@ void orc_destroy(orc_ctx *c)
     free(c->fJ2); free(c->fo); free(c->fxy); free(c->qb); free(c->qt); free(c->ql); free(c->qr);
     free(c->hsurf);
     c_free(c);
+    if (c->llo) fld_free(&c->o_ll);
     fld_t *all[] = {&c->h, &c->u, &c->v, &c->du, &c->dv, &c->dh, &c->gx, &c->gy, &c->ut, &c->vt,
                     &c->uq, &c->vq, &c->up, &c->vp, &c->Ju, &c->Jv, &c->Dx, &c->Dy, &c->div,
                     &c->y[0], &c->y[1], &c->y[2], &c->htot, &c->hu, &c->hv, &c->cu, &c->cv, &c->uh,
@@ -2180,6 +2186,171 @@ void orc_latlon_xy(orc_ctx *c, const double *f, int nlat, int nlon, double *out)
     fld_from_packed(b, f);
     ecs_xy_halo(c, b, 2);
     const mesh_t *m = &c->mxy;
+    const double alpha0 = -0.25 * PI_, beta0 = -0.25 * PI_;
+    for (int j = 1; j <= nlat; j++) {
+        const double phi = -0.5 * PI_ + (j - 1) * PI_ / (nlat - 1.0);
+        for (int i = 1; i <= nlon; i++) {
+            const double lam = (i - 1) * 2.0 * PI_ / nlon;
+            const double r[3] = {cos(phi) * cos(lam), cos(phi) * sin(lam), sin(phi)};
+            int t;
+            double alpha, beta;
+            cart_to_native(r, &t, &alpha, &beta);
+            double zdx = (alpha - alpha0) / m->hx + 1 - m->shift_i;
+            double zdy = (beta - beta0) / m->hy + 1 - m->shift_j;
+            const int xi = (int)zdx, yi = (int)zdy;
+            zdx = zdx - xi;
+            zdy = zdy - yi;
+            double wx[4], wy[4];
+            wx[0] = -zdx * (zdx - 1.0) * (zdx - 2.0) / 6.0;
+            wx[1] = (zdx + 1.0) * (zdx - 1.0) * (zdx - 2.0) / 2.0;
+            wx[2] = -(zdx + 1.0) * zdx * (zdx - 2.0) / 2.0;
+            wx[3] = (zdx + 1.0) * zdx * (zdx - 1.0) / 6.0;
+            wy[0] = -zdy * (zdy - 1.0) * (zdy - 2.0) / 6.0;
+            wy[1] = (zdy + 1.0) * (zdy - 1.0) * (zdy - 2.0) / 2.0;
+            wy[2] = -(zdy + 1.0) * zdy * (zdy - 2.0) / 2.0;
+            wy[3] = (zdy + 1.0) * zdy * (zdy - 1.0) / 6.0;
+            double acc = 0.0;
+            for (int q = -1; q <= 2; q++)
+                for (int p = -1; p <= 2; p++) acc = acc + wx[p + 1] * wy[q + 1] * FA(b, t, xi + p, yi + q);
+            out[(size_t)(j - 1) * nlon + (i - 1)] = acc;
+        }
+    }
+}
+
+/* ---- ECS_O scalar halo of width 2 and the lat-lon regrid of an o field ---- */
+
+/* init_halo_interp (ecs_halo_factory_mod.f90:190-230): for the cell-centre line i of a
+   virtual row j beyond the edge, the source face's cell left of the projected point
+   (*ind) and the cubic Lagrange weights w[0..3] on its cells ind-1 .. ind+2. */
+static void halo_o_weights(double dxa, int i, int j, double w[4], int *ind)
+{
+    const double zb = 0.25 * PI_ + (j - 0.5) * dxa;
+    double za = -0.25 * PI_ + (i - 0.5) * dxa;
+    double zx = tan(za);
+    const double zz = tan(zb);
+    zx = zx / zz;
+    za = atan(zx);
+    const int k = (int)floor((za + 0.25 * PI_ - 0.5 * dxa) / dxa) + 1;
+    const double zxi = (za + 0.25 * PI_) / dxa - (k - 0.5);
+    w[0] = -(zxi * (zxi - 1.0) * (zxi - 2.0) / 6.0);
+    w[1] = (zxi + 1.0) * (zxi - 1.0) * (zxi - 2.0) / 2.0;
+    w[2] = -((zxi + 1.0) * zxi * (zxi - 2.0) / 2.0);
+    w[3] = (zxi + 1.0) * zxi * (zxi - 1.0) / 6.0;
+    *ind = k;
+}
+
+static void llo_init(orc_ctx *c)
+{
+    if (c->llo) return;
+    build_o_exchange(&c->ex_o5, c->N, 5, 0);
+    fld_init(&c->o_ll, c->N, c->N, 5);
+    c->llo = 1;
+}
+
+/* get_ecs_halo + ext_ecs_tile_halo (ecs_halo_mod.f90:74-175) of an o field on whole
+   panels, halo width 2: the o-point exchange; the six special points of every cube corner
+   from the exchanged values (ecs_halo_corners / ecs_halo_1corner, :179-300); the rows
+   of virtual points interpolated along the neighbours' grid lines (ecs_halo_edges_x /
+   _y, ecs_ext_halo_1e, :340-477; the first row leaves out its two end points); then the
+   corner values put in place (ecs_halo_corners_put, :302-338). */
+static void ecs_o_halo(orc_ctx *c, fld_t *f)
+{
+    const int n = c->N, hw = 2, ni = n + 4;
+    const double dxa = c->mo.hx;
+    exch_do(&c->ex_o5, f, NULL);
+    /* the weights of the x edges, target i = -1 .. n+2, rows 1..hw (wx: both directions and
+       the corners use them) */
+    double *W = malloc(sizeof(double) * 4 * ni * hw);
+    int *K = malloc(sizeof(int) * ni * hw);
+#define WI(i, j) (((j) - 1) * ni + (i) + 1)
+    for (int j = 1; j <= hw; j++)
+        for (int i = -1; i <= n + 2; i++) halo_o_weights(dxa, i, j, &W[4 * WI(i, j)], &K[WI(i, j)]);
+    double *zl = malloc(sizeof(double) * (n + 2)), *zh = malloc(sizeof(double) * (n + 2));
+    static const int idirs[4] = {1, -1, -1, 1}, jdirs[4] = {1, 1, -1, -1};
+    for (int t = 0; t < NPAN; t++) {
+        double sp[4][6];
+        for (int q = 0; q < 4; q++) {
+            const int idir = idirs[q], jdir = jdirs[q];
+            const int ist = idir > 0 ? 0 : n + 1, jst = jdir > 0 ? 0 : n + 1;
+#define FC(i, j) FA(f, t, ist + idir * (i), jst + jdir * (j))
+            /* corner weights: pw(k, i, j) = w(k, i, j), mirrored (k -> 1-k, i -> n+1-i) where idir = -1 */
+#define PW(k, i, j) (idir > 0 ? W[4 * WI((i), (j)) + (k) + 1] : W[4 * WI(n + 1 - (i), (j)) + (1 - (k)) + 1])
+            const double z0 = PW(0, 1, 1), z1 = PW(1, 1, 1), z2 = PW(2, 1, 1);
+            const double zw = PW(-1, 1, 1), zw2 = zw * zw, zw3 = zw2 * zw;
+            double zx = z0 * FC(0, 1) + z1 * FC(0, 2) + z2 * FC(0, 3);
+            double zy = z0 * FC(1, 0) + z1 * FC(1, -1) + z2 * FC(1, -2);
+            double zz = z0 * FC(1, 1) + z1 * FC(2, 1) + z2 * FC(3, 1);
+            sp[q][0] = (zx + zw * zy + zw2 * zz) / (1 - zw3);
+            const double zfy1 = (zy + zw * zz + zw2 * zx) / (1 - zw3);
+            zx = z0 * FC(1, 0) + z1 * FC(2, 0) + z2 * FC(3, 0);
+            zy = z0 * FC(0, 1) + z1 * FC(-1, 1) + z2 * FC(-2, 1);
+            zz = z0 * FC(1, 1) + z1 * FC(1, 2) + z2 * FC(1, 3);
+            sp[q][1] = (zx + zw * zy + zw2 * zz) / (1 - zw3);
+            const double zfy2 = (zy + zw * zz + zw2 * zx) / (1 - zw3);
+            double zff1 = PW(-1, 1, 2) * FC(2, 0) + PW(0, 1, 2) * FC(2, -1) + PW(1, 1, 2) * FC(2, -2) +
+                          PW(2, 1, 2) * FC(2, -3);
+            double zff2 = PW(-1, 1, 2) * FC(0, 2) + PW(0, 1, 2) * FC(-1, 2) + PW(1, 1, 2) * FC(-2, 2) +
+                          PW(2, 1, 2) * FC(-3, 2);
+            sp[q][2] = 0.5 * (PW(-1, 0, 1) * zff1 + PW(0, 0, 1) * zfy1 + PW(1, 0, 1) * FC(0, 1) + PW(2, 0, 1) * FC(0, 2) +
+                              PW(-1, 0, 1) * zff2 + PW(0, 0, 1) * zfy2 + PW(1, 0, 1) * FC(1, 0) + PW(2, 0, 1) * FC(2, 0));
+            zff1 = PW(-1, 2, 1) * FC(1, 0) + PW(0, 2, 1) * FC(1, -1) + PW(1, 2, 1) * FC(1, -2) + PW(2, 2, 1) * FC(1, -3);
+            const double zff11 = PW(-1, 2, 2) * FC(2, -1) + PW(0, 2, 2) * FC(2, -2) + PW(1, 2, 2) * FC(2, -3) +
+                                 PW(2, 2, 2) * FC(2, -4);
+            zff2 = PW(-1, 2, 1) * FC(0, 1) + PW(0, 2, 1) * FC(-1, 1) + PW(1, 2, 1) * FC(-2, 1) + PW(2, 2, 1) * FC(-3, 1);
+            const double zff22 = PW(-1, 2, 2) * FC(-1, 2) + PW(0, 2, 2) * FC(-2, 2) + PW(1, 2, 2) * FC(-3, 2) +
+                                 PW(2, 2, 2) * FC(-4, 2);
+            sp[q][3] = PW(-1, 0, 2) * zff1 + PW(0, 0, 2) * FC(-1, 1) + PW(1, 0, 2) * FC(-1, 2) + PW(2, 0, 2) * FC(-1, 3);
+            sp[q][4] = PW(-1, 0, 2) * zff2 + PW(0, 0, 2) * FC(1, -1) + PW(1, 0, 2) * FC(2, -1) + PW(2, 0, 2) * FC(3, -1);
+            sp[q][5] = 0.5 * (PW(-1, -1, 2) * zff11 + PW(0, -1, 2) * zff1 + PW(1, -1, 2) * FC(-1, 1) +
+                              PW(2, -1, 2) * FC(-1, 2) + PW(-1, -1, 2) * zff22 + PW(0, -1, 2) * zff2 +
+                              PW(1, -1, 2) * FC(1, -1) + PW(2, -1, 2) * FC(2, -1));
+#undef PW
+        }
+        /* edges: virtual row m (1..hw) of each side from the exchanged row m of the neighbour */
+        for (int side = 0; side < 4; side++)
+            for (int m = 1; m <= hw; m++) {
+                for (int b = 1; b <= n; b++)
+                    zl[b] = side == 0 ? FA(f, t, b, 1 - m) : side == 1 ? FA(f, t, b, n + m)
+                          : side == 2 ? FA(f, t, 1 - m, b) : FA(f, t, n + m, b);
+                const int a0 = m == 1 ? 2 : 1, a1 = m == 1 ? n - 1 : n;
+                for (int a = a0; a <= a1; a++) {
+                    const double *w = &W[4 * WI(a, m)];
+                    const int ii = K[WI(a, m)];
+                    zh[a] = w[0] * zl[ii - 1] + w[1] * zl[ii] + w[2] * zl[ii + 1] + w[3] * zl[ii + 2];
+                }
+                for (int a = a0; a <= a1; a++) {
+                    if (side == 0) FA(f, t, a, 1 - m) = zh[a];
+                    else if (side == 1) FA(f, t, a, n + m) = zh[a];
+                    else if (side == 2) FA(f, t, 1 - m, a) = zh[a];
+                    else FA(f, t, n + m, a) = zh[a];
+                }
+            }
+        /* the special points: corner-local (0,1), (1,0), (0,0), (-1,0), (0,-1), (-1,-1) */
+        static const int pi_[6] = {0, 1, 0, -1, 0, -1}, pj_[6] = {1, 0, 0, 0, -1, -1};
+        for (int q = 0; q < 4; q++) {
+            const int idir = idirs[q], jdir = jdirs[q];
+            const int ist = idir > 0 ? 0 : n + 1, jst = jdir > 0 ? 0 : n + 1;
+            for (int p = 0; p < 6; p++) FC(pi_[p], pj_[p]) = sp[q][p];
+        }
+#undef FC
+    }
+#undef WI
+    free(W); free(K); free(zl); free(zh);
+}
+
+/* latlon_regrid_t%do_regrid of an o field (the curl output of output_curl on Ch,
+   swm_output_diag_mod.f90:78-90; swm_output_diag_factory_mod.f90:48-52 curl_points 'o';
+   init_halo_for_interp 'o' cubic: the ECS_O halo of width 2, regrid_factory_mod.f90:285-287):
+   the cubic stencils of latlon_regrid_mod.f90:286-365 on the cell-centre mesh
+   (shift 1/2).  f: (6, N, N) packed; out[j][i], i fastest. */
+void orc_latlon_o(orc_ctx *c, const double *f, int nlat, int nlon, double *out)
+{
+    llo_init(c);
+    fld_t *b = &c->o_ll;
+    for (size_t k = 0; k < b->psz * NPAN; k++) b->p[k] = NAN;
+    fld_from_packed(b, f);
+    ecs_o_halo(c, b);
+    const mesh_t *m = &c->mo;
     const double alpha0 = -0.25 * PI_, beta0 = -0.25 * PI_;
     for (int j = 1; j <= nlat; j++) {
         const double phi = -0.5 * PI_ + (j - 1) * PI_ / (nlat - 1.0);

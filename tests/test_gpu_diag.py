@@ -246,3 +246,55 @@ def test_latlon_div_regrid_matches_oracle(operator, order):
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
     assert np.abs(out.regrid_div(st, member=0)).max() == 0.0
     dom.destroy()
+
+
+@pytest.mark.parametrize("precision,tol,order,grid", [("fp64", 1e-12, 42, None), ("fp64", 1e-12, 21, (37, 50)),
+                                                      ("fp64", 1e-12, 63, None), ("fp32", 1e-5, 42, None)])
+def test_latlon_curl_regrid_matches_oracle(precision, tol, order, grid):
+    """The curl.dat field of output_curl: curl_ch_sbp_sat_<order> of the covariant wind on
+    the cell centres, its ECS_O halo (exchange, virtual rows, the six special points of
+    each cube corner) and the cubic stencils on the cell-centre mesh, against the
+    oracle, for a wind whose panel-edge copies disagree."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import LatlonOutputer
+    from oracle.oracle import Oracle
+    N = 24
+    o = Oracle(N, sbp_order=order)
+    rng = np.random.default_rng(21)
+    h, u, v = o.ts2(u0=20.0, h_mean=1000.0, axis=(0.3, 0.0, 0.95))
+    u = u + rng.standard_normal(u.shape)
+    v = v + rng.standard_normal(v.shape)
+    nlat, nlon = grid if grid else (None, None)
+    ref = o.latlon_curl(u, v, nlat, nlon)
+    dom = create_domain(N, precision=precision, sbp_order=order, n_members=2)
+    st = create_stvec_swm(dom)
+    st.upload(h, u, v, member=1)
+    st.upload(h, 0 * u, 0 * v, member=0)
+    out = LatlonOutputer(dom, nlat, nlon)
+    got = out.regrid_curl(st, member=1)
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
+    assert np.abs(out.regrid_curl(st, member=0)).max() == 0.0
+    dom.destroy()
+
+
+def test_latlon_curl_solid_body_rotation_large_cube():
+    """At C192: the regridded curl of a solid-body rotation is its exact vorticity
+    2 u0 / a (r . axis) to the discretisation error, near the cube corners too."""
+    from ch_swe_b200 import create_domain, create_stvec_swm
+    from ch_swe_b200.diag import LatlonOutputer
+    from ch_swe_b200.testcases import williamson2
+    from oracle.oracle import EARTH_RADIUS
+    N, u0 = 192, 20.0
+    axis = np.array([np.sin(0.7), 0.0, np.cos(0.7)])
+    dom = create_domain(N, precision="fp64")
+    st = create_stvec_swm(dom).upload(*williamson2(N, u0=u0, h_mean=1000.0, axis=axis))
+    f = LatlonOutputer(dom).regrid_curl(st)
+    nlat, nlon = f.shape
+    phi = -np.pi / 2 + np.arange(nlat) * np.pi / (nlat - 1)
+    lam = np.arange(nlon) * 2 * np.pi / nlon
+    P, L = np.meshgrid(phi, lam, indexing="ij")
+    rdot = np.cos(P) * np.cos(L) * axis[0] + np.cos(P) * np.sin(L) * axis[1] + np.sin(P) * axis[2]
+    exact = 2 * u0 / EARTH_RADIUS * rdot
+    assert np.abs(f - exact).max() < 1e-3 * 2 * u0 / EARTH_RADIUS
+    dom.destroy()

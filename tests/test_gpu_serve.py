@@ -19,17 +19,21 @@ def _stream(n, seed, sizes=(24, 48), steps=(24, 64)):
     return poisson_stream(n, rate=2000.0, seed=seed, sizes=sizes, steps=steps)
 
 
-def test_mixed_results_equal_alone_bitwise():
-    """Same tile alone and in the mix: bit-identical states (both precisions, both operators)."""
+@pytest.mark.parametrize("grouped", [False, True])
+def test_mixed_results_equal_alone_bitwise(grouped):
+    """Same kernel configuration alone and in the mix: bit-identical states (both
+    precisions, both operators); grouped: the linear pools of a precision tick as one
+    group launch over their cube sizes."""
     from ch_swe_b200.serve import Server, run_alone
-    reqs = _stream(20, 11)
-    srv = Server(hbm_budget_bytes=2 << 30, max_tick=8, max_slots={24: 6, 48: 4})
+    reqs = _stream(20, 11, sizes=(24, 32, 48))
+    srv = Server(hbm_budget_bytes=2 << 30, max_tick=8, max_slots={24: 6, 32: 4, 48: 4}, grouped=grouped)
     stats = srv.run(reqs, realtime=False)
     srv.close()
     assert stats.n == len(reqs)
     assert {r.operator for r in reqs} == {"linear", "advective"}
+    assert (srv.group_ticks > 0) == grouped
     for r in reqs:
-        alone = run_alone(r, tile=r.pool_tile)
+        alone = run_alone(r, kernel_config=r.pool_cfg)
         for a, b, name in zip(r.result, alone, "huv"):
             assert np.array_equal(a, b), (r.rid, r.N, r.precision, name, np.abs(a - b).max())
 
