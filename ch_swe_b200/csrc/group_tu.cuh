@@ -68,4 +68,12 @@ bool GroupTU<T>::rk4_step(int tm, int occ, int runs, const GroupTable<T> &g, uns
     return false;
 }
 
+template <class T>
+cudaError_t GroupTU<T>::upload_tables(const Link *links, const int *cube_edges)
+{
+    cudaError_t e = cudaMemcpyToSymbol(c_link, links, sizeof(Link) * NPAN * 4);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cube_edge, cube_edges, sizeof(int) * 12 * 2);
+    return e;
+}
+
 }  // namespace chswe

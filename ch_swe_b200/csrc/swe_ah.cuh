@@ -144,44 +144,80 @@ __host__ __device__ constexpr int ah_reach() { return ORD == 21 ? 1 : (ORD == 63
 // neighbour's vector is handed over as the 'cross' exchange does, halo_vec); the
 // tendency and the RK update of k_stage (modes 0..4; FP32 mode 4 Kahan-compensated).
 template <class T, int MODE, int ORD>
-__global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, const T *__restrict__ E, T *V0, T *Y1,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_ah_stage(const T *__restrict__ Yin, const T *__restrict__ E, T *V0, T *Y1,
                                                   T *ACC, T *CMP, Dims d, AhView<T> a, MetricView<T> m, StageArgs sa,
                                                   T grav)
 {
     constexpr int R = ah_reach<ORD>(), W = AH_TX + 2 * R, H = AH_TY + 2 * R;
+    constexpr int NW = (H * W + 255) / 256;            // window points per thread
+    constexpr int NB = sizeof(T) == 8 ? 2 : 4;         // of them loaded per batch
+    constexpr int RR = AH_TY / 8;                      // tile rows per thread
     __shared__ T sH[H * W], sF[H * W], sG[H * W];
     const int N = d.N, n = N + 1;
     const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
     if (member_frozen(sa.dtm, mem)) return;
-    const int i0 = 1 + blockIdx.x * AH_TX, j0 = 1 + blockIdx.y * AH_TY;
+    // balanced tiles of at most AH_TX x AH_TY vertices (no slivers at the panel's far side)
+    const int i0 = 1 + (blockIdx.x * n) / gridDim.x, i1 = 1 + ((blockIdx.x + 1) * n) / gridDim.x;
+    const int j0 = 1 + (blockIdx.y * n) / gridDim.y, j1 = 1 + ((blockIdx.y + 1) * n) / gridDim.y;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const T *y = Yin + mem * d.ms;
     const T *yh = y + t * d.ps, *yu = yh + d.fs, *yv = yh + 2 * d.fs;
+    const int64_t po = mem * d.ms + t * d.ps;
+    const int64_t fs = d.fs;
     pdl_trigger();
     pdl_wait();
-    // the window: the tile's rows over the x reach and its columns over the y reach (the
-    // corners are never read); vertices outside the panel hold zeros (no stencil reads them)
-    for (int q = tid; q < H * W; q += 256) {
-        const int wi = q % W, wj = q / W;
-        const int i = i0 - R + wi, j = j0 - R + wj;
-        const bool band = (wj >= R && wj < R + AH_TY) || (wi >= R && wi < R + AH_TX);
-        T h = T(0), f = T(0), g = T(0);
-        if (band && i >= 1 && i <= n && j >= 1 && j <= n) {
-            const int64_t o = box_off(d.P, i, j);
-            const T u = __ldcg(yu + o), v = __ldcg(yv + o), J = __ldg(a.J + o);
-            h = __ldcg(yh + o);
-            f = J * (__ldg(a.Q1 + o) * u + __ldg(a.Q2 + o) * v);
-            g = J * (__ldg(a.Q2 + o) * u + __ldg(a.Q3 + o) * v);
+    // the RK operands of this thread's vertices, in flight during the window phase
+    constexpr bool LV = MODE >= 1, LA = MODE >= 2, LC = (sizeof(T) == 4) && MODE == 4;
+    T pv[3][RR], pa[3][RR], pc[3][RR];
+#pragma unroll
+    for (int rr = 0; rr < RR; rr++) {
+        const int i = i0 + threadIdx.x, j = j0 + threadIdx.y + 8 * rr;
+        const bool ok = i < i1 && j < j1;
+        const int64_t o = po + box_off(d.P, i, j);
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            pv[f][rr] = LV && ok ? V0[o + f * fs] : T(0);
+            pa[f][rr] = LA && ok ? ACC[o + f * fs] : T(0);
+            pc[f][rr] = LC && ok ? CMP[o + f * fs] : T(0);
         }
-        sH[q] = h;
-        sF[q] = f;
-        sG[q] = g;
+    }
+    // the window: the tile's rows over the x reach and its columns over the y reach (the
+    // corners are never read); vertices outside the panel hold zeros (no stencil reads
+    // them).  Each batch issues all of its loads before its first multiply.
+#pragma unroll
+    for (int b0 = 0; b0 < NW; b0 += NB) {
+        T rh[NB], ru[NB], rv[NB], rj[NB], r1[NB], r2[NB], r3[NB];
+#pragma unroll
+        for (int k = 0; k < NB; k++) {
+            const int q = tid + (b0 + k) * 256;
+            const int wi = q % W, wj = q / W;
+            const int i = i0 - R + wi, j = j0 - R + wj;
+            const bool band = (wj >= R && wj < R + AH_TY) || (wi >= R && wi < R + AH_TX);
+            const bool ok = b0 + k < NW && q < H * W && band && i >= 1 && i <= n && j >= 1 && j <= n;
+            const int64_t o = ok ? box_off(d.P, i, j) : 0;
+            rh[k] = ok ? __ldcg(yh + o) : T(0);
+            ru[k] = ok ? __ldcg(yu + o) : T(0);
+            rv[k] = ok ? __ldcg(yv + o) : T(0);
+            rj[k] = ok ? __ldg(a.J + o) : T(0);
+            r1[k] = ok ? __ldg(a.Q1 + o) : T(0);
+            r2[k] = ok ? __ldg(a.Q2 + o) : T(0);
+            r3[k] = ok ? __ldg(a.Q3 + o) : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < NB; k++) {
+            const int q = tid + (b0 + k) * 256;
+            if (b0 + k < NW && q < H * W) {
+                sH[q] = rh[k];
+                sF[q] = rj[k] * (r1[k] * ru[k] + r2[k] * rv[k]);
+                sG[q] = rj[k] * (r2[k] * ru[k] + r3[k] * rv[k]);
+            }
+        }
     }
     __syncthreads();
-#pragma unroll 1
-    for (int rr = 0; rr < AH_TY / 8; rr++) {
+#pragma unroll
+    for (int rr = 0; rr < RR; rr++) {
         const int i = i0 + threadIdx.x, j = j0 + threadIdx.y + 8 * rr;
-        if (i > n || j > n) continue;
+        if (i >= i1 || j >= j1) continue;
         const int ro = (j - j0 + R) * W - i0 + R, co = i - i0 + R - j0 * W + R * W;
         // row j of the window at column k, column i at row l
         T gx = dn2n<T, ORD>(i, n, [&](int k) { return sH[ro + k]; }) * m.inv_hxa;
@@ -230,25 +266,24 @@ __global__ void __launch_bounds__(256) k_ah_stage(const T *__restrict__ Yin, con
     const T ut = a.Q1[o] * u + a.Q2[o] * v, vt = a.Q2[o] * u + a.Q3[o] * v;
     const T fJ = a.fJ[t * d.ps + o];
     const T k3[3] = {-T(sa.Hm[mem]) * dv, -grav * gx + fJ * vt, -grav * gy - fJ * ut};
-    const int64_t po = mem * d.ms + t * d.ps + o;
     const T dt = T(sa.dtm ? sa.dtm[mem] : sa.dt);
 #pragma unroll
     for (int f = 0; f < 3; f++) {
-        const int64_t of = po + f * d.fs;
+        const int64_t of = po + o + f * fs;
         if constexpr (MODE == 0) {
             Y1[of] = k3[f];
         } else if constexpr (MODE <= 3) {
             const T ca = (MODE == 3) ? dt : T(0.5) * dt;
             const T cb = (MODE == 1) ? dt / T(6) : dt / T(3);
-            Y1[of] = V0[of] + ca * k3[f];
-            ACC[of] = (MODE == 1) ? cb * k3[f] : ACC[of] + cb * k3[f];
+            Y1[of] = pv[f][rr] + ca * k3[f];
+            ACC[of] = (MODE == 1) ? cb * k3[f] : pa[f][rr] + cb * k3[f];
         } else if constexpr (sizeof(T) == 4) {
-            float sv = V0[of], cv = CMP[of];
-            kahan_add(sv, cv, ACC[of] + (dt / T(6)) * k3[f]);
+            float sv = pv[f][rr], cv = pc[f][rr];
+            kahan_add(sv, cv, pa[f][rr] + (dt / T(6)) * k3[f]);
             V0[of] = sv;
             CMP[of] = cv;
         } else {
-            V0[of] = V0[of] + (ACC[of] + (dt / T(6)) * k3[f]);
+            V0[of] = pv[f][rr] + (pa[f][rr] + (dt / T(6)) * k3[f]);
         }
     }
     }

@@ -392,6 +392,8 @@ static cudaError_t upload_link_tables()
     if (e == cudaSuccess) e = StageTU<double, 33>::upload_tables(l, q);
     if (e == cudaSuccess) e = FusedTU<float>::upload_tables(l);
     if (e == cudaSuccess) e = FusedTU<double>::upload_tables(l);
+    if (e == cudaSuccess) e = GroupTU<float>::upload_tables(l, q);
+    if (e == cudaSuccess) e = GroupTU<double>::upload_tables(l, q);
     return e;
 }
 
@@ -1464,6 +1466,7 @@ static void launch_ah(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc
     const int n = c->cfg.N + 1, M = c->cfg.n_members;
     launch_k(k_ah_edge<T, ORD>, dim3((n + 127) / 128, NPAN * 4, M), dim3(128), 0, c->stream, (const T *)yin,
              (T *)c->edge, c->dims, av, mv, dtm);
+    // balanced tiles of at most AH_TX x AH_TY vertices
     const dim3 pb(32, 8), pg((n + AH_TX - 1) / AH_TX, (n + AH_TY - 1) / AH_TY, NPAN * M);
     const T g = T(c->cfg.grav);
     const T *Y = (const T *)yin, *E = (const T *)c->edge;
@@ -1624,12 +1627,15 @@ extern "C" int swe_operator_contravariant(swe_ctx *c, swe_stvec *vout, const swe
         return SWE_OK;
     }
     const int M = c->cfg.n_members;
-    if (c->elem == 8)
-        if (!launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d, (double *)c->es, c->dims,
-                                 c->m64.v, c->stream)) c->launch_miss = true;
-    else
-        if (!launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d, (float *)c->es, c->dims,
-                                c->m32.v, c->stream)) c->launch_miss = true;
+    bool ok;
+    if (c->elem == 8) {
+        ok = launch_co2contra<double>(c->tile, c->occ, c->runs, c->ord, M, (const double *)vin->d, (double *)vout->d,
+                                      (double *)c->es, c->dims, c->m64.v, c->stream);
+    } else {
+        ok = launch_co2contra<float>(c->tile, c->occ, c->runs, c->ord, M, (const float *)vin->d, (float *)vout->d,
+                                     (float *)c->es, c->dims, c->m32.v, c->stream);
+    }
+    if (!ok) return fail(c, SWE_EINVAL, "swe_operator_contravariant: no built contravariant kernel for the configuration");
     c->launches++;
     CU_LAUNCHED(c);
     return SWE_OK;

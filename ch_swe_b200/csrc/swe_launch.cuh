@@ -169,6 +169,8 @@ struct GroupTU {
     // false: (tm, occ, runs) is not a built group configuration; nothing was launched
     static bool rk4_step(int tm, int occ, int runs, const GroupTable<T> &g, unsigned tiles, unsigned edges,
                          cudaStream_t st);
+    // this translation unit's copies of the panel links and cube edges (constant memory)
+    static cudaError_t upload_tables(const Link *links, const int *cube_edges);
 };
 
 // Tiles of the fused stage: ceil((N+1) / FUSED_TW) columns and ceil((N+1) / th) rows
