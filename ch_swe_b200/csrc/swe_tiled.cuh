@@ -434,15 +434,17 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
 
     pdl_trigger();
     pdl_wait();
-    // The linear operator copies its windows (h, ut, vt, J on the u and v meshes)
-    // straight into shared memory with asynchronous copies: one memory round trip and
-    // no register staging; the J ut and J vt products follow in the first pass phase.
-    // The advective operator stages through registers (it substitutes the
-    // pre-averaging boundary h and the mass flux).
-    constexpr bool ASYNC = !ADV;
-    if constexpr (ASYNC) {
-        const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0), ov = box_off(P, svt.x0, svt.y0);
+    // The windows (h, ut, vt, J on the u and v meshes; for the advective operator also
+    // the mass flux, into the up and vp windows until the first pass phase reads it)
+    // go straight into shared memory by asynchronous copies: one memory round trip and
+    // no register staging.  The J ut and J vt products (J Fu, J Fv) and the advective
+    // operator's substitutions in the h window follow in the first pass phase.
+    const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0), ov = box_off(P, svt.x0, svt.y0);
+    {
         const T *gh = yp + oh, *gu = wp + d.fs + ou, *gv = wp + 2 * d.fs + ov, *gjy = m.Jy + ou, *gjx = m.Jx + ov;
+        // the fields whose divergence is taken: ut, vt, or the advective operator's mass flux
+        const T *gfu = ADV ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
+        const T *gfv = ADV ? (const T *)a.F + mo + t * d.ps + 2 * d.fs + ov : nullptr;
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
@@ -453,79 +455,22 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
                 __pipeline_memcpy_async(sh.a + r * PW + c, gh + go, sizeof(T));
                 __pipeline_memcpy_async(sut.a + r * PW + c, gu + go, sizeof(T));
                 __pipeline_memcpy_async(svt.a + r * PW + c, gv + go, sizeof(T));
-                if (r >= 2 && r < th + 2) __pipeline_memcpy_async(sju.a + (r - 2) * PW + c, gjy + go, sizeof(T));
-                if (c >= 2 && c < tw + 2) __pipeline_memcpy_async(sjv.a + r * PT + (c - 2), gjx + go, sizeof(T));
+                if (r >= 2 && r < th + 2) {
+                    __pipeline_memcpy_async(sju.a + (r - 2) * PW + c, gjy + go, sizeof(T));
+                    if constexpr (ADV) __pipeline_memcpy_async(sup.a + (r - 2) * PW + c, gfu + go, sizeof(T));
+                }
+                if (c >= 2 && c < tw + 2) {
+                    __pipeline_memcpy_async(sjv.a + r * PT + (c - 2), gjx + go, sizeof(T));
+                    if constexpr (ADV) __pipeline_memcpy_async(svp.a + r * PT + (c - 2), gfv + go, sizeof(T));
+                }
             }
         }
         __pipeline_commit();
-    } else {
-        // ---- batch 1a: h and ut windows with J ut
-        {
-            const int64_t oh = box_off(P, sh.x0, sh.y0), ou = box_off(P, sut.x0, sut.y0);
-            const T *gh = yp + oh, *gu = wp + d.fs + ou, *gjy = m.Jy + ou;
-            // the field whose divergence is taken: ut, or the mass flux of the advective operator
-            const T *gf = ADV ? (const T *)a.F + mo + t * d.ps + d.fs + ou : nullptr;
-            T rh[IT_WIN], ru[IT_WIN], rjy[IT_WIN], rfu[IT_WIN];
-            const T *hpre = ADV ? (const T *)a.HB : nullptr;
-            // only windows that reach a panel-boundary vertex read the pre-averaging values
-            const bool etile = i0 <= 3 || i1 + 2 >= n || j0 <= 3 || j1 + 2 >= n;
-    #pragma unroll
-            for (int it = 0; it < IT_WIN; it++) {
-                const int q = threadIdx.x + it * STAGE_THREADS;
-                int r, c;
-                split(q, w5, iw5, r, c);
-                const bool ok = q < w5 * h5;
-                const int go = r * P + c;
-                const bool jr = ok && r >= 2 && r < th + 2;
-                rh[it] = ok ? __ldg(gh + go) : T(0);
-                if (ADV && etile && ok) {
-                    // advective operator: the gradient reads h as it was before the averaging
-                    const int hi = sh.x0 + c, hj = sh.y0 + r;
-                    if (hi >= 1 && hi <= n && hj >= 1 && hj <= n && (hi == 1 || hi == n || hj == 1 || hj == n))
-                        rh[it] = __ldg(hpre + (hi == 1 || hi == n ? hb_index(N, mem, t, hi == 1 ? SIDE_L : SIDE_R, hj)
-                                                               : hb_index(N, mem, t, hj == 1 ? SIDE_B : SIDE_T, hi)));
-                }
-                // orography: the gradient's input is h + h_surf (zero margins)
-                if (ADV && a.HS && ok) rh[it] += __ldg((const T *)a.HS + t * d.ps + oh + go);
-                ru[it] = ok ? __ldg(gu + go) : T(0);
-                rjy[it] = jr ? __ldg(gjy + go) : T(0);
-                rfu[it] = ADV && jr ? __ldg(gf + go) : ru[it];
-            }
-    #pragma unroll
-            for (int it = 0; it < IT_WIN; it++) {
-                const int q = threadIdx.x + it * STAGE_THREADS;
-                int r, c;
-                split(q, w5, iw5, r, c);
-                if (q < w5 * h5) {
-                    sh.a[r * PW + c] = rh[it];
-                    sut.a[r * PW + c] = ru[it];
-                    if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] = rjy[it] * rfu[it];
-                }
-            }
-        }
     }
     // ---- batch 1b: vt window with J vt, the h halos across the panel edges, and
     // fJ2 (or the synchronised edge value) for the up / vp passes
     T f1[IT_RW][RBW], f2[IT_STRIP];
     {
-        const int64_t ov = box_off(P, svt.x0, svt.y0);
-        const T *gv = wp + 2 * d.fs + ov, *gjx = m.Jx + ov;
-        const T *gf = ADV ? (const T *)a.F + mo + t * d.ps + 2 * d.fs + ov : nullptr;
-        T rv[IT_WIN], rjx[IT_WIN], rfv[IT_WIN];
-        if constexpr (!ASYNC) {
-#pragma unroll
-            for (int it = 0; it < IT_WIN; it++) {
-                const int q = threadIdx.x + it * STAGE_THREADS;
-                int r, c;
-                split(q, w5, iw5, r, c);
-                const bool ok = q < w5 * h5;
-                const int go = r * P + c;
-                const bool jc = ok && c >= 2 && c < tw + 2;
-                rv[it] = ok ? __ldg(gv + go) : T(0);
-                rjx[it] = jc ? __ldg(gjx + go) : T(0);
-                rfv[it] = ADV && jc ? __ldg(gf + go) : rv[it];
-            }
-        }
         T hx0 = 0, hx1 = 0, hy0 = 0, hy1 = 0;
         const int q = threadIdx.x;
         const T *hpre = ADV ? (const T *)a.HB : nullptr;
@@ -574,18 +519,6 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
             else if (l >= 1 && l <= n && on_boundary(k, l, n)) f2[it] = edge_entry(E, N, mem, t, k, l)[1];
             else f2[it] = __ldg(fJ2 + box_off(P, k, l));
         }
-        if constexpr (!ASYNC) {
-#pragma unroll
-            for (int it = 0; it < IT_WIN; it++) {
-                const int qq = threadIdx.x + it * STAGE_THREADS;
-                int r, c;
-                split(qq, w5, iw5, r, c);
-                if (qq < w5 * h5) {
-                    svt.a[r * PW + c] = rv[it];
-                    if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] = rjx[it] * rfv[it];
-                }
-            }
-        }
         if (q < th) { hl[q] = hx0; hr[q] = hx1; }
         if (q < tw) { hb[q] = hy0; ht[q] = hy1; }
     }
@@ -609,20 +542,35 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
             mjx[it][mm] = hv ? __ldg(m.iJx + o) : T(0);
         }
     }
-    if constexpr (ASYNC) __pipeline_wait_prior(0);
+    __pipeline_wait_prior(0);
     __syncthreads();
-    if constexpr (ASYNC) {
-        // J ut on the rows, J vt on the columns of the windows (read from the second phase on)
+    {
+        // J ut on the rows, J vt on the columns of the windows (read from the second phase
+        // on); the advective operator: J times its mass flux, and in the h window the
+        // values before the averaging of the duplicated boundary vertices (which the
+        // gradient reads; only windows that reach a panel-boundary vertex) plus the
+        // orography h_surf (the gradient's input is h + h_surf; zero margins)
+        const T *hpre = ADV ? (const T *)a.HB : nullptr;
+        const bool etile = i0 <= 3 || i1 + 2 >= n || j0 <= 3 || j1 + 2 >= n;
 #pragma unroll
         for (int it = 0; it < IT_WIN; it++) {
             const int q = threadIdx.x + it * STAGE_THREADS;
             int r, c;
             split(q, w5, iw5, r, c);
             if (q < w5 * h5) {
-                if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] *= sut.a[r * PW + c];
-                if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] *= svt.a[r * PW + c];
+                if (r >= 2 && r < th + 2) sju.a[(r - 2) * PW + c] *= (ADV ? sup.a[(r - 2) * PW + c] : sut.a[r * PW + c]);
+                if (c >= 2 && c < tw + 2) sjv.a[r * PT + (c - 2)] *= (ADV ? svp.a[r * PT + (c - 2)] : svt.a[r * PW + c]);
+                if constexpr (ADV) {
+                    const int hi = sh.x0 + c, hj = sh.y0 + r;
+                    if (etile && hi >= 1 && hi <= n && hj >= 1 && hj <= n && (hi == 1 || hi == n || hj == 1 || hj == n))
+                        sh.a[r * PW + c] = __ldg(hpre + (hi == 1 || hi == n ? hb_index(N, mem, t, hi == 1 ? SIDE_L : SIDE_R, hj)
+                                                                      : hb_index(N, mem, t, hj == 1 ? SIDE_B : SIDE_T, hi)));
+                    if (a.HS) sh.a[r * PW + c] += __ldg((const T *)a.HS + t * d.ps + oh + r * P + c);
+                }
             }
         }
+        // the mass flux in the up and vp windows is read above: the passes below overwrite them
+        if constexpr (ADV) __syncthreads();
     }
 
     // ---- P1: up = fJ2 I_c2i,y(vt): columns of the up window, runs along the tile rows
