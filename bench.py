@@ -446,8 +446,9 @@ def run_serving(args, torch):
     return {
         "workload": f"{SRV_REQUESTS} requests, Poisson {SRV_RATE:g}/s (seed {SRV_SEED}), N in {list(serve.SIZES)}, "
                     "24-576 RK4 steps, FP32/FP64 50/50, linear/advective operator 50/50, 1-4 seeded Gaussians",
-        "grouped": {"what": "the linear pools of each precision tick together: one grid per kernel over "
-                               "their cube sizes (swe_group_rk4_steps_members), 12 launches per RK4 step",
+        "grouped": {"what": "the linear pools of each precision up to C96 tick together: one grid per kernel "
+                               "over their cube sizes (swe_group_rk4_steps_members), 12 launches per RK4 step; "
+                               "C192 and C384 pools on their own streams and autotuned configurations",
                     "group_ticks": group_ticks},
         "requests": stats.n, "makespan_s": stats.makespan_s, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
         "mean_ms": stats.mean_ms, "requests_per_s": stats.requests_per_s,

@@ -525,7 +525,11 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
 
     // ---- batch 2 (in flight during the passes): the final pass's metric, or the
     // synchronised divergence on the panel boundary, by output run
-    T mja[IT_RT][RBT], mjy[IT_RT][RBT], mjx[IT_RT][RBT];
+    // (the advective operator: also its tendencies of the thread's points)
+    T mja[IT_RT][RBT], mjy[IT_RT][RBT], mjx[IT_RT][RBT], mau[IT_RT][RBT], mav[IT_RT][RBT];
+    const T *Aa = (const T *)a.A;
+    // advective tendencies of this panel (u, v fields)
+    const T *Au = ADV ? Aa + mo + t * d.ps + d.fs : nullptr, *Av = ADV ? Aa + mo + t * d.ps + 2 * d.fs : nullptr;
 #pragma unroll
     for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
@@ -540,6 +544,10 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
             mja[it][mm] = !ok ? T(0) : on_boundary(i, j, n) ? edge_entry(E, N, mem, t, i, j)[2] : __ldg(m.iJa + o);
             mjy[it][mm] = hu ? __ldg(m.iJy + o) : T(0);
             mjx[it][mm] = hv ? __ldg(m.iJx + o) : T(0);
+            if constexpr (ADV) {
+                mau[it][mm] = hu ? __ldg(Au + o) : T(0);
+                mav[it][mm] = hv ? __ldg(Av + o) : T(0);
+            }
         }
     }
     __pipeline_wait_prior(0);
@@ -699,9 +707,6 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
     // RK4 update below are coalesced row by row)
     const T H = T(a.Hm[mem]);
     T kh[IT_RT][RBT], ku[IT_RT][RBT], kv[IT_RT][RBT];
-    const T *Aa = (const T *)a.A;
-    // advective tendencies of this panel (u, v fields), indexed in 32 bits
-    const T *Au = ADV ? Aa + mo + t * d.ps + d.fs : nullptr, *Av = ADV ? Aa + mo + t * d.ps + 2 * d.fs : nullptr;
 #pragma unroll
     for (int it = 0; it < IT_RT; it++) {
         const int q = threadIdx.x + it * STAGE_THREADS;
@@ -728,7 +733,7 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
                 for (int mm = 0; mm < RBT; mm++) {
                     const int j = jr + mm;
                     if constexpr (ADV) {
-                        const T au = __ldg(Au + box_off32(P, i, j));
+                        const T au = mau[it][mm];
                         ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
                     } else {
                         ku[it][mm] = skx.at(i, j) + scx.at(i, j) * mjy[it][mm];
@@ -744,7 +749,7 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
             for (int mm = 0; mm < RBT; mm++) {
                 if constexpr (ADV) {
                     const int j = jr + mm;
-                    T av = __ldg(Av + box_off32(P, i, j));
+                    T av = mav[it][mm];
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
                     kv[it][mm] = (av + -m.grav * gy[mm]) + run_interp<T, RBT, ORD>(v, mm) * mjx[it][mm];
                 } else {
@@ -768,7 +773,7 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
             if (i <= N) {
                 if constexpr (ADV) {
                     // advective operator: (A + (-g) grad_x h) + Coriolis, A synchronised on the duplicated edge rows
-                    T au = __ldg(Au + box_off32(P, i, j));
+                    T au = mau[it][mm];
                     if (j == 1 || j == n) au = adv_edge_sync(Aa, d, mem, t, 1, i, j, au);
                     ku[it][mm] = (au + skx.at(i, j)) + scx.at(i, j) * mjy[it][mm];
                 } else {
@@ -781,7 +786,7 @@ __device__ __forceinline__ void stage_tile(const Blk &bk, const T *__restrict__ 
                 if (j >= N + 1 - SB::NSAT) gy += T(SB::satw(N + 1 - j)) * (ht[x] - hcol(n));
                 gy = gy * m.inv_hxa;
                 if constexpr (ADV) {
-                    T av = __ldg(Av + box_off32(P, i, j));
+                    T av = mav[it][mm];
                     if (i == 1 || i == n) av = adv_edge_sync(Aa, d, mem, t, 2, i, j, av);
                     kv[it][mm] = (av + -m.grav * gy) + ii2c_u<T, ORD>(j, N, pcol) * mjx[it][mm];
                 } else {

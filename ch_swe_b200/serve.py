@@ -16,11 +16,12 @@ Continuous batching:
   requests of that pool are uploaded into the free slots;
 - pools run on separate streams, so the work of different cube sizes and
   precisions overlaps on the device;
-- with grouped=True, the linear pools of one precision share one kernel
-  configuration and tick together as a group (swe_group_rk4_steps_members): one
-  grid per kernel covers every cube size of the group, twelve launches per RK4 step
-  for all of them; the tick is as long as the shortest remaining integration of the
-  group.
+- with grouped=True, the linear pools of one precision up to cube size
+  group_max_n share one kernel configuration and tick together as a group
+  (swe_group_rk4_steps_members): one grid per kernel covers every cube size of the
+  group, twelve launches per RK4 step for all of them; the tick is as long as the
+  shortest remaining integration of the group.  Larger cubes fill the GPU with one
+  member and keep their own pools, streams and autotuned configurations.
 
 Admission by HBM budget: a pool is created when a request needs one and its
 slots fit in the budget that other pools leave free (idle empty pools are
@@ -261,7 +262,7 @@ class ServeStats:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int = 16 << 30, max_tick: int = 16, max_slots=None, tiles=None,
-                 grouped: bool = False):
+                 grouped: bool = False, group_max_n: int = 96):
         import torch
         self.torch = torch
         self.budget = int(hbm_budget_bytes)
@@ -269,6 +270,7 @@ class Server:
         self.max_slots = dict(MAX_SLOTS if max_slots is None else max_slots)
         self.tiles = dict(tiles or {})
         self.grouped = bool(grouped)
+        self.group_max_n = int(group_max_n)
         self.pools: dict[tuple, Pool] = {}
         # precision -> (the grouped pools' keys, DomainGroup)
         self.groups: dict[str, tuple] = {}
@@ -320,7 +322,8 @@ class Server:
         cap = min(want, free // per)
         if cap < 1:
             return None
-        cfg = GROUP_CONFIG[req.precision] if self.grouped and req.operator == "linear" else None
+        cfg = (GROUP_CONFIG[req.precision]
+               if self.grouped and req.operator == "linear" and req.N <= self.group_max_n else None)
         pool = Pool(req.N, req.precision, int(cap), self.torch, tile=self.tiles.get(key), operator=req.operator,
                     kernel_config=cfg)
         self.pools[key] = pool
