@@ -99,4 +99,33 @@ class rk4_gpu_t {
     }
 };
 
+// Several domains' RK4 steps as one grid per kernel (swe_group_*: up to 8 linear Ch
+// contexts of one precision and split kernel configuration, any cube sizes); no
+// reference counterpart, the reference advances one state per timescheme%step.
+class group_gpu_t {
+  public:
+    explicit group_gpu_t(const std::vector<const domain_gpu_t *> &doms)
+    {
+        std::vector<swe_ctx *> c;
+        for (const domain_gpu_t *d : doms) c.push_back(d->ctx());
+        check(swe_group_create(c.data(), (int)c.size(), &g_), c.empty() ? nullptr : c[0], "swe_group_create");
+    }
+    ~group_gpu_t() { if (g_) swe_group_destroy(g_); }
+    group_gpu_t(const group_gpu_t &) = delete;
+    group_gpu_t &operator=(const group_gpu_t &) = delete;
+    // nsteps RK4 steps of states[k] with the per-member time steps dts[k]
+    void steps_members(const std::vector<stvec_swm_gpu_t *> &states, const std::vector<const double *> &dts, int nsteps)
+    {
+        std::vector<swe_stvec *> v;
+        for (stvec_swm_gpu_t *s : states) v.push_back(s->handle());
+        const int rc = swe_group_rk4_steps_members(g_, v.data(), dts.data(), nsteps);
+        if (rc != SWE_OK)
+            throw std::runtime_error(std::string("group steps: status ") + std::to_string(rc) + " (" +
+                                     swe_group_last_error(g_) + ")");
+    }
+
+  private:
+    swe_group *g_ = nullptr;
+};
+
 }  // namespace chswe_host
