@@ -1546,8 +1546,9 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     const bool fork = c->side && c->branches;
     if (fork) {
         // The averaging of h and the wind halo depend on the stage input only, the
-        // wind at the vertices on k_co2contra: they run on the side stream beside
-        // k_co2contra, k_flux and k_edge, and join before k_adv.
+        // wind at the vertices and the advective tendencies (which read neither h
+        // nor the mass flux) on k_co2contra: they run on the side stream beside
+        // k_co2contra, k_flux and k_edge, and join before the stage kernel.
         cudaEventRecord(c->ev_fork, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_fork, 0);
         launch_k(k_havg<T>, hg, dim3(HAVG_THREADS), 0, c->side, (T *)yin, (T *)c->hb, c->dims, dtm);
@@ -1558,6 +1559,8 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
         cudaEventRecord(c->ev_co2, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_co2, 0);
         launch_k(k_uhvh<T>, pg, pb, 0, c->side, (const T *)c->w, (T *)c->ph, c->dims, dtm);
+        launch_k(k_adv<T>, pg, pb, 0, c->side, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
+                 (T *)c->adt, c->dims, av, mv, dtm);
         cudaEventRecord(c->ev_side, c->side);
         cudaStreamWaitEvent(c->stream, c->ev_havg, 0);
     } else {
@@ -1574,9 +1577,9 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     } else {
         launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
         launch_k(k_vhalo<T>, vg, dim3(256), 0, c->stream, (const T *)yin, (T *)c->vh, c->dims, av, M, dtm);
+        launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
+                 (T *)c->adt, c->dims, av, mv, dtm);
     }
-    launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
-             (T *)c->adt, c->dims, av, mv, dtm);
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb, c->hs};
     if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                     (T *)cmp, c->dims, mv, a, c->stream)) c->launch_miss = true;
