@@ -5,7 +5,8 @@ the C ABI in include/chswe.h.  See ``ch_swe_b200.swm`` for the reference-shaped 
 """
 from ._lib import SweError, load  # noqa: F401
 from .swm import (Domain, OperatorSwmLin, Rk4, StvecSwm, create_domain, create_stvec_swm,  # noqa: F401
-                  create_swm_operator, create_timescheme, edge_links, state_shapes)
+                  create_swm_diff_operator, create_swm_operator, create_timescheme, edge_links, state_shapes)
 
 __all__ = ["SweError", "load", "Domain", "OperatorSwmLin", "Rk4", "StvecSwm", "create_domain",
-           "create_stvec_swm", "create_swm_operator", "create_timescheme", "edge_links", "state_shapes"]
+           "create_stvec_swm", "create_swm_diff_operator", "create_swm_operator", "create_timescheme", "edge_links",
+           "state_shapes"]

@@ -18,6 +18,7 @@
 #include "swe_advective.cuh"
 #include "swe_ah.cuh"
 #include "swe_cgrid.cuh"
+#include "swe_diff.cuh"
 #include "swe_kernels.cuh"
 #include "swe_launch.cuh"
 
@@ -288,6 +289,8 @@ struct swe_ctx {
     DevAh<double> ah64;
     DevAh<float> ah32;
     double *qa = nullptr;            // SBP_Ah quadrature weights J hx hy Ax Ay at the vertices (one box)
+    void *dif = nullptr;             // diffusion scratch: 5 sets of [member][4 fields][panel][box] (first use)
+    void *dif_b = nullptr;           // contravariant basis b1, b2 of the vertices, [panel][6][box] (first use)
     // C staggering (cfg.staggering == SWE_STAG_C): h on the cell centres, u on the x
     // points, v on the y points; the C-grid gradient, divergence and co2contra
     bool cstag = false;
@@ -990,6 +993,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
     cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
+    cudaFree(c->dif); cudaFree(c->dif_b);
     cudaFree(c->fmet); cudaFree(c->derr); cudaFree(c->hs); cudaFree(c->cmet);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -2056,6 +2060,125 @@ __global__ void k_quad(const T *__restrict__ y, const T *__restrict__ w, const d
         __syncthreads();
     }
     if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+// ---------------------------------------------------------------------------
+// horizontal diffusion on the Ah staggering (swe_diff.cuh)
+// ---------------------------------------------------------------------------
+template <class T>
+static int dif_setup(swe_ctx *c)
+{
+    const int N = c->cfg.N, n = N + 1, P = c->dims.P;
+    const size_t box = (size_t)c->dims.ps, M = (size_t)c->cfg.n_members;
+    if (!c->dif_b) {
+        // b1, b2 of the equiangular vertices on each panel (metric_2d_ecs_mod.f90:377-395)
+        std::vector<T> h((size_t)NPAN * 6 * box, T(0));
+        const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
+        for (int p = 0; p < NPAN; p++)
+            for (int j = 1; j <= n; j++)
+                for (int i = 1; i <= n; i++) {
+                    const double al = -0.25 * pi + (i - 1) * hx, be = -0.25 * pi + (j - 1) * hx;
+                    double bp[3], b1[3], b2[3];
+                    b1p(al, be, bp);
+                    p2r(p, bp, b1);
+                    b2p(al, be, bp);
+                    p2r(p, bp, b2);
+                    const size_t o = (size_t)box_off(P, i, j);
+                    for (int k = 0; k < 3; k++) {
+                        h[((size_t)p * 6 + k) * box + o] = T(b1[k]);
+                        h[((size_t)p * 6 + 3 + k) * box + o] = T(b2[k]);
+                    }
+                }
+        if (cudaMalloc(&c->dif_b, h.size() * sizeof(T)) != cudaSuccess)
+            return fail(c, SWE_ENOMEM, "diffusion basis allocation failed");
+        CU(c, cudaMemcpy(c->dif_b, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    if (!c->dif && cudaMalloc(&c->dif, 5 * M * DIF_FIELDS * NPAN * box * sizeof(T)) != cudaSuccess)
+        return fail(c, SWE_ENOMEM, "diffusion scratch allocation failed");
+    return SWE_OK;
+}
+
+// The diffusion coefficient of hordiff_scalar_t (diff_order 2, diff_coeff = coeff a hx,
+// hordiff_factory_mod.f90:193-227, hordiff_scalar_mod.f90:46): -(coeff a hx)^4.
+static double dif_coeff(const swe_ctx *c, double coeff)
+{
+    const double hx = 0.5 * 3.141592653589793238462643383279502884 / c->cfg.N;
+    const double dc = coeff * c->cfg.radius * hx;
+    return -1.0 * ((dc * dc) * (dc * dc));
+}
+
+// y: the state (read; updated in place unless out), out: the tendency (apply).
+template <class T>
+static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, double uv_coeff, double h_coeff)
+{
+    int rc = dif_setup<T>(c);
+    if (rc) return rc;
+    const int N = c->cfg.N, n = N + 1, M = c->cfg.n_members;
+    const Dims d = c->dims;
+    const size_t set = (size_t)M * DIF_FIELDS * NPAN * d.ps;
+    T *X = (T *)c->dif, *D1X = X + set, *D1Y = X + 2 * set, *R = X + 3 * set, *A = X + 4 * set;
+    const AhView<T> &av = ah_view<T>(c);
+    const MetricView<T> &mv = metric_view<T>(c);
+    const double hxa = 0.5 * 3.141592653589793238462643383279502884 / N * c->cfg.radius;
+    const DifView<T> dv{(const T *)c->dif_b, hxa * hxa};
+    const dim3 pb(32, 8), pm((n + 31) / 32, (n + 7) / 8, NPAN * M), pf((n + 31) / 32, (n + 7) / 8, NPAN * M * DIF_FIELDS);
+    const dim3 sg((4 * N + 255) / 256, 1, NPAN * M * DIF_FIELDS);
+    launch_k(k_dif_prep<T>, pm, pb, 0, c->stream, (const T *)y, X, d, dv);
+    // L(X) -> A, then L(A) -> X
+    T *src = X, *dst = A;
+    for (int pass = 0; pass < 2; pass++) {
+        launch_k(k_dif_d1<T>, pf, pb, 0, c->stream, (const T *)src, D1X, D1Y, d, av);
+        launch_k(k_dif_lap<T>, pf, pb, 0, c->stream, (const T *)src, (const T *)D1X, (const T *)D1Y, R, dst, d, av, dv);
+        launch_k(k_dif_sync<T>, sg, dim3(256), 0, c->stream, (const T *)R, dst, d);
+        std::swap(src, dst);
+    }
+    launch_k(k_dif_vraw<T>, pm, pb, 0, c->stream, (const T *)X, D1X, D1Y, d, dv, T(dif_coeff(c, uv_coeff)));
+    if (out)
+        launch_k(k_dif_update<T, true>, pm, pb, 0, c->stream, y, out, (const T *)X, (const T *)D1X, (const T *)D1Y, d, mv,
+                 T(dif_coeff(c, h_coeff)), T(0));
+    else
+        launch_k(k_dif_update<T, false>, pm, pb, 0, c->stream, y, (T *)nullptr, (const T *)X, (const T *)D1X,
+                 (const T *)D1Y, d, mv, T(dif_coeff(c, h_coeff)), T(dt));
+    c->launches += 9;
+    return SWE_OK;
+}
+
+static int diffusion_check(swe_ctx *c, int lap_order, const char *what)
+{
+    if (!c->ah)
+        return fail(c, SWE_EINVAL,
+                    "%s: the reference's narrow-Laplacian diffusion (hordiff_*_Ah_sbp_*_narrow) acts on the Ah "
+                    "staggering; this context is not Ah",
+                    what);
+    if (lap_order != 21)
+        return fail(c, SWE_EINVAL, "%s: the _sbp_%d_narrow diffusion is not built (the _sbp_21_narrow one is)", what,
+                    lap_order);
+    return SWE_OK;
+}
+
+extern "C" int swe_diffusion_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin, int lap_order, double uv_coeff,
+                                   double h_coeff)
+{
+    if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
+    int rc = diffusion_check(c, lap_order, "swe_diffusion_apply");
+    if (rc) return rc;
+    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)vin->d, (double *)vout->d, 0.0, uv_coeff, h_coeff)
+                      : enqueue_diffusion<float>(c, (float *)vin->d, (float *)vout->d, 0.0, uv_coeff, h_coeff);
+    if (rc) return rc;
+    CU_LAUNCHED(c);
+    return SWE_OK;
+}
+
+extern "C" int swe_diffusion_step(swe_ctx *c, swe_stvec *v, double dt, int lap_order, double uv_coeff, double h_coeff)
+{
+    if (!c || !v || v->ctx != c) return SWE_EINVAL;
+    int rc = diffusion_check(c, lap_order, "swe_diffusion_step");
+    if (rc) return rc;
+    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)v->d, nullptr, dt, uv_coeff, h_coeff)
+                      : enqueue_diffusion<float>(c, (float *)v->d, nullptr, dt, uv_coeff, h_coeff);
+    if (rc) return rc;
+    CU_LAUNCHED(c);
+    return SWE_OK;
 }
 
 extern "C" int swe_integrals(swe_ctx *c, const swe_stvec *vec, int member, double *mass, double *energy)

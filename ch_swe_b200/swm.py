@@ -559,10 +559,61 @@ def create_group(domains) -> DomainGroup:
     return DomainGroup(domains)
 
 
+class OperatorSwmDiff:
+    """operator_swm_diff_t (operator_swm_diff_mod.f90:27-49): hordiff_uv on (u, v) and hordiff
+    on h, the narrow-Laplacian diffusion of the Ah staggering."""
+
+    def __init__(self, domain: Domain, lap_order: int, uv_coeff: float, h_coeff: float):
+        self.domain = domain
+        self.lap_order = int(lap_order)
+        self.uv_coeff = float(uv_coeff)
+        self.h_coeff = float(h_coeff)
+
+    def apply(self, vout: StvecSwm, vin: StvecSwm, domain: Domain | None = None):
+        if not isinstance(vout, StvecSwm) or not isinstance(vin, StvecSwm):
+            raise ValueError("swm operator failure: vin or vout of wrong type")
+        check(_lib.load().swe_diffusion_apply(self.domain.ctx, vout.handle, vin.handle, self.lap_order,
+                                              self.uv_coeff, self.h_coeff), self.domain.ctx, "diffusion apply")
+
+
+def create_swm_diff_operator(config: dict, domain: Domain) -> OperatorSwmDiff:
+    """operator_swm_diff_factory_mod.f90:11-36 with the hordiff names of the Ah staggering
+    (hordiff_factory_mod.f90:33-44,61-68): hordiff_uv_name 'hordiff_vec_xyz_Ah_sbp_21_narrow'
+    with uv_diff_coeff, hordiff_h_name 'hordiff_scalar_Ah_sbp_21_narrow' with h_diff_coeff."""
+    if domain.horizontal_staggering != "Ah":
+        raise ValueError("the narrow-Laplacian diffusion operators need a domain created with "
+                         "horizontal_staggering='Ah'")
+    uv, h = config.get("hordiff_uv_name"), config.get("hordiff_h_name")
+    orders = set()
+    for name, prefix in ((uv, "hordiff_vec_xyz_Ah_sbp_"), (h, "hordiff_scalar_Ah_sbp_")):
+        if not (isinstance(name, str) and name.startswith(prefix) and name.endswith("_narrow")):
+            raise ValueError(f"unsupported hordiff operator: {name}")
+        orders.add(name[len(prefix):-len("_narrow")])
+    if orders != {"21"}:
+        raise ValueError(f"hordiff operators {uv}, {h}: the _sbp_21_narrow pair is built")
+    return OperatorSwmDiff(domain, 21, config.get("uv_diff_coeff", 0.0), config.get("h_diff_coeff", 0.0))
+
+
+class ExplicitEul1:
+    """explicit_Eul1_t (explicit_Eul1_mod.f90:20-28): v0 += dt operator(v0)."""
+
+    def step(self, v0: StvecSwm, operator, domain: Domain | None, dt: float):
+        if isinstance(operator, OperatorSwmDiff):
+            check(_lib.load().swe_diffusion_step(operator.domain.ctx, v0.handle, float(dt), operator.lap_order,
+                                                 operator.uv_coeff, operator.h_coeff), operator.domain.ctx,
+                  "diffusion step")
+            return
+        tend = v0.create_similar()
+        operator.apply(tend, v0, domain)
+        v0.update(float(dt), tend)
+
+
 def create_timescheme(state: StvecSwm, name: str):
-    if name != "rk4":
-        raise ValueError(f"unknown timescheme_name: {name}")
-    return Rk4()
+    if name == "rk4":
+        return Rk4()
+    if name == "explicit_Eul1":
+        return ExplicitEul1()
+    raise ValueError(f"unknown timescheme_name: {name}")
 
 
 def edge_links() -> np.ndarray:

@@ -183,6 +183,21 @@ int swe_group_rk4_steps_members(swe_group *g, swe_stvec *const *states, const do
 int swe_group_synchronize(swe_group *g);
 const char *swe_group_last_error(const swe_group *g);
 long long swe_group_launch_count(const swe_group *g);
+/* Horizontal diffusion of an Ah context (every member):
+     swe_diffusion_apply <- operator_swm_diff_t%apply(vout, vin, domain)
+                            src/models/shallow_water/operator/operator_swm_diff_mod.f90:27-49
+     swe_diffusion_step  <- explicit_Eul1_t%step(v, operator_diff, domain, dt), the diffusion
+                            step after each dynamics step (shallow_water_mod.f90:95-100,117-118;
+                            src/time_schemes/explicit_Eul1_mod.f90:20-28): v += dt tendency
+   with hordiff_vec_xyz_Ah_sbp_<lap_order>_narrow (coefficient uv_coeff) for u, v and
+   hordiff_scalar_Ah_sbp_<lap_order>_narrow (h_coeff) for h
+   (src/differential_operators/horizontal/hordiff/hordiff_factory_mod.f90:33-44,61-68):
+   tendency -(coeff a hx)^4 L(L(f)) of h and of the wind's Cartesian components, L the
+   narrow SBP Laplacian (src/differential_operators/horizontal/laplace/laplace_Ah_sbp21_narrow_mod.f90).
+   lap_order 21 is built; other orders and non-Ah contexts return SWE_EINVAL.  vout != vin. */
+int swe_diffusion_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin, int lap_order, double uv_coeff,
+                        double h_coeff);
+int swe_diffusion_step(swe_ctx *ctx, swe_stvec *v, double dt, int lap_order, double uv_coeff, double h_coeff);
 /* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
 int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
 

@@ -77,6 +77,10 @@ def lib():
         L.orc_ah_apply.argtypes = [ctypes.c_void_p] + [_dp] * 6
         L.orc_ah_rk4.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int]
         L.orc_ah_integrals.argtypes = [ctypes.c_void_p] + [_dp] * 5
+        L.orc_diff_apply.argtypes = [ctypes.c_void_p] + [_dp] * 6 + [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.orc_lap_ah.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+        L.orc_diff_step.argtypes = [ctypes.c_void_p] + [_dp] * 3 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                                  ctypes.c_double, ctypes.c_int]
         L.orc_latlon_vec.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_latlon_xy.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
         L.orc_latlon_o.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp]
@@ -152,6 +156,32 @@ class Oracle:
     def ah_rk4(self, h, u, v, dt: float, nsteps: int):
         a = [np.array(x, dtype=np.float64, order="C") for x in (h, u, v)]
         lib().orc_ah_rk4(self._c, *(_p(x) for x in a), float(dt), int(nsteps))
+        return tuple(a)
+
+    # diffusion on the Ah staggering (hordiff_vec_xyz_Ah_sbp_21_narrow for u, v and
+    # hordiff_scalar_Ah_sbp_21_narrow for h; lap_order 21)
+    def diff_apply(self, h, u, v, uv_coeff: float, h_coeff: float, lap_order: int = 21):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (h, u, v)]
+        out = [np.zeros_like(a[0]) for _ in range(3)]
+        rc = lib().orc_diff_apply(self._c, *(_p(x) for x in a), *(_p(x) for x in out), int(lap_order),
+                                  float(uv_coeff), float(h_coeff))
+        if rc != 0:
+            raise ValueError(f"no {lap_order} narrow Laplacian diffusion in the oracle")
+        return tuple(out)
+
+    def lap_ah(self, f, lap_order: int = 21):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros_like(a)
+        if lib().orc_lap_ah(self._c, _p(a), _p(out), int(lap_order)) != 0:
+            raise ValueError(f"no {lap_order} narrow Laplacian in the oracle")
+        return out
+
+    def diff_step(self, h, u, v, dt: float, uv_coeff: float, h_coeff: float, nsteps: int = 1, lap_order: int = 21):
+        a = [np.array(x, dtype=np.float64, order="C") for x in (h, u, v)]
+        rc = lib().orc_diff_step(self._c, *(_p(x) for x in a), float(dt), int(lap_order), float(uv_coeff),
+                                 float(h_coeff), int(nsteps))
+        if rc != 0:
+            raise ValueError(f"no {lap_order} narrow Laplacian diffusion in the oracle")
         return tuple(a)
 
     def ah_integrals(self, h, u, v):

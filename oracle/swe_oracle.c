@@ -461,6 +461,7 @@ typedef struct {
     double shift_i, shift_j, hx, hy;
     double *J, *Q1, *Q2, *Q3, *rx, *ry, *rz; /* [t][j][i] interior, 1-based mapped to 0 */
     double *a1, *a2;                         /* [t][j][i][3] */
+    double *b1, *b2;                         /* contravariant basis, [t][j][i][3] */
     double *Ax, *Ay;                         /* SBP norm weights */
 } mesh_t;
 
@@ -545,6 +546,7 @@ static void mesh_build(mesh_t *m, int N, double shift_i, double shift_j)
     m->Q2 = malloc(sizeof(double) * n); m->Q3 = malloc(sizeof(double) * n);
     m->rx = malloc(sizeof(double) * n); m->ry = malloc(sizeof(double) * n); m->rz = malloc(sizeof(double) * n);
     m->a1 = malloc(sizeof(double) * n * 3); m->a2 = malloc(sizeof(double) * n * 3);
+    m->b1 = malloc(sizeof(double) * n * 3); m->b2 = malloc(sizeof(double) * n * 3);
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= m->ny; j++) {
             double beta = alpha0 + (j - 1 + shift_j) * m->hy;
@@ -564,6 +566,11 @@ static void mesh_build(mesh_t *m, int N, double shift_i, double shift_j)
                                  (1.0 + pow(ta, 2.0)) * (1.0 + pow(tb, 2.0)) / s15, -tb * (1.0 + pow(tb, 2.0)) / s15};
                 proto2real(t, a1p, &m->a1[3 * k]);
                 proto2real(t, a2p, &m->a2[3 * k]);
+                double bp[3];
+                b1_proto(alpha, beta, bp);
+                proto2real(t, bp, &m->b1[3 * k]);
+                b2_proto(alpha, beta, bp);
+                proto2real(t, bp, &m->b2[3 * k]);
                 double s2 = sigm * sigm;
                 m->Q1[k] = s2 / (1.0 + ta * ta);
                 m->Q2[k] = s2 * ta * tb / ((1 + ta * ta) * (1 + tb * tb));
@@ -579,7 +586,7 @@ static void mesh_build(mesh_t *m, int N, double shift_i, double shift_j)
 static void mesh_free(mesh_t *m)
 {
     free(m->J); free(m->Q1); free(m->Q2); free(m->Q3); free(m->rx); free(m->ry); free(m->rz);
-    free(m->a1); free(m->a2); free(m->Ax); free(m->Ay);
+    free(m->a1); free(m->a2); free(m->b1); free(m->b2); free(m->Ax); free(m->Ay);
 }
 
 /* ------------------------------------------------------------------ */
@@ -897,6 +904,8 @@ typedef struct orc_ctx {
     int ah;
     double *fxy;                 /* Coriolis parameter on xy, [t][j][i] */
     fld_t ah_u, ah_v, ah_du, ah_dv, ah_gx, ah_gy, ah_ut, ah_vt, ah_Ju, ah_Jv, ah_y[3], ah_k[4][3];
+    /* diffusion on the Ah staggering (allocated on first use) */
+    fld_t df_d1x, df_d1y, df_d2x, df_d2y, df_dxy, df_dyx, df_x[3], df_t[3];
 } orc_ctx;
 
 /* calc_coriolis_parameter (coriolis_factory_mod.f90:239-280) at point k of mesh m */
@@ -1025,6 +1034,9 @@ void orc_destroy(orc_ctx *c)
                     &c->ah_y[0], &c->ah_y[1], &c->ah_y[2]};
     for (unsigned q = 0; q < sizeof(all) / sizeof(all[0]); q++) fld_free(all[q]);
     for (int s = 0; s < 4; s++) for (int f = 0; f < 3; f++) { fld_free(&c->k[s][f]); fld_free(&c->ah_k[s][f]); }
+    fld_t *df[] = {&c->df_d1x, &c->df_d1y, &c->df_d2x, &c->df_d2y, &c->df_dxy, &c->df_dyx,
+                   &c->df_x[0], &c->df_x[1], &c->df_x[2], &c->df_t[0], &c->df_t[1], &c->df_t[2]};
+    for (unsigned q = 0; q < sizeof(df) / sizeof(df[0]); q++) fld_free(df[q]);
     free(c);
 }
 
@@ -1852,6 +1864,164 @@ static void op_apply_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, f
             for (int i = 1; i <= n; i++) FA(dh, t, i, j) = -c->H * FA(&c->div, t, i, j);
 }
 
+/* ---- diffusion on the Ah staggering: operator_swm_diff_t%apply (operator_swm_diff_mod.f90:27-49)
+   with hordiff_vec_xyz_Ah_sbp_21_narrow for (u, v) and hordiff_scalar_Ah_sbp_21_narrow for h
+   (hordiff_factory_mod.f90:33-34,61-62), stepped by explicit_Eul1 (explicit_Eul1_mod.f90:20-28)
+   after each step of the dynamics (shallow_water_mod.f90:95-100,117-118) ---- */
+
+static void diff_alloc(orc_ctx *c)
+{
+    if (c->df_d1x.p) return;
+    const int n = c->N + 1, hw = 2;
+    fld_t *df[] = {&c->df_d1x, &c->df_d1y, &c->df_d2x, &c->df_d2y, &c->df_dxy, &c->df_dyx,
+                   &c->df_x[0], &c->df_x[1], &c->df_x[2], &c->df_t[0], &c->df_t[1], &c->df_t[2]};
+    for (unsigned q = 0; q < sizeof(df) / sizeof(df[0]); q++) fld_init(df[q], n, n, hw);
+}
+
+/* laplace_Ah_sbp21_narrow_t%calc_laplace (laplace_Ah_sbp21_narrow_mod.f90:25-56) with
+   calc_tile_d1x_d1y (:58-85) and calc_laplace_tile (:86-239): the narrow second differences
+   with the variable coefficients Qi11 J and Qi22 J, the mixed terms D1(Qi12 J D1 f), the
+   boundary penalties (all four added to d2f_x, as the reference does), the division by
+   (hx a)^2 and by J, then the Ah scalar sync.  out may be f.  The halo exchanges of f,
+   d1f_x and d1f_y ahead of the tile sweeps feed no stencil (every difference is one-sided
+   at the panel edges) and are left out. */
+static void lap_ah21(orc_ctx *c, fld_t *out, fld_t *f)
+{
+    const int n = c->N + 1;
+    const mesh_t *m = &c->mxy;
+    fld_t *d1x = &c->df_d1x, *d1y = &c->df_d1y, *d2x = &c->df_d2x, *d2y = &c->df_d2y;
+    fld_t *dxy = &c->df_dxy, *dyx = &c->df_dyx;
+#define BX(i, j) (m->Q1[MI(m, t, i, j)] * m->J[MI(m, t, i, j)])
+#define BY(i, j) (m->Q3[MI(m, t, i, j)] * m->J[MI(m, t, i, j)])
+    for (int t = 0; t < NPAN; t++) {
+        diff_n2n(d1x, f, t, 0, n, 1, n, 21);
+        diff_n2n(d1y, f, t, 1, n, 1, n, 21);
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                FA(d1x, t, i, j) = FA(d1x, t, i, j) * m->J[k] * m->Q2[k];
+                FA(d1y, t, i, j) = FA(d1y, t, i, j) * m->J[k] * m->Q2[k];
+            }
+    }
+    const double h2 = (m->hx * c->a) * (m->hx * c->a);
+    for (int t = 0; t < NPAN; t++) {
+        for (int j = 1; j <= n; j++) {
+            double bc = BX(1, j), bp = BX(2, j);
+            double cc = -(bc + bp), cp = +(bc + bp);
+            FA(d2x, t, 1, j) = (cc * FA(f, t, 1, j) + cp * FA(f, t, 2, j));
+            for (int i = 2; i <= n - 1; i++) {
+                const double bm = BX(i - 1, j);
+                bc = BX(i, j); bp = BX(i + 1, j);
+                const double cm = (bm + bc) / 2;
+                cc = -(bm + 2 * bc + bp) / 2;
+                cp = (bp + bc) / 2;
+                FA(d2x, t, i, j) = (cp * FA(f, t, i + 1, j) + cc * FA(f, t, i, j) + cm * FA(f, t, i - 1, j));
+            }
+            bc = BX(n, j);
+            const double bm = BX(n - 1, j);
+            cc = -(bc + bm);
+            const double cm = +(bc + bm);
+            FA(d2x, t, n, j) = cm * FA(f, t, n - 1, j) + cc * FA(f, t, n, j);
+        }
+        for (int i = 1; i <= n; i++) {
+            const double bc = BY(i, 1), bp = BY(i, 2);
+            const double cc = -(bc + bp), cp = +(bc + bp);
+            FA(d2y, t, i, 1) = cc * FA(f, t, i, 1) + cp * FA(f, t, i, 2);
+        }
+        for (int j = 2; j <= n - 1; j++)
+            for (int i = 1; i <= n; i++) {
+                const double bm = BY(i, j - 1), bc = BY(i, j), bp = BY(i, j + 1);
+                const double cm = (bm + bc) / 2, cc = -(bm + 2 * bc + bp) / 2, cp = (bp + bc) / 2;
+                FA(d2y, t, i, j) = (cp * FA(f, t, i, j + 1) + cc * FA(f, t, i, j) + cm * FA(f, t, i, j - 1));
+            }
+        for (int i = 1; i <= n; i++) {
+            const double bc = BY(i, n), bm = BY(i, n - 1);
+            const double cc = -(bc + bm), cm = +(bc + bm);
+            FA(d2y, t, i, n) = cm * FA(f, t, i, n - 1) + cc * FA(f, t, i, n);
+        }
+        for (int j = 1; j <= n; j++) {
+            const double penalty = 2.0 * (-2.0 * FA(d1y, t, 1, j));
+            FA(d2x, t, 1, j) = FA(d2x, t, 1, j) - 0.5 * penalty;
+        }
+        for (int j = 1; j <= n; j++) {
+            const double penalty = 2.0 * (2 * FA(d1y, t, n, j));
+            FA(d2x, t, n, j) = FA(d2x, t, n, j) - 0.5 * penalty;
+        }
+        for (int i = 1; i <= n; i++) {
+            const double penalty = 2.0 * (-2 * FA(d1x, t, i, 1));
+            FA(d2x, t, i, 1) = FA(d2x, t, i, 1) - 0.5 * penalty;
+        }
+        for (int i = 1; i <= n; i++) {
+            const double penalty = 2.0 * (2 * FA(d1x, t, i, n));
+            FA(d2x, t, i, n) = FA(d2x, t, i, n) - 0.5 * penalty;
+        }
+        diff_n2n(dyx, d1x, t, 1, n, 1, n, 21);
+        diff_n2n(dxy, d1y, t, 0, n, 1, n, 21);
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                double v = 1.0 * FA(d2x, t, i, j) + 1.0 * FA(d2y, t, i, j);
+                v = v + 1.0 * FA(dxy, t, i, j) + 1.0 * FA(dyx, t, i, j);
+                FA(out, t, i, j) = v / h2;
+            }
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) FA(out, t, i, j) = FA(out, t, i, j) / m->J[MI(m, t, i, j)];
+    }
+#undef BX
+#undef BY
+    exch_do(&c->ex_xy1_full_s, out, NULL);
+    for (int t = 0; t < NPAN; t++) sync_ah_scalar(c, out, t);
+}
+
+/* hordiff_scalar_t%calc_diff (hordiff_scalar_mod.f90:30-50), diff_order 2 with
+   diff_coeff = coeff a hx (hordiff_factory_mod.f90:276-298): tend = -(coeff a hx)^4 L(L(f)).
+   f_work receives the iterate (it may be f). */
+static void hordiff_ah21(orc_ctx *c, fld_t *tend, fld_t *f, fld_t *work, double coeff)
+{
+    const int n = c->N + 1;
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) FA(work, t, i, j) = 1.0 * FA(f, t, i, j);
+    lap_ah21(c, work, work);
+    lap_ah21(c, work, work);
+    const double dc = coeff * c->a * c->mxy.hx;
+    const double k = -1.0 * ((dc * dc) * (dc * dc));
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) FA(tend, t, i, j) = k * FA(work, t, i, j);
+}
+
+/* operator_swm_diff_t%apply: (du, dv) by hordiff_colocated_xyz_t%calc_diff_vec_xyz
+   (hordiff_colocated_mod.f90:42-58: covariant components to Cartesian with the contravariant
+   basis, the scalar diffusion of each Cartesian component, back with the same basis as
+   cart2cube_vec does for covariant components, vec_math_mod.f90:196-219, then the covariant
+   ECS Ah vector sync), dh by the scalar diffusion */
+static void op_diff_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v, double uv_coeff,
+                       double h_coeff)
+{
+    const int n = c->N + 1;
+    const mesh_t *m = &c->mxy;
+    diff_alloc(c);
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                for (int d = 0; d < 3; d++)
+                    FA(&c->df_x[d], t, i, j) = m->b1[3 * k + d] * FA(u, t, i, j) + m->b2[3 * k + d] * FA(v, t, i, j);
+            }
+    for (int d = 0; d < 3; d++) hordiff_ah21(c, &c->df_t[d], &c->df_x[d], &c->df_x[d], uv_coeff);
+    for (int t = 0; t < NPAN; t++)
+        for (int j = 1; j <= n; j++)
+            for (int i = 1; i <= n; i++) {
+                const size_t k = MI(m, t, i, j);
+                const double tx = FA(&c->df_t[0], t, i, j), ty = FA(&c->df_t[1], t, i, j), tz = FA(&c->df_t[2], t, i, j);
+                FA(du, t, i, j) = tx * m->b1[3 * k] + ty * m->b1[3 * k + 1] + tz * m->b1[3 * k + 2];
+                FA(dv, t, i, j) = tx * m->b2[3 * k] + ty * m->b2[3 * k + 1] + tz * m->b2[3 * k + 2];
+            }
+    exch_do(&c->ex_xy1_cross_v, du, dv);
+    for (int t = 0; t < NPAN; t++) sync_grad_on_edges(c, dv, du, t);
+    hordiff_ah21(c, dh, h, &c->df_x[0], h_coeff);
+}
+
 /* stvec assign/update over interior points (grid_field_mod.f90:442-534) */
 static void st_assign2(fld_t *y[3], double s1, fld_t *a[3], double s2, fld_t *b[3])
 {
@@ -2389,6 +2559,44 @@ void orc_ah_apply(orc_ctx *c, const double *h, const double *u, const double *v,
     fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
     op_apply_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v);
     fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
+}
+/* the diffusion operator's tendency (lap_order 21: the _sbp_21_narrow operators) */
+int orc_diff_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv,
+                   int lap_order, double uv_coeff, double h_coeff)
+{
+    if (lap_order != 21) return -1;
+    fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
+    op_diff_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v, uv_coeff, h_coeff);
+    fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
+    return 0;
+}
+/* the narrow Laplacian alone (laplace_Ah_sbp<lap_order>_narrow), for tests of the operator */
+int orc_lap_ah(orc_ctx *c, const double *f, double *out, int lap_order)
+{
+    if (lap_order != 21) return -1;
+    diff_alloc(c);
+    fld_from_packed(&c->df_x[0], f);
+    lap_ah21(c, &c->df_t[0], &c->df_x[0]);
+    fld_to_packed(&c->df_t[0], out);
+    return 0;
+}
+/* nsteps explicit_Eul1 steps of the diffusion: v0 = v0 + dt tend (stvec update_s1v1) */
+int orc_diff_step(orc_ctx *c, double *h, double *u, double *v, double dt, int lap_order, double uv_coeff,
+                  double h_coeff, int nsteps)
+{
+    if (lap_order != 21) return -1;
+    const int n = c->N + 1;
+    fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
+    fld_t *y[3] = {&c->h, &c->ah_u, &c->ah_v}, *k[3] = {&c->dh, &c->ah_du, &c->ah_dv};
+    for (int s = 0; s < nsteps; s++) {
+        op_diff_ah(c, k[0], k[1], k[2], y[0], y[1], y[2], uv_coeff, h_coeff);
+        for (int f = 0; f < 3; f++)
+            for (int t = 0; t < NPAN; t++)
+                for (int j = 1; j <= n; j++)
+                    for (int i = 1; i <= n; i++) FA(y[f], t, i, j) = FA(y[f], t, i, j) + dt * FA(k[f], t, i, j);
+    }
+    fld_to_packed(&c->h, h); fld_to_packed(&c->ah_u, u); fld_to_packed(&c->ah_v, v);
+    return 0;
 }
 void orc_ah_rk4(orc_ctx *c, double *h, double *u, double *v, double dt, int nsteps)
 {

@@ -1,0 +1,117 @@
+"""The oracle's diffusion on the Ah staggering (laplace_Ah_sbp21_narrow,
+hordiff_scalar_Ah_sbp_21_narrow, hordiff_vec_xyz_Ah_sbp_21_narrow, explicit_Eul1), pinned
+by properties that a wrong metric factor, penalty sign, stencil offset or sync order
+breaks: the narrow SBP Laplacian is self-adjoint and negative semi-definite in the
+J-weighted SBP 2-1 node quadrature and conserves mass (continuous fields: the
+duplicated panel-edge vertices agree), kills constants, and converges to the
+spherical Laplacian (second order inside the panels, first order on their edges; the
+cube corners keep an O(1) error of the panel-wise operator); the scalar tendency is
+-(c a hx)^4 L(L(h)); the wind's follows the Cartesian components; one Euler step is
+v + dt tendency."""
+import numpy as np
+import pytest
+
+from oracle.oracle import EARTH_RADIUS, Oracle
+
+A = EARTH_RADIUS
+
+
+def smooth_field(o, seed):
+    """A random smooth function of the position: equal on the duplicated vertices."""
+    rng = np.random.default_rng(seed)
+    x, y, z = o.metric(0, 5), o.metric(0, 6), o.metric(0, 7)
+    f = np.zeros_like(x)
+    for _ in range(4):
+        k = rng.normal(size=3) * 2.0
+        f += rng.normal() * np.sin(k[0] * x + k[1] * y + k[2] * z + rng.uniform(0, 2 * np.pi))
+    return f
+
+
+def quad_weights(o):
+    n = o.N + 1
+    w1 = np.ones(n)
+    w1[0] = w1[-1] = 0.5   # Q21_A (sbp_operators_collection_mod.f90:22)
+    return o.metric(0, 0) * w1[None, :, None] * w1[None, None, :]
+
+
+@pytest.fixture(scope="module")
+def orc(oracle_built):
+    return Oracle(16)
+
+
+def test_laplacian_kills_constants(orc):
+    L = orc.lap_ah(np.full((6, 17, 17), 7.5))
+    assert np.abs(L).max() * A * A / 7.5 < 1e-9
+
+
+@pytest.mark.parametrize("N", [8, 13, 16])
+def test_laplacian_self_adjoint_negative_and_conservative(N, oracle_built):
+    o = Oracle(N)
+    w = quad_weights(o)
+    f, g = smooth_field(o, 1), smooth_field(o, 2)
+    Lf, Lg = o.lap_ah(f), o.lap_ah(g)
+    s1, s2 = (w * g * Lf).sum(), (w * f * Lg).sum()
+    assert abs(s1 - s2) / abs(s1) < 1e-12
+    assert abs((w * Lf).sum()) / np.abs(w * Lf).sum() < 1e-12
+    assert (w * f * Lf).sum() < 0 and (w * g * Lg).sum() < 0
+
+
+def test_laplacian_converges_to_spherical_laplacian(oracle_built):
+    err = {}
+    for N in (16, 32):
+        o = Oracle(N)
+        z = o.metric(0, 7)
+        e = (o.lap_ah(z) + 2.0 / A ** 2 * z) / (2.0 / A ** 2)
+        inner = np.abs(e[:, 1:-1, 1:-1]).max()
+        edges = np.abs(np.concatenate([e[:, 0, 1:-1].ravel(), e[:, -1, 1:-1].ravel(),
+                                       e[:, 1:-1, 0].ravel(), e[:, 1:-1, -1].ravel()])).max()
+        err[N] = (inner, edges)
+    assert err[32][0] / err[16][0] < 0.3      # second order inside the panels
+    assert err[32][1] / err[16][1] < 0.6      # first order on the panel edges
+    assert err[32][0] < 1e-3
+
+
+def test_scalar_diffusion_is_minus_c4_bilaplacian(orc):
+    o = orc
+    h = smooth_field(o, 5) * 100.0
+    c = 0.01
+    dh, du, dv = o.diff_apply(h, np.zeros_like(h), np.zeros_like(h), uv_coeff=0.03, h_coeff=c)
+    dc = c * A * (0.5 * np.pi / o.N)
+    want = -1.0 * ((dc * dc) * (dc * dc)) * o.lap_ah(o.lap_ah(h))
+    assert np.abs(dh - want).max() <= 1e-14 * np.abs(want).max()
+    assert np.abs(du).max() == 0.0 and np.abs(dv).max() == 0.0
+
+
+def test_vector_diffusion_of_solid_rotation(oracle_built):
+    """The Cartesian components of a solid rotation are first-degree harmonics: L(L(V)) =
+    4 V / a^4 up to discretisation error, so (du, dv) -> -4 (c hx)^4 (V.b1, V.b2), and
+    V.b1 = Qi11 u + Qi12 v, V.b2 = Qi12 u + Qi22 v for covariant (u, v)."""
+    from ch_swe_b200.testcases import williamson2
+    err = []
+    for N in (16, 32):
+        o = Oracle(N)
+        h, u, v = williamson2(N, staggering="Ah")
+        c = 0.03
+        _, du, dv = o.diff_apply(h, u, v, uv_coeff=c, h_coeff=0.0)
+        k = -4.0 * (c * 0.5 * np.pi / N) ** 4
+        Q1, Q2, Q3 = o.metric(0, 1), o.metric(0, 2), o.metric(0, 3)
+        wu, wv = k * (Q1 * u + Q2 * v), k * (Q2 * u + Q3 * v)
+        s = max(np.abs(wu).max(), np.abs(wv).max())
+        err.append(max(np.abs(du - wu)[:, 2:-2, 2:-2].max(), np.abs(dv - wv)[:, 2:-2, 2:-2].max()) / s)
+    assert err[1] < 0.05 and err[1] / err[0] < 0.6
+
+
+def test_euler_step_is_state_plus_dt_tendency(orc):
+    o = orc
+    rng = np.random.default_rng(9)
+    st = tuple(smooth_field(o, s) * m + 0.01 * rng.standard_normal((6, 17, 17)) for s, m in ((11, 50.0), (12, 10.0),
+                                                                                                (13, 10.0)))
+    t = o.diff_apply(*st, uv_coeff=0.03, h_coeff=0.01)
+    out = o.diff_step(*st, dt=600.0, uv_coeff=0.03, h_coeff=0.01, nsteps=1)
+    for a, x, d in zip(out, st, t):
+        assert np.array_equal(a, x + 600.0 * d)
+
+
+def test_other_orders_refused(orc):
+    with pytest.raises(ValueError):
+        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=42)
