@@ -2071,8 +2071,10 @@ static int dif_setup(swe_ctx *c)
     const int N = c->cfg.N, n = N + 1, P = c->dims.P;
     const size_t box = (size_t)c->dims.ps, M = (size_t)c->cfg.n_members;
     if (!c->dif_b) {
-        // b1, b2 of the equiangular vertices on each panel (metric_2d_ecs_mod.f90:377-395)
-        std::vector<T> h((size_t)NPAN * 6 * box, T(0));
+        // b1, b2 of the equiangular vertices on each panel (metric_2d_ecs_mod.f90:377-395),
+        // then the 4-2 closure blocks of every boundary line
+        const size_t nb = (size_t)NPAN * 6 * box;
+        std::vector<T> h(nb + (size_t)2 * n * 2 * 48, T(0));
         const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
         for (int p = 0; p < NPAN; p++)
             for (int j = 1; j <= n; j++)
@@ -2089,6 +2091,24 @@ static int dif_setup(swe_ctx *c)
                         h[((size_t)p * 6 + 3 + k) * box + o] = T(b2[k]);
                     }
                 }
+        if (N >= 11) {
+            double D[6][8][8];
+            lap42_dense(D);
+            const HostMetric mxy = host_metric(N, 0.0, 0.0);
+            auto bq = [&](int dir, int line, int k) {   // Qi11 J at (k, line) or Qi22 J at (line, k)
+                const size_t q = dir == 0 ? (size_t)(line - 1) * n + (k - 1) : (size_t)(k - 1) * n + (line - 1);
+                return (dir == 0 ? mxy.Q1[q] : mxy.Q3[q]) * mxy.J[q];
+            };
+            for (int dir = 0; dir < 2; dir++)
+                for (int line = 1; line <= n; line++)
+                    for (int side = 0; side < 2; side++)
+                        for (int r = 0; r < 6; r++)
+                            for (int cc = 0; cc < 8; cc++) {
+                                double m = 0.0;
+                                for (int k = 1; k <= 8; k++) m = m + D[r][cc][k - 1] * bq(dir, line, side ? n + 1 - k : k);
+                                h[nb + (size_t)dif_m42_index(n, dir, line, side) + r * 8 + cc] = T(m);
+                            }
+        }
         if (cudaMalloc(&c->dif_b, h.size() * sizeof(T)) != cudaSuccess)
             return fail(c, SWE_ENOMEM, "diffusion basis allocation failed");
         CU(c, cudaMemcpy(c->dif_b, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
@@ -2109,7 +2129,7 @@ static double dif_coeff(const swe_ctx *c, double coeff)
 
 // y: the state (read; updated in place unless out), out: the tendency (apply).
 template <class T>
-static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, double uv_coeff, double h_coeff)
+static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, int lap_order, double uv_coeff, double h_coeff)
 {
     int rc = dif_setup<T>(c);
     if (rc) return rc;
@@ -2120,15 +2140,17 @@ static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, double uv_coef
     const AhView<T> &av = ah_view<T>(c);
     const MetricView<T> &mv = metric_view<T>(c);
     const double hxa = 0.5 * 3.141592653589793238462643383279502884 / N * c->cfg.radius;
-    const DifView<T> dv{(const T *)c->dif_b, hxa * hxa};
+    const DifView<T> dv{(const T *)c->dif_b, (const T *)c->dif_b + (size_t)NPAN * 6 * d.ps, hxa * hxa};
     const dim3 pb(32, 8), pm((n + 31) / 32, (n + 7) / 8, NPAN * M), pf((n + 31) / 32, (n + 7) / 8, NPAN * M * DIF_FIELDS);
     const dim3 sg((4 * N + 255) / 256, 1, NPAN * M * DIF_FIELDS);
     launch_k(k_dif_prep<T>, pm, pb, 0, c->stream, (const T *)y, X, d, dv);
     // L(X) -> A, then L(A) -> X
     T *src = X, *dst = A;
+    const bool o42 = lap_order == 42;
     for (int pass = 0; pass < 2; pass++) {
-        launch_k(k_dif_d1<T>, pf, pb, 0, c->stream, (const T *)src, D1X, D1Y, d, av);
-        launch_k(k_dif_lap<T>, pf, pb, 0, c->stream, (const T *)src, (const T *)D1X, (const T *)D1Y, R, dst, d, av, dv);
+        launch_k(o42 ? k_dif_d1<T, 42> : k_dif_d1<T, 21>, pf, pb, 0, c->stream, (const T *)src, D1X, D1Y, d, av);
+        launch_k(o42 ? k_dif_lap<T, 42> : k_dif_lap<T, 21>, pf, pb, 0, c->stream, (const T *)src, (const T *)D1X,
+                 (const T *)D1Y, R, dst, d, av, dv);
         launch_k(k_dif_sync<T>, sg, dim3(256), 0, c->stream, (const T *)R, dst, d);
         std::swap(src, dst);
     }
@@ -2150,9 +2172,11 @@ static int diffusion_check(swe_ctx *c, int lap_order, const char *what)
                     "%s: the reference's narrow-Laplacian diffusion (hordiff_*_Ah_sbp_*_narrow) acts on the Ah "
                     "staggering; this context is not Ah",
                     what);
-    if (lap_order != 21)
-        return fail(c, SWE_EINVAL, "%s: the _sbp_%d_narrow diffusion is not built (the _sbp_21_narrow one is)", what,
-                    lap_order);
+    if (lap_order != 21 && lap_order != 42)
+        return fail(c, SWE_EINVAL, "%s: the _sbp_%d_narrow diffusion is not built (the _sbp_21_narrow and "
+                    "_sbp_42_narrow ones are)", what, lap_order);
+    if (lap_order == 42 && c->cfg.N < 11)
+        return fail(c, SWE_EINVAL, "%s: the _sbp_42_narrow closure blocks of six rows overlap below N = 11", what);
     return SWE_OK;
 }
 
@@ -2162,8 +2186,9 @@ extern "C" int swe_diffusion_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec 
     if (!c || !vout || !vin || vout->ctx != c || vin->ctx != c || vout == vin) return SWE_EINVAL;
     int rc = diffusion_check(c, lap_order, "swe_diffusion_apply");
     if (rc) return rc;
-    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)vin->d, (double *)vout->d, 0.0, uv_coeff, h_coeff)
-                      : enqueue_diffusion<float>(c, (float *)vin->d, (float *)vout->d, 0.0, uv_coeff, h_coeff);
+    rc = c->elem == 8
+             ? enqueue_diffusion<double>(c, (double *)vin->d, (double *)vout->d, 0.0, lap_order, uv_coeff, h_coeff)
+             : enqueue_diffusion<float>(c, (float *)vin->d, (float *)vout->d, 0.0, lap_order, uv_coeff, h_coeff);
     if (rc) return rc;
     CU_LAUNCHED(c);
     return SWE_OK;
@@ -2174,8 +2199,8 @@ extern "C" int swe_diffusion_step(swe_ctx *c, swe_stvec *v, double dt, int lap_o
     if (!c || !v || v->ctx != c) return SWE_EINVAL;
     int rc = diffusion_check(c, lap_order, "swe_diffusion_step");
     if (rc) return rc;
-    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)v->d, nullptr, dt, uv_coeff, h_coeff)
-                      : enqueue_diffusion<float>(c, (float *)v->d, nullptr, dt, uv_coeff, h_coeff);
+    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)v->d, nullptr, dt, lap_order, uv_coeff, h_coeff)
+                      : enqueue_diffusion<float>(c, (float *)v->d, nullptr, dt, lap_order, uv_coeff, h_coeff);
     if (rc) return rc;
     CU_LAUNCHED(c);
     return SWE_OK;

@@ -1,16 +1,17 @@
 // swe_diff.cuh -- horizontal diffusion on the Ah staggering, the operator the reference
 // applies after each step of the dynamics (shallow_water_mod.f90:95-100,117-118;
-// operator_swm_diff_mod.f90:27-49) in its _sbp_21_narrow form
-// (hordiff_factory_mod.f90:33-34,61-62):
-//   h:     hordiff_scalar_Ah_sbp_21_narrow   tend = -(c a hx)^4 L(L(h))
-//   u, v:  hordiff_vec_xyz_Ah_sbp_21_narrow  the covariant wind to Cartesian components
+// operator_swm_diff_mod.f90:27-49) in its _sbp_21_narrow and _sbp_42_narrow forms
+// (hordiff_factory_mod.f90:33-38,61-66):
+//   h:     hordiff_scalar_Ah_sbp_<ord>_narrow   tend = -(c a hx)^4 L(L(h))
+//   u, v:  hordiff_vec_xyz_Ah_sbp_<ord>_narrow  the covariant wind to Cartesian components
 //          with the contravariant basis, the same scalar diffusion of each component,
 //          back with the same basis (as cart2cube_vec does for covariant components,
 //          vec_math_mod.f90:196-219), then the covariant ECS Ah vector sync
 //          (hordiff_colocated_mod.f90:42-58)
-// L is laplace_Ah_sbp21_narrow (laplace_Ah_sbp21_narrow_mod.f90:25-239): narrow second
-// differences with the variable coefficients Qi11 J, Qi22 J, the mixed terms
-// D1(Qi12 J D1 f), boundary penalties, / (hx a)^2 / J, and the Ah scalar sync.
+// L is laplace_Ah_sbp<ord>_narrow (laplace_Ah_sbp21_narrow_mod.f90:25-239,
+// laplace_Ah_sbp42_narrow_mod.f90:27-761): narrow second differences with the variable
+// coefficients Qi11 J, Qi22 J, the mixed terms D1(Qi12 J D1 f), boundary penalties,
+// / (hx a)^2 / J, and the Ah scalar sync.
 //
 // The four scalar fields of a member (h and the three Cartesian wind components) are
 // diffused together: scratch sets hold [member][field 0..3][panel][box], and every
@@ -26,18 +27,123 @@ namespace chswe {
 
 constexpr int DIF_FIELDS = 4;   // h, and the wind's x, y, z components
 
+// Closure rows 1..6 of the narrow SBP 4-2 second difference with a variable coefficient
+// (laplace_Ah_sbp42_narrow_mod.f90:121-262): entry m_rc (r <= c) of the symmetric boundary
+// block as sum_k w b_k over the coefficients b_k = Qi J at node k; row r of the difference
+// is -(1 / h_r) sum_c m_rc f_c with the node norm h_r, mirrored at the far end (:284-423).
+struct Lap42Term {
+    int r, c, k;
+    double w;
+};
+static constexpr Lap42Term LAP42_M[] = {
+    {1, 1, 1, 12.0 / 17.0}, {1, 1, 2, 59.0 / 192.0}, {1, 1, 3, 27010400129.0 / 345067064608.0},
+    {1, 1, 4, 69462376031.0 / 2070402387648.0}, {1, 2, 1, -59.0 / 68.0}, {1, 2, 3, -6025413881.0 / 21126554976.0},
+    {1, 2, 4, -537416663.0 / 7042184992.0}, {1, 3, 1, 2.0 / 17.0}, {1, 3, 2, -59.0 / 192.0},
+    {1, 3, 3, 2083938599.0 / 8024815456.0}, {1, 3, 4, 213318005.0 / 16049630912.0}, {1, 4, 1, 3.0 / 68.0},
+    {1, 4, 3, -1244724001.0 / 21126554976.0}, {1, 4, 4, 752806667.0 / 21126554976.0},
+    {1, 5, 3, 49579087.0 / 10149031312.0}, {1, 5, 4, -49579087.0 / 10149031312.0}, {1, 6, 3, 1.0 / 784.0},
+    {1, 6, 4, -1.0 / 784.0}, {2, 2, 1, 3481.0 / 3264.0}, {2, 2, 3, 9258282831623875.0 / 7669235228057664.0},
+    {2, 2, 4, 236024329996203.0 / 1278205871342944.0}, {2, 3, 1, -59.0 / 408.0},
+    {2, 3, 3, -29294615794607.0 / 29725717938208.0}, {2, 3, 4, -2944673881023.0 / 29725717938208.0},
+    {2, 4, 1, -59.0 / 1088.0}, {2, 4, 3, 260297319232891.0 / 2556411742685888.0},
+    {2, 4, 4, -60834186813841.0 / 1278205871342944.0}, {2, 5, 3, -1328188692663.0 / 37594290333616.0},
+    {2, 5, 4, 1328188692663.0 / 37594290333616.0}, {2, 6, 3, -8673.0 / 2904112.0}, {2, 6, 4, 8673.0 / 2904112.0},
+    {3, 3, 1, 1.0 / 51.0}, {3, 3, 2, 59.0 / 192.0}, {3, 3, 3, 378288882302546512209.0 / 270764341349677687456.0},
+    {3, 3, 4, 13777050223300597.0 / 26218083221499456.0}, {3, 3, 5, 564461.0 / 13384296.0}, {3, 4, 1, 1.0 / 136.0},
+    {3, 4, 3, -4836340090442187227.0 / 5525802884687299744.0}, {3, 4, 4, -17220493277981.0 / 89177153814624.0},
+    {3, 4, 5, -125059.0 / 743572.0}, {3, 5, 3, 1613976761032884305.0 / 7963657098519931984.0},
+    {3, 5, 4, -10532412077335.0 / 42840005263888.0}, {3, 5, 5, 564461.0 / 4461432.0},
+    {3, 6, 3, 33235054191.0 / 26452850508784.0}, {3, 6, 4, -960119.0 / 1280713392.0}, {3, 6, 5, -3391.0 / 6692148.0},
+    {4, 4, 1, 3.0 / 1088.0}, {4, 4, 3, 507284006600757858213.0 / 475219048083107777984.0},
+    {4, 4, 4, 1950062198436997.0 / 3834617614028832.0}, {4, 4, 5, 1869103.0 / 2230716.0}, {4, 4, 6, 1.0 / 24.0},
+    {4, 5, 3, -4959271814984644613.0 / 20965546238960637264.0}, {4, 5, 4, -15998714909649.0 / 37594290333616.0},
+    {4, 5, 5, -375177.0 / 743572.0}, {4, 5, 6, -1.0 / 6.0}, {4, 6, 3, 752806667.0 / 539854092016.0},
+    {4, 6, 4, 1063649.0 / 8712336.0}, {4, 6, 5, -368395.0 / 2230716.0}, {4, 6, 6, 1.0 / 8.0},
+    {5, 5, 3, 8386761355510099813.0 / 128413970713633903242.0}, {5, 5, 4, 2224717261773437.0 / 2763180339520776.0},
+    {5, 5, 5, 280535.0 / 371786.0}, {5, 5, 6, 5.0 / 6.0}, {5, 5, 7, 1.0 / 24.0},
+    {5, 6, 3, -13091810925.0 / 13226425254392.0}, {5, 6, 4, -35039615.0 / 213452232.0},
+    {5, 6, 5, -1118749.0 / 2230716.0}, {5, 6, 6, -1.0 / 2.0}, {5, 6, 7, -1.0 / 6.0}, {5, 7, 5, 1.0 / 8.0},
+    {5, 7, 6, -1.0 / 6.0}, {5, 7, 7, 1.0 / 8.0}, {6, 6, 3, 660204843.0 / 13226425254392.0},
+    {6, 6, 4, 3290636.0 / 80044587.0}, {6, 6, 5, 5580181.0 / 6692148.0}, {6, 6, 6, 3.0 / 4.0}, {6, 6, 7, 5.0 / 6.0},
+    {6, 6, 8, 1.0 / 24.0}, {6, 7, 5, -1.0 / 6.0}, {6, 7, 6, -1.0 / 2.0}, {6, 7, 7, -1.0 / 2.0},
+    {6, 7, 8, -1.0 / 6.0}, {6, 8, 6, 1.0 / 8.0}, {6, 8, 7, -1.0 / 6.0}, {6, 8, 8, 1.0 / 8.0}
+};
+// The block densely, [r-1][c-1][k-1] with both triangles.
+static inline void lap42_dense(double D[6][8][8])
+{
+    for (int r = 0; r < 6; r++)
+        for (int c = 0; c < 8; c++)
+            for (int k = 0; k < 8; k++) D[r][c][k] = 0.0;
+    for (const Lap42Term &q : LAP42_M) {
+        D[q.r - 1][q.c - 1][q.k - 1] = q.w;
+        if (q.c <= 6) D[q.c - 1][q.r - 1][q.k - 1] = q.w;
+    }
+}
+__host__ __device__ constexpr double lap42_h(int r)
+{
+    return r == 1 ? 17.0 / 48 : (r == 2 ? 59.0 / 48 : (r == 3 ? 43.0 / 48 : (r == 4 ? 49.0 / 48 : 1.0)));
+}
+
+// Row k of the narrow second difference of order ORD on a line of n nodes with the
+// coefficients b(1..n) (the d2f_x / d2f_y sweeps of calc_laplace_tile); M: the line's
+// closure blocks (near end, then far end) for the 4-2 order.
+template <class T, int ORD, class B, class F>
+__device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, const T *M)
+{
+    if constexpr (ORD == 21) {
+        if (k == 1) {
+            const T bc = b(1), bp = b(2);
+            return (-(bc + bp) * f(1) + (bc + bp) * f(2));
+        }
+        if (k == n) {
+            const T bc = b(n), bm = b(n - 1);
+            return (bc + bm) * f(n - 1) + (-(bc + bm)) * f(n);
+        }
+        const T bm = b(k - 1), bc = b(k), bp = b(k + 1);
+        const T cm = (bm + bc) / T(2), cc = -(bm + T(2) * bc + bp) / T(2), cp = (bp + bc) / T(2);
+        return (cp * f(k + 1) + cc * f(k) + cm * f(k - 1));
+    } else {
+        if (k >= 7 && k <= n - 6) {
+            const T bmm = b(k - 2), bm = b(k - 1), bc = b(k), bp = b(k + 1), bpp = b(k + 2);
+            const T cmm = T(1.0 / 6.0) * bm - T(1.0 / 8.0) * bmm - T(1.0 / 8.0) * bc;
+            const T cm = T(1.0 / 6.0) * bmm + T(1.0 / 6.0) * bp + T(1.0 / 2.0) * bm + T(1.0 / 2.0) * bc;
+            const T cc = -T(1.0 / 24.0) * bmm - T(5.0 / 6.0) * bm - T(5.0 / 6.0) * bp - T(1.0 / 24.0) * bpp -
+                         T(3.0 / 4.0) * bc;
+            const T cp = T(1.0 / 6.0) * bm + T(1.0 / 6.0) * bpp + T(1.0 / 2.0) * bc + T(1.0 / 2.0) * bp;
+            const T cpp = T(1.0 / 6.0) * bp - T(1.0 / 8.0) * bc - T(1.0 / 8.0) * bpp;
+            return (cmm * f(k - 2) + cm * f(k - 1) + cc * f(k) + cp * f(k + 1) + cpp * f(k + 2));
+        }
+        const bool lo = k <= 6;
+        const int r = lo ? k : n + 1 - k;
+        const T *m = M + (lo ? 0 : 48) + (r - 1) * 8;
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc = acc + __ldg(m + c) * f(lo ? c + 1 : n - c);
+        return T(-1.0 / lap42_h(r)) * acc;
+    }
+}
+
 // One scalar field of the scratch sets: field q of member mem.
 __device__ __forceinline__ int64_t dif_base(const Dims &d, int mem, int q)
 {
     return ((int64_t)mem * DIF_FIELDS + q) * NPAN * d.ps;
 }
 
-// The contravariant basis b1, b2 (Cartesian, unit sphere) of every vertex: [panel][6][box].
+// The contravariant basis b1, b2 (Cartesian, unit sphere) of every vertex: [panel][6][box];
+// for the 4-2 order the closure blocks m_rc = sum_k w b_k of every boundary line, built on
+// the host in FP64: [direction x, y][line 1..n][near, far end][row 0..5][column 0..7]
+// (line j of the x direction has b_k = Qi11 J at (k, j) from the near end, at (n+1-k, j)
+// from the far end; the y direction Qi22 J along column i).
 template <class T>
 struct DifView {
     const T *b;
+    const T *m42;
     double h2;   // (hx a)^2
 };
+__host__ __device__ __forceinline__ int64_t dif_m42_index(int n, int dir, int line, int side)
+{
+    return ((((int64_t)dir * n + (line - 1)) * 2 + side) * 48);
+}
 
 // (h, b1 u + b2 v) of the state -> the four scalar fields of each member.
 template <class T>
@@ -58,9 +164,9 @@ __global__ void __launch_bounds__(256) k_dif_prep(const T *__restrict__ Y, T *__
         X[dif_base(d, mem, 1 + k) + t * d.ps + o] = b[k * d.ps] * u + b[(3 + k) * d.ps] * w;
 }
 
-// calc_tile_d1x_d1y: d1x = D1x(f) J Qi12, d1y = D1y(f) J Qi12 (sbp_diff_21 node differences).
-// Grid z: panel + NPAN * (field + 4 member).
-template <class T>
+// calc_tile_d1x_d1y: d1x = D1x(f) J Qi12, d1y = D1y(f) J Qi12 (sbp_diff_<ORD> node
+// differences).  Grid z: panel + NPAN * (field + 4 member).
+template <class T, int ORD>
 __global__ void __launch_bounds__(256) k_dif_d1(const T *__restrict__ F, T *__restrict__ D1X, T *__restrict__ D1Y, Dims d,
                                                 AhView<T> a)
 {
@@ -74,13 +180,13 @@ __global__ void __launch_bounds__(256) k_dif_d1(const T *__restrict__ F, T *__re
     const GV<T> f{F + base, d.P};
     const int64_t o = box_off(d.P, i, j);
     const T J = __ldg(a.J + o), Q2 = __ldg(a.Q2 + o);
-    D1X[base + o] = dn2n21<T>(i, n, [&](int k) { return f(k, j); }) * J * Q2;
-    D1Y[base + o] = dn2n21<T>(j, n, [&](int l) { return f(i, l); }) * J * Q2;
+    D1X[base + o] = dn2n<T, ORD>(i, n, [&](int k) { return f(k, j); }) * J * Q2;
+    D1Y[base + o] = dn2n<T, ORD>(j, n, [&](int l) { return f(i, l); }) * J * Q2;
 }
 
 // calc_laplace_tile and divide_by_J_self: the panel-local Laplacian of every vertex; the
 // panel-boundary vertices' values go to R (for the sync), the others to OUT.
-template <class T>
+template <class T, int ORD>
 __global__ void __launch_bounds__(256) k_dif_lap(const T *__restrict__ F, const T *__restrict__ D1X,
                                                  const T *__restrict__ D1Y, T *__restrict__ R, T *__restrict__ OUT, Dims d,
                                                  AhView<T> a, DifView<T> v)
@@ -94,38 +200,18 @@ __global__ void __launch_bounds__(256) k_dif_lap(const T *__restrict__ F, const 
     if (i > n || j > n) return;
     const GV<T> f{F + base, d.P}, dx1{D1X + base, d.P}, dy1{D1Y + base, d.P};
     const GV<T> J{a.J, d.P}, Q1{a.Q1, d.P}, Q3{a.Q3, d.P};
-    auto bx = [&](int k) { return Q1(k, j) * J(k, j); };
-    auto by = [&](int l) { return Q3(i, l) * J(i, l); };
-    T d2x, d2y;
-    if (i == 1) {
-        const T bc = bx(1), bp = bx(2);
-        d2x = (-(bc + bp) * f(1, j) + (bc + bp) * f(2, j));
-    } else if (i == n) {
-        const T bc = bx(n), bm = bx(n - 1);
-        d2x = (bc + bm) * f(n - 1, j) + (-(bc + bm)) * f(n, j);
-    } else {
-        const T bm = bx(i - 1), bc = bx(i), bp = bx(i + 1);
-        const T cm = (bm + bc) / T(2), cc = -(bm + T(2) * bc + bp) / T(2), cp = (bp + bc) / T(2);
-        d2x = (cp * f(i + 1, j) + cc * f(i, j) + cm * f(i - 1, j));
-    }
-    if (j == 1) {
-        const T bc = by(1), bp = by(2);
-        d2y = -(bc + bp) * f(i, 1) + (bc + bp) * f(i, 2);
-    } else if (j == n) {
-        const T bc = by(n), bm = by(n - 1);
-        d2y = (bc + bm) * f(i, n - 1) + (-(bc + bm)) * f(i, n);
-    } else {
-        const T bm = by(j - 1), bc = by(j), bp = by(j + 1);
-        const T cm = (bm + bc) / T(2), cc = -(bm + T(2) * bc + bp) / T(2), cp = (bp + bc) / T(2);
-        d2y = (cp * f(i, j + 1) + cc * f(i, j) + cm * f(i, j - 1));
-    }
-    // the boundary penalties, all on d2f_x and in the reference's order
-    if (i == 1) d2x = d2x - T(0.5) * (T(2) * (T(-2) * dy1(1, j)));
-    if (i == n) d2x = d2x - T(0.5) * (T(2) * (T(2) * dy1(n, j)));
-    if (j == 1) d2x = d2x - T(0.5) * (T(2) * (T(-2) * dx1(i, 1)));
-    if (j == n) d2x = d2x - T(0.5) * (T(2) * (T(2) * dx1(i, n)));
-    const T dyx = dn2n21<T>(j, n, [&](int l) { return dx1(i, l); });
-    const T dxy = dn2n21<T>(i, n, [&](int k) { return dy1(k, j); });
+    T d2x = narrow_d2<T, ORD>(i, n, [&](int k) { return Q1(k, j) * J(k, j); }, [&](int k) { return f(k, j); },
+                              v.m42 + dif_m42_index(n, 0, j, 0));
+    const T d2y = narrow_d2<T, ORD>(j, n, [&](int l) { return Q3(i, l) * J(i, l); }, [&](int l) { return f(i, l); },
+                                    v.m42 + dif_m42_index(n, 1, i, 0));
+    // the boundary penalties 1/h_1 (-+2 d1f), all on d2f_x and in the reference's order
+    const T pen = ORD == 21 ? T(2) : T(48.0 / 17);
+    if (i == 1) d2x = d2x - T(0.5) * (pen * (T(-2) * dy1(1, j)));
+    if (i == n) d2x = d2x - T(0.5) * (pen * (T(2) * dy1(n, j)));
+    if (j == 1) d2x = d2x - T(0.5) * (pen * (T(-2) * dx1(i, 1)));
+    if (j == n) d2x = d2x - T(0.5) * (pen * (T(2) * dx1(i, n)));
+    const T dyx = dn2n<T, ORD>(j, n, [&](int l) { return dx1(i, l); });
+    const T dxy = dn2n<T, ORD>(i, n, [&](int k) { return dy1(k, j); });
     T r = d2x + d2y;
     r = r + dxy + dyx;
     r = r / T(v.h2);

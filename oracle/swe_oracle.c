@@ -1878,24 +1878,114 @@ static void diff_alloc(orc_ctx *c)
     for (unsigned q = 0; q < sizeof(df) / sizeof(df[0]); q++) fld_init(df[q], n, n, hw);
 }
 
-/* laplace_Ah_sbp21_narrow_t%calc_laplace (laplace_Ah_sbp21_narrow_mod.f90:25-56) with
-   calc_tile_d1x_d1y (:58-85) and calc_laplace_tile (:86-239): the narrow second differences
-   with the variable coefficients Qi11 J and Qi22 J, the mixed terms D1(Qi12 J D1 f), the
-   boundary penalties (all four added to d2f_x, as the reference does), the division by
-   (hx a)^2 and by J, then the Ah scalar sync.  out may be f.  The halo exchanges of f,
-   d1f_x and d1f_y ahead of the tile sweeps feed no stencil (every difference is one-sided
-   at the panel edges) and are left out. */
-static void lap_ah21(orc_ctx *c, fld_t *out, fld_t *f)
+/* Closure rows 1..6 of the narrow SBP 4-2 second difference with a variable coefficient
+   (laplace_Ah_sbp42_narrow_mod.f90:121-262): entry m_rc (r <= c) of the symmetric boundary
+   block as sum_k w b_k over the coefficients b_k = Qi J at node k; row r of the difference is
+   -(1 / h_r) sum_c m_rc f_c with the node norm h_r (the same block mirrored at the far end,
+   :284-423) */
+static const struct { int r, c, k; double w; } LAP42_M[] = {
+    {1, 1, 1, 12.0 / 17.0}, {1, 1, 2, 59.0 / 192.0}, {1, 1, 3, 27010400129.0 / 345067064608.0},
+    {1, 1, 4, 69462376031.0 / 2070402387648.0}, {1, 2, 1, -59.0 / 68.0}, {1, 2, 3, -6025413881.0 / 21126554976.0},
+    {1, 2, 4, -537416663.0 / 7042184992.0}, {1, 3, 1, 2.0 / 17.0}, {1, 3, 2, -59.0 / 192.0},
+    {1, 3, 3, 2083938599.0 / 8024815456.0}, {1, 3, 4, 213318005.0 / 16049630912.0}, {1, 4, 1, 3.0 / 68.0},
+    {1, 4, 3, -1244724001.0 / 21126554976.0}, {1, 4, 4, 752806667.0 / 21126554976.0},
+    {1, 5, 3, 49579087.0 / 10149031312.0}, {1, 5, 4, -49579087.0 / 10149031312.0}, {1, 6, 3, 1.0 / 784.0},
+    {1, 6, 4, -1.0 / 784.0}, {2, 2, 1, 3481.0 / 3264.0}, {2, 2, 3, 9258282831623875.0 / 7669235228057664.0},
+    {2, 2, 4, 236024329996203.0 / 1278205871342944.0}, {2, 3, 1, -59.0 / 408.0},
+    {2, 3, 3, -29294615794607.0 / 29725717938208.0}, {2, 3, 4, -2944673881023.0 / 29725717938208.0},
+    {2, 4, 1, -59.0 / 1088.0}, {2, 4, 3, 260297319232891.0 / 2556411742685888.0},
+    {2, 4, 4, -60834186813841.0 / 1278205871342944.0}, {2, 5, 3, -1328188692663.0 / 37594290333616.0},
+    {2, 5, 4, 1328188692663.0 / 37594290333616.0}, {2, 6, 3, -8673.0 / 2904112.0}, {2, 6, 4, 8673.0 / 2904112.0},
+    {3, 3, 1, 1.0 / 51.0}, {3, 3, 2, 59.0 / 192.0}, {3, 3, 3, 378288882302546512209.0 / 270764341349677687456.0},
+    {3, 3, 4, 13777050223300597.0 / 26218083221499456.0}, {3, 3, 5, 564461.0 / 13384296.0}, {3, 4, 1, 1.0 / 136.0},
+    {3, 4, 3, -4836340090442187227.0 / 5525802884687299744.0}, {3, 4, 4, -17220493277981.0 / 89177153814624.0},
+    {3, 4, 5, -125059.0 / 743572.0}, {3, 5, 3, 1613976761032884305.0 / 7963657098519931984.0},
+    {3, 5, 4, -10532412077335.0 / 42840005263888.0}, {3, 5, 5, 564461.0 / 4461432.0},
+    {3, 6, 3, 33235054191.0 / 26452850508784.0}, {3, 6, 4, -960119.0 / 1280713392.0}, {3, 6, 5, -3391.0 / 6692148.0},
+    {4, 4, 1, 3.0 / 1088.0}, {4, 4, 3, 507284006600757858213.0 / 475219048083107777984.0},
+    {4, 4, 4, 1950062198436997.0 / 3834617614028832.0}, {4, 4, 5, 1869103.0 / 2230716.0}, {4, 4, 6, 1.0 / 24.0},
+    {4, 5, 3, -4959271814984644613.0 / 20965546238960637264.0}, {4, 5, 4, -15998714909649.0 / 37594290333616.0},
+    {4, 5, 5, -375177.0 / 743572.0}, {4, 5, 6, -1.0 / 6.0}, {4, 6, 3, 752806667.0 / 539854092016.0},
+    {4, 6, 4, 1063649.0 / 8712336.0}, {4, 6, 5, -368395.0 / 2230716.0}, {4, 6, 6, 1.0 / 8.0},
+    {5, 5, 3, 8386761355510099813.0 / 128413970713633903242.0}, {5, 5, 4, 2224717261773437.0 / 2763180339520776.0},
+    {5, 5, 5, 280535.0 / 371786.0}, {5, 5, 6, 5.0 / 6.0}, {5, 5, 7, 1.0 / 24.0},
+    {5, 6, 3, -13091810925.0 / 13226425254392.0}, {5, 6, 4, -35039615.0 / 213452232.0},
+    {5, 6, 5, -1118749.0 / 2230716.0}, {5, 6, 6, -1.0 / 2.0}, {5, 6, 7, -1.0 / 6.0}, {5, 7, 5, 1.0 / 8.0},
+    {5, 7, 6, -1.0 / 6.0}, {5, 7, 7, 1.0 / 8.0}, {6, 6, 3, 660204843.0 / 13226425254392.0},
+    {6, 6, 4, 3290636.0 / 80044587.0}, {6, 6, 5, 5580181.0 / 6692148.0}, {6, 6, 6, 3.0 / 4.0}, {6, 6, 7, 5.0 / 6.0},
+    {6, 6, 8, 1.0 / 24.0}, {6, 7, 5, -1.0 / 6.0}, {6, 7, 6, -1.0 / 2.0}, {6, 7, 7, -1.0 / 2.0},
+    {6, 7, 8, -1.0 / 6.0}, {6, 8, 6, 1.0 / 8.0}, {6, 8, 7, -1.0 / 6.0}, {6, 8, 8, 1.0 / 8.0}
+};
+static const double LAP42_H[6] = {17.0 / 48, 59.0 / 48, 43.0 / 48, 49.0 / 48, 1, 1};
+
+/* the narrow second difference of a line of n nodes (b, f, out 1-based): the d2f_x / d2f_y
+   sweeps of calc_laplace_tile (laplace_Ah_sbp21_narrow_mod.f90:116-191 for 2-1,
+   laplace_Ah_sbp42_narrow_mod.f90:121-699 for 4-2) */
+static void narrow_d2_line(int ord, int n, const double *b, const double *f, double *out)
+{
+    if (ord == 21) {
+        double bc = b[1], bp = b[2];
+        out[1] = (-(bc + bp) * f[1] + (bc + bp) * f[2]);
+        for (int i = 2; i <= n - 1; i++) {
+            const double bm = b[i - 1], bcc = b[i], bpp = b[i + 1];
+            const double cm = (bm + bcc) / 2, cc = -(bm + 2 * bcc + bpp) / 2, cp = (bpp + bcc) / 2;
+            out[i] = (cp * f[i + 1] + cc * f[i] + cm * f[i - 1]);
+        }
+        bc = b[n];
+        const double bm = b[n - 1];
+        out[n] = (bc + bm) * f[n - 1] + (-(bc + bm)) * f[n];
+        return;
+    }
+    static double D[6][8][8];
+    static int ready = 0;
+    if (!ready) {
+        for (unsigned q = 0; q < sizeof(LAP42_M) / sizeof(LAP42_M[0]); q++) {
+            const int r = LAP42_M[q].r, c = LAP42_M[q].c, k = LAP42_M[q].k;
+            D[r - 1][c - 1][k - 1] = LAP42_M[q].w;
+            if (c <= 6) D[c - 1][r - 1][k - 1] = LAP42_M[q].w;
+        }
+        ready = 1;
+    }
+    for (int side = 0; side < 2; side++)
+        for (int r = 1; r <= 6; r++) {
+            double acc = 0.0;
+            for (int cc = 1; cc <= 8; cc++) {
+                double m = 0.0;
+                for (int k = 1; k <= 8; k++) m = m + D[r - 1][cc - 1][k - 1] * b[side ? n + 1 - k : k];
+                acc = acc + m * f[side ? n + 1 - cc : cc];
+            }
+            out[side ? n + 1 - r : r] = -1.0 / LAP42_H[r - 1] * acc;
+        }
+    for (int i = 7; i <= n - 6; i++) {
+        const double bmm = b[i - 2], bm = b[i - 1], bc = b[i], bp = b[i + 1], bpp = b[i + 2];
+        const double cmm = 1.0 / 6.0 * bm - 1.0 / 8.0 * bmm - 1.0 / 8.0 * bc;
+        const double cm = 1.0 / 6.0 * bmm + 1.0 / 6.0 * bp + 1.0 / 2.0 * bm + 1.0 / 2.0 * bc;
+        const double cc = -1.0 / 24.0 * bmm - 5.0 / 6.0 * bm - 5.0 / 6.0 * bp - 1.0 / 24.0 * bpp - 3.0 / 4.0 * bc;
+        const double cp = 1.0 / 6.0 * bm + 1.0 / 6.0 * bpp + 1.0 / 2.0 * bc + 1.0 / 2.0 * bp;
+        const double cpp = 1.0 / 6.0 * bp - 1.0 / 8.0 * bc - 1.0 / 8.0 * bpp;
+        out[i] = (cmm * f[i - 2] + cm * f[i - 1] + cc * f[i] + cp * f[i + 1] + cpp * f[i + 2]);
+    }
+}
+
+/* laplace_Ah_sbp<ord>_narrow_t%calc_laplace (laplace_Ah_sbp21_narrow_mod.f90:25-56 and
+   laplace_Ah_sbp42_narrow_mod.f90:27-63) with calc_tile_d1x_d1y and calc_laplace_tile:
+   the narrow second differences with the variable coefficients Qi11 J and Qi22 J, the mixed
+   terms D1(Qi12 J D1 f), the boundary penalties 1/h_1 (-+2 d1f) (all four added to d2f_x, as
+   the reference does), the division by (hx a)^2 and by J, then the Ah scalar sync.  out may
+   be f.  The halo exchanges of f, d1f_x and d1f_y ahead of the tile sweeps feed no stencil
+   (every difference is one-sided at the panel edges) and are left out. */
+static void lap_ah(orc_ctx *c, fld_t *out, fld_t *f, int ord)
 {
     const int n = c->N + 1;
     const mesh_t *m = &c->mxy;
     fld_t *d1x = &c->df_d1x, *d1y = &c->df_d1y, *d2x = &c->df_d2x, *d2y = &c->df_d2y;
     fld_t *dxy = &c->df_dxy, *dyx = &c->df_dyx;
-#define BX(i, j) (m->Q1[MI(m, t, i, j)] * m->J[MI(m, t, i, j)])
-#define BY(i, j) (m->Q3[MI(m, t, i, j)] * m->J[MI(m, t, i, j)])
+    const double pen = ord == 21 ? 2.0 : 48.0 / 17;   /* 1 / h_1 of the node norm */
+    double *bl = malloc(sizeof(double) * (n + 1)), *fl = malloc(sizeof(double) * (n + 1)),
+           *ol = malloc(sizeof(double) * (n + 1));
     for (int t = 0; t < NPAN; t++) {
-        diff_n2n(d1x, f, t, 0, n, 1, n, 21);
-        diff_n2n(d1y, f, t, 1, n, 1, n, 21);
+        diff_n2n(d1x, f, t, 0, n, 1, n, ord);
+        diff_n2n(d1y, f, t, 1, n, 1, n, ord);
         for (int j = 1; j <= n; j++)
             for (int i = 1; i <= n; i++) {
                 const size_t k = MI(m, t, i, j);
@@ -1906,57 +1996,41 @@ static void lap_ah21(orc_ctx *c, fld_t *out, fld_t *f)
     const double h2 = (m->hx * c->a) * (m->hx * c->a);
     for (int t = 0; t < NPAN; t++) {
         for (int j = 1; j <= n; j++) {
-            double bc = BX(1, j), bp = BX(2, j);
-            double cc = -(bc + bp), cp = +(bc + bp);
-            FA(d2x, t, 1, j) = (cc * FA(f, t, 1, j) + cp * FA(f, t, 2, j));
-            for (int i = 2; i <= n - 1; i++) {
-                const double bm = BX(i - 1, j);
-                bc = BX(i, j); bp = BX(i + 1, j);
-                const double cm = (bm + bc) / 2;
-                cc = -(bm + 2 * bc + bp) / 2;
-                cp = (bp + bc) / 2;
-                FA(d2x, t, i, j) = (cp * FA(f, t, i + 1, j) + cc * FA(f, t, i, j) + cm * FA(f, t, i - 1, j));
-            }
-            bc = BX(n, j);
-            const double bm = BX(n - 1, j);
-            cc = -(bc + bm);
-            const double cm = +(bc + bm);
-            FA(d2x, t, n, j) = cm * FA(f, t, n - 1, j) + cc * FA(f, t, n, j);
-        }
-        for (int i = 1; i <= n; i++) {
-            const double bc = BY(i, 1), bp = BY(i, 2);
-            const double cc = -(bc + bp), cp = +(bc + bp);
-            FA(d2y, t, i, 1) = cc * FA(f, t, i, 1) + cp * FA(f, t, i, 2);
-        }
-        for (int j = 2; j <= n - 1; j++)
             for (int i = 1; i <= n; i++) {
-                const double bm = BY(i, j - 1), bc = BY(i, j), bp = BY(i, j + 1);
-                const double cm = (bm + bc) / 2, cc = -(bm + 2 * bc + bp) / 2, cp = (bp + bc) / 2;
-                FA(d2y, t, i, j) = (cp * FA(f, t, i, j + 1) + cc * FA(f, t, i, j) + cm * FA(f, t, i, j - 1));
+                const size_t k = MI(m, t, i, j);
+                bl[i] = m->Q1[k] * m->J[k];
+                fl[i] = FA(f, t, i, j);
             }
+            narrow_d2_line(ord, n, bl, fl, ol);
+            for (int i = 1; i <= n; i++) FA(d2x, t, i, j) = ol[i];
+        }
         for (int i = 1; i <= n; i++) {
-            const double bc = BY(i, n), bm = BY(i, n - 1);
-            const double cc = -(bc + bm), cm = +(bc + bm);
-            FA(d2y, t, i, n) = cm * FA(f, t, i, n - 1) + cc * FA(f, t, i, n);
+            for (int j = 1; j <= n; j++) {
+                const size_t k = MI(m, t, i, j);
+                bl[j] = m->Q3[k] * m->J[k];
+                fl[j] = FA(f, t, i, j);
+            }
+            narrow_d2_line(ord, n, bl, fl, ol);
+            for (int j = 1; j <= n; j++) FA(d2y, t, i, j) = ol[j];
         }
         for (int j = 1; j <= n; j++) {
-            const double penalty = 2.0 * (-2.0 * FA(d1y, t, 1, j));
+            const double penalty = pen * (-2.0 * FA(d1y, t, 1, j));
             FA(d2x, t, 1, j) = FA(d2x, t, 1, j) - 0.5 * penalty;
         }
         for (int j = 1; j <= n; j++) {
-            const double penalty = 2.0 * (2 * FA(d1y, t, n, j));
+            const double penalty = pen * (2 * FA(d1y, t, n, j));
             FA(d2x, t, n, j) = FA(d2x, t, n, j) - 0.5 * penalty;
         }
         for (int i = 1; i <= n; i++) {
-            const double penalty = 2.0 * (-2 * FA(d1x, t, i, 1));
+            const double penalty = pen * (-2 * FA(d1x, t, i, 1));
             FA(d2x, t, i, 1) = FA(d2x, t, i, 1) - 0.5 * penalty;
         }
         for (int i = 1; i <= n; i++) {
-            const double penalty = 2.0 * (2 * FA(d1x, t, i, n));
+            const double penalty = pen * (2 * FA(d1x, t, i, n));
             FA(d2x, t, i, n) = FA(d2x, t, i, n) - 0.5 * penalty;
         }
-        diff_n2n(dyx, d1x, t, 1, n, 1, n, 21);
-        diff_n2n(dxy, d1y, t, 0, n, 1, n, 21);
+        diff_n2n(dyx, d1x, t, 1, n, 1, n, ord);
+        diff_n2n(dxy, d1y, t, 0, n, 1, n, ord);
         for (int j = 1; j <= n; j++)
             for (int i = 1; i <= n; i++) {
                 double v = 1.0 * FA(d2x, t, i, j) + 1.0 * FA(d2y, t, i, j);
@@ -1966,8 +2040,7 @@ static void lap_ah21(orc_ctx *c, fld_t *out, fld_t *f)
         for (int j = 1; j <= n; j++)
             for (int i = 1; i <= n; i++) FA(out, t, i, j) = FA(out, t, i, j) / m->J[MI(m, t, i, j)];
     }
-#undef BX
-#undef BY
+    free(bl); free(fl); free(ol);
     exch_do(&c->ex_xy1_full_s, out, NULL);
     for (int t = 0; t < NPAN; t++) sync_ah_scalar(c, out, t);
 }
@@ -1975,14 +2048,14 @@ static void lap_ah21(orc_ctx *c, fld_t *out, fld_t *f)
 /* hordiff_scalar_t%calc_diff (hordiff_scalar_mod.f90:30-50), diff_order 2 with
    diff_coeff = coeff a hx (hordiff_factory_mod.f90:276-298): tend = -(coeff a hx)^4 L(L(f)).
    f_work receives the iterate (it may be f). */
-static void hordiff_ah21(orc_ctx *c, fld_t *tend, fld_t *f, fld_t *work, double coeff)
+static void hordiff_ah(orc_ctx *c, fld_t *tend, fld_t *f, fld_t *work, double coeff, int ord)
 {
     const int n = c->N + 1;
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= n; j++)
             for (int i = 1; i <= n; i++) FA(work, t, i, j) = 1.0 * FA(f, t, i, j);
-    lap_ah21(c, work, work);
-    lap_ah21(c, work, work);
+    lap_ah(c, work, work, ord);
+    lap_ah(c, work, work, ord);
     const double dc = coeff * c->a * c->mxy.hx;
     const double k = -1.0 * ((dc * dc) * (dc * dc));
     for (int t = 0; t < NPAN; t++)
@@ -1996,7 +2069,7 @@ static void hordiff_ah21(orc_ctx *c, fld_t *tend, fld_t *f, fld_t *work, double 
    cart2cube_vec does for covariant components, vec_math_mod.f90:196-219, then the covariant
    ECS Ah vector sync), dh by the scalar diffusion */
 static void op_diff_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fld_t *u, fld_t *v, double uv_coeff,
-                       double h_coeff)
+                       double h_coeff, int ord)
 {
     const int n = c->N + 1;
     const mesh_t *m = &c->mxy;
@@ -2008,7 +2081,7 @@ static void op_diff_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fl
                 for (int d = 0; d < 3; d++)
                     FA(&c->df_x[d], t, i, j) = m->b1[3 * k + d] * FA(u, t, i, j) + m->b2[3 * k + d] * FA(v, t, i, j);
             }
-    for (int d = 0; d < 3; d++) hordiff_ah21(c, &c->df_t[d], &c->df_x[d], &c->df_x[d], uv_coeff);
+    for (int d = 0; d < 3; d++) hordiff_ah(c, &c->df_t[d], &c->df_x[d], &c->df_x[d], uv_coeff, ord);
     for (int t = 0; t < NPAN; t++)
         for (int j = 1; j <= n; j++)
             for (int i = 1; i <= n; i++) {
@@ -2019,7 +2092,7 @@ static void op_diff_ah(orc_ctx *c, fld_t *dh, fld_t *du, fld_t *dv, fld_t *h, fl
             }
     exch_do(&c->ex_xy1_cross_v, du, dv);
     for (int t = 0; t < NPAN; t++) sync_grad_on_edges(c, dv, du, t);
-    hordiff_ah21(c, dh, h, &c->df_x[0], h_coeff);
+    hordiff_ah(c, dh, h, &c->df_x[0], h_coeff, ord);
 }
 
 /* stvec assign/update over interior points (grid_field_mod.f90:442-534) */
@@ -2560,23 +2633,29 @@ void orc_ah_apply(orc_ctx *c, const double *h, const double *u, const double *v,
     op_apply_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v);
     fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
 }
-/* the diffusion operator's tendency (lap_order 21: the _sbp_21_narrow operators) */
+/* the narrow Laplacian orders built: 2-1, and 4-2 where its two closure blocks of six rows
+   do not overlap (N >= 11) */
+static int diff_order_ok(const orc_ctx *c, int lap_order)
+{
+    return lap_order == 21 || (lap_order == 42 && c->N >= 11);
+}
+/* the diffusion operator's tendency (lap_order 21 or 42: the _sbp_<order>_narrow operators) */
 int orc_diff_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv,
                    int lap_order, double uv_coeff, double h_coeff)
 {
-    if (lap_order != 21) return -1;
+    if (!diff_order_ok(c, lap_order)) return -1;
     fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
-    op_diff_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v, uv_coeff, h_coeff);
+    op_diff_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v, uv_coeff, h_coeff, lap_order);
     fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
     return 0;
 }
 /* the narrow Laplacian alone (laplace_Ah_sbp<lap_order>_narrow), for tests of the operator */
 int orc_lap_ah(orc_ctx *c, const double *f, double *out, int lap_order)
 {
-    if (lap_order != 21) return -1;
+    if (!diff_order_ok(c, lap_order)) return -1;
     diff_alloc(c);
     fld_from_packed(&c->df_x[0], f);
-    lap_ah21(c, &c->df_t[0], &c->df_x[0]);
+    lap_ah(c, &c->df_t[0], &c->df_x[0], lap_order);
     fld_to_packed(&c->df_t[0], out);
     return 0;
 }
@@ -2584,12 +2663,12 @@ int orc_lap_ah(orc_ctx *c, const double *f, double *out, int lap_order)
 int orc_diff_step(orc_ctx *c, double *h, double *u, double *v, double dt, int lap_order, double uv_coeff,
                   double h_coeff, int nsteps)
 {
-    if (lap_order != 21) return -1;
+    if (!diff_order_ok(c, lap_order)) return -1;
     const int n = c->N + 1;
     fld_from_packed(&c->h, h); fld_from_packed(&c->ah_u, u); fld_from_packed(&c->ah_v, v);
     fld_t *y[3] = {&c->h, &c->ah_u, &c->ah_v}, *k[3] = {&c->dh, &c->ah_du, &c->ah_dv};
     for (int s = 0; s < nsteps; s++) {
-        op_diff_ah(c, k[0], k[1], k[2], y[0], y[1], y[2], uv_coeff, h_coeff);
+        op_diff_ah(c, k[0], k[1], k[2], y[0], y[1], y[2], uv_coeff, h_coeff, lap_order);
         for (int f = 0; f < 3; f++)
             for (int t = 0; t < NPAN; t++)
                 for (int j = 1; j <= n; j++)

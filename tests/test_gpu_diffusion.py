@@ -1,9 +1,9 @@
-"""GPU parity of the diffusion on the Ah staggering (hordiff_vec_xyz_Ah_sbp_21_narrow for
-u, v, hordiff_scalar_Ah_sbp_21_narrow for h, explicit_Eul1) against the CPU oracle: FP64
-tendencies within 1e-12 relative (max-norm over the field's max-norm) for random states
-whose duplicated panel-edge copies disagree and for smooth ones, Euler steps and the
-driver's RK4-then-diffusion loop likewise; FP32 against FP64 in relative L2; members
-independent; non-Ah contexts and unbuilt orders refused."""
+"""GPU parity of the diffusion on the Ah staggering (hordiff_vec_xyz_Ah_sbp_<o>_narrow for
+u, v, hordiff_scalar_Ah_sbp_<o>_narrow for h, o = 21 or 42, explicit_Eul1) against the CPU
+oracle: FP64 tendencies within 1e-12 relative (max-norm over the field's max-norm) for
+random states whose duplicated panel-edge copies disagree, Euler steps and the driver's
+RK4-then-diffusion loop likewise; FP32 against FP64 in relative L2; members independent;
+non-Ah contexts and unbuilt orders refused."""
 import numpy as np
 import pytest
 
@@ -15,6 +15,11 @@ FP64_RTOL = 1e-12
 H = 1000.0
 DIFF = {"hordiff_uv_name": "hordiff_vec_xyz_Ah_sbp_21_narrow", "uv_diff_coeff": 0.03,
         "hordiff_h_name": "hordiff_scalar_Ah_sbp_21_narrow", "h_diff_coeff": 0.01}
+
+
+def diff_config(order):
+    return {**DIFF, "hordiff_uv_name": f"hordiff_vec_xyz_Ah_sbp_{order}_narrow",
+            "hordiff_h_name": f"hordiff_scalar_Ah_sbp_{order}_narrow"}
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -46,37 +51,39 @@ def ah_domain(N, precision="fp64", members=1, order=21):
     return dom, op
 
 
-@pytest.mark.parametrize("N", [8, 12, 17, 24, 33])
-def test_apply_parity_fp64_random(N):
+@pytest.mark.parametrize("order,N", [(21, 8), (21, 12), (21, 17), (21, 24), (21, 33), (42, 11), (42, 12), (42, 17),
+                                     (42, 24), (42, 33)])
+def test_apply_parity_fp64_random(order, N):
     from ch_swe_b200 import create_stvec_swm, create_swm_diff_operator
     from oracle.oracle import Oracle
     st = random_state(N, 700 + N)
-    ref = Oracle(N, h_mean=H).diff_apply(*st, uv_coeff=0.03, h_coeff=0.01)
+    ref = Oracle(N, h_mean=H).diff_apply(*st, uv_coeff=0.03, h_coeff=0.01, lap_order=order)
     dom, _ = ah_domain(N)
-    dif = create_swm_diff_operator(DIFF, dom)
+    dif = create_swm_diff_operator(diff_config(order), dom)
     x = create_stvec_swm(dom).upload(*st)
     y = create_stvec_swm(dom)
     dif.apply(y, x, dom)
     for g, r, name in zip(y.download(), ref, "huv"):
-        assert rel(g, r) < FP64_RTOL, (N, name, rel(g, r))
+        assert rel(g, r) < FP64_RTOL, (order, N, name, rel(g, r))
     dom.destroy()
 
 
-def test_euler_steps_and_driver_loop_fp64():
-    """Six driver steps on a Gaussian hill: RK4 of the Ah linear operator (SBP 2-1), then
-    one explicit_Eul1 diffusion step (shallow_water_mod.f90:112-118)."""
+@pytest.mark.parametrize("order", [21, 42])
+def test_euler_steps_and_driver_loop_fp64(order):
+    """Six driver steps on a Gaussian hill: RK4 of the Ah linear operator of the same SBP
+    order, then one explicit_Eul1 diffusion step (shallow_water_mod.f90:112-118)."""
     from ch_swe_b200 import create_stvec_swm, create_swm_diff_operator, create_timescheme
     from ch_swe_b200.testcases import gaussian_hill
     from oracle.oracle import Oracle
     N, dt = 20, 900.0
     st = gaussian_hill(N, lam0=0.5, phi0=0.6, d0=0.3, amp=5.0, staggering="Ah")
-    o = Oracle(N, h_mean=H, sbp_order=21)
+    o = Oracle(N, h_mean=H, sbp_order=order)
     ref = st
     for _ in range(6):
         ref = o.ah_rk4(*ref, dt, 1)
-        ref = o.diff_step(*ref, dt=dt, uv_coeff=0.03, h_coeff=0.01)
-    dom, op = ah_domain(N)
-    dif = create_swm_diff_operator(DIFF, dom)
+        ref = o.diff_step(*ref, dt=dt, uv_coeff=0.03, h_coeff=0.01, lap_order=order)
+    dom, op = ah_domain(N, order=order)
+    dif = create_swm_diff_operator(diff_config(order), dom)
     x = create_stvec_swm(dom).upload(*st)
     rk, eul = create_timescheme(x, "rk4"), create_timescheme(x, "explicit_Eul1")
     for _ in range(6):
@@ -130,9 +137,17 @@ def test_refusals():
     assert load().swe_diffusion_apply(ch.ctx, y.handle, x.handle, 21, 0.03, 0.01) != 0
     ch.destroy()
     dom, _ = ah_domain(16)
-    with pytest.raises(ValueError):
+    with pytest.raises(ValueError):   # one order for both operators
         create_swm_diff_operator({**DIFF, "hordiff_h_name": "hordiff_scalar_Ah_sbp_42_narrow"}, dom)
+    with pytest.raises(ValueError):
+        create_swm_diff_operator(diff_config(63), dom)
     x = create_stvec_swm(dom)
-    assert load().swe_diffusion_step(dom.ctx, x.handle, 1.0, 42, 0.03, 0.01) != 0
-    assert SweError is not None
+    assert load().swe_diffusion_step(dom.ctx, x.handle, 1.0, 63, 0.03, 0.01) != 0
     dom.destroy()
+    small, _ = ah_domain(8)
+    with pytest.raises(ValueError):   # the 4-2 closure blocks overlap below N = 11
+        create_swm_diff_operator(diff_config(42), small)
+    x = create_stvec_swm(small)
+    assert load().swe_diffusion_step(small.ctx, x.handle, 1.0, 42, 0.03, 0.01) != 0
+    assert SweError is not None
+    small.destroy()

@@ -1,13 +1,14 @@
-"""The oracle's diffusion on the Ah staggering (laplace_Ah_sbp21_narrow,
-hordiff_scalar_Ah_sbp_21_narrow, hordiff_vec_xyz_Ah_sbp_21_narrow, explicit_Eul1), pinned
-by properties that a wrong metric factor, penalty sign, stencil offset or sync order
-breaks: the narrow SBP Laplacian is self-adjoint and negative semi-definite in the
-J-weighted SBP 2-1 node quadrature and conserves mass (continuous fields: the
-duplicated panel-edge vertices agree), kills constants, and converges to the
-spherical Laplacian (second order inside the panels, first order on their edges; the
-cube corners keep an O(1) error of the panel-wise operator); the scalar tendency is
--(c a hx)^4 L(L(h)); the wind's follows the Cartesian components; one Euler step is
-v + dt tendency."""
+"""The oracle's diffusion on the Ah staggering (laplace_Ah_sbp21_narrow and
+laplace_Ah_sbp42_narrow, hordiff_scalar_Ah_sbp_*_narrow, hordiff_vec_xyz_Ah_sbp_*_narrow,
+explicit_Eul1), pinned by properties that a wrong metric factor, closure coefficient,
+penalty sign, stencil offset or sync order breaks: the narrow SBP Laplacian is
+self-adjoint and negative semi-definite in the J-weighted SBP node quadrature of its
+order and conserves mass (continuous fields: the duplicated panel-edge vertices
+agree), kills constants, and converges to the spherical Laplacian (2-1: second order
+inside the panels, first order on their edges, an O(1) error of the panel-wise operator
+at the cube corners; 4-2: second order in L2, first order on the edges and corners);
+the scalar tendency is -(c a hx)^4 L(L(h)); the wind's follows the Cartesian
+components; one Euler step is v + dt tendency."""
 import numpy as np
 import pytest
 
@@ -27,10 +28,13 @@ def smooth_field(o, seed):
     return f
 
 
-def quad_weights(o):
+def quad_weights(o, order=21):
+    """J times the node norm: Q21_A, Q42_A (sbp_operators_collection_mod.f90:22,35)."""
     n = o.N + 1
     w1 = np.ones(n)
-    w1[0] = w1[-1] = 0.5   # Q21_A (sbp_operators_collection_mod.f90:22)
+    edge = [0.5] if order == 21 else [17 / 48, 59 / 48, 43 / 48, 49 / 48]
+    for i, v in enumerate(edge):
+        w1[i] = w1[-1 - i] = v
     return o.metric(0, 0) * w1[None, :, None] * w1[None, None, :]
 
 
@@ -39,17 +43,18 @@ def orc(oracle_built):
     return Oracle(16)
 
 
-def test_laplacian_kills_constants(orc):
-    L = orc.lap_ah(np.full((6, 17, 17), 7.5))
+@pytest.mark.parametrize("order", [21, 42])
+def test_laplacian_kills_constants(orc, order):
+    L = orc.lap_ah(np.full((6, 17, 17), 7.5), order)
     assert np.abs(L).max() * A * A / 7.5 < 1e-9
 
 
-@pytest.mark.parametrize("N", [8, 13, 16])
-def test_laplacian_self_adjoint_negative_and_conservative(N, oracle_built):
+@pytest.mark.parametrize("order,N", [(21, 8), (21, 13), (21, 16), (42, 12), (42, 16), (42, 23)])
+def test_laplacian_self_adjoint_negative_and_conservative(order, N, oracle_built):
     o = Oracle(N)
-    w = quad_weights(o)
+    w = quad_weights(o, order)
     f, g = smooth_field(o, 1), smooth_field(o, 2)
-    Lf, Lg = o.lap_ah(f), o.lap_ah(g)
+    Lf, Lg = o.lap_ah(f, order), o.lap_ah(g, order)
     s1, s2 = (w * g * Lf).sum(), (w * f * Lg).sum()
     assert abs(s1 - s2) / abs(s1) < 1e-12
     assert abs((w * Lf).sum()) / np.abs(w * Lf).sum() < 1e-12
@@ -69,6 +74,18 @@ def test_laplacian_converges_to_spherical_laplacian(oracle_built):
     assert err[32][0] / err[16][0] < 0.3      # second order inside the panels
     assert err[32][1] / err[16][1] < 0.6      # first order on the panel edges
     assert err[32][0] < 1e-3
+
+
+def test_laplacian42_converges(oracle_built):
+    err = {}
+    for N in (16, 32):
+        o = Oracle(N)
+        z = o.metric(0, 7)
+        e = (o.lap_ah(z, 42) + 2.0 / A ** 2 * z) / (2.0 / A ** 2)
+        err[N] = (np.sqrt((e ** 2).mean()), np.abs(e).max())
+    assert err[32][0] / err[16][0] < 0.35     # second order in L2
+    assert err[32][1] / err[16][1] < 0.6      # first order at the edges and corners
+    assert err[32][1] < 0.05
 
 
 def test_scalar_diffusion_is_minus_c4_bilaplacian(orc):
@@ -112,6 +129,8 @@ def test_euler_step_is_state_plus_dt_tendency(orc):
         assert np.array_equal(a, x + 600.0 * d)
 
 
-def test_other_orders_refused(orc):
+def test_other_orders_refused(orc, oracle_built):
     with pytest.raises(ValueError):
-        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=42)
+        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=63)
+    with pytest.raises(ValueError):   # 4-2's closure blocks overlap below N = 11
+        Oracle(10).diff_apply(*(np.zeros((6, 11, 11)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=42)
