@@ -99,6 +99,31 @@ class rk4_gpu_t {
     }
 };
 
+// operator_swm_diff_t (src/models/shallow_water/operator/operator_swm_diff_mod.f90:27-49) on the
+// Ah staggering: hordiff_vec_xyz_Ah_sbp_<order>_narrow and hordiff_scalar_Ah_sbp_<order>_narrow,
+// order 21 or 42.
+class operator_swm_diff_gpu_t {
+  public:
+    operator_swm_diff_gpu_t(const domain_gpu_t &d, int order, double uv_coeff, double h_coeff)
+        : d_(d), order_(order), uv_(uv_coeff), h_(h_coeff)
+    {
+    }
+    void apply(stvec_swm_gpu_t &vout, const stvec_swm_gpu_t &vin)
+    {
+        check(swe_diffusion_apply(d_.ctx(), vout.handle(), vin.handle(), order_, uv_, h_), d_.ctx(), "diffusion apply");
+    }
+    // explicit_Eul1_t%step (src/time_schemes/explicit_Eul1_mod.f90:20-28): v0 += dt apply(v0)
+    void euler_step(stvec_swm_gpu_t &v0, double dt)
+    {
+        check(swe_diffusion_step(d_.ctx(), v0.handle(), dt, order_, uv_, h_), d_.ctx(), "diffusion step");
+    }
+
+  private:
+    const domain_gpu_t &d_;
+    int order_;
+    double uv_, h_;
+};
+
 // Several domains' RK4 steps as one grid per kernel (swe_group_*: up to 8 linear Ch
 // contexts of one precision and split kernel configuration, any cube sizes); no
 // reference counterpart, the reference advances one state per timescheme%step.
