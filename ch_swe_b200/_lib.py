@@ -37,6 +37,7 @@ EXPORTED = [
     "swe_set_orography", "swe_c_grad", "swe_c_div",
     "swe_group_create", "swe_group_destroy", "swe_group_rk4_steps_members", "swe_group_synchronize",
     "swe_group_last_error", "swe_group_launch_count", "swe_diffusion_apply", "swe_diffusion_step",
+    "swe_set_diffusion",
 ]
 
 
@@ -104,6 +105,7 @@ def load(path: str = LIB_PATH):
     L.swe_integrals.argtypes = [_vp, _vp, ctypes.c_int, _dp, _dp]
     L.swe_diffusion_apply.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
     L.swe_diffusion_step.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    L.swe_set_diffusion.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
     L.swe_launch_count.argtypes = [_vp]
     L.swe_launch_count.restype = ctypes.c_longlong
     L.swe_edge_links.argtypes = [ctypes.POINTER(ctypes.c_int)]

@@ -290,6 +290,8 @@ struct swe_ctx {
     DevAh<float> ah32;
     double *qa = nullptr;            // SBP_Ah quadrature weights J hx hy Ax Ay at the vertices (one box)
     void *dif = nullptr;             // diffusion scratch: 5 sets of [member][4 fields][panel][box] (first use)
+    int dif_order = 0;               // the diffusion step after every RK4 step (0: none; swe_set_diffusion)
+    double dif_uv = 0.0, dif_h = 0.0;
     void *dif_b = nullptr;           // contravariant basis b1, b2 of the vertices, [panel][6][box] (first use)
     // C staggering (cfg.staggering == SWE_STAG_C): h on the cell centres, u on the x
     // points, v on the y points; the C-grid gradient, divergence and co2contra
@@ -1672,6 +1674,11 @@ extern "C" int swe_c_div(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
 }
 
 // One RK4 step as 8 launches: stage s reads yin and writes y1 (double-buffered).
+template <class T>
+static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, const double *dtm, int lap_order, double uv_coeff,
+                             double h_coeff);
+
+// One RK4 step, then the diffusion step when one is set (shallow_water_mod.f90:112-118).
 static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt, const double *dtm = nullptr)
 {
     void *V = v0->d, *A = c->acc;
@@ -1688,6 +1695,9 @@ static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt, const double *dtm 
         enqueue_stage<float>(c, c->ya, V, c->yb, A, v0->cmp, 3, dt, dtm, m);
         enqueue_stage<float>(c, c->yb, V, nullptr, A, v0->cmp, 4, dt, dtm, m);
     }
+    // the scratch and tables exist (swe_set_diffusion set them up outside any capture)
+    if (c->dif_order && c->elem == 8) enqueue_diffusion<double>(c, (double *)V, nullptr, dt, dtm, c->dif_order, c->dif_uv, c->dif_h);
+    else if (c->dif_order) enqueue_diffusion<float>(c, (float *)V, nullptr, dt, dtm, c->dif_order, c->dif_uv, c->dif_h);
 }
 
 static int ensure_cmp(swe_stvec *v)
@@ -2129,7 +2139,8 @@ static double dif_coeff(const swe_ctx *c, double coeff)
 
 // y: the state (read; updated in place unless out), out: the tendency (apply).
 template <class T>
-static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, int lap_order, double uv_coeff, double h_coeff)
+static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, const double *dtm, int lap_order, double uv_coeff,
+                             double h_coeff)
 {
     int rc = dif_setup<T>(c);
     if (rc) return rc;
@@ -2157,10 +2168,10 @@ static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, int lap_order,
     launch_k(k_dif_vraw<T>, pm, pb, 0, c->stream, (const T *)X, D1X, D1Y, d, dv, T(dif_coeff(c, uv_coeff)));
     if (out)
         launch_k(k_dif_update<T, true>, pm, pb, 0, c->stream, y, out, (const T *)X, (const T *)D1X, (const T *)D1Y, d, mv,
-                 T(dif_coeff(c, h_coeff)), T(0));
+                 T(dif_coeff(c, h_coeff)), T(0), (const double *)nullptr);
     else
         launch_k(k_dif_update<T, false>, pm, pb, 0, c->stream, y, (T *)nullptr, (const T *)X, (const T *)D1X,
-                 (const T *)D1Y, d, mv, T(dif_coeff(c, h_coeff)), T(dt));
+                 (const T *)D1Y, d, mv, T(dif_coeff(c, h_coeff)), T(dt), dtm);
     c->launches += 9;
     return SWE_OK;
 }
@@ -2187,8 +2198,8 @@ extern "C" int swe_diffusion_apply(swe_ctx *c, swe_stvec *vout, const swe_stvec 
     int rc = diffusion_check(c, lap_order, "swe_diffusion_apply");
     if (rc) return rc;
     rc = c->elem == 8
-             ? enqueue_diffusion<double>(c, (double *)vin->d, (double *)vout->d, 0.0, lap_order, uv_coeff, h_coeff)
-             : enqueue_diffusion<float>(c, (float *)vin->d, (float *)vout->d, 0.0, lap_order, uv_coeff, h_coeff);
+             ? enqueue_diffusion<double>(c, (double *)vin->d, (double *)vout->d, 0.0, nullptr, lap_order, uv_coeff, h_coeff)
+             : enqueue_diffusion<float>(c, (float *)vin->d, (float *)vout->d, 0.0, nullptr, lap_order, uv_coeff, h_coeff);
     if (rc) return rc;
     CU_LAUNCHED(c);
     return SWE_OK;
@@ -2199,10 +2210,28 @@ extern "C" int swe_diffusion_step(swe_ctx *c, swe_stvec *v, double dt, int lap_o
     if (!c || !v || v->ctx != c) return SWE_EINVAL;
     int rc = diffusion_check(c, lap_order, "swe_diffusion_step");
     if (rc) return rc;
-    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)v->d, nullptr, dt, lap_order, uv_coeff, h_coeff)
-                      : enqueue_diffusion<float>(c, (float *)v->d, nullptr, dt, lap_order, uv_coeff, h_coeff);
+    rc = c->elem == 8 ? enqueue_diffusion<double>(c, (double *)v->d, nullptr, dt, nullptr, lap_order, uv_coeff, h_coeff)
+                      : enqueue_diffusion<float>(c, (float *)v->d, nullptr, dt, nullptr, lap_order, uv_coeff, h_coeff);
     if (rc) return rc;
     CU_LAUNCHED(c);
+    return SWE_OK;
+}
+
+// The diffusion step after every RK4 step of swe_rk4_step(s) and swe_rk4_steps_members
+// (with each member's time step; frozen members stay put), captured with the RK4 stages.
+extern "C" int swe_set_diffusion(swe_ctx *c, int lap_order, double uv_coeff, double h_coeff)
+{
+    if (!c) return SWE_EINVAL;
+    if (lap_order != 0) {
+        int rc = diffusion_check(c, lap_order, "swe_set_diffusion");
+        if (rc) return rc;
+        rc = c->elem == 8 ? dif_setup<double>(c) : dif_setup<float>(c);
+        if (rc) return rc;
+    }
+    if (c->dif_order != lap_order || c->dif_uv != uv_coeff || c->dif_h != h_coeff) drop_graph(c);
+    c->dif_order = lap_order;
+    c->dif_uv = uv_coeff;
+    c->dif_h = h_coeff;
     return SWE_OK;
 }
 

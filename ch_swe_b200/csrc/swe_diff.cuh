@@ -282,11 +282,12 @@ __global__ void __launch_bounds__(256) k_dif_vraw(const T *__restrict__ B, T *__
 
 // The covariant ECS Ah vector sync of (u, v) tendencies (syncronize_grad_on_edges with
 // (U, V) = (v, u), ecs_Ah_vec_sync_mod.f90:34-125), h's tendency c_h L(L(h)), then
-// APPLY: the tendency into OUT; otherwise the Euler update Y += dt tend (explicit_Eul1).
+// APPLY: the tendency into OUT; otherwise the Euler update Y += dt tend (explicit_Eul1),
+// dt per member from dtm when given.
 template <class T, bool APPLY>
 __global__ void __launch_bounds__(256) k_dif_update(T *Y, T *__restrict__ OUT, const T *__restrict__ B,
                                                     const T *__restrict__ UR, const T *__restrict__ VR, Dims d,
-                                                    MetricView<T> m, T kh, T dt)
+                                                    MetricView<T> m, T kh, T dt, const double *__restrict__ dtm)
 {
     const int N = d.N, n = N + 1;
     const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
@@ -334,6 +335,7 @@ __global__ void __launch_bounds__(256) k_dif_update(T *Y, T *__restrict__ OUT, c
         OUT[po + d.fs] = gx;
         OUT[po + 2 * d.fs] = gy;
     } else {
+        if (dtm) dt = T(dtm[mem]);
         Y[po] = Y[po] + dt * th;
         Y[po + d.fs] = Y[po + d.fs] + dt * gx;
         Y[po + 2 * d.fs] = Y[po + 2 * d.fs] + dt * gy;

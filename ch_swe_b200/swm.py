@@ -205,6 +205,16 @@ class Domain:
         check(_lib.load().swe_autotune(self.ctx, int(nreps), ctypes.byref(best), ms), self.ctx, "swe_autotune")
         return {t: ms[k] for k, t in enumerate(self.TILES)}
 
+    def set_diffusion(self, operator=None):
+        """The driver loop's diffusion (shallow_water_mod.f90:112-118) inside the RK4 steps:
+        every RK4 step of this domain is followed by one explicit_Eul1 step of the
+        OperatorSwmDiff with the same dt, captured in the same graphs; None turns it off."""
+        if operator is None:
+            rc = _lib.load().swe_set_diffusion(self.ctx, 0, 0.0, 0.0)
+        else:
+            rc = _lib.load().swe_set_diffusion(self.ctx, operator.lap_order, operator.uv_coeff, operator.h_coeff)
+        check(rc, self.ctx, "set diffusion")
+
     def destroy(self):
         if self._ctx:
             _lib.load().swe_ctx_destroy(self._ctx)

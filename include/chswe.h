@@ -198,6 +198,11 @@ long long swe_group_launch_count(const swe_group *g);
 int swe_diffusion_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin, int lap_order, double uv_coeff,
                         double h_coeff);
 int swe_diffusion_step(swe_ctx *ctx, swe_stvec *v, double dt, int lap_order, double uv_coeff, double h_coeff);
+/* The driver loop's diffusion inside the RK4 steps: after this call every RK4 step of
+   swe_rk4_step / swe_rk4_steps / swe_rk4_steps_members is followed by swe_diffusion_step
+   with the same dt (each member's own with swe_rk4_steps_members; frozen members stay),
+   captured in the same CUDA graphs.  lap_order 0 turns it off. */
+int swe_set_diffusion(swe_ctx *ctx, int lap_order, double uv_coeff, double h_coeff);
 /* FP64 SBP-quadrature mass <h,1> and linear energy H/2(<u,ut>+<v,vt>) + g/2<h,h> of one member. */
 int swe_integrals(swe_ctx *ctx, const swe_stvec *vec, int member, double *mass, double *energy);
 

@@ -94,6 +94,55 @@ def test_euler_steps_and_driver_loop_fp64(order):
     dom.destroy()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_diffusion_captured_with_rk4_steps(precision):
+    """Domain.set_diffusion: eleven graph-replayed RK4 steps (one graph of eight, three
+    single steps), each followed by the diffusion step, give the bits of the step-by-step
+    loop; per-member time steps diffuse each member with its own dt and leave a frozen
+    member as it was."""
+    from ch_swe_b200 import create_stvec_swm, create_swm_diff_operator, create_timescheme
+    from ch_swe_b200.testcases import gaussian_hill
+    N, dt = 20, 900.0
+    st = gaussian_hill(N, lam0=0.5, phi0=0.6, d0=0.3, amp=5.0, staggering="Ah")
+    a, opa = ah_domain(N, precision, order=42)
+    b, opb = ah_domain(N, precision, order=42)
+    dif_a, dif_b = create_swm_diff_operator(diff_config(42), a), create_swm_diff_operator(diff_config(42), b)
+    xa, xb = create_stvec_swm(a).upload(*st), create_stvec_swm(b).upload(*st)
+    a.set_diffusion(dif_a)
+    create_timescheme(xa, "rk4").steps(xa, opa, a, dt, 11)
+    rk, eul = create_timescheme(xb, "rk4"), create_timescheme(xb, "explicit_Eul1")
+    for _ in range(11):
+        rk.step(xb, opb, b, dt)
+        eul.step(xb, dif_b, b, dt)
+    for g, r in zip(xa.download(), xb.download()):
+        assert np.array_equal(g, r)
+    a.set_diffusion(None)
+    a.destroy()
+    b.destroy()
+    # per-member time steps: member 1 with its own dt, member 2 frozen
+    m, opm = ah_domain(N, precision, members=3, order=42)
+    m.set_diffusion(create_swm_diff_operator(diff_config(42), m))
+    xm = create_stvec_swm(m)
+    for k in range(3):
+        xm.upload(*st, member=k)
+    frozen = xm.download(member=2)
+    create_timescheme(xm, "rk4").steps_members(xm, opm, [dt, 0.5 * dt, 0.0], 3)
+    one, op1 = ah_domain(N, precision, order=42)
+    d1 = create_swm_diff_operator(diff_config(42), one)
+    x1 = create_stvec_swm(one).upload(*st)
+    rk1, eul1 = create_timescheme(x1, "rk4"), create_timescheme(x1, "explicit_Eul1")
+    for _ in range(3):
+        rk1.step(x1, op1, one, 0.5 * dt)
+        eul1.step(x1, d1, one, 0.5 * dt)
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    for g, r in zip(xm.download(member=1), x1.download()):
+        assert rel(g, r) < tol
+    for g, r in zip(xm.download(member=2), frozen):
+        assert np.array_equal(g, r)
+    m.destroy()
+    one.destroy()
+
+
 def test_fp32_against_fp64_and_members():
     from ch_swe_b200 import create_stvec_swm, create_swm_diff_operator, create_timescheme
     from ch_swe_b200.testcases import williamson2
