@@ -25,7 +25,7 @@ GROUP_SOURCES = ["group_f.cu", "group_d.cu"]
 SOURCES = ["swe_api.cu", *STAGE_SOURCES, *FUSED_SOURCES, *GROUP_SOURCES]
 COMMON_HEADERS = ["swe_common.cuh", "swe_kernels.cuh", "swe_sbp.cuh", "sbp63.h", "swe_advective.cuh", "swe_launch.cuh",
                   "swe_fused.cuh", "swe_tma.cuh"]
-UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh", "swe_cgrid.cuh", "swe_diff.cuh"],
+UNIT_HEADERS = {"swe_api.cu": COMMON_HEADERS + ["swe_ah.cuh", "swe_cgrid.cuh", "swe_diff.cuh", "lap63.h"],
                 **{src: COMMON_HEADERS + ["fused_tu.cuh"] for src in FUSED_SOURCES}}
 STAGE_HEADERS = COMMON_HEADERS + ["swe_tiled.cuh", "swe_stage_tu.cuh"]
 UNIT_HEADERS.update({src: COMMON_HEADERS + ["swe_tiled.cuh", "swe_group.cuh", "group_tu.cuh"] for src in GROUP_SOURCES})

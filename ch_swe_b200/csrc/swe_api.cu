@@ -2083,8 +2083,8 @@ static int dif_setup(swe_ctx *c)
     if (!c->dif_b) {
         // b1, b2 of the equiangular vertices on each panel (metric_2d_ecs_mod.f90:377-395),
         // then the 4-2 closure blocks of every boundary line
-        const size_t nb = (size_t)NPAN * 6 * box;
-        std::vector<T> h(nb + (size_t)2 * n * 2 * 48, T(0));
+        const size_t nb = (size_t)NPAN * 6 * box, n42 = (size_t)2 * n * 2 * 48;
+        std::vector<T> h(nb + n42 + (size_t)2 * n * 2 * 108, T(0));
         const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
         for (int p = 0; p < NPAN; p++)
             for (int j = 1; j <= n; j++)
@@ -2101,23 +2101,33 @@ static int dif_setup(swe_ctx *c)
                         h[((size_t)p * 6 + 3 + k) * box + o] = T(b2[k]);
                     }
                 }
-        if (N >= 11) {
-            double D[6][8][8];
-            lap42_dense(D);
-            const HostMetric mxy = host_metric(N, 0.0, 0.0);
-            auto bq = [&](int dir, int line, int k) {   // Qi11 J at (k, line) or Qi22 J at (line, k)
-                const size_t q = dir == 0 ? (size_t)(line - 1) * n + (k - 1) : (size_t)(k - 1) * n + (line - 1);
-                return (dir == 0 ? mxy.Q1[q] : mxy.Q3[q]) * mxy.J[q];
-            };
+        const HostMetric mxy = host_metric(N, 0.0, 0.0);
+        auto bq = [&](int dir, int line, int k) {   // Qi11 J at (k, line) or Qi22 J at (line, k)
+            const size_t q = dir == 0 ? (size_t)(line - 1) * n + (k - 1) : (size_t)(k - 1) * n + (line - 1);
+            return (dir == 0 ? mxy.Q1[q] : mxy.Q3[q]) * mxy.J[q];
+        };
+        // m_rc = sum_k w_rck b_k of each boundary line, rows R x columns C of a dense table
+        auto blocks = [&](const double *W, int R, int C, size_t off) {
             for (int dir = 0; dir < 2; dir++)
                 for (int line = 1; line <= n; line++)
                     for (int side = 0; side < 2; side++)
-                        for (int r = 0; r < 6; r++)
-                            for (int cc = 0; cc < 8; cc++) {
+                        for (int r = 0; r < R; r++)
+                            for (int cc = 0; cc < C; cc++) {
                                 double m = 0.0;
-                                for (int k = 1; k <= 8; k++) m = m + D[r][cc][k - 1] * bq(dir, line, side ? n + 1 - k : k);
-                                h[nb + (size_t)dif_m42_index(n, dir, line, side) + r * 8 + cc] = T(m);
+                                for (int k = 1; k <= C; k++)
+                                    m = m + W[((size_t)r * C + cc) * C + (k - 1)] * bq(dir, line, side ? n + 1 - k : k);
+                                h[off + (size_t)dif_block_index(n, dir, line, side, R * C) + r * C + cc] = T(m);
                             }
+        };
+        if (N >= 11) {
+            double D[6][8][8];
+            lap42_dense(D);
+            blocks(&D[0][0][0], 6, 8, nb);
+        }
+        if (N >= 17) {
+            std::vector<double> E(9 * 12 * 12, 0.0);
+            for (const Lap63Term &q : LAP63_M) E[((size_t)(q.r - 1) * 12 + (q.c - 1)) * 12 + (q.k - 1)] = q.w;
+            blocks(E.data(), 9, 12, nb + n42);
         }
         if (cudaMalloc(&c->dif_b, h.size() * sizeof(T)) != cudaSuccess)
             return fail(c, SWE_ENOMEM, "diffusion basis allocation failed");
@@ -2151,17 +2161,18 @@ static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, const double *
     const AhView<T> &av = ah_view<T>(c);
     const MetricView<T> &mv = metric_view<T>(c);
     const double hxa = 0.5 * 3.141592653589793238462643383279502884 / N * c->cfg.radius;
-    const DifView<T> dv{(const T *)c->dif_b, (const T *)c->dif_b + (size_t)NPAN * 6 * d.ps, hxa * hxa};
+    const T *mb42 = (const T *)c->dif_b + (size_t)NPAN * 6 * d.ps;
+    const DifView<T> dv{(const T *)c->dif_b, mb42, mb42 + (size_t)2 * n * 2 * 48, hxa * hxa};
     const dim3 pb(32, 8), pm((n + 31) / 32, (n + 7) / 8, NPAN * M), pf((n + 31) / 32, (n + 7) / 8, NPAN * M * DIF_FIELDS);
     const dim3 sg((4 * N + 255) / 256, 1, NPAN * M * DIF_FIELDS);
     launch_k(k_dif_prep<T>, pm, pb, 0, c->stream, (const T *)y, X, d, dv);
     // L(X) -> A, then L(A) -> X
     T *src = X, *dst = A;
-    const bool o42 = lap_order == 42;
     for (int pass = 0; pass < 2; pass++) {
-        launch_k(o42 ? k_dif_d1<T, 42> : k_dif_d1<T, 21>, pf, pb, 0, c->stream, (const T *)src, D1X, D1Y, d, av);
-        launch_k(o42 ? k_dif_lap<T, 42> : k_dif_lap<T, 21>, pf, pb, 0, c->stream, (const T *)src, (const T *)D1X,
-                 (const T *)D1Y, R, dst, d, av, dv);
+        launch_k(lap_order == 63 ? k_dif_d1<T, 63> : (lap_order == 42 ? k_dif_d1<T, 42> : k_dif_d1<T, 21>), pf, pb, 0,
+                 c->stream, (const T *)src, D1X, D1Y, d, av);
+        launch_k(lap_order == 63 ? k_dif_lap<T, 63> : (lap_order == 42 ? k_dif_lap<T, 42> : k_dif_lap<T, 21>), pf, pb, 0,
+                 c->stream, (const T *)src, (const T *)D1X, (const T *)D1Y, R, dst, d, av, dv);
         launch_k(k_dif_sync<T>, sg, dim3(256), 0, c->stream, (const T *)R, dst, d);
         std::swap(src, dst);
     }
@@ -2183,11 +2194,12 @@ static int diffusion_check(swe_ctx *c, int lap_order, const char *what)
                     "%s: the reference's narrow-Laplacian diffusion (hordiff_*_Ah_sbp_*_narrow) acts on the Ah "
                     "staggering; this context is not Ah",
                     what);
-    if (lap_order != 21 && lap_order != 42)
-        return fail(c, SWE_EINVAL, "%s: the _sbp_%d_narrow diffusion is not built (the _sbp_21_narrow and "
-                    "_sbp_42_narrow ones are)", what, lap_order);
+    if (lap_order != 21 && lap_order != 42 && lap_order != 63)
+        return fail(c, SWE_EINVAL, "%s: no _sbp_%d_narrow diffusion (the orders are 21, 42 and 63)", what, lap_order);
     if (lap_order == 42 && c->cfg.N < 11)
         return fail(c, SWE_EINVAL, "%s: the _sbp_42_narrow closure blocks of six rows overlap below N = 11", what);
+    if (lap_order == 63 && c->cfg.N < 17)
+        return fail(c, SWE_EINVAL, "%s: the _sbp_63_narrow closure blocks of nine rows overlap below N = 17", what);
     return SWE_OK;
 }
 

@@ -1,7 +1,7 @@
 // swe_diff.cuh -- horizontal diffusion on the Ah staggering, the operator the reference
 // applies after each step of the dynamics (shallow_water_mod.f90:95-100,117-118;
-// operator_swm_diff_mod.f90:27-49) in its _sbp_21_narrow and _sbp_42_narrow forms
-// (hordiff_factory_mod.f90:33-38,61-66):
+// operator_swm_diff_mod.f90:27-49) in its _sbp_21_narrow, _sbp_42_narrow and
+// _sbp_63_narrow forms (hordiff_factory_mod.f90:33-44,61-68):
 //   h:     hordiff_scalar_Ah_sbp_<ord>_narrow   tend = -(c a hx)^4 L(L(h))
 //   u, v:  hordiff_vec_xyz_Ah_sbp_<ord>_narrow  the covariant wind to Cartesian components
 //          with the contravariant basis, the same scalar diffusion of each component,
@@ -9,7 +9,8 @@
 //          vec_math_mod.f90:196-219), then the covariant ECS Ah vector sync
 //          (hordiff_colocated_mod.f90:42-58)
 // L is laplace_Ah_sbp<ord>_narrow (laplace_Ah_sbp21_narrow_mod.f90:25-239,
-// laplace_Ah_sbp42_narrow_mod.f90:27-761): narrow second differences with the variable
+// laplace_Ah_sbp42_narrow_mod.f90:27-761, laplace_Ah_sbp63_narrow_mod.f90:498-1715):
+// narrow second differences with the variable
 // coefficients Qi11 J, Qi22 J, the mixed terms D1(Qi12 J D1 f), boundary penalties,
 // / (hx a)^2 / J, and the Ah scalar sync.
 //
@@ -21,6 +22,7 @@
 // projected back), k_dif_update (the vector sync and the Euler update or the tendency).
 #pragma once
 
+#include "lap63.h"
 #include "swe_ah.cuh"
 
 namespace chswe {
@@ -84,6 +86,11 @@ __host__ __device__ constexpr double lap42_h(int r)
     return r == 1 ? 17.0 / 48 : (r == 2 ? 59.0 / 48 : (r == 3 ? 43.0 / 48 : (r == 4 ? 49.0 / 48 : 1.0)));
 }
 
+// Closure block shape of the narrow second difference of an order: rows x columns.
+template <int ORD> struct NarrowBlock;
+template <> struct NarrowBlock<42> { static constexpr int R = 6, C = 8; };
+template <> struct NarrowBlock<63> { static constexpr int R = 9, C = 12; };
+
 // Row k of the narrow second difference of order ORD on a line of n nodes with the
 // coefficients b(1..n) (the d2f_x / d2f_y sweeps of calc_laplace_tile); M: the line's
 // closure blocks (near end, then far end) for the 4-2 order.
@@ -102,6 +109,34 @@ __device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, con
         const T bm = b(k - 1), bc = b(k), bp = b(k + 1);
         const T cm = (bm + bc) / T(2), cc = -(bm + T(2) * bc + bp) / T(2), cp = (bp + bc) / T(2);
         return (cp * f(k + 1) + cc * f(k) + cm * f(k - 1));
+    } else if constexpr (ORD == 63) {
+        if (k >= 10 && k <= n - 9) {
+            // laplace_Ah_sbp63_narrow_mod.f90:860-880
+            const T bmmm = b(k - 3), bmm = b(k - 2), bm = b(k - 1), bc = b(k), bp = b(k + 1), bpp = b(k + 2),
+                    bppp = b(k + 3);
+            const T a33 = T(11.0 / 360), a32 = T(-1.0 / 40), a31 = T(-1.0 / 40), a30 = T(11.0 / 360);
+            const T a23 = T(-1.0 / 20), a22 = T(-7.0 / 40), a21 = T(3.0 / 10), a20 = T(-7.0 / 40), a2p = T(-1.0 / 20);
+            const T a13 = T(1.0 / 40), a12 = T(3.0 / 10), a11 = T(17.0 / 40), a10 = T(17.0 / 40), a1p = T(3.0 / 10),
+                    a1q = T(1.0 / 40);
+            const T c3 = T(-1.0 / 180), c2 = T(-1.0 / 8), c1 = T(-19.0 / 20), c0 = T(-101.0 / 180);
+            const T cmmm = a33 * bmmm + a32 * bmm + a31 * bm + a30 * bc;
+            const T cmm = a23 * bmmm + a22 * bmm + a21 * bm + a20 * bc + a2p * bp;
+            const T cm = a13 * bmmm + a12 * bmm + a11 * bm + a10 * bc + a1p * bp + a1q * bpp;
+            const T ccc = c3 * bmmm + c2 * bmm + c1 * bm + c0 * bc + c1 * bp + c2 * bpp + c3 * bppp;
+            const T cp = a13 * bppp + a12 * bpp + a11 * bp + a10 * bc + a1p * bm + a1q * bmm;
+            const T cpp = a23 * bppp + a22 * bpp + a21 * bp + a20 * bc + a2p * bm;
+            const T cppp = a33 * bppp + a32 * bpp + a31 * bp + a30 * bc;
+            return (cmmm * f(k - 3) + cmm * f(k - 2) + cm * f(k - 1) + ccc * f(k) + cp * f(k + 1) + cpp * f(k + 2) +
+                    cppp * f(k + 3));
+        }
+        constexpr int R = NarrowBlock<63>::R, C = NarrowBlock<63>::C;
+        const bool lo = k <= R;
+        const int r = lo ? k : n + 1 - k;
+        const T *m = M + (lo ? 0 : R * C) + (r - 1) * C;
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < C; c++) acc = acc + __ldg(m + c) * f(lo ? c + 1 : n - c);
+        return T(1) * acc;
     } else {
         if (k >= 7 && k <= n - 6) {
             const T bmm = b(k - 2), bm = b(k - 1), bc = b(k), bp = b(k + 1), bpp = b(k + 2);
@@ -115,7 +150,7 @@ __device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, con
         }
         const bool lo = k <= 6;
         const int r = lo ? k : n + 1 - k;
-        const T *m = M + (lo ? 0 : 48) + (r - 1) * 8;
+        const T *m = M + (lo ? 0 : NarrowBlock<42>::R * NarrowBlock<42>::C) + (r - 1) * NarrowBlock<42>::C;
         T acc = T(0);
 #pragma unroll
         for (int c = 0; c < 8; c++) acc = acc + __ldg(m + c) * f(lo ? c + 1 : n - c);
@@ -130,19 +165,19 @@ __device__ __forceinline__ int64_t dif_base(const Dims &d, int mem, int q)
 }
 
 // The contravariant basis b1, b2 (Cartesian, unit sphere) of every vertex: [panel][6][box];
-// for the 4-2 order the closure blocks m_rc = sum_k w b_k of every boundary line, built on
-// the host in FP64: [direction x, y][line 1..n][near, far end][row 0..5][column 0..7]
+// for the 4-2 and 6-3 orders the closure blocks m_rc = sum_k w b_k of every boundary line,
+// built on the host in FP64: [direction x, y][line 1..n][near, far end][row][column]
 // (line j of the x direction has b_k = Qi11 J at (k, j) from the near end, at (n+1-k, j)
 // from the far end; the y direction Qi22 J along column i).
 template <class T>
 struct DifView {
     const T *b;
-    const T *m42;
+    const T *m42, *m63;
     double h2;   // (hx a)^2
 };
-__host__ __device__ __forceinline__ int64_t dif_m42_index(int n, int dir, int line, int side)
+__host__ __device__ __forceinline__ int64_t dif_block_index(int n, int dir, int line, int side, int rc)
 {
-    return ((((int64_t)dir * n + (line - 1)) * 2 + side) * 48);
+    return ((((int64_t)dir * n + (line - 1)) * 2 + side) * rc);
 }
 
 // (h, b1 u + b2 v) of the state -> the four scalar fields of each member.
@@ -200,12 +235,15 @@ __global__ void __launch_bounds__(256) k_dif_lap(const T *__restrict__ F, const 
     if (i > n || j > n) return;
     const GV<T> f{F + base, d.P}, dx1{D1X + base, d.P}, dy1{D1Y + base, d.P};
     const GV<T> J{a.J, d.P}, Q1{a.Q1, d.P}, Q3{a.Q3, d.P};
+    // one end's closure block
+    constexpr int RC = ORD == 63 ? NarrowBlock<63>::R * NarrowBlock<63>::C : NarrowBlock<42>::R * NarrowBlock<42>::C;
+    const T *mb = ORD == 63 ? v.m63 : v.m42;
     T d2x = narrow_d2<T, ORD>(i, n, [&](int k) { return Q1(k, j) * J(k, j); }, [&](int k) { return f(k, j); },
-                              v.m42 + dif_m42_index(n, 0, j, 0));
+                              mb + dif_block_index(n, 0, j, 0, RC));
     const T d2y = narrow_d2<T, ORD>(j, n, [&](int l) { return Q3(i, l) * J(i, l); }, [&](int l) { return f(i, l); },
-                                    v.m42 + dif_m42_index(n, 1, i, 0));
+                                    mb + dif_block_index(n, 1, i, 0, RC));
     // the boundary penalties 1/h_1 (-+2 d1f), all on d2f_x and in the reference's order
-    const T pen = ORD == 21 ? T(2) : T(48.0 / 17);
+    const T pen = ORD == 21 ? T(2) : (ORD == 42 ? T(48.0 / 17) : T(43200.0 / 13649));
     if (i == 1) d2x = d2x - T(0.5) * (pen * (T(-2) * dy1(1, j)));
     if (i == n) d2x = d2x - T(0.5) * (pen * (T(2) * dy1(n, j)));
     if (j == 1) d2x = d2x - T(0.5) * (pen * (T(-2) * dx1(i, 1)));

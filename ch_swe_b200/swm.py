@@ -590,7 +590,7 @@ def create_swm_diff_operator(config: dict, domain: Domain) -> OperatorSwmDiff:
     """operator_swm_diff_factory_mod.f90:11-36 with the hordiff names of the Ah staggering
     (hordiff_factory_mod.f90:33-44,61-68): hordiff_uv_name 'hordiff_vec_xyz_Ah_sbp_<o>_narrow'
     with uv_diff_coeff, hordiff_h_name 'hordiff_scalar_Ah_sbp_<o>_narrow' with h_diff_coeff,
-    o = 21 or 42, the same for both."""
+    o = 21, 42 or 63, the same for both."""
     if domain.horizontal_staggering != "Ah":
         raise ValueError("the narrow-Laplacian diffusion operators need a domain created with "
                          "horizontal_staggering='Ah'")
@@ -600,12 +600,14 @@ def create_swm_diff_operator(config: dict, domain: Domain) -> OperatorSwmDiff:
         if not (isinstance(name, str) and name.startswith(prefix) and name.endswith("_narrow")):
             raise ValueError(f"unsupported hordiff operator: {name}")
         orders.add(name[len(prefix):-len("_narrow")])
-    if orders not in ({"21"}, {"42"}):
-        raise ValueError(f"hordiff operators {uv}, {h}: the _sbp_21_narrow and _sbp_42_narrow pairs are built "
-                         "(one order for both)")
+    if orders not in ({"21"}, {"42"}, {"63"}):
+        raise ValueError(f"hordiff operators {uv}, {h}: the _sbp_21_narrow, _sbp_42_narrow and _sbp_63_narrow "
+                         "pairs are built (one order for both)")
     order = int(orders.pop())
     if order == 42 and domain.N < 11:
         raise ValueError("the _sbp_42_narrow diffusion needs N >= 11 (its closure blocks of six rows overlap below)")
+    if order == 63 and domain.N < 17:
+        raise ValueError("the _sbp_63_narrow diffusion needs N >= 17 (its closure blocks of nine rows overlap below)")
     return OperatorSwmDiff(domain, order, config.get("uv_diff_coeff", 0.0), config.get("h_diff_coeff", 0.0))
 
 

@@ -193,8 +193,9 @@ long long swe_group_launch_count(const swe_group *g);
    hordiff_scalar_Ah_sbp_<lap_order>_narrow (h_coeff) for h
    (src/differential_operators/horizontal/hordiff/hordiff_factory_mod.f90:33-44,61-68):
    tendency -(coeff a hx)^4 L(L(f)) of h and of the wind's Cartesian components, L the
-   narrow SBP Laplacian (src/differential_operators/horizontal/laplace/laplace_Ah_sbp21_narrow_mod.f90).
-   lap_order 21 is built; other orders and non-Ah contexts return SWE_EINVAL.  vout != vin. */
+   narrow SBP Laplacian (src/differential_operators/horizontal/laplace/laplace_Ah_sbp{21,42,63}_narrow_mod.f90).
+   lap_order 21, 42 (N >= 11) or 63 (N >= 17); other orders and non-Ah contexts return
+   SWE_EINVAL.  vout != vin. */
 int swe_diffusion_apply(swe_ctx *ctx, swe_stvec *vout, const swe_stvec *vin, int lap_order, double uv_coeff,
                         double h_coeff);
 int swe_diffusion_step(swe_ctx *ctx, swe_stvec *v, double dt, int lap_order, double uv_coeff, double h_coeff);

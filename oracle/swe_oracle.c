@@ -68,6 +68,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include "sbp63.h"
+#include "lap63.h"
 
 #define NPAN 6
 
@@ -1920,7 +1921,8 @@ static const double LAP42_H[6] = {17.0 / 48, 59.0 / 48, 43.0 / 48, 49.0 / 48, 1,
 
 /* the narrow second difference of a line of n nodes (b, f, out 1-based): the d2f_x / d2f_y
    sweeps of calc_laplace_tile (laplace_Ah_sbp21_narrow_mod.f90:116-191 for 2-1,
-   laplace_Ah_sbp42_narrow_mod.f90:121-699 for 4-2) */
+   laplace_Ah_sbp42_narrow_mod.f90:121-699 for 4-2, laplace_Ah_sbp63_narrow_mod.f90:589-1664
+   for 6-3) */
 static void narrow_d2_line(int ord, int n, const double *b, const double *f, double *out)
 {
     if (ord == 21) {
@@ -1934,6 +1936,44 @@ static void narrow_d2_line(int ord, int n, const double *b, const double *f, dou
         bc = b[n];
         const double bm = b[n - 1];
         out[n] = (bc + bm) * f[n - 1] + (-(bc + bm)) * f[n];
+        return;
+    }
+    if (ord == 63) {
+        static double E[9][12][12];
+        static int ready63 = 0;
+        if (!ready63) {
+            for (unsigned q = 0; q < sizeof(LAP63_M) / sizeof(LAP63_M[0]); q++)
+                E[LAP63_M[q].r - 1][LAP63_M[q].c - 1][LAP63_M[q].k - 1] = LAP63_M[q].w;
+            ready63 = 1;
+        }
+        for (int side = 0; side < 2; side++)
+            for (int r = 1; r <= 9; r++) {
+                double acc = 0.0;
+                for (int cc = 1; cc <= 12; cc++) {
+                    double m = 0.0;
+                    for (int k = 1; k <= 12; k++) m = m + E[r - 1][cc - 1][k - 1] * b[side ? n + 1 - k : k];
+                    acc = acc + m * f[side ? n + 1 - cc : cc];
+                }
+                out[side ? n + 1 - r : r] = 1.0 * acc;
+            }
+        /* the interior rows (laplace_Ah_sbp63_narrow_mod.f90:860-880) */
+        const double a33 = 11.0 / 360, a32 = -1.0 / 40, a31 = -1.0 / 40, a30 = 11.0 / 360;
+        const double a23 = -1.0 / 20, a22 = -7.0 / 40, a21 = 3.0 / 10, a20 = -7.0 / 40, a2p = -1.0 / 20;
+        const double a13 = 1.0 / 40, a12 = 3.0 / 10, a11 = 17.0 / 40, a10 = 17.0 / 40, a1p = 3.0 / 10, a1q = 1.0 / 40;
+        const double c3 = -1.0 / 180, c2 = -1.0 / 8, c1 = -19.0 / 20, c0 = -101.0 / 180;
+        for (int i = 10; i <= n - 9; i++) {
+            const double bmmm = b[i - 3], bmm = b[i - 2], bm = b[i - 1], bc = b[i], bp = b[i + 1], bpp = b[i + 2],
+                         bppp = b[i + 3];
+            const double cmmm = a33 * bmmm + a32 * bmm + a31 * bm + a30 * bc;
+            const double cmm = a23 * bmmm + a22 * bmm + a21 * bm + a20 * bc + a2p * bp;
+            const double cm = a13 * bmmm + a12 * bmm + a11 * bm + a10 * bc + a1p * bp + a1q * bpp;
+            const double ccc = c3 * bmmm + c2 * bmm + c1 * bm + c0 * bc + c1 * bp + c2 * bpp + c3 * bppp;
+            const double cp = a13 * bppp + a12 * bpp + a11 * bp + a10 * bc + a1p * bm + a1q * bmm;
+            const double cpp = a23 * bppp + a22 * bpp + a21 * bp + a20 * bc + a2p * bm;
+            const double cppp = a33 * bppp + a32 * bpp + a31 * bp + a30 * bc;
+            out[i] = (cmmm * f[i - 3] + cmm * f[i - 2] + cm * f[i - 1] + ccc * f[i] + cp * f[i + 1] + cpp * f[i + 2] +
+                      cppp * f[i + 3]);
+        }
         return;
     }
     static double D[6][8][8];
@@ -1980,7 +2020,7 @@ static void lap_ah(orc_ctx *c, fld_t *out, fld_t *f, int ord)
     const mesh_t *m = &c->mxy;
     fld_t *d1x = &c->df_d1x, *d1y = &c->df_d1y, *d2x = &c->df_d2x, *d2y = &c->df_d2y;
     fld_t *dxy = &c->df_dxy, *dyx = &c->df_dyx;
-    const double pen = ord == 21 ? 2.0 : 48.0 / 17;   /* 1 / h_1 of the node norm */
+    const double pen = ord == 21 ? 2.0 : (ord == 42 ? 48.0 / 17 : 43200.0 / 13649);   /* 1 / h_1 of the node norm */
     double *bl = malloc(sizeof(double) * (n + 1)), *fl = malloc(sizeof(double) * (n + 1)),
            *ol = malloc(sizeof(double) * (n + 1));
     for (int t = 0; t < NPAN; t++) {
@@ -2633,11 +2673,11 @@ void orc_ah_apply(orc_ctx *c, const double *h, const double *u, const double *v,
     op_apply_ah(c, &c->dh, &c->ah_du, &c->ah_dv, &c->h, &c->ah_u, &c->ah_v);
     fld_to_packed(&c->dh, dh); fld_to_packed(&c->ah_du, du); fld_to_packed(&c->ah_dv, dv);
 }
-/* the narrow Laplacian orders built: 2-1, and 4-2 where its two closure blocks of six rows
-   do not overlap (N >= 11) */
+/* the narrow Laplacian orders built: 2-1, 4-2 where its two closure blocks of six rows do not
+   overlap (N >= 11), 6-3 where its blocks of nine rows do not (N >= 17) */
 static int diff_order_ok(const orc_ctx *c, int lap_order)
 {
-    return lap_order == 21 || (lap_order == 42 && c->N >= 11);
+    return lap_order == 21 || (lap_order == 42 && c->N >= 11) || (lap_order == 63 && c->N >= 17);
 }
 /* the diffusion operator's tendency (lap_order 21 or 42: the _sbp_<order>_narrow operators) */
 int orc_diff_apply(orc_ctx *c, const double *h, const double *u, const double *v, double *dh, double *du, double *dv,

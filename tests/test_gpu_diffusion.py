@@ -1,5 +1,5 @@
 """GPU parity of the diffusion on the Ah staggering (hordiff_vec_xyz_Ah_sbp_<o>_narrow for
-u, v, hordiff_scalar_Ah_sbp_<o>_narrow for h, o = 21 or 42, explicit_Eul1) against the CPU
+u, v, hordiff_scalar_Ah_sbp_<o>_narrow for h, o = 21, 42 or 63, explicit_Eul1) against the CPU
 oracle: FP64 tendencies within 1e-12 relative (max-norm over the field's max-norm) for
 random states whose duplicated panel-edge copies disagree, Euler steps and the driver's
 RK4-then-diffusion loop likewise; FP32 against FP64 in relative L2; members independent;
@@ -52,7 +52,7 @@ def ah_domain(N, precision="fp64", members=1, order=21):
 
 
 @pytest.mark.parametrize("order,N", [(21, 8), (21, 12), (21, 17), (21, 24), (21, 33), (42, 11), (42, 12), (42, 17),
-                                     (42, 24), (42, 33)])
+                                     (42, 24), (42, 33), (63, 17), (63, 24), (63, 33)])
 def test_apply_parity_fp64_random(order, N):
     from ch_swe_b200 import create_stvec_swm, create_swm_diff_operator
     from oracle.oracle import Oracle
@@ -68,7 +68,7 @@ def test_apply_parity_fp64_random(order, N):
     dom.destroy()
 
 
-@pytest.mark.parametrize("order", [21, 42])
+@pytest.mark.parametrize("order", [21, 42, 63])
 def test_euler_steps_and_driver_loop_fp64(order):
     """Six driver steps on a Gaussian hill: RK4 of the Ah linear operator of the same SBP
     order, then one explicit_Eul1 diffusion step (shallow_water_mod.f90:112-118)."""
@@ -189,8 +189,11 @@ def test_refusals():
     with pytest.raises(ValueError):   # one order for both operators
         create_swm_diff_operator({**DIFF, "hordiff_h_name": "hordiff_scalar_Ah_sbp_42_narrow"}, dom)
     with pytest.raises(ValueError):
+        create_swm_diff_operator(diff_config(43), dom)
+    with pytest.raises(ValueError):   # the 6-3 closure blocks overlap below N = 17
         create_swm_diff_operator(diff_config(63), dom)
     x = create_stvec_swm(dom)
+    assert load().swe_diffusion_step(dom.ctx, x.handle, 1.0, 43, 0.03, 0.01) != 0
     assert load().swe_diffusion_step(dom.ctx, x.handle, 1.0, 63, 0.03, 0.01) != 0
     dom.destroy()
     small, _ = ah_domain(8)

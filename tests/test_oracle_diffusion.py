@@ -1,12 +1,13 @@
-"""The oracle's diffusion on the Ah staggering (laplace_Ah_sbp21_narrow and
-laplace_Ah_sbp42_narrow, hordiff_scalar_Ah_sbp_*_narrow, hordiff_vec_xyz_Ah_sbp_*_narrow,
+"""The oracle's diffusion on the Ah staggering (laplace_Ah_sbp{21,42,63}_narrow,
+hordiff_scalar_Ah_sbp_*_narrow, hordiff_vec_xyz_Ah_sbp_*_narrow,
 explicit_Eul1), pinned by properties that a wrong metric factor, closure coefficient,
 penalty sign, stencil offset or sync order breaks: the narrow SBP Laplacian is
 self-adjoint and negative semi-definite in the J-weighted SBP node quadrature of its
 order and conserves mass (continuous fields: the duplicated panel-edge vertices
 agree), kills constants, and converges to the spherical Laplacian (2-1: second order
 inside the panels, first order on their edges, an O(1) error of the panel-wise operator
-at the cube corners; 4-2: second order in L2, first order on the edges and corners);
+at the cube corners; 4-2: second order in L2, first order on the edges and corners;
+6-3: about third order in L2, second order in the max-norm);
 the scalar tendency is -(c a hx)^4 L(L(h)); the wind's follows the Cartesian
 components; one Euler step is v + dt tendency."""
 import numpy as np
@@ -28,11 +29,15 @@ def smooth_field(o, seed):
     return f
 
 
+H63 = [0.3159490740740741, 1.3903935185185186, 0.6275462962962963, 1.2405092592592593, 0.9116898148148148,
+       1.0139120370370371]   # the 6-3 node norm (sbp_operators_collection_mod.f90:38-40)
+
+
 def quad_weights(o, order=21):
-    """J times the node norm: Q21_A, Q42_A (sbp_operators_collection_mod.f90:22,35)."""
+    """J times the node norm: Q21_A, Q42_A, Q63_A (sbp_operators_collection_mod.f90:22,35,38-40)."""
     n = o.N + 1
     w1 = np.ones(n)
-    edge = [0.5] if order == 21 else [17 / 48, 59 / 48, 43 / 48, 49 / 48]
+    edge = {21: [0.5], 42: [17 / 48, 59 / 48, 43 / 48, 49 / 48], 63: H63}[order]
     for i, v in enumerate(edge):
         w1[i] = w1[-1 - i] = v
     return o.metric(0, 0) * w1[None, :, None] * w1[None, None, :]
@@ -43,13 +48,15 @@ def orc(oracle_built):
     return Oracle(16)
 
 
-@pytest.mark.parametrize("order", [21, 42])
-def test_laplacian_kills_constants(orc, order):
-    L = orc.lap_ah(np.full((6, 17, 17), 7.5), order)
+@pytest.mark.parametrize("order", [21, 42, 63])
+def test_laplacian_kills_constants(order, oracle_built):
+    o = Oracle(17)
+    L = o.lap_ah(np.full((6, 18, 18), 7.5), order)
     assert np.abs(L).max() * A * A / 7.5 < 1e-9
 
 
-@pytest.mark.parametrize("order,N", [(21, 8), (21, 13), (21, 16), (42, 12), (42, 16), (42, 23)])
+@pytest.mark.parametrize("order,N", [(21, 8), (21, 13), (21, 16), (42, 12), (42, 16), (42, 23), (63, 17), (63, 24),
+                                     (63, 33)])
 def test_laplacian_self_adjoint_negative_and_conservative(order, N, oracle_built):
     o = Oracle(N)
     w = quad_weights(o, order)
@@ -86,6 +93,18 @@ def test_laplacian42_converges(oracle_built):
     assert err[32][0] / err[16][0] < 0.35     # second order in L2
     assert err[32][1] / err[16][1] < 0.6      # first order at the edges and corners
     assert err[32][1] < 0.05
+
+
+def test_laplacian63_converges(oracle_built):
+    err = {}
+    for N in (24, 48):
+        o = Oracle(N)
+        z = o.metric(0, 7)
+        e = (o.lap_ah(z, 63) + 2.0 / A ** 2 * z) / (2.0 / A ** 2)
+        err[N] = (np.sqrt((e ** 2).mean()), np.abs(e).max())
+    assert err[48][0] / err[24][0] < 0.2      # about third order in L2
+    assert err[48][1] / err[24][1] < 0.35     # second order in the max-norm
+    assert err[48][1] < 5e-3
 
 
 def test_scalar_diffusion_is_minus_c4_bilaplacian(orc):
@@ -131,6 +150,8 @@ def test_euler_step_is_state_plus_dt_tendency(orc):
 
 def test_other_orders_refused(orc, oracle_built):
     with pytest.raises(ValueError):
-        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=63)
+        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=43)
     with pytest.raises(ValueError):   # 4-2's closure blocks overlap below N = 11
         Oracle(10).diff_apply(*(np.zeros((6, 11, 11)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=42)
+    with pytest.raises(ValueError):   # 6-3's closure blocks overlap below N = 17
+        orc.diff_apply(*(np.zeros((6, 17, 17)),) * 3, uv_coeff=0.0, h_coeff=0.0, lap_order=63)
