@@ -358,6 +358,11 @@ def run_nonlinear(args, torch, dist, world):
     return out
 
 
+# the diffusion of the reference's Ah experiments (rh4_run.sh: uv 0.03, h 0.01, explicit_Eul1)
+AH_DIFF = {"hordiff_uv_name": "hordiff_vec_xyz_Ah_sbp_42_narrow", "uv_diff_coeff": 0.03,
+           "hordiff_h_name": "hordiff_scalar_Ah_sbp_42_narrow", "h_diff_coeff": 0.01}
+
+
 def run_ah(args, torch, dist, world):
     """The Ah staggering of the linear operator (h, u, v on the vertices, node SBP 4-2
     operators with projections) on the day workload: C192, dt 150 s, 576 RK4 steps,
@@ -388,12 +393,37 @@ def run_ah(args, torch, dist, world):
         from ch_swe_b200 import replicas
         ms = replicas.max_over_ranks(ms, dist, device="cuda")
     m1, e1 = op.integrals(x)
+    # the driver loop with the diffusion step after every RK4 step, in the same graphs
+    from ch_swe_b200 import create_swm_diff_operator
+    dif = create_swm_diff_operator(AH_DIFF, dom)
+    dom.set_diffusion(dif)
+    x.upload(h, z, z)
+    rk.steps(x, op, dom, DT, 8)
+    x.upload(h, z, z)
+    md0, _ = op.integrals(x)
+    torch.cuda.synchronize()
+    a.record(stream)
+    rk.steps(x, op, dom, DT, NSTEPS)
+    b.record(stream)
+    torch.cuda.synchronize()
+    msd = a.elapsed_time(b)
+    if world > 1:
+        from ch_swe_b200 import replicas
+        msd = replicas.max_over_ranks(msd, dist, device="cuda")
+    md1, _ = op.integrals(x)
+    dom.set_diffusion(None)
     dom.destroy()
     return {"workload": f"C{N_CELLS} linear SWE on the Ah staggering (div_ah_sbp_proj_42, grad_ah_sbp_proj_42, "
                         f"coriolis_colocated, co2contra_colocated), FP32, dt {DT:g} s, {NSTEPS} RK4 steps, "
                         "the day workload's Gaussian with the wind at rest",
             "value": world * 6 * N_CELLS ** 2 * NSTEPS / (ms / 1e3), "unit": "cell-updates/s",
-            "ms_total": ms, "mass_rel_drift": (m1 - m0) / abs(m0), "energy_rel_drift": (e1 - e0) / abs(e0)}
+            "ms_total": ms, "mass_rel_drift": (m1 - m0) / abs(m0), "energy_rel_drift": (e1 - e0) / abs(e0),
+            "with_diffusion": {
+                "what": "each RK4 step followed by one explicit_Eul1 step of " + AH_DIFF["hordiff_uv_name"] + " (uv "
+                        f"coefficient {AH_DIFF['uv_diff_coeff']}) and " + AH_DIFF["hordiff_h_name"] +
+                        f" (h coefficient {AH_DIFF['h_diff_coeff']}), captured with the RK4 stages",
+                "value": world * 6 * N_CELLS ** 2 * NSTEPS / (msd / 1e3), "unit": "cell-updates/s",
+                "ms_total": msd, "mass_rel_drift": (md1 - md0) / abs(md0)}}
 
 
 def run_serving(args, torch):
@@ -681,12 +711,15 @@ def run_profile_leg(args):
         op = create_swm_operator(dom.grav, {"swm_operator_type": "advective_swm_operator"}, dom)
         st = create_stvec_swm(dom).upload(*testcases.williamson2(NL_N, axis=axis))
         dt = NL_DT
-    elif args.profile_leg == "ah":
+    elif args.profile_leg in ("ah", "ah_diffusion"):
         dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN, horizontal_staggering="Ah")
         op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
         h = workload_ic()[0][0]
         st = create_stvec_swm(dom).upload(h, np.zeros_like(h), np.zeros_like(h))
         dt = DT
+        if args.profile_leg == "ah_diffusion":
+            from ch_swe_b200 import create_swm_diff_operator
+            dom.set_diffusion(create_swm_diff_operator(AH_DIFF, dom))
     else:
         dom = create_domain(N_CELLS, precision="fp32", h_mean=H_MEAN)
         op = create_swm_operator(dom.grav, {"swm_operator_type": "linear_swm_operator", "h_mean": H_MEAN}, dom)
@@ -724,7 +757,7 @@ def main():
     ap.add_argument("--rk4-steps", type=int, default=NSTEPS,
                     help="RK4 steps per bench step (default: one day = 576; shorter only for profiling runs)")
     ap.add_argument("--no-ah", action="store_true", help="skip the Ah-staggering leg")
-    ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear", "ah"], default=None,
+    ap.add_argument("--profile-leg", choices=["day", "ensemble", "nonlinear", "ah", "ah_diffusion"], default=None,
                     help="run --rk4-steps steps of one workload only (for ncu captures; prints no bench line)")
     args = ap.parse_args()
     if args.profile_leg:
