@@ -2083,8 +2083,8 @@ static int dif_setup(swe_ctx *c)
     if (!c->dif_b) {
         // b1, b2 of the equiangular vertices on each panel (metric_2d_ecs_mod.f90:377-395),
         // then the 4-2 closure blocks of every boundary line
-        const size_t nb = (size_t)NPAN * 6 * box, n42 = (size_t)2 * n * 2 * 48;
-        std::vector<T> h(nb + n42 + (size_t)2 * n * 2 * 108, T(0));
+        const size_t nb = (size_t)NPAN * 6 * box, n42 = (size_t)2 * n * 2 * 48, n63 = (size_t)2 * n * 2 * 108;
+        std::vector<T> h(nb + n42 + n63 + (size_t)2 * (3 + 5 + 7) * box, T(0));
         const double pi = 3.141592653589793238462643383279502884, hx = 0.5 * pi / N;
         for (int p = 0; p < NPAN; p++)
             for (int j = 1; j <= n; j++)
@@ -2129,6 +2129,51 @@ static int dif_setup(swe_ctx *c)
             for (const Lap63Term &q : LAP63_M) E[((size_t)(q.r - 1) * 12 + (q.c - 1)) * 12 + (q.k - 1)] = q.w;
             blocks(E.data(), 9, 12, nb + n42);
         }
+        // interior stencil weights of every vertex, the expressions of the reference's
+        // interior sweeps (laplace_Ah_sbp21_narrow_mod.f90:131-143,
+        // laplace_Ah_sbp42_narrow_mod.f90:263-282, laplace_Ah_sbp63_narrow_mod.f90:860-880)
+        const size_t ow = nb + n42 + n63;
+        for (int dir = 0; dir < 2; dir++)
+            for (int j = 1; j <= n; j++)
+                for (int i = 1; i <= n; i++) {
+                    const int k = dir == 0 ? i : j, line = dir == 0 ? j : i;
+                    auto bb = [&](int q) { return bq(dir, line, q); };
+                    const size_t o = (size_t)box_off(P, i, j);
+                    auto put = [&](int ord, int q, double w) {
+                        const size_t base = ow + (ord == 21 ? 0 : (ord == 42 ? 2 * 3 * box : 2 * 8 * box));
+                        h[base + ((size_t)dir * narrow_width(ord) + q) * box + o] = T(w);
+                    };
+                    if (k > 1 && k < n) {
+                        const double bm = bb(k - 1), bc = bb(k), bp = bb(k + 1);
+                        put(21, 0, (bm + bc) / 2);
+                        put(21, 1, -(bm + 2 * bc + bp) / 2);
+                        put(21, 2, (bp + bc) / 2);
+                    }
+                    if (k >= 7 && k <= n - 6) {
+                        const double bmm = bb(k - 2), bm = bb(k - 1), bc = bb(k), bp = bb(k + 1), bpp = bb(k + 2);
+                        put(42, 0, 1.0 / 6.0 * bm - 1.0 / 8.0 * bmm - 1.0 / 8.0 * bc);
+                        put(42, 1, 1.0 / 6.0 * bmm + 1.0 / 6.0 * bp + 1.0 / 2.0 * bm + 1.0 / 2.0 * bc);
+                        put(42, 2, -1.0 / 24.0 * bmm - 5.0 / 6.0 * bm - 5.0 / 6.0 * bp - 1.0 / 24.0 * bpp - 3.0 / 4.0 * bc);
+                        put(42, 3, 1.0 / 6.0 * bm + 1.0 / 6.0 * bpp + 1.0 / 2.0 * bc + 1.0 / 2.0 * bp);
+                        put(42, 4, 1.0 / 6.0 * bp - 1.0 / 8.0 * bc - 1.0 / 8.0 * bpp);
+                    }
+                    if (k >= 10 && k <= n - 9) {
+                        const double bmmm = bb(k - 3), bmm = bb(k - 2), bm = bb(k - 1), bc = bb(k), bp = bb(k + 1),
+                                     bpp = bb(k + 2), bppp = bb(k + 3);
+                        const double a33 = 11.0 / 360, a32 = -1.0 / 40, a31 = -1.0 / 40, a30 = 11.0 / 360;
+                        const double a23 = -1.0 / 20, a22 = -7.0 / 40, a21 = 3.0 / 10, a20 = -7.0 / 40, a2p = -1.0 / 20;
+                        const double a13 = 1.0 / 40, a12 = 3.0 / 10, a11 = 17.0 / 40, a10 = 17.0 / 40, a1p = 3.0 / 10,
+                                     a1q = 1.0 / 40;
+                        const double c3 = -1.0 / 180, c2 = -1.0 / 8, c1 = -19.0 / 20, c0 = -101.0 / 180;
+                        put(63, 0, a33 * bmmm + a32 * bmm + a31 * bm + a30 * bc);
+                        put(63, 1, a23 * bmmm + a22 * bmm + a21 * bm + a20 * bc + a2p * bp);
+                        put(63, 2, a13 * bmmm + a12 * bmm + a11 * bm + a10 * bc + a1p * bp + a1q * bpp);
+                        put(63, 3, c3 * bmmm + c2 * bmm + c1 * bm + c0 * bc + c1 * bp + c2 * bpp + c3 * bppp);
+                        put(63, 4, a13 * bppp + a12 * bpp + a11 * bp + a10 * bc + a1p * bm + a1q * bmm);
+                        put(63, 5, a23 * bppp + a22 * bpp + a21 * bp + a20 * bc + a2p * bm);
+                        put(63, 6, a33 * bppp + a32 * bpp + a31 * bp + a30 * bc);
+                    }
+                }
         if (cudaMalloc(&c->dif_b, h.size() * sizeof(T)) != cudaSuccess)
             return fail(c, SWE_ENOMEM, "diffusion basis allocation failed");
         CU(c, cudaMemcpy(c->dif_b, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
@@ -2161,8 +2206,9 @@ static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, const double *
     const AhView<T> &av = ah_view<T>(c);
     const MetricView<T> &mv = metric_view<T>(c);
     const double hxa = 0.5 * 3.141592653589793238462643383279502884 / N * c->cfg.radius;
-    const T *mb42 = (const T *)c->dif_b + (size_t)NPAN * 6 * d.ps;
-    const DifView<T> dv{(const T *)c->dif_b, mb42, mb42 + (size_t)2 * n * 2 * 48, hxa * hxa};
+    const T *mb42 = (const T *)c->dif_b + (size_t)NPAN * 6 * d.ps, *mb63 = mb42 + (size_t)2 * n * 2 * 48;
+    const T *w21 = mb63 + (size_t)2 * n * 2 * 108, *w42 = w21 + (size_t)2 * 3 * d.ps, *w63 = w42 + (size_t)2 * 5 * d.ps;
+    const DifView<T> dv{(const T *)c->dif_b, mb42, mb63, w21, w42, w63, hxa * hxa};
     const dim3 pb(32, 8), pm((n + 31) / 32, (n + 7) / 8, NPAN * M), pf((n + 31) / 32, (n + 7) / 8, NPAN * M * DIF_FIELDS);
     const dim3 sg((4 * N + 255) / 256, 1, NPAN * M * DIF_FIELDS);
     launch_k(k_dif_prep<T>, pm, pb, 0, c->stream, (const T *)y, X, d, dv);

@@ -95,40 +95,30 @@ template <> struct NarrowBlock<63> { static constexpr int R = 9, C = 12; };
 // coefficients b(1..n) (the d2f_x / d2f_y sweeps of calc_laplace_tile); M: the line's
 // closure blocks (near end, then far end) for the 4-2 order.
 template <class T, int ORD, class B, class F>
-__device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, const T *M)
+__device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, const T *M, const T *Wi, int64_t ws)
 {
+    // inside the closure rows: the interior stencil with the vertex's tabulated weights
+    // Wi[q * ws], q over the offsets -h .. h, summed in the reference's order
+    if constexpr (ORD == 21) {
+        if (k > 1 && k < n) return (__ldg(Wi + 2 * ws) * f(k + 1) + __ldg(Wi + ws) * f(k) + __ldg(Wi) * f(k - 1));
+    } else if constexpr (ORD == 42) {
+        if (k >= 7 && k <= n - 6)
+            return (__ldg(Wi) * f(k - 2) + __ldg(Wi + ws) * f(k - 1) + __ldg(Wi + 2 * ws) * f(k) +
+                    __ldg(Wi + 3 * ws) * f(k + 1) + __ldg(Wi + 4 * ws) * f(k + 2));
+    } else {
+        if (k >= 10 && k <= n - 9)
+            return (__ldg(Wi) * f(k - 3) + __ldg(Wi + ws) * f(k - 2) + __ldg(Wi + 2 * ws) * f(k - 1) +
+                    __ldg(Wi + 3 * ws) * f(k) + __ldg(Wi + 4 * ws) * f(k + 1) + __ldg(Wi + 5 * ws) * f(k + 2) +
+                    __ldg(Wi + 6 * ws) * f(k + 3));
+    }
     if constexpr (ORD == 21) {
         if (k == 1) {
             const T bc = b(1), bp = b(2);
             return (-(bc + bp) * f(1) + (bc + bp) * f(2));
         }
-        if (k == n) {
-            const T bc = b(n), bm = b(n - 1);
-            return (bc + bm) * f(n - 1) + (-(bc + bm)) * f(n);
-        }
-        const T bm = b(k - 1), bc = b(k), bp = b(k + 1);
-        const T cm = (bm + bc) / T(2), cc = -(bm + T(2) * bc + bp) / T(2), cp = (bp + bc) / T(2);
-        return (cp * f(k + 1) + cc * f(k) + cm * f(k - 1));
+        const T bc = b(n), bm = b(n - 1);   // k == n
+        return (bc + bm) * f(n - 1) + (-(bc + bm)) * f(n);
     } else if constexpr (ORD == 63) {
-        if (k >= 10 && k <= n - 9) {
-            // laplace_Ah_sbp63_narrow_mod.f90:860-880
-            const T bmmm = b(k - 3), bmm = b(k - 2), bm = b(k - 1), bc = b(k), bp = b(k + 1), bpp = b(k + 2),
-                    bppp = b(k + 3);
-            const T a33 = T(11.0 / 360), a32 = T(-1.0 / 40), a31 = T(-1.0 / 40), a30 = T(11.0 / 360);
-            const T a23 = T(-1.0 / 20), a22 = T(-7.0 / 40), a21 = T(3.0 / 10), a20 = T(-7.0 / 40), a2p = T(-1.0 / 20);
-            const T a13 = T(1.0 / 40), a12 = T(3.0 / 10), a11 = T(17.0 / 40), a10 = T(17.0 / 40), a1p = T(3.0 / 10),
-                    a1q = T(1.0 / 40);
-            const T c3 = T(-1.0 / 180), c2 = T(-1.0 / 8), c1 = T(-19.0 / 20), c0 = T(-101.0 / 180);
-            const T cmmm = a33 * bmmm + a32 * bmm + a31 * bm + a30 * bc;
-            const T cmm = a23 * bmmm + a22 * bmm + a21 * bm + a20 * bc + a2p * bp;
-            const T cm = a13 * bmmm + a12 * bmm + a11 * bm + a10 * bc + a1p * bp + a1q * bpp;
-            const T ccc = c3 * bmmm + c2 * bmm + c1 * bm + c0 * bc + c1 * bp + c2 * bpp + c3 * bppp;
-            const T cp = a13 * bppp + a12 * bpp + a11 * bp + a10 * bc + a1p * bm + a1q * bmm;
-            const T cpp = a23 * bppp + a22 * bpp + a21 * bp + a20 * bc + a2p * bm;
-            const T cppp = a33 * bppp + a32 * bpp + a31 * bp + a30 * bc;
-            return (cmmm * f(k - 3) + cmm * f(k - 2) + cm * f(k - 1) + ccc * f(k) + cp * f(k + 1) + cpp * f(k + 2) +
-                    cppp * f(k + 3));
-        }
         constexpr int R = NarrowBlock<63>::R, C = NarrowBlock<63>::C;
         const bool lo = k <= R;
         const int r = lo ? k : n + 1 - k;
@@ -138,16 +128,6 @@ __device__ __forceinline__ T narrow_d2(int k, int n, const B &b, const F &f, con
         for (int c = 0; c < C; c++) acc = acc + __ldg(m + c) * f(lo ? c + 1 : n - c);
         return T(1) * acc;
     } else {
-        if (k >= 7 && k <= n - 6) {
-            const T bmm = b(k - 2), bm = b(k - 1), bc = b(k), bp = b(k + 1), bpp = b(k + 2);
-            const T cmm = T(1.0 / 6.0) * bm - T(1.0 / 8.0) * bmm - T(1.0 / 8.0) * bc;
-            const T cm = T(1.0 / 6.0) * bmm + T(1.0 / 6.0) * bp + T(1.0 / 2.0) * bm + T(1.0 / 2.0) * bc;
-            const T cc = -T(1.0 / 24.0) * bmm - T(5.0 / 6.0) * bm - T(5.0 / 6.0) * bp - T(1.0 / 24.0) * bpp -
-                         T(3.0 / 4.0) * bc;
-            const T cp = T(1.0 / 6.0) * bm + T(1.0 / 6.0) * bpp + T(1.0 / 2.0) * bc + T(1.0 / 2.0) * bp;
-            const T cpp = T(1.0 / 6.0) * bp - T(1.0 / 8.0) * bc - T(1.0 / 8.0) * bpp;
-            return (cmm * f(k - 2) + cm * f(k - 1) + cc * f(k) + cp * f(k + 1) + cpp * f(k + 2));
-        }
         const bool lo = k <= 6;
         const int r = lo ? k : n + 1 - k;
         const T *m = M + (lo ? 0 : NarrowBlock<42>::R * NarrowBlock<42>::C) + (r - 1) * NarrowBlock<42>::C;
@@ -169,12 +149,16 @@ __device__ __forceinline__ int64_t dif_base(const Dims &d, int mem, int q)
 // built on the host in FP64: [direction x, y][line 1..n][near, far end][row][column]
 // (line j of the x direction has b_k = Qi11 J at (k, j) from the near end, at (n+1-k, j)
 // from the far end; the y direction Qi22 J along column i).
+// The interior stencil weights of every vertex (the metric is the same on every panel):
+// [direction x, y][offset -h .. h][box] for each order (3, 5, 7 offsets), host-built in FP64.
 template <class T>
 struct DifView {
     const T *b;
     const T *m42, *m63;
+    const T *w21, *w42, *w63;
     double h2;   // (hx a)^2
 };
+__host__ __device__ constexpr int narrow_width(int ord) { return ord == 21 ? 3 : (ord == 42 ? 5 : 7); }
 __host__ __device__ __forceinline__ int64_t dif_block_index(int n, int dir, int line, int side, int rc)
 {
     return ((((int64_t)dir * n + (line - 1)) * 2 + side) * rc);
@@ -238,10 +222,12 @@ __global__ void __launch_bounds__(256) k_dif_lap(const T *__restrict__ F, const 
     // one end's closure block
     constexpr int RC = ORD == 63 ? NarrowBlock<63>::R * NarrowBlock<63>::C : NarrowBlock<42>::R * NarrowBlock<42>::C;
     const T *mb = ORD == 63 ? v.m63 : v.m42;
+    const T *wi = (ORD == 21 ? v.w21 : (ORD == 42 ? v.w42 : v.w63)) + box_off(d.P, i, j);
+    const int64_t wd = (int64_t)narrow_width(ORD) * d.ps;   // the y weights follow the x weights
     T d2x = narrow_d2<T, ORD>(i, n, [&](int k) { return Q1(k, j) * J(k, j); }, [&](int k) { return f(k, j); },
-                              mb + dif_block_index(n, 0, j, 0, RC));
+                              mb + dif_block_index(n, 0, j, 0, RC), wi, d.ps);
     const T d2y = narrow_d2<T, ORD>(j, n, [&](int l) { return Q3(i, l) * J(i, l); }, [&](int l) { return f(i, l); },
-                                    mb + dif_block_index(n, 1, i, 0, RC));
+                                    mb + dif_block_index(n, 1, i, 0, RC), wi + wd, d.ps);
     // the boundary penalties 1/h_1 (-+2 d1f), all on d2f_x and in the reference's order
     const T pen = ORD == 21 ? T(2) : (ORD == 42 ? T(48.0 / 17) : T(43200.0 / 13649));
     if (i == 1) d2x = d2x - T(0.5) * (pen * (T(-2) * dy1(1, j)));
