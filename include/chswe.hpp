@@ -117,6 +117,11 @@ class operator_swm_diff_gpu_t {
     {
         check(swe_diffusion_step(d_.ctx(), v0.handle(), dt, order_, uv_, h_), d_.ctx(), "diffusion step");
     }
+    // the driver loop (src/models/shallow_water/shallow_water_mod.f90:112-118) on the device:
+    // every RK4 step of the domain is followed by euler_step, inside the captured graphs;
+    // detach() restores plain RK4 steps
+    void attach() { check(swe_set_diffusion(d_.ctx(), order_, uv_, h_), d_.ctx(), "set diffusion"); }
+    void detach() { check(swe_set_diffusion(d_.ctx(), 0, 0.0, 0.0), d_.ctx(), "set diffusion"); }
 
   private:
     const domain_gpu_t &d_;
