@@ -101,7 +101,7 @@ class rk4_gpu_t {
 
 // operator_swm_diff_t (src/models/shallow_water/operator/operator_swm_diff_mod.f90:27-49) on the
 // Ah staggering: hordiff_vec_xyz_Ah_sbp_<order>_narrow and hordiff_scalar_Ah_sbp_<order>_narrow,
-// order 21 or 42.
+// order 21, 42 (N >= 11) or 63 (N >= 17).
 class operator_swm_diff_gpu_t {
   public:
     operator_swm_diff_gpu_t(const domain_gpu_t &d, int order, double uv_coeff, double h_coeff)
