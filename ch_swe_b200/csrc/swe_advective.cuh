@@ -11,10 +11,10 @@
 //            the panel edges interpolated along the neighbour's grid lines; also the
 //            flux edge strips for the divergence sync
 //   k_edge   (swe_kernels.cuh) Coriolis from the ut/vt strips, divergence from the flux strips
-//   k_uhvh   ut, vt interpolated to the xy points
 //   k_vhalo  covariant u, v at the virtual points beyond the panel edges (bicubic
 //            from the neighbour face, projected on this face's basis)
-//   k_adv    up4 advection and Christoffel terms of u and v
+//   k_advt   up4 advection and Christoffel terms of u and v, with ut, vt interpolated
+//            to the xy points and back inside its shared-memory tiles
 //   k_stage  (swe_tiled.cuh) divergence of the flux, gradient, Coriolis, A and the RK update
 #pragma once
 
@@ -34,7 +34,7 @@ struct AdvView {
     const int *hidx;   //   4 ints per point: ixu, iyu, ixv, iyv
     const T *hw;       //   18 per point: wxu[4], wyu[4], wxv[4], wyv[4], a.b1, a.b2
     const T *S;        // Christoffel S on the y mesh (3 boxes: S11, S12, S22 of u) then x mesh (3 boxes, v)
-    T neg_radius;      // -a, the scale of the covariant Christoffel terms
+    T inv_neg_radius;  // -1/a, the scale of the covariant Christoffel terms
     int hp;            // vector halo points per panel: 24 N + 12
 };
 
@@ -221,28 +221,6 @@ __global__ void __launch_bounds__(256) k_flux(const T *__restrict__ Y, const T *
 }
 
 // ---------------------------------------------------------------------------
-// k_uhvh: uh = I_c2i,x(ut), vh = I_c2i,y(vt) on the xy points (interp2d_uv2pvec_Ch_sbp42)
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(256) k_uhvh(const T *__restrict__ W, T *__restrict__ PH, Dims d,
-                                              const double *__restrict__ dtm)
-{
-    const int N = d.N, n = N + 1;
-    const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
-    if (member_frozen(dtm, mem)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    pdl_trigger();
-    pdl_wait();
-    if (i > n || j > n) return;
-    const int64_t po = mem * d.ms + t * d.ps;
-    const GV<T> U{W + po + d.fs, d.P}, V{W + po + 2 * d.fs, d.P};
-    const int64_t o = box_off(d.P, i, j);
-    PH[po + d.fs + o] = ic2i<T>(i, n, [&](int c) { return U(c, j); });
-    PH[po + 2 * d.fs + o] = ic2i<T>(j, n, [&](int c) { return V(i, c); });
-    (void)N;
-}
-
-// ---------------------------------------------------------------------------
 // k_vhalo: covariant wind at the virtual points beyond the panel edges
 // (ecs_halo_vec_Ch_mod.f90:29-60): bicubic interpolation of the source face's u (y
 // mesh) and v (x mesh), projected on this face's basis vector.
@@ -303,90 +281,166 @@ __device__ __forceinline__ T v_ext(const T *y, const T *vh, const Dims &d, int h
     return __ldg(y + t * d.ps + 2 * d.fs + (j - 1 + MG) * d.P + (i - 1 + MG));
 }
 
-// up4 derivative along one direction (v_nabla_mod.f90:127-141), values at offsets -3..3
+// up4 derivative along one direction (v_nabla_mod.f90:127-141), values at offsets -3..3;
+// the reference's division by 12 is a product with 1/12 here (within rounding)
 template <class T>
 __device__ __forceinline__ T up4_diff(T c, const T f[7])
 {
     const T zl = T(0.5) + copysign(T(0.5), c), zr = T(1) - zl;
     return (zl * (T(3) * f[4] + T(10) * f[3] - T(18) * f[2] + T(6) * f[1] - f[0]) -
-            zr * (T(3) * f[2] + T(10) * f[3] - T(18) * f[4] + T(6) * f[5] - f[6])) /
-           T(12);
+            zr * (T(3) * f[2] + T(10) * f[3] - T(18) * f[4] + T(6) * f[5] - f[6])) *
+           T(1.0 / 12.0);
 }
 
 // ---------------------------------------------------------------------------
-// k_adv: A_u, A_v = up4 advection + Christoffel terms (before the edge sync)
+// k_advt: A_u, A_v = up4 advection + Christoffel terms (before the edge sync), tiled.
+// A block takes ADV_TX x TY xy points of one
+// panel and stages in shared memory
+//   us, vs  the covariant u (y mesh) and v (x mesh) over the tile and the 3-point reach
+//           of the up4 stencils, the points beyond the panel from the vector halo;
+//   vhs     vh = I_c2i,y(vt) on the xy points of the tile's rows and of the columns the
+//           i2c rows of its u points read;
+//   uhs     uh = I_c2i,x(ut) likewise for the v points
+// (interp2d_uv2pvec_Ch_sbp42), then evaluates each point from shared memory: v at u
+// points = I_i2c,x(vh), u at v points = I_i2c,y(uh) (interp2d_pvec2uv_Ch_sbp42).  Tiles
+// whose windows and interpolation stencils lie inside the panel fill them with direct
+// loads and the interior interpolation rows; the others through the vector halo and the
+// closure rows.  The interpolations take the operands of the point-wise formulas in the
+// same order.
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(256) k_adv(const T *__restrict__ Y, const T *__restrict__ W,
-                                             const T *__restrict__ PH, const T *__restrict__ VH, T *__restrict__ A,
-                                             Dims d, AdvView<T> av, MetricView<T> m, const double *__restrict__ dtm)
+constexpr int ADV_TX = 32, ADV_THREADS = 256, ADV_WW = ADV_TX + 6;
+
+template <class T, int TY>
+__global__ void __launch_bounds__(ADV_THREADS) k_advt(const T *__restrict__ Y, const T *__restrict__ W,
+                                                      const T *__restrict__ VH, T *__restrict__ A, Dims d,
+                                                      AdvView<T> av, MetricView<T> m, const double *__restrict__ dtm)
 {
+    constexpr int WH = TY + 6, WW = ADV_WW, TX = ADV_TX;
+    __shared__ T us[WH * WW], vs[WH * WW];   // cell (c, r) = index (i0 - 2 + c, j0 - 2 + r)
+    __shared__ T vhs[TY * WW];               // rows j0+1 .. j0+TY, columns i0-2 .. i0+TX+3
+    __shared__ T uhs[WH * TX];               // rows j0-2 .. j0+TY+3, columns i0+1 .. i0+TX
     const int N = d.N, n = N + 1;
     const int mem = blockIdx.z / NPAN, t = blockIdx.z % NPAN;
     if (member_frozen(dtm, mem)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int tx = threadIdx.x, tid = threadIdx.y * 32 + threadIdx.x;
     pdl_trigger();
     pdl_wait();
-    if (i > n || j > n) return;
     const T *y = Y + mem * d.ms;
     const T *vh = VH + (int64_t)mem * NPAN * av.hp;
     const int64_t po = mem * d.ms + t * d.ps;
-    const int64_t o = box_off(d.P, i, j);
-    const int64_t box = d.ps;
-    if (i <= N) {
-        // u point: ut and v_at_u = I_i2c,x(vh)
-        const T a = __ldg(W + po + d.fs + o);
-        const GV<T> VHp{PH + po + 2 * d.fs, d.P};
-        const T b = ii2c<T>(i, N, [&](int c) { return VHp(c, j); });
-        T fx[7], fy[7];
-        const T *ur = y + t * d.ps + d.fs + (j - 1 + MG) * d.P + (i - 1 + MG);   // u(i, j)
-        if (i >= 4 && i <= N - 3) {
+    const int P = d.P;
+    const GV<T> UT{W + po + d.fs, P}, VT{W + po + 2 * d.fs, P};
+    // the tile's u points: i in (i0, iu], j in (j0, ju]; v points: i in (i0, iv], j in (j0, jv]
+    const int iu = min(i0 + TX, N), ju = min(j0 + TY, n);
+    const int iv = min(i0 + TX, n), jv = min(j0 + TY, N);
+    if (i0 >= 4 && j0 >= 4 && i0 + TX + 4 <= N && j0 + TY + 4 <= N) {
+        // windows, interpolation stencils and i2c rows all inside the panel
+        const T *ub = y + t * d.ps + d.fs + (int64_t)(j0 - 3 + MG) * P + (i0 - 3 + MG);   // u(i0-2, j0-2)
+        const T *vb = ub + d.fs;
 #pragma unroll
-            for (int k = 0; k < 7; k++) fx[k] = __ldg(ur + (k - 3));
-        } else {
-#pragma unroll
-            for (int k = 0; k < 7; k++) fx[k] = u_ext(y, vh, d, av.hp, t, i - 3 + k, j);
+        for (int q = 0; q < (WH + 7) / 8; q++) {
+            const int r = threadIdx.y + 8 * q;
+            if (r < WH) {
+                const int64_t ro = (int64_t)r * P;
+                us[r * WW + tx] = __ldg(ub + ro + tx);
+                vs[r * WW + tx] = __ldg(vb + ro + tx);
+                if (tx < WW - 32) {
+                    us[r * WW + tx + 32] = __ldg(ub + ro + tx + 32);
+                    vs[r * WW + tx + 32] = __ldg(vb + ro + tx + 32);
+                }
+            }
         }
-        if (j >= 4 && j <= N - 2) {
-#pragma unroll
-            for (int k = 0; k < 7; k++) fy[k] = __ldg(ur + (k - 3) * d.P);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 7; k++) fy[k] = u_ext(y, vh, d, av.hp, t, i, j - 3 + k);
+        const T *vt0 = VT.p + (int64_t)(j0 + MG) * P + (i0 - 3 + MG);   // vt(i0-2, j0+1)
+#pragma unroll 2
+        for (int e = tid; e < TY * WW; e += ADV_THREADS) {
+            const int r = e / WW, c = e % WW;
+            const T *q = vt0 + (int64_t)r * P + c;   // vt(i0-2+c, j0+1+r)
+            vhs[e] = (T(9) * (__ldg(q) + __ldg(q - P)) - (__ldg(q + P) + __ldg(q - 2 * P))) * T(0.0625);
         }
-        const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
-        T tend = -(a * dx + b * dy) * m.inv_hxa;
-        const T g11 = __ldg(av.S + o), g21 = __ldg(av.S + box + o), g22 = __ldg(av.S + 2 * box + o);
-        tend = tend - (a * a * g11 + T(2) * a * b * g21 + b * b * g22) / av.neg_radius;
-        A[po + d.fs + o] = tend;
+        const T *ut0 = UT.p + (int64_t)(j0 - 3 + MG) * P + (i0 + MG);   // ut(i0+1, j0-2)
+#pragma unroll 2
+        for (int e = tid; e < WH * TX; e += ADV_THREADS) {
+            const int r = e / TX, c = e % TX;
+            const T *q = ut0 + (int64_t)r * P + c;   // ut(i0+1+c, j0-2+r)
+            uhs[e] = (T(9) * (__ldg(q) + __ldg(q - 1)) - (__ldg(q + 1) + __ldg(q - 2))) * T(0.0625);
+        }
+    } else {
+#pragma unroll 1
+        for (int e = tid; e < WH * WW; e += ADV_THREADS) {
+            const int r = e / WW, c = e % WW;
+            const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+            // u: the x reach of the rows (j0, ju], the y reach of the columns (i0, iu]
+            if ((jj > j0 && jj <= ju && ii <= iu + 3) || (ii > i0 && ii <= iu && jj <= ju + 3))
+                us[e] = u_ext(y, vh, d, av.hp, t, ii, jj);
+            if ((jj > j0 && jj <= jv && ii <= iv + 3) || (ii > i0 && ii <= iv && jj <= jv + 3))
+                vs[e] = v_ext(y, vh, d, av.hp, t, ii, jj);
+        }
+        // vh on the xy points (c, j): j in (j0, ju], c in [lo, hi] (the i2c rows of the
+        // centres (i0, iu] read these: interior i-1 .. i+2, closures 1..5 and N-3 .. N+1)
+        if (i0 < N) {
+            const int lo = max(1, min(i0, N - 3)), hi = min(n, i0 + TX + 3);
+#pragma unroll 1
+            for (int e = tid; e < TY * WW; e += ADV_THREADS) {
+                const int r = e / WW, c = e % WW;
+                const int ii = i0 - 2 + c, jj = j0 + 1 + r;
+                if (ii >= lo && ii <= hi && jj <= ju) vhs[e] = ic2i<T>(jj, n, [&](int q) { return VT(ii, q); });
+            }
+        }
+        if (j0 < N) {
+            const int lo = max(1, min(j0, N - 3)), hi = min(n, j0 + TY + 3);
+#pragma unroll 1
+            for (int e = tid; e < WH * TX; e += ADV_THREADS) {
+                const int r = e / TX, c = e % TX;
+                const int ii = i0 + 1 + c, jj = j0 - 2 + r;
+                if (jj >= lo && jj <= hi && ii <= iv) uhs[e] = ic2i<T>(ii, n, [&](int q) { return UT(q, jj); });
+            }
+        }
     }
-    if (j <= N) {
-        // v point: u_at_v = I_i2c,y(uh) and vt
-        const T b = __ldg(W + po + 2 * d.fs + o);
-        const GV<T> UHp{PH + po + d.fs, d.P};
-        const T a = ii2c<T>(j, N, [&](int c) { return UHp(i, c); });
-        T fx[7], fy[7];
-        const T *vr = y + t * d.ps + 2 * d.fs + (j - 1 + MG) * d.P + (i - 1 + MG);   // v(i, j)
-        if (i >= 4 && i <= N - 2) {
+    __syncthreads();
+    const int i = i0 + 1 + tx;
+    const int64_t box = d.ps;
+#pragma unroll 1
+    for (int r = threadIdx.y; r < TY; r += ADV_THREADS / TX) {
+        const int j = j0 + 1 + r;
+        const int64_t o = box_off(P, i, j);
+        if (i <= iu && j <= ju) {
+            // u point: ut and v_at_u = I_i2c,x(vh)
+            const T a = __ldg(W + po + d.fs + o);
+            const T *vr = vhs + r * WW - (i0 - 2);
+            const T b = ii2c<T>(i, N, [&](int q) { return vr[q]; });
+            const T *w = us + (r + 3) * WW + (tx + 3);   // u(i, j)
+            T fx[7], fy[7];
 #pragma unroll
-            for (int k = 0; k < 7; k++) fx[k] = __ldg(vr + (k - 3));
-        } else {
-#pragma unroll
-            for (int k = 0; k < 7; k++) fx[k] = v_ext(y, vh, d, av.hp, t, i - 3 + k, j);
+            for (int k = 0; k < 7; k++) {
+                fx[k] = w[k - 3];
+                fy[k] = w[(k - 3) * WW];
+            }
+            const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
+            T tend = -(a * dx + b * dy) * m.inv_hxa;
+            const T g11 = __ldg(av.S + o), g21 = __ldg(av.S + box + o), g22 = __ldg(av.S + 2 * box + o);
+            tend = tend - (a * a * g11 + T(2) * a * b * g21 + b * b * g22) * av.inv_neg_radius;
+            A[po + d.fs + o] = tend;
         }
-        if (j >= 4 && j <= N - 3) {
+        if (i <= iv && j <= jv) {
+            // v point: u_at_v = I_i2c,y(uh) and vt
+            const T b = __ldg(W + po + 2 * d.fs + o);
+            const T *uc = uhs + tx - (j0 - 2) * TX;
+            const T a = ii2c<T>(j, N, [&](int q) { return uc[q * TX]; });
+            const T *w = vs + (r + 3) * WW + (tx + 3);   // v(i, j)
+            T fx[7], fy[7];
 #pragma unroll
-            for (int k = 0; k < 7; k++) fy[k] = __ldg(vr + (k - 3) * d.P);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 7; k++) fy[k] = v_ext(y, vh, d, av.hp, t, i, j - 3 + k);
+            for (int k = 0; k < 7; k++) {
+                fx[k] = w[k - 3];
+                fy[k] = w[(k - 3) * WW];
+            }
+            const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
+            T tend = -(a * dx + b * dy) * m.inv_hxa;
+            const T *S = av.S + 3 * box;
+            const T g11 = __ldg(S + o), g21 = __ldg(S + box + o), g22 = __ldg(S + 2 * box + o);
+            tend = tend - (a * a * g11 + T(2) * a * b * g21 + b * b * g22) * av.inv_neg_radius;
+            A[po + 2 * d.fs + o] = tend;
         }
-        const T dx = up4_diff(a, fx), dy = up4_diff(b, fy);
-        T tend = -(a * dx + b * dy) * m.inv_hxa;
-        const T *S = av.S + 3 * box;
-        const T g11 = __ldg(S + o), g21 = __ldg(S + box + o), g22 = __ldg(S + 2 * box + o);
-        tend = tend - (a * a * g11 + T(2) * a * b * g21 + b * b * g22) / av.neg_radius;
-        A[po + 2 * d.fs + o] = tend;
     }
 }
 

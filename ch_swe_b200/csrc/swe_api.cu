@@ -277,7 +277,7 @@ struct swe_ctx {
     bool adv = false;
     DevAdv<double> a64;
     DevAdv<float> a32;
-    void *fl = nullptr, *adt = nullptr, *ph = nullptr;   // mass flux, advective tendencies, uh/vh (state boxes)
+    void *fl = nullptr, *adt = nullptr;   // mass flux, advective tendencies (state boxes)
     void *fs = nullptr;              // mass-flux edge strips
     void *vh = nullptr;              // covariant wind at the virtual points beyond the panel edges
     void *hb = nullptr;              // panel-boundary h before the in-place averaging
@@ -897,7 +897,7 @@ static int build_adv_tables(swe_ctx *c, DevAdv<T> &da)
     v.xyind = da.ibase;
     v.hsrc = da.ibase + i_src;
     v.hidx = da.ibase + i_idx;
-    v.neg_radius = T(-c->cfg.radius);
+    v.inv_neg_radius = T(-1.0 / c->cfg.radius);
     v.hp = hp;
     return SWE_OK;
 }
@@ -993,7 +993,7 @@ static void free_ctx(swe_ctx *c)
     cudaFree(c->ya); cudaFree(c->yb); cudaFree(c->acc); cudaFree(c->w); cudaFree(c->edge); cudaFree(c->es);
     cudaFree(c->qw); cudaFree(c->red); cudaFree(c->otab); cudaFree(c->ll_i); cudaFree(c->ll_d); cudaFree(c->llo_i); cudaFree(c->llo_d);
     cudaFree(c->a64.base); cudaFree(c->a64.ibase); cudaFree(c->a32.base); cudaFree(c->a32.ibase);
-    cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->ph); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
+    cudaFree(c->fl); cudaFree(c->adt); cudaFree(c->fs); cudaFree(c->vh); cudaFree(c->ones); cudaFree(c->hb);
     cudaFree(c->ah64.base); cudaFree(c->ah32.base); cudaFree(c->qa); cudaFree(c->negones);
     cudaFree(c->dif); cudaFree(c->dif_b);
     cudaFree(c->fmet); cudaFree(c->derr); cudaFree(c->hs); cudaFree(c->cmet);
@@ -1088,7 +1088,7 @@ extern "C" int swe_ctx_create(const swe_cfg *cfg, swe_ctx **out)
         if (cudaMemset(c->es, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
         if (cfg->operator_kind == SWE_OP_ADVECTIVE) {
             c->adv = true;
-            if ((rc = alloc_box(c, &c->fl)) || (rc = alloc_box(c, &c->adt)) || (rc = alloc_box(c, &c->ph))) return bail(rc);
+            if ((rc = alloc_box(c, &c->fl)) || (rc = alloc_box(c, &c->adt))) return bail(rc);
             if (cudaMalloc(&c->fs, sb) != cudaSuccess) return bail(SWE_ENOMEM);
             if (cudaMemset(c->fs, 0, sb) != cudaSuccess) return bail(SWE_ECUDA);
             const size_t vb = (size_t)cfg->n_members * NPAN * vh_points(N) * c->elem;
@@ -1508,6 +1508,22 @@ static bool enqueue_fused(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     return true;
 }
 
+// The advective tendencies (k_advt): tiles of 32 x 16 xy points from C128 on, 32 x 8
+// below (where taller tiles would leave fewer blocks than SMs).
+template <class T>
+static void launch_adv(swe_ctx *c, const void *yin, const AdvView<T> &av, const MetricView<T> &mv, const double *dtm,
+                       cudaStream_t st)
+{
+    const int n = c->cfg.N + 1, M = c->cfg.n_members;
+    const dim3 b(ADV_TX, ADV_THREADS / ADV_TX);
+    if (c->cfg.N >= 128)
+        launch_k(k_advt<T, 16>, dim3((n + ADV_TX - 1) / ADV_TX, (n + 15) / 16, NPAN * M), b, 0, st, (const T *)yin,
+                 (const T *)c->w, (const T *)c->vh, (T *)c->adt, c->dims, av, mv, dtm);
+    else
+        launch_k(k_advt<T, 8>, dim3((n + ADV_TX - 1) / ADV_TX, (n + 7) / 8, NPAN * M), b, 0, st, (const T *)yin,
+                 (const T *)c->w, (const T *)c->vh, (T *)c->adt, c->dims, av, mv, dtm);
+}
+
 template <class T>
 static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void *acc, float *cmp, int mode, double dt,
                           const double *dtm,
@@ -1564,9 +1580,7 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
                             c->stream, dtm)) c->launch_miss = true;
         cudaEventRecord(c->ev_co2, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_co2, 0);
-        launch_k(k_uhvh<T>, pg, pb, 0, c->side, (const T *)c->w, (T *)c->ph, c->dims, dtm);
-        launch_k(k_adv<T>, pg, pb, 0, c->side, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
-                 (T *)c->adt, c->dims, av, mv, dtm);
+        launch_adv<T>(c, yin, av, mv, dtm, c->side);
         cudaEventRecord(c->ev_side, c->side);
         cudaStreamWaitEvent(c->stream, c->ev_havg, 0);
     } else {
@@ -1581,15 +1595,13 @@ static void enqueue_stage(swe_ctx *c, const void *yin, void *v0, void *y1, void 
     if (fork) {
         cudaStreamWaitEvent(c->stream, c->ev_side, 0);
     } else {
-        launch_k(k_uhvh<T>, pg, pb, 0, c->stream, (const T *)c->w, (T *)c->ph, c->dims, dtm);
         launch_k(k_vhalo<T>, vg, dim3(256), 0, c->stream, (const T *)yin, (T *)c->vh, c->dims, av, M, dtm);
-        launch_k(k_adv<T>, pg, pb, 0, c->stream, (const T *)yin, (const T *)c->w, (const T *)c->ph, (const T *)c->vh,
-                 (T *)c->adt, c->dims, av, mv, dtm);
+        launch_adv<T>(c, yin, av, mv, dtm, c->stream);
     }
     StageArgs a{mode, dt, c->ones, dtm, c->fl, c->adt, c->hb, c->hs};
     if (!launch_stage<T>(c->tile, c->occ, c->runs, c->ord, M, (const T *)yin, (const T *)c->w, (const T *)c->edge, (T *)v0, (T *)y1, (T *)acc,
                     (T *)cmp, c->dims, mv, a, c->stream)) c->launch_miss = true;
-    c->launches += 8;
+    c->launches += 7;
 }
 
 static void enqueue_apply(swe_ctx *c, void *out, const void *in)
