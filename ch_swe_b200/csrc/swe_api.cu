@@ -1685,12 +1685,12 @@ extern "C" int swe_c_div(swe_ctx *c, swe_stvec *vout, const swe_stvec *vin)
     return SWE_OK;
 }
 
-// One RK4 step as 8 launches: stage s reads yin and writes y1 (double-buffered).
 template <class T>
 static int enqueue_diffusion(swe_ctx *c, T *y, T *out, double dt, const double *dtm, int lap_order, double uv_coeff,
                              double h_coeff);
 
-// One RK4 step, then the diffusion step when one is set (shallow_water_mod.f90:112-118).
+// One RK4 step (four stages: stage s reads its input and writes the next one, double
+// buffered), then the diffusion step when one is set (shallow_water_mod.f90:112-118).
 static void enqueue_rk4(swe_ctx *c, swe_stvec *v0, double dt, const double *dtm = nullptr)
 {
     void *V = v0->d, *A = c->acc;
